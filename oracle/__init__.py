@@ -1,0 +1,317 @@
+"""CPU oracle for the Gaussian rasterizer hot path -- TEST INFRASTRUCTURE ONLY.
+
+Only ``tests/``, ``__graft_entry__.smoke()`` and the CPU-baseline leg of
+``bench.py`` import this package, always as the checker, never as the thing
+measured or shipped.  The product (``word2world_b200``) never imports it.
+
+``liborc_w2w.so`` (built from ``w2w_oracle.c`` + ``raster_core.h``) restates
+the reference extension ``cudaForwardBackwardRenderer`` in C:
+
+* ``forward``  -- projection.cu, ADRculling.cu, gaussianForwardPass.cu,
+  gaussianRasterizer.cu:77-117, prepareSort.cu, gaussianTiles.cu,
+  pixelGaussiansFull.cu / pixelGaussiansDev.cuh / gaussEval.h;
+* ``backward`` -- backward.cu + gradientPass.cu (``mode="reference"``), or the
+  exact derivative of the forward (``mode="exact"``).
+
+``precision="f32"`` is the bit-level restatement; ``"f64"`` is the same
+algorithm evaluated in double (the fp64 re-evaluation).
+
+Pinning: the fp32 restatement's fusion patterns (``PINNED_VARIANTS``) were
+fixed by comparing against the reference extension run on a B200
+(``tests/golden/make_golden.py`` writes those fixtures; ``tests/test_oracle_golden.py``
+checks the oracle against them).
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+from dataclasses import dataclass
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "liborc_w2w.so")
+
+_FAMILIES = [("RQ", 9), ("SIGMA", 6), ("VIEW_A", 4), ("VIEW_B", 4), ("RAYR2", 1), ("DPROJ", 6), ("SIGV", 6),
+             ("DOT3", 3), ("DET", 1), ("PROJ_A", 4), ("PROJ_B", 4), ("PIX", 2), ("ADR_DELTA", 1), ("BL_DET", 1),
+             ("BL_TX", 1), ("BL_TY", 1), ("BL_NUM", 1), ("BL_DEPTH", 1), ("SH_DOT", 1), ("SH_ACC", 1)]
+VARIANT_NAMES = [f"{n}{i}" if k > 1 else n for n, k in _FAMILIES for i in range(k)]
+# Fusion pattern per expression instance (see raster_core.h s1/s2/d2/s3).
+# Pinned against the reference extension's geometry buffers on a B200
+# (16,384 + 2,048 + 16,384 Gaussians, three cameras): with these values
+# depth, means2D, cov3D, conic/opacity, radii, tiles-touched and offsets are
+# bit-identical.  Pattern 1 (fuse the first product) everywhere except:
+#   RQ0: 2-4(yy+zz) unfused; RQ2: xz+ry fuses r*y; RQ6: xz-ry fuses -r*y;
+#   PIX0/PIX1: the NDC multiply is fused into "+1" and "*W - 0.5" is fused.
+PINNED_VARIANTS = {name: 1 for name in VARIANT_NAMES}
+PINNED_VARIANTS.update({"RQ0": 0, "RQ2": 2, "RQ6": 2, "PIX0": 2, "PIX1": 2})
+
+_lib = None
+
+
+def build(force: bool = False) -> str:
+    if force or not os.path.exists(LIB_PATH) or _stale():
+        subprocess.run(["make", "-s", "-C", HERE, "liborc_w2w.so"], check=True)
+    return LIB_PATH
+
+
+def _stale() -> bool:
+    t = os.path.getmtime(LIB_PATH)
+    return any(os.path.getmtime(os.path.join(HERE, f)) > t for f in ("w2w_oracle.c", "raster_core.h"))
+
+
+class _Cfg(ctypes.Structure):
+    _fields_ = [("W", ctypes.c_int), ("H", ctypes.c_int), ("degree", ctypes.c_int), ("M", ctypes.c_int),
+                ("compat_spill", ctypes.c_int), ("focal_x", ctypes.c_float),
+                ("view", ctypes.c_float * 16), ("proj", ctypes.c_float * 16),
+                ("campos", ctypes.c_float * 3), ("bg", ctypes.c_float * 3)]
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            build()
+        _lib = ctypes.CDLL(LIB_PATH)
+        set_variants(PINNED_VARIANTS)
+    return _lib
+
+
+def set_variants(variants: dict):
+    L = _lib if _lib is not None else lib()
+    for k, v in variants.items():
+        L.orc_set_variant(VARIANT_NAMES.index(k), int(v))
+
+
+def get_variants() -> dict:
+    L = lib()
+    return {n: L.orc_get_variant(i) for i, n in enumerate(VARIANT_NAMES)}
+
+
+def _p(a):
+    return a.ctypes.data_as(ctypes.c_void_p)
+
+
+@dataclass
+class RasterSettings:
+    W: int
+    H: int
+    viewmatrix: np.ndarray
+    projmatrix: np.ndarray
+    campos: np.ndarray
+    focal_x: float
+    degree: int = 3
+    bg: tuple = (1.0, 1.0, 1.0)
+    compat_spill: bool = True
+    tan_fovx: float | None = None
+    tan_fovy: float | None = None
+
+    @staticmethod
+    def from_camera(cam, degree=3, bg=(1.0, 1.0, 1.0), compat_spill=True):
+        return RasterSettings(W=cam.width, H=cam.height, viewmatrix=cam.viewmatrix, projmatrix=cam.projmatrix,
+                              campos=cam.campos, focal_x=cam.focal_x, degree=degree, bg=bg,
+                              compat_spill=compat_spill, tan_fovx=cam.tanfovx, tan_fovy=cam.tanfovy)
+
+    def cstruct(self, M: int) -> _Cfg:
+        c = _Cfg()
+        c.W, c.H, c.degree, c.M = self.W, self.H, self.degree, M
+        c.compat_spill = 1 if self.compat_spill else 0
+        c.focal_x = np.float32(self.focal_x)
+        for i, v in enumerate(np.asarray(self.viewmatrix, np.float32).reshape(-1)):
+            c.view[i] = v
+        for i, v in enumerate(np.asarray(self.projmatrix, np.float32).reshape(-1)):
+            c.proj[i] = v
+        for i in range(3):
+            c.campos[i] = float(np.float32(self.campos[i]))
+            c.bg[i] = float(np.float32(self.bg[i]))
+        return c
+
+
+def _f(a, dt=np.float32):
+    return np.ascontiguousarray(a, dtype=dt)
+
+
+def preprocess(s: RasterSettings, means3D, scales, rotations, opacities, shs, precision: str = "f32") -> dict:
+    """Per-Gaussian stage only (projection, ADR culling, SH colour)."""
+    L = lib()
+    sfx = "_f32" if precision == "f32" else "_f64"
+    R_ = np.float32 if precision == "f32" else np.float64
+    means3D, scales, rotations = _f(means3D), _f(scales), _f(rotations)
+    opac = _f(opacities).reshape(-1)
+    shs = _f(shs)
+    P = means3D.shape[0]
+    M = shs.shape[1] if shs.ndim == 3 and shs.shape[0] > 0 else 0
+    cfg = s.cstruct(M)
+    out = dict(
+        cov3D=np.zeros((P, 6), R_), cov2D=np.zeros((P, 3), R_), det=np.zeros(P, R_),
+        conic_opac=np.zeros((P, 4), R_), means2D=np.zeros((P, 2), R_), depth=np.zeros(P, R_),
+        radii=np.zeros(P, np.int32), tiles=np.zeros(P, np.uint32), rects=np.zeros((P, 4), np.int32),
+        rgb=np.zeros((P, 3), R_), clamped=np.zeros((P, 3), np.uint8), visible=np.zeros(P, np.uint8),
+        clamp_hit=np.zeros(P, np.uint8), adr_margin=np.zeros(P, np.float64))
+    getattr(L, "orc_preprocess" + sfx)(
+        ctypes.byref(cfg), ctypes.c_int(P), _p(means3D), _p(scales), _p(rotations), _p(opac), _p(shs),
+        _p(out["cov3D"]), _p(out["cov2D"]), _p(out["det"]), _p(out["conic_opac"]), _p(out["means2D"]),
+        _p(out["depth"]), _p(out["radii"]), _p(out["tiles"]), _p(out["rects"]), _p(out["rgb"]),
+        _p(out["clamped"]), _p(out["visible"]), _p(out["clamp_hit"]), _p(out["adr_margin"]))
+    return out
+
+
+def forward(s: RasterSettings, means3D, scales, rotations, opacities, shs, precision: str = "f32") -> dict:
+    """Full forward.  Returns every intermediate the reference keeps
+    (geometry, binning and image state) plus the images."""
+    L = lib()
+    sfx = "_f32" if precision == "f32" else "_f64"
+    R_ = np.float32 if precision == "f32" else np.float64
+    means3D, scales, rotations = _f(means3D), _f(scales), _f(rotations)
+    opac = _f(opacities).reshape(-1)
+    shs = _f(shs)
+    P = means3D.shape[0]
+    M = shs.shape[1] if shs.ndim == 3 and shs.shape[0] > 0 else 0
+    cfg = s.cstruct(M)
+    out = dict(
+        cov3D=np.zeros((P, 6), R_), cov2D=np.zeros((P, 3), R_), det=np.zeros(P, R_),
+        conic_opac=np.zeros((P, 4), R_), means2D=np.zeros((P, 2), R_), depth=np.zeros(P, R_),
+        radii=np.zeros(P, np.int32), tiles=np.zeros(P, np.uint32), rects=np.zeros((P, 4), np.int32),
+        rgb=np.zeros((P, 3), R_), clamped=np.zeros((P, 3), np.uint8), visible=np.zeros(P, np.uint8),
+        clamp_hit=np.zeros(P, np.uint8), adr_margin=np.zeros(P, np.float64))
+    getattr(L, "orc_preprocess" + sfx)(
+        ctypes.byref(cfg), ctypes.c_int(P), _p(means3D), _p(scales), _p(rotations), _p(opac), _p(shs),
+        _p(out["cov3D"]), _p(out["cov2D"]), _p(out["det"]), _p(out["conic_opac"]), _p(out["means2D"]),
+        _p(out["depth"]), _p(out["radii"]), _p(out["tiles"]), _p(out["rects"]), _p(out["rgb"]),
+        _p(out["clamped"]), _p(out["visible"]), _p(out["clamp_hit"]), _p(out["adr_margin"]))
+    offsets = np.zeros(P, np.uint32)
+    L.orc_inclusive_scan_u32(_p(out["tiles"]), _p(offsets), ctypes.c_longlong(P))
+    R = int(offsets[-1]) if P else 0
+    keys = np.zeros(max(R, 1), np.uint64)
+    vals = np.zeros(max(R, 1), np.uint32)
+    cand = np.zeros(max(R, 1), np.int32)
+    fn = getattr(L, "orc_emit" + sfx)
+    fn.restype = ctypes.c_longlong
+    dropped = fn(ctypes.byref(cfg), ctypes.c_int(P), _p(out["means2D"]), _p(out["depth"]), _p(out["radii"]),
+                 _p(out["rects"]), _p(offsets), ctypes.c_longlong(R), _p(keys), _p(vals), _p(cand))
+    keys, vals, cand = keys[:R], vals[:R], cand[:R]
+    unsorted_keys, unsorted_vals = keys.copy(), vals.copy()
+    L.orc_sort_pairs_u64(_p(keys), _p(vals), ctypes.c_longlong(R))
+    gw, gh = (s.W + 15) // 16, (s.H + 15) // 16
+    ranges = np.zeros((gw * gh, 2), np.uint32)
+    L.orc_tile_ranges(_p(keys), ctypes.c_longlong(R), _p(ranges), ctypes.c_int(gw * gh))
+    HW = s.H * s.W
+    color = np.zeros((3, s.H, s.W), R_)
+    depth_img = np.zeros((1, s.H, s.W), R_)
+    alpha = np.zeros((1, s.H, s.W), R_)
+    n_contrib = np.zeros(HW, np.uint32)
+    T_final = np.zeros(HW, R_)
+    margin = np.zeros(HW, np.float64)
+    sig = np.zeros(HW, np.uint64)
+    getattr(L, "orc_blend" + sfx)(
+        ctypes.byref(cfg), _p(ranges), _p(vals if R else np.zeros(1, np.uint32)), _p(out["means2D"]),
+        _p(out["cov2D"]), _p(out["conic_opac"]), _p(out["rgb"]), _p(out["depth"]), _p(color), _p(depth_img),
+        _p(alpha), _p(n_contrib), _p(T_final), _p(margin), _p(sig))
+    out.update(offsets=offsets, num_rendered=R, unsorted_keys=unsorted_keys, unsorted_vals=unsorted_vals,
+               candidates=cand, spill_dropped=int(dropped), keys=keys, point_list=vals, ranges=ranges,
+               color=color, depth_img=depth_img, alpha=alpha, n_contrib=n_contrib.reshape(s.H, s.W),
+               T_final=T_final.reshape(s.H, s.W), blend_margin=margin.reshape(s.H, s.W),
+               blend_signature=sig.reshape(s.H, s.W),
+               settings=s, precision=precision, P=P, M=M,
+               inputs=dict(means3D=means3D, scales=scales, rotations=rotations, opacities=opac, shs=shs))
+    return out
+
+
+def blend(s: RasterSettings, geom: dict, ranges, point_list, precision: str = "f32") -> dict:
+    """Blend stage alone, from given per-tile ranges and sorted Gaussian ids
+    (used to replay another implementation's binning)."""
+    L = lib()
+    sfx = "_f32" if precision == "f32" else "_f64"
+    R_ = np.float32 if precision == "f32" else np.float64
+    cfg = s.cstruct(0)
+    HW = s.H * s.W
+    color = np.zeros((3, s.H, s.W), R_)
+    depth_img = np.zeros((1, s.H, s.W), R_)
+    alpha = np.zeros((1, s.H, s.W), R_)
+    n_contrib = np.zeros(HW, np.uint32)
+    T_final = np.zeros(HW, R_)
+    margin = np.zeros(HW, np.float64)
+    sig = np.zeros(HW, np.uint64)
+    ranges = np.ascontiguousarray(ranges, np.uint32)
+    pl = np.ascontiguousarray(point_list, np.uint32) if len(point_list) else np.zeros(1, np.uint32)
+    getattr(L, "orc_blend" + sfx)(
+        ctypes.byref(cfg), _p(ranges), _p(pl), _p(_f(geom["means2D"], R_)), _p(_f(geom["cov2D"], R_)),
+        _p(_f(geom["conic_opac"], R_)), _p(_f(geom["rgb"], R_)), _p(_f(geom["depth"], R_)), _p(color),
+        _p(depth_img), _p(alpha), _p(n_contrib), _p(T_final), _p(margin), _p(sig))
+    return dict(color=color, depth_img=depth_img, alpha=alpha, n_contrib=n_contrib.reshape(s.H, s.W),
+                T_final=T_final.reshape(s.H, s.W), blend_margin=margin.reshape(s.H, s.W),
+                blend_signature=sig.reshape(s.H, s.W))
+
+
+def backward(fwd: dict, dL_dcolor, dL_ddepth=None, dL_dalpha=None, mode: str = "reference",
+             tan_fovx: float | None = None, tan_fovy: float | None = None, scale_modifier: float = 1.0) -> dict:
+    """Gradients for the forward ``fwd``.  Returns the eight tensors of
+    ``rasterize_gaussians_backward`` (rasterize_points.cu:139-148) by name."""
+    L = lib()
+    s: RasterSettings = fwd["settings"]
+    prec = fwd["precision"]
+    sfx = "_f32" if prec == "f32" else "_f64"
+    R_ = np.float32 if prec == "f32" else np.float64
+    P, M = fwd["P"], fwd["M"]
+    H, W = s.H, s.W
+    cfg = s.cstruct(M)
+    inp = fwd["inputs"]
+    dLc = _f(dL_dcolor)
+    dLd = _f(np.zeros((1, H, W)) if dL_ddepth is None else dL_ddepth)
+    dLa = _f(np.zeros((1, H, W)) if dL_dalpha is None else dL_dalpha)
+    pl = fwd["point_list"] if fwd["num_rendered"] else np.zeros(1, np.uint32)
+    g = dict(dL_dmeans2D=np.zeros((P, 3), R_), dL_dcolors=np.zeros((P, 3), R_), dL_dopacity=np.zeros((P, 1), R_),
+             dL_dmeans3D=np.zeros((P, 3), R_), dL_dcov3D=np.zeros((P, 6), R_), dL_dsh=np.zeros((P, M, 3), R_),
+             dL_dscales=np.zeros((P, 3), R_), dL_drotations=np.zeros((P, 4), R_))
+    if mode == "reference":
+        dm2 = np.zeros((P, 3)); dcon = np.zeros((P, 4)); dop = np.zeros(P); dcol = np.zeros((P, 3)); ddep = np.zeros(P)
+        getattr(L, "orc_backward_render" + sfx)(
+            ctypes.byref(cfg), _p(fwd["ranges"]), _p(pl), _p(fwd["means2D"]), _p(fwd["conic_opac"]),
+            _p(fwd["rgb"]), _p(fwd["depth"]), _p(np.ascontiguousarray(fwd["alpha"].reshape(-1))),
+            _p(np.ascontiguousarray(fwd["n_contrib"].reshape(-1))), _p(dLc), _p(dLd), _p(dLa),
+            _p(dm2), _p(dcon), _p(dop), _p(dcol), _p(ddep))
+        tfx = s.tan_fovx if tan_fovx is None else tan_fovx
+        tfy = s.tan_fovy if tan_fovy is None else tan_fovy
+        h_x = np.float32(W) / (np.float32(2.0) * np.float32(tfx))
+        h_y = np.float32(H) / (np.float32(2.0) * np.float32(tfy))
+        dconR = dcon.astype(R_)
+        CT = ctypes.c_float if prec == "f32" else ctypes.c_double
+        getattr(L, "orc_backward_cov2d" + sfx)(
+            ctypes.c_int(P), _p(inp["means3D"]), _p(fwd["radii"]), _p(fwd["cov3D"]), CT(h_x), CT(h_y),
+            CT(np.float32(tfx)), CT(np.float32(tfy)), _p(_f(s.viewmatrix).reshape(-1)), _p(dconR),
+            _p(g["dL_dcov3D"]), _p(g["dL_dmeans3D"]))
+        g["dL_dmeans2D"][:] = dm2.astype(R_)
+        g["dL_dcolors"][:] = dcol.astype(R_)
+        g["dL_dopacity"][:, 0] = dop.astype(R_)
+        ddepR = ddep.astype(R_)
+        getattr(L, "orc_backward_preprocess" + sfx)(
+            ctypes.c_int(P), ctypes.c_int(M), _p(inp["means3D"]), _p(fwd["radii"]), _p(inp["shs"]),
+            _p(fwd["clamped"]), _p(inp["scales"]), _p(inp["rotations"]), CT(scale_modifier),
+            _p(_f(s.viewmatrix).reshape(-1)), _p(_f(s.projmatrix).reshape(-1)), _p(_f(s.campos)),
+            _p(g["dL_dmeans2D"]), _p(g["dL_dcolors"]), _p(ddepR), _p(g["dL_dcov3D"]),
+            _p(g["dL_dmeans3D"]), _p(g["dL_dsh"]), _p(g["dL_dscales"]), _p(g["dL_drotations"]))
+        g["dL_dconic"] = dconR
+        g["dL_ddepths"] = ddepR
+    elif mode == "exact":
+        getattr(L, "orc_backward_exact" + sfx)(
+            ctypes.byref(cfg), ctypes.c_int(P), _p(inp["means3D"]), _p(inp["scales"]), _p(inp["rotations"]),
+            _p(inp["opacities"]), _p(inp["shs"]), _p(fwd["ranges"]), _p(pl), _p(fwd["means2D"]),
+            _p(fwd["cov2D"]), _p(fwd["cov3D"]), _p(fwd["rgb"]), _p(fwd["depth"]), _p(fwd["radii"]),
+            _p(np.ascontiguousarray(fwd["T_final"].reshape(-1))),
+            _p(np.ascontiguousarray(fwd["n_contrib"].reshape(-1))), _p(dLc), _p(dLd), _p(dLa),
+            _p(g["dL_dmeans2D"]), _p(g["dL_dcolors"]), _p(g["dL_dopacity"]), _p(g["dL_dmeans3D"]),
+            _p(g["dL_dcov3D"]), _p(g["dL_dsh"]), _p(g["dL_dscales"]), _p(g["dL_drotations"]))
+    else:
+        raise ValueError(mode)
+    return g
+
+
+def scalar_loss(fwd: dict, dL_dcolor, dL_ddepth=None, dL_dalpha=None) -> float:
+    """L = <dL/dC, C> + <dL/dD, D> + <dL/dA, A> in double (for finite differences)."""
+    L_ = float(np.sum(np.asarray(fwd["color"], np.float64) * np.asarray(dL_dcolor, np.float64)))
+    if dL_ddepth is not None:
+        L_ += float(np.sum(np.asarray(fwd["depth_img"], np.float64) * np.asarray(dL_ddepth, np.float64)))
+    if dL_dalpha is not None:
+        L_ += float(np.sum(np.asarray(fwd["alpha"], np.float64) * np.asarray(dL_dalpha, np.float64)))
+    return L_
