@@ -1,0 +1,171 @@
+/*
+ * w2w_raster.h -- C ABI of the sm_100a Gaussian rasterizer.
+ *
+ * Drop-in replacement for the rasterizer path of Word2World's
+ * cudaForwardBackwardRenderer extension: the forward is
+ * RasterizeGaussiansCUDA / gaussianForwardPass, the backward
+ * RasterizeGaussiansBackwardCUDA / backward.  Plain C types only: device
+ * pointers, sizes and a CUDA stream.  Every device buffer -- inputs, outputs
+ * and the three opaque state buffers -- is allocated by the caller; the
+ * library never allocates device memory and never synchronises the device
+ * except where stated (w2w_forward_geometry reads one 16-byte header back to
+ * the host, as the reference reads R back, prepareSort.cu:382-387).
+ *
+ * Conventions (identical to the reference):
+ *   means3D [P,3], scales [P,3] (activated), rotations [P,4] (w,x,y,z,
+ *   normalised), opacities [P] (activated), shs [P,M,3] (RGB innermost);
+ *   viewmatrix / projmatrix: 16 floats read column-major (the transposed
+ *   matrices the reference trainer passes); campos = minus the camera
+ *   position; image outputs are CHW float32; radii int32[P].
+ *
+ * Status codes: 0 ok, otherwise a W2W_ERR_* value (w2w_status_string()).
+ */
+#ifndef W2W_RASTER_H
+#define W2W_RASTER_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct CUstream_st* w2w_stream_t; /* a cudaStream_t; NULL = legacy default stream */
+
+enum {
+    W2W_OK = 0,
+    W2W_ERR_INVALID = 1,   /* bad argument (null pointer, negative size, mismatched state) */
+    W2W_ERR_CUDA = 2,      /* a CUDA launch or runtime call failed */
+    W2W_ERR_CAPACITY = 3,  /* instance count exceeds what the state buffer was sized for */
+    W2W_ERR_TIMEOUT = 4,   /* a bounded device-side wait gave up (results invalid) */
+    W2W_ERR_SCRATCH = 5    /* scratch buffer smaller than required */
+};
+
+/* Camera and image settings.  Pointer fields are device pointers. */
+typedef struct {
+    int P;                   /* number of Gaussians */
+    int degree;              /* SH degree evaluated (0..3) */
+    int M;                   /* SH coefficients stored per Gaussian */
+    int width, height;       /* image size (the reference fixes 800x800) */
+    float focal_x;           /* forward Jacobian focal length, pixels (both axes, as the reference) */
+    float tan_fovx, tan_fovy;/* backward: focal = width / (2 tan_fovx) (gradientPass.cu:119-120) */
+    float scale_modifier;    /* backward scale multiplier (backward.cu:463) */
+    int compat_spill;        /* 1: the reference's key-emission rectangle (see w2w_forward_render) */
+    const float* viewmatrix; /* [16] */
+    const float* projmatrix; /* [16] */
+    const float* campos;     /* [3] */
+    const float* background; /* [3]; the reference forward hard-codes white */
+} w2w_settings;
+
+/* Returned by the geometry phase; sizes the binning state and the sort. */
+typedef struct {
+    long long num_rendered;   /* R: sum of tiles touched (the reference's num_rendered) */
+    uint32_t depth_min_bits;  /* range of the depth bits of Gaussians that emit keys */
+    uint32_t depth_max_bits;
+    uint32_t error;           /* device error bits (0 = none) */
+    uint32_t reserved;
+} w2w_geometry_info;
+
+int w2w_version(void);
+const char* w2w_status_string(int status);
+
+/* ---- state buffer sizes (bytes; caller allocates device memory) ------------
+ * Replace the resize callbacks of rasterize_points.cu:81-87 and the
+ * cudaMalloc'd temporaries of gaussianRasterizer.cu:209-212. */
+size_t w2w_geometry_state_bytes(int P);
+size_t w2w_image_state_bytes(int width, int height);
+size_t w2w_binning_state_bytes(long long num_rendered, int width, int height);
+size_t w2w_backward_scratch_bytes(int P);
+
+/* Offsets (bytes) of named arrays inside the state buffers, for inspection
+ * and parity tests.  Returns (size_t)-1 for an unknown name.
+ *   geometry: "depth","clamped","means2D","cov3D","conic_opacity","rgb",
+ *             "tiles_touched","offsets","rect","prev_reach","record","header"
+ *   image:    "n_contrib","ranges","T_final","tile_max"
+ *   binning:  "header","keys_a","keys_b","vals_a","vals_b" */
+size_t w2w_geometry_offset(int P, const char* name);
+size_t w2w_image_offset(int width, int height, const char* name);
+size_t w2w_binning_offset(long long num_rendered, int width, int height, const char* name);
+
+/* ---- forward --------------------------------------------------------------
+ * Phase 1 (replaces projection.cu ProjectG, ADRculling.cu tileCulling,
+ * gaussianForwardPass.cu calcColour and the scan of gaussianRasterizer.cu:233,
+ * i.e. gaussianForwardPass, gaussianRasterizer.cu:118-237): one fused kernel.  Writes radii and
+ * the geometry state, then reads the instance count and depth-bit range back
+ * into *info (synchronising `stream` once). */
+int w2w_forward_geometry(const w2w_settings* s, const float* means3D, const float* scales,
+                         const float* rotations, const float* opacities, const float* shs,
+                         int* radii, void* geom_state, w2w_geometry_info* info, w2w_stream_t stream);
+
+/* Phase 2 (replaces prepareAndSort, prepareSort.cu:362-435, gaussianTiles,
+ * gaussianTiles.cu:6-33, and pixelGaussiansFull, pixelGaussiansFull.cu:99-122):
+ * key emission, onesweep radix sort, tile ranges, blending.  binning_state
+ * must be w2w_binning_state_bytes(info->num_rendered, W, H) long.  Sort keys
+ * keep only the bits in which keys can differ (tile bits and the low depth
+ * bits below the depths' common prefix), packed into 32 bits when they fit;
+ * the order equals that of the reference's 64-bit (tile << 32 | depth bits)
+ * keys.  With
+ * compat_spill=1 keys are emitted over the reference's emission rectangle;
+ * where that writes past a Gaussian's allocation the lowest-index writer owns
+ * each slot (the reference leaves this to a race).  Outputs: color [3,H,W],
+ * depth [1,H,W], alpha [1,H,W] (sum of alpha*T, as the reference). */
+int w2w_forward_render(const w2w_settings* s, const void* geom_state, const w2w_geometry_info* info,
+                       void* binning_state, void* image_state, float* out_color, float* out_depth,
+                       float* out_alpha, w2w_stream_t stream);
+
+/* Device error word of a geometry / binning state (synchronises `stream`). */
+int w2w_state_error(const void* state, int which /* 0 geometry, 1 binning */, w2w_stream_t stream);
+
+/* ---- backward -------------------------------------------------------------
+ * Replaces RasterizeGaussiansBackwardCUDA (rasterize_points.cu:158-246) and
+ * backward (gradientPass.cu:26-207).  grad_mode 0 = the reference's formulas,
+ * 1 = the exact derivative of the forward.  All eight outputs are fully
+ * written (no pre-zeroing needed); dL_dmeans2D is [P,3] with the third
+ * component 0; dL_dcov3D is [P,6]; dL_dsh is [P,M,3]. */
+int w2w_backward(const w2w_settings* s, const float* means3D, const float* scales, const float* rotations,
+                 const float* shs, const int* radii, const void* geom_state,
+                 long long num_rendered, const void* binning_state, const void* image_state,
+                 const float* out_alpha, const float* dL_dcolor, const float* dL_ddepth,
+                 const float* dL_dalpha, int grad_mode, void* scratch, size_t scratch_bytes,
+                 float* dL_dmeans2D, float* dL_dcolors, float* dL_dopacity, float* dL_dmeans3D,
+                 float* dL_dcov3D, float* dL_dsh, float* dL_dscales, float* dL_drotations,
+                 w2w_stream_t stream);
+
+/* ---- stages ---------------------------------------------------------------
+ * Stable sort of (uint64 key, uint32 value) pairs on key bits
+ * [begin_bit, end_bit).  Replaces radix_sort_2bit_coalesced
+ * (prepareSort.cu:303-360).  keys_out/vals_out may not alias the inputs. */
+size_t w2w_sort_scratch_bytes(long long n);
+int w2w_sort_pairs_u64(const uint64_t* keys_in, const uint32_t* vals_in, uint64_t* keys_out,
+                       uint32_t* vals_out, long long n, int begin_bit, int end_bit, void* scratch,
+                       size_t scratch_bytes, w2w_stream_t stream);
+
+/* Inclusive / exclusive scan of uint32 values (single-pass decoupled
+ * lookback).  Replaces kogge_stone_inclusive_scan_shared_memory
+ * (gaussianRasterizer.cu:77-117). */
+size_t w2w_scan_scratch_bytes(long long n);
+int w2w_scan_u32(const uint32_t* in, uint32_t* out, long long n, int exclusive, void* scratch,
+                 size_t scratch_bytes, w2w_stream_t stream);
+
+/* Per-tile [start, end) from sorted keys whose tile id is key >> tile_shift
+ * (gaussianTiles.cu:6-33); tiles without entries get (0, 0). */
+int w2w_tile_ranges(const uint64_t* sorted_keys, long long n, int tile_shift, uint32_t* ranges,
+                    int num_tiles, w2w_stream_t stream);
+
+/* Blend from a given sorted Gaussian list and tile ranges (the reference's
+ * pixelGaussiansFull on its own inputs), writing the image state fields
+ * ranges (a copy), n_contrib, T_final and tile_max and the three images. */
+int w2w_blend(const w2w_settings* s, const void* geom_state, const uint32_t* ranges,
+              const uint32_t* point_list, void* image_state, float* out_color, float* out_depth,
+              float* out_alpha, w2w_stream_t stream);
+
+/* Copy the sorted keys, expanded to the reference's 64-bit layout
+ * (tile << 32 | depth bits), out of a binning state. */
+int w2w_binning_keys64(const void* binning_state, long long num_rendered, int width, int height,
+                       uint64_t* out, w2w_stream_t stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* W2W_RASTER_H */

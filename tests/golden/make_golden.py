@@ -108,10 +108,12 @@ def case_list():
                                    cam=dict(az=200.0, el=-15.0, r=2.5), size=800, degree=3, grads="all")
     c["crop128_1k_small"] = dict(scene=dict(P=1024, seed=5, layout="shell"), cam=dict(az=45.0, el=10.0, r=2.5),
                                  size=128, degree=3, grads="all")
+    c["native800_1k_far"] = dict(scene=dict(P=1024, seed=13, layout="shell"), cam=dict(az=120.0, el=-20.0, r=6.0),
+                                 size=800, degree=3, grads="all")
     return c
 
 
-SMALL_CASES = ["crop128_1k_small"]
+SMALL_CASES = ["crop128_1k_small", "native800_1k_far"]
 
 
 def build_case(spec):
@@ -163,11 +165,17 @@ def run_case(ref, name, spec, full: bool, repeats: int = 3):
     names = ["dL_dmeans2D", "dL_dcolors", "dL_dopacity", "dL_dmeans3D", "dL_dcov3D", "dL_dsh", "dL_dscales",
              "dL_drotations"]
     res = dict(P=P, R=int(R), size=S, degree=spec["degree"], radii=radii.cpu().numpy())
-    crop = slice(0, FRAME) if full else slice(0, S)
-    res["color"] = color.cpu().numpy()[:, crop, crop]
-    res["depth_img"] = depth.cpu().numpy()[:, crop, crop]
-    res["alpha"] = alpha.cpu().numpy()[:, crop, crop]
-    res["n_contrib"] = im["n_contrib"][crop, crop]
+    if full:
+        y0, y1, x0, x1 = 0, FRAME, 0, FRAME
+    else:  # the tile-aligned box of non-empty pixels (everything else is background)
+        nz = np.nonzero(im["n_contrib"][:S, :S])
+        y0, y1 = int(nz[0].min()) // 16 * 16, (int(nz[0].max()) // 16 + 1) * 16
+        x0, x1 = int(nz[1].min()) // 16 * 16, (int(nz[1].max()) // 16 + 1) * 16
+    res["img_box"] = np.array([y0, y1, x0, x1])
+    res["color"] = color.cpu().numpy()[:, y0:y1, x0:x1]
+    res["depth_img"] = depth.cpu().numpy()[:, y0:y1, x0:x1]
+    res["alpha"] = alpha.cpu().numpy()[:, y0:y1, x0:x1]
+    res["n_contrib"] = im["n_contrib"][y0:y1, x0:x1]
     res["ranges"] = im["ranges"]
     for k, v in g.items():
         res["geom_" + k] = v

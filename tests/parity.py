@@ -56,3 +56,53 @@ def spill_classes(ref_keys, ref_vals, orc_keys, orc_vals, candidates) -> dict:
     cand = candidates[:R]
     return dict(R=int(R), n_diff=int(diff.sum()), n_diff_single=int((diff & (cand <= 1)).sum()),
                 n_multi=int((cand > 1).sum()), n_diff_multi=int((diff & (cand > 1)).sum()))
+
+
+GEOM_FIELDS = ["depth", "means2D", "cov3D", "conic_opac", "rgb", "tiles", "offsets"]
+
+
+def geometry_mismatches(mine: dict, orc: dict, visible=None) -> dict:
+    """Bit mismatches per geometry field (float fields compared as fp32 bits).
+    ``visible``: only Gaussians that passed the projection are compared for
+    fields the reference leaves unwritten for culled ones."""
+    out = {}
+    for k in GEOM_FIELDS:
+        a, b = np.asarray(mine[k]), np.asarray(orc[k])
+        if b.dtype.kind == "f":
+            b = b.astype(np.float32)
+        if visible is not None and k not in ("cov3D", "tiles", "offsets"):
+            a, b = a[visible], b[visible]
+        out[k] = bit_mismatch(a, b)
+    out["radii"] = bit_mismatch(mine["radii"], orc["radii"])
+    if "clamped" in mine and "clamped" in orc:
+        out["clamped"] = bit_mismatch(mine["clamped"], orc["clamped"])
+    return out
+
+
+def ncontrib_check(mine_nc, orc_nc, orc_margin, margin=1e-5):
+    """Contributor counts must match except at pixels whose blend decisions
+    sit within ``margin`` (relative) of an alpha or transmittance threshold,
+    where the device exp and the C library's exp may round differently."""
+    diff = np.asarray(mine_nc) != np.asarray(orc_nc)
+    unexplained = diff & (np.asarray(orc_margin) >= margin)
+    return dict(n_diff=int(diff.sum()), n_unexplained=int(unexplained.sum()), n=int(diff.size), mask=diff)
+
+
+def grad_check(a, b, row_rtol=1e-3) -> dict:
+    """Gradient agreement of ``a`` with ``b``.  Elementwise bound
+    |a-b| <= ATOL + RTOL*|b| + row_rtol * max|b over the same Gaussian|: the
+    last term covers components that cancel to much less than their
+    Gaussian's other components, where fp32 accumulation order dominates."""
+    a = np.asarray(a, np.float64).reshape(len(a), -1)
+    b = np.asarray(b, np.float64).reshape(len(b), -1)
+    d = np.abs(a - b)
+    row = np.abs(b).max(axis=1, keepdims=True) if b.size else b
+    tol = ATOL + RTOL * np.abs(b) + row_rtol * row
+    nb = float(np.linalg.norm(b.ravel())) or 1.0
+    return dict(norm_rel=float(np.linalg.norm((a - b).ravel()) / nb), n_bad=int((d > tol).sum()),
+                n_elem_strict=int((d > ATOL + RTOL * np.abs(b)).sum()), max_abs=float(d.max()) if d.size else 0.0,
+                n=int(d.size))
+
+
+GRAD_NAMES = ["dL_dmeans2D", "dL_dcolors", "dL_dopacity", "dL_dmeans3D", "dL_dcov3D", "dL_dsh", "dL_dscales",
+              "dL_drotations"]

@@ -1,0 +1,63 @@
+"""The C-ABI library loads and exports every function include/w2w_raster.h
+declares; host-only entry points behave (no GPU needed, no kernel launched)."""
+import ctypes
+import os
+import re
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+HEADER = os.path.join(ROOT, "include", "w2w_raster.h")
+LIB = os.path.join(ROOT, "word2world_b200", "libw2w_raster.so")
+
+
+def declared_functions():
+    text = open(HEADER).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(w2w_[A-Za-z0-9_]+)\s*\(", text)))
+
+
+@pytest.fixture(scope="module")
+def lib():
+    if not os.path.exists(LIB):
+        import word2world_b200.build as b
+        b.build_lib()
+    return ctypes.CDLL(LIB)
+
+
+def test_exports_every_declared_symbol(lib):
+    names = declared_functions()
+    assert len(names) >= 15
+    missing = [n for n in names if not hasattr(lib, n)]
+    assert not missing, missing
+
+
+def test_host_only_entry_points(lib):
+    lib.w2w_status_string.restype = ctypes.c_char_p
+    assert lib.w2w_version() >= 1
+    assert lib.w2w_status_string(0) == b"ok"
+    assert b"invalid" in lib.w2w_status_string(1)
+    for fn in ("w2w_geometry_state_bytes",):
+        getattr(lib, fn).restype = ctypes.c_size_t
+    lib.w2w_image_state_bytes.restype = ctypes.c_size_t
+    lib.w2w_binning_state_bytes.restype = ctypes.c_size_t
+    lib.w2w_sort_scratch_bytes.restype = ctypes.c_size_t
+    lib.w2w_geometry_offset.restype = ctypes.c_size_t
+    a, b = lib.w2w_geometry_state_bytes(1000), lib.w2w_geometry_state_bytes(2000)
+    assert 0 < a < b and a % 256 == 0
+    assert lib.w2w_image_state_bytes(256, 256) > 0
+    assert lib.w2w_binning_state_bytes(ctypes.c_longlong(100000), 256, 256) > 100000 * 24
+    for name in (b"depth", b"means2D", b"cov3D", b"conic_opacity", b"rgb", b"tiles_touched", b"offsets", b"record"):
+        off = lib.w2w_geometry_offset(1000, name)
+        assert off % 256 == 0 and off < a
+    assert lib.w2w_geometry_offset(1000, b"nope") == ctypes.c_size_t(-1).value
+
+
+def test_invalid_arguments_rejected_without_gpu(lib):
+    # null settings / negative sizes are rejected before any CUDA call
+    assert lib.w2w_forward_geometry(None, None, None, None, None, None, None, None, None, None) == 1
+    assert lib.w2w_sort_pairs_u64(None, None, None, None, ctypes.c_longlong(-1), 0, 64, None, ctypes.c_size_t(0),
+                                  None) == 1
+    assert lib.w2w_sort_pairs_u64(None, None, None, None, ctypes.c_longlong(0), 0, 64, None, ctypes.c_size_t(0),
+                                  None) == 0
+    assert lib.w2w_scan_u32(None, None, ctypes.c_longlong(-5), 0, None, ctypes.c_size_t(0), None) == 1

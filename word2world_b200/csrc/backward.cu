@@ -1,0 +1,659 @@
+// Backward pass.
+//
+// Per-pixel pass (reference backward.cu:521-665): one CTA per tile, pixels
+// walk the tile's list back to front, recomputing each pair's alpha from the
+// stored state (final transmittance and last-contributor index) instead of
+// storing per-pair values.  Each entry's per-pixel contributions are summed
+// across the warp with shuffles and added with one atomic per warp (the
+// reference issues ten atomics per pixel-Gaussian pair).  A tile starts at its
+// largest contributor count: entries past it are skipped by every pixel.
+//
+// Per-Gaussian pass: the reference's computeCov2DCUDA (backward.cu:27-227) and
+// backwardPreprocessingKernel (backward.cu:229-519) fused into one thread per
+// Gaussian.
+//
+// grad_mode 0 reproduces the reference's formulas, including where they are
+// not the derivative of its forward (+0.3 on the 2-D covariance, a 1.3*tan box
+// clamp, colour-clamp masks, SH_C2[2] = 0.3154 and all 16 SH bands).  grad_mode
+// 1 is the exact derivative of the forward: the pair set is re-derived with the
+// forward's own Gaussian evaluation and the forward's final transmittance.
+#include "common.cuh"
+#include "kernels.h"
+
+namespace w2w {
+namespace {
+
+constexpr int kValues = 10;
+
+__device__ __forceinline__ float warp_sum(float v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+__device__ __forceinline__ void flush(const float (&c)[kValues], bool any_contrib, uint32_t id, int mode,
+                                      const BackwardArgs& a) {
+  if (!__any_sync(0xffffffffu, any_contrib)) return;
+  float s[kValues];
+#pragma unroll
+  for (int k = 0; k < kValues; ++k) s[k] = warp_sum(c[k]);
+  if ((threadIdx.x & 31) == 0) {
+    atomicAdd(a.dL_dcolors + 3 * size_t(id), s[0]);
+    atomicAdd(a.dL_dcolors + 3 * size_t(id) + 1, s[1]);
+    atomicAdd(a.dL_dcolors + 3 * size_t(id) + 2, s[2]);
+    atomicAdd(a.acc_depth + id, s[3]);
+    atomicAdd(a.dL_dmean2D + 3 * size_t(id), s[4]);
+    atomicAdd(a.dL_dmean2D + 3 * size_t(id) + 1, s[5]);
+    if (mode == 0) {
+      atomicAdd(a.acc_cov + 4 * size_t(id), s[6]);
+      atomicAdd(a.acc_cov + 4 * size_t(id) + 1, s[7]);
+      atomicAdd(a.acc_cov + 4 * size_t(id) + 3, s[8]);
+    } else {
+      atomicAdd(a.acc_cov + 4 * size_t(id), s[6]);
+      atomicAdd(a.acc_cov + 4 * size_t(id) + 1, s[7]);
+      atomicAdd(a.acc_cov + 4 * size_t(id) + 2, s[8]);
+    }
+    atomicAdd(a.dL_dopacity + id, s[9]);
+  }
+}
+
+// Reference formulas (backward.cu:552-663)
+__global__ void __launch_bounds__(kBlendThreads) render_ref_kernel(BackwardArgs a) {
+  __shared__ float4 s_rec[kBatch * 3];
+  __shared__ uint32_t s_id[kBatch];
+  const int gw = (a.W + kTile - 1) / kTile;
+  const int tile = blockIdx.y * gw + blockIdx.x;
+  const int px = blockIdx.x * kTile + (threadIdx.x & 15), py = blockIdx.y * kTile + (threadIdx.x >> 4);
+  const bool inside = px < a.W && py < a.H;
+  const uint2 range = a.ranges[tile];
+  const uint32_t nmax = min(a.tile_max[tile], range.y - range.x);
+  const size_t pix = inside ? size_t(py) * a.W + px : 0;
+  const size_t hw = size_t(a.W) * a.H;
+  const float T_final = inside ? 1.0f - a.out_alpha[pix] : 0.0f;
+  float T = T_final;
+  const uint32_t last = inside ? a.n_contrib[pix] : 0u;
+  float dLp0 = 0.f, dLp1 = 0.f, dLp2 = 0.f, dLd = 0.f, dLa = 0.f;
+  if (inside) {
+    dLp0 = a.dL_dcolor[pix];
+    dLp1 = a.dL_dcolor[hw + pix];
+    dLp2 = a.dL_dcolor[2 * hw + pix];
+    dLd = a.dL_ddepth[pix];
+    dLa = a.dL_dalpha[pix];
+  }
+  const float bg_dot = a.bg[0] * dLp0 + a.bg[1] * dLp1 + a.bg[2] * dLp2;
+  float acc0 = 0.f, acc1 = 0.f, acc2 = 0.f, acc_d = 0.f, acc_a = 0.f;
+  float last_alpha = 0.f, lc0 = 0.f, lc1 = 0.f, lc2 = 0.f, last_depth = 0.f;
+  const float ddelx_dx = 0.5f * float(a.W), ddely_dy = 0.5f * float(a.H);
+  const float pxf = float(px), pyf = float(py);
+  const float4* rec = reinterpret_cast<const float4*>(a.bwd_record);
+
+  for (int hi = int(nmax); hi > 0; hi -= kBatch) {
+    const int cnt = min(kBatch, hi);
+    __syncthreads();
+    if (int(threadIdx.x) < cnt) {
+      const uint32_t id = a.point_list[range.x + hi - 1 - threadIdx.x];
+      s_id[threadIdx.x] = id;
+      s_rec[3 * threadIdx.x] = __ldg(rec + 3 * size_t(id));
+      s_rec[3 * threadIdx.x + 1] = __ldg(rec + 3 * size_t(id) + 1);
+      s_rec[3 * threadIdx.x + 2] = __ldg(rec + 3 * size_t(id) + 2);
+    }
+    __syncthreads();
+    for (int j = 0; j < cnt; ++j) {
+      const uint32_t idx = uint32_t(hi - 1 - j);  // position in the tile's list
+      float c[kValues];
+#pragma unroll
+      for (int k = 0; k < kValues; ++k) c[k] = 0.f;
+      bool contrib = false;
+      if (inside && idx < last) {
+        // q0 = (mx, my, conic a, conic b), q1 = (conic c, opacity, depth, r), q2 = (g, b, _, _)
+        const float4 q0 = s_rec[3 * j], q1 = s_rec[3 * j + 1];
+        const float dx = q0.x - pxf, dy = q0.y - pyf;
+        const float power = -0.5f * (q0.z * dx * dx + q1.x * dy * dy) - q0.w * dx * dy;
+        if (power <= 0.0f) {
+          const float G = expf(power);
+          const float alpha = fminf(0.99f, q1.y * G);
+          if (alpha >= 1.0f / 255.0f) {
+            contrib = true;
+            const float4 q2 = s_rec[3 * j + 2];
+            T = T / (1.f - alpha);
+            const float dchdc = alpha * T;
+            float dL_dopa = 0.0f;
+            acc0 = last_alpha * lc0 + (1.f - last_alpha) * acc0;
+            lc0 = q1.w;
+            dL_dopa += (q1.w - acc0) * dLp0;
+            c[0] = dchdc * dLp0;
+            acc1 = last_alpha * lc1 + (1.f - last_alpha) * acc1;
+            lc1 = q2.x;
+            dL_dopa += (q2.x - acc1) * dLp1;
+            c[1] = dchdc * dLp1;
+            acc2 = last_alpha * lc2 + (1.f - last_alpha) * acc2;
+            lc2 = q2.y;
+            dL_dopa += (q2.y - acc2) * dLp2;
+            c[2] = dchdc * dLp2;
+            const float c_d = q1.z;
+            acc_d = last_alpha * last_depth + (1.f - last_alpha) * acc_d;
+            last_depth = c_d;
+            dL_dopa += (c_d - acc_d) * dLd;
+            c[3] = dchdc * dLd;
+            acc_a = last_alpha + (1.f - last_alpha) * acc_a;
+            dL_dopa += (1 - acc_a) * dLa;
+            dL_dopa *= T;
+            last_alpha = alpha;
+            dL_dopa += (-T_final / (1.f - alpha)) * bg_dot;
+            const float dL_dG = q1.y * dL_dopa;
+            const float gdx = G * dx, gdy = G * dy;
+            const float dG_ddelx = -gdx * q0.z - gdy * q0.w;
+            const float dG_ddely = -gdy * q1.x - gdx * q0.w;
+            c[4] = dL_dG * dG_ddelx * ddelx_dx;
+            c[5] = dL_dG * dG_ddely * ddely_dy;
+            c[6] = -0.5f * gdx * dx * dL_dG;
+            c[7] = -0.5f * gdx * dy * dL_dG;
+            c[8] = -0.5f * gdy * dy * dL_dG;
+            c[9] = G * dL_dopa;
+          }
+        }
+      }
+      flush(c, contrib, s_id[j], 0, a);
+    }
+  }
+}
+
+__device__ __forceinline__ float gauss_eval_fwd(float px, float py, float mx, float my, float cxx, float cxy,
+                                                float cyy, float det, float* mahal) {
+  using namespace fp;
+  const float dx = sub(px, mx), dy = sub(py, my);
+  const float tX = d2<BL_TX>(dx, cyy, dy, cxy);
+  const float tY = s2<BL_TY>(-dx, cxy, dy, cxx);
+  const float num = s2<BL_NUM>(tX, dx, tY, dy);
+  float m = div(num, det);
+  *mahal = m;
+  if (m < 0.0f) m = 1000.0f;
+  return expf(mul(-0.5f, m));
+}
+
+// Exact derivative of the forward blend.
+__global__ void __launch_bounds__(kBlendThreads) render_exact_kernel(BackwardArgs a) {
+  __shared__ float4 s_rec[kBatch * 3];
+  __shared__ uint32_t s_id[kBatch];
+  const int gw = (a.W + kTile - 1) / kTile;
+  const int tile = blockIdx.y * gw + blockIdx.x;
+  const int px = blockIdx.x * kTile + (threadIdx.x & 15), py = blockIdx.y * kTile + (threadIdx.x >> 4);
+  const bool inside = px < a.W && py < a.H;
+  const uint2 range = a.ranges[tile];
+  const uint32_t nmax = min(a.tile_max[tile], range.y - range.x);
+  const size_t pix = inside ? size_t(py) * a.W + px : 0;
+  const size_t hw = size_t(a.W) * a.H;
+  const float Tf = inside ? a.T_final[pix] : 0.0f;
+  float T = Tf;
+  const uint32_t last = inside ? a.n_contrib[pix] : 0u;
+  float dLp0 = 0.f, dLp1 = 0.f, dLp2 = 0.f, dLd = 0.f, dLa = 0.f;
+  if (inside) {
+    dLp0 = a.dL_dcolor[pix];
+    dLp1 = a.dL_dcolor[hw + pix];
+    dLp2 = a.dL_dcolor[2 * hw + pix];
+    dLd = a.dL_ddepth[pix];
+    dLa = a.dL_dalpha[pix];
+  }
+  // suffix sums behind the current entry (colour includes the background)
+  float S0 = Tf * a.bg[0], S1 = Tf * a.bg[1], S2 = Tf * a.bg[2], SD = 0.f, SW = 0.f;
+  const float hW = 0.5f * float(a.W), hH = 0.5f * float(a.H);
+  const float pxf = float(px), pyf = float(py);
+  const float4* rec = reinterpret_cast<const float4*>(a.record);
+  for (int hi = int(nmax); hi > 0; hi -= kBatch) {
+    const int cnt = min(kBatch, hi);
+    __syncthreads();
+    if (int(threadIdx.x) < cnt) {
+      const uint32_t id = a.point_list[range.x + hi - 1 - threadIdx.x];
+      s_id[threadIdx.x] = id;
+      s_rec[3 * threadIdx.x] = __ldg(rec + 3 * size_t(id));
+      s_rec[3 * threadIdx.x + 1] = __ldg(rec + 3 * size_t(id) + 1);
+      s_rec[3 * threadIdx.x + 2] = __ldg(rec + 3 * size_t(id) + 2);
+    }
+    __syncthreads();
+    for (int j = 0; j < cnt; ++j) {
+      const uint32_t idx = uint32_t(hi - 1 - j);
+      float c[kValues];
+#pragma unroll
+      for (int k = 0; k < kValues; ++k) c[k] = 0.f;
+      bool contrib = false;
+      if (inside && idx < last) {
+        // q0 = (mx, my, cxx, cxy), q1 = (cyy, det, opacity, depth), q2 = (r, g, b, _)
+        const float4 q0 = s_rec[3 * j], q1 = s_rec[3 * j + 1];
+        float mahal;
+        const float g = gauss_eval_fwd(pxf, pyf, q0.x, q0.y, q0.z, q0.w, q1.x, q1.y, &mahal);
+        const float og = mul(q1.z, g);
+        const float a_ = fminf(0.99f, og);
+        if (a_ >= 1.0f / 255.0f) {
+          contrib = true;
+          const float4 q2 = s_rec[3 * j + 2];
+          const float ia = 1.0f / (1.0f - a_);
+          T = T * ia;  // transmittance in front of this entry
+          const float aT = a_ * T;
+          float dLda = dLp0 * (q2.x * T - S0 * ia) + dLp1 * (q2.y * T - S1 * ia) + dLp2 * (q2.z * T - S2 * ia);
+          dLda += dLd * (q1.w * T - SD * ia);
+          dLda += dLa * (T - SW * ia);
+          c[0] = aT * dLp0;
+          c[1] = aT * dLp1;
+          c[2] = aT * dLp2;
+          c[3] = aT * dLd;
+          S0 += q2.x * aT;
+          S1 += q2.y * aT;
+          S2 += q2.z * aT;
+          SD += q1.w * aT;
+          SW += aT;
+          if (og < 0.99f) {
+            c[9] = dLda * g;
+            if (mahal >= 0.0f) {
+              const float dLdm = dLda * q1.z * (-0.5f * g);
+              const float cxx = q0.z, cxy = q0.w, cyy = q1.x, det = q1.y;
+              const float dx = pxf - q0.x, dy = pyf - q0.y;
+              const float idet = 1.0f / det;
+              c[4] = -dLdm * (2.f * cyy * dx - 2.f * cxy * dy) * idet * hW;
+              c[5] = -dLdm * (2.f * cxx * dy - 2.f * cxy * dx) * idet * hH;
+              const float num = mahal * det;
+              c[6] = dLdm * (dy * dy * idet - num * cyy * idet * idet);
+              c[7] = dLdm * (-2.f * dx * dy * idet + 2.f * num * cxy * idet * idet);
+              c[8] = dLdm * (dx * dx * idet - num * cxx * idet * idet);
+            }
+          }
+        }
+      }
+      flush(c, contrib, s_id[j], 1, a);
+    }
+  }
+}
+
+// Per-Gaussian, reference formulas (backward.cu:27-227 then :229-519)
+__constant__ float kSH_C2[5] = {1.0925484305920792f, -1.0925484305920792f, 0.31539156525252005f,
+                                -1.0925484305920792f, 0.5462742152960396f};
+__constant__ float kSH_C3[7] = {-0.5900435899266435f, 2.890611442640554f, -0.4570457994644658f,
+                                0.3731763325901154f,  -0.4570457994644658f, 1.445305721320277f,
+                                -0.5900435899266435f};
+
+__global__ void __launch_bounds__(256) gaussians_ref_kernel(BackwardArgs a) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= a.P) return;
+  const int M = a.M;
+  float* dsh = a.dL_dsh + size_t(i) * M * 3;
+  if (!(a.radii[i] > 0)) {
+    for (int k = 0; k < 3; ++k) a.dL_dmeans3D[3 * i + k] = 0.f;
+    for (int k = 0; k < 6; ++k) a.dL_dcov3D[6 * i + k] = 0.f;
+    for (int k = 0; k < M * 3; ++k) dsh[k] = 0.f;
+    for (int k = 0; k < 3; ++k) a.dL_dscales[3 * i + k] = 0.f;
+    for (int k = 0; k < 4; ++k) a.dL_drotations[4 * i + k] = 0.f;
+    return;
+  }
+  const float* view = a.view;
+  const float* proj = a.proj;
+  const float cx = a.means3D[3 * i], cy = a.means3D[3 * i + 1], cz = a.means3D[3 * i + 2];
+  const float* pc = a.cov3D + 6 * size_t(i);
+
+  // ---- computeCov2DCUDA ----
+  float vx = view[0] * cx + view[4] * cy + view[8] * cz + view[12];
+  float vy = view[1] * cx + view[5] * cy + view[9] * cz + view[13];
+  float vz = view[2] * cx + view[6] * cy + view[10] * cz + view[14];
+  const float vw = view[3] * cx + view[7] * cy + view[11] * cz + view[15];
+  const float w_inv = 1.0f / (vw + 1e-8f);
+  vx *= w_inv;
+  vy *= w_inv;
+  vz *= w_inv;
+  const float bound_x = 1.3f * a.tan_fovx, bound_y = 1.3f * a.tan_fovy;
+  const float proj_x = vx / vz, proj_y = vy / vz;
+  const float cpx = fminf(bound_x, fmaxf(-bound_x, proj_x));
+  const float cpy = fminf(bound_y, fmaxf(-bound_y, proj_y));
+  const float px = cpx * vz, py = cpy * vz;
+  const float mask_x = (proj_x >= -bound_x && proj_x <= bound_x) ? 1.0f : 0.0f;
+  const float mask_y = (proj_y >= -bound_y && proj_y <= bound_y) ? 1.0f : 0.0f;
+  const float z_inv = 1.0f / vz, z_inv2 = z_inv * z_inv;
+  const float h_x = a.h_x, h_y = a.h_y;
+  // J (glm column-major J[col][row]) and T = W * J
+  const float J[3][3] = {{h_x * z_inv, 0.f, -h_x * px * z_inv2}, {0.f, h_y * z_inv, -h_y * py * z_inv2}, {0.f, 0.f, 0.f}};
+  const float Wv[3][3] = {{view[0], view[4], view[8]}, {view[1], view[5], view[9]}, {view[2], view[6], view[10]}};
+  const float Vk[3][3] = {{pc[0], pc[1], pc[2]}, {pc[1], pc[3], pc[4]}, {pc[2], pc[4], pc[5]}};
+  float T[3][3], tmp[3][3], c2[3][3];
+#pragma unroll
+  for (int c = 0; c < 3; ++c)
+#pragma unroll
+    for (int r = 0; r < 3; ++r) T[c][r] = Wv[0][r] * J[c][0] + Wv[1][r] * J[c][1] + Wv[2][r] * J[c][2];
+#pragma unroll
+  for (int c = 0; c < 3; ++c)
+#pragma unroll
+    for (int r = 0; r < 3; ++r) tmp[c][r] = Vk[r][0] * T[c][0] + Vk[r][1] * T[c][1] + Vk[r][2] * T[c][2];
+#pragma unroll
+  for (int c = 0; c < 3; ++c)
+#pragma unroll
+    for (int r = 0; r < 3; ++r) c2[c][r] = T[r][0] * tmp[c][0] + T[r][1] * tmp[c][1] + T[r][2] * tmp[c][2];
+  c2[0][0] += 0.3f;
+  c2[1][1] += 0.3f;
+  const float ca = c2[0][0], cb = c2[0][1], cc = c2[1][1];
+  const float den = ca * cc - cb * cb;
+  const float dinv2 = 1.0f / (den * den + 1e-7f);
+  const float gx = a.acc_cov[4 * i], gy = a.acc_cov[4 * i + 1], gz = a.acc_cov[4 * i + 3];
+  float ga = 0.f, gb = 0.f, gc = 0.f;
+  float dc[6];
+  if (dinv2 > 0) {
+    ga = dinv2 * (-cc * cc * gx + 2.0f * cb * cc * gy + (den - ca * cc) * gz);
+    gb = dinv2 * 2.0f * (cb * cc * gx - (den + 2.0f * cb * cb) * gy + ca * cb * gz);
+    gc = dinv2 * (-ca * ca * gz + 2.0f * ca * cb * gy + (den - ca * cc) * gx);
+    dc[0] = T[0][0] * T[0][0] * ga + T[0][0] * T[1][0] * gb + T[1][0] * T[1][0] * gc;
+    dc[3] = T[0][1] * T[0][1] * ga + T[0][1] * T[1][1] * gb + T[1][1] * T[1][1] * gc;
+    dc[5] = T[0][2] * T[0][2] * ga + T[0][2] * T[1][2] * gb + T[1][2] * T[1][2] * gc;
+    dc[1] = 2.0f * (T[0][0] * T[0][1] * ga + (T[0][0] * T[1][1] + T[0][1] * T[1][0]) * gb * 0.5f + T[1][0] * T[1][1] * gc);
+    dc[2] = 2.0f * (T[0][0] * T[0][2] * ga + (T[0][0] * T[1][2] + T[0][2] * T[1][0]) * gb * 0.5f + T[1][0] * T[1][2] * gc);
+    dc[4] = 2.0f * (T[0][1] * T[0][2] * ga + (T[0][1] * T[1][2] + T[0][2] * T[1][1]) * gb * 0.5f + T[1][1] * T[1][2] * gc);
+  } else {
+    for (int k = 0; k < 6; ++k) dc[k] = 0.f;
+  }
+  for (int k = 0; k < 6; ++k) a.dL_dcov3D[6 * i + k] = dc[k];
+  const float gT00 = 2.0f * (T[0][0] * Vk[0][0] + T[0][1] * Vk[0][1] + T[0][2] * Vk[0][2]) * ga + (T[1][0] * Vk[0][0] + T[1][1] * Vk[0][1] + T[1][2] * Vk[0][2]) * gb;
+  const float gT01 = 2.0f * (T[0][0] * Vk[1][0] + T[0][1] * Vk[1][1] + T[0][2] * Vk[1][2]) * ga + (T[1][0] * Vk[1][0] + T[1][1] * Vk[1][1] + T[1][2] * Vk[1][2]) * gb;
+  const float gT02 = 2.0f * (T[0][0] * Vk[2][0] + T[0][1] * Vk[2][1] + T[0][2] * Vk[2][2]) * ga + (T[1][0] * Vk[2][0] + T[1][1] * Vk[2][1] + T[1][2] * Vk[2][2]) * gb;
+  const float gT10 = 2.0f * (T[1][0] * Vk[0][0] + T[1][1] * Vk[0][1] + T[1][2] * Vk[0][2]) * gc + (T[0][0] * Vk[0][0] + T[0][1] * Vk[0][1] + T[0][2] * Vk[0][2]) * gb;
+  const float gT11 = 2.0f * (T[1][0] * Vk[1][0] + T[1][1] * Vk[1][1] + T[1][2] * Vk[1][2]) * gc + (T[0][0] * Vk[1][0] + T[0][1] * Vk[1][1] + T[0][2] * Vk[1][2]) * gb;
+  const float gT12 = 2.0f * (T[1][0] * Vk[2][0] + T[1][1] * Vk[2][1] + T[1][2] * Vk[2][2]) * gc + (T[0][0] * Vk[2][0] + T[0][1] * Vk[2][1] + T[0][2] * Vk[2][2]) * gb;
+  const float gJ00 = Wv[0][0] * gT00 + Wv[0][1] * gT01 + Wv[0][2] * gT02;
+  const float gJ02 = Wv[2][0] * gT00 + Wv[2][1] * gT01 + Wv[2][2] * gT02;
+  const float gJ11 = Wv[1][0] * gT10 + Wv[1][1] * gT11 + Wv[1][2] * gT12;
+  const float gJ12 = Wv[2][0] * gT10 + Wv[2][1] * gT11 + Wv[2][2] * gT12;
+  const float z_inv3 = z_inv2 * z_inv;
+  const float gvx = mask_x * (-h_x * z_inv2 * gJ02);
+  const float gvy = mask_y * (-h_y * z_inv2 * gJ12);
+  const float gvz = -h_x * z_inv2 * gJ00 - h_y * z_inv2 * gJ11 + 2.0f * h_x * px * z_inv3 * gJ02 +
+                    2.0f * h_y * py * z_inv3 * gJ12;
+  float sd[3] = {view[0] * gvx + view[1] * gvy + view[2] * gvz, view[4] * gvx + view[5] * gvy + view[6] * gvz,
+                 view[8] * gvx + view[9] * gvy + view[10] * gvz};
+
+  // ---- backwardPreprocessingKernel ----
+  const float cw = proj[3] * cx + proj[7] * cy + proj[11] * cz + proj[15];
+  const float iw = 1.0f / (cw + 1e-7f);
+  const float iw2 = iw * iw;
+  const float ptx = (proj[0] * cx + proj[4] * cy + proj[8] * cz + proj[12]) * iw2;
+  const float pty = (proj[1] * cx + proj[5] * cy + proj[9] * cz + proj[13]) * iw2;
+  const float g2x = a.dL_dmean2D[3 * i], g2y = a.dL_dmean2D[3 * i + 1];
+  sd[0] += (proj[0] * iw - proj[3] * ptx) * g2x + (proj[1] * iw - proj[3] * pty) * g2y;
+  sd[1] += (proj[4] * iw - proj[7] * ptx) * g2x + (proj[5] * iw - proj[7] * pty) * g2y;
+  sd[2] += (proj[8] * iw - proj[11] * ptx) * g2x + (proj[9] * iw - proj[11] * pty) * g2y;
+  const float vzz = view[2] * cx + view[6] * cy + view[10] * cz + view[14];
+  const float gd = a.acc_depth[i];
+  sd[0] += (view[2] - view[3] * vzz) * gd;
+  sd[1] += (view[6] - view[7] * vzz) * gd;
+  sd[2] += (view[10] - view[11] * vzz) * gd;
+  // SH (all 16 bands, colour-clamp masks)
+  const float ox = cx - a.campos[0], oy = cy - a.campos[1], oz = cz - a.campos[2];
+  const float msq = ox * ox + oy * oy + oz * oz;
+  const float mag = sqrtf(msq + 1e-10f);
+  const float im = 1.0f / mag;
+  const float x = ox * im, y = oy * im, z = oz * im;
+  const float x2 = x * x, y2 = y * y, z2 = z * z, xy = x * y, xz = x * z, yz = y * z;
+  const float x2my2 = x2 - y2, tx2 = 3.0f * x2, ty2 = 3.0f * y2, fz2 = 4.0f * z2, wz2 = 2.0f * z2;
+  float cf[3];
+  for (int ch = 0; ch < 3; ++ch) cf[ch] = a.dL_dcolors[3 * i + ch] * (a.clamped[3 * i + ch] ? 0.0f : 1.0f);
+  const float SH_C0 = 0.28209479177387814f, SH_C1 = 0.4886025119029199f;
+  float basis[16];
+  basis[0] = SH_C0; basis[1] = -SH_C1 * y; basis[2] = SH_C1 * z; basis[3] = -SH_C1 * x;
+  basis[4] = kSH_C2[0] * xy; basis[5] = kSH_C2[1] * yz; basis[6] = kSH_C2[2] * (wz2 - x2 - y2);
+  basis[7] = kSH_C2[3] * xz; basis[8] = kSH_C2[4] * x2my2;
+  basis[9] = kSH_C3[0] * y * (tx2 - y2); basis[10] = kSH_C3[1] * xy * z; basis[11] = kSH_C3[2] * y * (fz2 - x2 - y2);
+  basis[12] = kSH_C3[3] * z * (wz2 - tx2 - ty2); basis[13] = kSH_C3[4] * x * (fz2 - x2 - y2);
+  basis[14] = kSH_C3[5] * z * x2my2; basis[15] = kSH_C3[6] * x * (x2 - ty2);
+  const int nb = M < 16 ? M : 16;
+  for (int k = 0; k < nb; ++k)
+    for (int ch = 0; ch < 3; ++ch) dsh[3 * k + ch] = basis[k] * cf[ch];
+  for (int k = nb * 3; k < M * 3; ++k) dsh[k] = 0.f;
+  const float* shd = a.shs + size_t(i) * M * 3;
+  auto SH = [&](int k, int ch) -> float { return k < M ? shd[3 * k + ch] : 0.0f; };
+  float ag[3] = {0.f, 0.f, 0.f};
+  auto dotc = [&](int k) { return SH(k, 0) * cf[0] + SH(k, 1) * cf[1] + SH(k, 2) * cf[2]; };
+  ag[0] -= SH_C1 * dotc(3);
+  ag[1] -= SH_C1 * dotc(1);
+  ag[2] += SH_C1 * dotc(2);
+  float d2x[3], d2y[3], d2z[3];
+  for (int ch = 0; ch < 3; ++ch) {
+    d2x[ch] = kSH_C2[0] * y * SH(4, ch) + kSH_C2[2] * (-2.0f * x) * SH(6, ch) + kSH_C2[3] * z * SH(7, ch) + kSH_C2[4] * (2.0f * x) * SH(8, ch);
+    d2y[ch] = kSH_C2[0] * x * SH(4, ch) + kSH_C2[1] * z * SH(5, ch) + kSH_C2[2] * (-2.0f * y) * SH(6, ch) + kSH_C2[4] * (-2.0f * y) * SH(8, ch);
+    d2z[ch] = kSH_C2[1] * y * SH(5, ch) + kSH_C2[2] * (4.0f * z) * SH(6, ch) + kSH_C2[3] * x * SH(7, ch);
+  }
+  ag[0] += d2x[0] * cf[0] + d2x[1] * cf[1] + d2x[2] * cf[2];
+  ag[1] += d2y[0] * cf[0] + d2y[1] * cf[1] + d2y[2] * cf[2];
+  ag[2] += d2z[0] * cf[0] + d2z[1] * cf[1] + d2z[2] * cf[2];
+  const float f3x[7] = {kSH_C3[0] * 6.0f * xy, kSH_C3[1] * yz, kSH_C3[2] * (-2.0f * xy), kSH_C3[3] * (-6.0f * xz),
+                        kSH_C3[4] * (fz2 - 3.0f * x2 - y2), kSH_C3[5] * 2.0f * xz, kSH_C3[6] * 3.0f * x2my2};
+  const float f3y[7] = {kSH_C3[0] * 3.0f * (x2 - y2), kSH_C3[1] * xz, kSH_C3[2] * (fz2 - 3.0f * y2 - x2),
+                        kSH_C3[3] * (-6.0f * yz), kSH_C3[4] * (-2.0f * xy), kSH_C3[5] * (-2.0f * yz),
+                        kSH_C3[6] * (-6.0f * xy)};
+  const float f3z[7] = {0.0f, kSH_C3[1] * xy, kSH_C3[2] * 8.0f * yz, kSH_C3[3] * 3.0f * (wz2 - x2 - y2),
+                        kSH_C3[4] * 8.0f * xz, kSH_C3[5] * x2my2, 0.0f};
+  float d3x[3] = {0.f, 0.f, 0.f}, d3y[3] = {0.f, 0.f, 0.f}, d3z[3] = {0.f, 0.f, 0.f};
+  for (int k = 0; k < 7; ++k)
+    for (int ch = 0; ch < 3; ++ch) {
+      const float s = SH(9 + k, ch);
+      d3x[ch] += f3x[k] * s;
+      d3y[ch] += f3y[k] * s;
+      d3z[ch] += f3z[k] * s;
+    }
+  ag[0] += d3x[0] * cf[0] + d3x[1] * cf[1] + d3x[2] * cf[2];
+  ag[1] += d3y[0] * cf[0] + d3y[1] * cf[1] + d3y[2] * cf[2];
+  ag[2] += d3z[0] * cf[0] + d3z[1] * cf[1] + d3z[2] * cf[2];
+  const float im3 = im * im * im;
+  const float rd[3] = {ox, oy, oz};
+  for (int r = 0; r < 3; ++r) {
+    float acc = 0.f;
+    for (int c = 0; c < 3; ++c) acc += ((c == r ? msq : 0.0f) - rd[c] * rd[r]) * im3 * ag[c];
+    sd[r] += acc;
+  }
+  a.dL_dmeans3D[3 * i] = sd[0];
+  a.dL_dmeans3D[3 * i + 1] = sd[1];
+  a.dL_dmeans3D[3 * i + 2] = sd[2];
+
+  // ---- scale / rotation (backward.cu:446-518) ----
+  const float qw = a.rotations[4 * i], qx = a.rotations[4 * i + 1], qy = a.rotations[4 * i + 2],
+              qz = a.rotations[4 * i + 3];
+  const float xx = qx * qx, yy = qy * qy, zz = qz * qz;
+  const float qxy = qx * qy, qxz = qx * qz, qyz = qy * qz;
+  const float xw = qx * qw, yw = qy * qw, zw = qz * qw;
+  const float sx = a.scale_modifier * a.scales[3 * i], sy = a.scale_modifier * a.scales[3 * i + 1],
+              sz = a.scale_modifier * a.scales[3 * i + 2];
+  const float m11 = sx * (1.f - 2.f * (yy + zz)), m12 = sx * 2.f * (qxy - zw), m13 = sx * 2.f * (qxz + yw);
+  const float m21 = sy * 2.f * (qxy + zw), m22 = sy * (1.f - 2.f * (xx + zz)), m23 = sy * 2.f * (qyz - xw);
+  const float m31 = sz * 2.f * (qxz - yw), m32 = sz * 2.f * (qyz + xw), m33 = sz * (1.f - 2.f * (xx + yy));
+  const float g11 = dc[0], g12 = dc[1], g13 = dc[2], g22 = dc[3], g23 = dc[4], g33 = dc[5];
+  const float a11 = 2.f * (m11 * g11 + m12 * g12 + m13 * g13);
+  const float a12 = 2.f * (m11 * g12 + m12 * g22 + m13 * g23);
+  const float a13 = 2.f * (m11 * g13 + m12 * g23 + m13 * g33);
+  const float a21 = 2.f * (m21 * g11 + m22 * g12 + m23 * g13);
+  const float a22 = 2.f * (m21 * g12 + m22 * g22 + m23 * g23);
+  const float a23 = 2.f * (m21 * g13 + m22 * g23 + m23 * g33);
+  const float a31 = 2.f * (m31 * g11 + m32 * g12 + m33 * g13);
+  const float a32 = 2.f * (m31 * g12 + m32 * g22 + m33 * g23);
+  const float a33 = 2.f * (m31 * g13 + m32 * g23 + m33 * g33);
+  a.dL_dscales[3 * i] = (1.f - 2.f * (yy + zz)) * a11 + 2.f * (qxy - zw) * a12 + 2.f * (qxz + yw) * a13;
+  a.dL_dscales[3 * i + 1] = 2.f * (qxy + zw) * a21 + (1.f - 2.f * (xx + zz)) * a22 + 2.f * (qyz - xw) * a23;
+  a.dL_dscales[3 * i + 2] = 2.f * (qxz - yw) * a31 + 2.f * (qyz + xw) * a32 + (1.f - 2.f * (xx + yy)) * a33;
+  float4 dq;
+  dq.x = 4.f * (-sz * (a31 * yw - a32 * xw + a33 * qxy) + sy * (a21 * zw - a22 * qxz + a23 * yy) + sx * (a12 * zw - a13 * yw - a11 * qyz));
+  dq.y = 4.f * (sz * (a31 * zw + a32 * zz - a33 * qyz) - sy * (a21 * yw + a22 * qxy + a23 * xx) + sx * (a12 * yy + a13 * zw + a11 * qxz));
+  dq.z = 4.f * (-sz * (a31 * xx + a32 * xw + a33 * qxz) + sy * (a21 * zw + a22 * yy + a23 * yw) - sx * (a12 * xw + a13 * xx + a11 * qxy));
+  dq.w = 4.f * (sz * (a31 * xw - a32 * xx + a33 * qxy) - sy * (a21 * qxz - a22 * zw + a23 * qyz) + sx * (a12 * qyz - a13 * zz + a11 * yy));
+  a.dL_drotations[4 * i] = dq.x;
+  a.dL_drotations[4 * i + 1] = dq.y;
+  a.dL_drotations[4 * i + 2] = dq.z;
+  a.dL_drotations[4 * i + 3] = dq.w;
+}
+
+// Per-Gaussian, exact derivative of the forward.
+__global__ void __launch_bounds__(256) gaussians_exact_kernel(BackwardArgs a) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= a.P) return;
+  const int M = a.M;
+  float* dsh = a.dL_dsh + size_t(i) * M * 3;
+  if (!(a.radii[i] > 0)) {
+    for (int k = 0; k < 3; ++k) a.dL_dmeans3D[3 * i + k] = 0.f;
+    for (int k = 0; k < 6; ++k) a.dL_dcov3D[6 * i + k] = 0.f;
+    for (int k = 0; k < M * 3; ++k) dsh[k] = 0.f;
+    for (int k = 0; k < 3; ++k) a.dL_dscales[3 * i + k] = 0.f;
+    for (int k = 0; k < 4; ++k) a.dL_drotations[4 * i + k] = 0.f;
+    return;
+  }
+  const float* V = a.view;
+  const float* PM = a.proj;
+  const float m0 = a.means3D[3 * i], m1 = a.means3D[3 * i + 1], m2 = a.means3D[3 * i + 2];
+  float gm[3] = {0.f, 0.f, 0.f};
+  // screen position / depth: ndc = clip.xyz / (clip.w + 1e-5); dL_dmean2D already holds dL/dNDC
+  float clip[4];
+  for (int r = 0; r < 4; ++r) clip[r] = PM[r] * m0 + PM[4 + r] * m1 + PM[8 + r] * m2 + PM[12 + r];
+  const float wi = 1.0f / (clip[3] + 1e-5f);
+  const float gn0 = a.dL_dmean2D[3 * i], gn1 = a.dL_dmean2D[3 * i + 1], gn2 = a.acc_depth[i];
+  const float gcl[4] = {gn0 * wi, gn1 * wi, gn2 * wi, -(gn0 * clip[0] + gn1 * clip[1] + gn2 * clip[2]) * wi * wi};
+  for (int c = 0; c < 3; ++c)
+    for (int r = 0; r < 4; ++r) gm[c] += PM[4 * c + r] * gcl[r];
+  // covariance chain
+  float t[3];
+  for (int r = 0; r < 3; ++r) t[r] = V[r] * m0 + V[4 + r] * m1 + V[8 + r] * m2 + V[12 + r];
+  const float L = float(a.W) / (2.0f * a.focal_x);
+  const float rx = t[0] / t[2], ry = t[1] / t[2];
+  const float nn = sqrtf(rx * rx + ry * ry) / L;
+  const bool clampd = nn > 1.0f;
+  float txp = t[0], typ = t[1];
+  if (clampd) { txp = rx / nn * t[2]; typ = ry / nn * t[2]; }
+  const float tz = t[2], f = a.focal_x;
+  const float rgt[3] = {V[0], V[4], V[8]}, upv[3] = {V[1], V[5], V[9]}, fw[3] = {V[2], V[6], V[10]};
+  float jx[3], jy[3];
+  for (int k = 0; k < 3; ++k) {
+    jx[k] = f * (rgt[k] / tz - txp * fw[k] / (tz * tz));
+    jy[k] = f * (upv[k] / tz - typ * fw[k] / (tz * tz));
+  }
+  const float* pc = a.cov3D + 6 * size_t(i);
+  const float S[3][3] = {{pc[0], pc[1], pc[2]}, {pc[1], pc[3], pc[4]}, {pc[2], pc[4], pc[5]}};
+  const float gxx = a.acc_cov[4 * i], gxy = a.acc_cov[4 * i + 1], gyy = a.acc_cov[4 * i + 2];
+  float Gf[3][3];
+  for (int p = 0; p < 3; ++p)
+    for (int q = 0; q < 3; ++q) Gf[p][q] = gxx * jx[p] * jx[q] + gyy * jy[p] * jy[q] + gxy * jx[p] * jy[q];
+  a.dL_dcov3D[6 * i + 0] = Gf[0][0];
+  a.dL_dcov3D[6 * i + 1] = Gf[0][1] + Gf[1][0];
+  a.dL_dcov3D[6 * i + 2] = Gf[0][2] + Gf[2][0];
+  a.dL_dcov3D[6 * i + 3] = Gf[1][1];
+  a.dL_dcov3D[6 * i + 4] = Gf[1][2] + Gf[2][1];
+  a.dL_dcov3D[6 * i + 5] = Gf[2][2];
+  float Sjx[3], Sjy[3];
+  for (int p = 0; p < 3; ++p) {
+    Sjx[p] = S[p][0] * jx[0] + S[p][1] * jx[1] + S[p][2] * jx[2];
+    Sjy[p] = S[p][0] * jy[0] + S[p][1] * jy[1] + S[p][2] * jy[2];
+  }
+  float gtxp = 0.f, gtyp = 0.f, gtz = 0.f;
+  for (int k = 0; k < 3; ++k) {
+    const float gjx = 2.f * gxx * Sjx[k] + gxy * Sjy[k];
+    const float gjy = 2.f * gyy * Sjy[k] + gxy * Sjx[k];
+    gtxp += gjx * (-f * fw[k] / (tz * tz));
+    gtyp += gjy * (-f * fw[k] / (tz * tz));
+    gtz += gjx * f * (-rgt[k] / (tz * tz) + 2.f * txp * fw[k] / (tz * tz * tz));
+    gtz += gjy * f * (-upv[k] / (tz * tz) + 2.f * typ * fw[k] / (tz * tz * tz));
+  }
+  float gt[3];
+  if (!clampd) {
+    gt[0] = gtxp; gt[1] = gtyp; gt[2] = gtz;
+  } else {
+    const float r2 = t[0] * t[0] + t[1] * t[1], r1 = sqrtf(r2), r3 = r2 * r1;
+    const float dxx = L * tz * t[1] * t[1] / r3, dxy = -L * tz * t[0] * t[1] / r3, dxz = L * t[0] / r1;
+    const float dyx = -L * tz * t[0] * t[1] / r3, dyy = L * tz * t[0] * t[0] / r3, dyz = L * t[1] / r1;
+    gt[0] = gtxp * dxx + gtyp * dyx;
+    gt[1] = gtxp * dxy + gtyp * dyy;
+    gt[2] = gtz + gtxp * dxz + gtyp * dyz;
+  }
+  for (int c = 0; c < 3; ++c)
+    for (int r = 0; r < 3; ++r) gm[c] += V[4 * c + r] * gt[r];
+  // Sigma = M M^T, M = R diag(s)
+  const float w = a.rotations[4 * i], x = a.rotations[4 * i + 1], y = a.rotations[4 * i + 2], z = a.rotations[4 * i + 3];
+  const float R[3][3] = {{1.f - 2.f * (y * y + z * z), 2.f * (x * y - w * z), 2.f * (x * z + w * y)},
+                         {2.f * (x * y + w * z), 1.f - 2.f * (x * x + z * z), 2.f * (y * z - w * x)},
+                         {2.f * (x * z - w * y), 2.f * (y * z + w * x), 1.f - 2.f * (x * x + y * y)}};
+  const float s[3] = {a.scales[3 * i], a.scales[3 * i + 1], a.scales[3 * i + 2]};
+  float dM[3][3];
+  for (int p = 0; p < 3; ++p)
+    for (int k = 0; k < 3; ++k) {
+      float acc = 0.f;
+      for (int q = 0; q < 3; ++q) acc += 0.5f * (Gf[p][q] + Gf[q][p]) * R[q][k] * s[k];
+      dM[p][k] = 2.f * acc;
+    }
+  for (int k = 0; k < 3; ++k) {
+    float acc = 0.f;
+    for (int p = 0; p < 3; ++p) acc += dM[p][k] * R[p][k];
+    a.dL_dscales[3 * i + k] = acc;
+  }
+  float dR[3][3];
+  for (int p = 0; p < 3; ++p)
+    for (int k = 0; k < 3; ++k) dR[p][k] = dM[p][k] * s[k];
+  a.dL_drotations[4 * i] = dR[0][1] * (-2.f * z) + dR[0][2] * (2.f * y) + dR[1][0] * (2.f * z) + dR[1][2] * (-2.f * x) +
+                           dR[2][0] * (-2.f * y) + dR[2][1] * (2.f * x);
+  a.dL_drotations[4 * i + 1] = dR[0][1] * (2.f * y) + dR[0][2] * (2.f * z) + dR[1][0] * (2.f * y) + dR[1][1] * (-4.f * x) +
+                               dR[1][2] * (-2.f * w) + dR[2][0] * (2.f * z) + dR[2][1] * (2.f * w) + dR[2][2] * (-4.f * x);
+  a.dL_drotations[4 * i + 2] = dR[0][0] * (-4.f * y) + dR[0][1] * (2.f * x) + dR[0][2] * (2.f * w) + dR[1][0] * (2.f * x) +
+                               dR[1][2] * (2.f * z) + dR[2][0] * (-2.f * w) + dR[2][1] * (2.f * z) + dR[2][2] * (-4.f * y);
+  a.dL_drotations[4 * i + 3] = dR[0][0] * (-4.f * z) + dR[0][1] * (-2.f * w) + dR[0][2] * (2.f * x) + dR[1][0] * (2.f * w) +
+                               dR[1][1] * (-4.f * z) + dR[1][2] * (2.f * y) + dR[2][0] * (2.f * x) + dR[2][1] * (2.f * y);
+  // colour: rgb = sum_k basis_k(dir) sh_k + 0.5 with the forward's constants
+  const float v0 = m0 - a.campos[0], v1 = m1 - a.campos[1], v2 = m2 - a.campos[2];
+  const float vn = sqrtf(v0 * v0 + v1 * v1 + v2 * v2);
+  const float X = v0 / vn, Y = v1 / vn, Z = v2 / vn;
+  const float gc0 = a.dL_dcolors[3 * i], gc1 = a.dL_dcolors[3 * i + 1], gc2 = a.dL_dcolors[3 * i + 2];
+  const float C1 = 0.4886025119029199f, C2a = 1.0925484305920792f, C2e = 0.5462742152960396f;
+  const float C30 = 0.5900435899266435f, C31 = 2.890611442640554f, C32 = 0.4570457994644658f;
+  const float C33 = 0.3731763325901154f, C35 = 1.445305721320277f;
+  const float xx = X * X, yy = Y * Y, zz = Z * Z;
+  float b[16], db[16][3];
+  for (int k = 0; k < 16; ++k) db[k][0] = db[k][1] = db[k][2] = 0.f;
+  b[0] = 0.28209479177387814f;
+  b[1] = -C1 * Y; db[1][1] = -C1;
+  b[2] = C1 * Z; db[2][2] = C1;
+  b[3] = -C1 * X; db[3][0] = -C1;
+  b[4] = C2a * X * Y; db[4][0] = C2a * Y; db[4][1] = C2a * X;
+  b[5] = -C2a * Y * Z; db[5][1] = -C2a * Z; db[5][2] = -C2a * Y;
+  b[6] = 0.3f * (2.f * zz - xx - yy); db[6][0] = -0.6f * X; db[6][1] = -0.6f * Y; db[6][2] = 1.2f * Z;
+  b[7] = -C2a * X * Z; db[7][0] = -C2a * Z; db[7][2] = -C2a * X;
+  b[8] = C2e * (xx - yy); db[8][0] = 2.f * C2e * X; db[8][1] = -2.f * C2e * Y;
+  b[9] = -C30 * Y * (3.f * xx - yy); db[9][0] = -6.f * C30 * X * Y; db[9][1] = -C30 * (3.f * xx - 3.f * yy);
+  b[10] = C31 * X * Y * Z; db[10][0] = C31 * Y * Z; db[10][1] = C31 * X * Z; db[10][2] = C31 * X * Y;
+  b[11] = -C32 * Y * (4.f * zz - xx - yy); db[11][0] = 2.f * C32 * X * Y; db[11][1] = -C32 * (4.f * zz - xx - 3.f * yy); db[11][2] = -8.f * C32 * Y * Z;
+  b[12] = C33 * Z * (2.f * zz - 3.f * xx - 3.f * yy); db[12][0] = -6.f * C33 * X * Z; db[12][1] = -6.f * C33 * Y * Z; db[12][2] = C33 * (6.f * zz - 3.f * xx - 3.f * yy);
+  b[13] = -C32 * X * (4.f * zz - xx - yy); db[13][0] = -C32 * (4.f * zz - 3.f * xx - yy); db[13][1] = 2.f * C32 * X * Y; db[13][2] = -8.f * C32 * X * Z;
+  b[14] = C35 * Z * (xx - yy); db[14][0] = 2.f * C35 * X * Z; db[14][1] = -2.f * C35 * Y * Z; db[14][2] = C35 * (xx - yy);
+  b[15] = -C30 * X * (xx - 3.f * yy); db[15][0] = -C30 * (3.f * xx - 3.f * yy); db[15][1] = 6.f * C30 * X * Y;
+  int de = a.degree > 3 ? 3 : a.degree;
+  while (de > 0 && (de + 1) * (de + 1) > M) --de;
+  const int nb = (de + 1) * (de + 1);
+  const float* shd = a.shs + size_t(i) * M * 3;
+  float gdir[3] = {0.f, 0.f, 0.f};
+  for (int k = 0; k < nb; ++k) {
+    dsh[3 * k] = b[k] * gc0;
+    dsh[3 * k + 1] = b[k] * gc1;
+    dsh[3 * k + 2] = b[k] * gc2;
+    const float sdot = shd[3 * k] * gc0 + shd[3 * k + 1] * gc1 + shd[3 * k + 2] * gc2;
+    gdir[0] += sdot * db[k][0];
+    gdir[1] += sdot * db[k][1];
+    gdir[2] += sdot * db[k][2];
+  }
+  for (int k = nb * 3; k < M * 3; ++k) dsh[k] = 0.f;
+  const float dd[3] = {X, Y, Z};
+  const float dot = dd[0] * gdir[0] + dd[1] * gdir[1] + dd[2] * gdir[2];
+  for (int p = 0; p < 3; ++p) gm[p] += (gdir[p] - dd[p] * dot) / vn;
+  a.dL_dmeans3D[3 * i] = gm[0];
+  a.dL_dmeans3D[3 * i + 1] = gm[1];
+  a.dL_dmeans3D[3 * i + 2] = gm[2];
+}
+
+}  // namespace
+
+void launch_backward_render(const BackwardArgs& a, cudaStream_t stream) {
+  const dim3 grid((a.W + kTile - 1) / kTile, (a.H + kTile - 1) / kTile);
+  if (grid.x == 0 || grid.y == 0) return;
+  if (a.grad_mode == 1) render_exact_kernel<<<grid, kBlendThreads, 0, stream>>>(a);
+  else render_ref_kernel<<<grid, kBlendThreads, 0, stream>>>(a);
+}
+
+void launch_backward_gaussians(const BackwardArgs& a, cudaStream_t stream) {
+  if (a.P <= 0) return;
+  const int blocks = (a.P + 255) / 256;
+  if (a.grad_mode == 1) gaussians_exact_kernel<<<blocks, 256, 0, stream>>>(a);
+  else gaussians_ref_kernel<<<blocks, 256, 0, stream>>>(a);
+}
+
+}  // namespace w2w

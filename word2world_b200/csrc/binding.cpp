@@ -1,0 +1,326 @@
+// Torch binding: the drop-in `rasterize_gaussians` / `rasterize_gaussians_backward`
+// pair with the reference extension's positional signatures and return tuples
+// (reference ext.cpp:5-7, rasterize_points.h:15-56, rasterize_points.cu:88-246),
+// plus the stage entry points used by tests and benchmarks.  Tensor checks and
+// allocation live here; all computation is the C ABI of libw2w_raster.so
+// (include/w2w_raster.h), enqueued on torch's current stream.
+#include <c10/cuda/CUDAGuard.h>
+#include <c10/cuda/CUDAStream.h>
+#include <torch/extension.h>
+
+#include <sstream>
+#include <stdexcept>
+#include <tuple>
+
+#include "../../include/w2w_raster.h"
+
+using torch::Tensor;
+
+namespace {
+
+void check(int rc, const char* what) {
+  if (rc != W2W_OK) {
+    std::ostringstream os;
+    os << what << " failed: " << w2w_status_string(rc) << " (status " << rc << ")";
+    throw std::runtime_error(os.str());
+  }
+}
+
+Tensor f32(const Tensor& t, const char* name, const torch::Device& dev) {
+  TORCH_CHECK(t.is_cuda(), name, " must be a CUDA tensor");
+  TORCH_CHECK(t.device() == dev, name, " must be on ", dev);
+  TORCH_CHECK(t.scalar_type() == torch::kFloat32, name, " must be float32");
+  return t.contiguous();
+}
+
+w2w_stream_t cur_stream() {
+  return reinterpret_cast<w2w_stream_t>(c10::cuda::getCurrentCUDAStream().stream());
+}
+
+struct Camera {
+  Tensor view, proj, campos, bg;
+};
+
+Camera camera(const Tensor& viewmatrix, const Tensor& projmatrix, const Tensor& campos,
+              const c10::optional<Tensor>& background, const torch::Device& dev) {
+  Camera c;
+  c.view = f32(viewmatrix, "viewmatrix", dev);
+  c.proj = f32(projmatrix, "projmatrix", dev);
+  c.campos = f32(campos, "campos", dev);
+  TORCH_CHECK(c.view.numel() == 16 && c.proj.numel() == 16, "view/projection matrices must have 16 elements");
+  TORCH_CHECK(c.campos.numel() == 3, "campos must have 3 elements");
+  if (background.has_value() && background->defined() && background->numel() > 0) {
+    c.bg = f32(*background, "background", dev);
+    TORCH_CHECK(c.bg.numel() == 3, "background must have 3 elements");
+  } else {
+    c.bg = torch::ones({3}, torch::TensorOptions().dtype(torch::kFloat32).device(dev));
+  }
+  return c;
+}
+
+std::tuple<int64_t, Tensor, Tensor, Tensor, Tensor, Tensor, Tensor, Tensor> rasterize_gaussians(
+    const Tensor& sh, double focal_y, const Tensor& scales, const Tensor& means3D, const Tensor& projmatrix,
+    int64_t degree, const Tensor& opacity, const Tensor& rotations, const Tensor& campos, const Tensor& viewmatrix,
+    double focal_x, int64_t image_height, int64_t image_width, const c10::optional<Tensor>& background,
+    bool compat_spill) {
+  (void)focal_y;  // the reference forward uses focal_x on both axes (projection.cu:100-101)
+  TORCH_CHECK(means3D.dim() == 2 && means3D.size(1) == 3, "means3D must be [P, 3]");
+  const auto dev = means3D.device();
+  const int64_t P = means3D.size(0);
+  c10::cuda::CUDAGuard guard(dev);
+  Tensor m = f32(means3D, "means3D", dev);
+  Tensor s = f32(scales, "scales", dev);
+  Tensor r = f32(rotations, "rotations", dev);
+  Tensor o = f32(opacity, "opacity", dev);
+  TORCH_CHECK(s.dim() == 2 && s.size(0) == P && s.size(1) == 3, "scales must be [P, 3]");
+  TORCH_CHECK(r.dim() == 2 && r.size(0) == P && r.size(1) == 4, "rotations must be [P, 4]");
+  TORCH_CHECK(o.numel() == P, "opacity must have P elements");
+  int64_t M = 0;
+  Tensor shc;
+  if (sh.numel() > 0) {
+    shc = f32(sh, "sh", dev);
+    TORCH_CHECK(shc.dim() == 3 && shc.size(0) == P && shc.size(2) == 3, "sh must be [P, M, 3]");
+    M = shc.size(1);
+  }
+  TORCH_CHECK(image_height > 0 && image_width > 0, "image size must be positive");
+  TORCH_CHECK(degree >= 0 && degree <= 3, "sh_degree must be in [0, 3]");
+  Camera cam = camera(viewmatrix, projmatrix, campos, background, dev);
+  const auto fopt = torch::TensorOptions().dtype(torch::kFloat32).device(dev);
+  const auto bopt = torch::TensorOptions().dtype(torch::kUInt8).device(dev);
+  const int W = int(image_width), H = int(image_height);
+  Tensor color = torch::empty({3, H, W}, fopt);
+  Tensor depth = torch::empty({1, H, W}, fopt);
+  Tensor alpha = torch::empty({1, H, W}, fopt);
+  Tensor radii = torch::empty({P}, torch::TensorOptions().dtype(torch::kInt32).device(dev));
+  Tensor geom = torch::empty({int64_t(w2w_geometry_state_bytes(int(P)))}, bopt);
+  Tensor img = torch::empty({int64_t(w2w_image_state_bytes(W, H))}, bopt);
+  w2w_settings st{};
+  st.P = int(P); st.degree = int(degree); st.M = int(M); st.width = W; st.height = H;
+  st.focal_x = float(focal_x);
+  st.tan_fovx = st.tan_fovy = 1.0f;
+  st.scale_modifier = 1.0f;
+  st.compat_spill = compat_spill ? 1 : 0;
+  st.viewmatrix = cam.view.data_ptr<float>();
+  st.projmatrix = cam.proj.data_ptr<float>();
+  st.campos = cam.campos.data_ptr<float>();
+  st.background = cam.bg.data_ptr<float>();
+  w2w_geometry_info info{};
+  const w2w_stream_t stream = cur_stream();
+  {
+    pybind11::gil_scoped_release nogil;
+    check(w2w_forward_geometry(&st, m.data_ptr<float>(), s.data_ptr<float>(), r.data_ptr<float>(),
+                               o.data_ptr<float>(), M > 0 ? shc.data_ptr<float>() : nullptr,
+                               radii.data_ptr<int>(), geom.data_ptr(), &info, stream),
+          "w2w_forward_geometry");
+  }
+  const int64_t R = info.num_rendered;
+  Tensor bin = torch::empty({int64_t(w2w_binning_state_bytes(R, W, H))}, bopt);
+  {
+    pybind11::gil_scoped_release nogil;
+    check(w2w_forward_render(&st, geom.data_ptr(), &info, bin.data_ptr(), img.data_ptr(), color.data_ptr<float>(),
+                             depth.data_ptr<float>(), alpha.data_ptr<float>(), stream),
+          "w2w_forward_render");
+  }
+  return std::make_tuple(R, color, depth, alpha, radii, geom, bin, img);
+}
+
+std::tuple<Tensor, Tensor, Tensor, Tensor, Tensor, Tensor, Tensor, Tensor> rasterize_gaussians_backward(
+    const Tensor& background, const Tensor& means3D, const Tensor& radii, const Tensor& colors_precomp,
+    const Tensor& scales, const Tensor& rotations, double scale_modifier, const Tensor& cov3D_precomp,
+    const Tensor& viewmatrix, const Tensor& projmatrix, double tan_fovx, double tan_fovy,
+    const Tensor& dL_dout_color, const Tensor& dL_dout_depth, const Tensor& dL_dout_alpha, const Tensor& sh,
+    int64_t degree, const Tensor& campos, const Tensor& geomBuffer, int64_t R, const Tensor& binningBuffer,
+    const Tensor& imageBuffer, const Tensor& alpha, bool debug, int64_t grad_mode) {
+  TORCH_CHECK(means3D.dim() == 2 && means3D.size(1) == 3, "means3D must be [P, 3]");
+  TORCH_CHECK(colors_precomp.numel() == 0 && cov3D_precomp.numel() == 0,
+              "precomputed colours / covariances are not supported: the forward always derives them from "
+              "SH coefficients, scales and rotations (as the reference forward does)");
+  TORCH_CHECK(grad_mode == 0 || grad_mode == 1, "grad_mode must be 0 (reference) or 1 (exact)");
+  const auto dev = means3D.device();
+  c10::cuda::CUDAGuard guard(dev);
+  const int64_t P = means3D.size(0);
+  Tensor m = f32(means3D, "means3D", dev);
+  Tensor s = f32(scales, "scales", dev);
+  Tensor r = f32(rotations, "rotations", dev);
+  Tensor g = f32(dL_dout_color, "dL_dout_color", dev);
+  TORCH_CHECK(g.dim() == 3 && g.size(0) == 3, "dL_dout_color must be [3, H, W]");
+  const int H = int(g.size(1)), W = int(g.size(2));
+  Tensor gd = f32(dL_dout_depth, "dL_dout_depth", dev);
+  Tensor ga = f32(dL_dout_alpha, "dL_dout_alpha", dev);
+  Tensor al = f32(alpha, "alpha", dev);
+  TORCH_CHECK(gd.numel() == int64_t(H) * W && ga.numel() == int64_t(H) * W && al.numel() == int64_t(H) * W,
+              "depth / alpha gradients and alpha must be [1, H, W]");
+  TORCH_CHECK(radii.is_cuda() && radii.scalar_type() == torch::kInt32 && radii.numel() == P, "radii must be int32 [P]");
+  Tensor rad = radii.contiguous();
+  int64_t M = 0;
+  Tensor shc;
+  if (sh.numel() > 0) {
+    shc = f32(sh, "sh", dev);
+    TORCH_CHECK(shc.dim() == 3 && shc.size(0) == P && shc.size(2) == 3, "sh must be [P, M, 3]");
+    M = shc.size(1);
+  }
+  TORCH_CHECK(geomBuffer.numel() >= int64_t(w2w_geometry_state_bytes(int(P))), "geomBuffer does not match P");
+  TORCH_CHECK(imageBuffer.numel() >= int64_t(w2w_image_state_bytes(W, H)), "imageBuffer does not match H, W");
+  TORCH_CHECK(binningBuffer.numel() >= int64_t(w2w_binning_state_bytes(R, W, H)), "binningBuffer does not match R");
+  Camera cam = camera(viewmatrix, projmatrix, campos, background, dev);
+  const auto fopt = torch::TensorOptions().dtype(torch::kFloat32).device(dev);
+  Tensor dmean2D = torch::empty({P, 3}, fopt), dcolors = torch::empty({P, 3}, fopt),
+         dopac = torch::empty({P, 1}, fopt), dmean3D = torch::empty({P, 3}, fopt),
+         dcov3D = torch::empty({P, 6}, fopt), dsh = torch::empty({P, M, 3}, fopt),
+         dscales = torch::empty({P, 3}, fopt), drot = torch::empty({P, 4}, fopt);
+  Tensor scratch = torch::empty({int64_t(w2w_backward_scratch_bytes(int(P)))},
+                                torch::TensorOptions().dtype(torch::kUInt8).device(dev));
+  w2w_settings st{};
+  st.P = int(P); st.degree = int(degree); st.M = int(M); st.width = W; st.height = H;
+  st.tan_fovx = float(tan_fovx); st.tan_fovy = float(tan_fovy);
+  st.focal_x = float(W / (2.0 * tan_fovx));
+  st.scale_modifier = float(scale_modifier);
+  st.viewmatrix = cam.view.data_ptr<float>();
+  st.projmatrix = cam.proj.data_ptr<float>();
+  st.campos = cam.campos.data_ptr<float>();
+  st.background = cam.bg.data_ptr<float>();
+  const w2w_stream_t stream = cur_stream();
+  {
+    pybind11::gil_scoped_release nogil;
+    check(w2w_backward(&st, m.data_ptr<float>(), s.data_ptr<float>(), r.data_ptr<float>(),
+                       M > 0 ? shc.data_ptr<float>() : nullptr, rad.data_ptr<int>(), geomBuffer.data_ptr(), R,
+                       binningBuffer.data_ptr(), imageBuffer.data_ptr(), al.data_ptr<float>(), g.data_ptr<float>(),
+                       gd.data_ptr<float>(), ga.data_ptr<float>(), int(grad_mode), scratch.data_ptr(),
+                       size_t(scratch.numel()), dmean2D.data_ptr<float>(), dcolors.data_ptr<float>(),
+                       dopac.data_ptr<float>(), dmean3D.data_ptr<float>(), dcov3D.data_ptr<float>(),
+                       M > 0 ? dsh.data_ptr<float>() : nullptr, dscales.data_ptr<float>(), drot.data_ptr<float>(),
+                       stream),
+          "w2w_backward");
+    if (debug) {
+      const int e = w2w_state_error(geomBuffer.data_ptr(), 0, stream);
+      if (e != 0) throw std::runtime_error("rasterizer device error word set: " + std::to_string(e));
+    }
+  }
+  return std::make_tuple(dmean2D, dcolors, dopac, dmean3D, dcov3D, dsh, dscales, drot);
+}
+
+// ---- stages ---------------------------------------------------------------
+
+std::tuple<Tensor, Tensor> sort_pairs_u64(const Tensor& keys, const Tensor& vals, int64_t begin_bit, int64_t end_bit) {
+  TORCH_CHECK(keys.is_cuda() && keys.scalar_type() == torch::kInt64, "keys must be a CUDA int64 tensor (raw u64 bits)");
+  TORCH_CHECK(vals.is_cuda() && vals.scalar_type() == torch::kInt32 && vals.numel() == keys.numel(),
+              "vals must be a CUDA int32 tensor with one value per key");
+  c10::cuda::CUDAGuard guard(keys.device());
+  Tensor k = keys.contiguous(), v = vals.contiguous();
+  const int64_t n = k.numel();
+  Tensor ko = torch::empty_like(k), vo = torch::empty_like(v);
+  Tensor scratch = torch::empty({int64_t(w2w_sort_scratch_bytes(n))}, k.options().dtype(torch::kUInt8));
+  check(w2w_sort_pairs_u64(reinterpret_cast<const uint64_t*>(k.data_ptr<int64_t>()),
+                           reinterpret_cast<const uint32_t*>(v.data_ptr<int>()),
+                           reinterpret_cast<uint64_t*>(ko.data_ptr<int64_t>()), reinterpret_cast<uint32_t*>(vo.data_ptr<int>()),
+                           n, int(begin_bit), int(end_bit), scratch.data_ptr(), size_t(scratch.numel()), cur_stream()),
+        "w2w_sort_pairs_u64");
+  return std::make_tuple(ko, vo);
+}
+
+Tensor scan_u32(const Tensor& x, bool exclusive) {
+  TORCH_CHECK(x.is_cuda() && x.scalar_type() == torch::kInt32, "x must be a CUDA int32 tensor (raw u32 bits)");
+  c10::cuda::CUDAGuard guard(x.device());
+  Tensor xi = x.contiguous();
+  Tensor out = torch::empty_like(xi);
+  const int64_t n = xi.numel();
+  Tensor scratch = torch::empty({int64_t(w2w_scan_scratch_bytes(n))}, xi.options().dtype(torch::kUInt8));
+  check(w2w_scan_u32(reinterpret_cast<const uint32_t*>(xi.data_ptr<int>()), reinterpret_cast<uint32_t*>(out.data_ptr<int>()),
+                     n, exclusive ? 1 : 0, scratch.data_ptr(), size_t(scratch.numel()), cur_stream()),
+        "w2w_scan_u32");
+  return out;
+}
+
+Tensor tile_ranges(const Tensor& sorted_keys, int64_t tile_shift, int64_t ntiles) {
+  TORCH_CHECK(sorted_keys.is_cuda() && sorted_keys.scalar_type() == torch::kInt64, "keys must be CUDA int64");
+  c10::cuda::CUDAGuard guard(sorted_keys.device());
+  Tensor k = sorted_keys.contiguous();
+  Tensor out = torch::empty({ntiles, 2}, k.options().dtype(torch::kInt32));
+  check(w2w_tile_ranges(reinterpret_cast<const uint64_t*>(k.data_ptr<int64_t>()), k.numel(), int(tile_shift),
+                        reinterpret_cast<uint32_t*>(out.data_ptr<int>()), int(ntiles), cur_stream()),
+        "w2w_tile_ranges");
+  return out;
+}
+
+std::tuple<Tensor, Tensor, Tensor, Tensor> blend(const Tensor& geomBuffer, int64_t P, const Tensor& ranges,
+                                                 const Tensor& point_list, int64_t image_height, int64_t image_width,
+                                                 const c10::optional<Tensor>& background) {
+  const auto dev = geomBuffer.device();
+  c10::cuda::CUDAGuard guard(dev);
+  const int W = int(image_width), H = int(image_height);
+  TORCH_CHECK(ranges.is_cuda() && ranges.scalar_type() == torch::kInt32 &&
+                  ranges.numel() == 2 * int64_t((W + 15) / 16) * ((H + 15) / 16),
+              "ranges must be int32 [tiles, 2]");
+  TORCH_CHECK(point_list.is_cuda() && point_list.scalar_type() == torch::kInt32, "point_list must be CUDA int32");
+  TORCH_CHECK(geomBuffer.numel() >= int64_t(w2w_geometry_state_bytes(int(P))), "geomBuffer does not match P");
+  Tensor rg = ranges.contiguous(), pl = point_list.contiguous();
+  Tensor bg = background.has_value() && background->numel() > 0
+                  ? f32(*background, "background", dev)
+                  : torch::ones({3}, torch::TensorOptions().dtype(torch::kFloat32).device(dev));
+  const auto fopt = torch::TensorOptions().dtype(torch::kFloat32).device(dev);
+  Tensor color = torch::empty({3, H, W}, fopt), depth = torch::empty({1, H, W}, fopt),
+         alpha = torch::empty({1, H, W}, fopt);
+  Tensor img = torch::empty({int64_t(w2w_image_state_bytes(W, H))}, fopt.dtype(torch::kUInt8));
+  w2w_settings st{};
+  st.P = int(P); st.width = W; st.height = H;
+  st.viewmatrix = bg.data_ptr<float>();  // unused by the blend; any device pointer
+  st.projmatrix = bg.data_ptr<float>();
+  st.campos = bg.data_ptr<float>();
+  st.background = bg.data_ptr<float>();
+  check(w2w_blend(&st, geomBuffer.data_ptr(), reinterpret_cast<const uint32_t*>(rg.data_ptr<int>()),
+                  pl.numel() ? reinterpret_cast<const uint32_t*>(pl.data_ptr<int>()) : nullptr, img.data_ptr(),
+                  color.data_ptr<float>(), depth.data_ptr<float>(), alpha.data_ptr<float>(), cur_stream()),
+        "w2w_blend");
+  return std::make_tuple(color, depth, alpha, img);
+}
+
+Tensor binning_keys64(const Tensor& binningBuffer, int64_t R, int64_t image_height, int64_t image_width) {
+  c10::cuda::CUDAGuard guard(binningBuffer.device());
+  Tensor out = torch::empty({R}, binningBuffer.options().dtype(torch::kInt64));
+  check(w2w_binning_keys64(binningBuffer.data_ptr(), R, int(image_width), int(image_height),
+                           reinterpret_cast<uint64_t*>(out.data_ptr<int64_t>()), cur_stream()),
+        "w2w_binning_keys64");
+  return out;
+}
+
+int64_t state_error(const Tensor& buf, int64_t which) {
+  c10::cuda::CUDAGuard guard(buf.device());
+  return w2w_state_error(buf.data_ptr(), int(which), cur_stream());
+}
+
+}  // namespace
+
+PYBIND11_MODULE(TORCH_EXTENSION_NAME, m) {
+  m.doc() = "sm_100a Gaussian rasterizer (drop-in for cudaForwardBackwardRenderer._C)";
+  m.def("rasterize_gaussians", &rasterize_gaussians, py::arg("sh"), py::arg("focal_y"), py::arg("scales"),
+        py::arg("means3D"), py::arg("projmatrix"), py::arg("sh_degree"), py::arg("opacity"), py::arg("rotations"),
+        py::arg("campos"), py::arg("viewmatrix"), py::arg("focal_x"), py::arg("image_height") = 800,
+        py::arg("image_width") = 800, py::arg("background") = py::none(), py::arg("compat_spill") = true);
+  m.def("rasterize_gaussians_backward", &rasterize_gaussians_backward, py::arg("background"), py::arg("means3D"),
+        py::arg("radii"), py::arg("colors_precomp"), py::arg("scales"), py::arg("rotations"),
+        py::arg("scale_modifier"), py::arg("cov3D_precomp"), py::arg("viewmatrix"), py::arg("projmatrix"),
+        py::arg("tan_fovx"), py::arg("tan_fovy"), py::arg("dL_dout_color"), py::arg("dL_dout_depth"),
+        py::arg("dL_dout_alpha"), py::arg("sh"), py::arg("degree"), py::arg("campos"), py::arg("geomBuffer"),
+        py::arg("R"), py::arg("binningBuffer"), py::arg("imageBuffer"), py::arg("alpha"), py::arg("debug"),
+        py::arg("grad_mode") = 0);
+  m.def("sort_pairs_u64", &sort_pairs_u64);
+  m.def("scan_u32", &scan_u32);
+  m.def("tile_ranges", &tile_ranges);
+  m.def("blend", &blend, py::arg("geomBuffer"), py::arg("P"), py::arg("ranges"), py::arg("point_list"),
+        py::arg("image_height"), py::arg("image_width"), py::arg("background") = py::none());
+  m.def("binning_keys64", &binning_keys64);
+  m.def("state_error", &state_error);
+  m.def("geometry_state_bytes", [](int64_t P) { return int64_t(w2w_geometry_state_bytes(int(P))); });
+  m.def("image_state_bytes", [](int64_t W, int64_t H) { return int64_t(w2w_image_state_bytes(int(W), int(H))); });
+  m.def("binning_state_bytes", [](int64_t R, int64_t W, int64_t H) {
+    return int64_t(w2w_binning_state_bytes(R, int(W), int(H)));
+  });
+  m.def("geometry_offset", [](int64_t P, const std::string& n) { return int64_t(w2w_geometry_offset(int(P), n.c_str())); });
+  m.def("image_offset", [](int64_t W, int64_t H, const std::string& n) {
+    return int64_t(w2w_image_offset(int(W), int(H), n.c_str()));
+  });
+  m.def("binning_offset", [](int64_t R, int64_t W, int64_t H, const std::string& n) {
+    return int64_t(w2w_binning_offset(R, int(W), int(H), n.c_str()));
+  });
+  m.def("version", &w2w_version);
+}

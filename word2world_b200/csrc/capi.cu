@@ -1,0 +1,467 @@
+// C ABI of the rasterizer (declared in include/w2w_raster.h): host
+// orchestration of the kernels, state-buffer layouts and argument checks.
+// The library never allocates device memory; every buffer comes from the
+// caller.  All work is enqueued on the caller's stream.
+#include <cstdio>
+#include <cstring>
+
+#include "../../include/w2w_raster.h"
+#include "common.cuh"
+#include "kernels.h"
+
+using namespace w2w;
+
+namespace {
+
+inline cudaStream_t S(w2w_stream_t s) { return reinterpret_cast<cudaStream_t>(s); }
+
+inline int check_launch() {
+  const cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) {
+    std::fprintf(stderr, "w2w: CUDA error: %s\n", cudaGetErrorString(e));
+    return W2W_ERR_CUDA;
+  }
+  return W2W_OK;
+}
+
+inline int tiles_x(int W) { return (W + kTile - 1) / kTile; }
+inline int tiles_y(int H) { return (H + kTile - 1) / kTile; }
+inline int num_tiles(int W, int H) { return tiles_x(W) * tiles_y(H); }
+
+inline int ceil_log2(uint32_t v) {  // bits needed for values in [0, v)
+  if (v <= 1) return 0;
+  int b = 0;
+  uint32_t x = v - 1;
+  while (x) { ++b; x >>= 1; }
+  return b;
+}
+
+bool settings_ok(const w2w_settings* s) {
+  return s && s->P >= 0 && s->width > 0 && s->height > 0 && s->M >= 0 && s->degree >= 0 &&
+         s->viewmatrix && s->projmatrix && s->campos && s->background && s->width < 65535 * kTile &&
+         s->height < 65535 * kTile;
+}
+
+template <typename T>
+T* at(void* base, size_t off) { return reinterpret_cast<T*>(static_cast<unsigned char*>(base) + off); }
+template <typename T>
+const T* at(const void* base, size_t off) {
+  return reinterpret_cast<const T*>(static_cast<const unsigned char*>(base) + off);
+}
+
+// Sort key layout, chosen on the host from the instance count, the tile
+// count and the depth-bit range: only the bits in which keys can differ are
+// sorted on, packed into 32 bits when they fit.
+struct KeyPlan {
+  int key64, depth_bits, tile_bits, bits;
+  uint32_t prefix;
+};
+KeyPlan plan_keys(const w2w_geometry_info& info, int W, int H) {
+  KeyPlan k{};
+  const uint32_t dmin = info.depth_min_bits, dmax = info.depth_max_bits;
+  const uint32_t x = dmin ^ dmax;
+  int db = 0;
+  while (db < 32 && (x >> db) != 0u) ++db;
+  k.depth_bits = db;
+  k.prefix = db >= 32 ? 0u : (dmin & ~((1u << db) - 1u));
+  k.tile_bits = ceil_log2(uint32_t(num_tiles(W, H)));
+  k.bits = k.tile_bits + k.depth_bits;
+  k.key64 = k.bits > 32 ? 1 : 0;
+  return k;
+}
+
+__global__ void write_bin_header(BinHeader* h, KeyPlan k, uint32_t R, uint32_t passes) {
+  h->error = 0;
+  h->key64 = k.key64;
+  h->depth_bits = k.depth_bits;
+  h->depth_prefix = k.prefix;
+  h->tile_bits = k.tile_bits;
+  h->passes = passes;
+  h->num_rendered = R;
+  for (int i = 0; i < 8; ++i) h->tile_counter[i] = 0;
+}
+
+template <typename K>
+__global__ void expand_keys(const BinHeader* h, const K* keys, long long n, uint64_t* out) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const uint32_t db = h->depth_bits;
+  const uint64_t k = uint64_t(keys[i]);
+  const uint64_t tile = db >= 64 ? 0 : (k >> db);
+  const uint32_t low = db >= 32 ? uint32_t(k) : uint32_t(k & ((1ull << db) - 1ull));
+  out[i] = (tile << 32) | uint64_t(h->depth_prefix | low);
+}
+
+__global__ void ranges_from_sorted(const uint64_t* keys, long long n, int shift, uint2* ranges, int ntiles) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const uint64_t t = keys[i] >> shift;
+  if (t >= uint64_t(ntiles)) return;
+  if (i == 0 || (keys[i - 1] >> shift) != t) ranges[t].x = uint32_t(i);
+  if (i == n - 1 || (keys[i + 1] >> shift) != t) ranges[t].y = uint32_t(i + 1);
+}
+
+size_t sort_scratch_layout(long long n, size_t* keys_tmp, size_t* vals_tmp, size_t* hist, size_t* status,
+                           size_t* counters, size_t* err) {
+  size_t o = 0;
+  auto take = [&](size_t bytes) { size_t a = align256(o); o = a + bytes; return a; };
+  const size_t nn = size_t(n > 0 ? n : 1);
+  *keys_tmp = take(nn * 8);
+  *vals_tmp = take(nn * 4);
+  *hist = take(size_t(kMaxPasses) * 256 * 4);
+  *status = take(sort_status_words(n) * 4);
+  *counters = take(kMaxPasses * 4);
+  *err = take(4);
+  return align256(o);
+}
+
+}  // namespace
+
+extern "C" {
+
+int w2w_version(void) { return 1; }
+
+const char* w2w_status_string(int status) {
+  switch (status) {
+    case W2W_OK: return "ok";
+    case W2W_ERR_INVALID: return "invalid argument";
+    case W2W_ERR_CUDA: return "CUDA error";
+    case W2W_ERR_CAPACITY: return "capacity exceeded";
+    case W2W_ERR_TIMEOUT: return "device wait timed out";
+    case W2W_ERR_SCRATCH: return "scratch buffer too small";
+    default: return "unknown status";
+  }
+}
+
+size_t w2w_geometry_state_bytes(int P) { return P < 0 ? 0 : GeomLayout(P).total; }
+size_t w2w_image_state_bytes(int W, int H) { return (W <= 0 || H <= 0) ? 0 : ImageLayout(W, H).total; }
+size_t w2w_binning_state_bytes(long long R, int W, int H) {
+  if (R < 0 || W <= 0 || H <= 0) return 0;
+  return BinLayout(R, num_tiles(W, H)).total;
+}
+size_t w2w_backward_scratch_bytes(int P) {
+  return P < 0 ? 0 : align256(size_t(P) * 16) + align256(size_t(P) * 4);
+}
+
+size_t w2w_geometry_offset(int P, const char* name) {
+  const GeomLayout L(P);
+  if (!name) return size_t(-1);
+  if (!strcmp(name, "header")) return L.header;
+  if (!strcmp(name, "depth")) return L.depth;
+  if (!strcmp(name, "clamped")) return L.clamped;
+  if (!strcmp(name, "means2D")) return L.means2D;
+  if (!strcmp(name, "cov3D")) return L.cov3D;
+  if (!strcmp(name, "conic_opacity")) return L.conic;
+  if (!strcmp(name, "rgb")) return L.rgb;
+  if (!strcmp(name, "tiles_touched")) return L.tiles;
+  if (!strcmp(name, "offsets")) return L.offsets;
+  if (!strcmp(name, "rect")) return L.rect;
+  if (!strcmp(name, "prev_reach")) return L.prev_reach;
+  if (!strcmp(name, "record")) return L.record;
+  if (!strcmp(name, "bwd_record")) return L.bwd_record;
+  return size_t(-1);
+}
+
+size_t w2w_image_offset(int W, int H, const char* name) {
+  const ImageLayout L(W, H);
+  if (!name) return size_t(-1);
+  if (!strcmp(name, "n_contrib")) return L.n_contrib;
+  if (!strcmp(name, "ranges")) return L.ranges;
+  if (!strcmp(name, "T_final")) return L.T_final;
+  if (!strcmp(name, "tile_max")) return L.tile_max;
+  return size_t(-1);
+}
+
+size_t w2w_binning_offset(long long R, int W, int H, const char* name) {
+  const BinLayout L(R, num_tiles(W, H));
+  if (!name) return size_t(-1);
+  if (!strcmp(name, "header")) return L.header;
+  if (!strcmp(name, "keys_a")) return L.keysA;
+  if (!strcmp(name, "keys_b")) return L.keysB;
+  if (!strcmp(name, "vals_a")) return L.valsA;
+  if (!strcmp(name, "vals_b")) return L.valsB;
+  return size_t(-1);
+}
+
+int w2w_forward_geometry(const w2w_settings* s, const float* means3D, const float* scales, const float* rotations,
+                         const float* opacities, const float* shs, int* radii, void* geom_state,
+                         w2w_geometry_info* info, w2w_stream_t stream) {
+  if (!settings_ok(s) || !info || (s->P > 0 && (!means3D || !scales || !rotations || !opacities || !radii ||
+                                                !geom_state || (s->M > 0 && !shs))))
+    return W2W_ERR_INVALID;
+  std::memset(info, 0, sizeof(*info));
+  if (s->P == 0) return W2W_OK;
+  const GeomLayout L(s->P);
+  cudaStream_t st = S(stream);
+  cudaMemsetAsync(geom_state, 0, L.depth, st);  // header + scan status
+  PreprocessArgs a{};
+  a.P = s->P; a.W = s->width; a.H = s->height; a.degree = s->degree; a.M = s->M;
+  a.compat_spill = s->compat_spill;
+  a.focal_x = s->focal_x;
+  a.view = s->viewmatrix; a.proj = s->projmatrix; a.campos = s->campos;
+  a.means3D = means3D; a.scales = scales; a.rotations = rotations; a.opacities = opacities; a.shs = shs;
+  a.radii = radii;
+  a.header = at<GeomHeader>(geom_state, L.header);
+  a.scan_status = at<unsigned long long>(geom_state, L.scan_status);
+  a.depth = at<float>(geom_state, L.depth);
+  a.clamped = at<uint8_t>(geom_state, L.clamped);
+  a.means2D = at<float>(geom_state, L.means2D);
+  a.cov3D = at<float>(geom_state, L.cov3D);
+  a.conic = at<float>(geom_state, L.conic);
+  a.rgb = at<float>(geom_state, L.rgb);
+  a.tiles = at<uint32_t>(geom_state, L.tiles);
+  a.offsets = at<uint32_t>(geom_state, L.offsets);
+  a.rect = at<uint32_t>(geom_state, L.rect);
+  a.prev_reach = at<uint32_t>(geom_state, L.prev_reach);
+  a.record = at<float>(geom_state, L.record);
+  a.bwd_record = at<float>(geom_state, L.bwd_record);
+  launch_preprocess(a, st);
+  int rc = check_launch();
+  if (rc) return rc;
+  GeomHeader h;
+  if (cudaMemcpyAsync(&h, a.header, sizeof(h), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+      cudaStreamSynchronize(st) != cudaSuccess)
+    return W2W_ERR_CUDA;
+  info->num_rendered = h.num_rendered;
+  info->depth_min_bits = ~h.depth_min;
+  info->depth_max_bits = h.depth_max;
+  info->error = h.error;
+  if (h.error & kErrTimeout) return W2W_ERR_TIMEOUT;
+  if (h.error & kErrCapacity) return W2W_ERR_CAPACITY;
+  return W2W_OK;
+}
+
+int w2w_forward_render(const w2w_settings* s, const void* geom_state, const w2w_geometry_info* info,
+                       void* binning_state, void* image_state, float* out_color, float* out_depth,
+                       float* out_alpha, w2w_stream_t stream) {
+  if (!settings_ok(s) || !info || !image_state || !out_color || !out_depth || !out_alpha) return W2W_ERR_INVALID;
+  const long long R = info->num_rendered;
+  if (R < 0 || R >= (1LL << 30)) return W2W_ERR_CAPACITY;
+  if (R > 0 && (!geom_state || !binning_state)) return W2W_ERR_INVALID;
+  cudaStream_t st = S(stream);
+  const int W = s->width, H = s->height, T = num_tiles(W, H);
+  const ImageLayout IL(W, H);
+  uint2* ranges = at<uint2>(image_state, IL.ranges);
+  const uint32_t* point_list = nullptr;
+  if (R == 0) {
+    cudaMemsetAsync(ranges, 0, sizeof(uint2) * size_t(T), st);
+  } else {
+    const GeomLayout GL(s->P);
+    const BinLayout BL(R, T);
+    const KeyPlan kp = plan_keys(*info, W, H);
+    const int passes = sort_passes(kp.bits);
+    BinHeader* bh = at<BinHeader>(binning_state, BL.header);
+    write_bin_header<<<1, 1, 0, st>>>(bh, kp, uint32_t(R), uint32_t(passes));
+    // the sort result lands in (keysA, valsA); key emission targets the
+    // buffer that makes the ping-pong end there
+    const bool odd = (passes % 2) == 1;
+    void* keysA = at<void>(binning_state, BL.keysA);
+    void* keysB = at<void>(binning_state, BL.keysB);
+    uint32_t* valsA = at<uint32_t>(binning_state, BL.valsA);
+    uint32_t* valsB = at<uint32_t>(binning_state, BL.valsB);
+    DuplicateArgs d{};
+    d.P = s->P; d.gw = tiles_x(W); d.R = uint32_t(R); d.key64 = kp.key64; d.depth_bits = uint32_t(kp.depth_bits);
+    d.tiles = at<uint32_t>(geom_state, GL.tiles);
+    d.offsets = at<uint32_t>(geom_state, GL.offsets);
+    d.rect = at<uint32_t>(geom_state, GL.rect);
+    d.prev_reach = at<uint32_t>(geom_state, GL.prev_reach);
+    d.depth = at<float>(geom_state, GL.depth);
+    d.keys = odd ? keysB : keysA;
+    d.vals = odd ? valsB : valsA;
+    launch_duplicate(d, st);
+    SortArgs so{};
+    so.n = R; so.key64 = kp.key64; so.begin_bit = 0; so.bits = kp.bits;
+    so.keys_in = d.keys; so.vals_in = d.vals;
+    so.keys_out = keysA; so.vals_out = valsA;
+    so.keys_tmp = keysB; so.vals_tmp = valsB;
+    so.hist = at<uint32_t>(binning_state, BL.hist);
+    so.status = at<uint32_t>(binning_state, BL.status);
+    so.counters = bh->tile_counter;
+    so.error = &bh->error;
+    so.tile_shift = kp.depth_bits;
+    so.num_tiles = T;
+    so.tile_hist = at<uint32_t>(binning_state, BL.tile_hist);
+    so.ranges = ranges;
+    launch_sort(so, st);
+    point_list = valsA;
+  }
+  BlendArgs b{};
+  b.W = W; b.H = H;
+  b.ranges = ranges;
+  b.point_list = point_list;
+  b.record = R > 0 ? at<float>(geom_state, GeomLayout(s->P).record) : nullptr;
+  b.bg = s->background;
+  b.out_color = out_color; b.out_depth = out_depth; b.out_alpha = out_alpha;
+  b.n_contrib = at<uint32_t>(image_state, IL.n_contrib);
+  b.T_final = at<float>(image_state, IL.T_final);
+  b.tile_max = at<uint32_t>(image_state, IL.tile_max);
+  launch_blend(b, st);
+  return check_launch();
+}
+
+int w2w_state_error(const void* state, int which, w2w_stream_t stream) {
+  if (!state) return -1;
+  uint32_t e = 0;
+  cudaStream_t st = S(stream);
+  if (cudaMemcpyAsync(&e, state, 4, cudaMemcpyDeviceToHost, st) != cudaSuccess || cudaStreamSynchronize(st) != cudaSuccess)
+    return -1;
+  (void)which;  // both headers start with their error word
+  return int(e);
+}
+
+int w2w_backward(const w2w_settings* s, const float* means3D, const float* scales, const float* rotations,
+                 const float* shs, const int* radii, const void* geom_state,
+                 long long R, const void* binning_state, const void* image_state, const float* out_alpha,
+                 const float* dL_dcolor, const float* dL_ddepth, const float* dL_dalpha, int grad_mode,
+                 void* scratch, size_t scratch_bytes, float* dL_dmeans2D, float* dL_dcolors, float* dL_dopacity,
+                 float* dL_dmeans3D, float* dL_dcov3D, float* dL_dsh, float* dL_dscales, float* dL_drotations,
+                 w2w_stream_t stream) {
+  if (!settings_ok(s) || (grad_mode != 0 && grad_mode != 1)) return W2W_ERR_INVALID;
+  const int P = s->P;
+  if (P == 0) return W2W_OK;
+  if (!means3D || !scales || !rotations || !radii || !geom_state || !image_state || !out_alpha ||
+      !dL_dcolor || !dL_ddepth || !dL_dalpha || !dL_dmeans2D || !dL_dcolors || !dL_dopacity || !dL_dmeans3D ||
+      !dL_dcov3D || !dL_dscales || !dL_drotations || (s->M > 0 && (!shs || !dL_dsh)) || (R > 0 && !binning_state))
+    return W2W_ERR_INVALID;
+  if (!scratch || scratch_bytes < w2w_backward_scratch_bytes(P)) return W2W_ERR_SCRATCH;
+  cudaStream_t st = S(stream);
+  const int W = s->width, H = s->height;
+  const GeomLayout GL(P);
+  const ImageLayout IL(W, H);
+  float* acc_cov = static_cast<float*>(scratch);
+  float* acc_depth = at<float>(scratch, align256(size_t(P) * 16));
+  cudaMemsetAsync(scratch, 0, w2w_backward_scratch_bytes(P), st);
+  cudaMemsetAsync(dL_dmeans2D, 0, sizeof(float) * 3 * size_t(P), st);
+  cudaMemsetAsync(dL_dcolors, 0, sizeof(float) * 3 * size_t(P), st);
+  cudaMemsetAsync(dL_dopacity, 0, sizeof(float) * size_t(P), st);
+  BackwardArgs a{};
+  a.P = P; a.W = W; a.H = H; a.degree = s->degree; a.M = s->M; a.grad_mode = grad_mode;
+  a.h_x = float(W) / (2.0f * s->tan_fovx);
+  a.h_y = float(H) / (2.0f * s->tan_fovy);
+  a.focal_x = a.h_x;  // exact mode: the forward's focal under the W / (2 tan) convention
+  a.tan_fovx = s->tan_fovx; a.tan_fovy = s->tan_fovy;
+  a.scale_modifier = s->scale_modifier;
+  a.view = s->viewmatrix; a.proj = s->projmatrix; a.campos = s->campos; a.bg = s->background;
+  a.means3D = means3D; a.scales = scales; a.rotations = rotations; a.shs = shs;
+  a.radii = radii;
+  a.cov3D = at<float>(geom_state, GL.cov3D);
+  a.clamped = at<uint8_t>(geom_state, GL.clamped);
+  a.record = at<float>(geom_state, GL.record);
+  a.bwd_record = at<float>(geom_state, GL.bwd_record);
+  a.ranges = at<uint2>(image_state, IL.ranges);
+  a.point_list = R > 0 ? at<uint32_t>(binning_state, BinLayout(R, num_tiles(W, H)).valsA) : nullptr;
+  a.n_contrib = at<uint32_t>(image_state, IL.n_contrib);
+  a.tile_max = at<uint32_t>(image_state, IL.tile_max);
+  a.T_final = at<float>(image_state, IL.T_final);
+  a.out_alpha = out_alpha;
+  a.dL_dcolor = dL_dcolor; a.dL_ddepth = dL_ddepth; a.dL_dalpha = dL_dalpha;
+  a.dL_dmean2D = dL_dmeans2D; a.acc_cov = acc_cov; a.dL_dopacity = dL_dopacity; a.dL_dcolors = dL_dcolors;
+  a.acc_depth = acc_depth;
+  a.dL_dmeans3D = dL_dmeans3D; a.dL_dcov3D = dL_dcov3D; a.dL_dsh = dL_dsh; a.dL_dscales = dL_dscales;
+  a.dL_drotations = dL_drotations;
+  if (R > 0) launch_backward_render(a, st);
+  launch_backward_gaussians(a, st);
+  return check_launch();
+}
+
+size_t w2w_sort_scratch_bytes(long long n) {
+  size_t a, b, c, d, e, f;
+  return sort_scratch_layout(n, &a, &b, &c, &d, &e, &f);
+}
+
+int w2w_sort_pairs_u64(const uint64_t* keys_in, const uint32_t* vals_in, uint64_t* keys_out, uint32_t* vals_out,
+                       long long n, int begin_bit, int end_bit, void* scratch, size_t scratch_bytes,
+                       w2w_stream_t stream) {
+  if (n < 0 || begin_bit < 0 || end_bit > 64 || end_bit < begin_bit) return W2W_ERR_INVALID;
+  if (n == 0) return W2W_OK;
+  if (!keys_in || !vals_in || !keys_out || !vals_out || keys_in == keys_out || vals_in == vals_out)
+    return W2W_ERR_INVALID;
+  if (n >= (1LL << 30)) return W2W_ERR_CAPACITY;
+  size_t kt, vt, hi, stt, ct, er;
+  const size_t need = sort_scratch_layout(n, &kt, &vt, &hi, &stt, &ct, &er);
+  if (!scratch || scratch_bytes < need) return W2W_ERR_SCRATCH;
+  cudaStream_t st = S(stream);
+  cudaMemsetAsync(at<uint32_t>(scratch, er), 0, 4, st);
+  SortArgs so{};
+  so.n = n; so.key64 = 1; so.begin_bit = begin_bit; so.bits = end_bit - begin_bit;
+  so.keys_in = keys_in; so.vals_in = vals_in;
+  so.keys_out = keys_out; so.vals_out = vals_out;
+  so.keys_tmp = at<void>(scratch, kt); so.vals_tmp = at<uint32_t>(scratch, vt);
+  so.hist = at<uint32_t>(scratch, hi);
+  so.status = at<uint32_t>(scratch, stt);
+  so.counters = at<uint32_t>(scratch, ct);
+  so.error = at<uint32_t>(scratch, er);
+  so.tile_shift = 0; so.num_tiles = 0; so.tile_hist = nullptr; so.ranges = nullptr;
+  launch_sort(so, st);
+  return check_launch();
+}
+
+size_t w2w_scan_scratch_bytes(long long n) { return align256(scan_status_words(n) * 8) + 256; }
+
+int w2w_scan_u32(const uint32_t* in, uint32_t* out, long long n, int exclusive, void* scratch,
+                 size_t scratch_bytes, w2w_stream_t stream) {
+  if (n < 0) return W2W_ERR_INVALID;
+  if (n == 0) return W2W_OK;
+  if (!in || !out) return W2W_ERR_INVALID;
+  if (!scratch || scratch_bytes < w2w_scan_scratch_bytes(n)) return W2W_ERR_SCRATCH;
+  unsigned long long* status = static_cast<unsigned long long*>(scratch);
+  uint32_t* tail = at<uint32_t>(scratch, align256(scan_status_words(n) * 8));
+  cudaStream_t st = S(stream);
+  cudaMemsetAsync(tail, 0, 8, st);
+  launch_scan(in, out, n, exclusive, status, tail, tail + 1, st);
+  return check_launch();
+}
+
+int w2w_tile_ranges(const uint64_t* sorted_keys, long long n, int tile_shift, uint32_t* ranges, int ntiles,
+                    w2w_stream_t stream) {
+  if (n < 0 || ntiles <= 0 || !ranges || (n > 0 && !sorted_keys) || tile_shift < 0 || tile_shift > 63)
+    return W2W_ERR_INVALID;
+  cudaStream_t st = S(stream);
+  cudaMemsetAsync(ranges, 0, sizeof(uint2) * size_t(ntiles), st);
+  if (n > 0)
+    ranges_from_sorted<<<int((n + 255) / 256), 256, 0, st>>>(sorted_keys, n, tile_shift,
+                                                              reinterpret_cast<uint2*>(ranges), ntiles);
+  return check_launch();
+}
+
+int w2w_blend(const w2w_settings* s, const void* geom_state, const uint32_t* ranges, const uint32_t* point_list,
+              void* image_state, float* out_color, float* out_depth, float* out_alpha, w2w_stream_t stream) {
+  if (!settings_ok(s) || !geom_state || !ranges || !image_state || !out_color || !out_depth || !out_alpha)
+    return W2W_ERR_INVALID;
+  const ImageLayout IL(s->width, s->height);
+  // keep the ranges in the image state so it is complete for a backward pass
+  uint2* own = at<uint2>(image_state, IL.ranges);
+  if (reinterpret_cast<const void*>(own) != reinterpret_cast<const void*>(ranges))
+    cudaMemcpyAsync(own, ranges, sizeof(uint2) * size_t(num_tiles(s->width, s->height)), cudaMemcpyDeviceToDevice,
+                    S(stream));
+  BlendArgs b{};
+  b.W = s->width; b.H = s->height;
+  b.ranges = own;
+  b.point_list = point_list;
+  b.record = at<float>(geom_state, GeomLayout(s->P).record);
+  b.bg = s->background;
+  b.out_color = out_color; b.out_depth = out_depth; b.out_alpha = out_alpha;
+  b.n_contrib = at<uint32_t>(image_state, IL.n_contrib);
+  b.T_final = at<float>(image_state, IL.T_final);
+  b.tile_max = at<uint32_t>(image_state, IL.tile_max);
+  launch_blend(b, S(stream));
+  return check_launch();
+}
+
+int w2w_binning_keys64(const void* binning_state, long long R, int W, int H, uint64_t* out, w2w_stream_t stream) {
+  if (R < 0 || !out || (R > 0 && !binning_state)) return W2W_ERR_INVALID;
+  if (R == 0) return W2W_OK;
+  const BinLayout BL(R, num_tiles(W, H));
+  const BinHeader* h = at<BinHeader>(binning_state, BL.header);
+  BinHeader hh;
+  cudaStream_t st = S(stream);
+  if (cudaMemcpyAsync(&hh, h, sizeof(hh), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+      cudaStreamSynchronize(st) != cudaSuccess)
+    return W2W_ERR_CUDA;
+  const int blocks = int((R + 255) / 256);
+  if (hh.key64) expand_keys<uint64_t><<<blocks, 256, 0, st>>>(h, at<uint64_t>(binning_state, BL.keysA), R, out);
+  else expand_keys<uint32_t><<<blocks, 256, 0, st>>>(h, at<uint32_t>(binning_state, BL.keysA), R, out);
+  return check_launch();
+}
+
+}  // extern "C"

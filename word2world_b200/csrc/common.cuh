@@ -1,0 +1,228 @@
+// Shared device-side definitions for the sm_100a Gaussian rasterizer.
+//
+// Floating point: every operation whose rounding affects a bit-exact output
+// (projection, ADR culling, key depth bits, blend decisions) is written with
+// explicit-rounding intrinsics (__fmul_rn, __fadd_rn, __fmaf_rn, __fdiv_rn,
+// __fsqrt_rn, __frcp_rn), which the compiler never contracts.  Where the
+// reference's compiler fused a multiply into an add, the same fusion is
+// written out here; the per-expression choices were established by comparing
+// against the reference extension's own buffers on a B200 and are listed in
+// pinned_fp.h (the CPU oracle carries the identical table).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "pinned_fp.h"
+
+namespace w2w {
+
+constexpr int kTile = 16;             // tile edge in pixels (reference: 16x16)
+constexpr int kBlendThreads = 256;    // one thread per tile pixel
+constexpr int kBatch = 256;           // Gaussians staged per shared-memory batch
+
+// Status codes written to the device error word (bitwise OR).
+enum : uint32_t {
+  kErrNone = 0,
+  kErrCapacity = 1u << 0,   // more instances than the binning state holds
+  kErrTimeout = 1u << 1,    // a bounded spin wait gave up
+  kErrRange = 1u << 2,      // an index fell outside its buffer and was skipped
+};
+
+// ---------------------------------------------------------------------------
+// explicit-rounding arithmetic
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ float mul(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ float add(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ float sub(float a, float b) { return __fsub_rn(a, b); }
+__device__ __forceinline__ float fma(float a, float b, float c) { return __fmaf_rn(a, b, c); }
+__device__ __forceinline__ float div(float a, float b) { return __fdiv_rn(a, b); }
+
+// a*b + c*d: 0 = both rounded, 1 = fuse a*b, 2 = fuse c*d
+template <int V>
+__device__ __forceinline__ float s2(float a, float b, float c, float d) {
+  if constexpr (V == 1) return fma(a, b, mul(c, d));
+  else if constexpr (V == 2) return fma(c, d, mul(a, b));
+  else return add(mul(a, b), mul(c, d));
+}
+// a*b - c*d
+template <int V>
+__device__ __forceinline__ float d2(float a, float b, float c, float d) {
+  if constexpr (V == 1) return fma(a, b, -mul(c, d));
+  else if constexpr (V == 2) return fma(-c, d, mul(a, b));
+  else return sub(mul(a, b), mul(c, d));
+}
+// (a*b + c*d) + e*f
+template <int V>
+__device__ __forceinline__ float s3(float a, float b, float c, float d, float e, float f) {
+  if constexpr (V == 1) return fma(e, f, fma(a, b, mul(c, d)));
+  else if constexpr (V == 2) return fma(e, f, fma(c, d, mul(a, b)));
+  else if constexpr (V == 3) return fma(e, f, add(mul(a, b), mul(c, d)));
+  else if constexpr (V == 4) return add(fma(a, b, mul(c, d)), mul(e, f));
+  else if constexpr (V == 5) return add(fma(c, d, mul(a, b)), mul(e, f));
+  else if constexpr (V == 6) return fma(a, b, fma(c, d, mul(e, f)));
+  else return add(add(mul(a, b), mul(c, d)), mul(e, f));
+}
+// a*b + c
+template <int V>
+__device__ __forceinline__ float s1(float a, float b, float c) {
+  if constexpr (V != 0) return fma(a, b, c);
+  else return add(mul(a, b), c);
+}
+
+// Row r of (column-major 4x4 m) * (x, y, z, 1): (m0 x + m1 y) + (m2 z + m3).
+template <int VA, int VB>
+__device__ __forceinline__ float m4row(const float* m, int r, float x, float y, float z) {
+  return add(s2<VA>(m[r], x, m[4 + r], y), s1<VB>(m[8 + r], z, m[12 + r]));
+}
+
+// ---------------------------------------------------------------------------
+// Per-Gaussian blend record: everything the per-pixel loops need, 48 bytes.
+// ---------------------------------------------------------------------------
+struct __align__(16) BlendRecord {
+  float mx, my;          // screen position (pixels)
+  float cxx, cxy, cyy;   // 2-D covariance
+  float det;             // the blend's own determinant of the covariance
+  float opacity;
+  float depth;           // NDC z
+  float r, g, b;         // colour (unclamped)
+  float pad;
+};
+static_assert(sizeof(BlendRecord) == 48, "BlendRecord layout");
+
+// Per-Gaussian record read by the reference-formula backward pass, 48 bytes.
+struct __align__(16) BackwardRecord {
+  float mx, my;
+  float conic_a, conic_b, conic_c;  // inverse 2-D covariance
+  float opacity;
+  float depth;
+  float r, g, b;
+  float pad0, pad1;
+};
+static_assert(sizeof(BackwardRecord) == 48, "BackwardRecord layout");
+
+// ---------------------------------------------------------------------------
+// State layouts.  All arrays start on 256-byte boundaries.
+// ---------------------------------------------------------------------------
+__host__ __device__ constexpr size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
+
+// Device-written header at the start of the geometry state.
+struct GeomHeader {
+  uint32_t error;          // kErr* bits
+  uint32_t depth_min;      // min/max of depth bits over Gaussians that emit keys
+  uint32_t depth_max;
+  uint32_t num_rendered;   // sum of tiles touched (the reference's R)
+  uint32_t scan_tiles_done;
+  uint32_t scan_tile_counter;
+  uint32_t pad[10];
+};
+
+constexpr int kPreThreads = 256;  // Gaussians per preprocess block (one scan tile)
+
+struct GeomLayout {
+  size_t header, scan_status, depth, clamped, means2D, cov3D, conic, rgb, tiles, offsets, rect, prev_reach,
+      record, bwd_record, total;
+  // header and scan_status are adjacent so one memset clears both
+  __host__ __device__ explicit GeomLayout(long long P) {
+    size_t o = 0;
+    auto take = [&](size_t bytes) { size_t a = align256(o); o = a + bytes; return a; };
+    const size_t p = size_t(P);
+    header = take(sizeof(GeomHeader));
+    scan_status = take(((p + kPreThreads - 1) / kPreThreads + 1) * 8);
+    depth = take(p * 4);
+    clamped = take(p * 3);
+    means2D = take(p * 8);
+    cov3D = take(p * 24);
+    conic = take(p * 16);
+    rgb = take(p * 12);
+    tiles = take(p * 4);
+    offsets = take(p * 4);
+    rect = take(p * 8);
+    prev_reach = take(p * 4);
+    record = take(p * sizeof(BlendRecord));
+    bwd_record = take(p * sizeof(BackwardRecord));
+    total = align256(o);
+  }
+};
+
+struct ImageLayout {
+  size_t n_contrib, ranges, T_final, tile_max, total;
+  __host__ __device__ ImageLayout(int W, int H) {
+    size_t o = 0;
+    auto take = [&](size_t bytes) { size_t a = align256(o); o = a + bytes; return a; };
+    const size_t hw = size_t(W) * size_t(H);
+    const size_t tiles = size_t((W + kTile - 1) / kTile) * size_t((H + kTile - 1) / kTile);
+    n_contrib = take(hw * 4);
+    ranges = take(tiles * 8);
+    T_final = take(hw * 4);
+    tile_max = take(tiles * 4);
+    total = align256(o);
+  }
+};
+
+// Sort configuration chosen on the host from (R, depth-bit range, tile count).
+struct BinHeader {
+  uint32_t error;
+  uint32_t key64;          // 1: 64-bit packed keys, 0: 32-bit packed keys
+  uint32_t depth_bits;     // low depth bits kept in the key
+  uint32_t depth_prefix;   // common high depth bits (restored when keys are expanded)
+  uint32_t tile_bits;
+  uint32_t passes;         // 8-bit digit passes
+  uint32_t num_rendered;
+  uint32_t pad[9];
+  uint32_t tile_counter[8];  // per-pass tile acquisition counters (onesweep)
+};
+
+constexpr int kSortThreads = 256;
+constexpr int kSortItems = 16;
+constexpr int kSortTile = kSortThreads * kSortItems;  // 4096 keys per onesweep tile
+constexpr int kMaxPasses = 8;
+
+struct BinLayout {
+  size_t header, keysA, keysB, valsA, valsB, hist, status, tile_hist, total;
+  __host__ __device__ BinLayout(long long R, int num_tiles) {
+    size_t o = 0;
+    auto take = [&](size_t bytes) { size_t a = align256(o); o = a + bytes; return a; };
+    const size_t r = size_t(R > 0 ? R : 1);
+    const size_t sort_tiles = (r + kSortTile - 1) / kSortTile;
+    header = take(sizeof(BinHeader));
+    keysA = take(r * 8);
+    keysB = take(r * 8);
+    valsA = take(r * 4);
+    valsB = take(r * 4);
+    hist = take(size_t(kMaxPasses) * 256 * 4);
+    status = take(size_t(kMaxPasses) * sort_tiles * 256 * 4);
+    tile_hist = take(size_t(num_tiles > 0 ? num_tiles : 1) * 4);
+    total = align256(o);
+  }
+};
+
+// ---------------------------------------------------------------------------
+// Bounded waits and release/acquire helpers
+// ---------------------------------------------------------------------------
+constexpr uint32_t kSpinLimit = 1u << 22;   // per wait; a few ms at most
+
+__device__ __forceinline__ uint32_t ld_acquire(const uint32_t* p) {
+  uint32_t v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ void st_release(uint32_t* p, uint32_t v) {
+  asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+__device__ __forceinline__ unsigned long long ld_acquire64(const unsigned long long* p) {
+  unsigned long long v;
+  asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ void st_release64(unsigned long long* p, unsigned long long v) {
+  asm volatile("st.release.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+
+__device__ __forceinline__ uint32_t lanemask_lt() {
+  uint32_t m;
+  asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+  return m;
+}
+
+}  // namespace w2w

@@ -1,0 +1,151 @@
+// Internal launch interfaces of the rasterizer kernels (not part of the C ABI).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "common.cuh"
+
+namespace w2w {
+
+struct PreprocessArgs {
+  int P, W, H, degree, M, compat_spill;
+  float focal_x;
+  const float* view;
+  const float* proj;
+  const float* campos;
+  const float* means3D;
+  const float* scales;
+  const float* rotations;
+  const float* opacities;
+  const float* shs;
+  int* radii;
+  GeomHeader* header;
+  unsigned long long* scan_status;
+  float* depth;
+  uint8_t* clamped;
+  float* means2D;
+  float* cov3D;
+  float* conic;
+  float* rgb;
+  uint32_t* tiles;
+  uint32_t* offsets;
+  uint32_t* rect;
+  uint32_t* prev_reach;
+  float* record;      // BlendRecord[P]
+  float* bwd_record;  // BackwardRecord[P]
+};
+void launch_preprocess(const PreprocessArgs& a, cudaStream_t stream);
+
+struct DuplicateArgs {
+  int P, gw;
+  uint32_t R;
+  int key64;
+  uint32_t depth_bits;
+  const uint32_t* tiles;
+  const uint32_t* offsets;
+  const uint32_t* rect;
+  const uint32_t* prev_reach;
+  const float* depth;
+  void* keys;
+  uint32_t* vals;
+};
+void launch_duplicate(const DuplicateArgs& a, cudaStream_t stream);
+
+// LSD radix sort of packed keys (uint32 or uint64) with uint32 values over
+// key bits [begin_bit, begin_bit + bits); 8-bit digits, one onesweep launch per
+// digit.  Pass p writes keys_out when (passes - 1 - p) is even, else keys_tmp,
+// so the result lands in keys_out; keys_in must not be keys_out.
+// `tile_hist` (may be null) receives a histogram of key >> tile_shift over
+// num_tiles bins, and `ranges` (may be null) the per-bin [start, end).
+struct SortArgs {
+  long long n;
+  int key64;
+  int begin_bit;   // lowest key bit sorted on
+  int bits;        // number of key bits sorted on, from begin_bit
+  const void* keys_in;     // first pass reads here (may equal keys_tmp, never keys_out unless passes == 0)
+  const uint32_t* vals_in;
+  void* keys_out;          // the sorted result always lands here
+  uint32_t* vals_out;
+  void* keys_tmp;          // ping-pong partner
+  uint32_t* vals_tmp;
+  uint32_t* hist;        // [kMaxPasses * 256]
+  uint32_t* status;      // [kMaxPasses * sort_tiles * 256]
+  uint32_t* counters;    // [kMaxPasses]
+  uint32_t* error;
+  int tile_shift;
+  int num_tiles;
+  uint32_t* tile_hist;
+  uint2* ranges;
+};
+int sort_passes(int bits);
+void launch_sort(const SortArgs& a, cudaStream_t stream);
+size_t sort_status_words(long long n);
+
+struct BlendArgs {
+  int W, H;
+  const uint2* ranges;
+  const uint32_t* point_list;
+  const float* record;
+  const float* bg;
+  float* out_color;
+  float* out_depth;
+  float* out_alpha;
+  uint32_t* n_contrib;
+  float* T_final;
+  uint32_t* tile_max;
+};
+void launch_blend(const BlendArgs& a, cudaStream_t stream);
+
+// Backward.  grad_mode 0 = the reference's formulas, 1 = exact derivative.
+struct BackwardArgs {
+  int P, W, H, degree, M, grad_mode;
+  float focal_x;           // exact mode (the forward's Jacobian focal)
+  float h_x, h_y;          // reference mode: W/(2 tan_fovx), H/(2 tan_fovy)
+  float tan_fovx, tan_fovy;
+  float scale_modifier;
+  const float* view;
+  const float* proj;
+  const float* campos;
+  const float* bg;
+  const float* means3D;
+  const float* scales;
+  const float* rotations;
+  const float* shs;
+  const int* radii;
+  const float* cov3D;
+  const uint8_t* clamped;
+  const float* record;
+  const float* bwd_record;
+  const uint2* ranges;
+  const uint32_t* point_list;
+  const uint32_t* n_contrib;
+  const uint32_t* tile_max;
+  const float* T_final;
+  const float* out_alpha;
+  const float* dL_dcolor;
+  const float* dL_ddepth;
+  const float* dL_dalpha;
+  // accumulated by the per-pixel pass (zeroed by the caller)
+  float* dL_dmean2D;   // [P,3]
+  float* acc_cov;      // [P,4]: reference mode dL/dconic (x,y,_,w); exact mode dL/dcov2D (xx,xy,yy,_)
+  float* dL_dopacity;  // [P]
+  float* dL_dcolors;   // [P,3]
+  float* acc_depth;    // [P]
+  // written by the per-Gaussian pass
+  float* dL_dmeans3D;
+  float* dL_dcov3D;
+  float* dL_dsh;
+  float* dL_dscales;
+  float* dL_drotations;
+};
+void launch_backward_render(const BackwardArgs& a, cudaStream_t stream);
+void launch_backward_gaussians(const BackwardArgs& a, cudaStream_t stream);
+
+}  // namespace w2w
+
+namespace w2w {
+size_t scan_status_words(long long n);
+void launch_scan(const uint32_t* in, uint32_t* out, long long n, int exclusive, unsigned long long* status,
+                 uint32_t* counter, uint32_t* err, cudaStream_t stream);
+}  // namespace w2w

@@ -1,0 +1,113 @@
+// Stand-alone single-pass scan of uint32 values with decoupled lookback
+// (replaces the recursive Kogge-Stone scan of gaussianRasterizer.cu:77-117,
+// which allocates, frees and synchronises the device at every level).  The
+// rasterizer itself fuses its scan into the preprocess kernel; this entry
+// point serves the isolated-stage workload and callers that scan alone.
+#include "common.cuh"
+#include "kernels.h"
+
+namespace w2w {
+namespace {
+
+constexpr int kScanThreads = 256;
+constexpr int kScanItems = 16;
+constexpr int kScanTile = kScanThreads * kScanItems;
+constexpr unsigned long long kAgg = 1ull << 62, kInc = 2ull << 62, kFlags = 3ull << 62;
+
+// 64-bit status words: flag in the top two bits, a uint32 partial sum (which
+// wraps modulo 2^32, as the reference's uint32 scan does) in the low bits.
+__global__ void __launch_bounds__(kScanThreads)
+scan_kernel(const uint32_t* __restrict__ in, uint32_t* __restrict__ out, long long n, int exclusive,
+            unsigned long long* status, uint32_t* counter, uint32_t* err) {
+  __shared__ uint32_t s_tile, s_prefix;
+  __shared__ uint32_t s_warp[kScanThreads / 32];
+  __shared__ uint32_t s_data[kScanTile];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  if (tid == 0) s_tile = atomicAdd(counter, 1u);
+  __syncthreads();
+  const long long tile = s_tile;
+  const long long base = tile * kScanTile;
+  // coalesced load into shared memory, then each thread scans a contiguous run
+  for (int i = tid; i < kScanTile; i += kScanThreads) {
+    const long long idx = base + i;
+    s_data[i] = idx < n ? in[idx] : 0u;
+  }
+  __syncthreads();
+  uint32_t v[kScanItems];
+  uint32_t run = 0;
+#pragma unroll
+  for (int k = 0; k < kScanItems; ++k) {
+    v[k] = s_data[tid * kScanItems + k];
+    run += v[k];
+  }
+  uint32_t x = run;
+#pragma unroll
+  for (int d = 1; d < 32; d <<= 1) {
+    const uint32_t o = __shfl_up_sync(0xffffffffu, x, d);
+    if (lane >= d) x += o;
+  }
+  if (lane == 31) s_warp[warp] = x;
+  __syncthreads();
+  if (warp == 0) {
+    uint32_t w = lane < kScanThreads / 32 ? s_warp[lane] : 0u;
+#pragma unroll
+    for (int d = 1; d < kScanThreads / 32; d <<= 1) {
+      const uint32_t o = __shfl_up_sync(0xffffffffu, w, d);
+      if (lane >= d) w += o;
+    }
+    if (lane < kScanThreads / 32) s_warp[lane] = w;
+  }
+  __syncthreads();
+  const uint32_t total = s_warp[kScanThreads / 32 - 1];
+  if (tid == 0) {
+    if (tile == 0) {
+      st_release64(status, kInc | total);
+      s_prefix = 0;
+    } else {
+      st_release64(status + tile, kAgg | total);
+      uint32_t acc = 0, spins = 0;
+      long long t = tile - 1;
+      while (t >= 0) {
+        const unsigned long long w = ld_acquire64(status + t);
+        const unsigned long long flag = w & kFlags;
+        if (flag == 0ull) {
+          if (++spins > kSpinLimit) { atomicOr(err, kErrTimeout); break; }
+          continue;
+        }
+        acc += uint32_t(w);
+        if (flag == kInc) break;
+        --t;
+      }
+      s_prefix = acc;
+      st_release64(status + tile, kInc | uint32_t(acc + total));
+    }
+  }
+  __syncthreads();
+  uint32_t pre = s_prefix + (warp > 0 ? s_warp[warp - 1] : 0u) + (x - run);
+#pragma unroll
+  for (int k = 0; k < kScanItems; ++k) {
+    const uint32_t incl = pre + v[k];
+    s_data[tid * kScanItems + k] = exclusive ? pre : incl;
+    pre = incl;
+  }
+  __syncthreads();
+  for (int i = tid; i < kScanTile; i += kScanThreads) {
+    const long long idx = base + i;
+    if (idx < n) out[idx] = s_data[i];
+  }
+}
+
+}  // namespace
+
+size_t scan_status_words(long long n) { return size_t((n + kScanTile - 1) / kScanTile) + 1; }
+
+void launch_scan(const uint32_t* in, uint32_t* out, long long n, int exclusive, unsigned long long* status,
+                 uint32_t* counter, uint32_t* err, cudaStream_t stream) {
+  if (n <= 0) return;
+  const long long tiles = (n + kScanTile - 1) / kScanTile;
+  cudaMemsetAsync(status, 0, sizeof(unsigned long long) * size_t(tiles), stream);
+  cudaMemsetAsync(counter, 0, sizeof(uint32_t), stream);
+  scan_kernel<<<int(tiles), kScanThreads, 0, stream>>>(in, out, n, exclusive, status, counter, err);
+}
+
+}  // namespace w2w

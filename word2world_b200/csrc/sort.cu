@@ -1,0 +1,291 @@
+// Stable LSD radix sort of (key, uint32 value) pairs, onesweep style
+// (replaces the reference's 32-pass 2-bit sort with a host round trip per pass,
+// prepareSort.cu:303-360, and the range kernel gaussianTiles.cu:6-33).
+//
+//   1. histogram kernel: one read of the keys gives the 256-bin digit
+//      histogram of every pass, plus the histogram of key >> tile_shift
+//      (the per-tile instance counts);
+//   2. offsets kernel: exclusive scans of those histograms; the tile scan is
+//      the per-tile [start, end) range table (empty tiles get (0, 0), as the
+//      reference's memset leaves them);
+//   3. one onesweep kernel per 8-bit digit: each CTA takes the next 4096-key
+//      tile (acquired through an atomic counter, so every earlier tile is
+//      already running), ranks its keys stably with warp-level match, publishes
+//      its per-digit counts and looks back over earlier tiles for their
+//      prefix (decoupled lookback), then scatters through shared memory so the
+//      global stores are coalesced.  Every wait is bounded: a wait that runs
+//      out sets kErrTimeout and the kernel finishes without hanging.
+//
+// Stability: keys are ranked in input order within a warp, warps in order
+// within a tile, tiles in order globally -- the same order the reference's
+// stable 2-bit passes produce, so equal keys keep their input order.
+#include "common.cuh"
+#include "kernels.h"
+
+namespace w2w {
+namespace {
+
+constexpr uint32_t kStatAgg = 1u << 30;
+constexpr uint32_t kStatInc = 2u << 30;
+constexpr uint32_t kStatMask = (1u << 30) - 1u;
+constexpr int kHistThreads = 256;
+constexpr int kSmemTileBins = 8192;
+
+template <typename K>
+__global__ void __launch_bounds__(kHistThreads)
+hist_kernel(const K* __restrict__ keys, long long n, int begin_bit, int passes, uint32_t* __restrict__ hist,
+            int tile_shift, int num_tiles, uint32_t* __restrict__ tile_hist) {
+  extern __shared__ uint32_t smem[];
+  uint32_t* sh = smem;                      // passes * 256
+  uint32_t* st = smem + passes * 256;       // num_tiles when they fit
+  const bool tiles_in_smem = tile_hist != nullptr && num_tiles <= kSmemTileBins;
+  for (int i = threadIdx.x; i < passes * 256; i += blockDim.x) sh[i] = 0;
+  if (tiles_in_smem)
+    for (int i = threadIdx.x; i < num_tiles; i += blockDim.x) st[i] = 0;
+  __syncthreads();
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+    const K k = keys[i];
+    for (int p = 0; p < passes; ++p) atomicAdd(&sh[p * 256 + int((k >> (begin_bit + 8 * p)) & 255)], 1u);
+    if (tile_hist != nullptr) {
+      const uint32_t t = uint32_t(k >> tile_shift);
+      if (t < uint32_t(num_tiles)) {
+        if (tiles_in_smem) atomicAdd(&st[t], 1u);
+        else atomicAdd(&tile_hist[t], 1u);
+      }
+    }
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < passes * 256; i += blockDim.x)
+    if (sh[i]) atomicAdd(&hist[i], sh[i]);
+  if (tiles_in_smem)
+    for (int i = threadIdx.x; i < num_tiles; i += blockDim.x)
+      if (st[i]) atomicAdd(&tile_hist[i], st[i]);
+}
+
+// Block-wide exclusive scan of one value per thread (blockDim.x <= 1024).
+__device__ uint32_t block_exclusive_scan(uint32_t v, uint32_t* s_warp, uint32_t* total) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+  uint32_t x = v;
+#pragma unroll
+  for (int d = 1; d < 32; d <<= 1) {
+    const uint32_t o = __shfl_up_sync(0xffffffffu, x, d);
+    if (lane >= d) x += o;
+  }
+  if (lane == 31) s_warp[warp] = x;
+  __syncthreads();
+  if (warp == 0) {
+    uint32_t w = lane < nw ? s_warp[lane] : 0u;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+      const uint32_t o = __shfl_up_sync(0xffffffffu, w, d);
+      if (lane >= d) w += o;
+    }
+    if (lane < nw) s_warp[lane] = w;
+  }
+  __syncthreads();
+  const uint32_t before = warp > 0 ? s_warp[warp - 1] : 0u;
+  if (total) *total = s_warp[nw - 1];
+  const uint32_t r = before + x - v;
+  __syncthreads();
+  return r;
+}
+
+// Digit histograms -> exclusive digit offsets (in place); tile histogram ->
+// [start, end) ranges.  One block of 1024 threads.
+__global__ void __launch_bounds__(1024)
+offsets_kernel(uint32_t* hist, int passes, const uint32_t* tile_hist, int num_tiles, uint2* ranges) {
+  __shared__ uint32_t s_warp[32];
+  __shared__ uint32_t s_carry;
+  for (int p = 0; p < passes; ++p) {
+    const uint32_t v = threadIdx.x < 256 ? hist[p * 256 + threadIdx.x] : 0u;
+    const uint32_t ex = block_exclusive_scan(v, s_warp, nullptr);
+    if (threadIdx.x < 256) hist[p * 256 + threadIdx.x] = ex;
+    __syncthreads();
+  }
+  if (tile_hist == nullptr || ranges == nullptr) return;
+  if (threadIdx.x == 0) s_carry = 0;
+  __syncthreads();
+  for (int base = 0; base < num_tiles; base += blockDim.x) {
+    const int t = base + threadIdx.x;
+    const uint32_t c = t < num_tiles ? tile_hist[t] : 0u;
+    uint32_t tot;
+    const uint32_t ex = block_exclusive_scan(c, s_warp, &tot);
+    const uint32_t start = s_carry + ex;
+    if (t < num_tiles) ranges[t] = c ? make_uint2(start, start + c) : make_uint2(0u, 0u);
+    __syncthreads();
+    if (threadIdx.x == 0) s_carry += tot;
+    __syncthreads();
+  }
+}
+
+template <typename K>
+__global__ void __launch_bounds__(kSortThreads)
+onesweep_kernel(const K* __restrict__ kin, const uint32_t* __restrict__ vin, K* __restrict__ kout,
+                uint32_t* __restrict__ vout, long long n, int shift, const uint32_t* __restrict__ digit_base,
+                uint32_t* status, uint32_t* counter, uint32_t* err) {
+  constexpr int kWarps = kSortThreads / 32;
+  __shared__ uint32_t s_wcnt[kWarps][256];
+  __shared__ uint32_t s_excl[256];
+  __shared__ uint32_t s_gofs[256];
+  __shared__ uint32_t s_warp[32];
+  __shared__ uint32_t s_tile;
+  extern __shared__ __align__(16) unsigned char s_dyn[];
+  K* s_keys = reinterpret_cast<K*>(s_dyn);
+  uint32_t* s_vals = reinterpret_cast<uint32_t*>(s_dyn + sizeof(K) * kSortTile);
+
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  if (tid == 0) s_tile = atomicAdd(counter, 1u);
+  for (int i = tid; i < kWarps * 256; i += kSortThreads) (&s_wcnt[0][0])[i] = 0u;
+  __syncthreads();
+  const long long tile = s_tile;
+  const long long base = tile * kSortTile;
+
+  K k[kSortItems];
+  uint32_t v[kSortItems];
+  uint32_t rank[kSortItems];
+  const uint32_t lt = lanemask_lt();
+#pragma unroll
+  for (int i = 0; i < kSortItems; ++i) {
+    const long long idx = base + warp * (32 * kSortItems) + i * 32 + lane;
+    const bool valid = idx < n;
+    k[i] = valid ? kin[idx] : K(0);
+    v[i] = valid ? vin[idx] : 0u;
+  }
+#pragma unroll
+  for (int i = 0; i < kSortItems; ++i) {
+    const long long idx = base + warp * (32 * kSortItems) + i * 32 + lane;
+    const bool valid = idx < n;
+    const uint32_t d = uint32_t(k[i] >> shift) & 255u;
+    const uint32_t peers = __match_any_sync(0xffffffffu, valid ? d : (0x10000u | uint32_t(lane)));
+    const uint32_t before = valid ? s_wcnt[warp][d] : 0u;
+    rank[i] = before + __popc(peers & lt);
+    __syncwarp();
+    if (valid && lane == __ffs(peers) - 1) s_wcnt[warp][d] = before + __popc(peers);
+    __syncwarp();
+  }
+  __syncthreads();
+
+  // per digit (one thread each): exclusive over warps, tile count, publish
+  uint32_t tile_cnt = 0;
+  {
+    const int d = tid;  // kSortThreads == 256 digits
+    uint32_t sum = 0;
+#pragma unroll
+    for (int w = 0; w < kWarps; ++w) {
+      const uint32_t c = s_wcnt[w][d];
+      s_wcnt[w][d] = sum;
+      sum += c;
+    }
+    tile_cnt = sum;
+    uint32_t* my = status + tile * 256 + d;
+    if (tile == 0) st_release(my, kStatInc | tile_cnt);
+    else st_release(my, kStatAgg | tile_cnt);
+  }
+  const uint32_t excl = block_exclusive_scan(tile_cnt, s_warp, nullptr);
+  {
+    const int d = tid;
+    s_excl[d] = excl;
+    uint32_t acc = 0;
+    if (tile > 0) {
+      long long t = tile - 1;
+      uint32_t spins = 0;
+      while (t >= 0) {
+        const uint32_t w = ld_acquire(status + t * 256 + d);
+        const uint32_t flag = w & ~kStatMask;
+        if (flag == 0u) {
+          if (++spins > kSpinLimit) { atomicOr(err, kErrTimeout); break; }
+          continue;
+        }
+        acc += w & kStatMask;
+        if (flag == kStatInc) break;
+        --t;
+      }
+      st_release(status + tile * 256 + d, kStatInc | (acc + tile_cnt));
+    }
+    s_gofs[d] = digit_base[d] + acc;
+  }
+  __syncthreads();
+#pragma unroll
+  for (int i = 0; i < kSortItems; ++i) {
+    const long long idx = base + warp * (32 * kSortItems) + i * 32 + lane;
+    if (idx < n) {
+      const uint32_t d = uint32_t(k[i] >> shift) & 255u;
+      const uint32_t pos = s_excl[d] + s_wcnt[warp][d] + rank[i];
+      s_keys[pos] = k[i];
+      s_vals[pos] = v[i];
+    }
+  }
+  __syncthreads();
+  const int nvalid = int(min((long long)kSortTile, n - base));
+  for (int j = tid; j < nvalid; j += kSortThreads) {
+    const K key = s_keys[j];
+    const uint32_t d = uint32_t(key >> shift) & 255u;
+    const long long out = (long long)s_gofs[d] + (j - (long long)s_excl[d]);
+    if (out >= 0 && out < n) {
+      kout[out] = key;
+      vout[out] = s_vals[j];
+    } else {
+      atomicOr(err, kErrRange);
+    }
+  }
+}
+
+template <typename K>
+void run_sort(const SortArgs& a, cudaStream_t stream) {
+  const int passes = sort_passes(a.bits);
+  const long long n = a.n;
+  if (n <= 0) return;
+  const long long tiles = (n + kSortTile - 1) / kSortTile;
+  cudaMemsetAsync(a.hist, 0, sizeof(uint32_t) * 256 * kMaxPasses, stream);
+  cudaMemsetAsync(a.counters, 0, sizeof(uint32_t) * kMaxPasses, stream);
+  cudaMemsetAsync(a.status, 0, sizeof(uint32_t) * 256 * size_t(tiles) * size_t(passes > 0 ? passes : 1), stream);
+  if (a.tile_hist) cudaMemsetAsync(a.tile_hist, 0, sizeof(uint32_t) * size_t(a.num_tiles), stream);
+  if (passes > 0 || a.tile_hist) {
+    int sms = 148;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, 0);
+    long long want = (n + kHistThreads * 16 - 1) / (kHistThreads * 16);
+    const int grid = int(max(1LL, min(want, (long long)sms * 8)));
+    const bool tiles_in_smem = a.tile_hist != nullptr && a.num_tiles <= kSmemTileBins;
+    const size_t smem = sizeof(uint32_t) * (size_t(passes) * 256 + (tiles_in_smem ? size_t(a.num_tiles) : 0));
+    if (smem > 48 * 1024)
+      cudaFuncSetAttribute(hist_kernel<K>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+    hist_kernel<K><<<grid, kHistThreads, smem, stream>>>(reinterpret_cast<const K*>(a.keys_in), n, a.begin_bit,
+                                                         passes, a.hist, a.tile_shift, a.num_tiles, a.tile_hist);
+    offsets_kernel<<<1, 1024, 0, stream>>>(a.hist, passes, a.tile_hist, a.num_tiles, a.ranges);
+  }
+  const size_t dyn = (sizeof(K) + sizeof(uint32_t)) * kSortTile;
+  cudaFuncSetAttribute(onesweep_kernel<K>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(dyn));
+  const K* kin = reinterpret_cast<const K*>(a.keys_in);
+  const uint32_t* vin = a.vals_in;
+  for (int p = 0; p < passes; ++p) {
+    const bool to_out = ((passes - 1 - p) % 2) == 0;
+    K* kout = reinterpret_cast<K*>(to_out ? a.keys_out : a.keys_tmp);
+    uint32_t* vout = to_out ? a.vals_out : a.vals_tmp;
+    onesweep_kernel<K><<<int(tiles), kSortThreads, dyn, stream>>>(
+        kin, vin, kout, vout, n, a.begin_bit + 8 * p, a.hist + 256 * p, a.status + size_t(p) * 256 * size_t(tiles),
+        a.counters + p, a.error);
+    kin = kout;
+    vin = vout;
+  }
+  if (passes == 0 && a.keys_in != a.keys_out) {
+    cudaMemcpyAsync(a.keys_out, a.keys_in, sizeof(K) * size_t(n), cudaMemcpyDeviceToDevice, stream);
+    cudaMemcpyAsync(a.vals_out, a.vals_in, sizeof(uint32_t) * size_t(n), cudaMemcpyDeviceToDevice, stream);
+  }
+}
+
+}  // namespace
+
+int sort_passes(int bits) { return bits <= 0 ? 0 : (bits + 7) / 8; }
+
+size_t sort_status_words(long long n) {
+  const long long tiles = (n + kSortTile - 1) / kSortTile;
+  return size_t(kMaxPasses) * 256 * size_t(tiles > 0 ? tiles : 1);
+}
+
+void launch_sort(const SortArgs& a, cudaStream_t stream) {
+  if (a.key64) run_sort<uint64_t>(a, stream);
+  else run_sort<uint32_t>(a, stream);
+}
+
+}  // namespace w2w

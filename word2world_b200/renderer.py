@@ -1,0 +1,149 @@
+"""Autograd wrapper and renderer shim with the reference's Python interface.
+
+``_render_gaussians_inline`` restates ``Renderer.py:28-110``: same argument
+list, same return tuple ``(color, radii, depth, alpha)``, same gradient
+routing (``dL/dmeans2D`` to the ``means2D`` placeholder, the densification
+signal).  Differences, all opt-in through trailing keywords:
+
+* ``image_height`` / ``image_width`` (the reference renders a fixed 800x800
+  and derives its focal length from 800, ``Renderer.py:39-40``); the defaults
+  keep 800;
+* ``grad_mode="reference"`` (the reference backward's formulas) or
+  ``"exact"`` (the derivative of the forward);
+* ``compat_spill`` (the reference's key-emission rectangle; default on).
+
+``Renderer`` restates ``Renderer.render`` (``Renderer.py:119-192``) over a
+structure-of-arrays parameter store instead of one Python object per Gaussian.
+"""
+from __future__ import annotations
+
+import math
+from dataclasses import dataclass
+
+import torch
+
+from . import _C
+
+GRAD_MODES = {"reference": 0, "exact": 1}
+
+
+def fill_missing_attributes(means3D, shs, colors_precomp, scales, rotations, cov3D_precomp):
+    """Empty tensors for absent optional inputs (``Renderer.py:8-23``)."""
+    empty = lambda: torch.empty(0, device=means3D.device, dtype=torch.float32)
+    return (shs if shs is not None else empty(), colors_precomp if colors_precomp is not None else empty(),
+            scales if scales is not None else empty(), rotations if rotations is not None else empty(),
+            cov3D_precomp if cov3D_precomp is not None else empty())
+
+
+class _RasterizeGaussians(torch.autograd.Function):
+    @staticmethod
+    def forward(ctx, means3D, means2D, sh, colors_precomp, opacities, scales, rotations, cov3Ds_precomp, bg,
+                scale_modifier, viewmatrix, projmatrix, tanfovx, tanfovy, sh_degree, campos, prefiltered, debug,
+                image_height, image_width, grad_mode, compat_spill):
+        focal_x = image_width / (2.0 * tanfovx)
+        focal_y = image_height / (2.0 * tanfovy)
+        num_rend, color, depth, alpha, radii, geom, binb, img = _C.rasterize_gaussians(
+            sh, focal_y, scales, means3D, projmatrix, sh_degree, opacities, rotations, campos, viewmatrix, focal_x,
+            image_height, image_width, bg, compat_spill)
+        ctx.num_rend = num_rend
+        ctx.bg = bg
+        ctx.scale_mod = scale_modifier
+        ctx.vmat = viewmatrix
+        ctx.pmat = projmatrix
+        ctx.fx = tanfovx
+        ctx.fy = tanfovy
+        ctx.sh_deg = sh_degree
+        ctx.campos = campos
+        ctx.debug = debug
+        ctx.grad_mode = grad_mode
+        ctx.save_for_backward(colors_precomp, means3D, scales, rotations, cov3Ds_precomp, radii, sh, geom, binb, img,
+                              alpha)
+        ctx.mark_non_differentiable(radii)
+        return color, radii, depth, alpha
+
+    @staticmethod
+    def backward(ctx, g_color, g_radii, g_depth, g_alpha):
+        (colors_precomp, means3D, scales, rotations, cov3Ds_precomp, radii, sh, geom, binb, img,
+         alpha) = ctx.saved_tensors
+        g_means2D, g_colors, g_opac, g_means3D, g_cov3D, g_sh, g_scales, g_rots = _C.rasterize_gaussians_backward(
+            ctx.bg, means3D, radii, colors_precomp, scales, rotations, ctx.scale_mod, cov3Ds_precomp, ctx.vmat,
+            ctx.pmat, ctx.fx, ctx.fy, g_color.contiguous(), g_depth.contiguous(), g_alpha.contiguous(), sh,
+            ctx.sh_deg, ctx.campos, geom, ctx.num_rend, binb, img, alpha, ctx.debug, ctx.grad_mode)
+        return (g_means3D, g_means2D, g_sh, None if colors_precomp.numel() == 0 else g_colors, g_opac, g_scales,
+                g_rots, None if cov3Ds_precomp.numel() == 0 else g_cov3D,
+                None, None, None, None, None, None, None, None, None, None, None, None, None, None)
+
+
+def _render_gaussians_inline(means3D, means2D, shs, colors_precomp, opacity, scales, rotations, cov3D_precomp, bg,
+                             scale_modifier, viewmatrix, projmatrix, tanfovx, tanfovy, sh_degree, campos,
+                             prefiltered=False, debug=False, image_height=800, image_width=800,
+                             grad_mode="reference", compat_spill=True):
+    """``Renderer.py:28-110``: rasterize and return ``(color, radii, depth, alpha)``."""
+    scale_modifier = 1  # the reference overrides it (Renderer.py:37)
+    shs, colors_precomp, scales, rotations, cov3D_precomp = fill_missing_attributes(
+        means3D, shs, colors_precomp, scales, rotations, cov3D_precomp)
+    if grad_mode not in GRAD_MODES:
+        raise ValueError(f"grad_mode must be one of {sorted(GRAD_MODES)}")
+    return _RasterizeGaussians.apply(means3D, means2D, shs, colors_precomp, opacity, scales, rotations,
+                                     cov3D_precomp, bg, scale_modifier, viewmatrix, projmatrix, tanfovx, tanfovy,
+                                     sh_degree, campos, prefiltered, debug, int(image_height), int(image_width),
+                                     GRAD_MODES[grad_mode], bool(compat_spill))
+
+
+@dataclass
+class GaussianParams:
+    """Raw per-Gaussian parameters as structure-of-arrays tensors (the
+    reference keeps one ``GaussianPrimitive`` object per Gaussian,
+    ``primitives.py:54-86``)."""
+    mean: torch.Tensor        # [P,3]
+    sh_dc: torch.Tensor       # [P,1,3]
+    sh_ac: torch.Tensor       # [P,15,3]
+    opacity: torch.Tensor     # [P,1] logits
+    svec: torch.Tensor        # [P,3] log-scales
+    quaternion: torch.Tensor  # [P,4] (w, x, y, z)
+
+    @staticmethod
+    def from_scene(scene, device="cuda", requires_grad=True):
+        t = lambda a: torch.tensor(a, device=device, dtype=torch.float32).requires_grad_(requires_grad)
+        return GaussianParams(t(scene.mean), t(scene.sh_dc), t(scene.sh_ac), t(scene.opacity), t(scene.svec),
+                              t(scene.quaternion))
+
+    def parameters(self):
+        return [self.mean, self.sh_dc, self.sh_ac, self.opacity, self.svec, self.quaternion]
+
+
+class Renderer:
+    """``Renderer.render`` (``Renderer.py:119-192``) over ``GaussianParams``.
+
+    ``sh_degree`` defaults to 0 as in the reference call (``Renderer.py:170``).
+    Unlike the reference, ``image_width`` / ``image_height`` are honoured.
+    """
+
+    def __init__(self, params: GaussianParams, sh_degree: int = 0, grad_mode: str = "reference",
+                 compat_spill: bool = True):
+        self.params = params
+        self.sh_degree = sh_degree
+        self.grad_mode = grad_mode
+        self.compat_spill = compat_spill
+
+    def render(self, FoVx, FoVy, world_view_transform, full_proj_transform, camera_center, image_width,
+               image_height):
+        p = self.params
+        accum_grads = torch.zeros_like(p.mean, requires_grad=True)
+        accum_grads.retain_grad()
+        tanfovx = math.tan(float(FoVx) * 0.5)
+        tanfovy = math.tan(float(FoVy) * 0.5)
+        # activation preamble (Renderer.py:164-167)
+        activated_opacity = torch.sigmoid(p.opacity)
+        activated_scales = torch.exp(p.svec)
+        rotations = torch.nn.functional.normalize(p.quaternion)
+        shs = torch.cat((p.sh_dc, p.sh_ac), dim=1)
+        bg = torch.ones(3, dtype=torch.float32, device=p.mean.device)
+        image, radii, _, _ = _render_gaussians_inline(
+            p.mean, accum_grads, shs, None, activated_opacity, activated_scales, rotations, None, bg, 1,
+            world_view_transform, full_proj_transform, tanfovx, tanfovy, self.sh_degree, camera_center, False,
+            False, image_height=int(image_height), image_width=int(image_width), grad_mode=self.grad_mode,
+            compat_spill=self.compat_spill)
+        available = radii > 0
+        # the reference's result keys, including its spelling of "avaialble_pts"
+        return {"image": image, "accum_grads": accum_grads, "avaialble_pts": available, "available_pts": available}

@@ -91,3 +91,24 @@ def scene_16k(seed: int = 0) -> Scene:
 def scene_500k(seed: int = 0) -> Scene:
     """500,000 Gaussians in a 0.6 ball (rendered at 512x512, 4 views)."""
     return make_scene(500000, seed=seed, layout="ball")
+
+
+# Isolated sort / scan stage workload ------------------------------------------
+
+def sort_workload(n: int, seed: int = 0, num_tiles: int = 4096, zipf_a: float = 1.2):
+    """(keys u64[n], values u32[n]): key = tile << 32 | float32 depth bits with
+    tile ids in [0, num_tiles) drawn from a Zipf(zipf_a) skew (p ~ 1/(k+1)^a),
+    depths U[0.5, 4.5]; value = position (the 1024x1024, 16x16-tile case)."""
+    rng = np.random.default_rng(seed)
+    p = 1.0 / np.power(np.arange(1, num_tiles + 1, dtype=np.float64), zipf_a)
+    p /= p.sum()
+    tiles = rng.choice(num_tiles, size=n, p=p).astype(np.uint64)
+    depth = rng.uniform(0.5, 4.5, size=n).astype(np.float32)
+    keys = (tiles << np.uint64(32)) | depth.view(np.uint32).astype(np.uint64)
+    return keys, np.arange(n, dtype=np.uint32)
+
+
+def scan_workload(n: int, seed: int = 0, lam: float = 8.0):
+    """Per-Gaussian tile-touch counts ~ Poisson(lam), uint32."""
+    rng = np.random.default_rng(seed)
+    return rng.poisson(lam, size=n).astype(np.uint32)
