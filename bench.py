@@ -1,0 +1,361 @@
+"""Benchmark: forward+backward views/s of the Gaussian rasterizer.
+
+Workload (the single-scene drop-in configuration): 500,000 Gaussians
+uniformly in a radius-0.6 ball, SH degree 3, 4 orbit views at 512x512,
+fp32 forward + backward through the torch.autograd.Function
+(_render_gaussians_inline) with synthetic N(0,1) upstream image gradients.
+A step renders and back-propagates all 4 views.  N GPUs run N replicas
+(no exchange step exists on this path), each its own 4 views.
+
+Prints one JSON line (rank 0).  `--impl reference` times the reference's
+path on the host cores instead (see run_reference).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "fwd+bwd views/s at 500k Gaussians 512x512"
+UNIT = "views/s"
+PEAKS_FILE = os.path.join(ROOT, "MEASURED_PEAKS.json")
+FALLBACK_HBM_GBS = 6650.0
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="w2w", choices=["w2w", "reference"])
+    ap.add_argument("--P", type=int, default=500_000)
+    ap.add_argument("--res", type=int, default=512)
+    ap.add_argument("--views", type=int, default=4)
+    ap.add_argument("--grad-mode", default="reference", choices=["reference", "exact"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--seed", type=int, default=0)
+    return ap.parse_args()
+
+
+def workload_config(a):
+    return {"workload": f"{a.P // 1000}k Gaussians in a radius-0.6 ball, {a.views} orbit views {a.res}x{a.res}, "
+                        f"SH degree 3, fp32 forward+backward through the autograd Function",
+            "gaussians": a.P, "views_per_gpu": a.views, "resolution": a.res, "sh_degree": 3,
+            "grad_mode": a.grad_mode, "compat_spill": True,
+            "l2": "inputs larger than L2 (about 1 GB of parameters, state and images touched per step)"}
+
+
+def peaks():
+    try:
+        with open(PEAKS_FILE) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+# ---------------------------------------------------------------------------
+# clocks sampled during the timed region
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.path = os.path.join("/tmp", f"w2w_clocks_{os.getpid()}.csv")
+
+    def __enter__(self):
+        try:
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.f,
+                                         stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+            self.f.close()
+
+    def summary(self):
+        try:
+            rows = [r.split(",") for r in open(self.path).read().strip().splitlines() if r.strip()]
+        except Exception:
+            rows = []
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in rows if r[1].strip().replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].strip().replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if len(r) > 5 + i and "Active" in r[5 + i]
+                          and "Not" not in r[5 + i]})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+# ---------------------------------------------------------------------------
+# this implementation
+# ---------------------------------------------------------------------------
+def build_inputs(a, device):
+    import numpy as np
+    import torch
+    from word2world_b200 import camera, scenes
+    sc = scenes.make_scene(a.P, seed=a.seed, layout="ball")
+    m, o, s, q, sh = sc.activate()
+    cams = camera.orbit_views(a.views, 2.5, a.res, a.res)
+    t = lambda x: torch.from_numpy(np.ascontiguousarray(x)).to(device)
+    leaves = dict(means3D=t(m), opacity=t(o), scales=t(s), rotations=t(q), shs=t(sh))
+    for v in leaves.values():
+        v.requires_grad_(True)
+    grads = [t(g) for g in scenes.upstream_grads(a.views, a.res, a.res, seed=a.seed + 1)]
+    cam_t = [dict(view=t(c.viewmatrix), proj=t(c.projmatrix), campos=t(c.campos), tanx=c.tanfovx, tany=c.tanfovy)
+             for c in cams]
+    return sc, cams, leaves, grads, cam_t
+
+
+def run_ours(a):
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+    from word2world_b200 import _C, dist as wd
+    from word2world_b200.renderer import _render_gaussians_inline
+    rank, world, local = wd.env_rank_world()
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    torch.cuda.set_device(local)
+    device = torch.device("cuda", local)
+    sc, cams, L, grads, cam_t = build_inputs(a, device)
+    bg = torch.ones(3, device=device)
+    means2D = torch.zeros_like(L["means3D"], requires_grad=True)
+
+    def step():
+        for k in L:
+            L[k].grad = None
+        means2D.grad = None
+        for v in range(a.views):
+            c = cam_t[v]
+            color, radii, depth, alpha = _render_gaussians_inline(
+                L["means3D"], means2D, L["shs"], None, L["opacity"], L["scales"], L["rotations"], None, bg, 1,
+                c["view"], c["proj"], c["tanx"], c["tany"], 3, c["campos"], image_height=a.res, image_width=a.res,
+                grad_mode=a.grad_mode)
+            torch.autograd.backward([color], [grads[v]])
+
+    # per-view instance counts and sort plan (for the roofline's algorithmic bytes)
+    plans = []
+    with torch.no_grad():
+        for v in range(a.views):
+            c = cam_t[v]
+            out = _C.rasterize_gaussians(L["shs"], a.res / (2 * c["tany"]), L["scales"], L["means3D"], c["proj"], 3,
+                                         L["opacity"], L["rotations"], c["campos"], c["view"],
+                                         a.res / (2 * c["tanx"]), a.res, a.res, bg, True)
+            info = _C.binning_info(out[6], out[0], a.res, a.res)
+            plans.append(dict(R=int(out[0]), **{k: int(x) for k, x in info.items()}))
+            del out
+    for _ in range(max(a.warmup, 1)):
+        step()
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    _C.stage_times()
+    _C.stage_timing(True)
+    launches0 = _C.launch_count()
+    stream = torch.cuda.current_stream()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        e0.record(stream)
+        for _ in range(a.steps):
+            step()
+        e1.record(stream)
+        torch.cuda.synchronize()
+    launches = _C.launch_count() - launches0
+    _C.stage_timing(False)
+    stages = _C.stage_times()
+    ms = e0.elapsed_time(e1)
+    if world > 1:
+        dist.barrier()
+    ms_max = wd.max_over_ranks(ms, device=device)
+    value = world * a.views * a.steps / (ms_max / 1e3)
+
+    # roofline of the dominant HBM-bound stage (per-launch algorithmic bytes / average launch time)
+    P, M = a.P, 16
+    Rm = statistics.mean(p["R"] for p in plans)
+    kb = 8 if any(p["key64"] for p in plans) else 4
+    alg_bytes = {
+        "preprocess": P * (12 + 12 + 16 + 4 + 12 * M + 24 + 12 + 3 + 16 + 8 + 4 + 4 + 4 + 8 + 48 + 48 + 4 + 4),
+        "duplicate": Rm * (kb + 4) + P * 24,
+        "sort_histogram": Rm * kb,
+        "sort_onesweep": Rm * 2 * (kb + 4),
+        "backward_gaussians": P * (12 + 4 + 24 + 16 + 12 + 12 + 4 + 3 + 12 * M + 12 + 16 + 12 + 24 + 12 * M + 12 + 16),
+    }
+    stage_ms = {k: v[0] for k, v in stages.items()}
+    stage_n = {k: v[1] for k, v in stages.items()}
+    total_stage = sum(stage_ms.values()) or 1.0
+    hbm, peak_kind = peaks()
+    hbm_stages = {k: stage_ms[k] for k in alg_bytes if stage_n.get(k)}
+    dom = max(hbm_stages, key=hbm_stages.get) if hbm_stages else None
+    roofline = None
+    if dom:
+        per_launch_ms = stage_ms[dom] / stage_n[dom] * (2 if dom == "sort_histogram" else 1)
+        ach = alg_bytes[dom] / (per_launch_ms / 1e3) / 1e9
+        roofline = {"kernel": dom, "bound": "hbm", "achieved": round(ach, 1), "peak": hbm, "unit": "GB/s",
+                    "frac": round(ach / hbm, 4), "peak_source": peak_kind, "traffic": None,
+                    "algorithmic_bytes_per_launch": int(alg_bytes[dom]), "avg_launch_ms": round(per_launch_ms, 4)}
+    stage_report = {k: {"ms_per_step": round(stage_ms[k] / a.steps, 4), "launches_per_step": stage_n[k] / a.steps,
+                        "share": round(stage_ms[k] / total_stage, 4)} for k in stage_ms if stage_n[k]}
+
+    result = {"metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": world, "steps": a.steps,
+              "warmup": a.warmup, "ms_per_step": round(ms_max / a.steps, 4), "higher_is_better": True,
+              "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded scene, N(0,1) dL/dimage)",
+              "config": dict(workload_config(a), parallelism=f"replicas x{world}", num_rendered_per_view=int(Rm),
+                             sort_key_bytes=kb, sort_passes=plans[0].get("passes")),
+              "gpu_launches": int(launches), "clocks": clk.summary(), "roofline": roofline, "stages": stage_report}
+
+    if not a.no_e2e:
+        result["e2e"] = run_e2e(a, sc, cams, device, world)
+    if rank == 0 and world == 1 and not a.no_cpu_baseline:
+        result["cpu_baseline"] = cpu_baseline(a)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(result), flush=True)
+
+
+def run_e2e(a, sc, cams, device, world):
+    """Same metric through the public Renderer API: raw parameters resident,
+    each step copies that step's upstream image gradients (and cameras) from
+    pinned host memory and reads the per-view losses back."""
+    import numpy as np
+    import torch
+    from word2world_b200 import dist as wd, scenes
+    from word2world_b200.renderer import GaussianParams, Renderer
+    params = GaussianParams.from_scene(sc, device=device)
+    r = Renderer(params, sh_degree=3, grad_mode=a.grad_mode)
+    host_g = [torch.from_numpy(g).pin_memory() for g in scenes.upstream_grads(a.views, a.res, a.res, seed=a.seed + 1)]
+    host_c = [(torch.from_numpy(c.viewmatrix).pin_memory(), torch.from_numpy(c.projmatrix).pin_memory(),
+               torch.from_numpy(c.campos).pin_memory()) for c in cams]
+    h2d = sum(g.numel() * 4 for g in host_g) + sum(sum(x.numel() * 4 for x in c) for c in host_c)
+    loss_host = torch.empty(a.views, dtype=torch.float32).pin_memory()
+
+    def step():
+        for p_ in params.parameters():
+            p_.grad = None
+        losses = []
+        for v, c in enumerate(cams):
+            g = host_g[v].to(device, non_blocking=True)
+            V, Pm, C = (x.to(device, non_blocking=True) for x in host_c[v])
+            out = r.render(c.fovx, c.fovy, V, Pm, C, a.res, a.res)
+            loss = (out["image"] * g).sum()
+            loss.backward()
+            losses.append(loss.detach())
+        loss_host.copy_(torch.stack(losses), non_blocking=True)
+        torch.cuda.current_stream().synchronize()
+        return loss_host
+
+    for _ in range(max(a.warmup, 1)):
+        step()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(a.steps):
+        step()
+    e1.record()
+    torch.cuda.synchronize()
+    ms = wd.max_over_ranks(e0.elapsed_time(e1), device=device)
+    return {"value": round(world * a.views * a.steps / (ms / 1e3), 3), "unit": UNIT, "h2d_bytes_per_step": int(h2d),
+            "d2h_bytes_per_step": int(loss_host.numel() * 4), "api": "word2world_b200.renderer.Renderer.render"}
+
+
+# ---------------------------------------------------------------------------
+# CPU baselines (the oracle: the reference has no CPU implementation)
+# ---------------------------------------------------------------------------
+_W = {}
+
+
+def _worker_init(P, res, views, seed):
+    sys.path.insert(0, ROOT)
+    from word2world_b200 import camera, scenes
+    sc = scenes.make_scene(P, seed=seed, layout="ball")
+    _W["arrays"] = sc.activate()
+    _W["cams"] = camera.orbit_views(views, 2.5, res, res)
+    _W["grads"] = scenes.upstream_grads(views, res, res, seed=seed + 1)
+
+
+def _worker_view(v):
+    import oracle
+    m, o, s, q, sh = _W["arrays"]
+    st = oracle.RasterSettings.from_camera(_W["cams"][v])
+    t = time.perf_counter()
+    f = oracle.forward(st, m, s, q, o, sh)
+    oracle.backward(f, _W["grads"][v])
+    return time.perf_counter() - t
+
+
+def cpu_baseline(a):
+    """The oracle (single thread) on a bounded sample: one view of the workload."""
+    _worker_init(a.P, a.res, a.views, a.seed)
+    _worker_view(0)  # warm (page in, allocator)
+    t = _worker_view(1 % a.views)
+    return {"value": round(1.0 / t, 4), "unit": UNIT, "cores": 1, "kind": "port",
+            "sample": f"1 view of the workload (fwd+bwd, reference formulas), {t:.2f} s, single thread"}
+
+
+def run_reference(a):
+    """Reference arm: the reference path has no CPU implementation, so its CPU
+    path is the oracle (a restatement of the reference's arithmetic) run with
+    one process per view on the host cores.  Each step renders and
+    back-propagates all views of the workload."""
+    import multiprocessing as mp
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    procs = max(1, min(a.views, os.cpu_count() or 1))
+    ctx = mp.get_context("spawn")
+    with ctx.Pool(procs, initializer=_worker_init, initargs=(a.P, a.res, a.views, a.seed)) as pool:
+        for _ in range(max(a.warmup, 1)):
+            pool.map(_worker_view, range(a.views))
+        t0 = time.perf_counter()
+        for _ in range(a.steps):
+            pool.map(_worker_view, range(a.views))
+        dt = time.perf_counter() - t0
+    value = a.views * a.steps / dt
+    result = {"metric": METRIC, "value": round(value, 4), "unit": UNIT, "n_gpus": int(os.environ.get("WORLD_SIZE", "1")),
+              "steps": a.steps, "warmup": a.warmup, "ms_per_step": round(dt / a.steps * 1e3, 2),
+              "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+              "data": "synthetic (seeded scene, N(0,1) dL/dimage)", "config": workload_config(a), "impl": "reference",
+              "cpu_baseline": {"value": round(value, 4), "unit": UNIT, "cores": procs, "kind": "port",
+                               "sample": f"all {a.views} views per step, one process per view"},
+              "e2e": {"value": round(value, 4), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(result), flush=True)
+
+
+def main():
+    a = parse()
+    if a.impl == "reference":
+        run_reference(a)
+    else:
+        run_ours(a)
+
+
+if __name__ == "__main__":
+    main()

@@ -164,6 +164,19 @@ int w2w_blend(const w2w_settings* s, const void* geom_state, const uint32_t* ran
 int w2w_binning_keys64(const void* binning_state, long long num_rendered, int width, int height,
                        uint64_t* out, w2w_stream_t stream);
 
+/* ---- observability ---------------------------------------------------------
+ * Number of kernels the library has launched in this process. */
+unsigned long long w2w_launch_count(void);
+/* Per-stage device timing with CUDA events recorded on the launching stream
+ * (off by default).  w2w_stage_timing returns the previous setting.
+ * w2w_stage_times waits for the recorded events, writes accumulated
+ * milliseconds and kernel launches per stage (w2w_stage_count() stages,
+ * named by w2w_stage_name) and resets the accumulators. */
+int w2w_stage_timing(int enable);
+int w2w_stage_count(void);
+const char* w2w_stage_name(int stage);
+int w2w_stage_times(double* ms, long long* launches, int max_stages);
+
 #ifdef __cplusplus
 }
 #endif

@@ -35,7 +35,8 @@ LIB_PATH = os.path.join(HERE, "liborc_w2w.so")
 
 _FAMILIES = [("RQ", 9), ("SIGMA", 6), ("VIEW_A", 4), ("VIEW_B", 4), ("RAYR2", 1), ("DPROJ", 6), ("SIGV", 6),
              ("DOT3", 3), ("DET", 1), ("PROJ_A", 4), ("PROJ_B", 4), ("PIX", 2), ("ADR_DELTA", 1), ("BL_DET", 1),
-             ("BL_TX", 1), ("BL_TY", 1), ("BL_NUM", 1), ("BL_DEPTH", 1), ("SH_DOT", 1), ("SH_ACC", 1)]
+             ("BL_TX", 1), ("BL_TY", 1), ("BL_NUM", 1), ("BL_DEPTH", 1), ("SH_DOT", 1), ("SH_ACC", 1),
+             ("SH2A", 1), ("SH2B", 1), ("SH3A", 1), ("SH3B", 1), ("SH3C", 1), ("SH3D", 1), ("SH3E", 1)]
 VARIANT_NAMES = [f"{n}{i}" if k > 1 else n for n, k in _FAMILIES for i in range(k)]
 # Fusion pattern per expression instance (see raster_core.h s1/s2/d2/s3).
 # Pinned against the reference extension's geometry buffers on a B200
@@ -44,8 +45,13 @@ VARIANT_NAMES = [f"{n}{i}" if k > 1 else n for n, k in _FAMILIES for i in range(
 # bit-identical.  Pattern 1 (fuse the first product) everywhere except:
 #   RQ0: 2-4(yy+zz) unfused; RQ2: xz+ry fuses r*y; RQ6: xz-ry fuses -r*y;
 #   PIX0/PIX1: the NDC multiply is fused into "+1" and "*W - 0.5" is fused.
+# The blend patterns (BL_*) were pinned on the reference's own sorted lists:
+# with them the contributor counts, alpha and depth images are bit-identical;
+# the SH patterns (SH*) make the colours bit-identical.
 PINNED_VARIANTS = {name: 1 for name in VARIANT_NAMES}
-PINNED_VARIANTS.update({"RQ0": 0, "RQ2": 2, "RQ6": 2, "PIX0": 2, "PIX1": 2})
+PINNED_VARIANTS.update({"RQ0": 0, "RQ2": 2, "RQ6": 2, "PIX0": 2, "PIX1": 2,
+                        "BL_DET": 1, "BL_TX": 1, "BL_TY": 2, "BL_NUM": 2, "BL_DEPTH": 1,
+                        "SH2A": 0, "SH2B": 0, "SH3A": 1, "SH3B": 0, "SH3C": 1, "SH3D": 0, "SH3E": 1})
 
 _lib = None
 

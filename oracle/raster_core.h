@@ -288,24 +288,41 @@ static void SFX(sh_one)(const float* mean, const float* campos, const float* sh,
         ACC((REAL)0.4886025119029199f * z, 2);
         ACC((REAL)-0.4886025119029199f * x, 3);
     }
+    /* polynomial terms; selectors choose which squares are fused into the
+     * subtractions (the squares are otherwise rounded products) */
+    REAL xx = x * x, yy = y * y, zz = z * z;
+    /* k*zz - xx - yy */
+    #define KZZ(v, k) ((v) == 1 ? RFMA(-y, y, RFMA(-x, x, (REAL)(k) * zz)) : \
+                      (v) == 2 ? RFMA(-y, y, (REAL)(k) * zz - xx) : \
+                      (v) == 3 ? RFMA(-x, x, (REAL)(k) * zz) - yy : ((REAL)(k) * zz - xx) - yy)
+    /* xx - yy */
+    #define XMY(v) ((v) == 1 ? RFMA(x, x, -yy) : (v) == 2 ? RFMA(-y, y, xx) : xx - yy)
     if (deg >= 2 && M > 8) {
-        REAL xx = x * x, yy = y * y, zz = z * z, xy = x * y, yz = y * z, xz = x * z;
+        REAL xy = x * y, yz = y * z, xz = x * z;
         ACC((REAL)1.0925484305920792f * xy, 4);
         ACC((REAL)-1.0925484305920792f * yz, 5);
-        ACC((REAL)0.3f * (((REAL)2 * zz - xx) - yy), 6);
+        ACC((REAL)0.3f * KZZ(orc_var[V_SH2A], 2), 6);
         ACC((REAL)-1.0925484305920792f * xz, 7);
-        ACC((REAL)0.5462742152960396f * (xx - yy), 8);
+        ACC((REAL)0.5462742152960396f * XMY(orc_var[V_SH2B]), 8);
     }
     if (deg >= 3 && M > 15) {
-        REAL xx = x * x, yy = y * y, zz = z * z;
-        ACC(((REAL)-0.5900435899266435f * y) * ((REAL)3 * xx - yy), 9);
+        int v3a = orc_var[V_SH3A], v3c = orc_var[V_SH3C], v3e = orc_var[V_SH3E];
+        REAL t9 = v3a == 1 ? RFMA((REAL)3, xx, -yy) : v3a == 2 ? RFMA(-y, y, (REAL)3 * xx) : (REAL)3 * xx - yy;
+        REAL t12 = v3c == 1 ? RFMA((REAL)-3, yy, RFMA((REAL)-3, xx, (REAL)2 * zz))
+                 : v3c == 2 ? RFMA((REAL)-3, yy, (REAL)2 * zz - (REAL)3 * xx)
+                 : v3c == 3 ? RFMA((REAL)-3, xx, (REAL)2 * zz) - (REAL)3 * yy
+                            : ((REAL)2 * zz - (REAL)3 * xx) - (REAL)3 * yy;
+        REAL t15 = v3e == 1 ? RFMA((REAL)-3, yy, xx) : v3e == 2 ? RFMA(x, x, -((REAL)3 * yy)) : xx - (REAL)3 * yy;
+        ACC(((REAL)-0.5900435899266435f * y) * t9, 9);
         ACC((((REAL)2.890611442640554f * x) * y) * z, 10);
-        ACC(((REAL)-0.4570457994644658f * y) * (((REAL)4 * zz - xx) - yy), 11);
-        ACC(((REAL)0.3731763325901154f * z) * (((REAL)2 * zz - (REAL)3 * xx) - (REAL)3 * yy), 12);
-        ACC(((REAL)-0.4570457994644658f * x) * (((REAL)4 * zz - xx) - yy), 13);
-        ACC(((REAL)1.445305721320277f * z) * (xx - yy), 14);
-        ACC(((REAL)-0.5900435899266435f * x) * (xx - (REAL)3 * yy), 15);
+        ACC(((REAL)-0.4570457994644658f * y) * KZZ(orc_var[V_SH3B], 4), 11);
+        ACC(((REAL)0.3731763325901154f * z) * t12, 12);
+        ACC(((REAL)-0.4570457994644658f * x) * KZZ(orc_var[V_SH3B], 4), 13);
+        ACC(((REAL)1.445305721320277f * z) * XMY(orc_var[V_SH3D]), 14);
+        ACC(((REAL)-0.5900435899266435f * x) * t15, 15);
     }
+    #undef KZZ
+    #undef XMY
 #undef ACC
     for (int k = 0; k < 3; ++k) {
         out[k] = out[k] + (REAL)0.5;

@@ -47,6 +47,7 @@ enum {
     V_PIX = V_PROJ_B + 4,     /* 2 */
     V_ADR_DELTA = V_PIX + 2,  /* 1 */
     V_BL_DET, V_BL_TX, V_BL_TY, V_BL_NUM, V_BL_DEPTH, V_SH_DOT, V_SH_ACC,
+    V_SH2A, V_SH2B, V_SH3A, V_SH3B, V_SH3C, V_SH3D, V_SH3E,
     V_COUNT
 };
 static int orc_var[V_COUNT];

@@ -183,9 +183,10 @@ def run_case(ref, name, spec, full: bool, repeats: int = 3):
         res["bin_" + k] = v
     for k, v in zip(names, grads):
         res[k] = v.cpu().numpy()
-    res["dL_dcolor_in"] = dLc[:, :S, :S]
-    res["dL_ddepth_in"] = dLd[:, :S, :S]
-    res["dL_dalpha_in"] = dLa[:, :S, :S]
+    # upstream gradients outside the image box meet no Gaussian and are not stored
+    res["dL_dcolor_in"] = dLc[:, y0:y1, x0:x1]
+    res["dL_ddepth_in"] = dLd[:, y0:y1, x0:x1]
+    res["dL_dalpha_in"] = dLa[:, y0:y1, x0:x1]
     res["in_means3D"], res["in_opac"], res["in_scales"], res["in_rots"], res["in_shs"] = means3D, opac, scales, rots, shs
     res["cam_view"], res["cam_proj"], res["cam_campos"] = ecam.viewmatrix, ecam.projmatrix, ecam.campos
     res["cam_focal_x"] = np.float32(cam.focal_x)

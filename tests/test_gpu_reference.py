@@ -5,8 +5,8 @@ The reference (``oracle/_ref``, built from the reference's own sources by
 crop-embedded (``camera.crop_embed``).  Checked:
 
 * every per-Gaussian field the reference stores is bit-identical (depth,
-  screen position, 3-D covariance, conic, radius, tiles touched, offsets);
-  colours agree to 1 ulp;
+  screen position, 3-D covariance, conic, colour, clamp flags, radius, tiles
+  touched, offsets);
 * key emission: at every slot of the unsorted key array that exactly one
   Gaussian writes, the reference's key and id equal the deterministic model
   (``oracle.forward`` = this implementation); at slots several Gaussians write
@@ -15,8 +15,8 @@ crop-embedded (``camera.crop_embed``).  Checked:
 * replayed on the reference's own unsorted keys, the sort reproduces the
   reference's sorted keys and Gaussian ids bit-exactly; replayed on its sorted
   keys, the tile ranges match; replayed on its sorted list, the blend
-  reproduces its contributor counts bit-exactly and its images within 1e-5 +
-  1e-4|x|, and the backward its gradients (parity.grad_check).
+  reproduces its contributor counts and its colour, alpha and depth images
+  bit-exactly, and the backward its gradients (parity.grad_check).
 """
 import importlib.machinery
 import importlib.util
@@ -89,11 +89,9 @@ def test_against_reference(ref, name):
     S = spec["size"]
     # ---- this implementation in the reference's 800x800 frame ----
     mine = gh.forward(arrays, ecam, degree=spec["degree"], focal_x=cam.focal_x)
-    for k in ("depth", "means2D", "cov3D", "conic_opac", "tiles", "offsets"):
+    for k in ("depth", "means2D", "cov3D", "conic_opac", "rgb", "clamped", "tiles", "offsets"):
         assert parity.bit_mismatch(mine[k], res["geom_" + k]) == 0, k
     assert parity.bit_mismatch(mine["radii"], res["radii"]) == 0
-    rgb_ulps = np.abs(mine["rgb"].view(np.int32).astype(np.int64) - res["geom_rgb"].view(np.int32).astype(np.int64))
-    assert rgb_ulps.max() <= 1, rgb_ulps.max()
     R = res["R"]
     assert mine["num_rendered"] == R
 
@@ -129,25 +127,28 @@ def test_against_reference(ref, name):
     nc = gh.unpack_image(img, FRAME, FRAME)["n_contrib"]
     assert parity.bit_mismatch(nc, res["n_contrib"]) == 0
     for k, v in (("color", color), ("alpha", alpha), ("depth_img", depth)):
-        e = parity.err_stats(v.cpu().numpy(), res[k])
-        assert e["n_bad"] == 0, (k, e)
-        print(f"{name}: replayed {k} bit mismatches {parity.bit_mismatch(v.cpu().numpy(), res[k])} of {e['n']}")
-    # backward on the replayed state
+        assert parity.bit_mismatch(v.cpu().numpy(), res[k]) == 0, k
+    # backward on the replayed state.  The reference backward starts from
+    # T_final = 1 - alpha (backward.cu:565), which amplifies a 1-ulp change of
+    # a nearly opaque pixel's alpha by up to 1e4, so both sides get the
+    # reference's own alpha image.
+    ref_alpha = np.asarray(res["alpha"], np.float32)
     binb = torch.zeros(_C.binning_state_bytes(R, FRAME, FRAME), dtype=torch.uint8, device="cuda")
     off = _C.binning_offset(R, FRAME, FRAME, "vals_a")
     binb[off:off + 4 * R] = torch.from_numpy(res["bin_point_list"].view(np.uint8)).cuda()
+    y0, y1, x0, x1 = res["img_box"]
     dLc = np.zeros((3, FRAME, FRAME), np.float32)
-    dLc[:, :S, :S] = res["dL_dcolor_in"]
+    dLc[:, y0:y1, x0:x1] = res["dL_dcolor_in"]
     dLd = np.zeros((1, FRAME, FRAME), np.float32)
-    dLd[:, :S, :S] = res["dL_ddepth_in"]
+    dLd[:, y0:y1, x0:x1] = res["dL_ddepth_in"]
     dLa = np.zeros((1, FRAME, FRAME), np.float32)
-    dLa[:, :S, :S] = res["dL_dalpha_in"]
+    dLa[:, y0:y1, x0:x1] = res["dL_dalpha_in"]
     empty = torch.empty(0, device="cuda")
     tan = float(cam.tanfovx * FRAME / cam.width), float(cam.tanfovy * FRAME / cam.height)
     g = _C.rasterize_gaussians_backward(
         torch.ones(3, device="cuda"), gh.dev(m), mine["_tensors"]["radii"], empty, gh.dev(s), gh.dev(q), 1.0, empty,
         gh.dev(ecam.viewmatrix), gh.dev(ecam.projmatrix), tan[0], tan[1], gh.dev(dLc), gh.dev(dLd), gh.dev(dLa),
-        gh.dev(sh), spec["degree"], gh.dev(ecam.campos), geom, R, binb, img, alpha, False, 0)
+        gh.dev(sh), spec["degree"], gh.dev(ecam.campos), geom, R, binb, img, gh.dev(ref_alpha), False, 0)
     report = {}
     for k, v in zip(parity.GRAD_NAMES, g):
         c = parity.grad_check(v.cpu().numpy(), res[k])

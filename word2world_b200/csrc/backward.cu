@@ -645,15 +645,19 @@ __global__ void __launch_bounds__(256) gaussians_exact_kernel(BackwardArgs a) {
 void launch_backward_render(const BackwardArgs& a, cudaStream_t stream) {
   const dim3 grid((a.W + kTile - 1) / kTile, (a.H + kTile - 1) / kTile);
   if (grid.x == 0 || grid.y == 0) return;
+  stage_begin(kStBwdRender, stream);
   if (a.grad_mode == 1) render_exact_kernel<<<grid, kBlendThreads, 0, stream>>>(a);
   else render_ref_kernel<<<grid, kBlendThreads, 0, stream>>>(a);
+  stage_end(kStBwdRender, stream, 1);
 }
 
 void launch_backward_gaussians(const BackwardArgs& a, cudaStream_t stream) {
   if (a.P <= 0) return;
   const int blocks = (a.P + 255) / 256;
+  stage_begin(kStBwdGaussians, stream);
   if (a.grad_mode == 1) gaussians_exact_kernel<<<blocks, 256, 0, stream>>>(a);
   else gaussians_ref_kernel<<<blocks, 256, 0, stream>>>(a);
+  stage_end(kStBwdGaussians, stream, 1);
 }
 
 }  // namespace w2w

@@ -322,5 +322,30 @@ PYBIND11_MODULE(TORCH_EXTENSION_NAME, m) {
   m.def("binning_offset", [](int64_t R, int64_t W, int64_t H, const std::string& n) {
     return int64_t(w2w_binning_offset(R, int(W), int(H), n.c_str()));
   });
+  m.def("binning_info", [](const Tensor& binningBuffer, int64_t R, int64_t H, int64_t W) {
+    // the sort plan recorded in a binning state's header (reads 64 bytes back)
+    py::dict d;
+    if (R <= 0) return d;
+    const int64_t off = int64_t(w2w_binning_offset(R, int(W), int(H), "header"));
+    Tensor h = binningBuffer.narrow(0, off, 64).cpu().contiguous();
+    const uint32_t* u = reinterpret_cast<const uint32_t*>(h.data_ptr());
+    d["key64"] = u[1]; d["depth_bits"] = u[2]; d["tile_bits"] = u[4]; d["passes"] = u[5];
+    return d;
+  });
   m.def("version", &w2w_version);
+  m.def("launch_count", []() { return (unsigned long long)w2w_launch_count(); });
+  m.def("stage_timing", [](bool on) { return w2w_stage_timing(on ? 1 : 0) != 0; });
+  m.def("stage_times", []() {
+    const int n = w2w_stage_count();
+    std::vector<double> ms(n);
+    std::vector<long long> cnt(n);
+    {
+      pybind11::gil_scoped_release nogil;
+      w2w_stage_times(ms.data(), cnt.data(), n);
+    }
+    py::dict d;
+    for (int i = 0; i < n; ++i)
+      d[py::str(w2w_stage_name(i))] = py::make_tuple(ms[i], cnt[i]);
+    return d;
+  });
 }

@@ -136,7 +136,9 @@ __global__ void __launch_bounds__(kBlendThreads) blend_kernel(BlendArgs a) {
 void launch_blend(const BlendArgs& a, cudaStream_t stream) {
   const dim3 grid((a.W + kTile - 1) / kTile, (a.H + kTile - 1) / kTile);
   if (grid.x == 0 || grid.y == 0) return;
+  stage_begin(kStBlend, stream);
   blend_kernel<<<grid, kBlendThreads, 0, stream>>>(a);
+  stage_end(kStBlend, stream, 1);
 }
 
 }  // namespace w2w

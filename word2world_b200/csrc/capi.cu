@@ -251,7 +251,9 @@ int w2w_forward_render(const w2w_settings* s, const void* geom_state, const w2w_
     const KeyPlan kp = plan_keys(*info, W, H);
     const int passes = sort_passes(kp.bits);
     BinHeader* bh = at<BinHeader>(binning_state, BL.header);
+    stage_begin(kStOther, st);
     write_bin_header<<<1, 1, 0, st>>>(bh, kp, uint32_t(R), uint32_t(passes));
+    stage_end(kStOther, st, 1);
     // the sort result lands in (keysA, valsA); key emission targets the
     // buffer that makes the ping-pong end there
     const bool odd = (passes % 2) == 1;
@@ -418,9 +420,12 @@ int w2w_tile_ranges(const uint64_t* sorted_keys, long long n, int tile_shift, ui
     return W2W_ERR_INVALID;
   cudaStream_t st = S(stream);
   cudaMemsetAsync(ranges, 0, sizeof(uint2) * size_t(ntiles), st);
-  if (n > 0)
+  if (n > 0) {
+    stage_begin(kStOther, st);
     ranges_from_sorted<<<int((n + 255) / 256), 256, 0, st>>>(sorted_keys, n, tile_shift,
                                                               reinterpret_cast<uint2*>(ranges), ntiles);
+    stage_end(kStOther, st, 1);
+  }
   return check_launch();
 }
 
@@ -459,8 +464,10 @@ int w2w_binning_keys64(const void* binning_state, long long R, int W, int H, uin
       cudaStreamSynchronize(st) != cudaSuccess)
     return W2W_ERR_CUDA;
   const int blocks = int((R + 255) / 256);
+  stage_begin(kStOther, st);
   if (hh.key64) expand_keys<uint64_t><<<blocks, 256, 0, st>>>(h, at<uint64_t>(binning_state, BL.keysA), R, out);
   else expand_keys<uint32_t><<<blocks, 256, 0, st>>>(h, at<uint32_t>(binning_state, BL.keysA), R, out);
+  stage_end(kStOther, st, 1);
   return check_launch();
 }
 

@@ -90,8 +90,10 @@ __global__ void __launch_bounds__(kDupThreads) duplicate_kernel(DuplicateArgs a)
 void launch_duplicate(const DuplicateArgs& a, cudaStream_t stream) {
   if (a.P <= 0 || a.R == 0) return;
   const int blocks = (a.P + kDupThreads - 1) / kDupThreads;
+  stage_begin(kStDuplicate, stream);
   if (a.key64) duplicate_kernel<true><<<blocks, kDupThreads, 0, stream>>>(a);
   else duplicate_kernel<false><<<blocks, kDupThreads, 0, stream>>>(a);
+  stage_end(kStDuplicate, stream, 1);
 }
 
 }  // namespace w2w

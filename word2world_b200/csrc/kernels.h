@@ -145,6 +145,15 @@ void launch_backward_gaussians(const BackwardArgs& a, cudaStream_t stream);
 }  // namespace w2w
 
 namespace w2w {
+// Launch accounting / stage timing (timing.cu).  Stages bracket the launches
+// of one logical step; `kernels` is how many kernels the stage launched.
+enum Stage {
+  kStPreprocess, kStDuplicate, kStSortHist, kStSortPass, kStBlend, kStBwdRender, kStBwdGaussians, kStScan,
+  kStOther, kNumStages
+};
+void stage_begin(int stage, cudaStream_t s);
+void stage_end(int stage, cudaStream_t s, int kernels);
+
 size_t scan_status_words(long long n);
 void launch_scan(const uint32_t* in, uint32_t* out, long long n, int exclusive, unsigned long long* status,
                  uint32_t* counter, uint32_t* err, cudaStream_t stream);

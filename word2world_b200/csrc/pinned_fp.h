@@ -1,11 +1,14 @@
 // Fusion pattern per expression instance in the per-Gaussian and per-pixel
 // arithmetic (see s1/s2/d2/s3 in common.cuh).  Established by comparing
-// against the reference extension's geometry buffers on a B200; with these
-// values depth, screen position, 3-D covariance, conic, radius and tile
-// counts are bit-identical to the reference.  Indices: RQ = rotation matrix
-// entries (column-major), SIGMA = stored covariance entries, VIEW/PROJ rows,
-// DPROJ = Jacobian rows (x then y), SIGV = Sigma*j rows, DOT3 = cxx/cxy/cyy,
-// PIX = screen x/y, BL_* = per-pixel Gaussian evaluation.
+// against the reference extension's buffers on a B200: with these values
+// depth, screen position, 3-D covariance, conic, colour, radius and tile
+// counts are bit-identical to the reference, and so are contributor counts,
+// alpha and depth images when blending the same sorted lists.  Indices:
+// RQ = rotation matrix entries (column-major), SIGMA = stored covariance
+// entries, VIEW/PROJ rows, DPROJ = Jacobian rows (x then y), SIGV = Sigma*j
+// rows, DOT3 = cxx/cxy/cyy, PIX = screen x/y, BL_* = per-pixel Gaussian
+// evaluation, SH* = colour polynomial terms.  The CPU oracle carries the
+// same table.
 #pragma once
 
 namespace w2w {
@@ -63,10 +66,17 @@ constexpr int PIX1 = 2;
 constexpr int ADR_DELTA = 1;
 constexpr int BL_DET = 1;
 constexpr int BL_TX = 1;
-constexpr int BL_TY = 1;
-constexpr int BL_NUM = 1;
+constexpr int BL_TY = 2;
+constexpr int BL_NUM = 2;
 constexpr int BL_DEPTH = 1;
 constexpr int SH_DOT = 1;
 constexpr int SH_ACC = 1;
+constexpr int SH2A = 0;
+constexpr int SH2B = 0;
+constexpr int SH3A = 1;
+constexpr int SH3B = 0;
+constexpr int SH3C = 1;
+constexpr int SH3D = 0;
+constexpr int SH3E = 1;
 }  // namespace fp
 }  // namespace w2w

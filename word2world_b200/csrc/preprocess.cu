@@ -154,6 +154,22 @@ __device__ __forceinline__ void project(const float* __restrict__ V, const float
   g.visible = true;
 }
 
+// k*zz - xx - yy with the squares optionally fused into the subtractions
+template <int V>
+__device__ __forceinline__ float kzz(float k, float x, float y, float xx, float yy, float zz) {
+  if constexpr (V == 1) return fma(-y, y, fma(-x, x, mul(k, zz)));
+  else if constexpr (V == 2) return fma(-y, y, sub(mul(k, zz), xx));
+  else if constexpr (V == 3) return sub(fma(-x, x, mul(k, zz)), yy);
+  else return sub(sub(mul(k, zz), xx), yy);
+}
+// xx - yy
+template <int V>
+__device__ __forceinline__ float xmy(float x, float y, float xx, float yy) {
+  if constexpr (V == 1) return fma(x, x, -yy);
+  else if constexpr (V == 2) return fma(-y, y, xx);
+  else return sub(xx, yy);
+}
+
 // SH colour (gaussianForwardPass.cu:195-263); coefficients needed by a degree
 // are used only when stored (degree d needs (d+1)^2 of them).
 __device__ __forceinline__ void sh_colour(const float* __restrict__ sh, int M, int deg, float px, float py, float pz,
@@ -174,24 +190,30 @@ __device__ __forceinline__ void sh_colour(const float* __restrict__ sh, int M, i
     acc(mul(kC1, z), 2);
     acc(mul(-kC1, x), 3);
   }
+  const float xx = mul(x, x), yy = mul(y, y), zz = mul(z, z);
   if (deg >= 2 && M > 8) {
-    const float xx = mul(x, x), yy = mul(y, y), zz = mul(z, z);
     const float xy = mul(x, y), yz = mul(y, z), xz = mul(x, z);
     acc(mul(kC2a, xy), 4);
     acc(mul(-kC2a, yz), 5);
-    acc(mul(0.3f, sub(sub(mul(2.0f, zz), xx), yy)), 6);
+    acc(mul(0.3f, kzz<SH2A>(2.0f, x, y, xx, yy, zz)), 6);
     acc(mul(-kC2a, xz), 7);
-    acc(mul(kC2e, sub(xx, yy)), 8);
+    acc(mul(kC2e, xmy<SH2B>(x, y, xx, yy)), 8);
   }
   if (deg >= 3 && M > 15) {
-    const float xx = mul(x, x), yy = mul(y, y), zz = mul(z, z);
-    acc(mul(mul(-kC30, y), sub(mul(3.0f, xx), yy)), 9);
+    // 3xx - yy, 2zz - 3xx - 3yy and xx - 3yy with the reference's fusions
+    const float t9 = SH3A == 1 ? fma(3.0f, xx, -yy) : SH3A == 2 ? fma(-y, y, mul(3.0f, xx)) : sub(mul(3.0f, xx), yy);
+    const float t12 = SH3C == 1 ? fma(-3.0f, yy, fma(-3.0f, xx, mul(2.0f, zz)))
+                    : SH3C == 2 ? fma(-3.0f, yy, sub(mul(2.0f, zz), mul(3.0f, xx)))
+                    : SH3C == 3 ? sub(fma(-3.0f, xx, mul(2.0f, zz)), mul(3.0f, yy))
+                                : sub(sub(mul(2.0f, zz), mul(3.0f, xx)), mul(3.0f, yy));
+    const float t15 = SH3E == 1 ? fma(-3.0f, yy, xx) : SH3E == 2 ? fma(x, x, -mul(3.0f, yy)) : sub(xx, mul(3.0f, yy));
+    acc(mul(mul(-kC30, y), t9), 9);
     acc(mul(mul(mul(kC31, x), y), z), 10);
-    acc(mul(mul(-kC32, y), sub(sub(mul(4.0f, zz), xx), yy)), 11);
-    acc(mul(mul(kC33, z), sub(sub(mul(2.0f, zz), mul(3.0f, xx)), mul(3.0f, yy))), 12);
-    acc(mul(mul(-kC32, x), sub(sub(mul(4.0f, zz), xx), yy)), 13);
-    acc(mul(mul(kC35, z), sub(xx, yy)), 14);
-    acc(mul(mul(-kC30, x), sub(xx, mul(3.0f, yy))), 15);
+    acc(mul(mul(-kC32, y), kzz<SH3B>(4.0f, x, y, xx, yy, zz)), 11);
+    acc(mul(mul(kC33, z), t12), 12);
+    acc(mul(mul(-kC32, x), kzz<SH3B>(4.0f, x, y, xx, yy, zz)), 13);
+    acc(mul(mul(kC35, z), xmy<SH3D>(x, y, xx, yy)), 14);
+    acc(mul(mul(-kC30, x), t15), 15);
   }
   rgb[0] = add(o0, 0.5f);
   rgb[1] = add(o1, 0.5f);
@@ -416,8 +438,10 @@ void launch_preprocess(const PreprocessArgs& a, cudaStream_t stream) {
   const int blocks = (a.P + kPreThreads - 1) / kPreThreads;
   if (blocks == 0) return;
   const bool sh16 = a.M == 16 && (reinterpret_cast<uintptr_t>(a.shs) & 15) == 0;
+  stage_begin(kStPreprocess, stream);
   if (sh16) preprocess_kernel<true><<<blocks, kPreThreads, 0, stream>>>(a);
   else preprocess_kernel<false><<<blocks, kPreThreads, 0, stream>>>(a);
+  stage_end(kStPreprocess, stream, 1);
 }
 
 }  // namespace w2w

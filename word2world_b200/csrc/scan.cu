@@ -107,7 +107,9 @@ void launch_scan(const uint32_t* in, uint32_t* out, long long n, int exclusive, 
   const long long tiles = (n + kScanTile - 1) / kScanTile;
   cudaMemsetAsync(status, 0, sizeof(unsigned long long) * size_t(tiles), stream);
   cudaMemsetAsync(counter, 0, sizeof(uint32_t), stream);
+  stage_begin(kStScan, stream);
   scan_kernel<<<int(tiles), kScanThreads, 0, stream>>>(in, out, n, exclusive, status, counter, err);
+  stage_end(kStScan, stream, 1);
 }
 
 }  // namespace w2w

@@ -250,9 +250,11 @@ void run_sort(const SortArgs& a, cudaStream_t stream) {
     const size_t smem = sizeof(uint32_t) * (size_t(passes) * 256 + (tiles_in_smem ? size_t(a.num_tiles) : 0));
     if (smem > 48 * 1024)
       cudaFuncSetAttribute(hist_kernel<K>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+    stage_begin(kStSortHist, stream);
     hist_kernel<K><<<grid, kHistThreads, smem, stream>>>(reinterpret_cast<const K*>(a.keys_in), n, a.begin_bit,
                                                          passes, a.hist, a.tile_shift, a.num_tiles, a.tile_hist);
     offsets_kernel<<<1, 1024, 0, stream>>>(a.hist, passes, a.tile_hist, a.num_tiles, a.ranges);
+    stage_end(kStSortHist, stream, 2);
   }
   const size_t dyn = (sizeof(K) + sizeof(uint32_t)) * kSortTile;
   cudaFuncSetAttribute(onesweep_kernel<K>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(dyn));
@@ -262,9 +264,11 @@ void run_sort(const SortArgs& a, cudaStream_t stream) {
     const bool to_out = ((passes - 1 - p) % 2) == 0;
     K* kout = reinterpret_cast<K*>(to_out ? a.keys_out : a.keys_tmp);
     uint32_t* vout = to_out ? a.vals_out : a.vals_tmp;
+    stage_begin(kStSortPass, stream);
     onesweep_kernel<K><<<int(tiles), kSortThreads, dyn, stream>>>(
         kin, vin, kout, vout, n, a.begin_bit + 8 * p, a.hist + 256 * p, a.status + size_t(p) * 256 * size_t(tiles),
         a.counters + p, a.error);
+    stage_end(kStSortPass, stream, 1);
     kin = kout;
     vin = vout;
   }
