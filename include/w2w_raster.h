@@ -147,6 +147,24 @@ size_t w2w_scan_scratch_bytes(long long n);
 int w2w_scan_u32(const uint32_t* in, uint32_t* out, long long n, int exclusive, void* scratch,
                  size_t scratch_bytes, w2w_stream_t stream);
 
+/* Allocation-free variant of w2w_scan_u32.  No counterpart in the reference.
+ * For callers that cannot call cudaMalloc or hand the library a scratch
+ * buffer: hosts whose device memory is owned by another allocator (a JVM or
+ * Go runtime reaching the library through JNI / cgo, a plugin host with its
+ * own pool) and hot loops in which an allocation's implicit device
+ * synchronisation is not acceptable.  The lookback scratch lives in a fixed
+ * device array inside the library (about 32 KB, held by every GPU that loads
+ * the library until the process exits), so the caller passes only the input
+ * and output.  At most W2W_SCAN_NOALLOC_MAX elements; larger n returns
+ * W2W_ERR_CAPACITY without launching anything.  The first call on a device
+ * looks up the array's device address (done once per device, with that
+ * device current), so make that first call before any stream capture on the
+ * device.  All calls share the one array and each clears the parts it needs
+ * before use; calls that overlap on the GPU (other streams, other threads)
+ * race on it, so serialise them.  Never calls cudaMalloc or cudaFree. */
+#define W2W_SCAN_NOALLOC_MAX (1LL << 24)
+int w2w_scan_u32_noalloc(const uint32_t* in, uint32_t* out, long long n, int exclusive, w2w_stream_t stream);
+
 /* Per-tile [start, end) from sorted keys whose tile id is key >> tile_shift
  * (gaussianTiles.cu:6-33); tiles without entries get (0, 0). */
 int w2w_tile_ranges(const uint64_t* sorted_keys, long long n, int tile_shift, uint32_t* ranges,

@@ -414,6 +414,24 @@ int w2w_scan_u32(const uint32_t* in, uint32_t* out, long long n, int exclusive, 
   return check_launch();
 }
 
+int w2w_scan_u32_noalloc(const uint32_t* in, uint32_t* out, long long n, int exclusive, w2w_stream_t stream) {
+  if (n < 0) return W2W_ERR_INVALID;
+  if (n == 0) return W2W_OK;
+  if (!in || !out) return W2W_ERR_INVALID;
+  if (n > scan_noalloc_max()) {
+    std::fprintf(stderr,
+                 "w2w_scan_u32_noalloc: %lld elements exceed the %lld this entry point's fixed scratch holds; "
+                 "use w2w_scan_u32 with a caller-provided scratch buffer\n",
+                 n, scan_noalloc_max());
+    return W2W_ERR_CAPACITY;
+  }
+  int rc = 0;
+  void* scratch = scan_noalloc_scratch(&rc);
+  if (rc != 0 || scratch == nullptr) return W2W_ERR_CUDA;
+  launch_scan_noalloc(in, out, n, exclusive, scratch, S(stream));
+  return check_launch();
+}
+
 int w2w_tile_ranges(const uint64_t* sorted_keys, long long n, int tile_shift, uint32_t* ranges, int ntiles,
                     w2w_stream_t stream) {
   if (n < 0 || ntiles <= 0 || !ranges || (n > 0 && !sorted_keys) || tile_shift < 0 || tile_shift > 63)

@@ -3,6 +3,8 @@
 // which allocates, frees and synchronises the device at every level).  The
 // rasterizer itself fuses its scan into the preprocess kernel; this entry
 // point serves the isolated-stage workload and callers that scan alone.
+#include <mutex>
+
 #include "common.cuh"
 #include "kernels.h"
 
@@ -97,9 +99,51 @@ scan_kernel(const uint32_t* __restrict__ in, uint32_t* __restrict__ out, long lo
   }
 }
 
+// Scratch of the allocation-free entry point: the lookback status words for
+// up to kScanNoAllocMax elements, then the tile counter and the error word.
+// Every device that loads this library holds it (about 32 KB) until exit.
+constexpr long long kScanNoAllocMax = 1LL << 24;
+constexpr size_t kNoAllocStatusBytes = size_t((kScanNoAllocMax + kScanTile - 1) / kScanTile) * 8;
+static __device__ __align__(256) unsigned char g_scan_scratch[kNoAllocStatusBytes + 256];
+
 }  // namespace
 
 size_t scan_status_words(long long n) { return size_t((n + kScanTile - 1) / kScanTile) + 1; }
+
+long long scan_noalloc_max() { return kScanNoAllocMax; }
+
+// Device address of g_scan_scratch on the current device.  Host code may not
+// use the symbol itself (on the host it is only a stand-in), so the address is
+// looked up once per device, with that device current, and cached.
+void* scan_noalloc_scratch(int* status) {
+  static std::mutex mu;
+  static void* addr[128] = {nullptr};
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 128) {
+    *status = 2;
+    return nullptr;
+  }
+  std::lock_guard<std::mutex> lk(mu);
+  if (addr[dev] == nullptr) {
+    void* p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_scan_scratch);
+    if (e != cudaSuccess || p == nullptr) {
+      *status = 2;
+      return nullptr;
+    }
+    addr[dev] = p;
+  }
+  *status = 0;
+  return addr[dev];
+}
+
+void launch_scan_noalloc(const uint32_t* in, uint32_t* out, long long n, int exclusive, void* scratch,
+                         cudaStream_t stream) {
+  unsigned long long* status = static_cast<unsigned long long*>(scratch);
+  uint32_t* tail = reinterpret_cast<uint32_t*>(static_cast<unsigned char*>(scratch) + kNoAllocStatusBytes);
+  cudaMemsetAsync(tail, 0, 8, stream);  // error word (launch_scan clears status and counter)
+  launch_scan(in, out, n, exclusive, status, tail, tail + 1, stream);
+}
 
 void launch_scan(const uint32_t* in, uint32_t* out, long long n, int exclusive, unsigned long long* status,
                  uint32_t* counter, uint32_t* err, cudaStream_t stream) {
