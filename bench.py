@@ -201,7 +201,7 @@ def run_ours(a):
     Rm = statistics.mean(p["R"] for p in plans)
     kb = 8 if any(p["key64"] for p in plans) else 4
     alg_bytes = {
-        "preprocess": P * (12 + 12 + 16 + 4 + 12 * M + 24 + 12 + 3 + 16 + 8 + 4 + 4 + 4 + 8 + 48 + 48 + 4 + 4),
+        "preprocess": P * (12 + 12 + 16 + 4 + 12 * M + 24 + 12 + 3 + 16 + 8 + 4 + 4 + 4 + 8 + 64 + 48 + 4 + 4),
         "duplicate": Rm * (kb + 4) + P * 24,
         "sort_histogram": Rm * kb,
         "sort_onesweep": Rm * 2 * (kb + 4),

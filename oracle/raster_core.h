@@ -522,8 +522,11 @@ void SFX(orc_backward_render)(const orc_cfg* cfg, const uint32_t* ranges, const 
                               const REAL* depth, const REAL* out_alpha, const uint32_t* n_contrib,
                               const float* dL_dpix, const float* dL_ddepth, const float* dL_dalpha,
                               double* dmean2D, double* dconic, double* dopac, double* dcolor,
-                              double* ddepth)
+                              double* ddepth, double* abs_sum)
 {
+    /* abs_sum[P*10] (may be NULL): per Gaussian, the sum of |contribution| of
+     * each accumulated value (colour r,g,b, depth, mean2D x,y, conic x,y,w,
+     * opacity) -- the scale of fp32 accumulation-order error */
     const int W = cfg->W, H = cfg->H, gw = (W + 15) / 16;
     const REAL ddelx_dx = (REAL)(0.5 * W), ddely_dy = (REAL)(0.5 * H);
     const REAL bg[3] = {cfg->bg[0], cfg->bg[1], cfg->bg[2]};
@@ -586,6 +589,17 @@ void SFX(orc_backward_render)(const orc_cfg* cfg, const uint32_t* ranges, const 
                 dconic[4 * id + 1] += (double)((REAL)-0.5 * gdx * dy * dLdG);
                 dconic[4 * id + 3] += (double)((REAL)-0.5 * gdy * dy * dLdG);
                 dopac[id] += (double)(G * dLdo);
+                if (abs_sum) {
+                    double* as = abs_sum + 10 * (size_t)id;
+                    for (int c = 0; c < 3; ++c) as[c] += fabs((double)(dchdc * dLp[c]));
+                    as[3] += fabs((double)(a * T * dLd));
+                    as[4] += fabs((double)(dLdG * dGdx * ddelx_dx));
+                    as[5] += fabs((double)(dLdG * dGdy * ddely_dy));
+                    as[6] += fabs((double)((REAL)-0.5 * gdx * dx * dLdG));
+                    as[7] += fabs((double)((REAL)-0.5 * gdx * dy * dLdG));
+                    as[8] += fabs((double)((REAL)-0.5 * gdy * dy * dLdG));
+                    as[9] += fabs((double)(G * dLdo));
+                }
             }
         }
     }

@@ -33,7 +33,7 @@ def unpack_geometry(geom, P):
         rgb=_field(g, o("rgb"), np.float32, 3 * P).reshape(P, 3),
         tiles=_field(g, o("tiles_touched"), np.uint32, P),
         offsets=_field(g, o("offsets"), np.uint32, P),
-        record=_field(g, o("record"), np.float32, 12 * P).reshape(P, 12),
+        record=_field(g, o("record"), np.float32, 16 * P).reshape(P, 16),
     )
     out["header"] = _field(g, o("header"), np.uint32, 8)
     return out

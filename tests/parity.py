@@ -88,16 +88,24 @@ def ncontrib_check(mine_nc, orc_nc, orc_margin, margin=1e-5):
     return dict(n_diff=int(diff.sum()), n_unexplained=int(unexplained.sum()), n=int(diff.size), mask=diff)
 
 
-def grad_check(a, b, row_rtol=1e-3) -> dict:
+# fp32 accumulation of N terms in different orders: the results differ by at
+# most a few ulps of the sum of |terms|; 64 ulps of margin.
+ACC_ULPS = 64 * 2.0 ** -24
+
+
+def grad_check(a, b, row_rtol=1e-3, abs_sum=None) -> dict:
     """Gradient agreement of ``a`` with ``b``.  Elementwise bound
-    |a-b| <= ATOL + RTOL*|b| + row_rtol * max|b over the same Gaussian|: the
-    last term covers components that cancel to much less than their
-    Gaussian's other components, where fp32 accumulation order dominates."""
+    |a-b| <= ATOL + RTOL*|b| + row_rtol * max|b over the same Gaussian|
+    [+ ACC_ULPS * sum|terms| when the per-element sum of absolute
+    contributions is given]: the extra terms cover components that cancel to
+    much less than their summands, where fp32 accumulation order dominates."""
     a = np.asarray(a, np.float64).reshape(len(a), -1)
     b = np.asarray(b, np.float64).reshape(len(b), -1)
     d = np.abs(a - b)
     row = np.abs(b).max(axis=1, keepdims=True) if b.size else b
     tol = ATOL + RTOL * np.abs(b) + row_rtol * row
+    if abs_sum is not None:
+        tol = tol + ACC_ULPS * np.asarray(abs_sum, np.float64).reshape(d.shape)
     nb = float(np.linalg.norm(b.ravel())) or 1.0
     return dict(norm_rel=float(np.linalg.norm((a - b).ravel()) / nb), n_bad=int((d > tol).sum()),
                 n_elem_strict=int((d > ATOL + RTOL * np.abs(b)).sum()), max_abs=float(d.max()) if d.size else 0.0,

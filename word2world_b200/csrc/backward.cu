@@ -25,36 +25,50 @@ namespace {
 
 constexpr int kValues = 10;
 
-__device__ __forceinline__ float warp_sum(float v) {
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-  return v;
+// Where each of the ten per-entry sums goes: after the transposed reduction
+// below, lane L (L even) holds the warp's sum of value (L >> 1); lanes 0..18
+// each add one of them to its gradient array.
+struct Target {
+  float* base;
+  int mult, off;
+  bool active;
+};
+
+__device__ __forceinline__ Target lane_target(const BackwardArgs& a, int mode) {
+  const int lane = threadIdx.x & 31, idx = (lane >> 1) & 15;
+  Target t{nullptr, 0, 0, (lane & 1) == 0 && idx < kValues};
+  if (idx < 3) t = Target{a.dL_dcolors, 3, idx, t.active};
+  else if (idx == 3) t = Target{a.acc_depth, 1, 0, t.active};
+  else if (idx < 6) t = Target{a.dL_dmean2D, 3, idx - 4, t.active};
+  else if (idx < 9) t = Target{a.acc_cov, 4, mode == 0 ? (idx == 8 ? 3 : idx - 6) : idx - 6, t.active};
+  else if (idx == 9) t = Target{a.dL_dopacity, 1, 0, t.active};
+  return t;
 }
 
-__device__ __forceinline__ void flush(const float (&c)[kValues], bool any_contrib, uint32_t id, int mode,
-                                      const BackwardArgs& a) {
+// Sum ten values over the warp with 16 shuffles (each step exchanges the half
+// of the partial sums a lane does not keep) and add each total with one
+// atomic, issued by ten lanes at once.
+__device__ __forceinline__ void flush(const float (&c)[kValues], bool any_contrib, uint32_t id, const Target& t) {
   if (!__any_sync(0xffffffffu, any_contrib)) return;
-  float s[kValues];
+  const unsigned full = 0xffffffffu;
+  const int lane = threadIdx.x & 31;
+  float v[16];
 #pragma unroll
-  for (int k = 0; k < kValues; ++k) s[k] = warp_sum(c[k]);
-  if ((threadIdx.x & 31) == 0) {
-    atomicAdd(a.dL_dcolors + 3 * size_t(id), s[0]);
-    atomicAdd(a.dL_dcolors + 3 * size_t(id) + 1, s[1]);
-    atomicAdd(a.dL_dcolors + 3 * size_t(id) + 2, s[2]);
-    atomicAdd(a.acc_depth + id, s[3]);
-    atomicAdd(a.dL_dmean2D + 3 * size_t(id), s[4]);
-    atomicAdd(a.dL_dmean2D + 3 * size_t(id) + 1, s[5]);
-    if (mode == 0) {
-      atomicAdd(a.acc_cov + 4 * size_t(id), s[6]);
-      atomicAdd(a.acc_cov + 4 * size_t(id) + 1, s[7]);
-      atomicAdd(a.acc_cov + 4 * size_t(id) + 3, s[8]);
-    } else {
-      atomicAdd(a.acc_cov + 4 * size_t(id), s[6]);
-      atomicAdd(a.acc_cov + 4 * size_t(id) + 1, s[7]);
-      atomicAdd(a.acc_cov + 4 * size_t(id) + 2, s[8]);
-    }
-    atomicAdd(a.dL_dopacity + id, s[9]);
-  }
+  for (int k = 0; k < 16; ++k) v[k] = k < kValues ? c[k] : 0.0f;
+  float w8[8], w4[4], w2[2];
+  bool b = lane & 16;
+#pragma unroll
+  for (int k = 0; k < 8; ++k) w8[k] = (b ? v[k + 8] : v[k]) + __shfl_xor_sync(full, b ? v[k] : v[k + 8], 16);
+  b = lane & 8;
+#pragma unroll
+  for (int k = 0; k < 4; ++k) w4[k] = (b ? w8[k + 4] : w8[k]) + __shfl_xor_sync(full, b ? w8[k] : w8[k + 4], 8);
+  b = lane & 4;
+#pragma unroll
+  for (int k = 0; k < 2; ++k) w2[k] = (b ? w4[k + 2] : w4[k]) + __shfl_xor_sync(full, b ? w4[k] : w4[k + 2], 4);
+  b = lane & 2;
+  float w1 = (b ? w2[1] : w2[0]) + __shfl_xor_sync(full, b ? w2[0] : w2[1], 2);
+  w1 += __shfl_xor_sync(full, w1, 1);
+  if (t.active) atomicAdd(t.base + size_t(t.mult) * id + t.off, w1);
 }
 
 // Reference formulas (backward.cu:552-663)
@@ -86,6 +100,7 @@ __global__ void __launch_bounds__(kBlendThreads) render_ref_kernel(BackwardArgs 
   const float ddelx_dx = 0.5f * float(a.W), ddely_dy = 0.5f * float(a.H);
   const float pxf = float(px), pyf = float(py);
   const float4* rec = reinterpret_cast<const float4*>(a.bwd_record);
+  const Target tgt = lane_target(a, 0);
 
   for (int hi = int(nmax); hi > 0; hi -= kBatch) {
     const int cnt = min(kBatch, hi);
@@ -106,15 +121,15 @@ __global__ void __launch_bounds__(kBlendThreads) render_ref_kernel(BackwardArgs 
       bool contrib = false;
       if (inside && idx < last) {
         // q0 = (mx, my, conic a, conic b), q1 = (conic c, opacity, depth, r), q2 = (g, b, _, _)
-        const float4 q0 = s_rec[3 * j], q1 = s_rec[3 * j + 1];
+        const float4 q0 = s_rec[3 * j], q1 = s_rec[3 * j + 1], q2 = s_rec[3 * j + 2];
         const float dx = q0.x - pxf, dy = q0.y - pyf;
         const float power = -0.5f * (q0.z * dx * dx + q1.x * dy * dy) - q0.w * dx * dy;
-        if (power <= 0.0f) {
+        // q2.z: below it, alpha < 1/255 for certain (BackwardRecord::skip)
+        if (power <= 0.0f && power >= q2.z) {
           const float G = expf(power);
           const float alpha = fminf(0.99f, q1.y * G);
           if (alpha >= 1.0f / 255.0f) {
             contrib = true;
-            const float4 q2 = s_rec[3 * j + 2];
             T = T / (1.f - alpha);
             const float dchdc = alpha * T;
             float dL_dopa = 0.0f;
@@ -153,7 +168,7 @@ __global__ void __launch_bounds__(kBlendThreads) render_ref_kernel(BackwardArgs 
           }
         }
       }
-      flush(c, contrib, s_id[j], 0, a);
+      flush(c, contrib, s_id[j], tgt);
     }
   }
 }
@@ -173,7 +188,7 @@ __device__ __forceinline__ float gauss_eval_fwd(float px, float py, float mx, fl
 
 // Exact derivative of the forward blend.
 __global__ void __launch_bounds__(kBlendThreads) render_exact_kernel(BackwardArgs a) {
-  __shared__ float4 s_rec[kBatch * 3];
+  __shared__ float4 s_rec[kBatch * 4];
   __shared__ uint32_t s_id[kBatch];
   const int gw = (a.W + kTile - 1) / kTile;
   const int tile = blockIdx.y * gw + blockIdx.x;
@@ -199,15 +214,17 @@ __global__ void __launch_bounds__(kBlendThreads) render_exact_kernel(BackwardArg
   const float hW = 0.5f * float(a.W), hH = 0.5f * float(a.H);
   const float pxf = float(px), pyf = float(py);
   const float4* rec = reinterpret_cast<const float4*>(a.record);
+  const Target tgt = lane_target(a, 1);
   for (int hi = int(nmax); hi > 0; hi -= kBatch) {
     const int cnt = min(kBatch, hi);
     __syncthreads();
     if (int(threadIdx.x) < cnt) {
       const uint32_t id = a.point_list[range.x + hi - 1 - threadIdx.x];
       s_id[threadIdx.x] = id;
-      s_rec[3 * threadIdx.x] = __ldg(rec + 3 * size_t(id));
-      s_rec[3 * threadIdx.x + 1] = __ldg(rec + 3 * size_t(id) + 1);
-      s_rec[3 * threadIdx.x + 2] = __ldg(rec + 3 * size_t(id) + 2);
+      s_rec[4 * threadIdx.x] = __ldg(rec + 4 * size_t(id));
+      s_rec[4 * threadIdx.x + 1] = __ldg(rec + 4 * size_t(id) + 1);
+      s_rec[4 * threadIdx.x + 2] = __ldg(rec + 4 * size_t(id) + 2);
+      s_rec[4 * threadIdx.x + 3] = __ldg(rec + 4 * size_t(id) + 3);
     }
     __syncthreads();
     for (int j = 0; j < cnt; ++j) {
@@ -217,15 +234,18 @@ __global__ void __launch_bounds__(kBlendThreads) render_exact_kernel(BackwardArg
       for (int k = 0; k < kValues; ++k) c[k] = 0.f;
       bool contrib = false;
       if (inside && idx < last) {
-        // q0 = (mx, my, cxx, cxy), q1 = (cyy, det, opacity, depth), q2 = (r, g, b, _)
-        const float4 q0 = s_rec[3 * j], q1 = s_rec[3 * j + 1];
-        float mahal;
-        const float g = gauss_eval_fwd(pxf, pyf, q0.x, q0.y, q0.z, q0.w, q1.x, q1.y, &mahal);
+        // q0 = (mx, my, cxx, cxy), q1 = (cyy, det, opacity, depth), q2 = (r, g, b, reject), q3 = conic
+        const float4 q0 = s_rec[4 * j], q1 = s_rec[4 * j + 1];
+        const float4 q2 = s_rec[4 * j + 2], q3 = s_rec[4 * j + 3];
+        const float ex = sub(pxf, q0.x), ey = sub(pyf, q0.y);
+        const float ax = q3.x * ex * ex, cyv = q3.z * ey * ey, bxy = 2.0f * q3.y * ex * ey;
+        const bool rejected = (ax + cyv + bxy) - 1e-4f * (ax + cyv + fabsf(bxy)) > q2.w;
+        float mahal = 0.0f;
+        const float g = rejected ? 0.0f : gauss_eval_fwd(pxf, pyf, q0.x, q0.y, q0.z, q0.w, q1.x, q1.y, &mahal);
         const float og = mul(q1.z, g);
         const float a_ = fminf(0.99f, og);
-        if (a_ >= 1.0f / 255.0f) {
+        if (!rejected && a_ >= 1.0f / 255.0f) {
           contrib = true;
-          const float4 q2 = s_rec[3 * j + 2];
           const float ia = 1.0f / (1.0f - a_);
           T = T * ia;  // transmittance in front of this entry
           const float aT = a_ * T;
@@ -258,7 +278,7 @@ __global__ void __launch_bounds__(kBlendThreads) render_exact_kernel(BackwardArg
           }
         }
       }
-      flush(c, contrib, s_id[j], 1, a);
+      flush(c, contrib, s_id[j], tgt);
     }
   }
 }

@@ -2,11 +2,13 @@
 // pixelGaussiansDev.cuh:5-96, gaussEval.h:7-29).
 //
 // One CTA per 16x16 tile, one thread per pixel.  The tile's sorted list is
-// staged 256 Gaussians at a time into shared memory (48-byte records,
+// staged 256 Gaussians at a time into shared memory (64-byte records,
 // gathered by id), double-buffered: the next batch's records are loaded into
 // registers while the current batch is blended and stored to the other buffer
 // afterwards.  The CTA stops as soon as every pixel of the tile has
-// terminated (the reference keeps loading every batch of the tile).
+// terminated (the reference keeps loading every batch of the tile).  Pairs
+// that certainly fall below the alpha threshold are rejected with a
+// quadratic-form test before the exact evaluation (BlendRecord::reject).
 //
 // Per pixel the arithmetic is the reference's, in its operation order: the
 // Gaussian is evaluated from the 2-D covariance and its determinant
@@ -32,8 +34,16 @@ __device__ __forceinline__ float gauss_eval(float px, float py, float mx, float 
   return expf(mul(-0.5f, m));
 }
 
+// True when the pair certainly has alpha < 1/255 (see BlendRecord::reject).
+__device__ __forceinline__ bool early_reject(float dx, float dy, float4 q3, float reject) {
+  const float ax = q3.x * dx * dx, cy = q3.z * dy * dy, bxy = 2.0f * q3.y * dx * dy;
+  const float qf = ax + cy + bxy;
+  const float mag = ax + cy + fabsf(bxy);
+  return qf - 1e-4f * mag > reject;
+}
+
 __global__ void __launch_bounds__(kBlendThreads) blend_kernel(BlendArgs a) {
-  __shared__ float4 s_rec[2][kBatch * 3];
+  __shared__ float4 s_rec[2][kBatch * 4];
   const int gw = (a.W + kTile - 1) / kTile;
   const int tile = blockIdx.y * gw + blockIdx.x;
   const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
@@ -49,16 +59,18 @@ __global__ void __launch_bounds__(kBlendThreads) blend_kernel(BlendArgs a) {
   bool done = !inside;
 
   const int nb = (n + kBatch - 1) / kBatch;
-  float4 r0, r1, r2;
+  float4 r0, r1, r2, r3;
   // first batch
   if (nb > 0 && int(threadIdx.x) < min(kBatch, n)) {
     const uint32_t id = a.point_list[range.x + threadIdx.x];
-    r0 = __ldg(rec + 3 * size_t(id));
-    r1 = __ldg(rec + 3 * size_t(id) + 1);
-    r2 = __ldg(rec + 3 * size_t(id) + 2);
-    s_rec[0][3 * threadIdx.x] = r0;
-    s_rec[0][3 * threadIdx.x + 1] = r1;
-    s_rec[0][3 * threadIdx.x + 2] = r2;
+    r0 = __ldg(rec + 4 * size_t(id));
+    r1 = __ldg(rec + 4 * size_t(id) + 1);
+    r2 = __ldg(rec + 4 * size_t(id) + 2);
+    r3 = __ldg(rec + 4 * size_t(id) + 3);
+    s_rec[0][4 * threadIdx.x] = r0;
+    s_rec[0][4 * threadIdx.x + 1] = r1;
+    s_rec[0][4 * threadIdx.x + 2] = r2;
+    s_rec[0][4 * threadIdx.x + 3] = r3;
   }
   const float min_alpha = 1.0f / 255.0f;
   for (int b = 0; b < nb; ++b) {
@@ -69,23 +81,26 @@ __global__ void __launch_bounds__(kBlendThreads) blend_kernel(BlendArgs a) {
     const bool has_next = (b + 1 < nb) && (next_base + int(threadIdx.x) < n);
     if (has_next) {
       const uint32_t id = a.point_list[range.x + next_base + threadIdx.x];
-      r0 = __ldg(rec + 3 * size_t(id));
-      r1 = __ldg(rec + 3 * size_t(id) + 1);
-      r2 = __ldg(rec + 3 * size_t(id) + 2);
+      r0 = __ldg(rec + 4 * size_t(id));
+      r1 = __ldg(rec + 4 * size_t(id) + 1);
+      r2 = __ldg(rec + 4 * size_t(id) + 2);
+      r3 = __ldg(rec + 4 * size_t(id) + 3);
     }
     const int cnt = min(kBatch, n - b * kBatch);
     if (!done) {
       const float4* s = s_rec[cur];
       for (int j = 0; j < cnt; ++j) {
         ++contributor;
-        const float4 q0 = s[3 * j], q1 = s[3 * j + 1];
-        // q0 = (mx, my, cxx, cxy), q1 = (cyy, det, opacity, depth)
+        const float4 q0 = s[4 * j];
+        // q0 = (mx, my, cxx, cxy), q1 = (cyy, det, opacity, depth), q2 = (r, g, b, reject), q3 = conic
+        if (early_reject(sub(pxf, q0.x), sub(pyf, q0.y), s[4 * j + 3], s[4 * j + 2].w)) continue;
+        const float4 q1 = s[4 * j + 1];
         const float g = gauss_eval(pxf, pyf, q0.x, q0.y, q0.z, q0.w, q1.x, q1.y);
         const float a_ = fminf(0.99f, mul(q1.z, g));
         if (a_ >= min_alpha) {
           const float nT = mul(T, sub(1.0f, a_));
           if (nT >= 0.0001f) {
-            const float4 q2 = s[3 * j + 2];
+            const float4 q2 = s[4 * j + 2];
             const float aT = mul(a_, T);
             C0 = fma(q2.x, aT, C0);
             C1 = fma(q2.y, aT, C1);
@@ -103,9 +118,10 @@ __global__ void __launch_bounds__(kBlendThreads) blend_kernel(BlendArgs a) {
     }
     if (has_next) {
       float4* s = s_rec[cur ^ 1];
-      s[3 * threadIdx.x] = r0;
-      s[3 * threadIdx.x + 1] = r1;
-      s[3 * threadIdx.x + 2] = r2;
+      s[4 * threadIdx.x] = r0;
+      s[4 * threadIdx.x + 1] = r1;
+      s[4 * threadIdx.x + 2] = r2;
+      s[4 * threadIdx.x + 3] = r3;
     }
   }
   if (inside) {

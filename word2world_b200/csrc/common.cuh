@@ -77,7 +77,13 @@ __device__ __forceinline__ float m4row(const float* m, int r, float x, float y, 
 }
 
 // ---------------------------------------------------------------------------
-// Per-Gaussian blend record: everything the per-pixel loops need, 48 bytes.
+// Per-Gaussian blend record: everything the per-pixel loops need, 64 bytes.
+// reject: a pixel whose conic quadratic form q satisfies
+// q - 1e-4 * |q terms| > reject cannot reach alpha >= 1/255 (reject =
+// 2 ln(255 o) + 1e-4; +inf when the covariance is not positive definite),
+// so the exact evaluation (IEEE divide + exp) is skipped for it.  The margin
+// is about 100x the rounding difference between q and the exact
+// mahalanobis / det, so the skip never changes a decision.
 // ---------------------------------------------------------------------------
 struct __align__(16) BlendRecord {
   float mx, my;          // screen position (pixels)
@@ -86,18 +92,22 @@ struct __align__(16) BlendRecord {
   float opacity;
   float depth;           // NDC z
   float r, g, b;         // colour (unclamped)
+  float reject;          // early-reject threshold on the quadratic form
+  float ca, cb, cc;      // inverse covariance (conic), for the early reject
   float pad;
 };
-static_assert(sizeof(BlendRecord) == 48, "BlendRecord layout");
+static_assert(sizeof(BlendRecord) == 64, "BlendRecord layout");
 
 // Per-Gaussian record read by the reference-formula backward pass, 48 bytes.
+// skip: -ln(255 o) - 1e-4; a pair whose exponent is below it has
+// alpha < 1/255 for certain, so its exp is not evaluated.
 struct __align__(16) BackwardRecord {
   float mx, my;
   float conic_a, conic_b, conic_c;  // inverse 2-D covariance
   float opacity;
   float depth;
   float r, g, b;
-  float pad0, pad1;
+  float skip, pad1;
 };
 static_assert(sizeof(BackwardRecord) == 48, "BackwardRecord layout");
 

@@ -120,7 +120,7 @@ offsets_kernel(uint32_t* hist, int passes, const uint32_t* tile_hist, int num_ti
 }
 
 template <typename K>
-__global__ void __launch_bounds__(kSortThreads)
+__global__ void __launch_bounds__(kSortThreads, sizeof(K) == 4 ? 3 : 2)
 onesweep_kernel(const K* __restrict__ kin, const uint32_t* __restrict__ vin, K* __restrict__ kout,
                 uint32_t* __restrict__ vout, long long n, int shift, const uint32_t* __restrict__ digit_base,
                 uint32_t* status, uint32_t* counter, uint32_t* err) {
