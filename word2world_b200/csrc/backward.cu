@@ -19,6 +19,7 @@
 // forward's own Gaussian evaluation and the forward's final transmittance.
 #include "common.cuh"
 #include "kernels.h"
+#include "tile_walk.cuh"
 
 namespace w2w {
 namespace {
@@ -71,105 +72,146 @@ __device__ __forceinline__ void flush(const float (&c)[kValues], bool any_contri
   if (t.active) atomicAdd(t.base + size_t(t.mult) * id + t.off, w1);
 }
 
-// Reference formulas (backward.cu:552-663)
-__global__ void __launch_bounds__(kBlendThreads) render_ref_kernel(BackwardArgs a) {
-  __shared__ float4 s_rec[kBatch * 3];
-  __shared__ uint32_t s_id[kBatch];
-  const int gw = (a.W + kTile - 1) / kTile;
-  const int tile = blockIdx.y * gw + blockIdx.x;
-  const int px = blockIdx.x * kTile + (threadIdx.x & 15), py = blockIdx.y * kTile + (threadIdx.x >> 4);
-  const bool inside = px < a.W && py < a.H;
-  const uint2 range = a.ranges[tile];
-  const uint32_t nmax = min(a.tile_max[tile], range.y - range.x);
-  const size_t pix = inside ? size_t(py) * a.W + px : 0;
-  const size_t hw = size_t(a.W) * a.H;
-  const float T_final = inside ? 1.0f - a.out_alpha[pix] : 0.0f;
-  float T = T_final;
-  const uint32_t last = inside ? a.n_contrib[pix] : 0u;
+// Pixel-loop prologue shared by both modes: this thread's pixel, its
+// upstream gradients and contributor count, the tile's walk length.
+struct BwdPixel {
+  TilePixel tp;
+  bool inside;
+  size_t pix, hw;
+  uint2 range;
+  int nmax;
+  uint32_t last, warp_last;
   float dLp0 = 0.f, dLp1 = 0.f, dLp2 = 0.f, dLd = 0.f, dLa = 0.f;
-  if (inside) {
-    dLp0 = a.dL_dcolor[pix];
-    dLp1 = a.dL_dcolor[hw + pix];
-    dLp2 = a.dL_dcolor[2 * hw + pix];
-    dLd = a.dL_ddepth[pix];
-    dLa = a.dL_dalpha[pix];
+  __device__ __forceinline__ explicit BwdPixel(const BackwardArgs& a) {
+    const int gw = (a.W + kTile - 1) / kTile;
+    const int tile = blockIdx.y * gw + blockIdx.x;
+    inside = tp.px < a.W && tp.py < a.H;
+    range = a.ranges[tile];
+    nmax = int(min(a.tile_max[tile], range.y - range.x));
+    pix = inside ? size_t(tp.py) * a.W + tp.px : 0;
+    hw = size_t(a.W) * a.H;
+    last = inside ? a.n_contrib[pix] : 0u;
+    warp_last = __reduce_max_sync(0xffffffffu, last);
+    if (inside) {
+      dLp0 = a.dL_dcolor[pix];
+      dLp1 = a.dL_dcolor[hw + pix];
+      dLp2 = a.dL_dcolor[2 * hw + pix];
+      dLd = a.dL_ddepth[pix];
+      dLa = a.dL_dalpha[pix];
+    }
   }
-  const float bg_dot = a.bg[0] * dLp0 + a.bg[1] * dLp1 + a.bg[2] * dLp2;
+};
+
+// Reference formulas (backward.cu:552-663), per pixel, for one entry:
+// q0 = (mx, my, conic a, conic b), q1 = (conic c, opacity, depth, r), q2 = (g, b, skip, _).
+struct RefChain {
+  float T, T_final, bg_dot;
   float acc0 = 0.f, acc1 = 0.f, acc2 = 0.f, acc_d = 0.f, acc_a = 0.f;
   float last_alpha = 0.f, lc0 = 0.f, lc1 = 0.f, lc2 = 0.f, last_depth = 0.f;
-  const float ddelx_dx = 0.5f * float(a.W), ddely_dy = 0.5f * float(a.H);
-  const float pxf = float(px), pyf = float(py);
-  const float4* rec = reinterpret_cast<const float4*>(a.bwd_record);
-  const Target tgt = lane_target(a, 0);
 
-  for (int hi = int(nmax); hi > 0; hi -= kBatch) {
-    const int cnt = min(kBatch, hi);
+  __device__ __forceinline__ void step(const BwdPixel& p, float4 q0, float4 q1, float4 q2, float dx, float dy,
+                                       float G, float alpha, float ddelx_dx, float ddely_dy, float (&c)[kValues]) {
+    T = T / (1.f - alpha);
+    const float dchdc = alpha * T;
+    float dL_dopa = 0.0f;
+    acc0 = last_alpha * lc0 + (1.f - last_alpha) * acc0;
+    lc0 = q1.w;
+    dL_dopa += (q1.w - acc0) * p.dLp0;
+    c[0] = dchdc * p.dLp0;
+    acc1 = last_alpha * lc1 + (1.f - last_alpha) * acc1;
+    lc1 = q2.x;
+    dL_dopa += (q2.x - acc1) * p.dLp1;
+    c[1] = dchdc * p.dLp1;
+    acc2 = last_alpha * lc2 + (1.f - last_alpha) * acc2;
+    lc2 = q2.y;
+    dL_dopa += (q2.y - acc2) * p.dLp2;
+    c[2] = dchdc * p.dLp2;
+    const float c_d = q1.z;
+    acc_d = last_alpha * last_depth + (1.f - last_alpha) * acc_d;
+    last_depth = c_d;
+    dL_dopa += (c_d - acc_d) * p.dLd;
+    c[3] = dchdc * p.dLd;
+    acc_a = last_alpha + (1.f - last_alpha) * acc_a;
+    dL_dopa += (1 - acc_a) * p.dLa;
+    dL_dopa *= T;
+    last_alpha = alpha;
+    dL_dopa += (-T_final / (1.f - alpha)) * bg_dot;
+    const float dL_dG = q1.y * dL_dopa;
+    const float gdx = G * dx, gdy = G * dy;
+    const float dG_ddelx = -gdx * q0.z - gdy * q0.w;
+    const float dG_ddely = -gdy * q1.x - gdx * q0.w;
+    c[4] = dL_dG * dG_ddelx * ddelx_dx;
+    c[5] = dL_dG * dG_ddely * ddely_dy;
+    c[6] = -0.5f * gdx * dx * dL_dG;
+    c[7] = -0.5f * gdx * dy * dL_dG;
+    c[8] = -0.5f * gdy * dy * dL_dG;
+    c[9] = G * dL_dopa;
+  }
+};
+
+// The reference's pair test and Gaussian value: power from the conic, skipped
+// when positive or (certainly) below alpha 1/255, alpha = min(0.99, o G).
+__device__ __forceinline__ bool ref_eval(float4 q0, float4 q1, float4 q2, float pxf, float pyf, float& dx, float& dy,
+                                         float& G, float& alpha) {
+  dx = q0.x - pxf;
+  dy = q0.y - pyf;
+  const float power = -0.5f * (q0.z * dx * dx + q1.x * dy * dy) - q0.w * dx * dy;
+  G = expf(power);
+  alpha = fminf(0.99f, q1.y * G);
+  return power <= 0.0f && power >= q2.z && alpha >= 1.0f / 255.0f;
+}
+
+__global__ void __launch_bounds__(kBlendThreads, 2) render_ref_kernel(BackwardArgs a) {
+  __shared__ TileWalkShared sm;
+  const BwdPixel p(a);
+  RefChain ch;
+  ch.T_final = p.inside ? 1.0f - a.out_alpha[p.pix] : 0.0f;
+  ch.T = ch.T_final;
+  ch.bg_dot = a.bg[0] * p.dLp0 + a.bg[1] * p.dLp1 + a.bg[2] * p.dLp2;
+  const float ddelx_dx = 0.5f * float(a.W), ddely_dy = 0.5f * float(a.H);
+  const float pxf = float(p.tp.px), pyf = float(p.tp.py);
+  const Target tgt = lane_target(a, 0);
+  const int nb = (p.nmax + kBatch - 1) / kBatch;
+  Staged st;
+  // batch b holds list positions hi-1, hi-2, ..., hi-cnt (hi = nmax - b*kBatch)
+  if (nb > 0) {
+    stage_load(st, a.bwd_record, a.point_list, p.range.x + p.nmax - 1 - threadIdx.x, int(threadIdx.x) < p.nmax);
+    stage_store(sm, 0, st, p.tp.X0, p.tp.Y0);
+  }
+  for (int b = 0; b < nb; ++b) {
+    const int cur = b & 1;
+    const int hi = p.nmax - b * kBatch;
     __syncthreads();
-    if (int(threadIdx.x) < cnt) {
-      const uint32_t id = a.point_list[range.x + hi - 1 - threadIdx.x];
-      s_id[threadIdx.x] = id;
-      s_rec[3 * threadIdx.x] = __ldg(rec + 3 * size_t(id));
-      s_rec[3 * threadIdx.x + 1] = __ldg(rec + 3 * size_t(id) + 1);
-      s_rec[3 * threadIdx.x + 2] = __ldg(rec + 3 * size_t(id) + 2);
-    }
-    __syncthreads();
-    for (int j = 0; j < cnt; ++j) {
-      const uint32_t idx = uint32_t(hi - 1 - j);  // position in the tile's list
-      float c[kValues];
+    const int hn = hi - kBatch;
+    if (b + 1 < nb) stage_load(st, a.bwd_record, a.point_list, p.range.x + hn - 1 - threadIdx.x,
+                               int(threadIdx.x) < hn);
+    // entries j < hi - warp_last sit at or past every contributor count of the warp
+    const int start = hi - int(p.warp_last);
+    if (start < kBatch) {
+      const float4* s = sm.rec[cur];
+      const uint32_t* ids = sm.id[cur];
+      ListIter it(sm.bal[cur][p.tp.warp], start > 0 ? start : 0);
+      for (;;) {
+        const int j0 = it.next();
+        if (j0 < 0) break;
+        const int j1r = it.next();
+        const int j1 = j1r < 0 ? j0 : j1r;
+        const float4 a0 = s[kRecVec * j0], a1 = s[kRecVec * j0 + 1], a2 = s[kRecVec * j0 + 2];
+        const float4 b0 = s[kRecVec * j1], b1 = s[kRecVec * j1 + 1], b2 = s[kRecVec * j1 + 2];
+        float dx0, dy0, G0, al0, dx1, dy1, G1, al1;
+        const bool ok0 = ref_eval(a0, a1, a2, pxf, pyf, dx0, dy0, G0, al0) && uint32_t(hi - 1 - j0) < p.last;
+        const bool ok1 = ref_eval(b0, b1, b2, pxf, pyf, dx1, dy1, G1, al1) && j1r >= 0 &&
+                         uint32_t(hi - 1 - j1) < p.last;
+        float c0[kValues], c1[kValues];
 #pragma unroll
-      for (int k = 0; k < kValues; ++k) c[k] = 0.f;
-      bool contrib = false;
-      if (inside && idx < last) {
-        // q0 = (mx, my, conic a, conic b), q1 = (conic c, opacity, depth, r), q2 = (g, b, _, _)
-        const float4 q0 = s_rec[3 * j], q1 = s_rec[3 * j + 1], q2 = s_rec[3 * j + 2];
-        const float dx = q0.x - pxf, dy = q0.y - pyf;
-        const float power = -0.5f * (q0.z * dx * dx + q1.x * dy * dy) - q0.w * dx * dy;
-        // q2.z: below it, alpha < 1/255 for certain (BackwardRecord::skip)
-        if (power <= 0.0f && power >= q2.z) {
-          const float G = expf(power);
-          const float alpha = fminf(0.99f, q1.y * G);
-          if (alpha >= 1.0f / 255.0f) {
-            contrib = true;
-            T = T / (1.f - alpha);
-            const float dchdc = alpha * T;
-            float dL_dopa = 0.0f;
-            acc0 = last_alpha * lc0 + (1.f - last_alpha) * acc0;
-            lc0 = q1.w;
-            dL_dopa += (q1.w - acc0) * dLp0;
-            c[0] = dchdc * dLp0;
-            acc1 = last_alpha * lc1 + (1.f - last_alpha) * acc1;
-            lc1 = q2.x;
-            dL_dopa += (q2.x - acc1) * dLp1;
-            c[1] = dchdc * dLp1;
-            acc2 = last_alpha * lc2 + (1.f - last_alpha) * acc2;
-            lc2 = q2.y;
-            dL_dopa += (q2.y - acc2) * dLp2;
-            c[2] = dchdc * dLp2;
-            const float c_d = q1.z;
-            acc_d = last_alpha * last_depth + (1.f - last_alpha) * acc_d;
-            last_depth = c_d;
-            dL_dopa += (c_d - acc_d) * dLd;
-            c[3] = dchdc * dLd;
-            acc_a = last_alpha + (1.f - last_alpha) * acc_a;
-            dL_dopa += (1 - acc_a) * dLa;
-            dL_dopa *= T;
-            last_alpha = alpha;
-            dL_dopa += (-T_final / (1.f - alpha)) * bg_dot;
-            const float dL_dG = q1.y * dL_dopa;
-            const float gdx = G * dx, gdy = G * dy;
-            const float dG_ddelx = -gdx * q0.z - gdy * q0.w;
-            const float dG_ddely = -gdy * q1.x - gdx * q0.w;
-            c[4] = dL_dG * dG_ddelx * ddelx_dx;
-            c[5] = dL_dG * dG_ddely * ddely_dy;
-            c[6] = -0.5f * gdx * dx * dL_dG;
-            c[7] = -0.5f * gdx * dy * dL_dG;
-            c[8] = -0.5f * gdy * dy * dL_dG;
-            c[9] = G * dL_dopa;
-          }
-        }
+        for (int k = 0; k < kValues; ++k) c0[k] = c1[k] = 0.f;
+        if (ok0) ch.step(p, a0, a1, a2, dx0, dy0, G0, al0, ddelx_dx, ddely_dy, c0);
+        if (ok1) ch.step(p, b0, b1, b2, dx1, dy1, G1, al1, ddelx_dx, ddely_dy, c1);
+        flush(c0, ok0, ids[j0], tgt);
+        flush(c1, ok1, ids[j1], tgt);
       }
-      flush(c, contrib, s_id[j], tgt);
     }
+    if (b + 1 < nb) stage_store(sm, cur ^ 1, st, p.tp.X0, p.tp.Y0);
   }
 }
 
@@ -186,100 +228,101 @@ __device__ __forceinline__ float gauss_eval_fwd(float px, float py, float mx, fl
   return expf(mul(-0.5f, m));
 }
 
-// Exact derivative of the forward blend.
-__global__ void __launch_bounds__(kBlendThreads) render_exact_kernel(BackwardArgs a) {
-  __shared__ float4 s_rec[kBatch * 4];
-  __shared__ uint32_t s_id[kBatch];
-  const int gw = (a.W + kTile - 1) / kTile;
-  const int tile = blockIdx.y * gw + blockIdx.x;
-  const int px = blockIdx.x * kTile + (threadIdx.x & 15), py = blockIdx.y * kTile + (threadIdx.x >> 4);
-  const bool inside = px < a.W && py < a.H;
-  const uint2 range = a.ranges[tile];
-  const uint32_t nmax = min(a.tile_max[tile], range.y - range.x);
-  const size_t pix = inside ? size_t(py) * a.W + px : 0;
-  const size_t hw = size_t(a.W) * a.H;
-  const float Tf = inside ? a.T_final[pix] : 0.0f;
-  float T = Tf;
-  const uint32_t last = inside ? a.n_contrib[pix] : 0u;
-  float dLp0 = 0.f, dLp1 = 0.f, dLp2 = 0.f, dLd = 0.f, dLa = 0.f;
-  if (inside) {
-    dLp0 = a.dL_dcolor[pix];
-    dLp1 = a.dL_dcolor[hw + pix];
-    dLp2 = a.dL_dcolor[2 * hw + pix];
-    dLd = a.dL_ddepth[pix];
-    dLa = a.dL_dalpha[pix];
-  }
-  // suffix sums behind the current entry (colour includes the background)
-  float S0 = Tf * a.bg[0], S1 = Tf * a.bg[1], S2 = Tf * a.bg[2], SD = 0.f, SW = 0.f;
-  const float hW = 0.5f * float(a.W), hH = 0.5f * float(a.H);
-  const float pxf = float(px), pyf = float(py);
-  const float4* rec = reinterpret_cast<const float4*>(a.record);
-  const Target tgt = lane_target(a, 1);
-  for (int hi = int(nmax); hi > 0; hi -= kBatch) {
-    const int cnt = min(kBatch, hi);
-    __syncthreads();
-    if (int(threadIdx.x) < cnt) {
-      const uint32_t id = a.point_list[range.x + hi - 1 - threadIdx.x];
-      s_id[threadIdx.x] = id;
-      s_rec[4 * threadIdx.x] = __ldg(rec + 4 * size_t(id));
-      s_rec[4 * threadIdx.x + 1] = __ldg(rec + 4 * size_t(id) + 1);
-      s_rec[4 * threadIdx.x + 2] = __ldg(rec + 4 * size_t(id) + 2);
-      s_rec[4 * threadIdx.x + 3] = __ldg(rec + 4 * size_t(id) + 3);
-    }
-    __syncthreads();
-    for (int j = 0; j < cnt; ++j) {
-      const uint32_t idx = uint32_t(hi - 1 - j);
-      float c[kValues];
-#pragma unroll
-      for (int k = 0; k < kValues; ++k) c[k] = 0.f;
-      bool contrib = false;
-      if (inside && idx < last) {
-        // q0 = (mx, my, cxx, cxy), q1 = (cyy, det, opacity, depth), q2 = (r, g, b, reject), q3 = conic
-        const float4 q0 = s_rec[4 * j], q1 = s_rec[4 * j + 1];
-        const float4 q2 = s_rec[4 * j + 2], q3 = s_rec[4 * j + 3];
-        const float ex = sub(pxf, q0.x), ey = sub(pyf, q0.y);
-        const float ax = q3.x * ex * ex, cyv = q3.z * ey * ey, bxy = 2.0f * q3.y * ex * ey;
-        const bool rejected = (ax + cyv + bxy) - 1e-4f * (ax + cyv + fabsf(bxy)) > q2.w;
-        float mahal = 0.0f;
-        const float g = rejected ? 0.0f : gauss_eval_fwd(pxf, pyf, q0.x, q0.y, q0.z, q0.w, q1.x, q1.y, &mahal);
-        const float og = mul(q1.z, g);
-        const float a_ = fminf(0.99f, og);
-        if (!rejected && a_ >= 1.0f / 255.0f) {
-          contrib = true;
-          const float ia = 1.0f / (1.0f - a_);
-          T = T * ia;  // transmittance in front of this entry
-          const float aT = a_ * T;
-          float dLda = dLp0 * (q2.x * T - S0 * ia) + dLp1 * (q2.y * T - S1 * ia) + dLp2 * (q2.z * T - S2 * ia);
-          dLda += dLd * (q1.w * T - SD * ia);
-          dLda += dLa * (T - SW * ia);
-          c[0] = aT * dLp0;
-          c[1] = aT * dLp1;
-          c[2] = aT * dLp2;
-          c[3] = aT * dLd;
-          S0 += q2.x * aT;
-          S1 += q2.y * aT;
-          S2 += q2.z * aT;
-          SD += q1.w * aT;
-          SW += aT;
-          if (og < 0.99f) {
-            c[9] = dLda * g;
-            if (mahal >= 0.0f) {
-              const float dLdm = dLda * q1.z * (-0.5f * g);
-              const float cxx = q0.z, cxy = q0.w, cyy = q1.x, det = q1.y;
-              const float dx = pxf - q0.x, dy = pyf - q0.y;
-              const float idet = 1.0f / det;
-              c[4] = -dLdm * (2.f * cyy * dx - 2.f * cxy * dy) * idet * hW;
-              c[5] = -dLdm * (2.f * cxx * dy - 2.f * cxy * dx) * idet * hH;
-              const float num = mahal * det;
-              c[6] = dLdm * (dy * dy * idet - num * cyy * idet * idet);
-              c[7] = dLdm * (-2.f * dx * dy * idet + 2.f * num * cxy * idet * idet);
-              c[8] = dLdm * (dx * dx * idet - num * cxx * idet * idet);
-            }
-          }
-        }
+// Exact derivative of the forward blend, per pixel, for one entry:
+// q0 = (mx, my, cxx, cxy), q1 = (cyy, det, opacity, depth), q2 = (r, g, b, _).
+struct ExactChain {
+  float T;
+  float S0, S1, S2, SD = 0.f, SW = 0.f;  // suffix sums behind the current entry (colour includes the background)
+
+  __device__ __forceinline__ void step(const BwdPixel& p, float4 q0, float4 q1, float4 q2, float pxf, float pyf,
+                                       float g, float og, float a_, float mahal, float hW, float hH,
+                                       float (&c)[kValues]) {
+    const float ia = 1.0f / (1.0f - a_);
+    T = T * ia;  // transmittance in front of this entry
+    const float aT = a_ * T;
+    float dLda = p.dLp0 * (q2.x * T - S0 * ia) + p.dLp1 * (q2.y * T - S1 * ia) + p.dLp2 * (q2.z * T - S2 * ia);
+    dLda += p.dLd * (q1.w * T - SD * ia);
+    dLda += p.dLa * (T - SW * ia);
+    c[0] = aT * p.dLp0;
+    c[1] = aT * p.dLp1;
+    c[2] = aT * p.dLp2;
+    c[3] = aT * p.dLd;
+    S0 += q2.x * aT;
+    S1 += q2.y * aT;
+    S2 += q2.z * aT;
+    SD += q1.w * aT;
+    SW += aT;
+    if (og < 0.99f) {
+      c[9] = dLda * g;
+      if (mahal >= 0.0f) {
+        const float dLdm = dLda * q1.z * (-0.5f * g);
+        const float cxx = q0.z, cxy = q0.w, cyy = q1.x, det = q1.y;
+        const float dx = pxf - q0.x, dy = pyf - q0.y;
+        const float idet = 1.0f / det;
+        c[4] = -dLdm * (2.f * cyy * dx - 2.f * cxy * dy) * idet * hW;
+        c[5] = -dLdm * (2.f * cxx * dy - 2.f * cxy * dx) * idet * hH;
+        const float num = mahal * det;
+        c[6] = dLdm * (dy * dy * idet - num * cyy * idet * idet);
+        c[7] = dLdm * (-2.f * dx * dy * idet + 2.f * num * cxy * idet * idet);
+        c[8] = dLdm * (dx * dx * idet - num * cxx * idet * idet);
       }
-      flush(c, contrib, s_id[j], tgt);
     }
+  }
+};
+
+__global__ void __launch_bounds__(kBlendThreads, 2) render_exact_kernel(BackwardArgs a) {
+  __shared__ TileWalkShared sm;
+  const BwdPixel p(a);
+  ExactChain ch;
+  const float Tf = p.inside ? a.T_final[p.pix] : 0.0f;
+  ch.T = Tf;
+  ch.S0 = Tf * a.bg[0];
+  ch.S1 = Tf * a.bg[1];
+  ch.S2 = Tf * a.bg[2];
+  const float hW = 0.5f * float(a.W), hH = 0.5f * float(a.H);
+  const float pxf = float(p.tp.px), pyf = float(p.tp.py);
+  const Target tgt = lane_target(a, 1);
+  const int nb = (p.nmax + kBatch - 1) / kBatch;
+  Staged st;
+  if (nb > 0) {
+    stage_load(st, a.record, a.point_list, p.range.x + p.nmax - 1 - threadIdx.x, int(threadIdx.x) < p.nmax);
+    stage_store(sm, 0, st, p.tp.X0, p.tp.Y0);
+  }
+  for (int b = 0; b < nb; ++b) {
+    const int cur = b & 1;
+    const int hi = p.nmax - b * kBatch;
+    __syncthreads();
+    const int hn = hi - kBatch;
+    if (b + 1 < nb) stage_load(st, a.record, a.point_list, p.range.x + hn - 1 - threadIdx.x, int(threadIdx.x) < hn);
+    const int start = hi - int(p.warp_last);
+    if (start < kBatch) {
+      const float4* s = sm.rec[cur];
+      const uint32_t* ids = sm.id[cur];
+      ListIter it(sm.bal[cur][p.tp.warp], start > 0 ? start : 0);
+      for (;;) {
+        const int j0 = it.next();
+        if (j0 < 0) break;
+        const int j1r = it.next();
+        const int j1 = j1r < 0 ? j0 : j1r;
+        const float4 a0 = s[kRecVec * j0], a1 = s[kRecVec * j0 + 1];
+        const float4 b0 = s[kRecVec * j1], b1 = s[kRecVec * j1 + 1];
+        float m0, m1;
+        const float g0 = gauss_eval_fwd(pxf, pyf, a0.x, a0.y, a0.z, a0.w, a1.x, a1.y, &m0);
+        const float g1 = gauss_eval_fwd(pxf, pyf, b0.x, b0.y, b0.z, b0.w, b1.x, b1.y, &m1);
+        const float og0 = mul(a1.z, g0), og1 = mul(b1.z, g1);
+        const float al0 = fminf(0.99f, og0), al1 = fminf(0.99f, og1);
+        const bool ok0 = al0 >= 1.0f / 255.0f && uint32_t(hi - 1 - j0) < p.last;
+        const bool ok1 = al1 >= 1.0f / 255.0f && j1r >= 0 && uint32_t(hi - 1 - j1) < p.last;
+        float c0[kValues], c1[kValues];
+#pragma unroll
+        for (int k = 0; k < kValues; ++k) c0[k] = c1[k] = 0.f;
+        if (ok0) ch.step(p, a0, a1, s[kRecVec * j0 + 2], pxf, pyf, g0, og0, al0, m0, hW, hH, c0);
+        if (ok1) ch.step(p, b0, b1, s[kRecVec * j1 + 2], pxf, pyf, g1, og1, al1, m1, hW, hH, c1);
+        flush(c0, ok0, ids[j0], tgt);
+        flush(c1, ok1, ids[j1], tgt);
+      }
+    }
+    if (b + 1 < nb) stage_store(sm, cur ^ 1, st, p.tp.X0, p.tp.Y0);
   }
 }
 

@@ -1,14 +1,12 @@
 // Per-tile front-to-back alpha blending (reference pixelGaussiansFull.cu:3-98,
 // pixelGaussiansDev.cuh:5-96, gaussEval.h:7-29).
 //
-// One CTA per 16x16 tile, one thread per pixel.  The tile's sorted list is
-// staged 256 Gaussians at a time into shared memory (64-byte records,
-// gathered by id), double-buffered: the next batch's records are loaded into
-// registers while the current batch is blended and stored to the other buffer
-// afterwards.  The CTA stops as soon as every pixel of the tile has
-// terminated (the reference keeps loading every batch of the tile).  Pairs
-// that certainly fall below the alpha threshold are rejected with a
-// quadratic-form test before the exact evaluation (BlendRecord::reject).
+// One CTA per 16x16 tile, one thread per pixel, one warp per 8x4 pixel block
+// (tile_walk.cuh).  Each warp walks only the list entries that can reach its
+// block with alpha >= 1/255, two at a time: both entries' Gaussian values are
+// evaluated before the two transmittance/colour updates, so the two
+// evaluations overlap.  The CTA stops as soon as every pixel of the tile has
+// terminated (the reference keeps loading every batch of the tile).
 //
 // Per pixel the arithmetic is the reference's, in its operation order: the
 // Gaussian is evaluated from the 2-D covariance and its determinant
@@ -18,6 +16,7 @@
 // contributor count is the 1-based index of the last blended entry.
 #include "common.cuh"
 #include "kernels.h"
+#include "tile_walk.cuh"
 
 namespace w2w {
 namespace {
@@ -34,111 +33,92 @@ __device__ __forceinline__ float gauss_eval(float px, float py, float mx, float 
   return expf(mul(-0.5f, m));
 }
 
-// True when the pair certainly has alpha < 1/255 (see BlendRecord::reject).
-__device__ __forceinline__ bool early_reject(float dx, float dy, float4 q3, float reject) {
-  const float ax = q3.x * dx * dx, cy = q3.z * dy * dy, bxy = 2.0f * q3.y * dx * dy;
-  const float qf = ax + cy + bxy;
-  const float mag = ax + cy + fabsf(bxy);
-  return qf - 1e-4f * mag > reject;
-}
+struct BlendPixel {
+  float C0 = 0.f, C1 = 0.f, C2 = 0.f, Wt = 0.f, D = 0.f, T = 1.0f;
+  uint32_t last = 0;
+  bool done;
+
+  // Entry with alpha `al` (record words q1, q2), 1-based list position `pos`.
+  __device__ __forceinline__ void step(float al, float4 q1, float4 q2, uint32_t pos) {
+    if (done || !(al >= 1.0f / 255.0f)) return;
+    const float nT = mul(T, sub(1.0f, al));
+    if (nT < 0.0001f) {
+      done = true;
+      return;
+    }
+    const float aT = mul(al, T);
+    C0 = fma(q2.x, aT, C0);
+    C1 = fma(q2.y, aT, C1);
+    C2 = fma(q2.z, aT, C2);
+    Wt = add(Wt, aT);
+    D = s1<fp::BL_DEPTH>(q1.w, aT, D);
+    T = nT;
+    last = pos;
+  }
+};
 
 __global__ void __launch_bounds__(kBlendThreads) blend_kernel(BlendArgs a) {
-  __shared__ float4 s_rec[2][kBatch * 4];
+  __shared__ TileWalkShared sm;
   const int gw = (a.W + kTile - 1) / kTile;
   const int tile = blockIdx.y * gw + blockIdx.x;
-  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
-  const int px = blockIdx.x * kTile + tx, py = blockIdx.y * kTile + ty;
-  const bool inside = px < a.W && py < a.H;
+  const TilePixel tp;
+  const bool inside = tp.px < a.W && tp.py < a.H;
   const uint2 range = a.ranges[tile];
   const int n = int(range.y - range.x);
-  const float pxf = float(px), pyf = float(py);
-  const float4* rec = reinterpret_cast<const float4*>(a.record);
+  const float pxf = float(tp.px), pyf = float(tp.py);
 
-  float C0 = 0.f, C1 = 0.f, C2 = 0.f, Wt = 0.f, D = 0.f, T = 1.0f;
-  uint32_t contributor = 0, last = 0;
-  bool done = !inside;
-
+  BlendPixel pix;
+  pix.done = !inside;
   const int nb = (n + kBatch - 1) / kBatch;
-  float4 r0, r1, r2, r3;
-  // first batch
-  if (nb > 0 && int(threadIdx.x) < min(kBatch, n)) {
-    const uint32_t id = a.point_list[range.x + threadIdx.x];
-    r0 = __ldg(rec + 4 * size_t(id));
-    r1 = __ldg(rec + 4 * size_t(id) + 1);
-    r2 = __ldg(rec + 4 * size_t(id) + 2);
-    r3 = __ldg(rec + 4 * size_t(id) + 3);
-    s_rec[0][4 * threadIdx.x] = r0;
-    s_rec[0][4 * threadIdx.x + 1] = r1;
-    s_rec[0][4 * threadIdx.x + 2] = r2;
-    s_rec[0][4 * threadIdx.x + 3] = r3;
+  Staged st;
+  if (nb > 0) {
+    stage_load(st, a.record, a.point_list, range.x + threadIdx.x, int(threadIdx.x) < n);
+    stage_store(sm, 0, st, tp.X0, tp.Y0);
   }
-  const float min_alpha = 1.0f / 255.0f;
   for (int b = 0; b < nb; ++b) {
     const int cur = b & 1;
-    // barrier: batch b is in shared memory; all pixels finished batch b-1
-    if (__syncthreads_count(done ? 1 : 0) == kBlendThreads) break;
+    // barrier: batch b is staged; every warp has finished batch b-1
+    if (__syncthreads_count(pix.done ? 1 : 0) == kBlendThreads) break;
     const int next_base = (b + 1) * kBatch;
-    const bool has_next = (b + 1 < nb) && (next_base + int(threadIdx.x) < n);
-    if (has_next) {
-      const uint32_t id = a.point_list[range.x + next_base + threadIdx.x];
-      r0 = __ldg(rec + 4 * size_t(id));
-      r1 = __ldg(rec + 4 * size_t(id) + 1);
-      r2 = __ldg(rec + 4 * size_t(id) + 2);
-      r3 = __ldg(rec + 4 * size_t(id) + 3);
-    }
-    const int cnt = min(kBatch, n - b * kBatch);
-    if (!done) {
-      const float4* s = s_rec[cur];
-      for (int j = 0; j < cnt; ++j) {
-        ++contributor;
-        const float4 q0 = s[4 * j];
-        // q0 = (mx, my, cxx, cxy), q1 = (cyy, det, opacity, depth), q2 = (r, g, b, reject), q3 = conic
-        if (early_reject(sub(pxf, q0.x), sub(pyf, q0.y), s[4 * j + 3], s[4 * j + 2].w)) continue;
-        const float4 q1 = s[4 * j + 1];
-        const float g = gauss_eval(pxf, pyf, q0.x, q0.y, q0.z, q0.w, q1.x, q1.y);
-        const float a_ = fminf(0.99f, mul(q1.z, g));
-        if (a_ >= min_alpha) {
-          const float nT = mul(T, sub(1.0f, a_));
-          if (nT >= 0.0001f) {
-            const float4 q2 = s[4 * j + 2];
-            const float aT = mul(a_, T);
-            C0 = fma(q2.x, aT, C0);
-            C1 = fma(q2.y, aT, C1);
-            C2 = fma(q2.z, aT, C2);
-            Wt = add(Wt, aT);
-            D = s1<fp::BL_DEPTH>(q1.w, aT, D);
-            T = nT;
-            last = contributor;
-          } else {
-            done = true;
-            break;
-          }
-        }
+    if (b + 1 < nb) stage_load(st, a.record, a.point_list, range.x + next_base + threadIdx.x,
+                               next_base + int(threadIdx.x) < n);
+    if (!__all_sync(0xffffffffu, pix.done)) {
+      const float4* s = sm.rec[cur];
+      ListIter it(sm.bal[cur][tp.warp]);
+      const uint32_t base = uint32_t(b * kBatch) + 1u;
+      for (;;) {
+        const int j0 = it.next();
+        if (j0 < 0) break;
+        const int j1r = it.next();
+        const int j1 = j1r < 0 ? j0 : j1r;
+        const float4 a0 = s[kRecVec * j0], a1 = s[kRecVec * j0 + 1];
+        const float4 b0 = s[kRecVec * j1], b1 = s[kRecVec * j1 + 1];
+        const float g0 = gauss_eval(pxf, pyf, a0.x, a0.y, a0.z, a0.w, a1.x, a1.y);
+        const float g1 = gauss_eval(pxf, pyf, b0.x, b0.y, b0.z, b0.w, b1.x, b1.y);
+        const float al0 = fminf(0.99f, mul(a1.z, g0));
+        const float al1 = fminf(0.99f, mul(b1.z, g1));
+        pix.step(al0, a1, s[kRecVec * j0 + 2], base + uint32_t(j0));
+        if (j1r >= 0) pix.step(al1, b1, s[kRecVec * j1 + 2], base + uint32_t(j1));
+        if (__all_sync(0xffffffffu, pix.done)) break;
       }
     }
-    if (has_next) {
-      float4* s = s_rec[cur ^ 1];
-      s[4 * threadIdx.x] = r0;
-      s[4 * threadIdx.x + 1] = r1;
-      s[4 * threadIdx.x + 2] = r2;
-      s[4 * threadIdx.x + 3] = r3;
-    }
+    if (b + 1 < nb) stage_store(sm, cur ^ 1, st, tp.X0, tp.Y0);
   }
   if (inside) {
-    const size_t pix = size_t(py) * a.W + px;
+    const size_t p = size_t(tp.py) * a.W + tp.px;
     const size_t hw = size_t(a.W) * a.H;
-    a.n_contrib[pix] = last;
-    a.out_alpha[pix] = Wt;
-    a.out_depth[pix] = D;
-    a.T_final[pix] = T;
-    a.out_color[pix] = fma(T, a.bg[0], C0);
-    a.out_color[hw + pix] = fma(T, a.bg[1], C1);
-    a.out_color[2 * hw + pix] = fma(T, a.bg[2], C2);
+    a.n_contrib[p] = pix.last;
+    a.out_alpha[p] = pix.Wt;
+    a.out_depth[p] = pix.D;
+    a.T_final[p] = pix.T;
+    a.out_color[p] = fma(pix.T, a.bg[0], pix.C0);
+    a.out_color[hw + p] = fma(pix.T, a.bg[1], pix.C1);
+    a.out_color[2 * hw + p] = fma(pix.T, a.bg[2], pix.C2);
   }
   // largest contributor count in the tile (the backward starts there)
   __shared__ uint32_t s_max[kBlendThreads / 32];
-  const uint32_t wm = __reduce_max_sync(0xffffffffu, last);
-  if ((threadIdx.x & 31) == 0) s_max[threadIdx.x >> 5] = wm;
+  const uint32_t wm = __reduce_max_sync(0xffffffffu, pix.last);
+  if (tp.lane == 0) s_max[tp.warp] = wm;
   __syncthreads();
   if (threadIdx.x == 0) {
     uint32_t m = 0;

@@ -77,13 +77,98 @@ __device__ __forceinline__ float m4row(const float* m, int r, float x, float y, 
 }
 
 // ---------------------------------------------------------------------------
-// Per-Gaussian blend record: everything the per-pixel loops need, 64 bytes.
-// reject: a pixel whose conic quadratic form q satisfies
-// q - 1e-4 * |q terms| > reject cannot reach alpha >= 1/255 (reject =
-// 2 ln(255 o) + 1e-4; +inf when the covariance is not positive definite),
-// so the exact evaluation (IEEE divide + exp) is skipped for it.  The margin
-// is about 100x the rounding difference between q and the exact
-// mahalanobis / det, so the skip never changes a decision.
+// Block culling.  The per-pixel loops run one warp per 8x4 pixel block of a
+// 16x16 tile (block b: columns 8*(b & 1) .. +7, rows 4*(b >> 1) .. +3).  For
+// every staged list entry the loader computes which of the tile's 8 blocks
+// the Gaussian can reach with alpha >= 1/255, and each warp walks only the
+// entries whose bit for its block is set.  A skipped entry is one every pixel
+// of the block skips anyway, so no decision changes.
+//
+// The test is exact for the ellipse E = {d : d^T Q d <= t'} against the
+// block's continuous pixel-centre rectangle grown by kCullPad: per band of 4
+// rows, E's x-extent over the band is [L, R] with
+//   R = max over v in band of (-beta v + sqrt(gamma - eps v^2)),
+//   L = min over v in band of (-beta v - sqrt(gamma - eps v^2)),
+// (beta = B/A, gamma = t'/A, eps = det/A^2 for Q = [[A, B], [B, C]]); R is
+// concave in v with its maximum at vr = -B hx / C, L convex with its minimum at
+// -vr, so each is one evaluation at the clamped extremum.
+//
+// Conservativeness.  A pixel reaches alpha >= 1/255 only if q = d^T Q d <=
+// t = 2 ln(255 o) + 2e-4 (the blend's own threshold is 1e-4 tighter; exp and
+// log rounding is far inside 1e-4).  The per-pixel evaluations round q (or the
+// mahalanobis distance / det) with a relative error of a few ulps of
+// mag = A dx^2 + 2|B dx dy| + C dy^2 <= k q, k = (sqrt(AC) + |B|)^2 / det.
+// The culling threshold t' = t (1 + 4e-4 k) + 1e-4 exceeds that by more than
+// 100x for k < 1024; beyond that (or with a non-positive-definite Q) nothing
+// is culled.  kCullPad = 1/16 pixel covers the rounding of the pixel offsets
+// and of L, R (below 1e-2 pixel for extents under 8192 pixels; larger
+// ellipses are not culled).
+// ---------------------------------------------------------------------------
+constexpr int kBlockW = 8, kBlockH = 4;  // pixel block per warp
+constexpr float kCullPad = 0.0625f;
+
+struct CullParams {
+  float hy;    // y half-extent of E; +inf: cull nothing, -1: cull everything
+  float beta, gamma, eps, vr;
+};
+
+// Ellipse parameters from the conic (A, B, C) and opacity.
+__device__ __forceinline__ CullParams make_cull_params(float A, float B, float C, float opacity) {
+  CullParams p{__int_as_float(0x7f800000), 0.f, 0.f, 0.f, 0.f};
+  if (!(opacity > 0.0f)) { p.hy = -1.0f; return p; }
+  const float t = 2.0f * logf(255.0f * opacity) + 2e-4f;
+  if (t < 0.0f) { p.hy = -1.0f; return p; }  // opacity < 1/255: alpha never reaches 1/255
+  if (!(A > 0.0f && C > 0.0f) || !(t < 1e30f)) return p;
+  const float det = A * C - B * B;
+  if (!(det > 0.0f)) return p;
+  const float sac = sqrtf(A * C) + fabsf(B);
+  const float k = sac * sac / det;
+  if (!(k < 1024.0f)) return p;
+  const float tt = t * (1.0f + 4e-4f * k) + 1e-4f;
+  const float hx = sqrtf(tt * C / det), hy = sqrtf(tt * A / det);
+  if (!(hx < 8192.0f && hy < 8192.0f)) return p;
+  p.hy = hy;
+  p.beta = B / A;
+  p.gamma = tt / A;
+  p.eps = det / (A * A);
+  p.vr = -B * hx / C;
+  return p;
+}
+
+__device__ __forceinline__ float sqrt_approx(float x) {
+  float y;
+  asm("sqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+
+// Bit b set: the Gaussian may reach alpha >= 1/255 in 8x4 block b of the tile
+// whose top-left pixel is (X0, Y0).  hy/beta/gamma/eps/vr as in CullParams.
+__device__ __forceinline__ uint32_t block_mask(float mx, float my, float hy, float beta, float gamma, float eps,
+                                               float vr, int X0, int Y0) {
+  if (!(hy >= 0.0f && hy < 1e30f)) return hy < 0.0f ? 0u : 0xffu;
+  const float ux = float(X0) - mx, vy = float(Y0) - my;
+  const float ulo0 = ux - kCullPad, uhi0 = ux + (7.0f + kCullPad);
+  const float ulo1 = ux + (8.0f - kCullPad), uhi1 = ux + (15.0f + kCullPad);
+  uint32_t m = 0;
+#pragma unroll
+  for (int by = 0; by < 4; ++by) {
+    const float v0 = vy + (float(4 * by) - kCullPad), v1 = vy + (float(4 * by + 3) + kCullPad);
+    const float a = fmaxf(v0, -hy), b = fminf(v1, hy);
+    const float vR = fminf(fmaxf(vr, a), b), vL = fminf(fmaxf(-vr, a), b);
+    const float R = sqrt_approx(fmaxf(0.0f, gamma - eps * vR * vR)) - beta * vR;
+    const float L = -sqrt_approx(fmaxf(0.0f, gamma - eps * vL * vL)) - beta * vL;
+    const bool band = a <= b;
+    const uint32_t c0 = (band && L <= uhi0 && R >= ulo0) ? 1u : 0u;
+    const uint32_t c1 = (band && L <= uhi1 && R >= ulo1) ? 2u : 0u;
+    m |= (c0 | c1) << (2 * by);
+  }
+  return m;
+}
+
+// ---------------------------------------------------------------------------
+// Per-Gaussian blend record (forward blend and exact backward), 64 bytes.
+// The first 48 bytes are what the per-pixel loops read from shared memory;
+// the last 20 are the block-culling parameters.
 // ---------------------------------------------------------------------------
 struct __align__(16) BlendRecord {
   float mx, my;          // screen position (pixels)
@@ -92,13 +177,11 @@ struct __align__(16) BlendRecord {
   float opacity;
   float depth;           // NDC z
   float r, g, b;         // colour (unclamped)
-  float reject;          // early-reject threshold on the quadratic form
-  float ca, cb, cc;      // inverse covariance (conic), for the early reject
-  float pad;
+  float hy, beta, gamma, eps, vr;  // CullParams
 };
 static_assert(sizeof(BlendRecord) == 64, "BlendRecord layout");
 
-// Per-Gaussian record read by the reference-formula backward pass, 48 bytes.
+// Per-Gaussian record read by the reference-formula backward pass, 64 bytes.
 // skip: -ln(255 o) - 1e-4; a pair whose exponent is below it has
 // alpha < 1/255 for certain, so its exp is not evaluated.
 struct __align__(16) BackwardRecord {
@@ -107,9 +190,10 @@ struct __align__(16) BackwardRecord {
   float opacity;
   float depth;
   float r, g, b;
-  float skip, pad1;
+  float skip;
+  float hy, beta, gamma, eps, vr;  // CullParams
 };
-static_assert(sizeof(BackwardRecord) == 48, "BackwardRecord layout");
+static_assert(sizeof(BackwardRecord) == 64, "BackwardRecord layout");
 
 // ---------------------------------------------------------------------------
 // State layouts.  All arrays start on 256-byte boundaries.

@@ -329,27 +329,28 @@ preprocess_kernel(PreprocessArgs a) {
     a.radii[i] = radius;
     a.tiles[i] = alloc;
     reinterpret_cast<uint2*>(a.rect)[i] = make_uint2(rect_lo, rect_hi);
-    // early-reject thresholds (see BlendRecord / BackwardRecord)
-    float reject = __int_as_float(0x7f800000), skip = -__int_as_float(0x7f800000);
+    // backward skip threshold (BackwardRecord::skip) and block-culling parameters
+    float skip = -__int_as_float(0x7f800000);
+    CullParams cp{-1.0f, 0.f, 0.f, 0.f, 0.f};
     if (g.visible) {
-      const float l = logf(255.0f * opacity);
-      const bool pd = g.det > 0.0f && g.cxx > 0.0f && g.cyy > 0.0f;
-      if (opacity <= 0.0f) reject = -__int_as_float(0x7f800000);
-      else if (pd) reject = 2.0f * l + 1e-4f;
-      skip = opacity > 0.0f ? -l - 1e-4f : __int_as_float(0x7f800000);
+      skip = opacity > 0.0f ? -logf(255.0f * opacity) - 1e-4f : __int_as_float(0x7f800000);
+      cp = make_cull_params(g.conic[0], g.conic[1], g.conic[2], opacity);
     }
     float4* rp = reinterpret_cast<float4*>(a.record) + 4 * size_t(i);
     rp[0] = make_float4(rec.mx, rec.my, rec.cxx, rec.cxy);
     rp[1] = make_float4(rec.cyy, rec.det, rec.opacity, rec.depth);
-    rp[2] = make_float4(rec.r, rec.g, rec.b, reject);
-    rp[3] = g.visible ? make_float4(g.conic[0], g.conic[1], g.conic[2], 0.f) : make_float4(0.f, 0.f, 0.f, 0.f);
-    float4* bp = reinterpret_cast<float4*>(a.bwd_record) + 3 * size_t(i);
+    rp[2] = make_float4(rec.r, rec.g, rec.b, cp.hy);
+    rp[3] = make_float4(cp.beta, cp.gamma, cp.eps, cp.vr);
+    float4* bp = reinterpret_cast<float4*>(a.bwd_record) + 4 * size_t(i);
     if (g.visible) {
       bp[0] = make_float4(g.mx, g.my, g.conic[0], g.conic[1]);
       bp[1] = make_float4(g.conic[2], opacity, g.depth, rgb[0]);
-      bp[2] = make_float4(rgb[1], rgb[2], skip, 0.f);
+      bp[2] = make_float4(rgb[1], rgb[2], skip, cp.hy);
+      bp[3] = make_float4(cp.beta, cp.gamma, cp.eps, cp.vr);
     } else {
       bp[0] = bp[1] = bp[2] = make_float4(0.f, 0.f, 0.f, 0.f);
+      bp[3] = make_float4(0.f, 0.f, 0.f, 0.f);
+      bp[2].w = -1.0f;
     }
   }
 
