@@ -75,6 +75,7 @@ __device__ __forceinline__ void flush(const float (&c)[kValues], bool any_contri
 // Pixel-loop prologue shared by both modes: this thread's pixel, its
 // upstream gradients and contributor count, the tile's walk length.
 struct BwdPixel {
+  int tile;
   TilePixel tp;
   bool inside;
   size_t pix, hw;
@@ -82,9 +83,8 @@ struct BwdPixel {
   int nmax;
   uint32_t last, warp_last;
   float dLp0 = 0.f, dLp1 = 0.f, dLp2 = 0.f, dLd = 0.f, dLa = 0.f;
-  __device__ __forceinline__ explicit BwdPixel(const BackwardArgs& a) {
-    const int gw = (a.W + kTile - 1) / kTile;
-    const int tile = blockIdx.y * gw + blockIdx.x;
+  __device__ __forceinline__ explicit BwdPixel(const BackwardArgs& a)
+      : tile(int(a.order[blockIdx.x])), tp(tile, (a.W + kTile - 1) / kTile) {
     inside = tp.px < a.W && tp.py < a.H;
     range = a.ranges[tile];
     nmax = int(min(a.tile_max[tile], range.y - range.x));
@@ -109,43 +109,45 @@ struct RefChain {
   float acc0 = 0.f, acc1 = 0.f, acc2 = 0.f, acc_d = 0.f, acc_a = 0.f;
   float last_alpha = 0.f, lc0 = 0.f, lc1 = 0.f, lc2 = 0.f, last_depth = 0.f;
 
-  __device__ __forceinline__ void step(const BwdPixel& p, float4 q0, float4 q1, float4 q2, float dx, float dy,
+  // ok false: the entry is skipped (state unchanged, contributions zero).
+  __device__ __forceinline__ void step(bool ok, const BwdPixel& p, float4 q0, float4 q1, float4 q2, float dx, float dy,
                                        float G, float alpha, float ddelx_dx, float ddely_dy, float (&c)[kValues]) {
-    T = T / (1.f - alpha);
-    const float dchdc = alpha * T;
+    const float Tn = T / (1.f - alpha);
+    const float dchdc = alpha * Tn;
     float dL_dopa = 0.0f;
-    acc0 = last_alpha * lc0 + (1.f - last_alpha) * acc0;
-    lc0 = q1.w;
-    dL_dopa += (q1.w - acc0) * p.dLp0;
-    c[0] = dchdc * p.dLp0;
-    acc1 = last_alpha * lc1 + (1.f - last_alpha) * acc1;
-    lc1 = q2.x;
-    dL_dopa += (q2.x - acc1) * p.dLp1;
-    c[1] = dchdc * p.dLp1;
-    acc2 = last_alpha * lc2 + (1.f - last_alpha) * acc2;
-    lc2 = q2.y;
-    dL_dopa += (q2.y - acc2) * p.dLp2;
-    c[2] = dchdc * p.dLp2;
+    const float n0 = last_alpha * lc0 + (1.f - last_alpha) * acc0;
+    dL_dopa += (q1.w - n0) * p.dLp0;
+    const float n1 = last_alpha * lc1 + (1.f - last_alpha) * acc1;
+    dL_dopa += (q2.x - n1) * p.dLp1;
+    const float n2 = last_alpha * lc2 + (1.f - last_alpha) * acc2;
+    dL_dopa += (q2.y - n2) * p.dLp2;
     const float c_d = q1.z;
-    acc_d = last_alpha * last_depth + (1.f - last_alpha) * acc_d;
-    last_depth = c_d;
-    dL_dopa += (c_d - acc_d) * p.dLd;
-    c[3] = dchdc * p.dLd;
-    acc_a = last_alpha + (1.f - last_alpha) * acc_a;
-    dL_dopa += (1 - acc_a) * p.dLa;
-    dL_dopa *= T;
-    last_alpha = alpha;
+    const float nd = last_alpha * last_depth + (1.f - last_alpha) * acc_d;
+    dL_dopa += (c_d - nd) * p.dLd;
+    const float na = last_alpha + (1.f - last_alpha) * acc_a;
+    dL_dopa += (1 - na) * p.dLa;
+    dL_dopa *= Tn;
     dL_dopa += (-T_final / (1.f - alpha)) * bg_dot;
     const float dL_dG = q1.y * dL_dopa;
     const float gdx = G * dx, gdy = G * dy;
     const float dG_ddelx = -gdx * q0.z - gdy * q0.w;
     const float dG_ddely = -gdy * q1.x - gdx * q0.w;
-    c[4] = dL_dG * dG_ddelx * ddelx_dx;
-    c[5] = dL_dG * dG_ddely * ddely_dy;
-    c[6] = -0.5f * gdx * dx * dL_dG;
-    c[7] = -0.5f * gdx * dy * dL_dG;
-    c[8] = -0.5f * gdy * dy * dL_dG;
-    c[9] = G * dL_dopa;
+    c[0] = ok ? dchdc * p.dLp0 : 0.f;
+    c[1] = ok ? dchdc * p.dLp1 : 0.f;
+    c[2] = ok ? dchdc * p.dLp2 : 0.f;
+    c[3] = ok ? dchdc * p.dLd : 0.f;
+    c[4] = ok ? dL_dG * dG_ddelx * ddelx_dx : 0.f;
+    c[5] = ok ? dL_dG * dG_ddely * ddely_dy : 0.f;
+    c[6] = ok ? -0.5f * gdx * dx * dL_dG : 0.f;
+    c[7] = ok ? -0.5f * gdx * dy * dL_dG : 0.f;
+    c[8] = ok ? -0.5f * gdy * dy * dL_dG : 0.f;
+    c[9] = ok ? G * dL_dopa : 0.f;
+    if (ok) {
+      T = Tn;
+      acc0 = n0; acc1 = n1; acc2 = n2; acc_d = nd; acc_a = na;
+      lc0 = q1.w; lc1 = q2.x; lc2 = q2.y; last_depth = c_d;
+      last_alpha = alpha;
+    }
   }
 };
 
@@ -203,10 +205,8 @@ __global__ void __launch_bounds__(kBlendThreads, 2) render_ref_kernel(BackwardAr
         const bool ok1 = ref_eval(b0, b1, b2, pxf, pyf, dx1, dy1, G1, al1) && j1r >= 0 &&
                          uint32_t(hi - 1 - j1) < p.last;
         float c0[kValues], c1[kValues];
-#pragma unroll
-        for (int k = 0; k < kValues; ++k) c0[k] = c1[k] = 0.f;
-        if (ok0) ch.step(p, a0, a1, a2, dx0, dy0, G0, al0, ddelx_dx, ddely_dy, c0);
-        if (ok1) ch.step(p, b0, b1, b2, dx1, dy1, G1, al1, ddelx_dx, ddely_dy, c1);
+        ch.step(ok0, p, a0, a1, a2, dx0, dy0, G0, al0, ddelx_dx, ddely_dy, c0);
+        ch.step(ok1, p, b0, b1, b2, dx1, dy1, G1, al1, ddelx_dx, ddely_dy, c1);
         flush(c0, ok0, ids[j0], tgt);
         flush(c1, ok1, ids[j1], tgt);
       }
@@ -706,8 +706,8 @@ __global__ void __launch_bounds__(256) gaussians_exact_kernel(BackwardArgs a) {
 }  // namespace
 
 void launch_backward_render(const BackwardArgs& a, cudaStream_t stream) {
-  const dim3 grid((a.W + kTile - 1) / kTile, (a.H + kTile - 1) / kTile);
-  if (grid.x == 0 || grid.y == 0) return;
+  const int grid = ((a.W + kTile - 1) / kTile) * ((a.H + kTile - 1) / kTile);
+  if (grid <= 0) return;
   stage_begin(kStBwdRender, stream);
   if (a.grad_mode == 1) render_exact_kernel<<<grid, kBlendThreads, 0, stream>>>(a);
   else render_ref_kernel<<<grid, kBlendThreads, 0, stream>>>(a);

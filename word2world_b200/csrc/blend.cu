@@ -3,8 +3,8 @@
 //
 // One CTA per 16x16 tile, one thread per pixel, one warp per 8x4 pixel block
 // (tile_walk.cuh).  Each warp walks only the list entries that can reach its
-// block with alpha >= 1/255, two at a time: both entries' Gaussian values are
-// evaluated before the two transmittance/colour updates, so the two
+// block with alpha >= 1/255, kBlendIlp at a time: all their Gaussian values are
+// evaluated before the sequential transmittance/colour updates, so the
 // evaluations overlap.  The CTA stops as soon as every pixel of the tile has
 // terminated (the reference keeps loading every batch of the tile).
 //
@@ -21,14 +21,20 @@
 namespace w2w {
 namespace {
 
-__device__ __forceinline__ float gauss_eval(float px, float py, float mx, float my, float cxx, float cxy, float cyy,
-                                            float det) {
+constexpr int kBlendIlp = 4;  // list entries evaluated together per warp (the list is read 4 bytes at a time)
+static_assert(kBlendIlp == 4, "packed list read");
+
+// The reference's Gaussian value (gaussEval.h:7-29) in two halves: the
+// mahalanobis numerator, then exp(-0.5 * num / det) with negative distances
+// mapped to 1000.
+__device__ __forceinline__ float gauss_num(float px, float py, float mx, float my, float cxx, float cxy, float cyy) {
   using namespace fp;
   const float dx = sub(px, mx), dy = sub(py, my);
   const float tX = d2<BL_TX>(dx, cyy, dy, cxy);
   const float tY = s2<BL_TY>(-dx, cxy, dy, cxx);
-  const float num = s2<BL_NUM>(tX, dx, tY, dy);
-  float m = div(num, det);
+  return s2<BL_NUM>(tX, dx, tY, dy);
+}
+__device__ __forceinline__ float gauss_from_m(float m) {
   if (m < 0.0f) m = 1000.0f;
   return expf(mul(-0.5f, m));
 }
@@ -39,29 +45,29 @@ struct BlendPixel {
   bool done;
 
   // Entry with alpha `al` (record words q1, q2), 1-based list position `pos`.
+  // Branch-free: the updates are selected, so a warp's lanes never diverge.
   __device__ __forceinline__ void step(float al, float4 q1, float4 q2, uint32_t pos) {
-    if (done || !(al >= 1.0f / 255.0f)) return;
+    const bool blend = !done && al >= 1.0f / 255.0f;
     const float nT = mul(T, sub(1.0f, al));
-    if (nT < 0.0001f) {
-      done = true;
-      return;
-    }
+    const bool term = blend && nT < 0.0001f;
+    const bool acc = blend && !term;
     const float aT = mul(al, T);
-    C0 = fma(q2.x, aT, C0);
-    C1 = fma(q2.y, aT, C1);
-    C2 = fma(q2.z, aT, C2);
-    Wt = add(Wt, aT);
-    D = s1<fp::BL_DEPTH>(q1.w, aT, D);
-    T = nT;
-    last = pos;
+    C0 = acc ? fma(q2.x, aT, C0) : C0;
+    C1 = acc ? fma(q2.y, aT, C1) : C1;
+    C2 = acc ? fma(q2.z, aT, C2) : C2;
+    Wt = acc ? add(Wt, aT) : Wt;
+    D = acc ? s1<fp::BL_DEPTH>(q1.w, aT, D) : D;
+    T = acc ? nT : T;
+    last = acc ? pos : last;
+    done = done || term;
   }
 };
 
-__global__ void __launch_bounds__(kBlendThreads) blend_kernel(BlendArgs a) {
+__global__ void __launch_bounds__(kBlendThreads, 2) blend_kernel(BlendArgs a) {
   __shared__ TileWalkShared sm;
   const int gw = (a.W + kTile - 1) / kTile;
-  const int tile = blockIdx.y * gw + blockIdx.x;
-  const TilePixel tp;
+  const int tile = int(a.order[blockIdx.x]);
+  const TilePixel tp(tile, gw);
   const bool inside = tp.px < a.W && tp.py < a.H;
   const uint2 range = a.ranges[tile];
   const int n = int(range.y - range.x);
@@ -84,21 +90,41 @@ __global__ void __launch_bounds__(kBlendThreads) blend_kernel(BlendArgs a) {
                                next_base + int(threadIdx.x) < n);
     if (!__all_sync(0xffffffffu, pix.done)) {
       const float4* s = sm.rec[cur];
-      ListIter it(sm.bal[cur][tp.warp]);
+      const int cnt = build_list(sm, cur, tp.warp, tp.lane);
+      const uint8_t* lst = sm.list[tp.warp];
       const uint32_t base = uint32_t(b * kBatch) + 1u;
-      for (;;) {
-        const int j0 = it.next();
-        if (j0 < 0) break;
-        const int j1r = it.next();
-        const int j1 = j1r < 0 ? j0 : j1r;
-        const float4 a0 = s[kRecVec * j0], a1 = s[kRecVec * j0 + 1];
-        const float4 b0 = s[kRecVec * j1], b1 = s[kRecVec * j1 + 1];
-        const float g0 = gauss_eval(pxf, pyf, a0.x, a0.y, a0.z, a0.w, a1.x, a1.y);
-        const float g1 = gauss_eval(pxf, pyf, b0.x, b0.y, b0.z, b0.w, b1.x, b1.y);
-        const float al0 = fminf(0.99f, mul(a1.z, g0));
-        const float al1 = fminf(0.99f, mul(b1.z, g1));
-        pix.step(al0, a1, s[kRecVec * j0 + 2], base + uint32_t(j0));
-        if (j1r >= 0) pix.step(al1, b1, s[kRecVec * j1 + 2], base + uint32_t(j1));
+      for (int k0 = 0; k0 < cnt; k0 += kBlendIlp) {
+        // kBlendIlp entries in flight: their Gaussian values are independent,
+        // only the transmittance/colour updates are sequential
+        const uint32_t packed = *reinterpret_cast<const uint32_t*>(lst + k0);
+        int j[kBlendIlp];
+#pragma unroll
+        for (int k = 0; k < kBlendIlp; ++k) j[k] = k0 + k < cnt ? int((packed >> (8 * k)) & 255u) : -1;
+        float al[kBlendIlp], num[kBlendIlp], m[kBlendIlp];
+        float4 q1[kBlendIlp], q2[kBlendIlp];
+        bool in_range = true;
+#pragma unroll
+        for (int k = 0; k < kBlendIlp; ++k) {
+          const int jj = j[k] < 0 ? j[0] : j[k];
+          const float4 q0 = s[kRecVec * jj];
+          q1[k] = s[kRecVec * jj + 1];
+          q2[k] = s[kRecVec * jj + 2];
+          num[k] = gauss_num(pxf, pyf, q0.x, q0.y, q0.z, q0.w, q1[k].x);
+          in_range = in_range && div_in_range(num[k], q1[k].y);
+        }
+        // the branch-free division when every lane's operands allow it
+        if (__all_sync(0xffffffffu, in_range)) {
+#pragma unroll
+          for (int k = 0; k < kBlendIlp; ++k) m[k] = div_markstein(num[k], q1[k].y);
+        } else {
+#pragma unroll
+          for (int k = 0; k < kBlendIlp; ++k) m[k] = div(num[k], q1[k].y);
+        }
+#pragma unroll
+        for (int k = 0; k < kBlendIlp; ++k)
+          al[k] = j[k] < 0 ? 0.0f : fminf(0.99f, mul(q1[k].z, gauss_from_m(m[k])));
+#pragma unroll
+        for (int k = 0; k < kBlendIlp; ++k) pix.step(al[k], q1[k], q2[k], base + uint32_t(j[k]));
         if (__all_sync(0xffffffffu, pix.done)) break;
       }
     }
@@ -129,12 +155,46 @@ __global__ void __launch_bounds__(kBlendThreads) blend_kernel(BlendArgs a) {
 
 }  // namespace
 
+// Bucket sort of the tiles by decreasing list length (quarter-octave buckets;
+// order within a bucket is arbitrary).  One CTA.
+__global__ void __launch_bounds__(1024) tile_order_kernel(const uint2* ranges, int num_tiles, uint32_t* order) {
+  constexpr int kBuckets = 130;
+  __shared__ uint32_t s_cnt[kBuckets];
+  __shared__ uint32_t s_pos[kBuckets];
+  auto bucket = [](uint32_t n) -> int {
+    if (n == 0) return 0;
+    const int e = 31 - __clz(n);
+    const uint32_t q = e >= 2 ? (n >> (e - 2)) & 3u : (n << (2 - e)) & 3u;
+    return 1 + 4 * e + int(q);
+  };
+  for (int i = threadIdx.x; i < kBuckets; i += blockDim.x) s_cnt[i] = 0;
+  __syncthreads();
+  for (int t = threadIdx.x; t < num_tiles; t += blockDim.x) {
+    const uint2 r = ranges[t];
+    atomicAdd(&s_cnt[bucket(r.y - r.x)], 1u);
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    uint32_t acc = 0;
+    for (int b = kBuckets - 1; b >= 0; --b) {
+      s_pos[b] = acc;
+      acc += s_cnt[b];
+    }
+  }
+  __syncthreads();
+  for (int t = threadIdx.x; t < num_tiles; t += blockDim.x) {
+    const uint2 r = ranges[t];
+    order[atomicAdd(&s_pos[bucket(r.y - r.x)], 1u)] = uint32_t(t);
+  }
+}
+
 void launch_blend(const BlendArgs& a, cudaStream_t stream) {
-  const dim3 grid((a.W + kTile - 1) / kTile, (a.H + kTile - 1) / kTile);
-  if (grid.x == 0 || grid.y == 0) return;
+  const int tiles = ((a.W + kTile - 1) / kTile) * ((a.H + kTile - 1) / kTile);
+  if (tiles <= 0) return;
   stage_begin(kStBlend, stream);
-  blend_kernel<<<grid, kBlendThreads, 0, stream>>>(a);
-  stage_end(kStBlend, stream, 1);
+  tile_order_kernel<<<1, 1024, 0, stream>>>(a.ranges, tiles, a.order);
+  blend_kernel<<<tiles, kBlendThreads, 0, stream>>>(a);
+  stage_end(kStBlend, stream, 2);
 }
 
 }  // namespace w2w

@@ -38,6 +38,34 @@ __device__ __forceinline__ float sub(float a, float b) { return __fsub_rn(a, b);
 __device__ __forceinline__ float fma(float a, float b, float c) { return __fmaf_rn(a, b, c); }
 __device__ __forceinline__ float div(float a, float b) { return __fdiv_rn(a, b); }
 
+// Correctly rounded a / b without branches, for operands in div_in_range.
+// Markstein's scheme (P. Markstein, IBM J. Res. Dev. 34(1), 1990; Muller et
+// al., Handbook of Floating-Point Arithmetic, ch. 5): from the hardware
+// reciprocal approximation y0 (rcp.approx, within 1 ulp), one Newton step
+// y = y0 + y0 (1 - b y0) gives RN(1/b) (checked against __frcp_rn for every
+// significand); q0 = RN(a y); two remainder corrections q <- q + (a - b q) y,
+// each remainder exact under fma, make q faithful and then, by Markstein's
+// theorem (y = RN(1/b), q faithful), equal to RN(a / b).
+__device__ __forceinline__ float rcp_approx(float x) {
+  float y;
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+__device__ __forceinline__ float div_markstein(float a, float b) {
+  const float y0 = rcp_approx(b);
+  const float y = fma(fma(-b, y0, 1.0f), y0, y0);
+  const float q0 = mul(a, y);
+  const float q1 = fma(fma(-b, q0, a), y, q0);
+  return fma(fma(-b, q1, a), y, q1);
+}
+// Operands for which div_markstein equals div: |b| in [2^-20, 2^60] and
+// a = 0 or |a| in [2^-60, 2^100], so the quotient lies in [2^-120, 2^120] and
+// no intermediate (reciprocal, product, remainders) leaves the normal range.
+__device__ __forceinline__ bool div_in_range(float a, float b) {
+  const float fa = fabsf(a), fb = fabsf(b);
+  return fb >= 0x1p-20f && fb <= 0x1p60f && fa <= 0x1p100f && (fa >= 0x1p-60f || fa == 0.0f);
+}
+
 // a*b + c*d: 0 = both rounded, 1 = fuse a*b, 2 = fuse c*d
 template <int V>
 __device__ __forceinline__ float s2(float a, float b, float c, float d) {
@@ -240,7 +268,7 @@ struct GeomLayout {
 };
 
 struct ImageLayout {
-  size_t n_contrib, ranges, T_final, tile_max, total;
+  size_t n_contrib, ranges, T_final, tile_max, order, total;
   __host__ __device__ ImageLayout(int W, int H) {
     size_t o = 0;
     auto take = [&](size_t bytes) { size_t a = align256(o); o = a + bytes; return a; };
@@ -250,6 +278,7 @@ struct ImageLayout {
     ranges = take(tiles * 8);
     T_final = take(hw * 4);
     tile_max = take(tiles * 4);
+    order = take(tiles * 4);
     total = align256(o);
   }
 };

@@ -94,6 +94,7 @@ struct BlendArgs {
   uint32_t* n_contrib;
   float* T_final;
   uint32_t* tile_max;
+  uint32_t* order;  // tiles in processing order (written here, reused by the backward)
 };
 void launch_blend(const BlendArgs& a, cudaStream_t stream);
 
@@ -121,6 +122,7 @@ struct BackwardArgs {
   const uint32_t* point_list;
   const uint32_t* n_contrib;
   const uint32_t* tile_max;
+  const uint32_t* order;   // tile processing order written by the blend
   const float* T_final;
   const float* out_alpha;
   const float* dL_dcolor;

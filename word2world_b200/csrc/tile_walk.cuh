@@ -23,20 +23,45 @@ struct TileWalkShared {
   float4 rec[2][kBatch * kRecVec];
   uint32_t id[2][kBatch];
   uint32_t bal[2][8][8];  // [buffer][block][32-entry chunk]
+  uint8_t list[8][kBatch];  // per warp: its entries of the current batch, in order
 };
 
-// Pixel of this thread.
+// Expand this warp's eight flag words into its entry list (in order); returns
+// the count.  Warp-collective.
+__device__ __forceinline__ int build_list(TileWalkShared& sm, int buf, int warp, int lane, int start = 0) {
+  __syncwarp();  // the previous walk's reads of the list are done
+  int count = 0;
+  const uint32_t lt = (1u << lane) - 1u;
+#pragma unroll
+  for (int c = 0; c < 8; ++c) {
+    uint32_t bits = sm.bal[buf][warp][c];
+    const int lo = start - 32 * c;  // entries below `start` are dropped
+    if (lo > 0) bits = lo >= 32 ? 0u : bits & (0xffffffffu << lo);
+    if ((bits >> lane) & 1u) sm.list[warp][count + __popc(bits & lt)] = uint8_t(32 * c + lane);
+    count += __popc(bits);
+  }
+  __syncwarp();
+  return count;
+}
+
+// Pixel of this thread in tile `tile` of a grid `gw` tiles wide.
 struct TilePixel {
   int X0, Y0, px, py, warp, lane;
-  __device__ __forceinline__ TilePixel() {
+  __device__ __forceinline__ TilePixel(int tile, int gw) {
     warp = threadIdx.x >> 5;
     lane = threadIdx.x & 31;
-    X0 = blockIdx.x * kTile;
-    Y0 = blockIdx.y * kTile;
+    X0 = (tile % gw) * kTile;
+    Y0 = (tile / gw) * kTile;
     px = X0 + kBlockW * (warp & 1) + (lane & 7);
     py = Y0 + kBlockH * (warp >> 1) + (lane >> 3);
   }
 };
+
+// Tiles are processed heaviest first: CTA b takes tile order[b], where order
+// lists the tiles by decreasing list length (tile_order_kernel), so the
+// longest lists start in the first wave instead of wherever the raster order
+// puts them.
+__global__ void tile_order_kernel(const uint2* ranges, int num_tiles, uint32_t* order);
 
 // One entry's record held in registers between its gather and its store.
 struct Staged {
