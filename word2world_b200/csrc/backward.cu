@@ -112,7 +112,9 @@ struct RefChain {
   // ok false: the entry is skipped (state unchanged, contributions zero).
   __device__ __forceinline__ void step(bool ok, const BwdPixel& p, float4 q0, float4 q1, float4 q2, float dx, float dy,
                                        float G, float alpha, float ddelx_dx, float ddely_dy, float (&c)[kValues]) {
-    const float Tn = T / (1.f - alpha);
+    // T in [~1e-4, 1] (the forward stops before T < 1e-4) and 1 - alpha in
+    // [0.01, 1]: both divisions are in div_markstein's range, which equals /
+    const float Tn = div_markstein(T, 1.f - alpha);
     const float dchdc = alpha * Tn;
     float dL_dopa = 0.0f;
     const float n0 = last_alpha * lc0 + (1.f - last_alpha) * acc0;
@@ -127,7 +129,7 @@ struct RefChain {
     const float na = last_alpha + (1.f - last_alpha) * acc_a;
     dL_dopa += (1 - na) * p.dLa;
     dL_dopa *= Tn;
-    dL_dopa += (-T_final / (1.f - alpha)) * bg_dot;
+    dL_dopa += div_markstein(-T_final, 1.f - alpha) * bg_dot;
     const float dL_dG = q1.y * dL_dopa;
     const float gdx = G * dx, gdy = G * dy;
     const float dG_ddelx = -gdx * q0.z - gdy * q0.w;
@@ -192,17 +194,17 @@ __global__ void __launch_bounds__(kBlendThreads, 2) render_ref_kernel(BackwardAr
     if (start < kBatch) {
       const float4* s = sm.rec[cur];
       const uint32_t* ids = sm.id[cur];
-      ListIter it(sm.bal[cur][p.tp.warp], start > 0 ? start : 0);
-      for (;;) {
-        const int j0 = it.next();
-        if (j0 < 0) break;
-        const int j1r = it.next();
-        const int j1 = j1r < 0 ? j0 : j1r;
+      const int cnt = build_list(sm, cur, p.tp.warp, p.tp.lane, start > 0 ? start : 0);
+      const uint8_t* lst = sm.list[p.tp.warp];
+      for (int k0 = 0; k0 < cnt; k0 += 2) {
+        const int j0 = lst[k0];
+        const bool has1 = k0 + 1 < cnt;
+        const int j1 = has1 ? int(lst[k0 + 1]) : j0;
         const float4 a0 = s[kRecVec * j0], a1 = s[kRecVec * j0 + 1], a2 = s[kRecVec * j0 + 2];
         const float4 b0 = s[kRecVec * j1], b1 = s[kRecVec * j1 + 1], b2 = s[kRecVec * j1 + 2];
         float dx0, dy0, G0, al0, dx1, dy1, G1, al1;
         const bool ok0 = ref_eval(a0, a1, a2, pxf, pyf, dx0, dy0, G0, al0) && uint32_t(hi - 1 - j0) < p.last;
-        const bool ok1 = ref_eval(b0, b1, b2, pxf, pyf, dx1, dy1, G1, al1) && j1r >= 0 &&
+        const bool ok1 = ref_eval(b0, b1, b2, pxf, pyf, dx1, dy1, G1, al1) && has1 &&
                          uint32_t(hi - 1 - j1) < p.last;
         float c0[kValues], c1[kValues];
         ch.step(ok0, p, a0, a1, a2, dx0, dy0, G0, al0, ddelx_dx, ddely_dy, c0);
@@ -215,17 +217,15 @@ __global__ void __launch_bounds__(kBlendThreads, 2) render_ref_kernel(BackwardAr
   }
 }
 
-__device__ __forceinline__ float gauss_eval_fwd(float px, float py, float mx, float my, float cxx, float cxy,
-                                                float cyy, float det, float* mahal) {
+// The forward's Gaussian value (blend.cu), split at its division so that a
+// warp's divisions can run branch-free together.
+__device__ __forceinline__ float gauss_num_fwd(float px, float py, float mx, float my, float cxx, float cxy,
+                                               float cyy) {
   using namespace fp;
   const float dx = sub(px, mx), dy = sub(py, my);
   const float tX = d2<BL_TX>(dx, cyy, dy, cxy);
   const float tY = s2<BL_TY>(-dx, cxy, dy, cxx);
-  const float num = s2<BL_NUM>(tX, dx, tY, dy);
-  float m = div(num, det);
-  *mahal = m;
-  if (m < 0.0f) m = 1000.0f;
-  return expf(mul(-0.5f, m));
+  return s2<BL_NUM>(tX, dx, tY, dy);
 }
 
 // Exact derivative of the forward blend, per pixel, for one entry:
@@ -234,39 +234,43 @@ struct ExactChain {
   float T;
   float S0, S1, S2, SD = 0.f, SW = 0.f;  // suffix sums behind the current entry (colour includes the background)
 
-  __device__ __forceinline__ void step(const BwdPixel& p, float4 q0, float4 q1, float4 q2, float pxf, float pyf,
-                                       float g, float og, float a_, float mahal, float hW, float hH,
+  // ok false: the entry is skipped (state unchanged, contributions zero).
+  __device__ __forceinline__ void step(bool ok, const BwdPixel& p, float4 q0, float4 q1, float4 q2, float pxf,
+                                       float pyf, float g, float og, float a_, float mahal, float hW, float hH,
                                        float (&c)[kValues]) {
-    const float ia = 1.0f / (1.0f - a_);
-    T = T * ia;  // transmittance in front of this entry
-    const float aT = a_ * T;
-    float dLda = p.dLp0 * (q2.x * T - S0 * ia) + p.dLp1 * (q2.y * T - S1 * ia) + p.dLp2 * (q2.z * T - S2 * ia);
-    dLda += p.dLd * (q1.w * T - SD * ia);
-    dLda += p.dLa * (T - SW * ia);
-    c[0] = aT * p.dLp0;
-    c[1] = aT * p.dLp1;
-    c[2] = aT * p.dLp2;
-    c[3] = aT * p.dLd;
-    S0 += q2.x * aT;
-    S1 += q2.y * aT;
-    S2 += q2.z * aT;
-    SD += q1.w * aT;
-    SW += aT;
-    if (og < 0.99f) {
-      c[9] = dLda * g;
-      if (mahal >= 0.0f) {
-        const float dLdm = dLda * q1.z * (-0.5f * g);
-        const float cxx = q0.z, cxy = q0.w, cyy = q1.x, det = q1.y;
-        const float dx = pxf - q0.x, dy = pyf - q0.y;
-        const float idet = 1.0f / det;
-        c[4] = -dLdm * (2.f * cyy * dx - 2.f * cxy * dy) * idet * hW;
-        c[5] = -dLdm * (2.f * cxx * dy - 2.f * cxy * dx) * idet * hH;
-        const float num = mahal * det;
-        c[6] = dLdm * (dy * dy * idet - num * cyy * idet * idet);
-        c[7] = dLdm * (-2.f * dx * dy * idet + 2.f * num * cxy * idet * idet);
-        c[8] = dLdm * (dx * dx * idet - num * cxx * idet * idet);
-      }
+    const float ia = rcp_markstein(1.0f - a_);  // 1 - alpha in [0.01, 1]
+    const float Tn = T * ia;  // transmittance in front of this entry
+    const float aT = a_ * Tn;
+    float dLda = p.dLp0 * (q2.x * Tn - S0 * ia) + p.dLp1 * (q2.y * Tn - S1 * ia) + p.dLp2 * (q2.z * Tn - S2 * ia);
+    dLda += p.dLd * (q1.w * Tn - SD * ia);
+    dLda += p.dLa * (Tn - SW * ia);
+    c[0] = ok ? aT * p.dLp0 : 0.f;
+    c[1] = ok ? aT * p.dLp1 : 0.f;
+    c[2] = ok ? aT * p.dLp2 : 0.f;
+    c[3] = ok ? aT * p.dLd : 0.f;
+    if (ok) {
+      T = Tn;
+      S0 += q2.x * aT;
+      S1 += q2.y * aT;
+      S2 += q2.z * aT;
+      SD += q1.w * aT;
+      SW += aT;
     }
+    const bool unclamped = ok && og < 0.99f;
+    c[9] = unclamped ? dLda * g : 0.f;
+    const bool inner = unclamped && mahal >= 0.0f;
+    const float dLdm = dLda * q1.z * (-0.5f * g);
+    const float cxx = q0.z, cxy = q0.w, cyy = q1.x, det = q1.y;
+    const float dx = pxf - q0.x, dy = pyf - q0.y;
+    // det >= 0.09 (the forward's +0.3 low-pass on a positive semi-definite
+    // covariance), where rcp_markstein is the correctly rounded 1/det
+    const float idet = rcp_markstein(det);
+    const float num = mahal * det;
+    c[4] = inner ? -dLdm * (2.f * cyy * dx - 2.f * cxy * dy) * idet * hW : 0.f;
+    c[5] = inner ? -dLdm * (2.f * cxx * dy - 2.f * cxy * dx) * idet * hH : 0.f;
+    c[6] = inner ? dLdm * (dy * dy * idet - num * cyy * idet * idet) : 0.f;
+    c[7] = inner ? dLdm * (-2.f * dx * dy * idet + 2.f * num * cxy * idet * idet) : 0.f;
+    c[8] = inner ? dLdm * (dx * dx * idet - num * cxx * idet * idet) : 0.f;
   }
 };
 
@@ -298,26 +302,33 @@ __global__ void __launch_bounds__(kBlendThreads, 2) render_exact_kernel(Backward
     if (start < kBatch) {
       const float4* s = sm.rec[cur];
       const uint32_t* ids = sm.id[cur];
-      ListIter it(sm.bal[cur][p.tp.warp], start > 0 ? start : 0);
-      for (;;) {
-        const int j0 = it.next();
-        if (j0 < 0) break;
-        const int j1r = it.next();
-        const int j1 = j1r < 0 ? j0 : j1r;
+      const int cnt = build_list(sm, cur, p.tp.warp, p.tp.lane, start > 0 ? start : 0);
+      const uint8_t* lst = sm.list[p.tp.warp];
+      for (int k0 = 0; k0 < cnt; k0 += 2) {
+        const int j0 = lst[k0];
+        const bool has1 = k0 + 1 < cnt;
+        const int j1 = has1 ? int(lst[k0 + 1]) : j0;
         const float4 a0 = s[kRecVec * j0], a1 = s[kRecVec * j0 + 1];
         const float4 b0 = s[kRecVec * j1], b1 = s[kRecVec * j1 + 1];
+        const float n0 = gauss_num_fwd(pxf, pyf, a0.x, a0.y, a0.z, a0.w, a1.x);
+        const float n1 = gauss_num_fwd(pxf, pyf, b0.x, b0.y, b0.z, b0.w, b1.x);
         float m0, m1;
-        const float g0 = gauss_eval_fwd(pxf, pyf, a0.x, a0.y, a0.z, a0.w, a1.x, a1.y, &m0);
-        const float g1 = gauss_eval_fwd(pxf, pyf, b0.x, b0.y, b0.z, b0.w, b1.x, b1.y, &m1);
+        if (__all_sync(0xffffffffu, div_in_range(n0, a1.y) && div_in_range(n1, b1.y))) {
+          m0 = div_markstein(n0, a1.y);
+          m1 = div_markstein(n1, b1.y);
+        } else {
+          m0 = div(n0, a1.y);
+          m1 = div(n1, b1.y);
+        }
+        const float g0 = expf(mul(-0.5f, m0 < 0.0f ? 1000.0f : m0));
+        const float g1 = expf(mul(-0.5f, m1 < 0.0f ? 1000.0f : m1));
         const float og0 = mul(a1.z, g0), og1 = mul(b1.z, g1);
         const float al0 = fminf(0.99f, og0), al1 = fminf(0.99f, og1);
         const bool ok0 = al0 >= 1.0f / 255.0f && uint32_t(hi - 1 - j0) < p.last;
-        const bool ok1 = al1 >= 1.0f / 255.0f && j1r >= 0 && uint32_t(hi - 1 - j1) < p.last;
+        const bool ok1 = al1 >= 1.0f / 255.0f && has1 && uint32_t(hi - 1 - j1) < p.last;
         float c0[kValues], c1[kValues];
-#pragma unroll
-        for (int k = 0; k < kValues; ++k) c0[k] = c1[k] = 0.f;
-        if (ok0) ch.step(p, a0, a1, s[kRecVec * j0 + 2], pxf, pyf, g0, og0, al0, m0, hW, hH, c0);
-        if (ok1) ch.step(p, b0, b1, s[kRecVec * j1 + 2], pxf, pyf, g1, og1, al1, m1, hW, hH, c1);
+        ch.step(ok0, p, a0, a1, s[kRecVec * j0 + 2], pxf, pyf, g0, og0, al0, m0, hW, hH, c0);
+        ch.step(ok1, p, b0, b1, s[kRecVec * j1 + 2], pxf, pyf, g1, og1, al1, m1, hW, hH, c1);
         flush(c0, ok0, ids[j0], tgt);
         flush(c1, ok1, ids[j1], tgt);
       }

@@ -51,9 +51,13 @@ __device__ __forceinline__ float rcp_approx(float x) {
   asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
   return y;
 }
-__device__ __forceinline__ float div_markstein(float a, float b) {
+// RN(1/b) for |b| in [2^-20, 2^60].
+__device__ __forceinline__ float rcp_markstein(float b) {
   const float y0 = rcp_approx(b);
-  const float y = fma(fma(-b, y0, 1.0f), y0, y0);
+  return fma(fma(-b, y0, 1.0f), y0, y0);
+}
+__device__ __forceinline__ float div_markstein(float a, float b) {
+  const float y = rcp_markstein(b);
   const float q0 = mul(a, y);
   const float q1 = fma(fma(-b, q0, a), y, q0);
   return fma(fma(-b, q1, a), y, q1);

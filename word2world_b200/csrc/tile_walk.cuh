@@ -9,8 +9,8 @@
 // stores the record's first 48 bytes to shared memory and computes the
 // entry's 8-bit block mask (block_mask in common.cuh).  One ballot per block
 // bit turns the masks into, per block, eight 32-bit words of "this entry can
-// reach my block" flags, and each warp walks only its own set bits, in list
-// order.
+// reach my block" flags; each warp expands its own words into a list of entry
+// indices (build_list) and walks only those, in list order.
 #pragma once
 
 #include "common.cuh"
@@ -107,34 +107,5 @@ __device__ __forceinline__ void stage_store(TileWalkShared& sm, int buf, const S
   }
   if (lane < 8) sm.bal[buf][lane][chunk] = mine;
 }
-
-// Walks the set bits of one block's eight flag words in increasing entry
-// order.  The words are warp-uniform, so the walk is too.
-struct ListIter {
-  const uint32_t* words;
-  uint32_t bits;
-  int chunk;
-  __device__ __forceinline__ ListIter(const uint32_t* w) : words(w), bits(w[0]), chunk(0) {}
-  // Starting at entry `start` (0 <= start; >= 256 walks nothing).
-  __device__ __forceinline__ ListIter(const uint32_t* w, int start) : words(w) {
-    if (start >= kBatch) {
-      chunk = 7;
-      bits = 0;
-    } else {
-      chunk = start >> 5;
-      bits = w[chunk] & (0xffffffffu << (start & 31));
-    }
-  }
-  // Next entry index within the batch, or -1.
-  __device__ __forceinline__ int next() {
-    while (bits == 0) {
-      if (chunk == 7) return -1;
-      bits = words[++chunk];
-    }
-    const int j = (chunk << 5) + __ffs(bits) - 1;
-    bits &= bits - 1;
-    return j;
-  }
-};
 
 }  // namespace w2w
