@@ -337,6 +337,60 @@ __global__ void __launch_bounds__(kBlendThreads, 2) render_exact_kernel(Backward
   }
 }
 
+// ---------------------------------------------------------------------------
+// Per-Gaussian passes: one thread per Gaussian, with the SH rows (up to 48
+// floats each) moved between global and shared memory by the whole warp, so
+// that global loads and stores are contiguous 128-byte runs instead of one
+// 192-byte-strided row per thread.
+// ---------------------------------------------------------------------------
+constexpr int kGaussThreads = 128;
+constexpr int kShStride = 49;  // odd row stride: row reads by 32 threads hit 32 banks
+
+__device__ __forceinline__ int sh_stride(int M) {
+  const int r = 3 * (M < 16 ? M : 16);
+  return r | 1;
+}
+
+// Rows [i0, i0 + n) of shs ([P, M, 3]), first min(M, 16) coefficients, into
+// s (row g at g * stride).  Warp-collective.
+__device__ __forceinline__ void sh_stage_in(const float* shs, int M, int i0, int n, float* s, int stride) {
+  const int rs = 3 * (M < 16 ? M : 16), rg = 3 * M, lane = threadIdx.x & 31;
+  if (rs > 0) {
+    int g = 0, c = lane;
+    while (c >= rs) { c -= rs; ++g; }
+    for (int e = lane; e < n * rs; e += 32) {
+      s[g * stride + c] = shs[size_t(i0 + g) * rg + c];
+      c += 32;
+      while (c >= rs) { c -= rs; ++g; }
+    }
+  }
+  __syncwarp();
+}
+
+// dsh rows [i0, i0 + n) ([P, M, 3]) = basis[k] * cf[ch] (k < 16; 0 beyond),
+// written contiguously; each thread's factors pass through s.  Warp-collective.
+__device__ __forceinline__ void sh_store_outer(float* dsh, int M, int i0, int n, float* s, const float (&basis)[16],
+                                               const float (&cf)[3], bool active) {
+  constexpr int kRow = 21;  // 16 basis + 3 colour factors, odd stride
+  const int lane = threadIdx.x & 31, rg = 3 * M;
+  __syncwarp();  // the SH rows in s have been read
+#pragma unroll
+  for (int k = 0; k < 16; ++k) s[lane * kRow + k] = active ? basis[k] : 0.f;
+#pragma unroll
+  for (int ch = 0; ch < 3; ++ch) s[lane * kRow + 16 + ch] = active ? cf[ch] : 0.f;
+  __syncwarp();
+  if (rg > 0) {
+    int g = 0, c = lane;
+    while (c >= rg) { c -= rg; ++g; }
+    for (int e = lane; e < n * rg; e += 32) {
+      const int k = c / 3, ch = c - 3 * k;
+      dsh[size_t(i0 + g) * rg + c] = k < 16 ? s[g * kRow + k] * s[g * kRow + 16 + ch] : 0.f;
+      c += 32;
+      while (c >= rg) { c -= rg; ++g; }
+    }
+  }
+}
+
 // Per-Gaussian, reference formulas (backward.cu:27-227 then :229-519)
 __constant__ float kSH_C2[5] = {1.0925484305920792f, -1.0925484305920792f, 0.31539156525252005f,
                                 -1.0925484305920792f, 0.5462742152960396f};
@@ -344,19 +398,12 @@ __constant__ float kSH_C3[7] = {-0.5900435899266435f, 2.890611442640554f, -0.457
                                 0.3731763325901154f,  -0.4570457994644658f, 1.445305721320277f,
                                 -0.5900435899266435f};
 
-__global__ void __launch_bounds__(256) gaussians_ref_kernel(BackwardArgs a) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= a.P) return;
+// One Gaussian (radius > 0) of the reference-formula pass: every output but
+// dL_dsh, plus the SH basis and masked colour gradient dL_dsh is built from.
+// sh_row: this Gaussian's SH coefficients (staged in shared memory).
+__device__ __forceinline__ void ref_gaussian(const BackwardArgs& a, int i, const float* sh_row, float (&basis)[16],
+                                             float (&cf)[3]) {
   const int M = a.M;
-  float* dsh = a.dL_dsh + size_t(i) * M * 3;
-  if (!(a.radii[i] > 0)) {
-    for (int k = 0; k < 3; ++k) a.dL_dmeans3D[3 * i + k] = 0.f;
-    for (int k = 0; k < 6; ++k) a.dL_dcov3D[6 * i + k] = 0.f;
-    for (int k = 0; k < M * 3; ++k) dsh[k] = 0.f;
-    for (int k = 0; k < 3; ++k) a.dL_dscales[3 * i + k] = 0.f;
-    for (int k = 0; k < 4; ++k) a.dL_drotations[4 * i + k] = 0.f;
-    return;
-  }
   const float* view = a.view;
   const float* proj = a.proj;
   const float cx = a.means3D[3 * i], cy = a.means3D[3 * i + 1], cz = a.means3D[3 * i + 2];
@@ -460,22 +507,15 @@ __global__ void __launch_bounds__(256) gaussians_ref_kernel(BackwardArgs a) {
   const float x = ox * im, y = oy * im, z = oz * im;
   const float x2 = x * x, y2 = y * y, z2 = z * z, xy = x * y, xz = x * z, yz = y * z;
   const float x2my2 = x2 - y2, tx2 = 3.0f * x2, ty2 = 3.0f * y2, fz2 = 4.0f * z2, wz2 = 2.0f * z2;
-  float cf[3];
   for (int ch = 0; ch < 3; ++ch) cf[ch] = a.dL_dcolors[3 * i + ch] * (a.clamped[3 * i + ch] ? 0.0f : 1.0f);
   const float SH_C0 = 0.28209479177387814f, SH_C1 = 0.4886025119029199f;
-  float basis[16];
   basis[0] = SH_C0; basis[1] = -SH_C1 * y; basis[2] = SH_C1 * z; basis[3] = -SH_C1 * x;
   basis[4] = kSH_C2[0] * xy; basis[5] = kSH_C2[1] * yz; basis[6] = kSH_C2[2] * (wz2 - x2 - y2);
   basis[7] = kSH_C2[3] * xz; basis[8] = kSH_C2[4] * x2my2;
   basis[9] = kSH_C3[0] * y * (tx2 - y2); basis[10] = kSH_C3[1] * xy * z; basis[11] = kSH_C3[2] * y * (fz2 - x2 - y2);
   basis[12] = kSH_C3[3] * z * (wz2 - tx2 - ty2); basis[13] = kSH_C3[4] * x * (fz2 - x2 - y2);
   basis[14] = kSH_C3[5] * z * x2my2; basis[15] = kSH_C3[6] * x * (x2 - ty2);
-  const int nb = M < 16 ? M : 16;
-  for (int k = 0; k < nb; ++k)
-    for (int ch = 0; ch < 3; ++ch) dsh[3 * k + ch] = basis[k] * cf[ch];
-  for (int k = nb * 3; k < M * 3; ++k) dsh[k] = 0.f;
-  const float* shd = a.shs + size_t(i) * M * 3;
-  auto SH = [&](int k, int ch) -> float { return k < M ? shd[3 * k + ch] : 0.0f; };
+  auto SH = [&](int k, int ch) -> float { return k < M ? sh_row[3 * k + ch] : 0.0f; };
   float ag[3] = {0.f, 0.f, 0.f};
   auto dotc = [&](int k) { return SH(k, 0) * cf[0] + SH(k, 1) * cf[1] + SH(k, 2) * cf[2]; };
   ag[0] -= SH_C1 * dotc(3);
@@ -554,20 +594,36 @@ __global__ void __launch_bounds__(256) gaussians_ref_kernel(BackwardArgs a) {
   a.dL_drotations[4 * i + 3] = dq.w;
 }
 
-// Per-Gaussian, exact derivative of the forward.
-__global__ void __launch_bounds__(256) gaussians_exact_kernel(BackwardArgs a) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= a.P) return;
-  const int M = a.M;
-  float* dsh = a.dL_dsh + size_t(i) * M * 3;
-  if (!(a.radii[i] > 0)) {
+__global__ void __launch_bounds__(kGaussThreads) gaussians_ref_kernel(BackwardArgs a) {
+  __shared__ float s_sh[kGaussThreads / 32][32 * kShStride];
+  const int lane = threadIdx.x & 31;
+  float* sw = s_sh[threadIdx.x >> 5];
+  const int i0 = blockIdx.x * kGaussThreads + (threadIdx.x & ~31);
+  if (i0 >= a.P) return;  // warp-uniform
+  const int n = min(32, a.P - i0);
+  const int i = i0 + lane;
+  const int stride = sh_stride(a.M);
+  sh_stage_in(a.shs, a.M, i0, n, sw, stride);
+  float basis[16], cf[3] = {0.f, 0.f, 0.f};
+  const bool active = lane < n && a.radii[i] > 0;
+  if (active) {
+    ref_gaussian(a, i, sw + lane * stride, basis, cf);
+  } else if (lane < n) {
     for (int k = 0; k < 3; ++k) a.dL_dmeans3D[3 * i + k] = 0.f;
     for (int k = 0; k < 6; ++k) a.dL_dcov3D[6 * i + k] = 0.f;
-    for (int k = 0; k < M * 3; ++k) dsh[k] = 0.f;
     for (int k = 0; k < 3; ++k) a.dL_dscales[3 * i + k] = 0.f;
     for (int k = 0; k < 4; ++k) a.dL_drotations[4 * i + k] = 0.f;
-    return;
   }
+  // dL_dsh[k][ch] = basis[k] * cf[ch] for the first min(M, 16) bands, 0 beyond
+  sh_store_outer(a.dL_dsh, a.M, i0, n, sw, basis, cf, active);
+}
+
+// Per-Gaussian, exact derivative of the forward.
+// One Gaussian (radius > 0) of the exact-derivative pass: every output but
+// dL_dsh, plus the outer-product factors of dL_dsh (see ref_gaussian).
+__device__ __forceinline__ void exact_gaussian(const BackwardArgs& a, int i, const float* sh_row,
+                                               float (&basis)[16], float (&cf)[3]) {
+  const int M = a.M;
   const float* V = a.view;
   const float* PM = a.proj;
   const float m0 = a.means3D[3 * i], m1 = a.means3D[3 * i + 1], m2 = a.means3D[3 * i + 2];
@@ -694,24 +750,48 @@ __global__ void __launch_bounds__(256) gaussians_exact_kernel(BackwardArgs a) {
   int de = a.degree > 3 ? 3 : a.degree;
   while (de > 0 && (de + 1) * (de + 1) > M) --de;
   const int nb = (de + 1) * (de + 1);
-  const float* shd = a.shs + size_t(i) * M * 3;
+  const float* shd = sh_row;
   float gdir[3] = {0.f, 0.f, 0.f};
   for (int k = 0; k < nb; ++k) {
-    dsh[3 * k] = b[k] * gc0;
-    dsh[3 * k + 1] = b[k] * gc1;
-    dsh[3 * k + 2] = b[k] * gc2;
     const float sdot = shd[3 * k] * gc0 + shd[3 * k + 1] * gc1 + shd[3 * k + 2] * gc2;
     gdir[0] += sdot * db[k][0];
     gdir[1] += sdot * db[k][1];
     gdir[2] += sdot * db[k][2];
   }
-  for (int k = nb * 3; k < M * 3; ++k) dsh[k] = 0.f;
+  // dL_dsh = b[k] * gc for the bands the forward used, 0 beyond
+  for (int k = 0; k < 16; ++k) basis[k] = k < nb ? b[k] : 0.f;
+  cf[0] = gc0;
+  cf[1] = gc1;
+  cf[2] = gc2;
   const float dd[3] = {X, Y, Z};
   const float dot = dd[0] * gdir[0] + dd[1] * gdir[1] + dd[2] * gdir[2];
   for (int p = 0; p < 3; ++p) gm[p] += (gdir[p] - dd[p] * dot) / vn;
   a.dL_dmeans3D[3 * i] = gm[0];
   a.dL_dmeans3D[3 * i + 1] = gm[1];
   a.dL_dmeans3D[3 * i + 2] = gm[2];
+}
+
+__global__ void __launch_bounds__(kGaussThreads) gaussians_exact_kernel(BackwardArgs a) {
+  __shared__ float s_sh[kGaussThreads / 32][32 * kShStride];
+  const int lane = threadIdx.x & 31;
+  float* sw = s_sh[threadIdx.x >> 5];
+  const int i0 = blockIdx.x * kGaussThreads + (threadIdx.x & ~31);
+  if (i0 >= a.P) return;  // warp-uniform
+  const int n = min(32, a.P - i0);
+  const int i = i0 + lane;
+  const int stride = sh_stride(a.M);
+  sh_stage_in(a.shs, a.M, i0, n, sw, stride);
+  float basis[16], cf[3] = {0.f, 0.f, 0.f};
+  const bool active = lane < n && a.radii[i] > 0;
+  if (active) {
+    exact_gaussian(a, i, sw + lane * stride, basis, cf);
+  } else if (lane < n) {
+    for (int k = 0; k < 3; ++k) a.dL_dmeans3D[3 * i + k] = 0.f;
+    for (int k = 0; k < 6; ++k) a.dL_dcov3D[6 * i + k] = 0.f;
+    for (int k = 0; k < 3; ++k) a.dL_dscales[3 * i + k] = 0.f;
+    for (int k = 0; k < 4; ++k) a.dL_drotations[4 * i + k] = 0.f;
+  }
+  sh_store_outer(a.dL_dsh, a.M, i0, n, sw, basis, cf, active);
 }
 
 }  // namespace
@@ -727,10 +807,10 @@ void launch_backward_render(const BackwardArgs& a, cudaStream_t stream) {
 
 void launch_backward_gaussians(const BackwardArgs& a, cudaStream_t stream) {
   if (a.P <= 0) return;
-  const int blocks = (a.P + 255) / 256;
+  const int blocks = (a.P + kGaussThreads - 1) / kGaussThreads;
   stage_begin(kStBwdGaussians, stream);
-  if (a.grad_mode == 1) gaussians_exact_kernel<<<blocks, 256, 0, stream>>>(a);
-  else gaussians_ref_kernel<<<blocks, 256, 0, stream>>>(a);
+  if (a.grad_mode == 1) gaussians_exact_kernel<<<blocks, kGaussThreads, 0, stream>>>(a);
+  else gaussians_ref_kernel<<<blocks, kGaussThreads, 0, stream>>>(a);
   stage_end(kStBwdGaussians, stream, 1);
 }
 
