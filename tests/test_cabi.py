@@ -20,7 +20,10 @@ def declared_functions():
 @pytest.fixture(scope="module")
 def lib():
     if not os.path.exists(LIB):
-        import word2world_b200.build as b
+        import importlib.util
+        spec = importlib.util.spec_from_file_location("w2w_build", os.path.join(os.path.dirname(LIB), "build.py"))
+        b = importlib.util.module_from_spec(spec)
+        spec.loader.exec_module(b)
         b.build_lib()
     return ctypes.CDLL(LIB)
 

@@ -22,7 +22,7 @@ try:
     from . import _C  # noqa: E402
 except ImportError as e:  # pragma: no cover - exercised only without a build
     raise ImportError(
-        "word2world_b200: the CUDA extension is not built (run `python -m word2world_b200.build`); "
+        "word2world_b200: the CUDA extension is not built (run `python word2world_b200/build.py`); "
         f"there is no CPU fallback. ({e})") from e
 
 LIB_PATH = os.path.join(_HERE, "libw2w_raster.so")

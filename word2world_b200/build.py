@@ -7,7 +7,8 @@
   linked to ``libw2w_raster.so`` through ``$ORIGIN``.
 
 Both land next to this file so they travel with the source tree.  Rebuilds only
-what is older than its sources.  ``python -m word2world_b200.build [--force]``.
+what is older than its sources.  ``python word2world_b200/build.py [--force]`` (run as a
+script: importing the package needs the extension this builds).
 """
 from __future__ import annotations
 
