@@ -304,6 +304,39 @@ def backward(fwd: dict, dL_dcolor, dL_ddepth=None, dL_dalpha=None, mode: str = "
         g["abs_dL_dcolors"] = abs_sum[:, 0:3]
         g["abs_dL_dmeans2D"] = np.concatenate([abs_sum[:, 4:6], np.zeros((P, 1))], axis=1)
         g["abs_dL_dopacity"] = abs_sum[:, 9:10]
+        # The per-Gaussian pass is linear in the accumulated values (colour,
+        # depth, mean2D, conic), so their accumulation-order error reaches its
+        # outputs as at most sum_i |L e_i| * abs_sum_i: one pass per
+        # accumulated component with that component's abs_sum as input.
+        derived = {k: np.zeros_like(g[k], dtype=np.float64)
+                   for k in ("dL_dmeans3D", "dL_dcov3D", "dL_dsh", "dL_dscales", "dL_drotations")}
+        for col in range(9):
+            d_m2 = np.zeros((P, 3), R_); d_col = np.zeros((P, 3), R_); d_dep = np.zeros(P, R_)
+            d_con = np.zeros((P, 4), R_)
+            v = abs_sum[:, col].astype(R_)
+            if col < 3:
+                d_col[:, col] = v
+            elif col == 3:
+                d_dep[:] = v
+            elif col < 6:
+                d_m2[:, col - 4] = v
+            else:
+                d_con[:, (0, 1, 3)[col - 6]] = v
+            o = {k: np.zeros_like(g[k]) for k in derived}
+            getattr(L, "orc_backward_cov2d" + sfx)(
+                ctypes.c_int(P), _p(inp["means3D"]), _p(fwd["radii"]), _p(fwd["cov3D"]), CT(h_x), CT(h_y),
+                CT(np.float32(tfx)), CT(np.float32(tfy)), _p(_f(s.viewmatrix).reshape(-1)), _p(d_con),
+                _p(o["dL_dcov3D"]), _p(o["dL_dmeans3D"]))
+            getattr(L, "orc_backward_preprocess" + sfx)(
+                ctypes.c_int(P), ctypes.c_int(M), _p(inp["means3D"]), _p(fwd["radii"]), _p(inp["shs"]),
+                _p(fwd["clamped"]), _p(inp["scales"]), _p(inp["rotations"]), CT(scale_modifier),
+                _p(_f(s.viewmatrix).reshape(-1)), _p(_f(s.projmatrix).reshape(-1)), _p(_f(s.campos)),
+                _p(d_m2), _p(d_col), _p(d_dep), _p(o["dL_dcov3D"]),
+                _p(o["dL_dmeans3D"]), _p(o["dL_dsh"]), _p(o["dL_dscales"]), _p(o["dL_drotations"]))
+            for k in derived:
+                derived[k] += np.abs(o[k].astype(np.float64))
+        for k, v in derived.items():
+            g["abs_" + k] = v
     elif mode == "exact":
         getattr(L, "orc_backward_exact" + sfx)(
             ctypes.byref(cfg), ctypes.c_int(P), _p(inp["means3D"]), _p(inp["scales"]), _p(inp["rotations"]),

@@ -108,7 +108,7 @@ size_t sort_scratch_layout(long long n, size_t* keys_tmp, size_t* vals_tmp, size
   const size_t nn = size_t(n > 0 ? n : 1);
   *keys_tmp = take(nn * 8);
   *vals_tmp = take(nn * 4);
-  *hist = take(size_t(kMaxPasses) * 256 * 4);
+  *hist = take(size_t(kMaxPasses) * kMaxBins * 4);
   *status = take(sort_status_words(n) * 4);
   *counters = take(kMaxPasses * 4);
   *err = take(4);

@@ -304,6 +304,8 @@ constexpr int kSortThreads = 256;
 constexpr int kSortItems = 16;
 constexpr int kSortTile = kSortThreads * kSortItems;  // 4096 keys per onesweep tile
 constexpr int kMaxPasses = 8;
+constexpr int kMaxDigitBits = 9;             // digit width: ceil(bits / ceil(bits / 9))
+constexpr int kMaxBins = 1 << kMaxDigitBits;
 
 struct BinLayout {
   size_t header, keysA, keysB, valsA, valsB, hist, status, tile_hist, total;
@@ -317,8 +319,8 @@ struct BinLayout {
     keysB = take(r * 8);
     valsA = take(r * 4);
     valsB = take(r * 4);
-    hist = take(size_t(kMaxPasses) * 256 * 4);
-    status = take(size_t(kMaxPasses) * sort_tiles * 256 * 4);
+    hist = take(size_t(kMaxPasses) * kMaxBins * 4);
+    status = take(size_t(kMaxPasses) * sort_tiles * kMaxBins * 4);
     tile_hist = take(size_t(num_tiles > 0 ? num_tiles : 1) * 4);
     total = align256(o);
   }

@@ -53,8 +53,9 @@ struct DuplicateArgs {
 void launch_duplicate(const DuplicateArgs& a, cudaStream_t stream);
 
 // LSD radix sort of packed keys (uint32 or uint64) with uint32 values over
-// key bits [begin_bit, begin_bit + bits); 8-bit digits, one onesweep launch per
-// digit.  Pass p writes keys_out when (passes - 1 - p) is even, else keys_tmp,
+// key bits [begin_bit, begin_bit + bits); digits of sort_digit_bits(bits) <= 9
+// bits (the last one narrower when bits is not a multiple), one onesweep launch
+// per digit.  Pass p writes keys_out when (passes - 1 - p) is even, else keys_tmp,
 // so the result lands in keys_out; keys_in must not be keys_out.
 // `tile_hist` (may be null) receives a histogram of key >> tile_shift over
 // num_tiles bins, and `ranges` (may be null) the per-bin [start, end).
@@ -69,8 +70,8 @@ struct SortArgs {
   uint32_t* vals_out;
   void* keys_tmp;          // ping-pong partner
   uint32_t* vals_tmp;
-  uint32_t* hist;        // [kMaxPasses * 256]
-  uint32_t* status;      // [kMaxPasses * sort_tiles * 256]
+  uint32_t* hist;        // [kMaxPasses * kMaxBins]
+  uint32_t* status;      // [kMaxPasses * sort_tiles * kMaxBins]
   uint32_t* counters;    // [kMaxPasses]
   uint32_t* error;
   int tile_shift;
@@ -79,6 +80,7 @@ struct SortArgs {
   uint2* ranges;
 };
 int sort_passes(int bits);
+int sort_digit_bits(int bits);
 void launch_sort(const SortArgs& a, cudaStream_t stream);
 size_t sort_status_words(long long n);
 

@@ -2,17 +2,21 @@
 // (replaces the reference's 32-pass 2-bit sort with a host round trip per pass,
 // prepareSort.cu:303-360, and the range kernel gaussianTiles.cu:6-33).
 //
-//   1. histogram kernel: one read of the keys gives the 256-bin digit
-//      histogram of every pass, plus the histogram of key >> tile_shift
-//      (the per-tile instance counts);
+// Digits are sort_digit_bits(bits) = ceil(bits / ceil(bits / 9)) wide (up to
+// 512 bins), so a 27-bit packed key takes 3 passes instead of 4 with 8-bit
+// digits; the last digit is narrower when bits is not a multiple.
+//
+//   1. histogram kernel: one read of the keys gives the digit histogram of
+//      every pass, plus the histogram of key >> tile_shift (the per-tile
+//      instance counts);
 //   2. offsets kernel: exclusive scans of those histograms; the tile scan is
 //      the per-tile [start, end) range table (empty tiles get (0, 0), as the
 //      reference's memset leaves them);
-//   3. one onesweep kernel per 8-bit digit: each CTA takes the next 4096-key
-//      tile (acquired through an atomic counter, so every earlier tile is
-//      already running), ranks its keys stably with warp-level match, publishes
-//      its per-digit counts and looks back over earlier tiles for their
-//      prefix (decoupled lookback), then scatters through shared memory so the
+//   3. one onesweep kernel per digit: each CTA takes the next 4096-key tile
+//      (acquired through an atomic counter, so every earlier tile is already
+//      running), ranks its keys stably with warp-level match, publishes its
+//      per-digit counts and looks back over earlier tiles for their prefix
+//      (decoupled lookback), then scatters through shared memory so the
 //      global stores are coalesced.  Every wait is bounded: a wait that runs
 //      out sets kErrTimeout and the kernel finishes without hanging.
 //
@@ -31,22 +35,31 @@ constexpr uint32_t kStatMask = (1u << 30) - 1u;
 constexpr int kHistThreads = 256;
 constexpr int kSmemTileBins = 8192;
 
+// Width of pass p's digit.
+__host__ __device__ __forceinline__ int pass_width(int p, int dbits, int bits) {
+  const int left = bits - p * dbits;
+  return left < dbits ? left : dbits;
+}
+
 template <typename K>
 __global__ void __launch_bounds__(kHistThreads)
-hist_kernel(const K* __restrict__ keys, long long n, int begin_bit, int passes, uint32_t* __restrict__ hist,
-            int tile_shift, int num_tiles, uint32_t* __restrict__ tile_hist) {
+hist_kernel(const K* __restrict__ keys, long long n, int begin_bit, int passes, int dbits, int bits,
+            uint32_t* __restrict__ hist, int tile_shift, int num_tiles, uint32_t* __restrict__ tile_hist) {
   extern __shared__ uint32_t smem[];
-  uint32_t* sh = smem;                      // passes * 256
-  uint32_t* st = smem + passes * 256;       // num_tiles when they fit
+  uint32_t* sh = smem;                      // passes * kMaxBins
+  uint32_t* st = smem + passes * kMaxBins;  // num_tiles when they fit
   const bool tiles_in_smem = tile_hist != nullptr && num_tiles <= kSmemTileBins;
-  for (int i = threadIdx.x; i < passes * 256; i += blockDim.x) sh[i] = 0;
+  for (int i = threadIdx.x; i < passes * kMaxBins; i += blockDim.x) sh[i] = 0;
   if (tiles_in_smem)
     for (int i = threadIdx.x; i < num_tiles; i += blockDim.x) st[i] = 0;
   __syncthreads();
   const long long stride = (long long)gridDim.x * blockDim.x;
   for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
     const K k = keys[i];
-    for (int p = 0; p < passes; ++p) atomicAdd(&sh[p * 256 + int((k >> (begin_bit + 8 * p)) & 255)], 1u);
+    for (int p = 0; p < passes; ++p) {
+      const uint32_t mask = (1u << pass_width(p, dbits, bits)) - 1u;
+      atomicAdd(&sh[p * kMaxBins + int((k >> (begin_bit + dbits * p)) & mask)], 1u);
+    }
     if (tile_hist != nullptr) {
       const uint32_t t = uint32_t(k >> tile_shift);
       if (t < uint32_t(num_tiles)) {
@@ -56,7 +69,7 @@ hist_kernel(const K* __restrict__ keys, long long n, int begin_bit, int passes, 
     }
   }
   __syncthreads();
-  for (int i = threadIdx.x; i < passes * 256; i += blockDim.x)
+  for (int i = threadIdx.x; i < passes * kMaxBins; i += blockDim.x)
     if (sh[i]) atomicAdd(&hist[i], sh[i]);
   if (tiles_in_smem)
     for (int i = threadIdx.x; i < num_tiles; i += blockDim.x)
@@ -98,9 +111,9 @@ offsets_kernel(uint32_t* hist, int passes, const uint32_t* tile_hist, int num_ti
   __shared__ uint32_t s_warp[32];
   __shared__ uint32_t s_carry;
   for (int p = 0; p < passes; ++p) {
-    const uint32_t v = threadIdx.x < 256 ? hist[p * 256 + threadIdx.x] : 0u;
+    const uint32_t v = threadIdx.x < kMaxBins ? hist[p * kMaxBins + threadIdx.x] : 0u;
     const uint32_t ex = block_exclusive_scan(v, s_warp, nullptr);
-    if (threadIdx.x < 256) hist[p * 256 + threadIdx.x] = ex;
+    if (threadIdx.x < kMaxBins) hist[p * kMaxBins + threadIdx.x] = ex;
     __syncthreads();
   }
   if (tile_hist == nullptr || ranges == nullptr) return;
@@ -119,15 +132,52 @@ offsets_kernel(uint32_t* hist, int passes, const uint32_t* tile_hist, int num_ti
   }
 }
 
+// Look back over earlier tiles for the exclusive prefixes of the adjacent
+// digits d, d + 1 (one 64-bit status load per tile while both are pending;
+// bounded wait).
+__device__ __forceinline__ uint2 lookback2(const uint32_t* status, long long tile, int d, uint32_t* err) {
+  uint32_t acc0 = 0, acc1 = 0, spins = 0;
+  long long t0 = tile - 1, t1 = tile - 1;
+  while (t0 >= 0 || t1 >= 0) {
+    uint32_t w0 = 0, w1 = 0;
+    if (t0 == t1) {
+      const unsigned long long w =
+          ld_acquire64(reinterpret_cast<const unsigned long long*>(status + t0 * kMaxBins + d));
+      w0 = uint32_t(w);
+      w1 = uint32_t(w >> 32);
+    } else {
+      if (t0 >= 0) w0 = ld_acquire(status + t0 * kMaxBins + d);
+      if (t1 >= 0) w1 = ld_acquire(status + t1 * kMaxBins + d + 1);
+    }
+    bool progressed = false;
+    if (t0 >= 0 && (w0 & ~kStatMask) != 0u) {
+      acc0 += w0 & kStatMask;
+      t0 = (w0 & ~kStatMask) == kStatInc ? -1 : t0 - 1;
+      progressed = true;
+    }
+    if (t1 >= 0 && (w1 & ~kStatMask) != 0u) {
+      acc1 += w1 & kStatMask;
+      t1 = (w1 & ~kStatMask) == kStatInc ? -1 : t1 - 1;
+      progressed = true;
+    }
+    if (!progressed && ++spins > kSpinLimit) {
+      atomicOr(err, kErrTimeout);
+      break;
+    }
+  }
+  return make_uint2(acc0, acc1);
+}
+
 template <typename K>
 __global__ void __launch_bounds__(kSortThreads, sizeof(K) == 4 ? 3 : 2)
 onesweep_kernel(const K* __restrict__ kin, const uint32_t* __restrict__ vin, K* __restrict__ kout,
-                uint32_t* __restrict__ vout, long long n, int shift, const uint32_t* __restrict__ digit_base,
-                uint32_t* status, uint32_t* counter, uint32_t* err) {
+                uint32_t* __restrict__ vout, long long n, int shift, int width,
+                const uint32_t* __restrict__ digit_base, uint32_t* status, uint32_t* counter, uint32_t* err) {
   constexpr int kWarps = kSortThreads / 32;
-  __shared__ uint32_t s_wcnt[kWarps][256];
-  __shared__ uint32_t s_excl[256];
-  __shared__ uint32_t s_gofs[256];
+  static_assert(kSortThreads * 2 >= kMaxBins, "at most two digits per thread");
+  __shared__ uint32_t s_wcnt[kWarps][kMaxBins];
+  __shared__ uint32_t s_excl[kMaxBins];
+  __shared__ uint32_t s_gofs[kMaxBins];
   __shared__ uint32_t s_warp[32];
   __shared__ uint32_t s_tile;
   extern __shared__ __align__(16) unsigned char s_dyn[];
@@ -135,8 +185,10 @@ onesweep_kernel(const K* __restrict__ kin, const uint32_t* __restrict__ vin, K* 
   uint32_t* s_vals = reinterpret_cast<uint32_t*>(s_dyn + sizeof(K) * kSortTile);
 
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int bins = 1 << width;
+  const uint32_t dmask = uint32_t(bins) - 1u;
   if (tid == 0) s_tile = atomicAdd(counter, 1u);
-  for (int i = tid; i < kWarps * 256; i += kSortThreads) (&s_wcnt[0][0])[i] = 0u;
+  for (int i = tid; i < kWarps * kMaxBins; i += kSortThreads) (&s_wcnt[0][0])[i] = 0u;
   __syncthreads();
   const long long tile = s_tile;
   const long long base = tile * kSortTile;
@@ -156,7 +208,7 @@ onesweep_kernel(const K* __restrict__ kin, const uint32_t* __restrict__ vin, K* 
   for (int i = 0; i < kSortItems; ++i) {
     const long long idx = base + warp * (32 * kSortItems) + i * 32 + lane;
     const bool valid = idx < n;
-    const uint32_t d = uint32_t(k[i] >> shift) & 255u;
+    const uint32_t d = uint32_t(k[i] >> shift) & dmask;
     const uint32_t peers = __match_any_sync(0xffffffffu, valid ? d : (0x10000u | uint32_t(lane)));
     const uint32_t before = valid ? s_wcnt[warp][d] : 0u;
     rank[i] = before + __popc(peers & lt);
@@ -166,51 +218,43 @@ onesweep_kernel(const K* __restrict__ kin, const uint32_t* __restrict__ vin, K* 
   }
   __syncthreads();
 
-  // per digit (one thread each): exclusive over warps, tile count, publish
-  uint32_t tile_cnt = 0;
-  {
-    const int d = tid;  // kSortThreads == 256 digits
-    uint32_t sum = 0;
+  // two adjacent digits per thread: exclusive over warps, tile counts, publish
+  const int d0 = 2 * tid, d1 = 2 * tid + 1;
+  uint32_t c0 = 0, c1 = 0;
+  if (d0 < bins) {
 #pragma unroll
     for (int w = 0; w < kWarps; ++w) {
-      const uint32_t c = s_wcnt[w][d];
-      s_wcnt[w][d] = sum;
-      sum += c;
+      const uint32_t x0 = s_wcnt[w][d0], x1 = s_wcnt[w][d1];
+      s_wcnt[w][d0] = c0;
+      s_wcnt[w][d1] = c1;
+      c0 += x0;
+      c1 += x1;
     }
-    tile_cnt = sum;
-    uint32_t* my = status + tile * 256 + d;
-    if (tile == 0) st_release(my, kStatInc | tile_cnt);
-    else st_release(my, kStatAgg | tile_cnt);
+    const uint32_t flag = tile == 0 ? kStatInc : kStatAgg;
+    st_release64(reinterpret_cast<unsigned long long*>(status + tile * kMaxBins + d0),
+                 (uint64_t(flag | c1) << 32) | (flag | c0));
   }
-  const uint32_t excl = block_exclusive_scan(tile_cnt, s_warp, nullptr);
-  {
-    const int d = tid;
-    s_excl[d] = excl;
-    uint32_t acc = 0;
+  const uint32_t excl = block_exclusive_scan(c0 + c1, s_warp, nullptr);
+  if (d0 < bins) {
+    s_excl[d0] = excl;
+    s_excl[d1] = excl + c0;
+    uint32_t a0 = 0, a1 = 0;
     if (tile > 0) {
-      long long t = tile - 1;
-      uint32_t spins = 0;
-      while (t >= 0) {
-        const uint32_t w = ld_acquire(status + t * 256 + d);
-        const uint32_t flag = w & ~kStatMask;
-        if (flag == 0u) {
-          if (++spins > kSpinLimit) { atomicOr(err, kErrTimeout); break; }
-          continue;
-        }
-        acc += w & kStatMask;
-        if (flag == kStatInc) break;
-        --t;
-      }
-      st_release(status + tile * 256 + d, kStatInc | (acc + tile_cnt));
+      const uint2 a = lookback2(status, tile, d0, err);
+      a0 = a.x;
+      a1 = a.y;
+      st_release64(reinterpret_cast<unsigned long long*>(status + tile * kMaxBins + d0),
+                   (uint64_t(kStatInc | (a1 + c1)) << 32) | (kStatInc | (a0 + c0)));
     }
-    s_gofs[d] = digit_base[d] + acc;
+    s_gofs[d0] = digit_base[d0] + a0;
+    s_gofs[d1] = digit_base[d1] + a1;
   }
   __syncthreads();
 #pragma unroll
   for (int i = 0; i < kSortItems; ++i) {
     const long long idx = base + warp * (32 * kSortItems) + i * 32 + lane;
     if (idx < n) {
-      const uint32_t d = uint32_t(k[i] >> shift) & 255u;
+      const uint32_t d = uint32_t(k[i] >> shift) & dmask;
       const uint32_t pos = s_excl[d] + s_wcnt[warp][d] + rank[i];
       s_keys[pos] = k[i];
       s_vals[pos] = v[i];
@@ -220,7 +264,7 @@ onesweep_kernel(const K* __restrict__ kin, const uint32_t* __restrict__ vin, K* 
   const int nvalid = int(min((long long)kSortTile, n - base));
   for (int j = tid; j < nvalid; j += kSortThreads) {
     const K key = s_keys[j];
-    const uint32_t d = uint32_t(key >> shift) & 255u;
+    const uint32_t d = uint32_t(key >> shift) & dmask;
     const long long out = (long long)s_gofs[d] + (j - (long long)s_excl[d]);
     if (out >= 0 && out < n) {
       kout[out] = key;
@@ -234,12 +278,14 @@ onesweep_kernel(const K* __restrict__ kin, const uint32_t* __restrict__ vin, K* 
 template <typename K>
 void run_sort(const SortArgs& a, cudaStream_t stream) {
   const int passes = sort_passes(a.bits);
+  const int dbits = sort_digit_bits(a.bits);
   const long long n = a.n;
   if (n <= 0) return;
   const long long tiles = (n + kSortTile - 1) / kSortTile;
-  cudaMemsetAsync(a.hist, 0, sizeof(uint32_t) * 256 * kMaxPasses, stream);
+  cudaMemsetAsync(a.hist, 0, sizeof(uint32_t) * kMaxBins * kMaxPasses, stream);
   cudaMemsetAsync(a.counters, 0, sizeof(uint32_t) * kMaxPasses, stream);
-  cudaMemsetAsync(a.status, 0, sizeof(uint32_t) * 256 * size_t(tiles) * size_t(passes > 0 ? passes : 1), stream);
+  cudaMemsetAsync(a.status, 0, sizeof(uint32_t) * kMaxBins * size_t(tiles) * size_t(passes > 0 ? passes : 1),
+                  stream);
   if (a.tile_hist) cudaMemsetAsync(a.tile_hist, 0, sizeof(uint32_t) * size_t(a.num_tiles), stream);
   if (passes > 0 || a.tile_hist) {
     int sms = 148;
@@ -247,12 +293,14 @@ void run_sort(const SortArgs& a, cudaStream_t stream) {
     long long want = (n + kHistThreads * 16 - 1) / (kHistThreads * 16);
     const int grid = int(max(1LL, min(want, (long long)sms * 8)));
     const bool tiles_in_smem = a.tile_hist != nullptr && a.num_tiles <= kSmemTileBins;
-    const size_t smem = sizeof(uint32_t) * (size_t(passes) * 256 + (tiles_in_smem ? size_t(a.num_tiles) : 0));
+    const size_t smem =
+        sizeof(uint32_t) * (size_t(passes) * kMaxBins + (tiles_in_smem ? size_t(a.num_tiles) : 0));
     if (smem > 48 * 1024)
       cudaFuncSetAttribute(hist_kernel<K>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
     stage_begin(kStSortHist, stream);
     hist_kernel<K><<<grid, kHistThreads, smem, stream>>>(reinterpret_cast<const K*>(a.keys_in), n, a.begin_bit,
-                                                         passes, a.hist, a.tile_shift, a.num_tiles, a.tile_hist);
+                                                         passes, dbits, a.bits, a.hist, a.tile_shift,
+                                                         a.num_tiles, a.tile_hist);
     offsets_kernel<<<1, 1024, 0, stream>>>(a.hist, passes, a.tile_hist, a.num_tiles, a.ranges);
     stage_end(kStSortHist, stream, 2);
   }
@@ -266,8 +314,8 @@ void run_sort(const SortArgs& a, cudaStream_t stream) {
     uint32_t* vout = to_out ? a.vals_out : a.vals_tmp;
     stage_begin(kStSortPass, stream);
     onesweep_kernel<K><<<int(tiles), kSortThreads, dyn, stream>>>(
-        kin, vin, kout, vout, n, a.begin_bit + 8 * p, a.hist + 256 * p, a.status + size_t(p) * 256 * size_t(tiles),
-        a.counters + p, a.error);
+        kin, vin, kout, vout, n, a.begin_bit + dbits * p, pass_width(p, dbits, a.bits), a.hist + kMaxBins * p,
+        a.status + size_t(p) * kMaxBins * size_t(tiles), a.counters + p, a.error);
     stage_end(kStSortPass, stream, 1);
     kin = kout;
     vin = vout;
@@ -280,11 +328,16 @@ void run_sort(const SortArgs& a, cudaStream_t stream) {
 
 }  // namespace
 
-int sort_passes(int bits) { return bits <= 0 ? 0 : (bits + 7) / 8; }
+int sort_passes(int bits) { return bits <= 0 ? 0 : (bits + kMaxDigitBits - 1) / kMaxDigitBits; }
+
+int sort_digit_bits(int bits) {
+  const int p = sort_passes(bits);
+  return p == 0 ? 0 : (bits + p - 1) / p;
+}
 
 size_t sort_status_words(long long n) {
   const long long tiles = (n + kSortTile - 1) / kSortTile;
-  return size_t(kMaxPasses) * 256 * size_t(tiles > 0 ? tiles : 1);
+  return size_t(kMaxPasses) * kMaxBins * size_t(tiles > 0 ? tiles : 1);
 }
 
 void launch_sort(const SortArgs& a, cudaStream_t stream) {
