@@ -14,7 +14,7 @@
 //      reference's memset leaves them);
 //   3. one onesweep kernel per digit: each CTA takes the next 4096-key tile
 //      (acquired through an atomic counter, so every earlier tile is already
-//      running), ranks its keys stably with warp-level match, publishes its
+//      running), ranks its keys stably with per-bit warp ballots, publishes its
 //      per-digit counts and looks back over earlier tiles for their prefix
 //      (decoupled lookback), then scatters through shared memory so the
 //      global stores are coalesced.  Every wait is bounded: a wait that runs
@@ -134,7 +134,9 @@ offsets_kernel(uint32_t* hist, int passes, const uint32_t* tile_hist, int num_ti
 
 // Look back over earlier tiles for the exclusive prefixes of the adjacent
 // digits d, d + 1 (one 64-bit status load per tile while both are pending;
-// bounded wait).
+// bounded wait).  Each status word carries its flag and count together and
+// nothing else written by its tile is read here, so relaxed loads and stores
+// suffice (no acquire/release ordering).
 __device__ __forceinline__ uint2 lookback2(const uint32_t* status, long long tile, int d, uint32_t* err) {
   uint32_t acc0 = 0, acc1 = 0, spins = 0;
   long long t0 = tile - 1, t1 = tile - 1;
@@ -142,12 +144,12 @@ __device__ __forceinline__ uint2 lookback2(const uint32_t* status, long long til
     uint32_t w0 = 0, w1 = 0;
     if (t0 == t1) {
       const unsigned long long w =
-          ld_acquire64(reinterpret_cast<const unsigned long long*>(status + t0 * kMaxBins + d));
+          ld_relaxed64(reinterpret_cast<const unsigned long long*>(status + t0 * kMaxBins + d));
       w0 = uint32_t(w);
       w1 = uint32_t(w >> 32);
     } else {
-      if (t0 >= 0) w0 = ld_acquire(status + t0 * kMaxBins + d);
-      if (t1 >= 0) w1 = ld_acquire(status + t1 * kMaxBins + d + 1);
+      if (t0 >= 0) w0 = ld_relaxed(status + t0 * kMaxBins + d);
+      if (t1 >= 0) w1 = ld_relaxed(status + t1 * kMaxBins + d + 1);
     }
     bool progressed = false;
     if (t0 >= 0 && (w0 & ~kStatMask) != 0u) {
@@ -204,21 +206,17 @@ onesweep_kernel(const K* __restrict__ kin, const uint32_t* __restrict__ vin, K* 
     k[i] = valid ? kin[idx] : K(0);
     v[i] = valid ? vin[idx] : 0u;
   }
+  // early counts: per-warp digit histograms, so the tile's counts are
+  // published before the ranking and successors find them sooner
 #pragma unroll
   for (int i = 0; i < kSortItems; ++i) {
     const long long idx = base + warp * (32 * kSortItems) + i * 32 + lane;
-    const bool valid = idx < n;
-    const uint32_t d = uint32_t(k[i] >> shift) & dmask;
-    const uint32_t peers = __match_any_sync(0xffffffffu, valid ? d : (0x10000u | uint32_t(lane)));
-    const uint32_t before = valid ? s_wcnt[warp][d] : 0u;
-    rank[i] = before + __popc(peers & lt);
-    __syncwarp();
-    if (valid && lane == __ffs(peers) - 1) s_wcnt[warp][d] = before + __popc(peers);
-    __syncwarp();
+    if (idx < n) atomicAdd(&s_wcnt[warp][uint32_t(k[i] >> shift) & dmask], 1u);
   }
   __syncthreads();
 
-  // two adjacent digits per thread: exclusive over warps, tile counts, publish
+  // two adjacent digits per thread: exclusive over warps (each warp's base
+  // within the digit), tile counts, publish
   const int d0 = 2 * tid, d1 = 2 * tid + 1;
   uint32_t c0 = 0, c1 = 0;
   if (d0 < bins) {
@@ -231,19 +229,48 @@ onesweep_kernel(const K* __restrict__ kin, const uint32_t* __restrict__ vin, K* 
       c1 += x1;
     }
     const uint32_t flag = tile == 0 ? kStatInc : kStatAgg;
-    st_release64(reinterpret_cast<unsigned long long*>(status + tile * kMaxBins + d0),
+    st_relaxed64(reinterpret_cast<unsigned long long*>(status + tile * kMaxBins + d0),
                  (uint64_t(flag | c1) << 32) | (flag | c0));
   }
-  const uint32_t excl = block_exclusive_scan(c0 + c1, s_warp, nullptr);
+  const uint32_t excl = block_exclusive_scan(c0 + c1, s_warp, nullptr);  // ends with a barrier
   if (d0 < bins) {
     s_excl[d0] = excl;
     s_excl[d1] = excl + c0;
+  }
+
+  // stable rank within the tile's digit: warp base + earlier items of the warp
+  // + earlier lanes of this item holding the same digit (one ballot per digit
+  // bit: constant cost whatever the number of distinct digits)
+#pragma unroll
+  for (int i = 0; i < kSortItems; ++i) {
+    const long long idx = base + warp * (32 * kSortItems) + i * 32 + lane;
+    const bool valid = idx < n;
+    const uint32_t d = uint32_t(k[i] >> shift) & dmask;
+    uint32_t pm = __ballot_sync(0xffffffffu, valid);
+#pragma unroll
+    for (int bt = 0; bt < kMaxDigitBits; ++bt) {
+      if (bt < width) {
+        const bool bit = (d >> bt) & 1u;
+        const uint32_t bal = __ballot_sync(0xffffffffu, bit);
+        pm &= bit ? bal : ~bal;
+      }
+    }
+    const uint32_t before = valid ? s_wcnt[warp][d] : 0u;
+    rank[i] = before + __popc(pm & lt);
+    __syncwarp();
+    if (valid && lane == __ffs(pm) - 1) s_wcnt[warp][d] = before + __popc(pm);
+    __syncwarp();
+  }
+
+  // exclusive prefix over earlier tiles (decoupled lookback), after the ranking
+  // so that predecessors have had that long to publish
+  if (d0 < bins) {
     uint32_t a0 = 0, a1 = 0;
     if (tile > 0) {
       const uint2 a = lookback2(status, tile, d0, err);
       a0 = a.x;
       a1 = a.y;
-      st_release64(reinterpret_cast<unsigned long long*>(status + tile * kMaxBins + d0),
+      st_relaxed64(reinterpret_cast<unsigned long long*>(status + tile * kMaxBins + d0),
                    (uint64_t(kStatInc | (a1 + c1)) << 32) | (kStatInc | (a0 + c0)));
     }
     s_gofs[d0] = digit_base[d0] + a0;
@@ -255,7 +282,7 @@ onesweep_kernel(const K* __restrict__ kin, const uint32_t* __restrict__ vin, K* 
     const long long idx = base + warp * (32 * kSortItems) + i * 32 + lane;
     if (idx < n) {
       const uint32_t d = uint32_t(k[i] >> shift) & dmask;
-      const uint32_t pos = s_excl[d] + s_wcnt[warp][d] + rank[i];
+      const uint32_t pos = s_excl[d] + rank[i];
       s_keys[pos] = k[i];
       s_vals[pos] = v[i];
     }
