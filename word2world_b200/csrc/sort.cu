@@ -170,10 +170,11 @@ __device__ __forceinline__ uint2 lookback2(const uint32_t* status, long long til
   return make_uint2(acc0, acc1);
 }
 
-template <typename K>
+// kWidth: this pass's digit width (compile-time, so the per-bit ballots unroll).
+template <typename K, int kWidth>
 __global__ void __launch_bounds__(kSortThreads, sizeof(K) == 4 ? 3 : 2)
 onesweep_kernel(const K* __restrict__ kin, const uint32_t* __restrict__ vin, K* __restrict__ kout,
-                uint32_t* __restrict__ vout, long long n, int shift, int width,
+                uint32_t* __restrict__ vout, long long n, int shift,
                 const uint32_t* __restrict__ digit_base, uint32_t* status, uint32_t* counter, uint32_t* err) {
   constexpr int kWarps = kSortThreads / 32;
   static_assert(kSortThreads * 2 >= kMaxBins, "at most two digits per thread");
@@ -187,7 +188,7 @@ onesweep_kernel(const K* __restrict__ kin, const uint32_t* __restrict__ vin, K* 
   uint32_t* s_vals = reinterpret_cast<uint32_t*>(s_dyn + sizeof(K) * kSortTile);
 
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const int bins = 1 << width;
+  constexpr int bins = 1 << kWidth;
   const uint32_t dmask = uint32_t(bins) - 1u;
   if (tid == 0) s_tile = atomicAdd(counter, 1u);
   for (int i = tid; i < kWarps * kMaxBins; i += kSortThreads) (&s_wcnt[0][0])[i] = 0u;
@@ -248,12 +249,10 @@ onesweep_kernel(const K* __restrict__ kin, const uint32_t* __restrict__ vin, K* 
     const uint32_t d = uint32_t(k[i] >> shift) & dmask;
     uint32_t pm = __ballot_sync(0xffffffffu, valid);
 #pragma unroll
-    for (int bt = 0; bt < kMaxDigitBits; ++bt) {
-      if (bt < width) {
-        const bool bit = (d >> bt) & 1u;
-        const uint32_t bal = __ballot_sync(0xffffffffu, bit);
-        pm &= bit ? bal : ~bal;
-      }
+    for (int bt = 0; bt < kWidth; ++bt) {
+      const bool bit = (d >> bt) & 1u;
+      const uint32_t bal = __ballot_sync(0xffffffffu, bit);
+      pm &= bit ? bal : ~bal;
     }
     const uint32_t before = valid ? s_wcnt[warp][d] : 0u;
     rank[i] = before + __popc(pm & lt);
@@ -302,6 +301,33 @@ onesweep_kernel(const K* __restrict__ kin, const uint32_t* __restrict__ vin, K* 
   }
 }
 
+template <typename K, int kWidth>
+void launch_onesweep_w(int tiles, cudaStream_t stream, const K* kin, const uint32_t* vin, K* kout, uint32_t* vout,
+                       long long n, int shift, const uint32_t* digit_base, uint32_t* status, uint32_t* counter,
+                       uint32_t* err) {
+  const size_t dyn = (sizeof(K) + sizeof(uint32_t)) * kSortTile;
+  cudaFuncSetAttribute(onesweep_kernel<K, kWidth>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(dyn));
+  onesweep_kernel<K, kWidth><<<tiles, kSortThreads, dyn, stream>>>(kin, vin, kout, vout, n, shift, digit_base,
+                                                                    status, counter, err);
+}
+
+template <typename K>
+void launch_onesweep(int width, int tiles, cudaStream_t stream, const K* kin, const uint32_t* vin, K* kout,
+                     uint32_t* vout, long long n, int shift, const uint32_t* digit_base, uint32_t* status,
+                     uint32_t* counter, uint32_t* err) {
+  switch (width) {
+#define W2W_ONESWEEP_CASE(W)                                                                                  \
+  case W:                                                                                                     \
+    launch_onesweep_w<K, W>(tiles, stream, kin, vin, kout, vout, n, shift, digit_base, status, counter, err); \
+    break;
+    W2W_ONESWEEP_CASE(1) W2W_ONESWEEP_CASE(2) W2W_ONESWEEP_CASE(3) W2W_ONESWEEP_CASE(4) W2W_ONESWEEP_CASE(5)
+    W2W_ONESWEEP_CASE(6) W2W_ONESWEEP_CASE(7) W2W_ONESWEEP_CASE(8) W2W_ONESWEEP_CASE(9)
+#undef W2W_ONESWEEP_CASE
+    default:
+      break;
+  }
+}
+
 template <typename K>
 void run_sort(const SortArgs& a, cudaStream_t stream) {
   const int passes = sort_passes(a.bits);
@@ -331,8 +357,6 @@ void run_sort(const SortArgs& a, cudaStream_t stream) {
     offsets_kernel<<<1, 1024, 0, stream>>>(a.hist, passes, a.tile_hist, a.num_tiles, a.ranges);
     stage_end(kStSortHist, stream, 2);
   }
-  const size_t dyn = (sizeof(K) + sizeof(uint32_t)) * kSortTile;
-  cudaFuncSetAttribute(onesweep_kernel<K>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(dyn));
   const K* kin = reinterpret_cast<const K*>(a.keys_in);
   const uint32_t* vin = a.vals_in;
   for (int p = 0; p < passes; ++p) {
@@ -340,9 +364,9 @@ void run_sort(const SortArgs& a, cudaStream_t stream) {
     K* kout = reinterpret_cast<K*>(to_out ? a.keys_out : a.keys_tmp);
     uint32_t* vout = to_out ? a.vals_out : a.vals_tmp;
     stage_begin(kStSortPass, stream);
-    onesweep_kernel<K><<<int(tiles), kSortThreads, dyn, stream>>>(
-        kin, vin, kout, vout, n, a.begin_bit + dbits * p, pass_width(p, dbits, a.bits), a.hist + kMaxBins * p,
-        a.status + size_t(p) * kMaxBins * size_t(tiles), a.counters + p, a.error);
+    launch_onesweep<K>(pass_width(p, dbits, a.bits), int(tiles), stream, kin, vin, kout, vout, n,
+                       a.begin_bit + dbits * p, a.hist + kMaxBins * p,
+                       a.status + size_t(p) * kMaxBins * size_t(tiles), a.counters + p, a.error);
     stage_end(kStSortPass, stream, 1);
     kin = kout;
     vin = vout;
