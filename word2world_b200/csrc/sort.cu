@@ -132,42 +132,54 @@ offsets_kernel(uint32_t* hist, int passes, const uint32_t* tile_hist, int num_ti
   }
 }
 
-// Look back over earlier tiles for the exclusive prefixes of the adjacent
-// digits d, d + 1 (one 64-bit status load per tile while both are pending;
-// bounded wait).  Each status word carries its flag and count together and
-// nothing else written by its tile is read here, so relaxed loads and stores
-// suffice (no acquire/release ordering).
+// Decoupled lookback for the adjacent digits d, d + 1.  Each step loads
+// kLookWindow predecessor status words per digit at once (relaxed loads: a
+// status word carries its flag and count together and nothing else written by
+// its tile is read here) and consumes them newest first: aggregates add up
+// until an inclusive prefix ends the walk; a tile that has not published yet
+// stops the step, which resumes there.  Bounded wait.
+constexpr int kLookWindow = 2;
+
+struct LookWalk {
+  long long t;  // next predecessor to read (-1: finished)
+  uint32_t acc;
+  // Consume window w (tiles t, t-1, ...); returns whether the walk advanced.
+  __device__ __forceinline__ bool consume(const uint32_t (&w)[kLookWindow]) {
+    const long long t0 = t;
+    bool stop = t < 0;
+#pragma unroll
+    for (int i = 0; i < kLookWindow; ++i) {
+      const uint32_t flag = w[i] & ~kStatMask;
+      if (!stop && flag != 0u) {
+        acc += w[i] & kStatMask;
+        t = flag == kStatInc ? -1 : t - 1;
+        stop = t < 0;
+      } else {
+        stop = true;
+      }
+    }
+    return t != t0;
+  }
+};
+
 __device__ __forceinline__ uint2 lookback2(const uint32_t* status, long long tile, int d, uint32_t* err) {
-  uint32_t acc0 = 0, acc1 = 0, spins = 0;
-  long long t0 = tile - 1, t1 = tile - 1;
-  while (t0 >= 0 || t1 >= 0) {
-    uint32_t w0 = 0, w1 = 0;
-    if (t0 == t1) {
-      const unsigned long long w =
-          ld_relaxed64(reinterpret_cast<const unsigned long long*>(status + t0 * kMaxBins + d));
-      w0 = uint32_t(w);
-      w1 = uint32_t(w >> 32);
-    } else {
-      if (t0 >= 0) w0 = ld_relaxed(status + t0 * kMaxBins + d);
-      if (t1 >= 0) w1 = ld_relaxed(status + t1 * kMaxBins + d + 1);
+  LookWalk a{tile - 1, 0u}, b{tile - 1, 0u};
+  uint32_t spins = 0;
+  while (a.t >= 0 || b.t >= 0) {
+    uint32_t wa[kLookWindow], wb[kLookWindow];
+#pragma unroll
+    for (int i = 0; i < kLookWindow; ++i) {
+      wa[i] = a.t - i >= 0 ? ld_relaxed(status + (a.t - i) * kMaxBins + d) : 0u;
+      wb[i] = b.t - i >= 0 ? ld_relaxed(status + (b.t - i) * kMaxBins + d + 1) : 0u;
     }
-    bool progressed = false;
-    if (t0 >= 0 && (w0 & ~kStatMask) != 0u) {
-      acc0 += w0 & kStatMask;
-      t0 = (w0 & ~kStatMask) == kStatInc ? -1 : t0 - 1;
-      progressed = true;
-    }
-    if (t1 >= 0 && (w1 & ~kStatMask) != 0u) {
-      acc1 += w1 & kStatMask;
-      t1 = (w1 & ~kStatMask) == kStatInc ? -1 : t1 - 1;
-      progressed = true;
-    }
-    if (!progressed && ++spins > kSpinLimit) {
+    const bool moved_a = a.consume(wa);
+    const bool moved_b = b.consume(wb);
+    if (!moved_a && !moved_b && ++spins > kSpinLimit) {
       atomicOr(err, kErrTimeout);
       break;
     }
   }
-  return make_uint2(acc0, acc1);
+  return make_uint2(a.acc, b.acc);
 }
 
 // kWidth: this pass's digit width (compile-time, so the per-bit ballots unroll).
