@@ -80,18 +80,18 @@ struct BwdPixel {
   bool inside;
   size_t pix, hw;
   uint2 range;
-  int nmax;
+  int walk;  // list positions [0, walk) may hold contributors of this warp's pixels
   uint32_t last, warp_last;
   float dLp0 = 0.f, dLp1 = 0.f, dLp2 = 0.f, dLd = 0.f, dLa = 0.f;
   __device__ __forceinline__ explicit BwdPixel(const BackwardArgs& a)
       : tile(int(a.order[blockIdx.x])), tp(tile, (a.W + kTile - 1) / kTile) {
     inside = tp.px < a.W && tp.py < a.H;
     range = a.ranges[tile];
-    nmax = int(min(a.tile_max[tile], range.y - range.x));
     pix = inside ? size_t(tp.py) * a.W + tp.px : 0;
     hw = size_t(a.W) * a.H;
     last = inside ? a.n_contrib[pix] : 0u;
     warp_last = __reduce_max_sync(0xffffffffu, last);
+    walk = int(min(warp_last, range.y - range.x));
     if (inside) {
       dLp0 = a.dL_dcolor[pix];
       dLp1 = a.dL_dcolor[hw + pix];
@@ -166,7 +166,7 @@ __device__ __forceinline__ bool ref_eval(float4 q0, float4 q1, float4 q2, float 
 }
 
 __global__ void __launch_bounds__(kBlendThreads, 2) render_ref_kernel(BackwardArgs a) {
-  __shared__ TileWalkShared sm;
+  __shared__ WarpChunk s_chunk[kBlendThreads / 32];
   const BwdPixel p(a);
   RefChain ch;
   ch.T_final = p.inside ? 1.0f - a.out_alpha[p.pix] : 0.0f;
@@ -175,45 +175,43 @@ __global__ void __launch_bounds__(kBlendThreads, 2) render_ref_kernel(BackwardAr
   const float ddelx_dx = 0.5f * float(a.W), ddely_dy = 0.5f * float(a.H);
   const float pxf = float(p.tp.px), pyf = float(p.tp.py);
   const Target tgt = lane_target(a, 0);
-  const int nb = (p.nmax + kBatch - 1) / kBatch;
-  Staged st;
-  // batch b holds list positions hi-1, hi-2, ..., hi-cnt (hi = nmax - b*kBatch)
-  if (nb > 0) {
-    stage_load(st, a.bwd_record, a.point_list, p.range.x + p.nmax - 1 - threadIdx.x, int(threadIdx.x) < p.nmax);
-    stage_store(sm, 0, st, p.tp.X0, p.tp.Y0);
+  WarpChunk& wc = s_chunk[p.tp.warp];
+  // back to front: chunk c holds list positions walk-1-32c, walk-2-32c, ... (lane j: walk-1-32c-j)
+  const int nc = (p.walk + kChunk - 1) / kChunk;
+  ChunkLoad ld;
+  uint32_t reach = 0;
+  if (nc > 0) {
+    chunk_load(ld, a.bwd_record, a.point_list, p.range.x + p.walk - 1 - p.tp.lane, p.tp.lane < p.walk);
+    reach = chunk_store(wc, ld, p.tp.bx, p.tp.by);
   }
-  for (int b = 0; b < nb; ++b) {
-    const int cur = b & 1;
-    const int hi = p.nmax - b * kBatch;
-    __syncthreads();
-    const int hn = hi - kBatch;
-    if (b + 1 < nb) stage_load(st, a.bwd_record, a.point_list, p.range.x + hn - 1 - threadIdx.x,
-                               int(threadIdx.x) < hn);
-    // entries j < hi - warp_last sit at or past every contributor count of the warp
-    const int start = hi - int(p.warp_last);
-    if (start < kBatch) {
-      const float4* s = sm.rec[cur];
-      const uint32_t* ids = sm.id[cur];
-      const int cnt = build_list(sm, cur, p.tp.warp, p.tp.lane, start > 0 ? start : 0);
-      const uint8_t* lst = sm.list[p.tp.warp];
-      for (int k0 = 0; k0 < cnt; k0 += 2) {
-        const int j0 = lst[k0];
-        const bool has1 = k0 + 1 < cnt;
-        const int j1 = has1 ? int(lst[k0 + 1]) : j0;
-        const float4 a0 = s[kRecVec * j0], a1 = s[kRecVec * j0 + 1], a2 = s[kRecVec * j0 + 2];
-        const float4 b0 = s[kRecVec * j1], b1 = s[kRecVec * j1 + 1], b2 = s[kRecVec * j1 + 2];
-        float dx0, dy0, G0, al0, dx1, dy1, G1, al1;
-        const bool ok0 = ref_eval(a0, a1, a2, pxf, pyf, dx0, dy0, G0, al0) && uint32_t(hi - 1 - j0) < p.last;
-        const bool ok1 = ref_eval(b0, b1, b2, pxf, pyf, dx1, dy1, G1, al1) && has1 &&
-                         uint32_t(hi - 1 - j1) < p.last;
-        float c0[kValues], c1[kValues];
-        ch.step(ok0, p, a0, a1, a2, dx0, dy0, G0, al0, ddelx_dx, ddely_dy, c0);
-        ch.step(ok1, p, b0, b1, b2, dx1, dy1, G1, al1, ddelx_dx, ddely_dy, c1);
-        flush(c0, ok0, ids[j0], tgt);
-        flush(c1, ok1, ids[j1], tgt);
-      }
+  for (int c = 0; c < nc; ++c) {
+    const int hi = p.walk - c * kChunk;  // chunk entry j is list position hi - 1 - j
+    const int hn = hi - kChunk;
+    const bool more = c + 1 < nc;
+    if (more) chunk_load(ld, a.bwd_record, a.point_list, p.range.x + hn - 1 - p.tp.lane, p.tp.lane < hn);
+    const float4* s = wc.rec;
+    uint32_t bits = reach;
+    while (bits != 0u) {
+      const int j0 = pop_entry(bits);
+      const int j1r = pop_entry(bits);
+      const bool has1 = j1r >= 0;
+      const int j1 = has1 ? j1r : j0;
+      const float4 a0 = s[kRecVec * j0], a1 = s[kRecVec * j0 + 1], a2 = s[kRecVec * j0 + 2];
+      const float4 b0 = s[kRecVec * j1], b1 = s[kRecVec * j1 + 1], b2 = s[kRecVec * j1 + 2];
+      float dx0, dy0, G0, al0, dx1, dy1, G1, al1;
+      const bool ok0 = ref_eval(a0, a1, a2, pxf, pyf, dx0, dy0, G0, al0) && uint32_t(hi - 1 - j0) < p.last;
+      const bool ok1 = ref_eval(b0, b1, b2, pxf, pyf, dx1, dy1, G1, al1) && has1 &&
+                       uint32_t(hi - 1 - j1) < p.last;
+      float c0[kValues], c1[kValues];
+      ch.step(ok0, p, a0, a1, a2, dx0, dy0, G0, al0, ddelx_dx, ddely_dy, c0);
+      ch.step(ok1, p, b0, b1, b2, dx1, dy1, G1, al1, ddelx_dx, ddely_dy, c1);
+      flush(c0, ok0, wc.id[j0], tgt);
+      flush(c1, ok1, wc.id[j1], tgt);
     }
-    if (b + 1 < nb) stage_store(sm, cur ^ 1, st, p.tp.X0, p.tp.Y0);
+    if (more) {
+      __syncwarp();
+      reach = chunk_store(wc, ld, p.tp.bx, p.tp.by);
+    }
   }
 }
 
@@ -275,7 +273,7 @@ struct ExactChain {
 };
 
 __global__ void __launch_bounds__(kBlendThreads, 2) render_exact_kernel(BackwardArgs a) {
-  __shared__ TileWalkShared sm;
+  __shared__ WarpChunk s_chunk[kBlendThreads / 32];
   const BwdPixel p(a);
   ExactChain ch;
   const float Tf = p.inside ? a.T_final[p.pix] : 0.0f;
@@ -286,54 +284,54 @@ __global__ void __launch_bounds__(kBlendThreads, 2) render_exact_kernel(Backward
   const float hW = 0.5f * float(a.W), hH = 0.5f * float(a.H);
   const float pxf = float(p.tp.px), pyf = float(p.tp.py);
   const Target tgt = lane_target(a, 1);
-  const int nb = (p.nmax + kBatch - 1) / kBatch;
-  Staged st;
-  if (nb > 0) {
-    stage_load(st, a.record, a.point_list, p.range.x + p.nmax - 1 - threadIdx.x, int(threadIdx.x) < p.nmax);
-    stage_store(sm, 0, st, p.tp.X0, p.tp.Y0);
+  WarpChunk& wc = s_chunk[p.tp.warp];
+  const int nc = (p.walk + kChunk - 1) / kChunk;
+  ChunkLoad ld;
+  uint32_t reach = 0;
+  if (nc > 0) {
+    chunk_load(ld, a.record, a.point_list, p.range.x + p.walk - 1 - p.tp.lane, p.tp.lane < p.walk);
+    reach = chunk_store(wc, ld, p.tp.bx, p.tp.by);
   }
-  for (int b = 0; b < nb; ++b) {
-    const int cur = b & 1;
-    const int hi = p.nmax - b * kBatch;
-    __syncthreads();
-    const int hn = hi - kBatch;
-    if (b + 1 < nb) stage_load(st, a.record, a.point_list, p.range.x + hn - 1 - threadIdx.x, int(threadIdx.x) < hn);
-    const int start = hi - int(p.warp_last);
-    if (start < kBatch) {
-      const float4* s = sm.rec[cur];
-      const uint32_t* ids = sm.id[cur];
-      const int cnt = build_list(sm, cur, p.tp.warp, p.tp.lane, start > 0 ? start : 0);
-      const uint8_t* lst = sm.list[p.tp.warp];
-      for (int k0 = 0; k0 < cnt; k0 += 2) {
-        const int j0 = lst[k0];
-        const bool has1 = k0 + 1 < cnt;
-        const int j1 = has1 ? int(lst[k0 + 1]) : j0;
-        const float4 a0 = s[kRecVec * j0], a1 = s[kRecVec * j0 + 1];
-        const float4 b0 = s[kRecVec * j1], b1 = s[kRecVec * j1 + 1];
-        const float n0 = gauss_num_fwd(pxf, pyf, a0.x, a0.y, a0.z, a0.w, a1.x);
-        const float n1 = gauss_num_fwd(pxf, pyf, b0.x, b0.y, b0.z, b0.w, b1.x);
-        float m0, m1;
-        if (__all_sync(0xffffffffu, div_in_range(n0, a1.y) && div_in_range(n1, b1.y))) {
-          m0 = div_markstein(n0, a1.y);
-          m1 = div_markstein(n1, b1.y);
-        } else {
-          m0 = div(n0, a1.y);
-          m1 = div(n1, b1.y);
-        }
-        const float g0 = expf(mul(-0.5f, m0 < 0.0f ? 1000.0f : m0));
-        const float g1 = expf(mul(-0.5f, m1 < 0.0f ? 1000.0f : m1));
-        const float og0 = mul(a1.z, g0), og1 = mul(b1.z, g1);
-        const float al0 = fminf(0.99f, og0), al1 = fminf(0.99f, og1);
-        const bool ok0 = al0 >= 1.0f / 255.0f && uint32_t(hi - 1 - j0) < p.last;
-        const bool ok1 = al1 >= 1.0f / 255.0f && has1 && uint32_t(hi - 1 - j1) < p.last;
-        float c0[kValues], c1[kValues];
-        ch.step(ok0, p, a0, a1, s[kRecVec * j0 + 2], pxf, pyf, g0, og0, al0, m0, hW, hH, c0);
-        ch.step(ok1, p, b0, b1, s[kRecVec * j1 + 2], pxf, pyf, g1, og1, al1, m1, hW, hH, c1);
-        flush(c0, ok0, ids[j0], tgt);
-        flush(c1, ok1, ids[j1], tgt);
+  for (int c = 0; c < nc; ++c) {
+    const int hi = p.walk - c * kChunk;
+    const int hn = hi - kChunk;
+    const bool more = c + 1 < nc;
+    if (more) chunk_load(ld, a.record, a.point_list, p.range.x + hn - 1 - p.tp.lane, p.tp.lane < hn);
+    const float4* s = wc.rec;
+    uint32_t bits = reach;
+    while (bits != 0u) {
+      const int j0 = pop_entry(bits);
+      const int j1r = pop_entry(bits);
+      const bool has1 = j1r >= 0;
+      const int j1 = has1 ? j1r : j0;
+      const float4 a0 = s[kRecVec * j0], a1 = s[kRecVec * j0 + 1];
+      const float4 b0 = s[kRecVec * j1], b1 = s[kRecVec * j1 + 1];
+      const float n0 = gauss_num_fwd(pxf, pyf, a0.x, a0.y, a0.z, a0.w, a1.x);
+      const float n1 = gauss_num_fwd(pxf, pyf, b0.x, b0.y, b0.z, b0.w, b1.x);
+      float m0, m1;
+      if (__all_sync(0xffffffffu, div_in_range(n0, a1.y) && div_in_range(n1, b1.y))) {
+        m0 = div_markstein(n0, a1.y);
+        m1 = div_markstein(n1, b1.y);
+      } else {
+        m0 = div(n0, a1.y);
+        m1 = div(n1, b1.y);
       }
+      const float g0 = expf(mul(-0.5f, m0 < 0.0f ? 1000.0f : m0));
+      const float g1 = expf(mul(-0.5f, m1 < 0.0f ? 1000.0f : m1));
+      const float og0 = mul(a1.z, g0), og1 = mul(b1.z, g1);
+      const float al0 = fminf(0.99f, og0), al1 = fminf(0.99f, og1);
+      const bool ok0 = al0 >= 1.0f / 255.0f && uint32_t(hi - 1 - j0) < p.last;
+      const bool ok1 = al1 >= 1.0f / 255.0f && has1 && uint32_t(hi - 1 - j1) < p.last;
+      float c0[kValues], c1[kValues];
+      ch.step(ok0, p, a0, a1, s[kRecVec * j0 + 2], pxf, pyf, g0, og0, al0, m0, hW, hH, c0);
+      ch.step(ok1, p, b0, b1, s[kRecVec * j1 + 2], pxf, pyf, g1, og1, al1, m1, hW, hH, c1);
+      flush(c0, ok0, wc.id[j0], tgt);
+      flush(c1, ok1, wc.id[j1], tgt);
     }
-    if (b + 1 < nb) stage_store(sm, cur ^ 1, st, p.tp.X0, p.tp.Y0);
+    if (more) {
+      __syncwarp();
+      reach = chunk_store(wc, ld, p.tp.bx, p.tp.by);
+    }
   }
 }
 

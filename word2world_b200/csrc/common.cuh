@@ -197,6 +197,20 @@ __device__ __forceinline__ uint32_t block_mask(float mx, float my, float hy, flo
   return m;
 }
 
+// Whether the Gaussian may reach alpha >= 1/255 in the 8x4 block whose
+// top-left pixel is (bx, by): block_mask's test for one block.
+__device__ __forceinline__ bool block_test(float mx, float my, float hy, float beta, float gamma, float eps, float vr,
+                                           int bx, int by) {
+  if (!(hy >= 0.0f && hy < 1e30f)) return !(hy < 0.0f);
+  const float ux = float(bx) - mx, vy = float(by) - my;
+  const float v0 = vy - kCullPad, v1 = vy + (3.0f + kCullPad);
+  const float a = fmaxf(v0, -hy), b = fminf(v1, hy);
+  const float vR = fminf(fmaxf(vr, a), b), vL = fminf(fmaxf(-vr, a), b);
+  const float R = sqrt_approx(fmaxf(0.0f, gamma - eps * vR * vR)) - beta * vR;
+  const float L = -sqrt_approx(fmaxf(0.0f, gamma - eps * vL * vL)) - beta * vL;
+  return a <= b && L <= ux + (7.0f + kCullPad) && R >= ux - kCullPad;
+}
+
 // ---------------------------------------------------------------------------
 // Per-Gaussian blend record (forward blend and exact backward), 64 bytes.
 // The first 48 bytes are what the per-pixel loops read from shared memory;

@@ -3,14 +3,19 @@
 //
 // A CTA of 256 threads owns one 16x16 tile; warp w owns the 8x4 pixel block
 // w (columns 8*(w & 1) .. +7, rows 4*(w >> 1) .. +3), lane l its pixel
-// (l & 7, l >> 3) inside the block.  The tile's list is staged kBatch entries
-// at a time, double-buffered: each thread gathers one entry's 64-byte record
-// by Gaussian id into registers while the warps walk the previous batch, then
-// stores the record's first 48 bytes to shared memory and computes the
-// entry's 8-bit block mask (block_mask in common.cuh).  One ballot per block
-// bit turns the masks into, per block, eight 32-bit words of "this entry can
-// reach my block" flags; each warp expands its own words into a list of entry
-// indices (build_list) and walks only those, in list order.
+// (l & 7, l >> 3) inside the block.
+//
+// Independent warps (backward passes): each warp walks the tile's list on its
+// own, down from its pixels' largest contributor count, kChunk entries at a
+// time: lane j gathers entry j's 64-byte record by
+// Gaussian id (the tile's warps gather the same records, so after the first
+// they come from L1), tests whether the Gaussian can reach the warp's block
+// with alpha >= 1/255 (block_test in common.cuh) and stores the record's first
+// 48 bytes to the warp's shared-memory slot; the ballot of the tests is the
+// list of entries the warp evaluates, in list order.  The next chunk's records
+// are gathered while the current one is walked.  Warps never wait for one
+// another: a warp whose block has little to do, or whose pixels have all
+// terminated, finishes early instead of idling at a per-batch barrier.
 #pragma once
 
 #include "common.cuh"
@@ -18,7 +23,91 @@
 namespace w2w {
 
 constexpr int kRecVec = 3;  // float4s of a record staged in shared memory
+constexpr int kChunk = 32;  // list entries staged per warp step (one per lane)
 
+struct WarpChunk {
+  float4 rec[kChunk * kRecVec];
+  uint32_t id[kChunk];
+};
+
+// Pixel of this thread in tile `tile` of a grid `gw` tiles wide.
+struct TilePixel {
+  int X0, Y0, px, py, warp, lane, bx, by;  // (bx, by): top-left pixel of the warp's block
+  __device__ __forceinline__ TilePixel(int tile, int gw) {
+    warp = threadIdx.x >> 5;
+    lane = threadIdx.x & 31;
+    X0 = (tile % gw) * kTile;
+    Y0 = (tile / gw) * kTile;
+    bx = X0 + kBlockW * (warp & 1);
+    by = Y0 + kBlockH * (warp >> 1);
+    px = bx + (lane & 7);
+    py = by + (lane >> 3);
+  }
+};
+
+// Tiles are processed heaviest first: CTA b takes tile order[b], where order
+// lists the tiles by decreasing list length (tile_order_kernel), so the
+// longest lists start in the first wave instead of wherever the raster order
+// puts them.
+__global__ void tile_order_kernel(const uint2* ranges, int num_tiles, uint32_t* order);
+
+// One entry's record held in registers between its gather and its store.
+struct ChunkLoad {
+  float4 r0, r1, r2, r3;
+  uint32_t id;
+  bool has;
+};
+
+// Gather entry `pos` of the point list (when `has`).  Records are four float4s;
+// r2.w and r3 hold the culling parameters (hy; beta, gamma, eps, vr).
+__device__ __forceinline__ void chunk_load(ChunkLoad& st, const float* record, const uint32_t* point_list, size_t pos,
+                                           bool has) {
+  st.has = has;
+  if (has) {
+    const float4* rec = reinterpret_cast<const float4*>(record);
+    st.id = point_list[pos];
+    const float4* r = rec + 4 * size_t(st.id);
+    st.r0 = __ldg(r);
+    st.r1 = __ldg(r + 1);
+    st.r2 = __ldg(r + 2);
+    st.r3 = __ldg(r + 3);
+  }
+}
+
+// Store lane j's gathered entry in slot j and return the ballot of "may reach
+// the block at (bx, by)".  Warp-collective; the caller has synchronised the
+// warp after its last read of the previous chunk.
+__device__ __forceinline__ uint32_t chunk_store(WarpChunk& c, const ChunkLoad& st, int bx, int by) {
+  const int lane = threadIdx.x & 31;
+  bool reach = false;
+  if (st.has) {
+    float4* s = &c.rec[kRecVec * lane];
+    s[0] = st.r0;
+    s[1] = st.r1;
+    s[2] = st.r2;
+    c.id[lane] = st.id;
+    reach = block_test(st.r0.x, st.r0.y, st.r2.w, st.r3.x, st.r3.y, st.r3.z, st.r3.w, bx, by);
+  }
+  __syncwarp();
+  return __ballot_sync(0xffffffffu, reach);
+}
+
+// Next set bit of `bits` (cleared), or -1.
+__device__ __forceinline__ int pop_entry(uint32_t& bits) {
+  if (bits == 0u) return -1;
+  const int j = __ffs(bits) - 1;
+  bits &= bits - 1u;
+  return j;
+}
+
+// ---------------------------------------------------------------------------
+// Cooperative batches (forward blend): the CTA stages kBatch entries at a time,
+// one per thread, double-buffered, with all 8 block bits computed once per
+// entry (block_mask); each warp expands its bits into an entry list
+// (build_list).  The blend walks far past most contributors (until every pixel
+// terminates), so sharing each entry's gather and test among the tile's warps
+// matters more there than letting warps run apart.
+// ---------------------------------------------------------------------------
 struct TileWalkShared {
   float4 rec[2][kBatch * kRecVec];
   uint32_t id[2][kBatch];
@@ -43,25 +132,6 @@ __device__ __forceinline__ int build_list(TileWalkShared& sm, int buf, int warp,
   __syncwarp();
   return count;
 }
-
-// Pixel of this thread in tile `tile` of a grid `gw` tiles wide.
-struct TilePixel {
-  int X0, Y0, px, py, warp, lane;
-  __device__ __forceinline__ TilePixel(int tile, int gw) {
-    warp = threadIdx.x >> 5;
-    lane = threadIdx.x & 31;
-    X0 = (tile % gw) * kTile;
-    Y0 = (tile / gw) * kTile;
-    px = X0 + kBlockW * (warp & 1) + (lane & 7);
-    py = Y0 + kBlockH * (warp >> 1) + (lane >> 3);
-  }
-};
-
-// Tiles are processed heaviest first: CTA b takes tile order[b], where order
-// lists the tiles by decreasing list length (tile_order_kernel), so the
-// longest lists start in the first wave instead of wherever the raster order
-// puts them.
-__global__ void tile_order_kernel(const uint2* ranges, int num_tiles, uint32_t* order);
 
 // One entry's record held in registers between its gather and its store.
 struct Staged {
