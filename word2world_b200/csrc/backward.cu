@@ -25,6 +25,10 @@ namespace w2w {
 namespace {
 
 constexpr int kValues = 10;
+// Warps (8x4 blocks) per CTA in the per-pixel passes.  The warps walk
+// independently; keeping a tile's eight on one SM lets them share the record
+// gathers through L1 (1, 2 and 4 warps per CTA measured slower).
+constexpr int kBwdWarps = 8;
 
 // Where each of the ten per-entry sums goes: after the transposed reduction
 // below, lane L (L even) holds the warp's sum of value (L >> 1); lanes 0..18
@@ -83,8 +87,10 @@ struct BwdPixel {
   int walk;  // list positions [0, walk) may hold contributors of this warp's pixels
   uint32_t last, warp_last;
   float dLp0 = 0.f, dLp1 = 0.f, dLp2 = 0.f, dLd = 0.f, dLa = 0.f;
+  // CTA b covers kBwdWarps of the 8 blocks of tile order[b / (8 / kBwdWarps)]
   __device__ __forceinline__ explicit BwdPixel(const BackwardArgs& a)
-      : tile(int(a.order[blockIdx.x])), tp(tile, (a.W + kTile - 1) / kTile) {
+      : tile(int(a.order[blockIdx.x / (8 / kBwdWarps)])),
+        tp(tile, (a.W + kTile - 1) / kTile, int(blockIdx.x % (8 / kBwdWarps)) * kBwdWarps + int(threadIdx.x >> 5)) {
     inside = tp.px < a.W && tp.py < a.H;
     range = a.ranges[tile];
     pix = inside ? size_t(tp.py) * a.W + tp.px : 0;
@@ -165,8 +171,8 @@ __device__ __forceinline__ bool ref_eval(float4 q0, float4 q1, float4 q2, float 
   return power <= 0.0f && power >= q2.z && alpha >= 1.0f / 255.0f;
 }
 
-__global__ void __launch_bounds__(kBlendThreads, 2) render_ref_kernel(BackwardArgs a) {
-  __shared__ WarpChunk s_chunk[kBlendThreads / 32];
+__global__ void __launch_bounds__(32 * kBwdWarps, 16 / kBwdWarps) render_ref_kernel(BackwardArgs a) {
+  __shared__ WarpChunk s_chunk[kBwdWarps];
   const BwdPixel p(a);
   RefChain ch;
   ch.T_final = p.inside ? 1.0f - a.out_alpha[p.pix] : 0.0f;
@@ -175,7 +181,7 @@ __global__ void __launch_bounds__(kBlendThreads, 2) render_ref_kernel(BackwardAr
   const float ddelx_dx = 0.5f * float(a.W), ddely_dy = 0.5f * float(a.H);
   const float pxf = float(p.tp.px), pyf = float(p.tp.py);
   const Target tgt = lane_target(a, 0);
-  WarpChunk& wc = s_chunk[p.tp.warp];
+  WarpChunk& wc = s_chunk[threadIdx.x >> 5];
   // back to front: chunk c holds list positions walk-1-32c, walk-2-32c, ... (lane j: walk-1-32c-j)
   const int nc = (p.walk + kChunk - 1) / kChunk;
   ChunkLoad ld;
@@ -272,8 +278,8 @@ struct ExactChain {
   }
 };
 
-__global__ void __launch_bounds__(kBlendThreads, 2) render_exact_kernel(BackwardArgs a) {
-  __shared__ WarpChunk s_chunk[kBlendThreads / 32];
+__global__ void __launch_bounds__(32 * kBwdWarps, 16 / kBwdWarps) render_exact_kernel(BackwardArgs a) {
+  __shared__ WarpChunk s_chunk[kBwdWarps];
   const BwdPixel p(a);
   ExactChain ch;
   const float Tf = p.inside ? a.T_final[p.pix] : 0.0f;
@@ -284,7 +290,7 @@ __global__ void __launch_bounds__(kBlendThreads, 2) render_exact_kernel(Backward
   const float hW = 0.5f * float(a.W), hH = 0.5f * float(a.H);
   const float pxf = float(p.tp.px), pyf = float(p.tp.py);
   const Target tgt = lane_target(a, 1);
-  WarpChunk& wc = s_chunk[p.tp.warp];
+  WarpChunk& wc = s_chunk[threadIdx.x >> 5];
   const int nc = (p.walk + kChunk - 1) / kChunk;
   ChunkLoad ld;
   uint32_t reach = 0;
@@ -352,14 +358,26 @@ __device__ __forceinline__ int sh_stride(int M) {
 // Rows [i0, i0 + n) of shs ([P, M, 3]), first min(M, 16) coefficients, into
 // s (row g at g * stride).  Warp-collective.
 __device__ __forceinline__ void sh_stage_in(const float* shs, int M, int i0, int n, float* s, int stride) {
+  constexpr int kInFlight = 8;  // loads issued before their stores
   const int rs = 3 * (M < 16 ? M : 16), rg = 3 * M, lane = threadIdx.x & 31;
   if (rs > 0) {
+    const int total = n * rs;
     int g = 0, c = lane;
     while (c >= rs) { c -= rs; ++g; }
-    for (int e = lane; e < n * rs; e += 32) {
-      s[g * stride + c] = shs[size_t(i0 + g) * rg + c];
-      c += 32;
-      while (c >= rs) { c -= rs; ++g; }
+    for (int e0 = 0; e0 < total; e0 += 32 * kInFlight) {
+      float v[kInFlight];
+      int dst[kInFlight];
+#pragma unroll
+      for (int k = 0; k < kInFlight; ++k) {
+        const bool ok = e0 + 32 * k + lane < total;
+        v[k] = ok ? __ldg(shs + size_t(i0 + g) * rg + c) : 0.f;
+        dst[k] = ok ? g * stride + c : -1;
+        c += 32;
+        while (c >= rs) { c -= rs; ++g; }
+      }
+#pragma unroll
+      for (int k = 0; k < kInFlight; ++k)
+        if (dst[k] >= 0) s[dst[k]] = v[k];
     }
   }
   __syncwarp();
@@ -399,13 +417,14 @@ __constant__ float kSH_C3[7] = {-0.5900435899266435f, 2.890611442640554f, -0.457
 // One Gaussian (radius > 0) of the reference-formula pass: every output but
 // dL_dsh, plus the SH basis and masked colour gradient dL_dsh is built from.
 // sh_row: this Gaussian's SH coefficients (staged in shared memory).
-__device__ __forceinline__ void ref_gaussian(const BackwardArgs& a, int i, const float* sh_row, float (&basis)[16],
+__device__ __forceinline__ void ref_gaussian(const BackwardArgs& a, int i, const float* sh_row, const float* mats, float (&basis)[16],
                                              float (&cf)[3]) {
   const int M = a.M;
-  const float* view = a.view;
-  const float* proj = a.proj;
-  const float cx = a.means3D[3 * i], cy = a.means3D[3 * i + 1], cz = a.means3D[3 * i + 2];
-  const float* pc = a.cov3D + 6 * size_t(i);
+  const float* cam = mats + 32;
+  const float* view = mats;
+  const float* proj = mats + 16;
+  const float cx = __ldg(&a.means3D[3 * i]), cy = __ldg(&a.means3D[3 * i + 1]), cz = __ldg(&a.means3D[3 * i + 2]);
+  const float* pc = a.cov3D + 6 * size_t(i);  // read with __ldg below
 
   // ---- computeCov2DCUDA ----
   float vx = view[0] * cx + view[4] * cy + view[8] * cz + view[12];
@@ -428,7 +447,7 @@ __device__ __forceinline__ void ref_gaussian(const BackwardArgs& a, int i, const
   // J (glm column-major J[col][row]) and T = W * J
   const float J[3][3] = {{h_x * z_inv, 0.f, -h_x * px * z_inv2}, {0.f, h_y * z_inv, -h_y * py * z_inv2}, {0.f, 0.f, 0.f}};
   const float Wv[3][3] = {{view[0], view[4], view[8]}, {view[1], view[5], view[9]}, {view[2], view[6], view[10]}};
-  const float Vk[3][3] = {{pc[0], pc[1], pc[2]}, {pc[1], pc[3], pc[4]}, {pc[2], pc[4], pc[5]}};
+  const float Vk[3][3] = {{__ldg(pc + 0), __ldg(pc + 1), __ldg(pc + 2)}, {__ldg(pc + 1), __ldg(pc + 3), __ldg(pc + 4)}, {__ldg(pc + 2), __ldg(pc + 4), __ldg(pc + 5)}};
   float T[3][3], tmp[3][3], c2[3][3];
 #pragma unroll
   for (int c = 0; c < 3; ++c)
@@ -447,7 +466,7 @@ __device__ __forceinline__ void ref_gaussian(const BackwardArgs& a, int i, const
   const float ca = c2[0][0], cb = c2[0][1], cc = c2[1][1];
   const float den = ca * cc - cb * cb;
   const float dinv2 = 1.0f / (den * den + 1e-7f);
-  const float gx = a.acc_cov[4 * i], gy = a.acc_cov[4 * i + 1], gz = a.acc_cov[4 * i + 3];
+  const float gx = __ldg(&a.acc_cov[4 * i]), gy = __ldg(&a.acc_cov[4 * i + 1]), gz = __ldg(&a.acc_cov[4 * i + 3]);
   float ga = 0.f, gb = 0.f, gc = 0.f;
   float dc[6];
   if (dinv2 > 0) {
@@ -488,24 +507,24 @@ __device__ __forceinline__ void ref_gaussian(const BackwardArgs& a, int i, const
   const float iw2 = iw * iw;
   const float ptx = (proj[0] * cx + proj[4] * cy + proj[8] * cz + proj[12]) * iw2;
   const float pty = (proj[1] * cx + proj[5] * cy + proj[9] * cz + proj[13]) * iw2;
-  const float g2x = a.dL_dmean2D[3 * i], g2y = a.dL_dmean2D[3 * i + 1];
+  const float g2x = __ldg(&a.dL_dmean2D[3 * i]), g2y = __ldg(&a.dL_dmean2D[3 * i + 1]);
   sd[0] += (proj[0] * iw - proj[3] * ptx) * g2x + (proj[1] * iw - proj[3] * pty) * g2y;
   sd[1] += (proj[4] * iw - proj[7] * ptx) * g2x + (proj[5] * iw - proj[7] * pty) * g2y;
   sd[2] += (proj[8] * iw - proj[11] * ptx) * g2x + (proj[9] * iw - proj[11] * pty) * g2y;
   const float vzz = view[2] * cx + view[6] * cy + view[10] * cz + view[14];
-  const float gd = a.acc_depth[i];
+  const float gd = __ldg(&a.acc_depth[i]);
   sd[0] += (view[2] - view[3] * vzz) * gd;
   sd[1] += (view[6] - view[7] * vzz) * gd;
   sd[2] += (view[10] - view[11] * vzz) * gd;
   // SH (all 16 bands, colour-clamp masks)
-  const float ox = cx - a.campos[0], oy = cy - a.campos[1], oz = cz - a.campos[2];
+  const float ox = cx - cam[0], oy = cy - cam[1], oz = cz - cam[2];
   const float msq = ox * ox + oy * oy + oz * oz;
   const float mag = sqrtf(msq + 1e-10f);
   const float im = 1.0f / mag;
   const float x = ox * im, y = oy * im, z = oz * im;
   const float x2 = x * x, y2 = y * y, z2 = z * z, xy = x * y, xz = x * z, yz = y * z;
   const float x2my2 = x2 - y2, tx2 = 3.0f * x2, ty2 = 3.0f * y2, fz2 = 4.0f * z2, wz2 = 2.0f * z2;
-  for (int ch = 0; ch < 3; ++ch) cf[ch] = a.dL_dcolors[3 * i + ch] * (a.clamped[3 * i + ch] ? 0.0f : 1.0f);
+  for (int ch = 0; ch < 3; ++ch) cf[ch] = __ldg(&a.dL_dcolors[3 * i + ch]) * (__ldg(&a.clamped[3 * i + ch]) ? 0.0f : 1.0f);
   const float SH_C0 = 0.28209479177387814f, SH_C1 = 0.4886025119029199f;
   basis[0] = SH_C0; basis[1] = -SH_C1 * y; basis[2] = SH_C1 * z; basis[3] = -SH_C1 * x;
   basis[4] = kSH_C2[0] * xy; basis[5] = kSH_C2[1] * yz; basis[6] = kSH_C2[2] * (wz2 - x2 - y2);
@@ -558,13 +577,13 @@ __device__ __forceinline__ void ref_gaussian(const BackwardArgs& a, int i, const
   a.dL_dmeans3D[3 * i + 2] = sd[2];
 
   // ---- scale / rotation (backward.cu:446-518) ----
-  const float qw = a.rotations[4 * i], qx = a.rotations[4 * i + 1], qy = a.rotations[4 * i + 2],
-              qz = a.rotations[4 * i + 3];
+  const float qw = __ldg(&a.rotations[4 * i]), qx = __ldg(&a.rotations[4 * i + 1]), qy = __ldg(&a.rotations[4 * i + 2]),
+              qz = __ldg(&a.rotations[4 * i + 3]);
   const float xx = qx * qx, yy = qy * qy, zz = qz * qz;
   const float qxy = qx * qy, qxz = qx * qz, qyz = qy * qz;
   const float xw = qx * qw, yw = qy * qw, zw = qz * qw;
-  const float sx = a.scale_modifier * a.scales[3 * i], sy = a.scale_modifier * a.scales[3 * i + 1],
-              sz = a.scale_modifier * a.scales[3 * i + 2];
+  const float sx = a.scale_modifier * __ldg(&a.scales[3 * i]), sy = a.scale_modifier * __ldg(&a.scales[3 * i + 1]),
+              sz = a.scale_modifier * __ldg(&a.scales[3 * i + 2]);
   const float m11 = sx * (1.f - 2.f * (yy + zz)), m12 = sx * 2.f * (qxy - zw), m13 = sx * 2.f * (qxz + yw);
   const float m21 = sy * 2.f * (qxy + zw), m22 = sy * (1.f - 2.f * (xx + zz)), m23 = sy * 2.f * (qyz - xw);
   const float m31 = sz * 2.f * (qxz - yw), m32 = sz * 2.f * (qyz + xw), m33 = sz * (1.f - 2.f * (xx + yy));
@@ -594,6 +613,13 @@ __device__ __forceinline__ void ref_gaussian(const BackwardArgs& a, int i, const
 
 __global__ void __launch_bounds__(kGaussThreads) gaussians_ref_kernel(BackwardArgs a) {
   __shared__ float s_sh[kGaussThreads / 32][32 * kShStride];
+  // view, projection, camera position: shared memory is never aliased by the
+  // outputs, so these stay in place across the output stores
+  __shared__ float s_mats[35];
+  if (threadIdx.x < 16) s_mats[threadIdx.x] = a.view[threadIdx.x];
+  else if (threadIdx.x < 32) s_mats[threadIdx.x] = a.proj[threadIdx.x - 16];
+  else if (threadIdx.x < 35) s_mats[threadIdx.x] = a.campos[threadIdx.x - 32];
+  __syncthreads();
   const int lane = threadIdx.x & 31;
   float* sw = s_sh[threadIdx.x >> 5];
   const int i0 = blockIdx.x * kGaussThreads + (threadIdx.x & ~31);
@@ -605,7 +631,7 @@ __global__ void __launch_bounds__(kGaussThreads) gaussians_ref_kernel(BackwardAr
   float basis[16], cf[3] = {0.f, 0.f, 0.f};
   const bool active = lane < n && a.radii[i] > 0;
   if (active) {
-    ref_gaussian(a, i, sw + lane * stride, basis, cf);
+    ref_gaussian(a, i, sw + lane * stride, s_mats, basis, cf);
   } else if (lane < n) {
     for (int k = 0; k < 3; ++k) a.dL_dmeans3D[3 * i + k] = 0.f;
     for (int k = 0; k < 6; ++k) a.dL_dcov3D[6 * i + k] = 0.f;
@@ -619,18 +645,19 @@ __global__ void __launch_bounds__(kGaussThreads) gaussians_ref_kernel(BackwardAr
 // Per-Gaussian, exact derivative of the forward.
 // One Gaussian (radius > 0) of the exact-derivative pass: every output but
 // dL_dsh, plus the outer-product factors of dL_dsh (see ref_gaussian).
-__device__ __forceinline__ void exact_gaussian(const BackwardArgs& a, int i, const float* sh_row,
+__device__ __forceinline__ void exact_gaussian(const BackwardArgs& a, int i, const float* sh_row, const float* mats,
                                                float (&basis)[16], float (&cf)[3]) {
   const int M = a.M;
-  const float* V = a.view;
-  const float* PM = a.proj;
-  const float m0 = a.means3D[3 * i], m1 = a.means3D[3 * i + 1], m2 = a.means3D[3 * i + 2];
+  const float* cam = mats + 32;
+  const float* V = mats;
+  const float* PM = mats + 16;
+  const float m0 = __ldg(&a.means3D[3 * i]), m1 = __ldg(&a.means3D[3 * i + 1]), m2 = __ldg(&a.means3D[3 * i + 2]);
   float gm[3] = {0.f, 0.f, 0.f};
   // screen position / depth: ndc = clip.xyz / (clip.w + 1e-5); dL_dmean2D already holds dL/dNDC
   float clip[4];
   for (int r = 0; r < 4; ++r) clip[r] = PM[r] * m0 + PM[4 + r] * m1 + PM[8 + r] * m2 + PM[12 + r];
   const float wi = 1.0f / (clip[3] + 1e-5f);
-  const float gn0 = a.dL_dmean2D[3 * i], gn1 = a.dL_dmean2D[3 * i + 1], gn2 = a.acc_depth[i];
+  const float gn0 = __ldg(&a.dL_dmean2D[3 * i]), gn1 = __ldg(&a.dL_dmean2D[3 * i + 1]), gn2 = __ldg(&a.acc_depth[i]);
   const float gcl[4] = {gn0 * wi, gn1 * wi, gn2 * wi, -(gn0 * clip[0] + gn1 * clip[1] + gn2 * clip[2]) * wi * wi};
   for (int c = 0; c < 3; ++c)
     for (int r = 0; r < 4; ++r) gm[c] += PM[4 * c + r] * gcl[r];
@@ -650,9 +677,9 @@ __device__ __forceinline__ void exact_gaussian(const BackwardArgs& a, int i, con
     jx[k] = f * (rgt[k] / tz - txp * fw[k] / (tz * tz));
     jy[k] = f * (upv[k] / tz - typ * fw[k] / (tz * tz));
   }
-  const float* pc = a.cov3D + 6 * size_t(i);
-  const float S[3][3] = {{pc[0], pc[1], pc[2]}, {pc[1], pc[3], pc[4]}, {pc[2], pc[4], pc[5]}};
-  const float gxx = a.acc_cov[4 * i], gxy = a.acc_cov[4 * i + 1], gyy = a.acc_cov[4 * i + 2];
+  const float* pc = a.cov3D + 6 * size_t(i);  // read with __ldg below
+  const float S[3][3] = {{__ldg(pc + 0), __ldg(pc + 1), __ldg(pc + 2)}, {__ldg(pc + 1), __ldg(pc + 3), __ldg(pc + 4)}, {__ldg(pc + 2), __ldg(pc + 4), __ldg(pc + 5)}};
+  const float gxx = __ldg(&a.acc_cov[4 * i]), gxy = __ldg(&a.acc_cov[4 * i + 1]), gyy = __ldg(&a.acc_cov[4 * i + 2]);
   float Gf[3][3];
   for (int p = 0; p < 3; ++p)
     for (int q = 0; q < 3; ++q) Gf[p][q] = gxx * jx[p] * jx[q] + gyy * jy[p] * jy[q] + gxy * jx[p] * jy[q];
@@ -690,11 +717,11 @@ __device__ __forceinline__ void exact_gaussian(const BackwardArgs& a, int i, con
   for (int c = 0; c < 3; ++c)
     for (int r = 0; r < 3; ++r) gm[c] += V[4 * c + r] * gt[r];
   // Sigma = M M^T, M = R diag(s)
-  const float w = a.rotations[4 * i], x = a.rotations[4 * i + 1], y = a.rotations[4 * i + 2], z = a.rotations[4 * i + 3];
+  const float w = __ldg(&a.rotations[4 * i]), x = __ldg(&a.rotations[4 * i + 1]), y = __ldg(&a.rotations[4 * i + 2]), z = __ldg(&a.rotations[4 * i + 3]);
   const float R[3][3] = {{1.f - 2.f * (y * y + z * z), 2.f * (x * y - w * z), 2.f * (x * z + w * y)},
                          {2.f * (x * y + w * z), 1.f - 2.f * (x * x + z * z), 2.f * (y * z - w * x)},
                          {2.f * (x * z - w * y), 2.f * (y * z + w * x), 1.f - 2.f * (x * x + y * y)}};
-  const float s[3] = {a.scales[3 * i], a.scales[3 * i + 1], a.scales[3 * i + 2]};
+  const float s[3] = {__ldg(&a.scales[3 * i]), __ldg(&a.scales[3 * i + 1]), __ldg(&a.scales[3 * i + 2])};
   float dM[3][3];
   for (int p = 0; p < 3; ++p)
     for (int k = 0; k < 3; ++k) {
@@ -719,10 +746,10 @@ __device__ __forceinline__ void exact_gaussian(const BackwardArgs& a, int i, con
   a.dL_drotations[4 * i + 3] = dR[0][0] * (-4.f * z) + dR[0][1] * (-2.f * w) + dR[0][2] * (2.f * x) + dR[1][0] * (2.f * w) +
                                dR[1][1] * (-4.f * z) + dR[1][2] * (2.f * y) + dR[2][0] * (2.f * x) + dR[2][1] * (2.f * y);
   // colour: rgb = sum_k basis_k(dir) sh_k + 0.5 with the forward's constants
-  const float v0 = m0 - a.campos[0], v1 = m1 - a.campos[1], v2 = m2 - a.campos[2];
+  const float v0 = m0 - cam[0], v1 = m1 - cam[1], v2 = m2 - cam[2];
   const float vn = sqrtf(v0 * v0 + v1 * v1 + v2 * v2);
   const float X = v0 / vn, Y = v1 / vn, Z = v2 / vn;
-  const float gc0 = a.dL_dcolors[3 * i], gc1 = a.dL_dcolors[3 * i + 1], gc2 = a.dL_dcolors[3 * i + 2];
+  const float gc0 = __ldg(&a.dL_dcolors[3 * i]), gc1 = __ldg(&a.dL_dcolors[3 * i + 1]), gc2 = __ldg(&a.dL_dcolors[3 * i + 2]);
   const float C1 = 0.4886025119029199f, C2a = 1.0925484305920792f, C2e = 0.5462742152960396f;
   const float C30 = 0.5900435899266435f, C31 = 2.890611442640554f, C32 = 0.4570457994644658f;
   const float C33 = 0.3731763325901154f, C35 = 1.445305721320277f;
@@ -771,6 +798,13 @@ __device__ __forceinline__ void exact_gaussian(const BackwardArgs& a, int i, con
 
 __global__ void __launch_bounds__(kGaussThreads) gaussians_exact_kernel(BackwardArgs a) {
   __shared__ float s_sh[kGaussThreads / 32][32 * kShStride];
+  // view, projection, camera position: shared memory is never aliased by the
+  // outputs, so these stay in place across the output stores
+  __shared__ float s_mats[35];
+  if (threadIdx.x < 16) s_mats[threadIdx.x] = a.view[threadIdx.x];
+  else if (threadIdx.x < 32) s_mats[threadIdx.x] = a.proj[threadIdx.x - 16];
+  else if (threadIdx.x < 35) s_mats[threadIdx.x] = a.campos[threadIdx.x - 32];
+  __syncthreads();
   const int lane = threadIdx.x & 31;
   float* sw = s_sh[threadIdx.x >> 5];
   const int i0 = blockIdx.x * kGaussThreads + (threadIdx.x & ~31);
@@ -782,7 +816,7 @@ __global__ void __launch_bounds__(kGaussThreads) gaussians_exact_kernel(Backward
   float basis[16], cf[3] = {0.f, 0.f, 0.f};
   const bool active = lane < n && a.radii[i] > 0;
   if (active) {
-    exact_gaussian(a, i, sw + lane * stride, basis, cf);
+    exact_gaussian(a, i, sw + lane * stride, s_mats, basis, cf);
   } else if (lane < n) {
     for (int k = 0; k < 3; ++k) a.dL_dmeans3D[3 * i + k] = 0.f;
     for (int k = 0; k < 6; ++k) a.dL_dcov3D[6 * i + k] = 0.f;
@@ -795,11 +829,12 @@ __global__ void __launch_bounds__(kGaussThreads) gaussians_exact_kernel(Backward
 }  // namespace
 
 void launch_backward_render(const BackwardArgs& a, cudaStream_t stream) {
-  const int grid = ((a.W + kTile - 1) / kTile) * ((a.H + kTile - 1) / kTile);
-  if (grid <= 0) return;
+  const int tiles = ((a.W + kTile - 1) / kTile) * ((a.H + kTile - 1) / kTile);
+  if (tiles <= 0) return;
+  const int grid = tiles * (8 / kBwdWarps);
   stage_begin(kStBwdRender, stream);
-  if (a.grad_mode == 1) render_exact_kernel<<<grid, kBlendThreads, 0, stream>>>(a);
-  else render_ref_kernel<<<grid, kBlendThreads, 0, stream>>>(a);
+  if (a.grad_mode == 1) render_exact_kernel<<<grid, 32 * kBwdWarps, 0, stream>>>(a);
+  else render_ref_kernel<<<grid, 32 * kBwdWarps, 0, stream>>>(a);
   stage_end(kStBwdRender, stream, 1);
 }
 

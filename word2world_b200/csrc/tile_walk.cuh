@@ -33,8 +33,9 @@ struct WarpChunk {
 // Pixel of this thread in tile `tile` of a grid `gw` tiles wide.
 struct TilePixel {
   int X0, Y0, px, py, warp, lane, bx, by;  // (bx, by): top-left pixel of the warp's block
-  __device__ __forceinline__ TilePixel(int tile, int gw) {
-    warp = threadIdx.x >> 5;
+  // warp: this thread's 8x4 block of the tile (0..7)
+  __device__ __forceinline__ TilePixel(int tile, int gw, int block) {
+    warp = block;
     lane = threadIdx.x & 31;
     X0 = (tile % gw) * kTile;
     Y0 = (tile / gw) * kTile;
@@ -43,6 +44,7 @@ struct TilePixel {
     px = bx + (lane & 7);
     py = by + (lane >> 3);
   }
+  __device__ __forceinline__ TilePixel(int tile, int gw) : TilePixel(tile, gw, int(threadIdx.x >> 5)) {}
 };
 
 // Tiles are processed heaviest first: CTA b takes tile order[b], where order
