@@ -396,13 +396,25 @@ __device__ __forceinline__ void sh_store_outer(float* dsh, int M, int i0, int n,
   for (int ch = 0; ch < 3; ++ch) s[lane * kRow + 16 + ch] = active ? cf[ch] : 0.f;
   __syncwarp();
   if (rg > 0) {
+    constexpr int kInFlight = 8;
+    const int total = n * rg;
     int g = 0, c = lane;
     while (c >= rg) { c -= rg; ++g; }
-    for (int e = lane; e < n * rg; e += 32) {
-      const int k = c / 3, ch = c - 3 * k;
-      dsh[size_t(i0 + g) * rg + c] = k < 16 ? s[g * kRow + k] * s[g * kRow + 16 + ch] : 0.f;
-      c += 32;
-      while (c >= rg) { c -= rg; ++g; }
+    for (int e0 = 0; e0 < total; e0 += 32 * kInFlight) {
+      float v[kInFlight];
+      size_t dst[kInFlight];
+#pragma unroll
+      for (int q = 0; q < kInFlight; ++q) {
+        const int k = c / 3, ch = c - 3 * k;
+        const bool ok = e0 + 32 * q + lane < total;
+        v[q] = ok && k < 16 ? s[g * kRow + k] * s[g * kRow + 16 + ch] : 0.f;
+        dst[q] = ok ? size_t(i0 + g) * rg + c : ~size_t(0);
+        c += 32;
+        while (c >= rg) { c -= rg; ++g; }
+      }
+#pragma unroll
+      for (int q = 0; q < kInFlight; ++q)
+        if (dst[q] != ~size_t(0)) dsh[dst[q]] = v[q];
     }
   }
 }

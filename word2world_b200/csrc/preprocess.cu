@@ -393,19 +393,21 @@ preprocess_kernel(PreprocessArgs a) {
   }
   __syncthreads();
   const Pair block_total = s_warp[kPreThreads / 32 - 1];
+  // decoupled lookback; each status word carries its flag and pair together
+  // and nothing else written by its tile is read, so relaxed accesses suffice
   if (threadIdx.x == 0) {
     unsigned long long* status = a.scan_status;
     if (tile == 0) {
-      st_release64(status + tile, pack(kFlagInc, block_total));
+      st_relaxed64(status + tile, pack(kFlagInc, block_total));
       s_prefix = Pair{0, 0};
     } else {
-      st_release64(status + tile, pack(kFlagAgg, block_total));
+      st_relaxed64(status + tile, pack(kFlagAgg, block_total));
       Pair ex{0, 0};
       bool first = true;
       int t = int(tile) - 1;
       uint32_t spins = 0;
       while (t >= 0) {
-        const unsigned long long w = ld_acquire64(status + t);
+        const unsigned long long w = ld_relaxed64(status + t);
         const unsigned long long flag = w & (3ull << 62);
         if (flag == 0) {
           if (++spins > kSpinLimit) { atomicOr(&hdr->error, kErrTimeout); break; }
@@ -418,7 +420,7 @@ preprocess_kernel(PreprocessArgs a) {
         --t;
       }
       s_prefix = ex;
-      st_release64(status + tile, pack(kFlagInc, combine(ex, block_total)));
+      st_relaxed64(status + tile, pack(kFlagInc, combine(ex, block_total)));
     }
   }
   __syncthreads();

@@ -61,16 +61,18 @@ scan_kernel(const uint32_t* __restrict__ in, uint32_t* __restrict__ out, long lo
   }
   __syncthreads();
   const uint32_t total = s_warp[kScanThreads / 32 - 1];
+  // decoupled lookback; a status word carries its flag and count together and
+  // nothing else written by its tile is read, so relaxed accesses suffice
   if (tid == 0) {
     if (tile == 0) {
-      st_release64(status, kInc | total);
+      st_relaxed64(status, kInc | total);
       s_prefix = 0;
     } else {
-      st_release64(status + tile, kAgg | total);
+      st_relaxed64(status + tile, kAgg | total);
       uint32_t acc = 0, spins = 0;
       long long t = tile - 1;
       while (t >= 0) {
-        const unsigned long long w = ld_acquire64(status + t);
+        const unsigned long long w = ld_relaxed64(status + t);
         const unsigned long long flag = w & kFlags;
         if (flag == 0ull) {
           if (++spins > kSpinLimit) { atomicOr(err, kErrTimeout); break; }
@@ -81,7 +83,7 @@ scan_kernel(const uint32_t* __restrict__ in, uint32_t* __restrict__ out, long lo
         --t;
       }
       s_prefix = acc;
-      st_release64(status + tile, kInc | uint32_t(acc + total));
+      st_relaxed64(status + tile, kInc | uint32_t(acc + total));
     }
   }
   __syncthreads();
