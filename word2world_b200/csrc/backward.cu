@@ -25,10 +25,15 @@ namespace w2w {
 namespace {
 
 constexpr int kValues = 10;
-// Warps (8x4 blocks) per CTA in the per-pixel passes.  The warps walk
-// independently; keeping a tile's eight on one SM lets them share the record
-// gathers through L1 (1, 2 and 4 warps per CTA measured slower).
-constexpr int kBwdWarps = 8;
+// Heavy tiles: their warps' walks are split in two at list position
+// mid = walk * kSplitNum / 16.  One CTA runs the back segment [mid, walk) in
+// full; a second CTA first replays the back segment's state recurrences only
+// (alpha and the transmittance / suffix updates, no gradients, no reduction:
+// about a quarter of a full entry's work) to reach the state at mid, then runs
+// [0, mid) in full.  Both compute the state with the same code in the same
+// order, so the second starts from exactly the state the first would have
+// reached; only the order of the atomic additions changes.
+constexpr int kSplitNum = 7;
 
 // Where each of the ten per-entry sums goes: after the transposed reduction
 // below, lane L (L even) holds the warp's sum of value (L >> 1); lanes 0..18
@@ -87,10 +92,8 @@ struct BwdPixel {
   int walk;  // list positions [0, walk) may hold contributors of this warp's pixels
   uint32_t last, warp_last;
   float dLp0 = 0.f, dLp1 = 0.f, dLp2 = 0.f, dLd = 0.f, dLa = 0.f;
-  // CTA b covers kBwdWarps of the 8 blocks of tile order[b / (8 / kBwdWarps)]
-  __device__ __forceinline__ explicit BwdPixel(const BackwardArgs& a)
-      : tile(int(a.order[blockIdx.x / (8 / kBwdWarps)])),
-        tp(tile, (a.W + kTile - 1) / kTile, int(blockIdx.x % (8 / kBwdWarps)) * kBwdWarps + int(threadIdx.x >> 5)) {
+  __device__ __forceinline__ BwdPixel(const BackwardArgs& a, int tile_)
+      : tile(tile_), tp(tile_, (a.W + kTile - 1) / kTile) {
     inside = tp.px < a.W && tp.py < a.H;
     range = a.ranges[tile];
     pix = inside ? size_t(tp.py) * a.W + tp.px : 0;
@@ -115,24 +118,48 @@ struct RefChain {
   float acc0 = 0.f, acc1 = 0.f, acc2 = 0.f, acc_d = 0.f, acc_a = 0.f;
   float last_alpha = 0.f, lc0 = 0.f, lc1 = 0.f, lc2 = 0.f, last_depth = 0.f;
 
+  // The state after entry (opacity-weighted alpha `alpha`, colour in q1.w,
+  // q2.x, q2.y, depth q1.z).  T in [~1e-4, 1] (the forward stops before
+  // T < 1e-4) and 1 - alpha in [0.01, 1]: the division is in div_markstein's
+  // range, which equals /.
+  struct Next {
+    float Tn, n0, n1, n2, nd, na;
+  };
+  __device__ __forceinline__ Next next(float alpha) const {
+    Next x;
+    x.Tn = div_markstein(T, 1.f - alpha);
+    x.n0 = last_alpha * lc0 + (1.f - last_alpha) * acc0;
+    x.n1 = last_alpha * lc1 + (1.f - last_alpha) * acc1;
+    x.n2 = last_alpha * lc2 + (1.f - last_alpha) * acc2;
+    x.nd = last_alpha * last_depth + (1.f - last_alpha) * acc_d;
+    x.na = last_alpha + (1.f - last_alpha) * acc_a;
+    return x;
+  }
+  __device__ __forceinline__ void commit(bool ok, const Next& x, float4 q1, float4 q2, float alpha) {
+    if (ok) {
+      T = x.Tn;
+      acc0 = x.n0; acc1 = x.n1; acc2 = x.n2; acc_d = x.nd; acc_a = x.na;
+      lc0 = q1.w; lc1 = q2.x; lc2 = q2.y; last_depth = q1.z;
+      last_alpha = alpha;
+    }
+  }
+  // State only (the walk of a later segment's prefix, see render_ref_kernel).
+  __device__ __forceinline__ void advance(bool ok, float4 q1, float4 q2, float alpha) {
+    commit(ok, next(alpha), q1, q2, alpha);
+  }
+
   // ok false: the entry is skipped (state unchanged, contributions zero).
   __device__ __forceinline__ void step(bool ok, const BwdPixel& p, float4 q0, float4 q1, float4 q2, float dx, float dy,
                                        float G, float alpha, float ddelx_dx, float ddely_dy, float (&c)[kValues]) {
-    // T in [~1e-4, 1] (the forward stops before T < 1e-4) and 1 - alpha in
-    // [0.01, 1]: both divisions are in div_markstein's range, which equals /
-    const float Tn = div_markstein(T, 1.f - alpha);
+    const Next x = next(alpha);
+    const float Tn = x.Tn, n0 = x.n0, n1 = x.n1, n2 = x.n2, nd = x.nd, na = x.na;
     const float dchdc = alpha * Tn;
     float dL_dopa = 0.0f;
-    const float n0 = last_alpha * lc0 + (1.f - last_alpha) * acc0;
     dL_dopa += (q1.w - n0) * p.dLp0;
-    const float n1 = last_alpha * lc1 + (1.f - last_alpha) * acc1;
     dL_dopa += (q2.x - n1) * p.dLp1;
-    const float n2 = last_alpha * lc2 + (1.f - last_alpha) * acc2;
     dL_dopa += (q2.y - n2) * p.dLp2;
     const float c_d = q1.z;
-    const float nd = last_alpha * last_depth + (1.f - last_alpha) * acc_d;
     dL_dopa += (c_d - nd) * p.dLd;
-    const float na = last_alpha + (1.f - last_alpha) * acc_a;
     dL_dopa += (1 - na) * p.dLa;
     dL_dopa *= Tn;
     dL_dopa += div_markstein(-T_final, 1.f - alpha) * bg_dot;
@@ -150,12 +177,7 @@ struct RefChain {
     c[7] = ok ? -0.5f * gdx * dy * dL_dG : 0.f;
     c[8] = ok ? -0.5f * gdy * dy * dL_dG : 0.f;
     c[9] = ok ? G * dL_dopa : 0.f;
-    if (ok) {
-      T = Tn;
-      acc0 = n0; acc1 = n1; acc2 = n2; acc_d = nd; acc_a = na;
-      lc0 = q1.w; lc1 = q2.x; lc2 = q2.y; last_depth = c_d;
-      last_alpha = alpha;
-    }
+    commit(ok, x, q1, q2, alpha);
   }
 };
 
@@ -171,9 +193,50 @@ __device__ __forceinline__ bool ref_eval(float4 q0, float4 q1, float4 q2, float 
   return power <= 0.0f && power >= q2.z && alpha >= 1.0f / 255.0f;
 }
 
-__global__ void __launch_bounds__(32 * kBwdWarps, 16 / kBwdWarps) render_ref_kernel(BackwardArgs a) {
-  __shared__ WarpChunk s_chunk[kBwdWarps];
-  const BwdPixel p(a);
+// Walk list positions [lo, top) back to front, kChunk at a time; body(bits,
+// hi) handles one staged chunk whose entry j is list position hi - 1 - j and
+// whose set bits are the entries that may reach this warp's block.
+template <typename Body>
+__device__ __forceinline__ void walk_back(const float* records, const uint32_t* point_list, uint32_t base, int lo,
+                                          int top, WarpChunk& wc, const TilePixel& tp, Body&& body) {
+  const int len = top - lo;
+  const int nc = len > 0 ? (len + kChunk - 1) / kChunk : 0;
+  ChunkLoad ld;
+  uint32_t reach = 0;
+  if (nc > 0) {
+    chunk_load(ld, records, point_list, base + top - 1 - tp.lane, tp.lane < len);
+    reach = chunk_store(wc, ld, tp.bx, tp.by);
+  }
+  for (int c = 0; c < nc; ++c) {
+    const int hi = top - c * kChunk;
+    const int hn = hi - kChunk;
+    const bool more = c + 1 < nc;
+    if (more) chunk_load(ld, records, point_list, base + hn - 1 - tp.lane, hn - 1 - tp.lane >= lo);
+    body(reach, hi);
+    if (more) {
+      __syncwarp();
+      reach = chunk_store(wc, ld, tp.bx, tp.by);
+    }
+  }
+}
+
+// CTA b's tile and role: the first 2 * split CTAs are the two halves of the
+// `split` heaviest tiles (role 1: back segment, role 2: front segment), the
+// rest one tile each (role 0), heaviest first.
+__device__ __forceinline__ int cta_tile(const BackwardArgs& a, int& role) {
+  const int b = int(blockIdx.x);
+  if (b < 2 * a.split) {
+    role = 1 + (b & 1);
+    return int(a.order_bwd[b >> 1]);
+  }
+  role = 0;
+  return int(a.order_bwd[b - a.split]);
+}
+
+__global__ void __launch_bounds__(kBlendThreads, 2) render_ref_kernel(BackwardArgs a) {
+  __shared__ WarpChunk s_chunk[kBlendThreads / 32];
+  int role;
+  const BwdPixel p(a, cta_tile(a, role));
   RefChain ch;
   ch.T_final = p.inside ? 1.0f - a.out_alpha[p.pix] : 0.0f;
   ch.T = ch.T_final;
@@ -182,21 +245,8 @@ __global__ void __launch_bounds__(32 * kBwdWarps, 16 / kBwdWarps) render_ref_ker
   const float pxf = float(p.tp.px), pyf = float(p.tp.py);
   const Target tgt = lane_target(a, 0);
   WarpChunk& wc = s_chunk[threadIdx.x >> 5];
-  // back to front: chunk c holds list positions walk-1-32c, walk-2-32c, ... (lane j: walk-1-32c-j)
-  const int nc = (p.walk + kChunk - 1) / kChunk;
-  ChunkLoad ld;
-  uint32_t reach = 0;
-  if (nc > 0) {
-    chunk_load(ld, a.bwd_record, a.point_list, p.range.x + p.walk - 1 - p.tp.lane, p.tp.lane < p.walk);
-    reach = chunk_store(wc, ld, p.tp.bx, p.tp.by);
-  }
-  for (int c = 0; c < nc; ++c) {
-    const int hi = p.walk - c * kChunk;  // chunk entry j is list position hi - 1 - j
-    const int hn = hi - kChunk;
-    const bool more = c + 1 < nc;
-    if (more) chunk_load(ld, a.bwd_record, a.point_list, p.range.x + hn - 1 - p.tp.lane, p.tp.lane < hn);
-    const float4* s = wc.rec;
-    uint32_t bits = reach;
+  const float4* s = wc.rec;
+  auto full = [&](uint32_t bits, int hi) {
     while (bits != 0u) {
       const int j0 = pop_entry(bits);
       const int j1r = pop_entry(bits);
@@ -214,10 +264,32 @@ __global__ void __launch_bounds__(32 * kBwdWarps, 16 / kBwdWarps) render_ref_ker
       flush(c0, ok0, wc.id[j0], tgt);
       flush(c1, ok1, wc.id[j1], tgt);
     }
-    if (more) {
-      __syncwarp();
-      reach = chunk_store(wc, ld, p.tp.bx, p.tp.by);
+  };
+  auto state_only = [&](uint32_t bits, int hi) {
+    while (bits != 0u) {
+      const int j0 = pop_entry(bits);
+      const int j1r = pop_entry(bits);
+      const bool has1 = j1r >= 0;
+      const int j1 = has1 ? j1r : j0;
+      const float4 a0 = s[kRecVec * j0], a1 = s[kRecVec * j0 + 1], a2 = s[kRecVec * j0 + 2];
+      const float4 b0 = s[kRecVec * j1], b1 = s[kRecVec * j1 + 1], b2 = s[kRecVec * j1 + 2];
+      float dx0, dy0, G0, al0, dx1, dy1, G1, al1;
+      const bool ok0 = ref_eval(a0, a1, a2, pxf, pyf, dx0, dy0, G0, al0) && uint32_t(hi - 1 - j0) < p.last;
+      const bool ok1 = ref_eval(b0, b1, b2, pxf, pyf, dx1, dy1, G1, al1) && has1 &&
+                       uint32_t(hi - 1 - j1) < p.last;
+      ch.advance(ok0, a1, a2, al0);
+      ch.advance(ok1, b1, b2, al1);
     }
+  };
+  const int mid = (p.walk * kSplitNum) / 16;
+  if (role == 0) {
+    walk_back(a.bwd_record, a.point_list, p.range.x, 0, p.walk, wc, p.tp, full);
+  } else if (role == 1) {
+    walk_back(a.bwd_record, a.point_list, p.range.x, mid, p.walk, wc, p.tp, full);
+  } else {
+    walk_back(a.bwd_record, a.point_list, p.range.x, mid, p.walk, wc, p.tp, state_only);
+    __syncwarp();
+    walk_back(a.bwd_record, a.point_list, p.range.x, 0, mid, wc, p.tp, full);
   }
 }
 
@@ -237,6 +309,21 @@ __device__ __forceinline__ float gauss_num_fwd(float px, float py, float mx, flo
 struct ExactChain {
   float T;
   float S0, S1, S2, SD = 0.f, SW = 0.f;  // suffix sums behind the current entry (colour includes the background)
+
+  // State only (the walk of a later segment's prefix).
+  __device__ __forceinline__ void advance(bool ok, float4 q1, float4 q2, float a_) {
+    const float ia = rcp_markstein(1.0f - a_);
+    const float Tn = T * ia;
+    const float aT = a_ * Tn;
+    if (ok) {
+      T = Tn;
+      S0 += q2.x * aT;
+      S1 += q2.y * aT;
+      S2 += q2.z * aT;
+      SD += q1.w * aT;
+      SW += aT;
+    }
+  }
 
   // ok false: the entry is skipped (state unchanged, contributions zero).
   __device__ __forceinline__ void step(bool ok, const BwdPixel& p, float4 q0, float4 q1, float4 q2, float pxf,
@@ -278,9 +365,10 @@ struct ExactChain {
   }
 };
 
-__global__ void __launch_bounds__(32 * kBwdWarps, 16 / kBwdWarps) render_exact_kernel(BackwardArgs a) {
-  __shared__ WarpChunk s_chunk[kBwdWarps];
-  const BwdPixel p(a);
+__global__ void __launch_bounds__(kBlendThreads, 2) render_exact_kernel(BackwardArgs a) {
+  __shared__ WarpChunk s_chunk[kBlendThreads / 32];
+  int role;
+  const BwdPixel p(a, cta_tile(a, role));
   ExactChain ch;
   const float Tf = p.inside ? a.T_final[p.pix] : 0.0f;
   ch.T = Tf;
@@ -291,39 +379,33 @@ __global__ void __launch_bounds__(32 * kBwdWarps, 16 / kBwdWarps) render_exact_k
   const float pxf = float(p.tp.px), pyf = float(p.tp.py);
   const Target tgt = lane_target(a, 1);
   WarpChunk& wc = s_chunk[threadIdx.x >> 5];
-  const int nc = (p.walk + kChunk - 1) / kChunk;
-  ChunkLoad ld;
-  uint32_t reach = 0;
-  if (nc > 0) {
-    chunk_load(ld, a.record, a.point_list, p.range.x + p.walk - 1 - p.tp.lane, p.tp.lane < p.walk);
-    reach = chunk_store(wc, ld, p.tp.bx, p.tp.by);
-  }
-  for (int c = 0; c < nc; ++c) {
-    const int hi = p.walk - c * kChunk;
-    const int hn = hi - kChunk;
-    const bool more = c + 1 < nc;
-    if (more) chunk_load(ld, a.record, a.point_list, p.range.x + hn - 1 - p.tp.lane, p.tp.lane < hn);
-    const float4* s = wc.rec;
-    uint32_t bits = reach;
+  const float4* s = wc.rec;
+  // the forward's Gaussian values of two entries (same division as the blend)
+  auto eval2 = [&](int j0, int j1, float& m0, float& m1, float& g0, float& g1) {
+    const float4 a0 = s[kRecVec * j0], a1 = s[kRecVec * j0 + 1];
+    const float4 b0 = s[kRecVec * j1], b1 = s[kRecVec * j1 + 1];
+    const float n0 = gauss_num_fwd(pxf, pyf, a0.x, a0.y, a0.z, a0.w, a1.x);
+    const float n1 = gauss_num_fwd(pxf, pyf, b0.x, b0.y, b0.z, b0.w, b1.x);
+    if (__all_sync(0xffffffffu, div_in_range(n0, a1.y) && div_in_range(n1, b1.y))) {
+      m0 = div_markstein(n0, a1.y);
+      m1 = div_markstein(n1, b1.y);
+    } else {
+      m0 = div(n0, a1.y);
+      m1 = div(n1, b1.y);
+    }
+    g0 = expf(mul(-0.5f, m0 < 0.0f ? 1000.0f : m0));
+    g1 = expf(mul(-0.5f, m1 < 0.0f ? 1000.0f : m1));
+  };
+  auto full = [&](uint32_t bits, int hi) {
     while (bits != 0u) {
       const int j0 = pop_entry(bits);
       const int j1r = pop_entry(bits);
       const bool has1 = j1r >= 0;
       const int j1 = has1 ? j1r : j0;
+      float m0, m1, g0, g1;
+      eval2(j0, j1, m0, m1, g0, g1);
       const float4 a0 = s[kRecVec * j0], a1 = s[kRecVec * j0 + 1];
       const float4 b0 = s[kRecVec * j1], b1 = s[kRecVec * j1 + 1];
-      const float n0 = gauss_num_fwd(pxf, pyf, a0.x, a0.y, a0.z, a0.w, a1.x);
-      const float n1 = gauss_num_fwd(pxf, pyf, b0.x, b0.y, b0.z, b0.w, b1.x);
-      float m0, m1;
-      if (__all_sync(0xffffffffu, div_in_range(n0, a1.y) && div_in_range(n1, b1.y))) {
-        m0 = div_markstein(n0, a1.y);
-        m1 = div_markstein(n1, b1.y);
-      } else {
-        m0 = div(n0, a1.y);
-        m1 = div(n1, b1.y);
-      }
-      const float g0 = expf(mul(-0.5f, m0 < 0.0f ? 1000.0f : m0));
-      const float g1 = expf(mul(-0.5f, m1 < 0.0f ? 1000.0f : m1));
       const float og0 = mul(a1.z, g0), og1 = mul(b1.z, g1);
       const float al0 = fminf(0.99f, og0), al1 = fminf(0.99f, og1);
       const bool ok0 = al0 >= 1.0f / 255.0f && uint32_t(hi - 1 - j0) < p.last;
@@ -334,10 +416,32 @@ __global__ void __launch_bounds__(32 * kBwdWarps, 16 / kBwdWarps) render_exact_k
       flush(c0, ok0, wc.id[j0], tgt);
       flush(c1, ok1, wc.id[j1], tgt);
     }
-    if (more) {
-      __syncwarp();
-      reach = chunk_store(wc, ld, p.tp.bx, p.tp.by);
+  };
+  auto state_only = [&](uint32_t bits, int hi) {
+    while (bits != 0u) {
+      const int j0 = pop_entry(bits);
+      const int j1r = pop_entry(bits);
+      const bool has1 = j1r >= 0;
+      const int j1 = has1 ? j1r : j0;
+      float m0, m1, g0, g1;
+      eval2(j0, j1, m0, m1, g0, g1);
+      const float4 a1 = s[kRecVec * j0 + 1], b1 = s[kRecVec * j1 + 1];
+      const float al0 = fminf(0.99f, mul(a1.z, g0)), al1 = fminf(0.99f, mul(b1.z, g1));
+      const bool ok0 = al0 >= 1.0f / 255.0f && uint32_t(hi - 1 - j0) < p.last;
+      const bool ok1 = al1 >= 1.0f / 255.0f && has1 && uint32_t(hi - 1 - j1) < p.last;
+      ch.advance(ok0, a1, s[kRecVec * j0 + 2], al0);
+      ch.advance(ok1, b1, s[kRecVec * j1 + 2], al1);
     }
+  };
+  const int mid = (p.walk * kSplitNum) / 16;
+  if (role == 0) {
+    walk_back(a.record, a.point_list, p.range.x, 0, p.walk, wc, p.tp, full);
+  } else if (role == 1) {
+    walk_back(a.record, a.point_list, p.range.x, mid, p.walk, wc, p.tp, full);
+  } else {
+    walk_back(a.record, a.point_list, p.range.x, mid, p.walk, wc, p.tp, state_only);
+    __syncwarp();
+    walk_back(a.record, a.point_list, p.range.x, 0, mid, wc, p.tp, full);
   }
 }
 
@@ -843,10 +947,13 @@ __global__ void __launch_bounds__(kGaussThreads) gaussians_exact_kernel(Backward
 void launch_backward_render(const BackwardArgs& a, cudaStream_t stream) {
   const int tiles = ((a.W + kTile - 1) / kTile) * ((a.H + kTile - 1) / kTile);
   if (tiles <= 0) return;
-  const int grid = tiles * (8 / kBwdWarps);
+  BackwardArgs b = a;
+  int sms = 148;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, 0);
+  b.split = min(tiles / 4, sms);  // the heaviest tiles by largest contributor count
   stage_begin(kStBwdRender, stream);
-  if (a.grad_mode == 1) render_exact_kernel<<<grid, 32 * kBwdWarps, 0, stream>>>(a);
-  else render_ref_kernel<<<grid, 32 * kBwdWarps, 0, stream>>>(a);
+  if (a.grad_mode == 1) render_exact_kernel<<<tiles + b.split, kBlendThreads, 0, stream>>>(b);
+  else render_ref_kernel<<<tiles + b.split, kBlendThreads, 0, stream>>>(b);
   stage_end(kStBwdRender, stream, 1);
 }
 

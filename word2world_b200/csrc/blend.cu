@@ -157,7 +157,8 @@ __global__ void __launch_bounds__(kBlendThreads, 2) blend_kernel(BlendArgs a) {
 
 // Bucket sort of the tiles by decreasing list length (quarter-octave buckets;
 // order within a bucket is arbitrary).  One CTA.
-__global__ void __launch_bounds__(1024) tile_order_kernel(const uint2* ranges, int num_tiles, uint32_t* order) {
+__global__ void __launch_bounds__(1024) tile_order_kernel(const uint2* ranges, const uint32_t* counts, int num_tiles,
+                                                          uint32_t* order) {
   constexpr int kBuckets = 130;
   __shared__ uint32_t s_cnt[kBuckets];
   __shared__ uint32_t s_pos[kBuckets];
@@ -169,10 +170,12 @@ __global__ void __launch_bounds__(1024) tile_order_kernel(const uint2* ranges, i
   };
   for (int i = threadIdx.x; i < kBuckets; i += blockDim.x) s_cnt[i] = 0;
   __syncthreads();
-  for (int t = threadIdx.x; t < num_tiles; t += blockDim.x) {
+  auto weight = [&](int t) -> uint32_t {
+    if (counts) return counts[t];
     const uint2 r = ranges[t];
-    atomicAdd(&s_cnt[bucket(r.y - r.x)], 1u);
-  }
+    return r.y - r.x;
+  };
+  for (int t = threadIdx.x; t < num_tiles; t += blockDim.x) atomicAdd(&s_cnt[bucket(weight(t))], 1u);
   __syncthreads();
   if (threadIdx.x == 0) {
     uint32_t acc = 0;
@@ -182,19 +185,18 @@ __global__ void __launch_bounds__(1024) tile_order_kernel(const uint2* ranges, i
     }
   }
   __syncthreads();
-  for (int t = threadIdx.x; t < num_tiles; t += blockDim.x) {
-    const uint2 r = ranges[t];
-    order[atomicAdd(&s_pos[bucket(r.y - r.x)], 1u)] = uint32_t(t);
-  }
+  for (int t = threadIdx.x; t < num_tiles; t += blockDim.x) order[atomicAdd(&s_pos[bucket(weight(t))], 1u)] = uint32_t(t);
 }
 
 void launch_blend(const BlendArgs& a, cudaStream_t stream) {
   const int tiles = ((a.W + kTile - 1) / kTile) * ((a.H + kTile - 1) / kTile);
   if (tiles <= 0) return;
   stage_begin(kStBlend, stream);
-  tile_order_kernel<<<1, 1024, 0, stream>>>(a.ranges, tiles, a.order);
+  tile_order_kernel<<<1, 1024, 0, stream>>>(a.ranges, nullptr, tiles, a.order);
   blend_kernel<<<tiles, kBlendThreads, 0, stream>>>(a);
-  stage_end(kStBlend, stream, 2);
+  // the backward's order: by the largest contributor count the blend just found
+  tile_order_kernel<<<1, 1024, 0, stream>>>(nullptr, a.tile_max, tiles, a.order_bwd);
+  stage_end(kStBlend, stream, 3);
 }
 
 }  // namespace w2w

@@ -170,6 +170,7 @@ size_t w2w_image_offset(int W, int H, const char* name) {
   if (!strcmp(name, "T_final")) return L.T_final;
   if (!strcmp(name, "tile_max")) return L.tile_max;
   if (!strcmp(name, "order")) return L.order;
+  if (!strcmp(name, "order_bwd")) return L.order_bwd;
   return size_t(-1);
 }
 
@@ -299,6 +300,7 @@ int w2w_forward_render(const w2w_settings* s, const void* geom_state, const w2w_
   b.T_final = at<float>(image_state, IL.T_final);
   b.tile_max = at<uint32_t>(image_state, IL.tile_max);
   b.order = at<uint32_t>(image_state, IL.order);
+  b.order_bwd = at<uint32_t>(image_state, IL.order_bwd);
   launch_blend(b, st);
   return check_launch();
 }
@@ -356,7 +358,7 @@ int w2w_backward(const w2w_settings* s, const float* means3D, const float* scale
   a.point_list = R > 0 ? at<uint32_t>(binning_state, BinLayout(R, num_tiles(W, H)).valsA) : nullptr;
   a.n_contrib = at<uint32_t>(image_state, IL.n_contrib);
   a.tile_max = at<uint32_t>(image_state, IL.tile_max);
-  a.order = at<uint32_t>(image_state, IL.order);
+  a.order_bwd = at<uint32_t>(image_state, IL.order_bwd);
   a.T_final = at<float>(image_state, IL.T_final);
   a.out_alpha = out_alpha;
   a.dL_dcolor = dL_dcolor; a.dL_ddepth = dL_ddepth; a.dL_dalpha = dL_dalpha;
@@ -471,6 +473,7 @@ int w2w_blend(const w2w_settings* s, const void* geom_state, const uint32_t* ran
   b.T_final = at<float>(image_state, IL.T_final);
   b.tile_max = at<uint32_t>(image_state, IL.tile_max);
   b.order = at<uint32_t>(image_state, IL.order);
+  b.order_bwd = at<uint32_t>(image_state, IL.order_bwd);
   launch_blend(b, S(stream));
   return check_launch();
 }

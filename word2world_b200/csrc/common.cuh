@@ -286,7 +286,7 @@ struct GeomLayout {
 };
 
 struct ImageLayout {
-  size_t n_contrib, ranges, T_final, tile_max, order, total;
+  size_t n_contrib, ranges, T_final, tile_max, order, order_bwd, total;
   __host__ __device__ ImageLayout(int W, int H) {
     size_t o = 0;
     auto take = [&](size_t bytes) { size_t a = align256(o); o = a + bytes; return a; };
@@ -297,6 +297,7 @@ struct ImageLayout {
     T_final = take(hw * 4);
     tile_max = take(tiles * 4);
     order = take(tiles * 4);
+    order_bwd = take(tiles * 4);
     total = align256(o);
   }
 };

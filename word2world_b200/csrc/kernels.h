@@ -96,7 +96,8 @@ struct BlendArgs {
   uint32_t* n_contrib;
   float* T_final;
   uint32_t* tile_max;
-  uint32_t* order;  // tiles in processing order (written here, reused by the backward)
+  uint32_t* order;      // tiles by decreasing list length (the blend's processing order)
+  uint32_t* order_bwd;  // tiles by decreasing largest contributor count (the backward's)
 };
 void launch_blend(const BlendArgs& a, cudaStream_t stream);
 
@@ -124,7 +125,8 @@ struct BackwardArgs {
   const uint32_t* point_list;
   const uint32_t* n_contrib;
   const uint32_t* tile_max;
-  const uint32_t* order;   // tile processing order written by the blend
+  const uint32_t* order_bwd;  // tile order by largest contributor count (written by the blend)
+  int split;               // heaviest tiles whose walks are split over two CTAs (set at launch)
   const float* T_final;
   const float* out_alpha;
   const float* dL_dcolor;

@@ -48,10 +48,10 @@ struct TilePixel {
 };
 
 // Tiles are processed heaviest first: CTA b takes tile order[b], where order
-// lists the tiles by decreasing list length (tile_order_kernel), so the
-// longest lists start in the first wave instead of wherever the raster order
-// puts them.
-__global__ void tile_order_kernel(const uint2* ranges, int num_tiles, uint32_t* order);
+// lists the tiles by decreasing weight (tile_order_kernel: the list length
+// from `ranges`, or `counts` when given), so the heaviest start in the first
+// wave instead of wherever the raster order puts them.
+__global__ void tile_order_kernel(const uint2* ranges, const uint32_t* counts, int num_tiles, uint32_t* order);
 
 // One entry's record held in registers between its gather and its store.
 struct ChunkLoad {
