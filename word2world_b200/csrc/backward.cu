@@ -25,15 +25,38 @@ namespace w2w {
 namespace {
 
 constexpr int kValues = 10;
-// Heavy tiles: their warps' walks are split in two at list position
-// mid = walk * kSplitNum / 16.  One CTA runs the back segment [mid, walk) in
-// full; a second CTA first replays the back segment's state recurrences only
-// (alpha and the transmittance / suffix updates, no gradients, no reduction:
-// about a quarter of a full entry's work) to reach the state at mid, then runs
-// [0, mid) in full.  Both compute the state with the same code in the same
-// order, so the second starts from exactly the state the first would have
-// reached; only the order of the atomic additions changes.
-constexpr int kSplitNum = 7;
+// Heavy tiles: each warp's walk is cut into kSplitWays segments, one CTA per
+// segment.  The CTA of a segment first replays the state recurrences of the
+// entries behind it (alpha and the transmittance / suffix updates only: no
+// gradients, no reduction, about kReplayCost of a full entry's work) to reach
+// the state at its segment's end, then walks its segment in full.  All CTAs
+// compute the state with the same code in the same order, so each starts from
+// exactly the state a single walk would have reached; only the order of the
+// atomic additions changes.  Segment lengths (from the back) make the
+// segments' work equal: L_0 = W, L_i = W - kReplayCost * (L_0 + ... + L_{i-1}).
+constexpr int kSplitWays = 2;
+constexpr float kReplayCost = 0.22f;
+
+// List positions [lo, hi) of segment k (0 = the back-most) of a walk of
+// length `walk`.
+__device__ __forceinline__ void segment_of(int walk, int k, int& lo, int& hi) {
+  float len[kSplitWays], before = 0.f, total = 0.f;
+#pragma unroll
+  for (int i = 0; i < kSplitWays; ++i) {
+    len[i] = 1.0f - kReplayCost * before;
+    before += len[i];
+  }
+  total = before;
+  float b0 = 0.f, b1 = 0.f;
+#pragma unroll
+  for (int i = 0; i < kSplitWays; ++i) {
+    if (i < k) b0 += len[i];
+    if (i <= k) b1 += len[i];
+  }
+  hi = walk - int(float(walk) * (b0 / total));
+  lo = k == kSplitWays - 1 ? 0 : walk - int(float(walk) * (b1 / total));
+  lo = max(0, min(lo, hi));
+}
 
 // Where each of the ten per-entry sums goes: after the transposed reduction
 // below, lane L (L even) holds the warp's sum of value (L >> 1); lanes 0..18
@@ -220,17 +243,17 @@ __device__ __forceinline__ void walk_back(const float* records, const uint32_t* 
   }
 }
 
-// CTA b's tile and role: the first 2 * split CTAs are the two halves of the
-// `split` heaviest tiles (role 1: back segment, role 2: front segment), the
-// rest one tile each (role 0), heaviest first.
-__device__ __forceinline__ int cta_tile(const BackwardArgs& a, int& role) {
+// CTA b's tile and segment: the first kSplitWays * split CTAs are the
+// segments of the `split` heaviest tiles (segment 0..kSplitWays-1), the rest
+// one whole tile each (segment -1), heaviest first.
+__device__ __forceinline__ int cta_tile(const BackwardArgs& a, int& seg) {
   const int b = int(blockIdx.x);
-  if (b < 2 * a.split) {
-    role = 1 + (b & 1);
-    return int(a.order_bwd[b >> 1]);
+  if (b < kSplitWays * a.split) {
+    seg = b % kSplitWays;
+    return int(a.order_bwd[b / kSplitWays]);
   }
-  role = 0;
-  return int(a.order_bwd[b - a.split]);
+  seg = -1;
+  return int(a.order_bwd[b - (kSplitWays - 1) * a.split]);
 }
 
 __global__ void __launch_bounds__(kBlendThreads, 2) render_ref_kernel(BackwardArgs a) {
@@ -281,15 +304,14 @@ __global__ void __launch_bounds__(kBlendThreads, 2) render_ref_kernel(BackwardAr
       ch.advance(ok1, b1, b2, al1);
     }
   };
-  const int mid = (p.walk * kSplitNum) / 16;
-  if (role == 0) {
+  if (role < 0) {
     walk_back(a.bwd_record, a.point_list, p.range.x, 0, p.walk, wc, p.tp, full);
-  } else if (role == 1) {
-    walk_back(a.bwd_record, a.point_list, p.range.x, mid, p.walk, wc, p.tp, full);
   } else {
-    walk_back(a.bwd_record, a.point_list, p.range.x, mid, p.walk, wc, p.tp, state_only);
+    int lo, hi;
+    segment_of(p.walk, role, lo, hi);
+    walk_back(a.bwd_record, a.point_list, p.range.x, hi, p.walk, wc, p.tp, state_only);
     __syncwarp();
-    walk_back(a.bwd_record, a.point_list, p.range.x, 0, mid, wc, p.tp, full);
+    walk_back(a.bwd_record, a.point_list, p.range.x, lo, hi, wc, p.tp, full);
   }
 }
 
@@ -433,15 +455,14 @@ __global__ void __launch_bounds__(kBlendThreads, 2) render_exact_kernel(Backward
       ch.advance(ok1, b1, s[kRecVec * j1 + 2], al1);
     }
   };
-  const int mid = (p.walk * kSplitNum) / 16;
-  if (role == 0) {
+  if (role < 0) {
     walk_back(a.record, a.point_list, p.range.x, 0, p.walk, wc, p.tp, full);
-  } else if (role == 1) {
-    walk_back(a.record, a.point_list, p.range.x, mid, p.walk, wc, p.tp, full);
   } else {
-    walk_back(a.record, a.point_list, p.range.x, mid, p.walk, wc, p.tp, state_only);
+    int lo, hi;
+    segment_of(p.walk, role, lo, hi);
+    walk_back(a.record, a.point_list, p.range.x, hi, p.walk, wc, p.tp, state_only);
     __syncwarp();
-    walk_back(a.record, a.point_list, p.range.x, 0, mid, wc, p.tp, full);
+    walk_back(a.record, a.point_list, p.range.x, lo, hi, wc, p.tp, full);
   }
 }
 
@@ -952,8 +973,9 @@ void launch_backward_render(const BackwardArgs& a, cudaStream_t stream) {
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, 0);
   b.split = min(tiles / 4, sms);  // the heaviest tiles by largest contributor count
   stage_begin(kStBwdRender, stream);
-  if (a.grad_mode == 1) render_exact_kernel<<<tiles + b.split, kBlendThreads, 0, stream>>>(b);
-  else render_ref_kernel<<<tiles + b.split, kBlendThreads, 0, stream>>>(b);
+  const int grid = tiles + (kSplitWays - 1) * b.split;
+  if (a.grad_mode == 1) render_exact_kernel<<<grid, kBlendThreads, 0, stream>>>(b);
+  else render_ref_kernel<<<grid, kBlendThreads, 0, stream>>>(b);
   stage_end(kStBwdRender, stream, 1);
 }
 

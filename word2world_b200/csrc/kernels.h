@@ -126,7 +126,7 @@ struct BackwardArgs {
   const uint32_t* n_contrib;
   const uint32_t* tile_max;
   const uint32_t* order_bwd;  // tile order by largest contributor count (written by the blend)
-  int split;               // heaviest tiles whose walks are split over two CTAs (set at launch)
+  int split;               // heaviest tiles whose walks are split over several CTAs (set at launch)
   const float* T_final;
   const float* out_alpha;
   const float* dL_dcolor;
