@@ -182,6 +182,52 @@ int w2w_blend(const w2w_settings* s, const void* geom_state, const uint32_t* ran
 int w2w_binning_keys64(const void* binning_state, long long num_rendered, int width, int height,
                        uint64_t* out, w2w_stream_t stream);
 
+/* ---- batched calls ----------------------------------------------------------
+ * Many views of many scenes rendered and back-propagated with one launch per
+ * stage.  No counterpart in the reference, whose call renders one view; each
+ * item's results equal the single-view entry points' on the same inputs
+ * (bit-identical images and per-tile lists; gradients up to float atomic
+ * order).  Item v's per-view element copies of its scene's Gaussians, tiles
+ * and pixels follow those of items 0..v-1: per-element arrays ([E] = sum of
+ * P) hold item v's Gaussians at [sum_{u<v} P_u, + P_v); images are packed,
+ * item v's colour as its own [3, H_v, W_v] block at 3 * (sum_{u<v} W_u H_u)
+ * and depth / alpha at sum_{u<v} W_u H_u.  All items share one M. */
+typedef struct {
+    const float* means3D;    /* device pointers into the item's scene, as in w2w_forward_geometry */
+    const float* scales;
+    const float* rotations;
+    const float* opacities;
+    const float* shs;
+    int P, M, degree, width, height;
+    float focal_x, tan_fovx, tan_fovy, scale_modifier;
+    float viewmatrix[16];    /* by value (host memory), column-major as in w2w_settings */
+    float projmatrix[16];
+    float campos[3];
+    float background[3];
+} w2w_batch_item;
+
+size_t w2w_batch_geometry_state_bytes(const w2w_batch_item* items, int n);
+size_t w2w_batch_image_state_bytes(const w2w_batch_item* items, int n);
+size_t w2w_batch_binning_state_bytes(long long num_rendered, const w2w_batch_item* items, int n);
+size_t w2w_batch_backward_scratch_bytes(const w2w_batch_item* items, int n);
+/* Projection, colour, culling and the instance scan of every item (radii [E]).
+ * Copies the item table into the geometry state. */
+int w2w_batch_forward_geometry(const w2w_batch_item* items, int n, int compat_spill, int* radii,
+                               void* geom_state, w2w_geometry_info* info, w2w_stream_t stream);
+/* Keys (global tile, depth) of all items, one sort, one blend launch. */
+int w2w_batch_forward_render(const w2w_batch_item* items, int n, const void* geom_state,
+                             const w2w_geometry_info* info, void* binning_state, void* image_state,
+                             float* out_color, float* out_depth, float* out_alpha, w2w_stream_t stream);
+/* Per-element gradients ([E, ...]; a scene's gradient is the sum over its
+ * items' element ranges). */
+int w2w_batch_backward(const w2w_batch_item* items, int n, const void* geom_state, long long num_rendered,
+                       const void* binning_state, const void* image_state, const int* radii,
+                       const float* out_alpha, const float* dL_dcolor, const float* dL_ddepth,
+                       const float* dL_dalpha, int grad_mode, void* scratch, size_t scratch_bytes,
+                       float* dL_dmeans2D, float* dL_dcolors, float* dL_dopacity, float* dL_dmeans3D,
+                       float* dL_dcov3D, float* dL_dsh, float* dL_dscales, float* dL_drotations,
+                       w2w_stream_t stream);
+
 /* ---- observability ---------------------------------------------------------
  * Number of kernels the library has launched in this process. */
 unsigned long long w2w_launch_count(void);

@@ -1,0 +1,251 @@
+"""Batched rendering: many views of many scenes with one launch per stage.
+
+The reference renders one view per call (``Renderer.render`` ->
+``rasterize_gaussians`` / ``rasterize_gaussians_backward``).  A batch here is a
+list of items, each one view (camera, resolution, background) of one scene
+(its activated parameter tensors, resident on the device); the whole batch is
+projected, culled, scanned, keyed, sorted, blended and back-propagated with
+one launch per stage through the C ABI's ``w2w_batch_*`` entry points
+(include/w2w_raster.h).  Each item's image equals what a single-view call
+returns for it (bit-identical), and its gradients equal the single-view
+call's up to the order of float atomic additions.
+
+Keys are (global tile, depth): one sort serves every item, and every tile's
+list is exactly the list its item alone would produce, including the
+reference's key-emission spill (the instance scan restarts its spill
+component at every item).
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from dataclasses import dataclass, field
+
+import numpy as np
+import torch
+
+from . import _C  # noqa: F401  (loads libw2w_raster.so through the binding; also fails loudly when unbuilt)
+from .camera import Camera
+
+_LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "libw2w_raster.so")
+_lib = None
+
+GRAD_MODES = {"reference": 0, "exact": 1}
+
+
+class _Item(ctypes.Structure):
+    _fields_ = [("means3D", ctypes.c_void_p), ("scales", ctypes.c_void_p), ("rotations", ctypes.c_void_p),
+                ("opacities", ctypes.c_void_p), ("shs", ctypes.c_void_p),
+                ("P", ctypes.c_int), ("M", ctypes.c_int), ("degree", ctypes.c_int), ("width", ctypes.c_int),
+                ("height", ctypes.c_int),
+                ("focal_x", ctypes.c_float), ("tan_fovx", ctypes.c_float), ("tan_fovy", ctypes.c_float),
+                ("scale_modifier", ctypes.c_float),
+                ("viewmatrix", ctypes.c_float * 16), ("projmatrix", ctypes.c_float * 16),
+                ("campos", ctypes.c_float * 3), ("background", ctypes.c_float * 3)]
+
+
+class _Info(ctypes.Structure):
+    _fields_ = [("num_rendered", ctypes.c_longlong), ("depth_min_bits", ctypes.c_uint32),
+                ("depth_max_bits", ctypes.c_uint32), ("error", ctypes.c_uint32), ("reserved", ctypes.c_uint32)]
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        L = ctypes.CDLL(_LIB_PATH)
+        for fn in ("w2w_batch_geometry_state_bytes", "w2w_batch_image_state_bytes",
+                   "w2w_batch_binning_state_bytes", "w2w_batch_backward_scratch_bytes"):
+            getattr(L, fn).restype = ctypes.c_size_t
+        L.w2w_batch_binning_state_bytes.argtypes = [ctypes.c_longlong, ctypes.c_void_p, ctypes.c_int]
+        L.w2w_status_string.restype = ctypes.c_char_p
+        _lib = L
+    return _lib
+
+
+def _check(rc: int, what: str):
+    if rc != 0:
+        raise RuntimeError(f"{what}: {lib().w2w_status_string(rc).decode()} (status {rc})")
+
+
+@dataclass
+class Scene:
+    """Activated parameters of one scene, resident on the device (the
+    reference's ``Renderer.render`` inputs after its activation preamble)."""
+    means3D: torch.Tensor     # [P,3]
+    opacities: torch.Tensor   # [P,1]
+    scales: torch.Tensor      # [P,3]
+    rotations: torch.Tensor   # [P,4] (w, x, y, z)
+    shs: torch.Tensor         # [P,M,3]
+    sh_degree: int = 3
+
+    @property
+    def P(self) -> int:
+        return int(self.means3D.shape[0])
+
+    @classmethod
+    def from_arrays(cls, arrays, device, sh_degree: int = 3) -> "Scene":
+        m, o, s, q, sh = arrays
+        t = lambda a: torch.from_numpy(np.ascontiguousarray(a, dtype=np.float32)).to(device)
+        return cls(t(m), t(o), t(s), t(q), t(sh), sh_degree)
+
+
+@dataclass
+class View:
+    scene: int                 # index into the batch's scene list
+    camera: Camera
+    background: tuple = (1.0, 1.0, 1.0)
+
+
+@dataclass
+class BatchResult:
+    """Forward outputs of a batch; ``color[v]`` etc. are views into the
+    packed buffers."""
+    color: list
+    depth: list
+    alpha: list
+    radii: list
+    num_rendered: int
+    state: dict = field(repr=False, default_factory=dict)
+
+
+class BatchRenderer:
+    """Forward + backward of a list of (scene, view) items, one launch per stage."""
+
+    def __init__(self, grad_mode: str = "reference", compat_spill: bool = True, device=None):
+        self.grad_mode = GRAD_MODES[grad_mode]
+        self.compat_spill = int(bool(compat_spill))
+        self.device = torch.device(device) if device is not None else torch.device("cuda", torch.cuda.current_device())
+
+    # ---- item table -------------------------------------------------------
+    def _items(self, scenes, views):
+        n = len(views)
+        arr = (_Item * n)()
+        M = None
+        for v, view in enumerate(views):
+            sc = scenes[view.scene]
+            for name in ("means3D", "opacities", "scales", "rotations", "shs"):
+                t = getattr(sc, name)
+                if not (t.is_cuda and t.dtype == torch.float32 and t.is_contiguous()):
+                    raise ValueError(f"scene {view.scene}: {name} must be a contiguous float32 CUDA tensor")
+            m = int(sc.shs.shape[1])
+            if M is None:
+                M = m
+            elif m != M:
+                raise ValueError("all scenes of a batch need the same number of SH coefficients")
+            cam = view.camera
+            it = arr[v]
+            it.means3D, it.scales, it.rotations = sc.means3D.data_ptr(), sc.scales.data_ptr(), sc.rotations.data_ptr()
+            it.opacities, it.shs = sc.opacities.data_ptr(), sc.shs.data_ptr()
+            it.P, it.M, it.degree = sc.P, m, int(sc.sh_degree)
+            it.width, it.height = int(cam.width), int(cam.height)
+            it.focal_x = float(cam.focal_x)
+            it.tan_fovx, it.tan_fovy = float(cam.tanfovx), float(cam.tanfovy)
+            it.scale_modifier = 1.0
+            it.viewmatrix[:] = [float(x) for x in np.asarray(cam.viewmatrix, np.float32).reshape(-1)]
+            it.projmatrix[:] = [float(x) for x in np.asarray(cam.projmatrix, np.float32).reshape(-1)]
+            it.campos[:] = [float(x) for x in np.asarray(cam.campos, np.float32).reshape(-1)]
+            it.background[:] = [float(x) for x in view.background]
+        return arr, M
+
+    @staticmethod
+    def layout(views):
+        """First pixel of every item in the packed per-pixel buffers (colour:
+        three times that), and the total pixel count."""
+        pb, p = [], 0
+        for v in views:
+            pb.append(p)
+            p += int(v.camera.width) * int(v.camera.height)
+        return pb, p
+
+    # ---- forward ------------------------------------------------------------
+    def forward(self, scenes, views) -> BatchResult:
+        L = lib()
+        arr, M = self._items(scenes, views)
+        n = len(views)
+        stream = ctypes.c_void_p(torch.cuda.current_stream(self.device).cuda_stream)
+        E = sum(scenes[v.scene].P for v in views)
+        dev = self.device
+        geom = torch.empty(int(L.w2w_batch_geometry_state_bytes(arr, n)), dtype=torch.uint8, device=dev)
+        radii = torch.empty(max(E, 1), dtype=torch.int32, device=dev)
+        info = _Info()
+        _check(L.w2w_batch_forward_geometry(arr, n, self.compat_spill, ctypes.c_void_p(radii.data_ptr()),
+                                            ctypes.c_void_p(geom.data_ptr()), ctypes.byref(info), stream),
+               "batch forward geometry")
+        R = int(info.num_rendered)
+        binb = torch.empty(max(int(L.w2w_batch_binning_state_bytes(R, arr, n)), 1), dtype=torch.uint8, device=dev)
+        img = torch.empty(int(L.w2w_batch_image_state_bytes(arr, n)), dtype=torch.uint8, device=dev)
+        pbase, npix = self.layout(views)
+        color = torch.empty(3 * npix, dtype=torch.float32, device=dev)
+        depth = torch.empty(npix, dtype=torch.float32, device=dev)
+        alpha = torch.empty(npix, dtype=torch.float32, device=dev)
+        _check(L.w2w_batch_forward_render(arr, n, ctypes.c_void_p(geom.data_ptr()), ctypes.byref(info),
+                                          ctypes.c_void_p(binb.data_ptr()), ctypes.c_void_p(img.data_ptr()),
+                                          ctypes.c_void_p(color.data_ptr()), ctypes.c_void_p(depth.data_ptr()),
+                                          ctypes.c_void_p(alpha.data_ptr()), stream), "batch forward render")
+        cols, deps, alps, rads = [], [], [], []
+        e = 0
+        for v, view in enumerate(views):
+            H, W = int(view.camera.height), int(view.camera.width)
+            p = pbase[v]
+            cols.append(color[3 * p:3 * p + 3 * H * W].view(3, H, W))
+            deps.append(depth[p:p + H * W].view(1, H, W))
+            alps.append(alpha[p:p + H * W].view(1, H, W))
+            P = scenes[view.scene].P
+            rads.append(radii[e:e + P])
+            e += P
+        state = dict(arr=arr, n=n, M=M, E=E, R=R, geom=geom, binb=binb, img=img, radii=radii, alpha=alpha,
+                     npix=npix, pbase=pbase, scenes=scenes, views=views)
+        return BatchResult(cols, deps, alps, rads, R, state)
+
+    # ---- backward -----------------------------------------------------------
+    def backward(self, res: BatchResult, dL_dcolor, dL_ddepth=None, dL_dalpha=None, per_element: bool = False):
+        """Gradients for upstream image gradients given per item (lists of
+        [3,H,W] / [1,H,W] tensors).  Returns, per scene, the sum over its
+        items of dL/d(means3D, opacity, scales, rotations, shs) plus the
+        per-item dL/dmeans2D; ``per_element`` also returns the raw per-item
+        tensors (the single-view call's eight outputs for every item)."""
+        L = lib()
+        st = res.state
+        arr, n, M, E, R = st["arr"], st["n"], st["M"], st["E"], st["R"]
+        dev = self.device
+        stream = ctypes.c_void_p(torch.cuda.current_stream(dev).cuda_stream)
+        views, scenes = st["views"], st["scenes"]
+        dlc = torch.cat([g.reshape(-1) for g in dL_dcolor]).contiguous()
+        zeros = torch.zeros(st["npix"], dtype=torch.float32, device=dev)
+        dld = torch.cat([g.reshape(-1) for g in dL_ddepth]).contiguous() if dL_ddepth is not None else zeros
+        dla = torch.cat([g.reshape(-1) for g in dL_dalpha]).contiguous() if dL_dalpha is not None else zeros
+        scratch = torch.empty(int(L.w2w_batch_backward_scratch_bytes(arr, n)), dtype=torch.uint8, device=dev)
+        f = lambda *s: torch.empty(*s, dtype=torch.float32, device=dev)
+        Eg = max(E, 1)
+        g_m2, g_col, g_op = f(Eg, 3), f(Eg, 3), f(Eg, 1)
+        g_m3, g_cov, g_sh, g_sc, g_rot = f(Eg, 3), f(Eg, 6), f(Eg, max(M, 1), 3), f(Eg, 3), f(Eg, 4)
+        p = lambda t: ctypes.c_void_p(t.data_ptr())
+        _check(L.w2w_batch_backward(arr, n, p(st["geom"]), ctypes.c_longlong(R), p(st["binb"]), p(st["img"]),
+                                    p(st["radii"]), p(st["alpha"]), p(dlc), p(dld), p(dla), self.grad_mode,
+                                    p(scratch), ctypes.c_size_t(scratch.numel()), p(g_m2), p(g_col), p(g_op),
+                                    p(g_m3), p(g_cov), p(g_sh), p(g_sc), p(g_rot), stream), "batch backward")
+        # per-scene sums of the items' element ranges (one index_add per tensor)
+        offsets, total = [], 0
+        for sc in scenes:
+            offsets.append(total)
+            total += sc.P
+        idx = torch.cat([torch.arange(scenes[v.scene].P, device=dev) + offsets[v.scene] for v in views])
+        out = {}
+        for name, t in (("means3D", g_m3), ("opacities", g_op), ("scales", g_sc), ("rotations", g_rot),
+                        ("shs", g_sh)):
+            acc = torch.zeros((total,) + tuple(t.shape[1:]), dtype=torch.float32, device=dev)
+            acc.index_add_(0, idx, t[:E])
+            out[name] = [acc[offsets[s]:offsets[s] + scenes[s].P] for s in range(len(scenes))]
+        e = 0
+        out["means2D"] = []
+        raw = []
+        for v in views:
+            P = scenes[v.scene].P
+            out["means2D"].append(g_m2[e:e + P])
+            if per_element:
+                raw.append((g_m2[e:e + P], g_col[e:e + P], g_op[e:e + P], g_m3[e:e + P], g_cov[e:e + P],
+                            g_sh[e:e + P], g_sc[e:e + P], g_rot[e:e + P]))
+            e += P
+        if per_element:
+            out["per_item"] = raw
+        return out

@@ -115,19 +115,25 @@ struct BwdPixel {
   int walk;  // list positions [0, walk) may hold contributors of this warp's pixels
   uint32_t last, warp_last;
   float dLp0 = 0.f, dLp1 = 0.f, dLp2 = 0.f, dLd = 0.f, dLa = 0.f;
-  __device__ __forceinline__ BwdPixel(const BackwardArgs& a, int tile_)
-      : tile(tile_), tp(tile_, (a.W + kTile - 1) / kTile) {
-    inside = tp.px < a.W && tp.py < a.H;
+  int W, H;         // this tile's image size
+  size_t pbase;     // its first pixel in the (packed) per-pixel buffers
+  const float* bg;
+  __device__ __forceinline__ BwdPixel(const BackwardArgs& a, int tile_, int local_tile, int W_, int H_, size_t pbase_,
+                                      const float* bg_)
+      : tile(tile_), tp(local_tile, (W_ + kTile - 1) / kTile), W(W_), H(H_), pbase(pbase_), bg(bg_) {
+    inside = tp.px < W && tp.py < H;
     range = a.ranges[tile];
-    pix = inside ? size_t(tp.py) * a.W + tp.px : 0;
-    hw = size_t(a.W) * a.H;
+    hw = size_t(W) * H;
+    pix = inside ? pbase + size_t(tp.py) * W + tp.px : 0;
     last = inside ? a.n_contrib[pix] : 0u;
     warp_last = __reduce_max_sync(0xffffffffu, last);
     walk = int(min(warp_last, range.y - range.x));
     if (inside) {
-      dLp0 = a.dL_dcolor[pix];
-      dLp1 = a.dL_dcolor[hw + pix];
-      dLp2 = a.dL_dcolor[2 * hw + pix];
+      // colour planes: an image's three planes sit together at 3 * pbase
+      const size_t cp = 3 * pbase + (pix - pbase);
+      dLp0 = a.dL_dcolor[cp];
+      dLp1 = a.dL_dcolor[hw + cp];
+      dLp2 = a.dL_dcolor[2 * hw + cp];
       dLd = a.dL_ddepth[pix];
       dLa = a.dL_dalpha[pix];
     }
@@ -246,6 +252,18 @@ __device__ __forceinline__ void walk_back(const float* records, const uint32_t* 
 // CTA b's tile and segment: the first kSplitWays * split CTAs are the
 // segments of the `split` heaviest tiles (segment 0..kSplitWays-1), the rest
 // one whole tile each (segment -1), heaviest first.
+// Pixel-loop prologue for CTA blockIdx.x: its tile's image (the call's, or its
+// batch item's) and segment role.
+__device__ __forceinline__ BwdPixel make_bwd_pixel(const BackwardArgs& a, int tile, const float*& bg) {
+  if (a.items == nullptr) {
+    bg = a.bg;
+    return BwdPixel(a, tile, tile, a.W, a.H, 0, a.bg);
+  }
+  const BatchItem& it = a.items[find_item_tile(a.items, a.num_items, uint32_t(tile))];
+  bg = it.bg;
+  return BwdPixel(a, tile, tile - int(it.tile_base), it.W, it.H, size_t(it.pix_base), it.bg);
+}
+
 __device__ __forceinline__ int cta_tile(const BackwardArgs& a, int& seg) {
   const int b = int(blockIdx.x);
   if (b < kSplitWays * a.split) {
@@ -259,12 +277,14 @@ __device__ __forceinline__ int cta_tile(const BackwardArgs& a, int& seg) {
 __global__ void __launch_bounds__(kBlendThreads, 2) render_ref_kernel(BackwardArgs a) {
   __shared__ WarpChunk s_chunk[kBlendThreads / 32];
   int role;
-  const BwdPixel p(a, cta_tile(a, role));
+  const int gtile = cta_tile(a, role);
+  const float* bgp;
+  const BwdPixel p = make_bwd_pixel(a, gtile, bgp);
   RefChain ch;
   ch.T_final = p.inside ? 1.0f - a.out_alpha[p.pix] : 0.0f;
   ch.T = ch.T_final;
-  ch.bg_dot = a.bg[0] * p.dLp0 + a.bg[1] * p.dLp1 + a.bg[2] * p.dLp2;
-  const float ddelx_dx = 0.5f * float(a.W), ddely_dy = 0.5f * float(a.H);
+  ch.bg_dot = bgp[0] * p.dLp0 + bgp[1] * p.dLp1 + bgp[2] * p.dLp2;
+  const float ddelx_dx = 0.5f * float(p.W), ddely_dy = 0.5f * float(p.H);
   const float pxf = float(p.tp.px), pyf = float(p.tp.py);
   const Target tgt = lane_target(a, 0);
   WarpChunk& wc = s_chunk[threadIdx.x >> 5];
@@ -390,14 +410,16 @@ struct ExactChain {
 __global__ void __launch_bounds__(kBlendThreads, 2) render_exact_kernel(BackwardArgs a) {
   __shared__ WarpChunk s_chunk[kBlendThreads / 32];
   int role;
-  const BwdPixel p(a, cta_tile(a, role));
+  const int gtile = cta_tile(a, role);
+  const float* bgp;
+  const BwdPixel p = make_bwd_pixel(a, gtile, bgp);
   ExactChain ch;
   const float Tf = p.inside ? a.T_final[p.pix] : 0.0f;
   ch.T = Tf;
-  ch.S0 = Tf * a.bg[0];
-  ch.S1 = Tf * a.bg[1];
-  ch.S2 = Tf * a.bg[2];
-  const float hW = 0.5f * float(a.W), hH = 0.5f * float(a.H);
+  ch.S0 = Tf * bgp[0];
+  ch.S1 = Tf * bgp[1];
+  ch.S2 = Tf * bgp[2];
+  const float hW = 0.5f * float(p.W), hH = 0.5f * float(p.H);
   const float pxf = float(p.tp.px), pyf = float(p.tp.py);
   const Target tgt = lane_target(a, 1);
   WarpChunk& wc = s_chunk[threadIdx.x >> 5];
@@ -551,16 +573,41 @@ __constant__ float kSH_C3[7] = {-0.5900435899266435f, 2.890611442640554f, -0.457
                                 0.3731763325901154f,  -0.4570457994644658f, 1.445305721320277f,
                                 -0.5900435899266435f};
 
+// The scene and camera of one element: the call's, or its batch item's.
+struct GView {
+  const float* means3D;
+  const float* scales;
+  const float* rotations;
+  const float* mats;  // view (16), projection (16), camera position (3)
+  int gi;             // index within the scene
+  int W, degree;
+  float h_x, h_y, tan_fovx, tan_fovy, focal_x, scale_modifier;
+};
+
+__device__ __forceinline__ GView make_gview(const BackwardArgs& a, int i, const float* s_mats) {
+  GView g;
+  if (a.items == nullptr) {
+    g = GView{a.means3D, a.scales, a.rotations, s_mats, i, a.W, a.degree, a.h_x, a.h_y, a.tan_fovx, a.tan_fovy,
+              a.focal_x, a.scale_modifier};
+  } else {
+    const BatchItem& it = a.items[find_item_elem(a.items, a.num_items, uint32_t(i))];
+    g = GView{it.means3D, it.scales, it.rotations, it.view, i - int(it.elem_base), it.W, it.degree, it.h_x, it.h_y,
+              it.tan_fovx, it.tan_fovy, it.h_x, it.scale_modifier};
+  }
+  return g;
+}
+
 // One Gaussian (radius > 0) of the reference-formula pass: every output but
 // dL_dsh, plus the SH basis and masked colour gradient dL_dsh is built from.
 // sh_row: this Gaussian's SH coefficients (staged in shared memory).
-__device__ __forceinline__ void ref_gaussian(const BackwardArgs& a, int i, const float* sh_row, const float* mats, float (&basis)[16],
+__device__ __forceinline__ void ref_gaussian(const BackwardArgs& a, int i, const GView& gv, const float* sh_row, float (&basis)[16],
                                              float (&cf)[3]) {
   const int M = a.M;
+  const float* mats = gv.mats;
   const float* cam = mats + 32;
   const float* view = mats;
   const float* proj = mats + 16;
-  const float cx = __ldg(&a.means3D[3 * i]), cy = __ldg(&a.means3D[3 * i + 1]), cz = __ldg(&a.means3D[3 * i + 2]);
+  const float cx = __ldg(&gv.means3D[3 * gv.gi]), cy = __ldg(&gv.means3D[3 * gv.gi + 1]), cz = __ldg(&gv.means3D[3 * gv.gi + 2]);
   const float* pc = a.cov3D + 6 * size_t(i);  // read with __ldg below
 
   // ---- computeCov2DCUDA ----
@@ -572,7 +619,7 @@ __device__ __forceinline__ void ref_gaussian(const BackwardArgs& a, int i, const
   vx *= w_inv;
   vy *= w_inv;
   vz *= w_inv;
-  const float bound_x = 1.3f * a.tan_fovx, bound_y = 1.3f * a.tan_fovy;
+  const float bound_x = 1.3f * gv.tan_fovx, bound_y = 1.3f * gv.tan_fovy;
   const float proj_x = vx / vz, proj_y = vy / vz;
   const float cpx = fminf(bound_x, fmaxf(-bound_x, proj_x));
   const float cpy = fminf(bound_y, fmaxf(-bound_y, proj_y));
@@ -580,7 +627,7 @@ __device__ __forceinline__ void ref_gaussian(const BackwardArgs& a, int i, const
   const float mask_x = (proj_x >= -bound_x && proj_x <= bound_x) ? 1.0f : 0.0f;
   const float mask_y = (proj_y >= -bound_y && proj_y <= bound_y) ? 1.0f : 0.0f;
   const float z_inv = 1.0f / vz, z_inv2 = z_inv * z_inv;
-  const float h_x = a.h_x, h_y = a.h_y;
+  const float h_x = gv.h_x, h_y = gv.h_y;
   // J (glm column-major J[col][row]) and T = W * J
   const float J[3][3] = {{h_x * z_inv, 0.f, -h_x * px * z_inv2}, {0.f, h_y * z_inv, -h_y * py * z_inv2}, {0.f, 0.f, 0.f}};
   const float Wv[3][3] = {{view[0], view[4], view[8]}, {view[1], view[5], view[9]}, {view[2], view[6], view[10]}};
@@ -714,13 +761,13 @@ __device__ __forceinline__ void ref_gaussian(const BackwardArgs& a, int i, const
   a.dL_dmeans3D[3 * i + 2] = sd[2];
 
   // ---- scale / rotation (backward.cu:446-518) ----
-  const float qw = __ldg(&a.rotations[4 * i]), qx = __ldg(&a.rotations[4 * i + 1]), qy = __ldg(&a.rotations[4 * i + 2]),
-              qz = __ldg(&a.rotations[4 * i + 3]);
+  const float qw = __ldg(&gv.rotations[4 * gv.gi]), qx = __ldg(&gv.rotations[4 * gv.gi + 1]), qy = __ldg(&gv.rotations[4 * gv.gi + 2]),
+              qz = __ldg(&gv.rotations[4 * gv.gi + 3]);
   const float xx = qx * qx, yy = qy * qy, zz = qz * qz;
   const float qxy = qx * qy, qxz = qx * qz, qyz = qy * qz;
   const float xw = qx * qw, yw = qy * qw, zw = qz * qw;
-  const float sx = a.scale_modifier * __ldg(&a.scales[3 * i]), sy = a.scale_modifier * __ldg(&a.scales[3 * i + 1]),
-              sz = a.scale_modifier * __ldg(&a.scales[3 * i + 2]);
+  const float sx = gv.scale_modifier * __ldg(&gv.scales[3 * gv.gi]), sy = gv.scale_modifier * __ldg(&gv.scales[3 * gv.gi + 1]),
+              sz = gv.scale_modifier * __ldg(&gv.scales[3 * gv.gi + 2]);
   const float m11 = sx * (1.f - 2.f * (yy + zz)), m12 = sx * 2.f * (qxy - zw), m13 = sx * 2.f * (qxz + yw);
   const float m21 = sy * 2.f * (qxy + zw), m22 = sy * (1.f - 2.f * (xx + zz)), m23 = sy * 2.f * (qyz - xw);
   const float m31 = sz * 2.f * (qxz - yw), m32 = sz * 2.f * (qyz + xw), m33 = sz * (1.f - 2.f * (xx + yy));
@@ -753,9 +800,11 @@ __global__ void __launch_bounds__(kGaussThreads) gaussians_ref_kernel(BackwardAr
   // view, projection, camera position: shared memory is never aliased by the
   // outputs, so these stay in place across the output stores
   __shared__ float s_mats[35];
-  if (threadIdx.x < 16) s_mats[threadIdx.x] = a.view[threadIdx.x];
-  else if (threadIdx.x < 32) s_mats[threadIdx.x] = a.proj[threadIdx.x - 16];
-  else if (threadIdx.x < 35) s_mats[threadIdx.x] = a.campos[threadIdx.x - 32];
+  if (a.items == nullptr) {  // a batched call's matrices live in its item table
+    if (threadIdx.x < 16) s_mats[threadIdx.x] = a.view[threadIdx.x];
+    else if (threadIdx.x < 32) s_mats[threadIdx.x] = a.proj[threadIdx.x - 16];
+    else if (threadIdx.x < 35) s_mats[threadIdx.x] = a.campos[threadIdx.x - 32];
+  }
   __syncthreads();
   const int lane = threadIdx.x & 31;
   float* sw = s_sh[threadIdx.x >> 5];
@@ -764,11 +813,21 @@ __global__ void __launch_bounds__(kGaussThreads) gaussians_ref_kernel(BackwardAr
   const int n = min(32, a.P - i0);
   const int i = i0 + lane;
   const int stride = sh_stride(a.M);
-  sh_stage_in(a.shs, a.M, i0, n, sw, stride);
+  const GView gv = make_gview(a, lane < n ? i : i0, s_mats);
+  if (a.items == nullptr) {
+    sh_stage_in(a.shs, a.M, i0, n, sw, stride);
+  } else {  // a warp's elements may belong to different scenes: each thread its own row
+    const int rs = 3 * (a.M < 16 ? a.M : 16);
+    if (lane < n) {
+      const float* row = a.items[find_item_elem(a.items, a.num_items, uint32_t(i))].shs + size_t(gv.gi) * 3 * a.M;
+      for (int c = 0; c < rs; ++c) sw[lane * stride + c] = __ldg(row + c);
+    }
+    __syncwarp();
+  }
   float basis[16], cf[3] = {0.f, 0.f, 0.f};
   const bool active = lane < n && a.radii[i] > 0;
   if (active) {
-    ref_gaussian(a, i, sw + lane * stride, s_mats, basis, cf);
+    ref_gaussian(a, i, gv, sw + lane * stride, basis, cf);
   } else if (lane < n) {
     for (int k = 0; k < 3; ++k) a.dL_dmeans3D[3 * i + k] = 0.f;
     for (int k = 0; k < 6; ++k) a.dL_dcov3D[6 * i + k] = 0.f;
@@ -782,13 +841,14 @@ __global__ void __launch_bounds__(kGaussThreads) gaussians_ref_kernel(BackwardAr
 // Per-Gaussian, exact derivative of the forward.
 // One Gaussian (radius > 0) of the exact-derivative pass: every output but
 // dL_dsh, plus the outer-product factors of dL_dsh (see ref_gaussian).
-__device__ __forceinline__ void exact_gaussian(const BackwardArgs& a, int i, const float* sh_row, const float* mats,
+__device__ __forceinline__ void exact_gaussian(const BackwardArgs& a, int i, const GView& gv, const float* sh_row,
                                                float (&basis)[16], float (&cf)[3]) {
   const int M = a.M;
+  const float* mats = gv.mats;
   const float* cam = mats + 32;
   const float* V = mats;
   const float* PM = mats + 16;
-  const float m0 = __ldg(&a.means3D[3 * i]), m1 = __ldg(&a.means3D[3 * i + 1]), m2 = __ldg(&a.means3D[3 * i + 2]);
+  const float m0 = __ldg(&gv.means3D[3 * gv.gi]), m1 = __ldg(&gv.means3D[3 * gv.gi + 1]), m2 = __ldg(&gv.means3D[3 * gv.gi + 2]);
   float gm[3] = {0.f, 0.f, 0.f};
   // screen position / depth: ndc = clip.xyz / (clip.w + 1e-5); dL_dmean2D already holds dL/dNDC
   float clip[4];
@@ -801,13 +861,13 @@ __device__ __forceinline__ void exact_gaussian(const BackwardArgs& a, int i, con
   // covariance chain
   float t[3];
   for (int r = 0; r < 3; ++r) t[r] = V[r] * m0 + V[4 + r] * m1 + V[8 + r] * m2 + V[12 + r];
-  const float L = float(a.W) / (2.0f * a.focal_x);
+  const float L = float(gv.W) / (2.0f * gv.focal_x);
   const float rx = t[0] / t[2], ry = t[1] / t[2];
   const float nn = sqrtf(rx * rx + ry * ry) / L;
   const bool clampd = nn > 1.0f;
   float txp = t[0], typ = t[1];
   if (clampd) { txp = rx / nn * t[2]; typ = ry / nn * t[2]; }
-  const float tz = t[2], f = a.focal_x;
+  const float tz = t[2], f = gv.focal_x;
   const float rgt[3] = {V[0], V[4], V[8]}, upv[3] = {V[1], V[5], V[9]}, fw[3] = {V[2], V[6], V[10]};
   float jx[3], jy[3];
   for (int k = 0; k < 3; ++k) {
@@ -854,11 +914,11 @@ __device__ __forceinline__ void exact_gaussian(const BackwardArgs& a, int i, con
   for (int c = 0; c < 3; ++c)
     for (int r = 0; r < 3; ++r) gm[c] += V[4 * c + r] * gt[r];
   // Sigma = M M^T, M = R diag(s)
-  const float w = __ldg(&a.rotations[4 * i]), x = __ldg(&a.rotations[4 * i + 1]), y = __ldg(&a.rotations[4 * i + 2]), z = __ldg(&a.rotations[4 * i + 3]);
+  const float w = __ldg(&gv.rotations[4 * gv.gi]), x = __ldg(&gv.rotations[4 * gv.gi + 1]), y = __ldg(&gv.rotations[4 * gv.gi + 2]), z = __ldg(&gv.rotations[4 * gv.gi + 3]);
   const float R[3][3] = {{1.f - 2.f * (y * y + z * z), 2.f * (x * y - w * z), 2.f * (x * z + w * y)},
                          {2.f * (x * y + w * z), 1.f - 2.f * (x * x + z * z), 2.f * (y * z - w * x)},
                          {2.f * (x * z - w * y), 2.f * (y * z + w * x), 1.f - 2.f * (x * x + y * y)}};
-  const float s[3] = {__ldg(&a.scales[3 * i]), __ldg(&a.scales[3 * i + 1]), __ldg(&a.scales[3 * i + 2])};
+  const float s[3] = {__ldg(&gv.scales[3 * gv.gi]), __ldg(&gv.scales[3 * gv.gi + 1]), __ldg(&gv.scales[3 * gv.gi + 2])};
   float dM[3][3];
   for (int p = 0; p < 3; ++p)
     for (int k = 0; k < 3; ++k) {
@@ -909,7 +969,7 @@ __device__ __forceinline__ void exact_gaussian(const BackwardArgs& a, int i, con
   b[13] = -C32 * X * (4.f * zz - xx - yy); db[13][0] = -C32 * (4.f * zz - 3.f * xx - yy); db[13][1] = 2.f * C32 * X * Y; db[13][2] = -8.f * C32 * X * Z;
   b[14] = C35 * Z * (xx - yy); db[14][0] = 2.f * C35 * X * Z; db[14][1] = -2.f * C35 * Y * Z; db[14][2] = C35 * (xx - yy);
   b[15] = -C30 * X * (xx - 3.f * yy); db[15][0] = -C30 * (3.f * xx - 3.f * yy); db[15][1] = 6.f * C30 * X * Y;
-  int de = a.degree > 3 ? 3 : a.degree;
+  int de = gv.degree > 3 ? 3 : gv.degree;
   while (de > 0 && (de + 1) * (de + 1) > M) --de;
   const int nb = (de + 1) * (de + 1);
   const float* shd = sh_row;
@@ -938,9 +998,11 @@ __global__ void __launch_bounds__(kGaussThreads) gaussians_exact_kernel(Backward
   // view, projection, camera position: shared memory is never aliased by the
   // outputs, so these stay in place across the output stores
   __shared__ float s_mats[35];
-  if (threadIdx.x < 16) s_mats[threadIdx.x] = a.view[threadIdx.x];
-  else if (threadIdx.x < 32) s_mats[threadIdx.x] = a.proj[threadIdx.x - 16];
-  else if (threadIdx.x < 35) s_mats[threadIdx.x] = a.campos[threadIdx.x - 32];
+  if (a.items == nullptr) {  // a batched call's matrices live in its item table
+    if (threadIdx.x < 16) s_mats[threadIdx.x] = a.view[threadIdx.x];
+    else if (threadIdx.x < 32) s_mats[threadIdx.x] = a.proj[threadIdx.x - 16];
+    else if (threadIdx.x < 35) s_mats[threadIdx.x] = a.campos[threadIdx.x - 32];
+  }
   __syncthreads();
   const int lane = threadIdx.x & 31;
   float* sw = s_sh[threadIdx.x >> 5];
@@ -949,11 +1011,21 @@ __global__ void __launch_bounds__(kGaussThreads) gaussians_exact_kernel(Backward
   const int n = min(32, a.P - i0);
   const int i = i0 + lane;
   const int stride = sh_stride(a.M);
-  sh_stage_in(a.shs, a.M, i0, n, sw, stride);
+  const GView gv = make_gview(a, lane < n ? i : i0, s_mats);
+  if (a.items == nullptr) {
+    sh_stage_in(a.shs, a.M, i0, n, sw, stride);
+  } else {  // a warp's elements may belong to different scenes: each thread its own row
+    const int rs = 3 * (a.M < 16 ? a.M : 16);
+    if (lane < n) {
+      const float* row = a.items[find_item_elem(a.items, a.num_items, uint32_t(i))].shs + size_t(gv.gi) * 3 * a.M;
+      for (int c = 0; c < rs; ++c) sw[lane * stride + c] = __ldg(row + c);
+    }
+    __syncwarp();
+  }
   float basis[16], cf[3] = {0.f, 0.f, 0.f};
   const bool active = lane < n && a.radii[i] > 0;
   if (active) {
-    exact_gaussian(a, i, sw + lane * stride, s_mats, basis, cf);
+    exact_gaussian(a, i, gv, sw + lane * stride, basis, cf);
   } else if (lane < n) {
     for (int k = 0; k < 3; ++k) a.dL_dmeans3D[3 * i + k] = 0.f;
     for (int k = 0; k < 6; ++k) a.dL_dcov3D[6 * i + k] = 0.f;
@@ -966,7 +1038,7 @@ __global__ void __launch_bounds__(kGaussThreads) gaussians_exact_kernel(Backward
 }  // namespace
 
 void launch_backward_render(const BackwardArgs& a, cudaStream_t stream) {
-  const int tiles = ((a.W + kTile - 1) / kTile) * ((a.H + kTile - 1) / kTile);
+  const int tiles = a.items ? a.total_tiles : ((a.W + kTile - 1) / kTile) * ((a.H + kTile - 1) / kTile);
   if (tiles <= 0) return;
   BackwardArgs b = a;
   int sms = 148;

@@ -65,10 +65,22 @@ struct BlendPixel {
 
 __global__ void __launch_bounds__(kBlendThreads, 2) blend_kernel(BlendArgs a) {
   __shared__ TileWalkShared sm;
-  const int gw = (a.W + kTile - 1) / kTile;
   const int tile = int(a.order[blockIdx.x]);
-  const TilePixel tp(tile, gw);
-  const bool inside = tp.px < a.W && tp.py < a.H;
+  // this tile's image: the call's, or its batch item's
+  int W = a.W, H = a.H, ltile = tile;
+  size_t pbase = 0;
+  const float* bg = a.bg;
+  if (a.items != nullptr) {
+    const BatchItem& it = a.items[find_item_tile(a.items, a.num_items, uint32_t(tile))];
+    W = it.W;
+    H = it.H;
+    ltile = tile - int(it.tile_base);
+    pbase = size_t(it.pix_base);
+    bg = it.bg;
+  }
+  const int gw = (W + kTile - 1) / kTile;
+  const TilePixel tp(ltile, gw);
+  const bool inside = tp.px < W && tp.py < H;
   const uint2 range = a.ranges[tile];
   const int n = int(range.y - range.x);
   const float pxf = float(tp.px), pyf = float(tp.py);
@@ -131,15 +143,16 @@ __global__ void __launch_bounds__(kBlendThreads, 2) blend_kernel(BlendArgs a) {
     if (b + 1 < nb) stage_store(sm, cur ^ 1, st, tp.X0, tp.Y0);
   }
   if (inside) {
-    const size_t p = size_t(tp.py) * a.W + tp.px;
-    const size_t hw = size_t(a.W) * a.H;
+    const size_t q = size_t(tp.py) * W + tp.px;
+    const size_t p = pbase + q, cp = 3 * pbase + q;
+    const size_t hw = size_t(W) * H;
     a.n_contrib[p] = pix.last;
     a.out_alpha[p] = pix.Wt;
     a.out_depth[p] = pix.D;
     a.T_final[p] = pix.T;
-    a.out_color[p] = fma(pix.T, a.bg[0], pix.C0);
-    a.out_color[hw + p] = fma(pix.T, a.bg[1], pix.C1);
-    a.out_color[2 * hw + p] = fma(pix.T, a.bg[2], pix.C2);
+    a.out_color[cp] = fma(pix.T, bg[0], pix.C0);
+    a.out_color[hw + cp] = fma(pix.T, bg[1], pix.C1);
+    a.out_color[2 * hw + cp] = fma(pix.T, bg[2], pix.C2);
   }
   // largest contributor count in the tile (the backward starts there)
   __shared__ uint32_t s_max[kBlendThreads / 32];
@@ -189,7 +202,7 @@ __global__ void __launch_bounds__(1024) tile_order_kernel(const uint2* ranges, c
 }
 
 void launch_blend(const BlendArgs& a, cudaStream_t stream) {
-  const int tiles = ((a.W + kTile - 1) / kTile) * ((a.H + kTile - 1) / kTile);
+  const int tiles = a.items ? a.total_tiles : ((a.W + kTile - 1) / kTile) * ((a.H + kTile - 1) / kTile);
   if (tiles <= 0) return;
   stage_begin(kStBlend, stream);
   tile_order_kernel<<<1, 1024, 0, stream>>>(a.ranges, nullptr, tiles, a.order);

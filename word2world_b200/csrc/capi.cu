@@ -4,6 +4,7 @@
 // caller.  All work is enqueued on the caller's stream.
 #include <cstdio>
 #include <cstring>
+#include <vector>
 
 #include "../../include/w2w_raster.h"
 #include "common.cuh"
@@ -56,6 +57,19 @@ struct KeyPlan {
   int key64, depth_bits, tile_bits, bits;
   uint32_t prefix;
 };
+KeyPlan plan_keys_tiles(const w2w_geometry_info& info, int tiles) {
+  KeyPlan k{};
+  const uint32_t dmin = info.depth_min_bits, dmax = info.depth_max_bits;
+  const uint32_t x = dmin ^ dmax;
+  int db = 0;
+  while (db < 32 && (x >> db) != 0u) ++db;
+  k.depth_bits = db;
+  k.prefix = db >= 32 ? 0u : (dmin & ~((1u << db) - 1u));
+  k.tile_bits = ceil_log2(uint32_t(tiles));
+  k.bits = k.tile_bits + k.depth_bits;
+  k.key64 = k.bits > 32 ? 1 : 0;
+  return k;
+}
 KeyPlan plan_keys(const w2w_geometry_info& info, int W, int H) {
   KeyPlan k{};
   const uint32_t dmin = info.depth_min_bits, dmax = info.depth_max_bits;
@@ -493,6 +507,293 @@ int w2w_binning_keys64(const void* binning_state, long long R, int W, int H, uin
   if (hh.key64) expand_keys<uint64_t><<<blocks, 256, 0, st>>>(h, at<uint64_t>(binning_state, BL.keysA), R, out);
   else expand_keys<uint32_t><<<blocks, 256, 0, st>>>(h, at<uint32_t>(binning_state, BL.keysA), R, out);
   stage_end(kStOther, st, 1);
+  return check_launch();
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Batched calls: many views of many scenes in one launch per stage.  Items'
+// elements (per-view copies of their scene's Gaussians), tiles and pixels are
+// laid out back to back; keys are (global tile, depth) so one sort serves all
+// items and each tile's list is exactly the one its item alone would give.
+// ---------------------------------------------------------------------------
+namespace {
+
+struct BatchTotals {
+  long long elems = 0, pixels = 0;
+  int tiles = 0, M = -1;
+  bool ok = true;
+};
+
+BatchTotals batch_totals(const w2w_batch_item* items, int n) {
+  BatchTotals t;
+  if (!items || n <= 0) { t.ok = false; return t; }
+  for (int v = 0; v < n; ++v) {
+    const w2w_batch_item& it = items[v];
+    if (it.P < 0 || it.width <= 0 || it.height <= 0 || it.M < 0 || it.degree < 0 || it.width >= 65535 * kTile ||
+        it.height >= 65535 * kTile || (it.P > 0 && (!it.means3D || !it.scales || !it.rotations || !it.opacities ||
+                                                      (it.M > 0 && !it.shs)))) {
+      t.ok = false;
+      return t;
+    }
+    if (t.M < 0) t.M = it.M;
+    if (it.M != t.M) { t.ok = false; return t; }  // one SH row length per batch
+    t.elems += it.P;
+    t.pixels += (long long)it.width * it.height;
+    t.tiles += num_tiles(it.width, it.height);
+  }
+  if (t.elems >= (1LL << 30) || t.tiles >= (1 << 30)) t.ok = false;
+  return t;
+}
+
+struct BatchGeomLayout {
+  size_t items, item_end, total;
+  BatchGeomLayout(long long E, int n) {
+    const size_t g = GeomLayout(E).total;
+    items = g;
+    item_end = align256(items + size_t(n) * sizeof(BatchItem));
+    total = align256(item_end + size_t(n) * 4);
+  }
+};
+
+std::vector<BatchItem> device_items(const w2w_batch_item* items, int n) {
+  std::vector<BatchItem> d(static_cast<size_t>(n));
+  uint32_t eb = 0, tb = 0;
+  unsigned long long pb = 0;
+  for (int v = 0; v < n; ++v) {
+    const w2w_batch_item& it = items[v];
+    BatchItem& b = d[size_t(v)];
+    std::memset(&b, 0, sizeof(b));
+    b.means3D = it.means3D; b.scales = it.scales; b.rotations = it.rotations; b.opacities = it.opacities;
+    b.shs = it.shs;
+    b.P = it.P; b.M = it.M; b.degree = it.degree; b.W = it.width; b.H = it.height;
+    b.gw = tiles_x(it.width);
+    b.tiles = num_tiles(it.width, it.height);
+    b.focal_x = it.focal_x; b.tan_fovx = it.tan_fovx; b.tan_fovy = it.tan_fovy;
+    b.scale_modifier = it.scale_modifier;
+    b.h_x = float(it.width) / (2.0f * it.tan_fovx);
+    b.h_y = float(it.height) / (2.0f * it.tan_fovy);
+    std::memcpy(b.view, it.viewmatrix, sizeof(b.view));
+    std::memcpy(b.proj, it.projmatrix, sizeof(b.proj));
+    std::memcpy(b.campos, it.campos, 3 * sizeof(float));
+    std::memcpy(b.bg, it.background, 3 * sizeof(float));
+    b.elem_base = eb;
+    b.tile_base = tb;
+    b.pix_base = pb;
+    eb += uint32_t(it.P);
+    tb += uint32_t(b.tiles);
+    pb += (unsigned long long)it.width * it.height;
+  }
+  return d;
+}
+
+}  // namespace
+
+extern "C" {
+
+size_t w2w_batch_geometry_state_bytes(const w2w_batch_item* items, int n) {
+  const BatchTotals t = batch_totals(items, n);
+  return t.ok ? BatchGeomLayout(t.elems, n).total : 0;
+}
+
+size_t w2w_batch_image_state_bytes(const w2w_batch_item* items, int n) {
+  const BatchTotals t = batch_totals(items, n);
+  return t.ok ? ImageLayout(size_t(t.pixels), size_t(t.tiles)).total : 0;
+}
+
+size_t w2w_batch_binning_state_bytes(long long R, const w2w_batch_item* items, int n) {
+  const BatchTotals t = batch_totals(items, n);
+  return (t.ok && R >= 0) ? BinLayout(R, t.tiles).total : 0;
+}
+
+size_t w2w_batch_backward_scratch_bytes(const w2w_batch_item* items, int n) {
+  const BatchTotals t = batch_totals(items, n);
+  return t.ok ? align256(size_t(t.elems) * 16) + align256(size_t(t.elems) * 4) : 0;
+}
+
+int w2w_batch_forward_geometry(const w2w_batch_item* items, int n, int compat_spill, int* radii, void* geom_state,
+                               w2w_geometry_info* info, w2w_stream_t stream) {
+  const BatchTotals t = batch_totals(items, n);
+  if (!t.ok || !info || !geom_state || (t.elems > 0 && !radii)) return W2W_ERR_INVALID;
+  std::memset(info, 0, sizeof(*info));
+  const long long E = t.elems;
+  const GeomLayout L(E);
+  const BatchGeomLayout BL(E, n);
+  cudaStream_t st = S(stream);
+  const std::vector<BatchItem> host = device_items(items, n);
+  BatchItem* dev_items = at<BatchItem>(geom_state, BL.items);
+  if (cudaMemcpyAsync(dev_items, host.data(), sizeof(BatchItem) * size_t(n), cudaMemcpyHostToDevice, st) !=
+      cudaSuccess)
+    return W2W_ERR_CUDA;
+  if (E == 0) return W2W_OK;
+  cudaMemsetAsync(geom_state, 0, L.depth, st);  // header + scan status
+  cudaMemsetAsync(at<uint32_t>(geom_state, BL.item_end), 0, size_t(n) * 4, st);
+  PreprocessArgs a{};
+  a.P = int(E); a.compat_spill = compat_spill;
+  a.items = dev_items; a.num_items = n; a.item_end = at<uint32_t>(geom_state, BL.item_end);
+  // the 16-coefficient vector path needs every item's rows 16-byte aligned
+  bool sh16 = t.M == 16;
+  for (int v = 0; v < n && sh16; ++v)
+    if (items[v].P > 0 && (reinterpret_cast<uintptr_t>(items[v].shs) & 15) != 0) sh16 = false;
+  a.M = sh16 ? 16 : 0;
+  a.shs = sh16 ? items[0].shs : nullptr;
+  a.radii = radii;
+  a.header = at<GeomHeader>(geom_state, L.header);
+  a.scan_status = at<unsigned long long>(geom_state, L.scan_status);
+  a.depth = at<float>(geom_state, L.depth);
+  a.clamped = at<uint8_t>(geom_state, L.clamped);
+  a.means2D = at<float>(geom_state, L.means2D);
+  a.cov3D = at<float>(geom_state, L.cov3D);
+  a.conic = at<float>(geom_state, L.conic);
+  a.rgb = at<float>(geom_state, L.rgb);
+  a.tiles = at<uint32_t>(geom_state, L.tiles);
+  a.offsets = at<uint32_t>(geom_state, L.offsets);
+  a.rect = at<uint32_t>(geom_state, L.rect);
+  a.prev_reach = at<uint32_t>(geom_state, L.prev_reach);
+  a.record = at<float>(geom_state, L.record);
+  a.bwd_record = at<float>(geom_state, L.bwd_record);
+  launch_preprocess(a, st);
+  int rc = check_launch();
+  if (rc) return rc;
+  GeomHeader h;
+  if (cudaMemcpyAsync(&h, a.header, sizeof(h), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+      cudaStreamSynchronize(st) != cudaSuccess)
+    return W2W_ERR_CUDA;
+  info->num_rendered = h.num_rendered;
+  info->depth_min_bits = ~h.depth_min;
+  info->depth_max_bits = h.depth_max;
+  info->error = h.error;
+  if (h.error & kErrTimeout) return W2W_ERR_TIMEOUT;
+  if (h.error & kErrCapacity) return W2W_ERR_CAPACITY;
+  return W2W_OK;
+}
+
+int w2w_batch_forward_render(const w2w_batch_item* items, int n, const void* geom_state,
+                             const w2w_geometry_info* info, void* binning_state, void* image_state, float* out_color,
+                             float* out_depth, float* out_alpha, w2w_stream_t stream) {
+  const BatchTotals t = batch_totals(items, n);
+  if (!t.ok || !info || !geom_state || !image_state || !out_color || !out_depth || !out_alpha) return W2W_ERR_INVALID;
+  const long long R = info->num_rendered;
+  if (R < 0 || R >= (1LL << 30)) return W2W_ERR_CAPACITY;
+  if (R > 0 && !binning_state) return W2W_ERR_INVALID;
+  cudaStream_t st = S(stream);
+  const long long E = t.elems;
+  const int T = t.tiles;
+  const ImageLayout IL(size_t(t.pixels), size_t(T));
+  const BatchGeomLayout BGL(E, n);
+  const BatchItem* dev_items = at<BatchItem>(geom_state, BGL.items);
+  uint2* ranges = at<uint2>(image_state, IL.ranges);
+  const uint32_t* point_list = nullptr;
+  if (R == 0) {
+    cudaMemsetAsync(ranges, 0, sizeof(uint2) * size_t(T), st);
+  } else {
+    const GeomLayout GL(E);
+    const BinLayout BL(R, T);
+    const KeyPlan kp = plan_keys_tiles(*info, T);
+    const int passes = sort_passes(kp.bits);
+    BinHeader* bh = at<BinHeader>(binning_state, BL.header);
+    stage_begin(kStOther, st);
+    write_bin_header<<<1, 1, 0, st>>>(bh, kp, uint32_t(R), uint32_t(passes));
+    stage_end(kStOther, st, 1);
+    const bool odd = (passes % 2) == 1;
+    void* keysA = at<void>(binning_state, BL.keysA);
+    void* keysB = at<void>(binning_state, BL.keysB);
+    uint32_t* valsA = at<uint32_t>(binning_state, BL.valsA);
+    uint32_t* valsB = at<uint32_t>(binning_state, BL.valsB);
+    DuplicateArgs d{};
+    d.P = int(E); d.gw = 0; d.R = uint32_t(R); d.key64 = kp.key64; d.depth_bits = uint32_t(kp.depth_bits);
+    d.items = dev_items; d.num_items = n; d.item_end = at<uint32_t>(geom_state, BGL.item_end);
+    d.tiles = at<uint32_t>(geom_state, GL.tiles);
+    d.offsets = at<uint32_t>(geom_state, GL.offsets);
+    d.rect = at<uint32_t>(geom_state, GL.rect);
+    d.prev_reach = at<uint32_t>(geom_state, GL.prev_reach);
+    d.depth = at<float>(geom_state, GL.depth);
+    d.keys = odd ? keysB : keysA;
+    d.vals = odd ? valsB : valsA;
+    launch_duplicate(d, st);
+    SortArgs so{};
+    so.n = R; so.key64 = kp.key64; so.begin_bit = 0; so.bits = kp.bits;
+    so.keys_in = d.keys; so.vals_in = d.vals;
+    so.keys_out = keysA; so.vals_out = valsA;
+    so.keys_tmp = keysB; so.vals_tmp = valsB;
+    so.hist = at<uint32_t>(binning_state, BL.hist);
+    so.status = at<uint32_t>(binning_state, BL.status);
+    so.counters = bh->tile_counter;
+    so.error = &bh->error;
+    so.tile_shift = kp.depth_bits;
+    so.num_tiles = T;
+    so.tile_hist = at<uint32_t>(binning_state, BL.tile_hist);
+    so.ranges = ranges;
+    launch_sort(so, st);
+    point_list = valsA;
+  }
+  BlendArgs b{};
+  b.W = 0; b.H = 0;
+  b.items = dev_items; b.num_items = n; b.total_tiles = T;
+  b.ranges = ranges;
+  b.point_list = point_list;
+  b.record = R > 0 ? at<float>(geom_state, GeomLayout(E).record) : nullptr;
+  b.bg = nullptr;
+  b.out_color = out_color; b.out_depth = out_depth; b.out_alpha = out_alpha;
+  b.n_contrib = at<uint32_t>(image_state, IL.n_contrib);
+  b.T_final = at<float>(image_state, IL.T_final);
+  b.tile_max = at<uint32_t>(image_state, IL.tile_max);
+  b.order = at<uint32_t>(image_state, IL.order);
+  b.order_bwd = at<uint32_t>(image_state, IL.order_bwd);
+  launch_blend(b, st);
+  return check_launch();
+}
+
+int w2w_batch_backward(const w2w_batch_item* items, int n, const void* geom_state, long long R,
+                       const void* binning_state, const void* image_state, const int* radii, const float* out_alpha,
+                       const float* dL_dcolor, const float* dL_ddepth, const float* dL_dalpha, int grad_mode,
+                       void* scratch, size_t scratch_bytes, float* dL_dmeans2D, float* dL_dcolors, float* dL_dopacity,
+                       float* dL_dmeans3D, float* dL_dcov3D, float* dL_dsh, float* dL_dscales, float* dL_drotations,
+                       w2w_stream_t stream) {
+  const BatchTotals t = batch_totals(items, n);
+  if (!t.ok || (grad_mode != 0 && grad_mode != 1)) return W2W_ERR_INVALID;
+  const long long E = t.elems;
+  if (E == 0) return W2W_OK;
+  if (!geom_state || !image_state || !radii || !out_alpha || !dL_dcolor || !dL_ddepth || !dL_dalpha ||
+      !dL_dmeans2D || !dL_dcolors || !dL_dopacity || !dL_dmeans3D || !dL_dcov3D || !dL_dscales || !dL_drotations ||
+      (t.M > 0 && !dL_dsh) || (R > 0 && !binning_state))
+    return W2W_ERR_INVALID;
+  if (!scratch || scratch_bytes < w2w_batch_backward_scratch_bytes(items, n)) return W2W_ERR_SCRATCH;
+  cudaStream_t st = S(stream);
+  const int T = t.tiles;
+  const GeomLayout GL(E);
+  const BatchGeomLayout BGL(E, n);
+  const ImageLayout IL(size_t(t.pixels), size_t(T));
+  float* acc_cov = static_cast<float*>(scratch);
+  float* acc_depth = at<float>(scratch, align256(size_t(E) * 16));
+  cudaMemsetAsync(scratch, 0, w2w_batch_backward_scratch_bytes(items, n), st);
+  cudaMemsetAsync(dL_dmeans2D, 0, sizeof(float) * 3 * size_t(E), st);
+  cudaMemsetAsync(dL_dcolors, 0, sizeof(float) * 3 * size_t(E), st);
+  cudaMemsetAsync(dL_dopacity, 0, sizeof(float) * size_t(E), st);
+  BackwardArgs a{};
+  a.P = int(E); a.W = 0; a.H = 0; a.degree = 0; a.M = t.M; a.grad_mode = grad_mode;
+  a.items = at<BatchItem>(geom_state, BGL.items); a.num_items = n; a.total_tiles = T;
+  a.shs = nullptr;
+  a.radii = radii;
+  a.cov3D = at<float>(geom_state, GL.cov3D);
+  a.clamped = at<uint8_t>(geom_state, GL.clamped);
+  a.record = at<float>(geom_state, GL.record);
+  a.bwd_record = at<float>(geom_state, GL.bwd_record);
+  a.ranges = at<uint2>(image_state, IL.ranges);
+  a.point_list = R > 0 ? at<uint32_t>(binning_state, BinLayout(R, T).valsA) : nullptr;
+  a.n_contrib = at<uint32_t>(image_state, IL.n_contrib);
+  a.tile_max = at<uint32_t>(image_state, IL.tile_max);
+  a.order_bwd = at<uint32_t>(image_state, IL.order_bwd);
+  a.T_final = at<float>(image_state, IL.T_final);
+  a.out_alpha = out_alpha;
+  a.dL_dcolor = dL_dcolor; a.dL_ddepth = dL_ddepth; a.dL_dalpha = dL_dalpha;
+  a.dL_dmean2D = dL_dmeans2D; a.acc_cov = acc_cov; a.dL_dopacity = dL_dopacity; a.dL_dcolors = dL_dcolors;
+  a.acc_depth = acc_depth;
+  a.dL_dmeans3D = dL_dmeans3D; a.dL_dcov3D = dL_dcov3D; a.dL_dsh = dL_dsh; a.dL_dscales = dL_dscales;
+  a.dL_drotations = dL_drotations;
+  if (R > 0) launch_backward_render(a, st);
+  launch_backward_gaussians(a, st);
   return check_launch();
 }
 

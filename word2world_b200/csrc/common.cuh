@@ -287,11 +287,12 @@ struct GeomLayout {
 
 struct ImageLayout {
   size_t n_contrib, ranges, T_final, tile_max, order, order_bwd, total;
-  __host__ __device__ ImageLayout(int W, int H) {
+  __host__ __device__ ImageLayout(int W, int H)
+      : ImageLayout(size_t(W) * size_t(H), size_t((W + kTile - 1) / kTile) * size_t((H + kTile - 1) / kTile)) {}
+  // a batch: all items' pixels and tiles back to back
+  __host__ __device__ ImageLayout(size_t hw, size_t tiles) {
     size_t o = 0;
     auto take = [&](size_t bytes) { size_t a = align256(o); o = a + bytes; return a; };
-    const size_t hw = size_t(W) * size_t(H);
-    const size_t tiles = size_t((W + kTile - 1) / kTile) * size_t((H + kTile - 1) / kTile);
     n_contrib = take(hw * 4);
     ranges = take(tiles * 8);
     T_final = take(hw * 4);

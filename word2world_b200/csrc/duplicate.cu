@@ -10,6 +10,9 @@
 // it.  Entries are written in row-major order of the rectangle
 // (prepareSort.cu:191-204).
 //
+// Batched calls: every view's Gaussians emit into its own slot range, with its
+// own tile grid, and tile ids offset by the view's first global tile.
+//
 // Load balance: each warp expands 32 consecutive Gaussians; every lane emits
 // one entry per round, so large and small Gaussians cost the same per entry
 // and stores to consecutive slots are coalesced.
@@ -26,8 +29,15 @@ __global__ void __launch_bounds__(kDupThreads) duplicate_kernel(DuplicateArgs a)
   const int lane = threadIdx.x & 31;
   const int warp_global = (blockIdx.x * kDupThreads + threadIdx.x) >> 5;
   const int g = warp_global * 32 + lane;
-  uint32_t p0 = 0, cnt = 0, start = 0, x0 = 0, y0 = 0, w = 1, dlow = 0;
+  uint32_t p0 = 0, cnt = 0, start = 0, x0 = 0, y0 = 0, w = 1, dlow = 0, gwv = uint32_t(a.gw), tbase = 0;
   if (g < a.P) {  // Gaussians that emit nothing have an empty rectangle
+    uint32_t end = a.R;
+    if (a.items != nullptr) {  // batched: this view's tile grid, first tile id and end slot
+      const int item = find_item_elem(a.items, a.num_items, uint32_t(g));
+      gwv = uint32_t(a.items[item].gw);
+      tbase = a.items[item].tile_base;
+      end = a.item_end[item];
+    }
     start = a.offsets[g] - a.tiles[g];
     const uint2 rc = reinterpret_cast<const uint2*>(a.rect)[g];
     x0 = rc.x & 0xffffu;
@@ -37,7 +47,7 @@ __global__ void __launch_bounds__(kDupThreads) duplicate_kernel(DuplicateArgs a)
     const uint32_t n = (x1 > x0 && y1 > y0) ? (x1 - x0) * (y1 - y0) : 0u;
     const uint32_t reach = start + n;
     p0 = max(start, a.prev_reach[g]);
-    const uint32_t p1 = min(reach, a.R);
+    const uint32_t p1 = min(reach, end);
     cnt = p1 > p0 ? p1 - p0 : 0u;
     const uint32_t db = __float_as_uint(a.depth[g]);
     dlow = a.depth_bits >= 32 ? db : (db & ((1u << a.depth_bits) - 1u));
@@ -68,11 +78,13 @@ __global__ void __launch_bounds__(kDupThreads) duplicate_kernel(DuplicateArgs a)
     const uint32_t oy0 = __shfl_sync(0xffffffffu, y0, o);
     const uint32_t ow = __shfl_sync(0xffffffffu, w, o);
     const uint32_t odl = __shfl_sync(0xffffffffu, dlow, o);
+    const uint32_t ogw = __shfl_sync(0xffffffffu, gwv, o);
+    const uint32_t otb = __shfl_sync(0xffffffffu, tbase, o);
     if (e < total) {
       const uint32_t p = op0 + (e - oex);
       const uint32_t k = p - ost;
       const uint32_t ty = oy0 + k / ow, tx = ox0 + k % ow;
-      const uint32_t tile = ty * uint32_t(a.gw) + tx;
+      const uint32_t tile = otb + ty * ogw + tx;
       if (p < a.R) {
         if constexpr (kKey64) {
           reinterpret_cast<uint64_t*>(a.keys)[p] = (uint64_t(tile) << a.depth_bits) | odl;

@@ -8,8 +8,49 @@
 
 namespace w2w {
 
+// One view of one scene in a batched call (device copy of the item table).
+// Elements (the per-view copies of the scene's Gaussians), tiles and pixels of
+// all items are laid out back to back: item v owns elements
+// [elem_base, elem_base + P), global tile ids [tile_base, tile_base + tiles)
+// and image pixels [pix_base, pix_base + W*H) of every per-pixel buffer.
+struct BatchItem {
+  const float* means3D;
+  const float* scales;
+  const float* rotations;
+  const float* opacities;
+  const float* shs;
+  int P, M, degree, W, H, gw, tiles, pad0;
+  float focal_x, tan_fovx, tan_fovy, scale_modifier;
+  float h_x, h_y, pad1, pad2;  // W / (2 tan_fovx), H / (2 tan_fovy)
+  float view[16], proj[16], campos[4], bg[4];
+  uint32_t elem_base, tile_base;
+  unsigned long long pix_base;
+};
+
+// Item owning global element (or tile) index i: the last item whose base is
+// <= i (items with no elements share their successor's base and lose ties).
+__device__ __forceinline__ int find_item_elem(const BatchItem* items, int n, uint32_t i) {
+  int lo = 0, hi = n - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (items[mid].elem_base <= i) lo = mid; else hi = mid - 1;
+  }
+  return lo;
+}
+__device__ __forceinline__ int find_item_tile(const BatchItem* items, int n, uint32_t t) {
+  int lo = 0, hi = n - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (items[mid].tile_base <= t) lo = mid; else hi = mid - 1;
+  }
+  return lo;
+}
+
 struct PreprocessArgs {
   int P, W, H, degree, M, compat_spill;
+  const BatchItem* items;  // batched call: per-item scene and camera (then P = total elements); else null
+  int num_items;
+  uint32_t* item_end;      // batched call: end slot of each item's instances (written here)
   float focal_x;
   const float* view;
   const float* proj;
@@ -40,6 +81,9 @@ void launch_preprocess(const PreprocessArgs& a, cudaStream_t stream);
 struct DuplicateArgs {
   int P, gw;
   uint32_t R;
+  const BatchItem* items;   // batched call (then per-item tile grids, tile bases and end slots)
+  int num_items;
+  const uint32_t* item_end;
   int key64;
   uint32_t depth_bits;
   const uint32_t* tiles;
@@ -86,6 +130,8 @@ size_t sort_status_words(long long n);
 
 struct BlendArgs {
   int W, H;
+  const BatchItem* items;  // batched call (then per-item images packed at pix_base, 3 * pix_base for colour)
+  int num_items, total_tiles;
   const uint2* ranges;
   const uint32_t* point_list;
   const float* record;
@@ -104,6 +150,8 @@ void launch_blend(const BlendArgs& a, cudaStream_t stream);
 // Backward.  grad_mode 0 = the reference's formulas, 1 = exact derivative.
 struct BackwardArgs {
   int P, W, H, degree, M, grad_mode;
+  const BatchItem* items;  // batched call (then P = total elements, per-item cameras and packed images)
+  int num_items, total_tiles;
   float focal_x;           // exact mode (the forward's Jacobian focal)
   float h_x, h_y;          // reference mode: W/(2 tan_fovx), H/(2 tan_fovy)
   float tan_fovx, tan_fovy;

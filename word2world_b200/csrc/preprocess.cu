@@ -30,20 +30,27 @@ constexpr float kC32 = 0.4570457994644658f;
 constexpr float kC33 = 0.3731763325901154f;
 constexpr float kC35 = 1.445305721320277f;
 
-struct Pair {  // (sum of allocations, max over the segment of local start + emitted count)
-  uint32_t s, x;
+// Scan element: (sum of allocations, max over the span of local start +
+// emitted count, whether a view starts inside the span).  The max-plus
+// component restarts at a view's first Gaussian: a batched call's views are
+// independent key emissions (the spill of one view never reaches the next),
+// exactly as separate calls.
+struct Pair {
+  uint32_t s, x, f;
 };
 __device__ __forceinline__ Pair combine(Pair lo, Pair hi) {
-  return Pair{lo.s + hi.s, max(lo.x, lo.s + hi.x)};
+  return Pair{lo.s + hi.s, hi.f ? lo.s + hi.x : max(lo.x, lo.s + hi.x), lo.f | hi.f};
 }
 
 constexpr unsigned long long kFlagAgg = 1ull << 62;
 constexpr unsigned long long kFlagInc = 2ull << 62;
+constexpr uint32_t kPairMask = (1u << 30) - 1u;  // counts below 2^30
 __device__ __forceinline__ unsigned long long pack(unsigned long long flag, Pair p) {
-  return flag | ((unsigned long long)(p.s & 0x7fffffffu) << 31) | (unsigned long long)(p.x & 0x7fffffffu);
+  return flag | ((unsigned long long)(p.f & 1u) << 60) | ((unsigned long long)(p.s & kPairMask) << 30) |
+         (unsigned long long)(p.x & kPairMask);
 }
 __device__ __forceinline__ Pair unpack(unsigned long long w) {
-  return Pair{uint32_t((w >> 31) & 0x7fffffffu), uint32_t(w & 0x7fffffffu)};
+  return Pair{uint32_t((w >> 30) & kPairMask), uint32_t(w & kPairMask), uint32_t((w >> 60) & 1u)};
 }
 
 template <int V>
@@ -234,18 +241,34 @@ preprocess_kernel(PreprocessArgs a) {
   const uint32_t tile = s_tile;
   const int i = int(tile) * kPreThreads + int(threadIdx.x);
   const int P = a.P;
-  const int gw = (a.W + kTile - 1) / kTile, gh = (a.H + kTile - 1) / kTile;
+
+  // this element's scene and camera: the call's, or its batch item's
+  int gi = i, item = -1;
+  const float *means3D = a.means3D, *scales = a.scales, *rotations = a.rotations, *opacities = a.opacities,
+              *shs = a.shs, *view = a.view, *proj = a.proj, *campos = a.campos;
+  int M = a.M, degree = a.degree, Wd = a.W, Hd = a.H, item_P = P;
+  float focal = a.focal_x;
+  if (a.items != nullptr && i < P) {
+    item = find_item_elem(a.items, a.num_items, uint32_t(i));
+    const BatchItem& it = a.items[item];
+    gi = i - int(it.elem_base);
+    means3D = it.means3D; scales = it.scales; rotations = it.rotations; opacities = it.opacities; shs = it.shs;
+    view = it.view; proj = it.proj; campos = it.campos;
+    M = it.M; degree = it.degree; Wd = it.W; Hd = it.H; item_P = it.P;
+    focal = it.focal_x;
+  }
+  const int gw = (Wd + kTile - 1) / kTile, gh = (Hd + kTile - 1) / kTile;
 
   uint32_t alloc = 0, emit = 0;
   uint32_t depth_bits = 0;
   if (i < P) {
-    const float px = a.means3D[3 * i], py = a.means3D[3 * i + 1], pz = a.means3D[3 * i + 2];
-    const float sx = a.scales[3 * i], sy = a.scales[3 * i + 1], sz = a.scales[3 * i + 2];
-    const float4 q = make_float4(a.rotations[4 * i], a.rotations[4 * i + 1], a.rotations[4 * i + 2],
-                                 a.rotations[4 * i + 3]);
-    const float opacity = a.opacities[i];
+    const float px = means3D[3 * gi], py = means3D[3 * gi + 1], pz = means3D[3 * gi + 2];
+    const float sx = scales[3 * gi], sy = scales[3 * gi + 1], sz = scales[3 * gi + 2];
+    const float4 q = make_float4(rotations[4 * gi], rotations[4 * gi + 1], rotations[4 * gi + 2],
+                                 rotations[4 * gi + 3]);
+    const float opacity = opacities[gi];
     Geometry g;
-    project(a.view, a.proj, a.focal_x, float(a.W), float(a.H), px, py, pz, sx, sy, sz, q, g);
+    project(view, proj, focal, float(Wd), float(Hd), px, py, pz, sx, sy, sz, q, g);
     float* cov3 = a.cov3D + 6 * size_t(i);
 #pragma unroll
     for (int k = 0; k < 6; ++k) cov3[k] = g.cov3[k];
@@ -253,7 +276,7 @@ preprocess_kernel(PreprocessArgs a) {
     // SH colour
     float rgb[3];
     uint8_t clampf[3];
-    const float* shp = a.shs + size_t(i) * a.M * 3;
+    const float* shp = shs + size_t(gi) * M * 3;
     if constexpr (kSh16) {
       float buf[48];
       const float4* s4 = reinterpret_cast<const float4*>(shp);
@@ -262,9 +285,9 @@ preprocess_kernel(PreprocessArgs a) {
         const float4 t = __ldg(s4 + k);
         buf[4 * k] = t.x; buf[4 * k + 1] = t.y; buf[4 * k + 2] = t.z; buf[4 * k + 3] = t.w;
       }
-      sh_colour(buf, 16, a.degree, px, py, pz, a.campos, rgb, clampf);
+      sh_colour(buf, 16, degree, px, py, pz, campos, rgb, clampf);
     } else {
-      sh_colour(shp, a.M, a.degree, px, py, pz, a.campos, rgb, clampf);
+      sh_colour(shp, M, degree, px, py, pz, campos, rgb, clampf);
     }
     reinterpret_cast<float*>(a.rgb)[3 * i] = rgb[0];
     reinterpret_cast<float*>(a.rgb)[3 * i + 1] = rgb[1];
@@ -370,23 +393,25 @@ preprocess_kernel(PreprocessArgs a) {
 
   // block-wide inclusive scan of (alloc, emit) with the max-plus component
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  Pair v{alloc, emit};
+  Pair v{alloc, emit, uint32_t(i < P && gi == 0)};
 #pragma unroll
   for (int d = 1; d < 32; d <<= 1) {
     Pair o;
     o.s = __shfl_up_sync(0xffffffffu, v.s, d);
     o.x = __shfl_up_sync(0xffffffffu, v.x, d);
+    o.f = __shfl_up_sync(0xffffffffu, v.f, d);
     if (lane >= d) v = combine(o, v);
   }
   if (lane == 31) s_warp[warp] = v;
   __syncthreads();
   if (warp == 0) {
-    Pair w = lane < kPreThreads / 32 ? s_warp[lane] : Pair{0, 0};
+    Pair w = lane < kPreThreads / 32 ? s_warp[lane] : Pair{0, 0, 0};
 #pragma unroll
     for (int d = 1; d < kPreThreads / 32; d <<= 1) {
       Pair o;
       o.s = __shfl_up_sync(0xffffffffu, w.s, d);
       o.x = __shfl_up_sync(0xffffffffu, w.x, d);
+      o.f = __shfl_up_sync(0xffffffffu, w.f, d);
       if (lane >= d) w = combine(o, w);
     }
     if (lane < kPreThreads / 32) s_warp[lane] = w;  // inclusive over warps
@@ -399,10 +424,10 @@ preprocess_kernel(PreprocessArgs a) {
     unsigned long long* status = a.scan_status;
     if (tile == 0) {
       st_relaxed64(status + tile, pack(kFlagInc, block_total));
-      s_prefix = Pair{0, 0};
+      s_prefix = Pair{0, 0, 0};
     } else {
       st_relaxed64(status + tile, pack(kFlagAgg, block_total));
-      Pair ex{0, 0};
+      Pair ex{0, 0, 0};
       bool first = true;
       int t = int(tile) - 1;
       uint32_t spins = 0;
@@ -431,17 +456,20 @@ preprocess_kernel(PreprocessArgs a) {
   Pair ex_lane;
   ex_lane.s = __shfl_up_sync(0xffffffffu, v.s, 1);
   ex_lane.x = __shfl_up_sync(0xffffffffu, v.x, 1);
-  if (lane == 0) ex_lane = Pair{0, 0};
-  const Pair ex_warps = warp > 0 ? s_warp[warp - 1] : Pair{0, 0};
+  ex_lane.f = __shfl_up_sync(0xffffffffu, v.f, 1);
+  if (lane == 0) ex_lane = Pair{0, 0, 0};
+  const Pair ex_warps = warp > 0 ? s_warp[warp - 1] : Pair{0, 0, 0};
   const Pair excl = combine(prefix, combine(ex_warps, ex_lane));
   if (i < P) {
     a.offsets[i] = excl.s + alloc;
-    a.prev_reach[i] = excl.x;
+    // a view's first Gaussian has no earlier writer in its view
+    a.prev_reach[i] = gi == 0 ? excl.s : excl.x;
+    if (item >= 0 && gi == item_P - 1) a.item_end[item] = excl.s + alloc;
   }
   if (tile == uint32_t((P + kPreThreads - 1) / kPreThreads) - 1 && threadIdx.x == 0) {
     const Pair total = tile > 0 ? combine(prefix, block_total) : block_total;
     hdr->num_rendered = total.s;
-    if (total.s >= 0x7fffffffu || total.x >= 0x7fffffffu) atomicOr(&hdr->error, kErrCapacity);
+    if (total.s >= kPairMask || total.x >= kPairMask) atomicOr(&hdr->error, kErrCapacity);
   }
 }
 
