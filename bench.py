@@ -43,6 +43,11 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--no-batched", action="store_true", help="skip the batched-call measurement of the workload")
+    ap.add_argument("--config", default="single", choices=["single", "multiscene"],
+                    help="single: the 500k / 512^2 drop-in workload (default); multiscene: 64 scenes, batched "
+                         "calls vs sequential single-view calls")
+    ap.add_argument("--scenes", type=int, default=64)
     return ap.parse_args()
 
 
@@ -230,6 +235,8 @@ def run_ours(a):
                              sort_key_bytes=kb, sort_passes=plans[0].get("passes")),
               "gpu_launches": int(launches), "clocks": clk.summary(), "roofline": roofline, "stages": stage_report}
 
+    if not a.no_batched:
+        result["batched"] = run_batched_single(a, sc, cams, device, world, value)
     if not a.no_e2e:
         result["e2e"] = run_e2e(a, sc, cams, device, world)
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
@@ -284,6 +291,144 @@ def run_e2e(a, sc, cams, device, world):
     ms = wd.max_over_ranks(e0.elapsed_time(e1), device=device)
     return {"value": round(world * a.views * a.steps / (ms / 1e3), 3), "unit": UNIT, "h2d_bytes_per_step": int(h2d),
             "d2h_bytes_per_step": int(loss_host.numel() * 4), "api": "word2world_b200.renderer.Renderer.render"}
+
+
+# ---------------------------------------------------------------------------
+# batched calls
+# ---------------------------------------------------------------------------
+def run_batched_single(a, sc, cams, device, world, plain_value):
+    """The same workload (all views of the scene) as one batched call per
+    step: forward + backward of every view with one launch per stage."""
+    import torch
+    from word2world_b200 import dist as wd, scenes
+    from word2world_b200.batch import BatchRenderer, Scene, View
+    bs = Scene.from_arrays(sc.activate(), device)
+    views = [View(0, c) for c in cams]
+    grads = [torch.from_numpy(g).to(device) for g in scenes.upstream_grads(a.views, a.res, a.res, seed=a.seed + 1)]
+    br = BatchRenderer(grad_mode=a.grad_mode)
+
+    def step():
+        res = br.forward([bs], views)
+        br.backward(res, grads)
+
+    for _ in range(max(a.warmup, 1)):
+        step()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(a.steps):
+        step()
+    e1.record()
+    torch.cuda.synchronize()
+    ms = wd.max_over_ranks(e0.elapsed_time(e1), device=device)
+    v = world * a.views * a.steps / (ms / 1e3)
+    return {"value": round(v, 3), "unit": UNIT, "ms_per_step": round(ms / a.steps, 4),
+            "vs_plain": round(v / plain_value, 3),
+            "api": "word2world_b200.batch.BatchRenderer (all views of a step in one batched call)"}
+
+
+def multiscene_workload(a, device):
+    """64 scenes (default), Gaussian counts log-uniform in [10k, 1M], 4 orbit
+    views each at a resolution drawn from {256, 512, 1024}^2."""
+    import numpy as np
+    from word2world_b200 import camera, scenes
+    from word2world_b200.batch import Scene, View
+    rng = np.random.default_rng(a.seed + 17)
+    Ps = np.exp(rng.uniform(np.log(1e4), np.log(1e6), size=a.scenes)).astype(int)
+    res = rng.choice([256, 512, 1024], size=a.scenes)
+    scs, views = [], []
+    for k in range(a.scenes):
+        scs.append(Scene.from_arrays(scenes.make_scene(int(Ps[k]), seed=a.seed + 100 + k, layout="ball").activate(),
+                                     device))
+        for c in camera.orbit_views(4, 2.5, int(res[k]), int(res[k])):
+            views.append(View(k, c))
+    return scs, views, Ps, res
+
+
+def buckets(scs, views, budget=16_000_000):
+    """Split views into batches by resolution, each within an element-pixel
+    budget (elements x W x H / 512^2), which bounds a batch's instances."""
+    out = []
+    for r in sorted({int(v.camera.width) for v in views}):
+        cur, load = [], 0
+        for v in views:
+            if int(v.camera.width) != r:
+                continue
+            w = scs[v.scene].P * r * r / (512 * 512)
+            if cur and load + w > budget:
+                out.append(cur)
+                cur, load = [], 0
+            cur.append(v)
+            load += w
+        if cur:
+            out.append(cur)
+    return out
+
+
+def run_multiscene(a):
+    """Batched calls vs sequential single-view calls on the multi-scene
+    workload; both fwd+bwd of every view, N(0,1) upstream gradients."""
+    import numpy as np
+    import torch
+    from word2world_b200 import _C
+    from word2world_b200.batch import BatchRenderer
+    device = torch.device("cuda", 0)
+    torch.cuda.set_device(device)
+    scs, views, Ps, res = multiscene_workload(a, device)
+    gen = torch.Generator(device=device).manual_seed(a.seed + 1)
+    grads = [torch.randn(3, int(v.camera.height), int(v.camera.width), device=device, generator=gen) for v in views]
+    bg = torch.ones(3, device=device)
+    t = lambda x: torch.from_numpy(np.ascontiguousarray(x, dtype=np.float32)).to(device)
+    cams = [dict(view=t(v.camera.viewmatrix), proj=t(v.camera.projmatrix), campos=t(v.camera.campos)) for v in views]
+    empty = torch.empty(0, device=device)
+    gmode = 0 if a.grad_mode == "reference" else 1
+
+    def plain_step():
+        for i, v in enumerate(views):
+            sc, c, cam = scs[v.scene], v.camera, cams[i]
+            R, color, depth, alpha, radii, geom, binb, img = _C.rasterize_gaussians(
+                sc.shs, c.focal_y, sc.scales, sc.means3D, cam["proj"], 3, sc.opacities, sc.rotations,
+                cam["campos"], cam["view"], c.focal_x, c.height, c.width, bg, True)
+            z = torch.zeros(1, c.height, c.width, device=device)
+            _C.rasterize_gaussians_backward(bg, sc.means3D, radii, empty, sc.scales, sc.rotations, 1.0, empty,
+                                            cam["view"], cam["proj"], c.tanfovx, c.tanfovy, grads[i], z, z, sc.shs,
+                                            3, cam["campos"], geom, R, binb, img, alpha, False, gmode)
+
+    br = BatchRenderer(grad_mode=a.grad_mode)
+    groups = buckets(scs, views)
+    index = {id(v): i for i, v in enumerate(views)}
+
+    def batched_step():
+        for g in groups:
+            res_ = br.forward(scs, g)
+            br.backward(res_, [grads[index[id(v)]] for v in g])
+
+    def timed(fn):
+        for _ in range(max(a.warmup, 1)):
+            fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(a.steps):
+            fn()
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / a.steps
+
+    ms_plain = timed(plain_step)
+    ms_batch = timed(batched_step)
+    nv = len(views)
+    result = {"metric": "fwd+bwd views/s, 64 scenes (10k-1M Gaussians, 256-1024^2), batched vs plain",
+              "value": round(nv / (ms_batch / 1e3), 3), "unit": UNIT, "n_gpus": 1, "steps": a.steps,
+              "warmup": a.warmup, "ms_per_step": round(ms_batch, 3), "higher_is_better": True, "scaling": "weak",
+              "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded scenes, N(0,1) dL/dimage)",
+              "config": {"workload": f"{a.scenes} scenes, Gaussians log-uniform in [10k, 1M] (total "
+                                     f"{int(Ps.sum())}), 4 orbit views each at 256/512/1024^2, fwd+bwd",
+                         "views_per_step": nv, "batches_per_step": len(groups), "grad_mode": a.grad_mode},
+              "plain": {"value": round(nv / (ms_plain / 1e3), 3), "unit": UNIT, "ms_per_step": round(ms_plain, 3),
+                        "api": "sequential single-view _C.rasterize_gaussians + backward"},
+              "batched_vs_plain": round(ms_plain / ms_batch, 3)}
+    print(json.dumps(result), flush=True)
 
 
 # ---------------------------------------------------------------------------
@@ -353,6 +498,8 @@ def main():
     a = parse()
     if a.impl == "reference":
         run_reference(a)
+    elif a.config == "multiscene":
+        run_multiscene(a)
     else:
         run_ours(a)
 
