@@ -44,10 +44,13 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--no-batched", action="store_true", help="skip the batched-call measurement of the workload")
-    ap.add_argument("--config", default="single", choices=["single", "multiscene"],
+    ap.add_argument("--config", default="single", choices=["single", "multiscene", "serve"],
                     help="single: the 500k / 512^2 drop-in workload (default); multiscene: 64 scenes, batched "
-                         "calls vs sequential single-view calls")
+                         "calls vs sequential single-view calls; serve: Poisson requests over the 64 resident "
+                         "scenes, continuous batching vs one call at a time")
     ap.add_argument("--scenes", type=int, default=64)
+    ap.add_argument("--rate", type=float, default=200.0, help="serve: request arrival rate (req/s)")
+    ap.add_argument("--requests", type=int, default=400, help="serve: requests per run")
     return ap.parse_args()
 
 
@@ -431,6 +434,42 @@ def run_multiscene(a):
     print(json.dumps(result), flush=True)
 
 
+def run_serve(a):
+    """Serving: Poisson render+backward requests (1-8 views, 256-1024^2) over
+    the resident multi-scene workload, admitted under a 150 GB budget and
+    batched on arrival, against the same requests served one call at a time."""
+    import torch
+    from word2world_b200 import serve as sv
+    device = torch.device("cuda", 0)
+    torch.cuda.set_device(device)
+    scs, _, Ps, _ = multiscene_workload(a, device)
+    srv = sv.Server(scs, hbm_budget_bytes=150e9, grad_mode=a.grad_mode)
+    warm = sv.poisson_requests(8, a.rate, scs, seed=a.seed + 99, device=device)
+    srv.serve(warm, realtime=False)
+    srv.serve_plain(sv.poisson_requests(4, a.rate, scs, seed=a.seed + 98, device=device), realtime=False)
+    rates = sorted({a.rate, 500.0, 2000.0})
+    runs = {}
+    for rate in rates:
+        reqs = sv.poisson_requests(a.requests, rate, scs, seed=a.seed + 3, device=device)
+        info = srv.serve(reqs, realtime=True)
+        served = dict(sv.latency_stats(reqs), batches=info["batches"])
+        reqs2 = sv.poisson_requests(a.requests, rate, scs, seed=a.seed + 3, device=device)
+        srv.serve_plain(reqs2, realtime=True)
+        plain = sv.latency_stats(reqs2)
+        runs[f"{rate:g}"] = {"served": served, "plain": plain,
+                             "served_vs_plain_throughput": round(served["views_per_s"] / plain["views_per_s"], 3)}
+    head = runs[f"{a.rate:g}"]
+    result = {"metric": "serve: fwd+bwd views/s and p50/p95/p99 latency, Poisson requests over 64 resident scenes",
+              "value": head["served"]["views_per_s"], "unit": UNIT, "n_gpus": 1, "steps": 1, "warmup": 1,
+              "ms_per_step": None, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+              "data": "synthetic (seeded scenes and requests, N(0,1) dL/dimage)",
+              "config": {"workload": f"{a.requests} requests per arrival rate (Poisson), 1-8 views each at "
+                                     f"256/512/1024^2, over {a.scenes} resident scenes ({int(Ps.sum())} Gaussians), "
+                                     f"150 GB admission budget", "grad_mode": a.grad_mode, "rate": a.rate},
+              "served": head["served"], "plain": head["plain"], "by_rate": runs}
+    print(json.dumps(result), flush=True)
+
+
 # ---------------------------------------------------------------------------
 # CPU baselines (the oracle: the reference has no CPU implementation)
 # ---------------------------------------------------------------------------
@@ -500,6 +539,8 @@ def main():
         run_reference(a)
     elif a.config == "multiscene":
         run_multiscene(a)
+    elif a.config == "serve":
+        run_serve(a)
     else:
         run_ours(a)
 

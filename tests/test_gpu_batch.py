@@ -85,5 +85,5 @@ def test_batch_scene_gradient_is_sum_over_its_views():
     for s in range(len(scs)):
         items = [v for v, view in enumerate(views) if view.scene == s]
         want = sum(g["per_item"][v][3] for v in items)
-        got = g["means3D"][s]
+        got = g["means3D"][g["groups"].index(s)]
         assert torch.allclose(got, want, rtol=1e-6, atol=1e-7)

@@ -1,0 +1,57 @@
+"""Serving loop: admission under the memory budget (CPU), and each request's
+result the same alone and inside a mixed batch (GPU)."""
+from types import SimpleNamespace
+
+import numpy as np
+import pytest
+
+torch = pytest.importorskip("torch")
+
+try:
+    from word2world_b200 import serve as sv
+except ImportError:  # the extension is not built here
+    sv = None
+
+
+def _fake_req(rid, scene, res, nv):
+    cam = SimpleNamespace(width=res, height=res)
+    return SimpleNamespace(rid=rid, scene=scene, cameras=[cam] * nv)
+
+
+@pytest.mark.skipif(sv is None, reason="extension not built")
+def test_admission_respects_budget():
+    scenes = [SimpleNamespace(P=100_000), SimpleNamespace(P=10_000)]
+    srv = sv.Server.__new__(sv.Server)
+    srv.scenes, srv.max_instances = scenes, 1e12
+    q = [_fake_req(0, 0, 512, 4), _fake_req(1, 1, 256, 1), _fake_req(2, 0, 1024, 8)]
+    sizes = [sv.request_bytes(r, scenes) for r in q]
+    srv.budget = sizes[0] + sizes[1] + 1
+    assert [r.rid for r in srv._admit(q)] == [0, 1]
+    srv.budget = 1.0  # a single oversized request is still admitted alone
+    assert [r.rid for r in srv._admit(q)] == [0]
+
+
+@pytest.mark.gpu
+@pytest.mark.skipif(not torch.cuda.is_available(), reason="needs a GPU")
+def test_request_same_alone_and_in_the_mix():
+    import parity
+    from word2world_b200 import scenes as S
+    from word2world_b200.batch import Scene
+    scs = [Scene.from_arrays(S.make_scene(P, seed=20 + k, layout="ball").activate(), "cuda")
+           for k, P in enumerate((4000, 9000, 2500))]
+    reqs = sv.poisson_requests(10, rate=1000.0, scenes=scs, seed=5, views=(1, 3), res=(64, 96, 128))
+    srv = sv.Server(scs, keep_results=True)
+    srv.serve(reqs, realtime=False)
+    for r in (reqs[0], reqs[4], reqs[9]):
+        mixed_color, mixed_grads = r.color, r.scene_grads["per_item"]
+        alone = sv.Request(r.rid, r.scene, r.cameras, r.grads)
+        srv.run_batch([alone])
+        torch.cuda.synchronize()
+        for a, b in zip(alone.color, mixed_color):
+            assert parity.bit_mismatch(a.cpu().numpy(), b.cpu().numpy()) == 0
+        for ga, gb in zip(alone.scene_grads["per_item"], mixed_grads):
+            for name, x, y in zip(parity.GRAD_NAMES, ga, gb):
+                chk = parity.grad_check(x.cpu().numpy(), y.cpu().numpy())
+                assert chk["norm_rel"] <= 1e-5 and chk["n_bad"] == 0, (r.rid, name, chk)
+    st = sv.latency_stats(reqs)
+    assert st["requests"] == 10 and st["p99_ms"] >= st["p50_ms"] > 0

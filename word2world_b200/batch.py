@@ -198,12 +198,16 @@ class BatchRenderer:
         return BatchResult(cols, deps, alps, rads, R, state)
 
     # ---- backward -----------------------------------------------------------
-    def backward(self, res: BatchResult, dL_dcolor, dL_ddepth=None, dL_dalpha=None, per_element: bool = False):
+    def backward(self, res: BatchResult, dL_dcolor, dL_ddepth=None, dL_dalpha=None, per_element: bool = False,
+                 groups=None):
         """Gradients for upstream image gradients given per item (lists of
-        [3,H,W] / [1,H,W] tensors).  Returns, per scene, the sum over its
-        items of dL/d(means3D, opacity, scales, rotations, shs) plus the
-        per-item dL/dmeans2D; ``per_element`` also returns the raw per-item
-        tensors (the single-view call's eight outputs for every item)."""
+        [3,H,W] / [1,H,W] tensors).  Items are summed by group (default: by
+        scene; a serving loop groups by request): returns, per group, the sum
+        over its items of dL/d(means3D, opacity, scales, rotations, shs), in
+        order of first appearance (``out["groups"]`` lists the group ids),
+        plus the per-item dL/dmeans2D; ``per_element`` also returns the raw
+        per-item tensors (the single-view call's eight outputs for every
+        item)."""
         L = lib()
         st = res.state
         arr, n, M, E, R = st["arr"], st["n"], st["M"], st["E"], st["R"]
@@ -224,18 +228,22 @@ class BatchRenderer:
                                     p(st["radii"]), p(st["alpha"]), p(dlc), p(dld), p(dla), self.grad_mode,
                                     p(scratch), ctypes.c_size_t(scratch.numel()), p(g_m2), p(g_col), p(g_op),
                                     p(g_m3), p(g_cov), p(g_sh), p(g_sc), p(g_rot), stream), "batch backward")
-        # per-scene sums of the items' element ranges (one index_add per tensor)
-        offsets, total = [], 0
-        for sc in scenes:
-            offsets.append(total)
-            total += sc.P
-        idx = torch.cat([torch.arange(scenes[v.scene].P, device=dev) + offsets[v.scene] for v in views])
-        out = {}
+        # per-group sums of the items' element ranges (one index_add per tensor)
+        gid = [groups[v] if groups is not None else views[v].scene for v in range(n)]
+        order, base, total = [], {}, 0
+        for v in range(n):
+            if gid[v] not in base:
+                base[gid[v]] = total
+                order.append(gid[v])
+                total += scenes[views[v].scene].P
+        idx = torch.cat([torch.arange(scenes[views[v].scene].P, device=dev) + base[gid[v]] for v in range(n)])
+        size = {gid[v]: scenes[views[v].scene].P for v in range(n)}
+        out = {"groups": order}
         for name, t in (("means3D", g_m3), ("opacities", g_op), ("scales", g_sc), ("rotations", g_rot),
                         ("shs", g_sh)):
             acc = torch.zeros((total,) + tuple(t.shape[1:]), dtype=torch.float32, device=dev)
             acc.index_add_(0, idx, t[:E])
-            out[name] = [acc[offsets[s]:offsets[s] + scenes[s].P] for s in range(len(scenes))]
+            out[name] = [acc[base[g]:base[g] + size[g]] for g in order]
         e = 0
         out["means2D"] = []
         raw = []

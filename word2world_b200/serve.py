@@ -1,0 +1,189 @@
+"""Serving loop: render + backward requests over device-resident scenes,
+admitted under an HBM budget and batched as they arrive.
+
+A request is (scene, views, upstream image gradients).  Scenes stay resident
+on the device.  The loop is continuous batching: each time the GPU finishes a
+batch, every request that has arrived and fits the memory budget joins the
+next batch (one BatchRenderer forward + backward over all their views), so
+requests that arrive while others are on the GPU wait at most one batch.
+Each request's result is what it would get alone: its images are
+bit-identical and its gradients equal up to float atomic order
+(tests/test_serve.py).  Latency is arrival to completion; completion is when
+the batch holding the request has finished on the device.
+
+The reference has no serving loop; its per-call path is one
+``Renderer.render`` per view (here: one single-view call at a time, FIFO,
+``serve_plain``) and stands beside this as the baseline.
+"""
+from __future__ import annotations
+
+import time
+from dataclasses import dataclass, field
+
+import numpy as np
+import torch
+
+from .batch import BatchRenderer, View
+
+# per-element and per-instance state bytes of a batched call (geometry state,
+# gradients, binning state) used for admission; instances per element are
+# estimated from the resolution (about 12 per element at 512^2 for compact
+# scenes, scaling with the pixel count)
+ELEM_BYTES = 1100
+INST_BYTES = 24
+PIX_BYTES = 48
+
+
+@dataclass
+class Request:
+    rid: int
+    scene: int
+    cameras: list            # Camera per view
+    grads: list              # [3,H,W] upstream gradient per view (device)
+    arrival: float = 0.0     # seconds from the start of the run
+    # filled by the server
+    start: float = 0.0
+    done: float = 0.0
+    color: list = field(default_factory=list)
+    scene_grads: dict = field(default_factory=dict)
+
+    def views(self):
+        return [View(self.scene, c) for c in self.cameras]
+
+
+def request_bytes(req: Request, scenes) -> int:
+    P = scenes[req.scene].P
+    total = 0
+    for c in req.cameras:
+        pix = int(c.width) * int(c.height)
+        inst = 12.0 * P * pix / (512 * 512)
+        total += ELEM_BYTES * P + INST_BYTES * inst + PIX_BYTES * pix
+    return int(total)
+
+
+class Server:
+    """Continuous-batching request loop over resident scenes."""
+
+    def __init__(self, scenes, hbm_budget_bytes: float = 150e9, max_instances: float = 4e8,
+                 grad_mode: str = "reference", keep_results: bool = False):
+        self.scenes = scenes
+        self.budget = float(hbm_budget_bytes)
+        self.max_instances = float(max_instances)  # keeps a batch's instance count far below the 2^30 limit
+        self.renderer = BatchRenderer(grad_mode=grad_mode)
+        self.keep = keep_results
+
+    def _admit(self, queue):
+        """Requests (in arrival order) that fit the memory budget and the
+        instance bound of one batch; at least one."""
+        batch, mem, inst = [], 0.0, 0.0
+        for r in queue:
+            b = request_bytes(r, self.scenes)
+            i = sum(12.0 * self.scenes[r.scene].P * c.width * c.height / (512 * 512) for c in r.cameras)
+            if batch and (mem + b > self.budget or inst + i > self.max_instances):
+                break
+            batch.append(r)
+            mem += b
+            inst += i
+        return batch
+
+    def run_batch(self, batch):
+        views = [v for r in batch for v in r.views()]
+        grads = [g for r in batch for g in r.grads]
+        groups = [k for k, r in enumerate(batch) for _ in r.cameras]
+        res = self.renderer.forward(self.scenes, views)
+        out = self.renderer.backward(res, grads, per_element=self.keep, groups=groups)
+        k = 0
+        for j, r in enumerate(batch):  # each request: its scene's gradient summed over its views
+            r.scene_grads = {name: out[name][j] for name in ("means3D", "opacities", "scales", "rotations", "shs")}
+            if self.keep:
+                n = len(r.cameras)
+                r.color = [c.clone() for c in res.color[k:k + n]]
+                r.scene_grads["per_item"] = out["per_item"][k:k + n]
+                k += n
+        return res, out
+
+    def serve(self, requests, realtime: bool = True):
+        """Process requests (sorted by arrival).  With realtime, arrivals are
+        honoured against the wall clock (the loop waits for the next arrival
+        when idle); otherwise all requests are present at time 0."""
+        pending = sorted(requests, key=lambda r: r.arrival)
+        queue = []
+        t0 = time.perf_counter()
+        now = lambda: time.perf_counter() - t0
+        batches = 0
+        while pending or queue:
+            t = now()
+            while pending and (not realtime or pending[0].arrival <= t):
+                queue.append(pending.pop(0))
+            if not queue:
+                time.sleep(max(0.0, min(pending[0].arrival - t, 0.001)))
+                continue
+            batch = self._admit(queue)
+            queue = queue[len(batch):]
+            start = now()
+            self.run_batch(batch)
+            torch.cuda.synchronize()
+            end = now()
+            for r in batch:
+                r.start, r.done = start, end
+            batches += 1
+        return dict(batches=batches, wall=now())
+
+    def serve_plain(self, requests, realtime: bool = True):
+        """Baseline: one single-view call per view, one request at a time, FIFO."""
+        from . import _C
+        pending = sorted(requests, key=lambda r: r.arrival)
+        dev = self.renderer.device
+        bg = torch.ones(3, device=dev)
+        empty = torch.empty(0, device=dev)
+        gm = self.renderer.grad_mode
+        t0 = time.perf_counter()
+        now = lambda: time.perf_counter() - t0
+        for r in pending:
+            if realtime and r.arrival > now():
+                time.sleep(r.arrival - now())
+            r.start = now()
+            sc = self.scenes[r.scene]
+            for c, g in zip(r.cameras, r.grads):
+                tt = lambda a: torch.from_numpy(np.ascontiguousarray(a, dtype=np.float32)).to(dev)
+                V, Pm, C = tt(c.viewmatrix), tt(c.projmatrix), tt(c.campos)
+                R, color, depth, alpha, radii, geom, binb, img = _C.rasterize_gaussians(
+                    sc.shs, c.focal_y, sc.scales, sc.means3D, Pm, sc.sh_degree, sc.opacities, sc.rotations, C, V,
+                    c.focal_x, c.height, c.width, bg, True)
+                z = torch.zeros(1, c.height, c.width, device=dev)
+                _C.rasterize_gaussians_backward(bg, sc.means3D, radii, empty, sc.scales, sc.rotations, 1.0, empty,
+                                                V, Pm, c.tanfovx, c.tanfovy, g, z, z, sc.shs, sc.sh_degree, C, geom,
+                                                R, binb, img, alpha, False, gm)
+            torch.cuda.synchronize()
+            r.done = now()
+        return dict(wall=now())
+
+
+def latency_stats(requests):
+    lat = np.array([r.done - r.arrival for r in requests]) * 1e3
+    views = sum(len(r.cameras) for r in requests)
+    span = max(r.done for r in requests) - min(r.arrival for r in requests)
+    return {"p50_ms": round(float(np.percentile(lat, 50)), 3), "p95_ms": round(float(np.percentile(lat, 95)), 3),
+            "p99_ms": round(float(np.percentile(lat, 99)), 3), "mean_ms": round(float(lat.mean()), 3),
+            "requests": len(requests), "views": views, "views_per_s": round(views / span, 3),
+            "requests_per_s": round(len(requests) / span, 3)}
+
+
+def poisson_requests(n, rate, scenes, seed=0, device="cuda", views=(1, 8), res=(256, 512, 1024)):
+    """n requests with Poisson arrivals at `rate` per second over the resident
+    scenes: 1-8 orbit views each at a resolution from `res`, N(0,1) upstream
+    gradients."""
+    from .camera import orbit_camera
+    rng = np.random.default_rng(seed)
+    gaps = rng.exponential(1.0 / rate, size=n)
+    arrivals = np.cumsum(gaps) - gaps[0]
+    gen = torch.Generator(device=device).manual_seed(seed + 1)
+    out = []
+    for k in range(n):
+        s = int(rng.integers(len(scenes)))
+        nv = int(rng.integers(views[0], views[1] + 1))
+        r = int(rng.choice(res))
+        cams = [orbit_camera(float(rng.uniform(0, 360)), float(rng.uniform(-30, 30)), 2.5, r, r) for _ in range(nv)]
+        grads = [torch.randn(3, r, r, device=device, generator=gen) for _ in range(nv)]
+        out.append(Request(k, s, cams, grads, float(arrivals[k])))
+    return out
