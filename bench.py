@@ -44,10 +44,11 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--no-batched", action="store_true", help="skip the batched-call measurement of the workload")
-    ap.add_argument("--config", default="single", choices=["single", "multiscene", "serve"],
+    ap.add_argument("--config", default="single", choices=["single", "multiscene", "serve", "sortscan"],
                     help="single: the 500k / 512^2 drop-in workload (default); multiscene: 64 scenes, batched "
                          "calls vs sequential single-view calls; serve: Poisson requests over the 64 resident "
-                         "scenes, continuous batching vs one call at a time")
+                         "scenes, continuous batching vs one call at a time; sortscan: the sort and scan "
+                         "stages alone (20M keys, 2M counts), HBM GB/s")
     ap.add_argument("--scenes", type=int, default=64)
     ap.add_argument("--rate", type=float, default=200.0, help="serve: request arrival rate (req/s)")
     ap.add_argument("--requests", type=int, default=400, help="serve: requests per run")
@@ -88,7 +89,7 @@ class ClockSampler:
         try:
             self.f = open(self.path, "w")
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}",
-                                          "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.f,
+                                          "--format=csv,noheader,nounits", "-lms", "50"], stdout=self.f,
                                          stderr=subprocess.DEVNULL)
         except Exception:
             self.proc = None
@@ -470,6 +471,93 @@ def run_serve(a):
     print(json.dumps(result), flush=True)
 
 
+def run_sortscan(a):
+    """The sort and scan stages in isolation: a stable pair sort of 20M u64
+    keys (tile id in [0, 4096) with a Zipf(1.2) skew << 32 | float32 depth
+    bits, depths U[0.5, 4.5]; u32 payload = position) over the 44 significant
+    bits, and an exclusive u32 scan over 2M Poisson(8) tile-touch counts.
+    Each timed call is bracketed by CUDA events on the launching stream, with
+    a 512 MB write between calls so that no call starts with its input in L2.
+    Bytes per key: the minimum-traffic bound (key + value read and written
+    once, 24 B) and the traffic of the passes this sort runs (one histogram
+    read of the keys, 8 B, plus 24 B per onesweep pass)."""
+    import numpy as np
+    import torch
+    from word2world_b200 import _C, scenes
+    device = torch.device("cuda", 0)
+    torch.cuda.set_device(device)
+    n_sort, n_scan, bits = 20_000_000, 2_000_000, 44
+    keys_np, vals_np = scenes.sort_workload(n_sort, seed=a.seed)
+    counts_np = scenes.scan_workload(n_scan, seed=a.seed)
+    keys = torch.from_numpy(keys_np.view(np.int64)).to(device)
+    vals = torch.from_numpy(vals_np.view(np.int32)).to(device)
+    counts = torch.from_numpy(counts_np.view(np.int32)).to(device)
+    flush = torch.empty(512 << 20, dtype=torch.uint8, device=device)
+    stream = torch.cuda.current_stream()
+
+    def timed(fn):
+        for _ in range(max(a.warmup, 3)):
+            fn()
+        ms = []
+        for _ in range(a.steps):
+            flush.fill_(1)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            fn()
+            e1.record(stream)
+            torch.cuda.synchronize()
+            ms.append(e0.elapsed_time(e1))
+        return statistics.median(ms), ms
+
+    n0 = _C.launch_count()
+    ko, vo = _C.sort_pairs_u64(keys, vals, 0, bits)
+    sort_launches = _C.launch_count() - n0
+    ok_sort = bool((ko[1:] >= ko[:-1]).all()) and bool(torch.equal(keys[vo.long()], ko))
+    n0 = _C.launch_count()
+    sc = _C.scan_u32(counts, True)
+    scan_launches = _C.launch_count() - n0
+    ok_scan = int(sc[-1]) + int(counts[-1]) == int(counts_np.astype(np.uint64).sum())
+    del ko, vo, sc
+    peak, src = peaks()
+    with ClockSampler(0) as clk:
+        ms_sort, all_sort = timed(lambda: _C.sort_pairs_u64(keys, vals, 0, bits))
+        ms_scan, all_scan = timed(lambda: _C.scan_u32(counts, True))
+    passes = -(-bits // 9)
+    pass_bytes = 8 + 24 * passes
+    gbs = lambda b, n, ms: b * n / (ms * 1e-3) / 1e9
+    sort_gbs = gbs(pass_bytes, n_sort, ms_sort)
+    scan_gbs = gbs(8, n_scan, ms_scan)
+    # numpy on the host: stable argsort of a 2M-key sample, cumsum of the counts
+    t = time.perf_counter()
+    np.argsort(keys_np[:2_000_000], kind="stable")
+    cpu_sort = 2_000_000 / (time.perf_counter() - t)
+    result = {"metric": "sort stage HBM GB/s (20M u64 keys + u32 payload, 44 significant bits)",
+              "value": round(sort_gbs, 1), "unit": "GB/s", "n_gpus": 1, "steps": a.steps, "warmup": max(a.warmup, 3),
+              "ms_per_step": round(ms_sort, 4), "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+              "dtype": "u64", "data": "synthetic (seeded Zipf(1.2) tiles, U[0.5,4.5] depths, Poisson(8) counts)",
+              "config": {"workload": "stable pair sort of 20M u64 keys (tile<<32 | depth bits, 4096 tiles, "
+                                     "Zipf 1.2) + exclusive scan of 2M u32 counts", "keys": n_sort,
+                         "significant_bits": bits, "digit_bits": 9, "passes": passes, "scan_elements": n_scan,
+                         "l2": "512 MB write between timed calls"},
+              "roofline": {"bound": "hbm", "achieved": round(sort_gbs, 1), "peak": peak, "unit": "GB/s",
+                           "frac": round(sort_gbs / peak, 4), "peak_source": src,
+                           "bytes_per_key": pass_bytes, "traffic": None},
+              "sort": {"ms": round(ms_sort, 4), "ms_all": [round(x, 4) for x in all_sort],
+                       "gkeys_per_s": round(n_sort / (ms_sort * 1e-3) / 1e9, 3),
+                       "pass_traffic_gbs": round(sort_gbs, 1), "pass_traffic_frac": round(sort_gbs / peak, 4),
+                       "min_traffic_gbs": round(gbs(24, n_sort, ms_sort), 1),
+                       "min_traffic_frac": round(gbs(24, n_sort, ms_sort) / peak, 4),
+                       "launches": sort_launches, "sorted_and_permutation": ok_sort},
+              "scan": {"ms": round(ms_scan, 4), "ms_all": [round(x, 4) for x in all_scan],
+                       "gbs": round(scan_gbs, 1), "frac": round(scan_gbs / peak, 4),
+                       "launches": scan_launches, "total_matches": ok_scan},
+              "gpu_launches": sort_launches * a.steps + scan_launches * a.steps,
+              "cpu_baseline": {"value": round(cpu_sort / 1e6, 3), "unit": "Mkeys/s", "cores": 1, "kind": "port",
+                               "sample": "numpy stable argsort of the first 2M keys"},
+              "clocks": clk.summary()}
+    print(json.dumps(result), flush=True)
+
+
 # ---------------------------------------------------------------------------
 # CPU baselines (the oracle: the reference has no CPU implementation)
 # ---------------------------------------------------------------------------
@@ -541,6 +629,8 @@ def main():
         run_multiscene(a)
     elif a.config == "serve":
         run_serve(a)
+    elif a.config == "sortscan":
+        run_sortscan(a)
     else:
         run_ours(a)
 
