@@ -417,7 +417,7 @@ int w2w_sort_pairs_u64(const uint64_t* keys_in, const uint32_t* vals_in, uint64_
   return check_launch();
 }
 
-size_t w2w_scan_scratch_bytes(long long n) { return align256(scan_status_words(n) * 8) + 256; }
+size_t w2w_scan_scratch_bytes(long long n) { return align256(scan_scratch_bytes(n)); }
 
 int w2w_scan_u32(const uint32_t* in, uint32_t* out, long long n, int exclusive, void* scratch,
                  size_t scratch_bytes, w2w_stream_t stream) {
@@ -425,11 +425,7 @@ int w2w_scan_u32(const uint32_t* in, uint32_t* out, long long n, int exclusive, 
   if (n == 0) return W2W_OK;
   if (!in || !out) return W2W_ERR_INVALID;
   if (!scratch || scratch_bytes < w2w_scan_scratch_bytes(n)) return W2W_ERR_SCRATCH;
-  unsigned long long* status = static_cast<unsigned long long*>(scratch);
-  uint32_t* tail = at<uint32_t>(scratch, align256(scan_status_words(n) * 8));
-  cudaStream_t st = S(stream);
-  cudaMemsetAsync(tail, 0, 8, st);
-  launch_scan(in, out, n, exclusive, status, tail, tail + 1, st);
+  launch_scan(in, out, n, exclusive, scratch, S(stream));
   return check_launch();
 }
 
@@ -447,7 +443,7 @@ int w2w_scan_u32_noalloc(const uint32_t* in, uint32_t* out, long long n, int exc
   int rc = 0;
   void* scratch = scan_noalloc_scratch(&rc);
   if (rc != 0 || scratch == nullptr) return W2W_ERR_CUDA;
-  launch_scan_noalloc(in, out, n, exclusive, scratch, S(stream));
+  launch_scan(in, out, n, exclusive, scratch, S(stream));
   return check_launch();
 }
 

@@ -209,10 +209,8 @@ void stage_begin(int stage, cudaStream_t s);
 void stage_end(int stage, cudaStream_t s, int kernels);
 
 size_t scan_status_words(long long n);
-void launch_scan(const uint32_t* in, uint32_t* out, long long n, int exclusive, unsigned long long* status,
-                 uint32_t* counter, uint32_t* err, cudaStream_t stream);
+size_t scan_scratch_bytes(long long n);
+void launch_scan(const uint32_t* in, uint32_t* out, long long n, int exclusive, void* scratch, cudaStream_t stream);
 long long scan_noalloc_max();
 void* scan_noalloc_scratch(int* status);
-void launch_scan_noalloc(const uint32_t* in, uint32_t* out, long long n, int exclusive, void* scratch,
-                         cudaStream_t stream);
 }  // namespace w2w

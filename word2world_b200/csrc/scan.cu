@@ -61,29 +61,46 @@ scan_kernel(const uint32_t* __restrict__ in, uint32_t* __restrict__ out, long lo
   }
   __syncthreads();
   const uint32_t total = s_warp[kScanThreads / 32 - 1];
-  // decoupled lookback; a status word carries its flag and count together and
-  // nothing else written by its tile is read, so relaxed accesses suffice
-  if (tid == 0) {
+  // decoupled lookback by warp 0: each step reads the status words of the 32
+  // tiles before t at once and, once every one of them up to the nearest
+  // inclusive prefix has published, adds them up (bounded wait).  A status
+  // word carries its flag and count together and nothing else written by its
+  // tile is read, so relaxed accesses suffice.
+  if (warp == 0) {
     if (tile == 0) {
-      st_relaxed64(status, kInc | total);
-      s_prefix = 0;
+      if (lane == 0) {
+        st_relaxed64(status, kInc | total);
+        s_prefix = 0;
+      }
     } else {
-      st_relaxed64(status + tile, kAgg | total);
+      if (lane == 0) st_relaxed64(status + tile, kAgg | total);
       uint32_t acc = 0, spins = 0;
       long long t = tile - 1;
-      while (t >= 0) {
-        const unsigned long long w = ld_relaxed64(status + t);
+      while (true) {
+        const long long q = t - lane;
+        const unsigned long long w = q >= 0 ? ld_relaxed64(status + q) : kInc;
         const unsigned long long flag = w & kFlags;
-        if (flag == 0ull) {
-          if (++spins > kSpinLimit) { atomicOr(err, kErrTimeout); break; }
+        const uint32_t inc = __ballot_sync(0xffffffffu, flag == kInc);
+        const uint32_t ready = __ballot_sync(0xffffffffu, flag != 0ull);
+        const uint32_t need = inc ? ((inc & (0u - inc)) << 1) - 1u : 0xffffffffu;  // lanes up to the nearest inclusive
+        if ((ready & need) != need) {
+          if (++spins > kSpinLimit) {
+            if (lane == 0) atomicOr(err, kErrTimeout);
+            break;
+          }
           continue;
         }
-        acc += uint32_t(w);
-        if (flag == kInc) break;
-        --t;
+        uint32_t part = (need >> lane) & 1u ? uint32_t(w) : 0u;
+#pragma unroll
+        for (int d = 16; d > 0; d >>= 1) part += __shfl_xor_sync(0xffffffffu, part, d);
+        acc += part;
+        if (inc) break;
+        t -= 32;
       }
-      s_prefix = acc;
-      st_relaxed64(status + tile, kInc | uint32_t(acc + total));
+      if (lane == 0) {
+        s_prefix = acc;
+        st_relaxed64(status + tile, kInc | uint32_t(acc + total));
+      }
     }
   }
   __syncthreads();
@@ -101,16 +118,18 @@ scan_kernel(const uint32_t* __restrict__ in, uint32_t* __restrict__ out, long lo
   }
 }
 
-// Scratch of the allocation-free entry point: the lookback status words for
-// up to kScanNoAllocMax elements, then the tile counter and the error word.
-// Every device that loads this library holds it (about 32 KB) until exit.
+// Scratch of the allocation-free entry point, laid out like a caller's
+// scratch (see launch_scan) for up to kScanNoAllocMax elements.  Every device
+// that loads this library holds it (about 32 KB) until exit.
 constexpr long long kScanNoAllocMax = 1LL << 24;
 constexpr size_t kNoAllocStatusBytes = size_t((kScanNoAllocMax + kScanTile - 1) / kScanTile) * 8;
-static __device__ __align__(256) unsigned char g_scan_scratch[kNoAllocStatusBytes + 256];
+static __device__ __align__(256) unsigned char g_scan_scratch[256 + kNoAllocStatusBytes];
 
 }  // namespace
 
 size_t scan_status_words(long long n) { return size_t((n + kScanTile - 1) / kScanTile) + 1; }
+
+size_t scan_scratch_bytes(long long n) { return 256 + scan_status_words(n) * 8; }
 
 long long scan_noalloc_max() { return kScanNoAllocMax; }
 
@@ -139,22 +158,17 @@ void* scan_noalloc_scratch(int* status) {
   return addr[dev];
 }
 
-void launch_scan_noalloc(const uint32_t* in, uint32_t* out, long long n, int exclusive, void* scratch,
-                         cudaStream_t stream) {
-  unsigned long long* status = static_cast<unsigned long long*>(scratch);
-  uint32_t* tail = reinterpret_cast<uint32_t*>(static_cast<unsigned char*>(scratch) + kNoAllocStatusBytes);
-  cudaMemsetAsync(tail, 0, 8, stream);  // error word (launch_scan clears status and counter)
-  launch_scan(in, out, n, exclusive, status, tail, tail + 1, stream);
-}
-
-void launch_scan(const uint32_t* in, uint32_t* out, long long n, int exclusive, unsigned long long* status,
-                 uint32_t* counter, uint32_t* err, cudaStream_t stream) {
+// scratch: [tile counter u32, error word u32, pad to 256 B][one 64-bit status
+// word per tile]; one memset clears all of it.
+void launch_scan(const uint32_t* in, uint32_t* out, long long n, int exclusive, void* scratch, cudaStream_t stream) {
   if (n <= 0) return;
   const long long tiles = (n + kScanTile - 1) / kScanTile;
-  cudaMemsetAsync(status, 0, sizeof(unsigned long long) * size_t(tiles), stream);
-  cudaMemsetAsync(counter, 0, sizeof(uint32_t), stream);
+  unsigned char* b = static_cast<unsigned char*>(scratch);
+  cudaMemsetAsync(b, 0, 256 + sizeof(unsigned long long) * size_t(tiles), stream);
+  uint32_t* counter = reinterpret_cast<uint32_t*>(b);
+  unsigned long long* status = reinterpret_cast<unsigned long long*>(b + 256);
   stage_begin(kStScan, stream);
-  scan_kernel<<<int(tiles), kScanThreads, 0, stream>>>(in, out, n, exclusive, status, counter, err);
+  scan_kernel<<<int(tiles), kScanThreads, 0, stream>>>(in, out, n, exclusive, status, counter, counter + 1);
   stage_end(kStScan, stream, 1);
 }
 
