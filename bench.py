@@ -33,7 +33,7 @@ FALLBACK_HBM_GBS = 6650.0
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--steps", type=int, default=100)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="w2w", choices=["w2w", "reference"])
     ap.add_argument("--P", type=int, default=500_000)
@@ -93,6 +93,15 @@ class ClockSampler:
                                          stderr=subprocess.DEVNULL)
         except Exception:
             self.proc = None
+            return self
+        # nvidia-smi takes a moment to start: wait (at most 5 s) for its first
+        # row so that the samples cover the timed region from its start
+        t0 = time.time()
+        while time.time() - t0 < 5.0 and self.proc.poll() is None:
+            self.f.flush()
+            if os.path.getsize(self.path) > 0:
+                break
+            time.sleep(0.02)
         return self
 
     def __exit__(self, *exc):
@@ -309,7 +318,7 @@ def run_batched_single(a, sc, cams, device, world, plain_value):
     bs = Scene.from_arrays(sc.activate(), device)
     views = [View(0, c) for c in cams]
     grads = [torch.from_numpy(g).to(device) for g in scenes.upstream_grads(a.views, a.res, a.res, seed=a.seed + 1)]
-    br = BatchRenderer(grad_mode=a.grad_mode)
+    br = BatchRenderer(grad_mode=a.grad_mode, reuse_buffers=True)
 
     def step():
         res = br.forward([bs], views)
@@ -398,7 +407,7 @@ def run_multiscene(a):
                                             cam["view"], cam["proj"], c.tanfovx, c.tanfovy, grads[i], z, z, sc.shs,
                                             3, cam["campos"], geom, R, binb, img, alpha, False, gmode)
 
-    br = BatchRenderer(grad_mode=a.grad_mode)
+    br = BatchRenderer(grad_mode=a.grad_mode, reuse_buffers=True)
     groups = buckets(scs, views)
     index = {id(v): i for i, v in enumerate(views)}
 
@@ -439,21 +448,33 @@ def run_serve(a):
     """Serving: Poisson render+backward requests (1-8 views, 256-1024^2) over
     the resident multi-scene workload, admitted under a 150 GB budget and
     batched on arrival, against the same requests served one call at a time."""
+    import numpy as np
     import torch
     from word2world_b200 import serve as sv
     device = torch.device("cuda", 0)
     torch.cuda.set_device(device)
     scs, _, Ps, _ = multiscene_workload(a, device)
     srv = sv.Server(scs, hbm_budget_bytes=150e9, grad_mode=a.grad_mode)
-    warm = sv.poisson_requests(8, a.rate, scs, seed=a.seed + 99, device=device)
+    # warm-up: a backlog of requests served at once fills batches up to the
+    # admission bounds, so the workspace reaches its working size before the
+    # timed runs (a server reserves its memory before taking traffic)
+    warm = sv.poisson_requests(160, a.rate, scs, seed=a.seed + 99, device=device)
     srv.serve(warm, realtime=False)
+    del warm
     srv.serve_plain(sv.poisson_requests(4, a.rate, scs, seed=a.seed + 98, device=device), realtime=False)
     rates = sorted({a.rate, 500.0, 2000.0})
     runs = {}
     for rate in rates:
         reqs = sv.poisson_requests(a.requests, rate, scs, seed=a.seed + 3, device=device)
+        srv.batch_ms = []
+        grown = srv.renderer.ws.grown
         info = srv.serve(reqs, realtime=True)
-        served = dict(sv.latency_stats(reqs), batches=info["batches"])
+        bm = np.array(srv.batch_ms)
+        served = dict(sv.latency_stats(reqs), batches=info["batches"],
+                      workspace_growths=srv.renderer.ws.grown - grown,
+                      batch_ms_p50=round(float(np.percentile(bm, 50)), 3),
+                      batch_ms_p99=round(float(np.percentile(bm, 99)), 3),
+                      workspace_gb=round(srv.renderer.ws.bytes / 1e9, 2))
         reqs2 = sv.poisson_requests(a.requests, rate, scs, seed=a.seed + 3, device=device)
         srv.serve_plain(reqs2, realtime=True)
         plain = sv.latency_stats(reqs2)
@@ -602,21 +623,25 @@ def run_reference(a):
     if rank != 0:
         return
     procs = max(1, min(a.views, os.cpu_count() or 1))
+    # a CPU step takes seconds: at most 3 timed steps after one warm-up step
+    # keep the run within a few minutes whatever --steps asks
+    steps, warm = max(1, min(a.steps, 3)), 1
     ctx = mp.get_context("spawn")
     with ctx.Pool(procs, initializer=_worker_init, initargs=(a.P, a.res, a.views, a.seed)) as pool:
-        for _ in range(max(a.warmup, 1)):
+        for _ in range(warm):
             pool.map(_worker_view, range(a.views))
         t0 = time.perf_counter()
-        for _ in range(a.steps):
+        for _ in range(steps):
             pool.map(_worker_view, range(a.views))
         dt = time.perf_counter() - t0
-    value = a.views * a.steps / dt
+    value = a.views * steps / dt
     result = {"metric": METRIC, "value": round(value, 4), "unit": UNIT, "n_gpus": int(os.environ.get("WORLD_SIZE", "1")),
-              "steps": a.steps, "warmup": a.warmup, "ms_per_step": round(dt / a.steps * 1e3, 2),
+              "steps": steps, "warmup": warm, "ms_per_step": round(dt / steps * 1e3, 2),
               "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
               "data": "synthetic (seeded scene, N(0,1) dL/dimage)", "config": workload_config(a), "impl": "reference",
               "cpu_baseline": {"value": round(value, 4), "unit": UNIT, "cores": procs, "kind": "port",
-                               "sample": f"all {a.views} views per step, one process per view"},
+                               "sample": f"all {a.views} views per step, one process per view, {steps} timed "
+                                         f"steps (--steps {a.steps} asked)"},
               "e2e": {"value": round(value, 4), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(result), flush=True)
 

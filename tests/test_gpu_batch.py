@@ -38,14 +38,17 @@ def _plain(sc, view):
                                   c.width, bg, True), bg
 
 
-@pytest.mark.parametrize("grad_mode", ["reference", "exact"])
-def test_batch_matches_single_views(grad_mode):
+@pytest.mark.parametrize("grad_mode,reuse", [("reference", False), ("exact", False), ("reference", True)])
+def test_batch_matches_single_views(grad_mode, reuse):
     scs, views = _setup()
-    br = BatchRenderer(grad_mode=grad_mode)
-    res = br.forward(scs, views)
+    br = BatchRenderer(grad_mode=grad_mode, reuse_buffers=reuse)
     rng = np.random.default_rng(11)
     grads = [torch.from_numpy(rng.normal(size=(3, v.camera.height, v.camera.width)).astype(np.float32)).to(DEV)
              for v in views]
+    if reuse:  # leave another batch's contents in the workspace first
+        warm = br.forward(scs, views[::-1])
+        br.backward(warm, [torch.randn_like(g) for g in grads[::-1]])
+    res = br.forward(scs, views)
     g = br.backward(res, grads, per_element=True)
     torch.cuda.synchronize()
     npix_before = 0

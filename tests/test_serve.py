@@ -22,13 +22,29 @@ def _fake_req(rid, scene, res, nv):
 def test_admission_respects_budget():
     scenes = [SimpleNamespace(P=100_000), SimpleNamespace(P=10_000)]
     srv = sv.Server.__new__(sv.Server)
-    srv.scenes, srv.max_instances = scenes, 1e12
+    srv.scenes, srv.max_instances, srv.max_work = scenes, 1e12, 1e12
     q = [_fake_req(0, 0, 512, 4), _fake_req(1, 1, 256, 1), _fake_req(2, 0, 1024, 8)]
     sizes = [sv.request_bytes(r, scenes) for r in q]
     srv.budget = sizes[0] + sizes[1] + 1
     assert [r.rid for r in srv._admit(q)] == [0, 1]
     srv.budget = 1.0  # a single oversized request is still admitted alone
     assert [r.rid for r in srv._admit(q)] == [0]
+    srv.budget, srv.max_work = 1e15, 4 * 100_000 + 10_000  # the work bound: Gaussian-views per batch
+    assert [r.rid for r in srv._admit(q)] == [0, 1]
+
+
+@pytest.mark.skipif(sv is None, reason="extension not built")
+def test_workspace_grows_only_when_needed():
+    from word2world_b200.batch import _Workspace
+    ws = _Workspace(torch.device("cpu"))
+    a = ws.f32("g", 100, 3)
+    assert a.shape == (100, 3) and ws.grown == 1
+    b = ws.f32("g", 190, 3)  # within the 2x headroom: same storage
+    assert b.shape == (190, 3) and ws.grown == 1 and b.data_ptr() == a.data_ptr()
+    c = ws.f32("g", 1000, 3)
+    assert c.shape == (1000, 3) and ws.grown == 2
+    assert ws.f32("g", 0, 3).shape == (0, 3) and ws.i64("idx", 0).numel() == 0
+    assert ws.take("u", 7).numel() == 7 and ws.bytes % 256 == 0
 
 
 @pytest.mark.gpu
@@ -55,3 +71,8 @@ def test_request_same_alone_and_in_the_mix():
                 assert chk["norm_rel"] <= 1e-5 and chk["n_bad"] == 0, (r.rid, name, chk)
     st = sv.latency_stats(reqs)
     assert st["requests"] == 10 and st["p99_ms"] >= st["p50_ms"] > 0
+    # the same stream again: the workspace already holds the largest batch
+    grown = srv.renderer.ws.grown
+    srv.serve(sv.poisson_requests(10, rate=1000.0, scenes=scs, seed=5, views=(1, 3), res=(64, 96, 128)),
+              realtime=False)
+    assert srv.renderer.ws.grown == grown

@@ -108,13 +108,81 @@ class BatchResult:
     state: dict = field(repr=False, default_factory=dict)
 
 
-class BatchRenderer:
-    """Forward + backward of a list of (scene, view) items, one launch per stage."""
+class _Workspace:
+    """Grow-only device buffers, one per role, reused from call to call.
 
-    def __init__(self, grad_mode: str = "reference", compat_spill: bool = True, device=None):
+    Batches of different sizes would otherwise ask the caching allocator for
+    new multi-GB blocks of ever different sizes; when its cache cannot serve
+    one it synchronises and returns memory to the driver before retrying,
+    which stalls a serving loop for tens of milliseconds.  Here a role's
+    buffer is replaced only when a call needs more than it holds, by twice
+    the need, so a growing stream of batches settles after a few growths; the
+    old buffer goes back to the driver before the new one is taken, so the
+    cache never holds dead blocks of old sizes."""
+
+    def __init__(self, device):
+        self.device = device
+        self.bufs = {}
+        self.grown = 0
+
+    def take(self, role: str, nbytes: int) -> torch.Tensor:
+        need = int(nbytes)
+        b = self.bufs.get(role)
+        if b is None or b.numel() < need:
+            if self.bufs.pop(role, None) is not None and self.device.type == "cuda":
+                del b
+                torch.cuda.empty_cache()
+            size = (max(2 * need, 256) + 255) // 256 * 256
+            b = torch.empty(size, dtype=torch.uint8, device=self.device)
+            self.bufs[role] = b
+            self.grown += 1
+        return b[:need]
+
+    def f32(self, role: str, *shape) -> torch.Tensor:
+        n = int(np.prod(shape))
+        return self.take(role, 4 * n).view(torch.float32).view(*shape)
+
+    def i32(self, role: str, n: int) -> torch.Tensor:
+        return self.take(role, 4 * n).view(torch.int32)
+
+    def i64(self, role: str, n: int) -> torch.Tensor:
+        return self.take(role, 8 * n).view(torch.int64)
+
+    @property
+    def bytes(self) -> int:
+        return sum(b.numel() for b in self.bufs.values())
+
+
+class BatchRenderer:
+    """Forward + backward of a list of (scene, view) items, one launch per stage.
+
+    With ``reuse_buffers`` every device buffer of a call (state, images,
+    gradients) comes from a grow-only workspace owned by the renderer, so a
+    stream of batches of varying size makes no allocator calls once the
+    workspace has grown to the largest batch.  A forward's outputs are then
+    valid until the next forward, a backward's until the next backward."""
+
+    def __init__(self, grad_mode: str = "reference", compat_spill: bool = True, device=None,
+                 reuse_buffers: bool = False):
         self.grad_mode = GRAD_MODES[grad_mode]
         self.compat_spill = int(bool(compat_spill))
         self.device = torch.device(device) if device is not None else torch.device("cuda", torch.cuda.current_device())
+        self.ws = _Workspace(self.device) if reuse_buffers else None
+
+    def _u8(self, role, nbytes):
+        if self.ws is not None:
+            return self.ws.take(role, nbytes)
+        return torch.empty(int(nbytes), dtype=torch.uint8, device=self.device)
+
+    def _f32(self, role, *shape):
+        if self.ws is not None:
+            return self.ws.f32(role, *shape)
+        return torch.empty(*shape, dtype=torch.float32, device=self.device)
+
+    def _i32(self, role, n):
+        if self.ws is not None:
+            return self.ws.i32(role, n)
+        return torch.empty(n, dtype=torch.int32, device=self.device)
 
     # ---- item table -------------------------------------------------------
     def _items(self, scenes, views):
@@ -165,19 +233,19 @@ class BatchRenderer:
         stream = ctypes.c_void_p(torch.cuda.current_stream(self.device).cuda_stream)
         E = sum(scenes[v.scene].P for v in views)
         dev = self.device
-        geom = torch.empty(int(L.w2w_batch_geometry_state_bytes(arr, n)), dtype=torch.uint8, device=dev)
-        radii = torch.empty(max(E, 1), dtype=torch.int32, device=dev)
+        geom = self._u8("geom", int(L.w2w_batch_geometry_state_bytes(arr, n)))
+        radii = self._i32("radii", max(E, 1))
         info = _Info()
         _check(L.w2w_batch_forward_geometry(arr, n, self.compat_spill, ctypes.c_void_p(radii.data_ptr()),
                                             ctypes.c_void_p(geom.data_ptr()), ctypes.byref(info), stream),
                "batch forward geometry")
         R = int(info.num_rendered)
-        binb = torch.empty(max(int(L.w2w_batch_binning_state_bytes(R, arr, n)), 1), dtype=torch.uint8, device=dev)
-        img = torch.empty(int(L.w2w_batch_image_state_bytes(arr, n)), dtype=torch.uint8, device=dev)
+        binb = self._u8("binb", max(int(L.w2w_batch_binning_state_bytes(R, arr, n)), 1))
+        img = self._u8("img", int(L.w2w_batch_image_state_bytes(arr, n)))
         pbase, npix = self.layout(views)
-        color = torch.empty(3 * npix, dtype=torch.float32, device=dev)
-        depth = torch.empty(npix, dtype=torch.float32, device=dev)
-        alpha = torch.empty(npix, dtype=torch.float32, device=dev)
+        color = self._f32("color", 3 * npix)
+        depth = self._f32("depth", npix)
+        alpha = self._f32("alpha", npix)
         _check(L.w2w_batch_forward_render(arr, n, ctypes.c_void_p(geom.data_ptr()), ctypes.byref(info),
                                           ctypes.c_void_p(binb.data_ptr()), ctypes.c_void_p(img.data_ptr()),
                                           ctypes.c_void_p(color.data_ptr()), ctypes.c_void_p(depth.data_ptr()),
@@ -214,15 +282,22 @@ class BatchRenderer:
         dev = self.device
         stream = ctypes.c_void_p(torch.cuda.current_stream(dev).cuda_stream)
         views, scenes = st["views"], st["scenes"]
-        dlc = torch.cat([g.reshape(-1) for g in dL_dcolor]).contiguous()
-        zeros = torch.zeros(st["npix"], dtype=torch.float32, device=dev)
-        dld = torch.cat([g.reshape(-1) for g in dL_ddepth]).contiguous() if dL_ddepth is not None else zeros
-        dla = torch.cat([g.reshape(-1) for g in dL_dalpha]).contiguous() if dL_dalpha is not None else zeros
-        scratch = torch.empty(int(L.w2w_batch_backward_scratch_bytes(arr, n)), dtype=torch.uint8, device=dev)
-        f = lambda *s: torch.empty(*s, dtype=torch.float32, device=dev)
+        def packed(role, gs):
+            out = self._f32(role, 3 * st["npix"] if role == "dlc" else st["npix"])
+            torch.cat([g.reshape(-1) for g in gs], out=out)
+            return out
+        dlc = packed("dlc", dL_dcolor)
+        if dL_ddepth is None or dL_dalpha is None:
+            zeros = self._f32("zeros", st["npix"])
+            zeros.zero_()
+        dld = packed("dld", dL_ddepth) if dL_ddepth is not None else zeros
+        dla = packed("dla", dL_dalpha) if dL_dalpha is not None else zeros
+        scratch = self._u8("scratch", int(L.w2w_batch_backward_scratch_bytes(arr, n)))
         Eg = max(E, 1)
-        g_m2, g_col, g_op = f(Eg, 3), f(Eg, 3), f(Eg, 1)
-        g_m3, g_cov, g_sh, g_sc, g_rot = f(Eg, 3), f(Eg, 6), f(Eg, max(M, 1), 3), f(Eg, 3), f(Eg, 4)
+        f = self._f32
+        g_m2, g_col, g_op = f("g_m2", Eg, 3), f("g_col", Eg, 3), f("g_op", Eg, 1)
+        g_m3, g_cov, g_sh = f("g_m3", Eg, 3), f("g_cov", Eg, 6), f("g_sh", Eg, max(M, 1), 3)
+        g_sc, g_rot = f("g_sc", Eg, 3), f("g_rot", Eg, 4)
         p = lambda t: ctypes.c_void_p(t.data_ptr())
         _check(L.w2w_batch_backward(arr, n, p(st["geom"]), ctypes.c_longlong(R), p(st["binb"]), p(st["img"]),
                                     p(st["radii"]), p(st["alpha"]), p(dlc), p(dld), p(dla), self.grad_mode,
@@ -236,12 +311,21 @@ class BatchRenderer:
                 base[gid[v]] = total
                 order.append(gid[v])
                 total += scenes[views[v].scene].P
-        idx = torch.cat([torch.arange(scenes[views[v].scene].P, device=dev) + base[gid[v]] for v in range(n)])
+        # element e of item v goes to row base[group of v] + (e - first element of v)
+        idx = self.ws.i64("idx", E) if self.ws is not None else torch.empty(E, dtype=torch.int64, device=dev)
+        torch.arange(E, out=idx)
+        e0 = 0
+        for v in range(n):
+            P = scenes[views[v].scene].P
+            if base[gid[v]] != e0:
+                idx[e0:e0 + P] += base[gid[v]] - e0
+            e0 += P
         size = {gid[v]: scenes[views[v].scene].P for v in range(n)}
         out = {"groups": order}
         for name, t in (("means3D", g_m3), ("opacities", g_op), ("scales", g_sc), ("rotations", g_rot),
                         ("shs", g_sh)):
-            acc = torch.zeros((total,) + tuple(t.shape[1:]), dtype=torch.float32, device=dev)
+            acc = self._f32("acc_" + name, total, *t.shape[1:])
+            acc.zero_()
             acc.index_add_(0, idx, t[:E])
             out[name] = [acc[base[g]:base[g] + size[g]] for g in order]
         e = 0

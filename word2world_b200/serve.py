@@ -65,25 +65,37 @@ class Server:
     """Continuous-batching request loop over resident scenes."""
 
     def __init__(self, scenes, hbm_budget_bytes: float = 150e9, max_instances: float = 4e8,
-                 grad_mode: str = "reference", keep_results: bool = False):
+                 max_batch_work: float = 2e7, grad_mode: str = "reference", keep_results: bool = False):
         self.scenes = scenes
         self.budget = float(hbm_budget_bytes)
         self.max_instances = float(max_instances)  # keeps a batch's instance count far below the 2^30 limit
-        self.renderer = BatchRenderer(grad_mode=grad_mode)
+        # latency bound: Gaussian-views per batch (sum of P over its views).
+        # A batch's time is close to linear in it (about 2.5 ns each on a B200
+        # for 256-1024^2 views), so 2e7 keeps a batch near 50 ms and a request
+        # that arrives during one waits at most that long before its own.
+        self.max_work = float(max_batch_work)
+        # one grow-only workspace for every batch: no allocator calls once it
+        # has grown to the largest batch (a request's gradients are therefore
+        # valid until the next batch unless keep_results copies them)
+        self.renderer = BatchRenderer(grad_mode=grad_mode, reuse_buffers=True)
         self.keep = keep_results
+        self.batch_ms = []
 
     def _admit(self, queue):
-        """Requests (in arrival order) that fit the memory budget and the
-        instance bound of one batch; at least one."""
-        batch, mem, inst = [], 0.0, 0.0
+        """Requests (in arrival order) that fit the memory budget, the
+        instance bound and the work bound of one batch; at least one."""
+        batch, mem, inst, work = [], 0.0, 0.0, 0.0
         for r in queue:
             b = request_bytes(r, self.scenes)
-            i = sum(12.0 * self.scenes[r.scene].P * c.width * c.height / (512 * 512) for c in r.cameras)
-            if batch and (mem + b > self.budget or inst + i > self.max_instances):
+            P = self.scenes[r.scene].P
+            i = sum(12.0 * P * c.width * c.height / (512 * 512) for c in r.cameras)
+            w = float(P) * len(r.cameras)
+            if batch and (mem + b > self.budget or inst + i > self.max_instances or work + w > self.max_work):
                 break
             batch.append(r)
             mem += b
             inst += i
+            work += w
         return batch
 
     def run_batch(self, batch):
@@ -96,9 +108,10 @@ class Server:
         for j, r in enumerate(batch):  # each request: its scene's gradient summed over its views
             r.scene_grads = {name: out[name][j] for name in ("means3D", "opacities", "scales", "rotations", "shs")}
             if self.keep:
+                r.scene_grads = {name: g.clone() for name, g in r.scene_grads.items()}
                 n = len(r.cameras)
                 r.color = [c.clone() for c in res.color[k:k + n]]
-                r.scene_grads["per_item"] = out["per_item"][k:k + n]
+                r.scene_grads["per_item"] = [tuple(x.clone() for x in item) for item in out["per_item"][k:k + n]]
                 k += n
         return res, out
 
@@ -124,6 +137,7 @@ class Server:
             self.run_batch(batch)
             torch.cuda.synchronize()
             end = now()
+            self.batch_ms.append((end - start) * 1e3)
             for r in batch:
                 r.start, r.done = start, end
             batches += 1
