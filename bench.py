@@ -28,6 +28,10 @@ METRIC = "fwd+bwd views/s at 500k Gaussians 512x512"
 UNIT = "views/s"
 PEAKS_FILE = os.path.join(ROOT, "MEASURED_PEAKS.json")
 FALLBACK_HBM_GBS = 6650.0
+# DRAM bytes (read + write) per launch, from one ncu capture of the default
+# workload (500k Gaussians, 512x512; profiles/dram_traffic_500k_512x512.md)
+NCU_TRAFFIC_500K_512 = {"sort_onesweep": 49.0e6, "preprocess": 181.2e6, "duplicate": 12.2e6,
+                        "sort_histogram": 23.7e6, "backward_gaussians": 232.4e6}
 
 
 def parse():
@@ -236,7 +240,10 @@ def run_ours(a):
         per_launch_ms = stage_ms[dom] / stage_n[dom] * (2 if dom == "sort_histogram" else 1)
         ach = alg_bytes[dom] / (per_launch_ms / 1e3) / 1e9
         roofline = {"kernel": dom, "bound": "hbm", "achieved": round(ach, 1), "peak": hbm, "unit": "GB/s",
-                    "frac": round(ach / hbm, 4), "peak_source": peak_kind, "traffic": None,
+                    "frac": round(ach / hbm, 4), "peak_source": peak_kind,
+                    "traffic": NCU_TRAFFIC_500K_512.get(dom) if (a.P, a.res) == (500_000, 512) else None,
+                    "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum per launch "
+                                      "(profiles/dram_traffic_500k_512x512.md)",
                     "algorithmic_bytes_per_launch": int(alg_bytes[dom]), "avg_launch_ms": round(per_launch_ms, 4)}
     stage_report = {k: {"ms_per_step": round(stage_ms[k] / a.steps, 4), "launches_per_step": stage_n[k] / a.steps,
                         "share": round(stage_ms[k] / total_stage, 4)} for k in stage_ms if stage_n[k]}
