@@ -230,7 +230,7 @@ __device__ __forceinline__ void sh_colour(const float* __restrict__ sh, int M, i
 }
 
 template <bool kSh16>
-__global__ void __launch_bounds__(kPreThreads)
+__global__ void __launch_bounds__(kPreThreads, 3)
 preprocess_kernel(PreprocessArgs a) {
   __shared__ uint32_t s_tile;
   __shared__ Pair s_warp[kPreThreads / 32];
@@ -418,34 +418,56 @@ preprocess_kernel(PreprocessArgs a) {
   }
   __syncthreads();
   const Pair block_total = s_warp[kPreThreads / 32 - 1];
-  // decoupled lookback; each status word carries its flag and pair together
-  // and nothing else written by its tile is read, so relaxed accesses suffice
-  if (threadIdx.x == 0) {
+  // decoupled lookback by warp 0; each status word carries its flag and pair
+  // together and nothing else written by its tile is read, so relaxed
+  // accesses suffice.  Each step reads the 32 tiles before t at once and,
+  // once every one of them up to the nearest inclusive prefix has published,
+  // combines them in index order (an ordered shuffle tree, older tiles on the
+  // left); a serial walk would cost one L2 round trip per tile.
+  if (warp == 0) {
     unsigned long long* status = a.scan_status;
     if (tile == 0) {
-      st_relaxed64(status + tile, pack(kFlagInc, block_total));
-      s_prefix = Pair{0, 0, 0};
+      if (lane == 0) {
+        st_relaxed64(status + tile, pack(kFlagInc, block_total));
+        s_prefix = Pair{0, 0, 0};
+      }
     } else {
-      st_relaxed64(status + tile, pack(kFlagAgg, block_total));
+      if (lane == 0) st_relaxed64(status + tile, pack(kFlagAgg, block_total));
+      // (0, 0, 0) is an identity on both sides for every pair that occurs
       Pair ex{0, 0, 0};
-      bool first = true;
-      int t = int(tile) - 1;
+      long long t = int(tile) - 1;
       uint32_t spins = 0;
-      while (t >= 0) {
-        const unsigned long long w = ld_relaxed64(status + t);
+      while (true) {
+        const long long q = t - lane;
+        const unsigned long long w = q >= 0 ? ld_relaxed64(status + q) : kFlagInc;
         const unsigned long long flag = w & (3ull << 62);
-        if (flag == 0) {
-          if (++spins > kSpinLimit) { atomicOr(&hdr->error, kErrTimeout); break; }
+        const uint32_t inc = __ballot_sync(0xffffffffu, flag == kFlagInc);
+        const uint32_t ready = __ballot_sync(0xffffffffu, flag != 0ull);
+        const uint32_t need = inc ? ((inc & (0u - inc)) << 1) - 1u : 0xffffffffu;
+        if ((ready & need) != need) {
+          if (++spins > kSpinLimit) {
+            if (lane == 0) atomicOr(&hdr->error, kErrTimeout);
+            break;
+          }
           continue;
         }
-        const Pair p = unpack(w);
-        ex = first ? p : combine(p, ex);
-        first = false;
-        if (flag == kFlagInc) break;
-        --t;
+        Pair p = (need >> lane) & 1u ? unpack(w) : Pair{0, 0, 0};
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+          Pair o;
+          o.s = __shfl_down_sync(0xffffffffu, p.s, d);
+          o.x = __shfl_down_sync(0xffffffffu, p.x, d);
+          o.f = __shfl_down_sync(0xffffffffu, p.f, d);
+          if (lane + d < 32) p = combine(o, p);
+        }
+        ex = combine(p, ex);  // lane 0 holds the window; the walk so far is newer
+        if (inc) break;
+        t -= 32;
       }
-      s_prefix = ex;
-      st_relaxed64(status + tile, pack(kFlagInc, combine(ex, block_total)));
+      if (lane == 0) {
+        s_prefix = ex;
+        st_relaxed64(status + tile, pack(kFlagInc, combine(ex, block_total)));
+      }
     }
   }
   __syncthreads();
