@@ -1,0 +1,100 @@
+"""The drop-in Python boundary: ``_render_gaussians_inline`` (the
+torch.autograd.Function of Renderer.py:28-110) and ``Renderer.render``
+(Renderer.py:119-192) against the binding they wrap.
+
+* the autograd Function's image, radii, depth and alpha are the binding's
+  forward outputs bit for bit, and the gradients autograd delivers to its
+  inputs are the binding's backward outputs for the same upstream gradient;
+* ``Renderer.render`` is the reference's activation preamble (sigmoid
+  opacity, exp scales, normalised quaternion, concatenated SH) followed by
+  that Function: its image equals the Function's on torch-activated
+  parameters bit for bit, and the raw parameters' gradients equal autograd
+  through the same torch preamble;
+* the image agrees with the oracle on the same activated parameters."""
+import numpy as np
+import pytest
+
+torch = pytest.importorskip("torch")
+pytestmark = pytest.mark.gpu
+if not torch.cuda.is_available():
+    pytest.skip("needs a GPU", allow_module_level=True)
+
+import oracle  # noqa: E402
+import parity  # noqa: E402
+from word2world_b200 import _C, camera, scenes  # noqa: E402
+from word2world_b200.renderer import GaussianParams, Renderer, _render_gaussians_inline  # noqa: E402
+
+DEV = "cuda"
+
+
+def _setup(P=6000, S=128, seed=3):
+    sc = scenes.make_scene(P, seed=seed, layout="ball")
+    cam = camera.orbit_camera(40.0, 10.0, 2.5, S, S)
+    t = lambda a: torch.from_numpy(np.ascontiguousarray(a, dtype=np.float32)).to(DEV)
+    return sc, cam, t
+
+
+@pytest.mark.parametrize("grad_mode", ["reference", "exact"])
+def test_autograd_function_matches_binding(grad_mode):
+    sc, cam, t = _setup()
+    m, o, s, q, sh = sc.activate()
+    S = cam.width
+    leaves = [t(x).requires_grad_(True) for x in (m, sh, o, s, q)]
+    means3D, shs, opac, scales, rots = leaves
+    means2D = torch.zeros_like(means3D, requires_grad=True)
+    bg = torch.ones(3, device=DEV)
+    V, Pm, C = t(cam.viewmatrix), t(cam.projmatrix), t(cam.campos)
+    color, radii, depth, alpha = _render_gaussians_inline(
+        means3D, means2D, shs, None, opac, scales, rots, None, bg, 1.0, V, Pm, cam.tanfovx, cam.tanfovy, 3, C,
+        image_height=S, image_width=S, grad_mode=grad_mode)
+    R, color_b, depth_b, alpha_b, radii_b, geom, binb, img = _C.rasterize_gaussians(
+        shs.detach(), cam.focal_y, scales.detach(), means3D.detach(), Pm, 3, opac.detach(), rots.detach(), C, V,
+        cam.focal_x, S, S, bg, True)
+    for a, b in ((color, color_b), (depth, depth_b), (alpha, alpha_b), (radii, radii_b)):
+        assert parity.bit_mismatch(a.detach().cpu().numpy(), b.cpu().numpy()) == 0
+    g = torch.randn(3, S, S, device=DEV, generator=torch.Generator(device=DEV).manual_seed(1))
+    torch.autograd.backward([color], [g])
+    z = torch.zeros(1, S, S, device=DEV)
+    empty = torch.empty(0, device=DEV)
+    gb = _C.rasterize_gaussians_backward(bg, means3D.detach(), radii_b, empty, scales.detach(), rots.detach(), 1.0,
+                                         empty, V, Pm, cam.tanfovx, cam.tanfovy, g, z, z, shs.detach(), 3, C, geom,
+                                         R, binb, img, alpha_b, False, 0 if grad_mode == "reference" else 1)
+    want = dict(means2D=gb[0], opac=gb[2], means3D=gb[3], shs=gb[5], scales=gb[6], rots=gb[7])
+    got = dict(means2D=means2D.grad, opac=opac.grad, means3D=means3D.grad, shs=shs.grad, scales=scales.grad,
+               rots=rots.grad)
+    for k in want:
+        chk = parity.grad_check(got[k].cpu().numpy(), want[k].cpu().numpy())
+        assert chk["norm_rel"] <= 1e-5 and chk["n_bad"] == 0, (k, chk)
+
+
+def test_renderer_render_is_preamble_plus_function():
+    sc, cam, t = _setup(seed=4)
+    S = cam.width
+    params = GaussianParams.from_scene(sc, device=DEV)
+    r = Renderer(params, sh_degree=3)
+    out = r.render(cam.fovx, cam.fovy, t(cam.viewmatrix), t(cam.projmatrix), t(cam.campos), S, S)
+    assert set(out) >= {"image", "accum_grads", "avaialble_pts", "available_pts"}
+    g = torch.randn(3, S, S, device=DEV, generator=torch.Generator(device=DEV).manual_seed(2))
+    (out["image"] * g).sum().backward()
+    got = [p.grad.clone() for p in params.parameters()]
+
+    # the same preamble written out with torch ops, then the Function
+    raw = [p.detach().clone().requires_grad_(True) for p in params.parameters()]
+    mean, sh_dc, sh_ac, opac_l, svec, quat = raw
+    shs = torch.cat((sh_dc, sh_ac), dim=1)
+    means2D = torch.zeros_like(mean, requires_grad=True)
+    image, radii, _, _ = _render_gaussians_inline(
+        mean, means2D, shs, None, torch.sigmoid(opac_l), torch.exp(svec), torch.nn.functional.normalize(quat), None,
+        torch.ones(3, device=DEV), 1, t(cam.viewmatrix), t(cam.projmatrix), np.tan(cam.fovx / 2),
+        np.tan(cam.fovy / 2), 3, t(cam.campos), image_height=S, image_width=S)
+    assert parity.bit_mismatch(out["image"].detach().cpu().numpy(), image.detach().cpu().numpy()) == 0
+    assert torch.equal(out["available_pts"], radii > 0)
+    (image * g).sum().backward()
+    for name, a, b in zip(("mean", "sh_dc", "sh_ac", "opacity", "svec", "quaternion"), got, raw):
+        chk = parity.grad_check(a.cpu().numpy(), b.grad.cpu().numpy())
+        assert chk["norm_rel"] <= 1e-5 and chk["n_bad"] == 0, (name, chk)
+
+    # and the image is the oracle's on the activated parameters
+    m, o, s, q, sh = sc.activate()
+    f = oracle.forward(oracle.RasterSettings.from_camera(cam), m, s, q, o, sh)
+    np.testing.assert_allclose(out["image"].detach().cpu().numpy(), f["color"], rtol=1e-4, atol=1e-5)
