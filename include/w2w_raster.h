@@ -165,6 +165,20 @@ int w2w_scan_u32(const uint32_t* in, uint32_t* out, long long n, int exclusive, 
 #define W2W_SCAN_NOALLOC_MAX (1LL << 24)
 int w2w_scan_u32_noalloc(const uint32_t* in, uint32_t* out, long long n, int exclusive, w2w_stream_t stream);
 
+/* The activation preamble of Renderer.render (Renderer.py:164-167) in one
+ * pass: opacity = sigmoid(logit) [P], scales = exp(svec) [P,3], rotations =
+ * normalize(quaternion) [P,4], shs = cat(sh_dc [P,1,3], sh_ac [P,K,3]) [P,K+1,3];
+ * bit-identical to the reference's torch operations.  The backward maps the
+ * activated tensors' gradients to the raw parameters' (quaternion: the raw
+ * one; opacity and scales: the activated ones). */
+int w2w_activate_forward(long long P, int K, const float* opacity_logit, const float* svec, const float* quaternion,
+                         const float* sh_dc, const float* sh_ac, float* opacity, float* scales, float* rotations,
+                         float* shs, w2w_stream_t stream);
+int w2w_activate_backward(long long P, int K, const float* g_opacity, const float* g_scales,
+                          const float* g_rotations, const float* g_shs, const float* opacity, const float* scales,
+                          const float* quaternion, float* d_opacity_logit, float* d_svec, float* d_quaternion,
+                          float* d_sh_dc, float* d_sh_ac, w2w_stream_t stream);
+
 /* Per-tile [start, end) from sorted keys whose tile id is key >> tile_shift
  * (gaussianTiles.cu:6-33); tiles without entries get (0, 0). */
 int w2w_tile_ranges(const uint64_t* sorted_keys, long long n, int tile_shift, uint32_t* ranges,

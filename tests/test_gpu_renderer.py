@@ -98,3 +98,35 @@ def test_renderer_render_is_preamble_plus_function():
     m, o, s, q, sh = sc.activate()
     f = oracle.forward(oracle.RasterSettings.from_camera(cam), m, s, q, o, sh)
     np.testing.assert_allclose(out["image"].detach().cpu().numpy(), f["color"], rtol=1e-4, atol=1e-5)
+
+
+def test_fused_activation_matches_torch():
+    """The fused preamble is bit-identical to the torch operations forward and
+    equal up to rounding backward, including zero and huge quaternions and
+    saturating logits."""
+    from word2world_b200.renderer import activate
+    gen = torch.Generator(device=DEV).manual_seed(5)
+    P = 200_003
+    logit = (torch.randn(P, 1, device=DEV, generator=gen) * 6).requires_grad_(True)
+    svec = (torch.randn(P, 3, device=DEV, generator=gen) * 3).requires_grad_(True)
+    q = torch.randn(P, 4, device=DEV, generator=gen)
+    q[:1000] = 0.0
+    q[1000:2000] *= 1e-20
+    q[2000:3000] *= 1e15
+    q.requires_grad_(True)
+    dc = torch.randn(P, 1, 3, device=DEV, generator=gen).requires_grad_(True)
+    ac = torch.randn(P, 15, 3, device=DEV, generator=gen).requires_grad_(True)
+    got = activate(logit, svec, q, dc, ac)
+    want = (torch.sigmoid(logit), torch.exp(svec), torch.nn.functional.normalize(q), torch.cat((dc, ac), dim=1))
+    for a, b in zip(got, want):
+        assert a.shape == b.shape
+        assert parity.bit_mismatch(a.detach().cpu().numpy(), b.detach().cpu().numpy()) == 0
+    gs = [torch.randn(t.shape, device=DEV, generator=gen) for t in want]
+    gg = torch.autograd.grad(got, (logit, svec, q, dc, ac), gs)
+    gw = torch.autograd.grad(want, (logit, svec, q, dc, ac), gs)
+    for name, a, b in zip(("logit", "svec", "quaternion", "sh_dc", "sh_ac"), gg, gw):
+        a, b = a.cpu().numpy().reshape(P, -1), b.cpu().numpy().reshape(P, -1)
+        if name == "quaternion":  # away from the 1e-12 floor, where torch's clamp has a kink
+            a, b = a[1000:], b[1000:]
+        chk = parity.grad_check(a, b)
+        assert chk["norm_rel"] <= 1e-6 and chk["n_bad"] == 0, (name, chk)

@@ -218,6 +218,52 @@ std::tuple<Tensor, Tensor> sort_pairs_u64(const Tensor& keys, const Tensor& vals
   return std::make_tuple(ko, vo);
 }
 
+// Renderer.render's activation preamble (Renderer.py:164-167), fused.
+std::tuple<Tensor, Tensor, Tensor, Tensor> activate(const Tensor& opacity_logit, const Tensor& svec,
+                                                    const Tensor& quaternion, const Tensor& sh_dc,
+                                                    const Tensor& sh_ac) {
+  const auto dev = opacity_logit.device();
+  c10::cuda::CUDAGuard guard(dev);
+  Tensor o = f32(opacity_logit, "opacity", dev), s = f32(svec, "svec", dev), q = f32(quaternion, "quaternion", dev);
+  Tensor dc = f32(sh_dc, "sh_dc", dev), ac = f32(sh_ac, "sh_ac", dev);
+  const int64_t P = o.size(0);
+  TORCH_CHECK(o.numel() == P && s.numel() == 3 * P && q.numel() == 4 * P && dc.numel() == 3 * P,
+              "opacity [P,1], svec [P,3], quaternion [P,4], sh_dc [P,1,3] expected");
+  TORCH_CHECK(ac.dim() == 3 && ac.size(0) == P && ac.size(2) == 3, "sh_ac [P,K,3] expected");
+  const int64_t K = ac.size(1);
+  Tensor op = torch::empty_like(o), sc = torch::empty_like(s), rot = torch::empty_like(q);
+  Tensor shs = torch::empty({P, K + 1, 3}, o.options());
+  check(w2w_activate_forward(P, int(K), o.data_ptr<float>(), s.data_ptr<float>(), q.data_ptr<float>(),
+                             dc.data_ptr<float>(), ac.data_ptr<float>(), op.data_ptr<float>(), sc.data_ptr<float>(),
+                             rot.data_ptr<float>(), shs.data_ptr<float>(), cur_stream()),
+        "w2w_activate_forward");
+  return std::make_tuple(op, sc, rot, shs);
+}
+
+std::tuple<Tensor, Tensor, Tensor, Tensor, Tensor> activate_backward(const Tensor& g_opacity, const Tensor& g_scales,
+                                                                     const Tensor& g_rotations, const Tensor& g_shs,
+                                                                     const Tensor& opacity, const Tensor& scales,
+                                                                     const Tensor& quaternion) {
+  const auto dev = opacity.device();
+  c10::cuda::CUDAGuard guard(dev);
+  Tensor go = f32(g_opacity, "g_opacity", dev), gs = f32(g_scales, "g_scales", dev);
+  Tensor gr = f32(g_rotations, "g_rotations", dev), gsh = f32(g_shs, "g_shs", dev);
+  Tensor o = f32(opacity, "opacity", dev), s = f32(scales, "scales", dev), q = f32(quaternion, "quaternion", dev);
+  const int64_t P = o.size(0);
+  TORCH_CHECK(gsh.dim() == 3 && gsh.size(0) == P && gsh.size(2) == 3, "g_shs [P,K+1,3] expected");
+  TORCH_CHECK(go.numel() == P && gs.numel() == 3 * P && gr.numel() == 4 * P && s.numel() == 3 * P &&
+                  q.numel() == 4 * P, "gradient shapes do not match the parameters");
+  const int64_t K = gsh.size(1) - 1;
+  Tensor dlogit = torch::empty_like(o), dsvec = torch::empty_like(s), dq = torch::empty_like(q);
+  Tensor ddc = torch::empty({P, 1, 3}, o.options()), dac = torch::empty({P, K, 3}, o.options());
+  check(w2w_activate_backward(P, int(K), go.data_ptr<float>(), gs.data_ptr<float>(), gr.data_ptr<float>(),
+                              gsh.data_ptr<float>(), o.data_ptr<float>(), s.data_ptr<float>(), q.data_ptr<float>(),
+                              dlogit.data_ptr<float>(), dsvec.data_ptr<float>(), dq.data_ptr<float>(),
+                              ddc.data_ptr<float>(), dac.data_ptr<float>(), cur_stream()),
+        "w2w_activate_backward");
+  return std::make_tuple(dlogit, dsvec, dq, ddc, dac);
+}
+
 Tensor scan_u32(const Tensor& x, bool exclusive) {
   TORCH_CHECK(x.is_cuda() && x.scalar_type() == torch::kInt32, "x must be a CUDA int32 tensor (raw u32 bits)");
   c10::cuda::CUDAGuard guard(x.device());
@@ -305,6 +351,8 @@ PYBIND11_MODULE(TORCH_EXTENSION_NAME, m) {
         py::arg("grad_mode") = 0);
   m.def("sort_pairs_u64", &sort_pairs_u64);
   m.def("scan_u32", &scan_u32);
+  m.def("activate", &activate);
+  m.def("activate_backward", &activate_backward);
   m.def("tile_ranges", &tile_ranges);
   m.def("blend", &blend, py::arg("geomBuffer"), py::arg("P"), py::arg("ranges"), py::arg("point_list"),
         py::arg("image_height"), py::arg("image_width"), py::arg("background") = py::none());

@@ -447,6 +447,34 @@ int w2w_scan_u32_noalloc(const uint32_t* in, uint32_t* out, long long n, int exc
   return check_launch();
 }
 
+int w2w_activate_forward(long long P, int K, const float* opacity_logit, const float* svec, const float* quaternion,
+                         const float* sh_dc, const float* sh_ac, float* opacity, float* scales, float* rotations,
+                         float* shs, w2w_stream_t stream) {
+  if (P < 0 || K < 0) return W2W_ERR_INVALID;
+  if (P == 0) return W2W_OK;
+  if (!opacity_logit || !svec || !quaternion || !sh_dc || (K > 0 && !sh_ac) || !opacity || !scales ||
+      !rotations || !shs)
+    return W2W_ERR_INVALID;
+  ActivateArgs a{P, K, opacity_logit, svec, quaternion, sh_dc, sh_ac, opacity, scales, rotations, shs};
+  launch_activate(a, S(stream));
+  return check_launch();
+}
+
+int w2w_activate_backward(long long P, int K, const float* g_opacity, const float* g_scales,
+                          const float* g_rotations, const float* g_shs, const float* opacity, const float* scales,
+                          const float* quaternion, float* d_opacity_logit, float* d_svec, float* d_quaternion,
+                          float* d_sh_dc, float* d_sh_ac, w2w_stream_t stream) {
+  if (P < 0 || K < 0) return W2W_ERR_INVALID;
+  if (P == 0) return W2W_OK;
+  if (!g_opacity || !g_scales || !g_rotations || !g_shs || !opacity || !scales || !quaternion ||
+      !d_opacity_logit || !d_svec || !d_quaternion || !d_sh_dc || (K > 0 && !d_sh_ac))
+    return W2W_ERR_INVALID;
+  ActivateBackwardArgs a{P, K, g_opacity, g_scales, g_rotations, g_shs, opacity, scales, quaternion,
+                         d_opacity_logit, d_svec, d_quaternion, d_sh_dc, d_sh_ac};
+  launch_activate_backward(a, S(stream));
+  return check_launch();
+}
+
 int w2w_tile_ranges(const uint64_t* sorted_keys, long long n, int tile_shift, uint32_t* ranges, int ntiles,
                     w2w_stream_t stream) {
   if (n < 0 || ntiles <= 0 || !ranges || (n > 0 && !sorted_keys) || tile_shift < 0 || tile_shift > 63)

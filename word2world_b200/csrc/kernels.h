@@ -208,6 +208,23 @@ enum Stage {
 void stage_begin(int stage, cudaStream_t s);
 void stage_end(int stage, cudaStream_t s, int kernels);
 
+// Activation preamble of Renderer.render (activate.cu).
+struct ActivateArgs {
+  long long P;
+  int K;  // rest SH coefficients per Gaussian (sh_ac is [P, K, 3])
+  const float *opacity_logit, *svec, *quat, *sh_dc, *sh_ac;
+  float *opacity, *scales, *rotations, *shs;
+};
+struct ActivateBackwardArgs {
+  long long P;
+  int K;
+  const float *g_opacity, *g_scales, *g_rotations, *g_shs;  // gradients of the activated tensors
+  const float *opacity, *scales, *quat;                      // activated opacity and scales, raw quaternion
+  float *d_opacity_logit, *d_svec, *d_quat, *d_sh_dc, *d_sh_ac;
+};
+void launch_activate(const ActivateArgs& a, cudaStream_t stream);
+void launch_activate_backward(const ActivateBackwardArgs& a, cudaStream_t stream);
+
 size_t scan_status_words(long long n);
 size_t scan_scratch_bytes(long long n);
 void launch_scan(const uint32_t* in, uint32_t* out, long long n, int exclusive, void* scratch, cudaStream_t stream);

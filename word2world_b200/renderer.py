@@ -90,6 +90,35 @@ def _render_gaussians_inline(means3D, means2D, shs, colors_precomp, opacity, sca
                                      GRAD_MODES[grad_mode], bool(compat_spill))
 
 
+class _Activate(torch.autograd.Function):
+    """The activation preamble of ``Renderer.render`` (``Renderer.py:164-167``:
+    sigmoid opacity, exp scales, normalised quaternion, concatenated SH) as
+    one fused kernel each way; the forward is bit-identical to the torch
+    operations the reference runs."""
+
+    @staticmethod
+    def forward(ctx, opacity_logit, svec, quaternion, sh_dc, sh_ac):
+        opacity, scales, rotations, shs = _C.activate(opacity_logit, svec, quaternion, sh_dc, sh_ac)
+        ctx.save_for_backward(opacity, scales, quaternion)
+        ctx.rows = shs.shape[1]
+        return opacity, scales, rotations, shs
+
+    @staticmethod
+    def backward(ctx, g_opacity, g_scales, g_rotations, g_shs):
+        opacity, scales, quaternion = ctx.saved_tensors
+        z = lambda g, like: torch.zeros_like(like) if g is None else g
+        P = opacity.shape[0]
+        d_logit, d_svec, d_quat, d_dc, d_ac = _C.activate_backward(
+            z(g_opacity, opacity), z(g_scales, scales), z(g_rotations, quaternion),
+            z(g_shs, torch.empty(P, ctx.rows, 3, device=opacity.device)), opacity, scales, quaternion)
+        return d_logit, d_svec, d_quat, d_dc, d_ac
+
+
+def activate(opacity_logit, svec, quaternion, sh_dc, sh_ac):
+    """(opacity, scales, rotations, shs) from the raw parameters, differentiable."""
+    return _Activate.apply(opacity_logit, svec, quaternion, sh_dc, sh_ac)
+
+
 @dataclass
 class GaussianParams:
     """Raw per-Gaussian parameters as structure-of-arrays tensors (the
@@ -133,11 +162,9 @@ class Renderer:
         accum_grads.retain_grad()
         tanfovx = math.tan(float(FoVx) * 0.5)
         tanfovy = math.tan(float(FoVy) * 0.5)
-        # activation preamble (Renderer.py:164-167)
-        activated_opacity = torch.sigmoid(p.opacity)
-        activated_scales = torch.exp(p.svec)
-        rotations = torch.nn.functional.normalize(p.quaternion)
-        shs = torch.cat((p.sh_dc, p.sh_ac), dim=1)
+        # activation preamble (Renderer.py:164-167), one fused kernel each way
+        activated_opacity, activated_scales, rotations, shs = activate(p.opacity, p.svec, p.quaternion, p.sh_dc,
+                                                                       p.sh_ac)
         bg = torch.ones(3, dtype=torch.float32, device=p.mean.device)
         image, radii, _, _ = _render_gaussians_inline(
             p.mean, accum_grads, shs, None, activated_opacity, activated_scales, rotations, None, bg, 1,
