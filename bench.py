@@ -284,13 +284,29 @@ def run_e2e(a, sc, cams, device, world):
     h2d = sum(g.numel() * 4 for g in host_g) + sum(sum(x.numel() * 4 for x in c) for c in host_c)
     loss_host = torch.empty(a.views, dtype=torch.float32).pin_memory()
 
+    # the step's inputs are copied on a side stream, all views' at the step's
+    # start, so that view v's copy overlaps the rendering of views < v
+    copy_stream = torch.cuda.Stream(device=device)
+    main_stream = torch.cuda.current_stream(device)
+
     def step():
         for p_ in params.parameters():
             p_.grad = None
+        copy_stream.wait_stream(main_stream)  # the previous step is done with the buffers
+        staged = []
+        with torch.cuda.stream(copy_stream):
+            for v in range(len(cams)):
+                g = host_g[v].to(device, non_blocking=True)
+                VPC = tuple(x.to(device, non_blocking=True) for x in host_c[v])
+                ev = torch.cuda.Event()
+                ev.record(copy_stream)
+                staged.append((g, VPC, ev))
         losses = []
         for v, c in enumerate(cams):
-            g = host_g[v].to(device, non_blocking=True)
-            V, Pm, C = (x.to(device, non_blocking=True) for x in host_c[v])
+            g, (V, Pm, C), ev = staged[v]
+            main_stream.wait_event(ev)
+            for x in (g, V, Pm, C):
+                x.record_stream(main_stream)
             out = r.render(c.fovx, c.fovy, V, Pm, C, a.res, a.res)
             loss = (out["image"] * g).sum()
             loss.backward()
@@ -569,7 +585,10 @@ def run_sortscan(a):
                          "l2": "512 MB write between timed calls"},
               "roofline": {"bound": "hbm", "achieved": round(sort_gbs, 1), "peak": peak, "unit": "GB/s",
                            "frac": round(sort_gbs / peak, 4), "peak_source": src,
-                           "bytes_per_key": pass_bytes, "traffic": None},
+                           "bytes_per_key": pass_bytes,
+                           # DRAM bytes of one sort call (histogram + 5 passes), one ncu capture of this
+                           # workload (profiles/sort_scan_20M_2M.md); algorithmic: 128 B x 20M = 2.56 GB
+                           "traffic": 2.35e9, "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum"},
               "sort": {"ms": round(ms_sort, 4), "ms_all": [round(x, 4) for x in all_sort],
                        "gkeys_per_s": round(n_sort / (ms_sort * 1e-3) / 1e9, 3),
                        "pass_traffic_gbs": round(sort_gbs, 1), "pass_traffic_frac": round(sort_gbs / peak, 4),
