@@ -179,6 +179,29 @@ int w2w_activate_backward(long long P, int K, const float* g_opacity, const floa
                           const float* quaternion, float* d_opacity_logit, float* d_svec, float* d_quaternion,
                           float* d_sh_dc, float* d_sh_ac, w2w_stream_t stream);
 
+/* Voxel occupancy field for mesh extraction (compute_voxel_field.cu:25-124):
+ * occ[i + R (j + R k)] = sum over the Gaussians whose mean lies in voxel
+ * (i, j, k)'s block (B^3 blocks over [-1, 1]^3, grown by relax_ratio block
+ * sides) of opacity * exp(-1/2 d^T Sigma^-1 d), Sigma given by its upper
+ * triangle (xx, xy, xz, yy, yz, zz).  Each Gaussian is binned once into the
+ * blocks that hold its mean instead of being tested by every voxel.
+ * w2w_voxel_field takes device pointers and enqueues on `stream` (its
+ * temporaries come from the stream-ordered allocator; it synchronises the
+ * stream once, to size them); w2w_compute_voxel_field is the reference's
+ * entry point (compute_voxel_field_cuda), with host pointers.  2 <= R <= 2048,
+ * 1 <= B <= 1000, 0 <= relax_ratio <= 64; non-finite means are not supported. */
+int w2w_voxel_field(const float* means, const float* covs, const float* opacities, int n, int resolution,
+                    int num_blocks, float relax_ratio, float* occ, w2w_stream_t stream);
+int w2w_compute_voxel_field(float* h_occ, const float* h_means, const float* h_covs, const float* h_opacities,
+                            int n, int resolution, int num_blocks, float relax_ratio);
+
+/* Densification statistics of the training loop (gaussians_handler.py:116-118):
+ * for every Gaussian with radii[i] > 0, counter[i] += 1 and accum[i] +=
+ * |dL/dmean2D[i, 0:2]| (dL_dmeans2D [P,3], accum and counter [P], updated in
+ * place), in one pass and without a host synchronisation. */
+int w2w_densification_stats(long long P, const float* dL_dmeans2D, const int* radii, float* accum, float* counter,
+                            w2w_stream_t stream);
+
 /* Per-tile [start, end) from sorted keys whose tile id is key >> tile_shift
  * (gaussianTiles.cu:6-33); tiles without entries get (0, 0). */
 int w2w_tile_ranges(const uint64_t* sorted_keys, long long n, int tile_shift, uint32_t* ranges,

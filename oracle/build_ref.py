@@ -54,11 +54,31 @@ def so_path():
     return os.path.join(OUT, MODULE_NAME + ".so")
 
 
+VOXEL_SO = os.path.join(OUT, "compute_voxel_field.so")
+
+
+def build_voxel(ref_root="/root/reference"):
+    """The reference's voxel-field kernel (``compute_voxel_field.cu``) as a
+    shared library exporting ``compute_voxel_field_cuda``, compiled from its
+    one source file where it lies.  The source marks the export with the
+    Windows-only ``__declspec(dllexport)``; the command line defines that away."""
+    import subprocess
+    src = os.path.join(ref_root, "compute_voxel_field.cu")
+    if not os.path.exists(src):
+        raise FileNotFoundError(src)
+    os.makedirs(OUT, exist_ok=True)
+    nvcc = os.path.join(os.environ.get("CUDA_HOME", "/usr/local/cuda"), "bin", "nvcc")
+    subprocess.run([nvcc, "-O3", "-shared", "-Xcompiler", "-fPIC", "-gencode", "arch=compute_100a,code=sm_100a",
+                    "-D__declspec(x)=", src, "-o", VOXEL_SO], check=True)
+    return VOXEL_SO
+
+
 if __name__ == "__main__":
     ap = argparse.ArgumentParser()
     ap.add_argument("--ref-root", default="/root/reference")
     ap.add_argument("-v", action="store_true")
     a = ap.parse_args()
     build(a.ref_root, a.v)
-    print(so_path(), os.path.exists(so_path()))
+    build_voxel(a.ref_root)
+    print(so_path(), os.path.exists(so_path()), VOXEL_SO, os.path.exists(VOXEL_SO))
     sys.exit(0)

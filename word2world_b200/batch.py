@@ -83,6 +83,17 @@ class Scene:
         return int(self.means3D.shape[0])
 
     @classmethod
+    def from_ply(cls, path, device="cuda", sh_degree: int = 3) -> "Scene":
+        """A resident scene from a PLY file in the reference's layout
+        (``ply.save_ply``), activated as ``Renderer.render`` activates."""
+        from .ply import load_ply
+        d = load_ply(path)
+        t = lambda a: torch.from_numpy(np.ascontiguousarray(a, dtype=np.float32)).to(device)
+        opac, scales, rots, shs = _C.activate(t(d["opacity"]), t(d["svec"]), t(d["quaternion"]), t(d["sh_dc"]),
+                                              t(d["sh_ac"]))
+        return cls(t(d["mean"]), opac, scales, rots, shs, sh_degree)
+
+    @classmethod
     def from_arrays(cls, arrays, device, sh_degree: int = 3) -> "Scene":
         m, o, s, q, sh = arrays
         t = lambda a: torch.from_numpy(np.ascontiguousarray(a, dtype=np.float32)).to(device)

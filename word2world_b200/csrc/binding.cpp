@@ -264,6 +264,42 @@ std::tuple<Tensor, Tensor, Tensor, Tensor, Tensor> activate_backward(const Tenso
   return std::make_tuple(dlogit, dsvec, dq, ddc, dac);
 }
 
+// gaussians_handler.collect_densification_info (gaussians_handler.py:116-118), fused.
+void densification_stats(const Tensor& dL_dmeans2D, const Tensor& radii, Tensor& accum, Tensor& counter) {
+  const auto dev = dL_dmeans2D.device();
+  c10::cuda::CUDAGuard guard(dev);
+  Tensor g = f32(dL_dmeans2D, "dL_dmeans2D", dev);
+  TORCH_CHECK(radii.is_cuda() && radii.device() == dev && radii.scalar_type() == torch::kInt32,
+              "radii must be an int32 CUDA tensor on the gradient's device");
+  Tensor r = radii.contiguous();
+  const int64_t P = r.numel();
+  TORCH_CHECK(g.numel() == 3 * P, "dL_dmeans2D must be [P,3]");
+  for (const Tensor* t : {&accum, &counter}) {
+    TORCH_CHECK(t->is_cuda() && t->device() == dev && t->scalar_type() == torch::kFloat32 && t->is_contiguous() &&
+                    t->numel() == P, "accum and counter must be contiguous float32 [P] or [P,1] on the same device");
+  }
+  check(w2w_densification_stats(P, g.data_ptr<float>(), r.data_ptr<int>(), accum.data_ptr<float>(),
+                                counter.data_ptr<float>(), cur_stream()),
+        "w2w_densification_stats");
+}
+
+// Voxel occupancy field (compute_voxel_field.cu:25-124): [R, R, R], x fastest
+// in memory, as the reference wrapper reshapes it (compute_voxel_field_wrapper.py:101).
+Tensor voxel_field(const Tensor& means, const Tensor& covs, const Tensor& opacities, int64_t resolution,
+                   int64_t num_blocks, double relax_ratio) {
+  const auto dev = means.device();
+  c10::cuda::CUDAGuard guard(dev);
+  Tensor m = f32(means, "means", dev), c = f32(covs, "covs", dev), o = f32(opacities, "opacities", dev);
+  const int64_t n = m.numel() / 3;
+  TORCH_CHECK(m.numel() == 3 * n && c.numel() == 6 * n && o.numel() == n,
+              "means [N,3], covs [N,6] (xx, xy, xz, yy, yz, zz), opacities [N] expected");
+  Tensor occ = torch::empty({resolution, resolution, resolution}, m.options());
+  check(w2w_voxel_field(m.data_ptr<float>(), c.data_ptr<float>(), o.data_ptr<float>(), int(n), int(resolution),
+                        int(num_blocks), float(relax_ratio), occ.data_ptr<float>(), cur_stream()),
+        "w2w_voxel_field");
+  return occ;
+}
+
 Tensor scan_u32(const Tensor& x, bool exclusive) {
   TORCH_CHECK(x.is_cuda() && x.scalar_type() == torch::kInt32, "x must be a CUDA int32 tensor (raw u32 bits)");
   c10::cuda::CUDAGuard guard(x.device());
@@ -352,6 +388,8 @@ PYBIND11_MODULE(TORCH_EXTENSION_NAME, m) {
   m.def("sort_pairs_u64", &sort_pairs_u64);
   m.def("scan_u32", &scan_u32);
   m.def("activate", &activate);
+  m.def("densification_stats", &densification_stats);
+  m.def("voxel_field", &voxel_field);
   m.def("activate_backward", &activate_backward);
   m.def("tile_ranges", &tile_ranges);
   m.def("blend", &blend, py::arg("geomBuffer"), py::arg("P"), py::arg("ranges"), py::arg("point_list"),

@@ -475,6 +475,123 @@ int w2w_activate_backward(long long P, int K, const float* g_opacity, const floa
   return check_launch();
 }
 
+int w2w_voxel_field(const float* means, const float* covs, const float* opacities, int n, int resolution,
+                    int num_blocks, float relax_ratio, float* occ, w2w_stream_t stream) {
+  if (n < 0 || resolution < 2 || resolution > 2048 || num_blocks < 1 || num_blocks > 1000 ||
+      !(relax_ratio >= 0.0f && relax_ratio <= 64.0f) || !occ)
+    return W2W_ERR_INVALID;
+  if (n > 0 && (!means || !covs || !opacities)) return W2W_ERR_INVALID;
+  cudaStream_t st = S(stream);
+  const size_t voxels = size_t(resolution) * resolution * resolution;
+  if (n == 0) {
+    cudaMemsetAsync(occ, 0, voxels * 4, st);
+    return check_launch();
+  }
+  const int nb = num_blocks + 1;  // the last voxel of an axis falls in block num_blocks
+  const int nblocks = nb * nb * nb;
+  std::vector<void*> bufs;
+  auto alloc = [&](size_t bytes) -> void* {
+    void* p = nullptr;
+    if (cudaMallocAsync(&p, bytes > 0 ? bytes : 1, st) != cudaSuccess) return nullptr;
+    bufs.push_back(p);
+    return p;
+  };
+  auto release = [&]() {
+    for (void* p : bufs) cudaFreeAsync(p, st);
+    bufs.clear();
+  };
+  VoxelArgs a{};
+  a.P = n; a.R = resolution; a.B = num_blocks;
+  a.bs = 2.0f / float(num_blocks);
+  a.relax = relax_ratio;
+  a.means = means; a.covs = covs; a.opacities = opacities; a.occ = occ;
+  a.rec = static_cast<float4*>(alloc(size_t(n) * 48));
+  a.count = static_cast<uint32_t*>(alloc(size_t(n) * 4));
+  uint32_t* offsets = static_cast<uint32_t*>(alloc(size_t(n) * 4));
+  void* scan_scratch = alloc(scan_scratch_bytes(n));
+  if (!a.rec || !a.count || !offsets || !scan_scratch) { release(); return W2W_ERR_CUDA; }
+  a.offsets = offsets;
+  launch_voxel_prepare(a, st);
+  launch_scan(a.count, offsets, n, 1, scan_scratch, st);
+  uint32_t tail[2] = {0, 0};
+  cudaMemcpyAsync(&tail[0], offsets + (n - 1), 4, cudaMemcpyDeviceToHost, st);
+  cudaMemcpyAsync(&tail[1], a.count + (n - 1), 4, cudaMemcpyDeviceToHost, st);
+  if (cudaStreamSynchronize(st) != cudaSuccess) { release(); return check_launch(); }
+  const long long pairs = (long long)tail[0] + tail[1];
+  if (pairs >= (1LL << 30)) { release(); return W2W_ERR_CAPACITY; }
+  if (pairs == 0) {
+    cudaMemsetAsync(occ, 0, voxels * 4, st);
+    release();
+    return check_launch();
+  }
+  a.keys = static_cast<uint32_t*>(alloc(size_t(pairs) * 4));
+  a.vals = static_cast<uint32_t*>(alloc(size_t(pairs) * 4));
+  uint32_t* keys_out = static_cast<uint32_t*>(alloc(size_t(pairs) * 4));
+  uint32_t* vals_out = static_cast<uint32_t*>(alloc(size_t(pairs) * 4));
+  size_t kt, vt, hi, stt, ct, er;
+  const size_t sbytes = sort_scratch_layout(pairs, &kt, &vt, &hi, &stt, &ct, &er);
+  void* sort_scratch = alloc(sbytes);
+  uint32_t* tile_hist = static_cast<uint32_t*>(alloc(size_t(nblocks) * 4));
+  uint2* ranges = static_cast<uint2*>(alloc(size_t(nblocks) * 8));
+  if (!a.keys || !a.vals || !keys_out || !vals_out || !sort_scratch || !tile_hist || !ranges) {
+    release();
+    return W2W_ERR_CUDA;
+  }
+  launch_voxel_emit(a, st);
+  cudaMemsetAsync(at<uint32_t>(sort_scratch, er), 0, 4, st);
+  SortArgs so{};
+  so.n = pairs; so.key64 = 0; so.begin_bit = 0; so.bits = ceil_log2(uint32_t(nblocks));
+  so.keys_in = a.keys; so.vals_in = a.vals; so.keys_out = keys_out; so.vals_out = vals_out;
+  so.keys_tmp = at<void>(sort_scratch, kt); so.vals_tmp = at<uint32_t>(sort_scratch, vt);
+  so.hist = at<uint32_t>(sort_scratch, hi); so.status = at<uint32_t>(sort_scratch, stt);
+  so.counters = at<uint32_t>(sort_scratch, ct); so.error = at<uint32_t>(sort_scratch, er);
+  so.tile_shift = 0; so.num_tiles = nblocks; so.tile_hist = tile_hist; so.ranges = ranges;
+  launch_sort(so, st);
+  launch_voxel_field(a, vals_out, ranges, st);
+  uint32_t err = 0;
+  cudaMemcpyAsync(&err, so.error, 4, cudaMemcpyDeviceToHost, st);
+  const cudaError_t se = cudaStreamSynchronize(st);
+  release();
+  if (se != cudaSuccess) return check_launch();
+  if (err & kErrTimeout) return W2W_ERR_TIMEOUT;
+  if (err) return W2W_ERR_CAPACITY;
+  return check_launch();
+}
+
+int w2w_compute_voxel_field(float* h_occ, const float* h_means, const float* h_covs, const float* h_opacities,
+                            int n, int resolution, int num_blocks, float relax_ratio) {
+  if (!h_occ || n < 0 || resolution < 2 || resolution > 2048 || (n > 0 && (!h_means || !h_covs || !h_opacities)))
+    return W2W_ERR_INVALID;
+  const size_t voxels = size_t(resolution) * resolution * resolution;
+  float *d_occ = nullptr, *d_in = nullptr;
+  if (cudaMalloc(&d_occ, voxels * 4) != cudaSuccess) return W2W_ERR_CUDA;
+  const size_t nn = size_t(n);
+  if (cudaMalloc(&d_in, (nn * 10 > 0 ? nn * 10 : 1) * 4) != cudaSuccess) {
+    cudaFree(d_occ);
+    return W2W_ERR_CUDA;
+  }
+  if (n > 0) {
+    cudaMemcpy(d_in, h_means, nn * 12, cudaMemcpyHostToDevice);
+    cudaMemcpy(d_in + 3 * nn, h_covs, nn * 24, cudaMemcpyHostToDevice);
+    cudaMemcpy(d_in + 9 * nn, h_opacities, nn * 4, cudaMemcpyHostToDevice);
+  }
+  int rc = w2w_voxel_field(d_in, d_in + 3 * nn, d_in + 9 * nn, n, resolution, num_blocks, relax_ratio, d_occ,
+                           nullptr);
+  if (rc == W2W_OK && cudaMemcpy(h_occ, d_occ, voxels * 4, cudaMemcpyDeviceToHost) != cudaSuccess) rc = W2W_ERR_CUDA;
+  cudaFree(d_occ);
+  cudaFree(d_in);
+  return rc;
+}
+
+int w2w_densification_stats(long long P, const float* dL_dmeans2D, const int* radii, float* accum, float* counter,
+                            w2w_stream_t stream) {
+  if (P < 0) return W2W_ERR_INVALID;
+  if (P == 0) return W2W_OK;
+  if (!dL_dmeans2D || !radii || !accum || !counter) return W2W_ERR_INVALID;
+  launch_densify_stats(P, dL_dmeans2D, radii, accum, counter, S(stream));
+  return check_launch();
+}
+
 int w2w_tile_ranges(const uint64_t* sorted_keys, long long n, int tile_shift, uint32_t* ranges, int ntiles,
                     w2w_stream_t stream) {
   if (n < 0 || ntiles <= 0 || !ranges || (n > 0 && !sorted_keys) || tile_shift < 0 || tile_shift > 63)

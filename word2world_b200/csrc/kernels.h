@@ -224,6 +224,24 @@ struct ActivateBackwardArgs {
 };
 void launch_activate(const ActivateArgs& a, cudaStream_t stream);
 void launch_activate_backward(const ActivateBackwardArgs& a, cudaStream_t stream);
+// Voxel occupancy field (voxel.cu).
+struct VoxelArgs {
+  int P, R, B;
+  float bs, relax;  // block side 2 / B, growth of each block per side in block sides
+  const float *means, *covs, *opacities;
+  float4* rec;        // [3P] per Gaussian: mean + opacity, inverse covariance
+  uint32_t* count;    // [P] blocks each Gaussian is binned into
+  const uint32_t* offsets;  // [P] exclusive scan of count
+  uint32_t* keys;     // [pairs] block ids
+  uint32_t* vals;     // [pairs] Gaussian ids
+  float* occ;         // [R^3], x fastest
+};
+void launch_voxel_prepare(const VoxelArgs& a, cudaStream_t stream);
+void launch_voxel_emit(const VoxelArgs& a, cudaStream_t stream);
+void launch_voxel_field(const VoxelArgs& a, const uint32_t* list, const uint2* ranges, cudaStream_t stream);
+// Densification statistics (densify.cu).
+void launch_densify_stats(long long P, const float* dL_dmeans2D, const int* radii, float* accum, float* counter,
+                          cudaStream_t stream);
 
 size_t scan_status_words(long long n);
 size_t scan_scratch_bytes(long long n);

@@ -140,6 +140,39 @@ class GaussianParams:
     def parameters(self):
         return [self.mean, self.sh_dc, self.sh_ac, self.opacity, self.svec, self.quaternion]
 
+    def save_ply(self, path):
+        """The reference's PLY layout (``GaussianIO.save_as_ply``)."""
+        from .ply import save_ply
+        save_ply(path, self.mean, self.sh_dc, self.sh_ac, self.opacity, self.svec, self.quaternion)
+
+    @staticmethod
+    def load_ply(path, device="cuda", requires_grad=True):
+        from .ply import load_ply
+        d = load_ply(path)
+        t = lambda a: torch.tensor(a, device=device, dtype=torch.float32).requires_grad_(requires_grad)
+        return GaussianParams(t(d["mean"]), t(d["sh_dc"]), t(d["sh_ac"]), t(d["opacity"]), t(d["svec"]),
+                              t(d["quaternion"]))
+
+
+class DensificationStats:
+    """The training loop's densification statistics
+    (``gaussians_handler.collect_densification_info``,
+    ``gaussians_handler.py:116-118``): per Gaussian, the number of renders in
+    which it was visible and the sum of its screen-space gradient norms.
+    ``collect`` updates both in one fused pass, with no host synchronisation
+    (the reference indexes with a boolean mask)."""
+
+    def __init__(self, P: int, device="cuda"):
+        self.mean_gradient_accum = torch.zeros((P, 1), dtype=torch.float32, device=device)
+        self.counter = torch.zeros((P, 1), dtype=torch.float32, device=device)
+
+    def collect(self, viewspace_point_tensor, radii):
+        """``viewspace_point_tensor``: the render's ``accum_grads`` (its
+        ``.grad`` is read) or that gradient itself; ``radii``: the render's
+        radii (visible = radius > 0, the reference's ``avaialble_pts``)."""
+        g = viewspace_point_tensor.grad if viewspace_point_tensor.grad is not None else viewspace_point_tensor
+        _C.densification_stats(g.detach(), radii.to(torch.int32), self.mean_gradient_accum, self.counter)
+
 
 class Renderer:
     """``Renderer.render`` (``Renderer.py:119-192``) over ``GaussianParams``.
