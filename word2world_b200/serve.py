@@ -144,7 +144,9 @@ class Server:
         return dict(batches=batches, wall=now())
 
     def serve_plain(self, requests, realtime: bool = True):
-        """Baseline: one single-view call per view, one request at a time, FIFO."""
+        """Baseline: one single-view call per view, one request at a time,
+        FIFO; each request's gradients are summed over its views, as the
+        batched loop returns them."""
         from . import _C
         pending = sorted(requests, key=lambda r: r.arrival)
         dev = self.renderer.device
@@ -158,6 +160,7 @@ class Server:
                 time.sleep(r.arrival - now())
             r.start = now()
             sc = self.scenes[r.scene]
+            sums = None
             for c, g in zip(r.cameras, r.grads):
                 tt = lambda a: torch.from_numpy(np.ascontiguousarray(a, dtype=np.float32)).to(dev)
                 V, Pm, C = tt(c.viewmatrix), tt(c.projmatrix), tt(c.campos)
@@ -165,9 +168,17 @@ class Server:
                     sc.shs, c.focal_y, sc.scales, sc.means3D, Pm, sc.sh_degree, sc.opacities, sc.rotations, C, V,
                     c.focal_x, c.height, c.width, bg, True)
                 z = torch.zeros(1, c.height, c.width, device=dev)
-                _C.rasterize_gaussians_backward(bg, sc.means3D, radii, empty, sc.scales, sc.rotations, 1.0, empty,
-                                                V, Pm, c.tanfovx, c.tanfovy, g, z, z, sc.shs, sc.sh_degree, C, geom,
-                                                R, binb, img, alpha, False, gm)
+                out = _C.rasterize_gaussians_backward(bg, sc.means3D, radii, empty, sc.scales, sc.rotations, 1.0,
+                                                      empty, V, Pm, c.tanfovx, c.tanfovy, g, z, z, sc.shs,
+                                                      sc.sh_degree, C, geom, R, binb, img, alpha, False, gm)
+                grads = (out[3], out[2], out[6], out[7], out[5])  # means3D, opacities, scales, rotations, shs
+                if sums is None:
+                    sums = list(grads)
+                else:
+                    for acc, gr in zip(sums, grads):
+                        acc.add_(gr)
+            if self.keep:
+                r.scene_grads = dict(zip(("means3D", "opacities", "scales", "rotations", "shs"), sums))
             torch.cuda.synchronize()
             r.done = now()
         return dict(wall=now())
