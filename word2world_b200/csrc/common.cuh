@@ -317,8 +317,7 @@ struct BinHeader {
 };
 
 constexpr int kSortThreads = 256;
-constexpr int kSortItems = 16;
-constexpr int kSortTile = kSortThreads * kSortItems;  // 4096 keys per onesweep tile
+constexpr int kSortTileMin = 4096;  // smallest onesweep tile of any key type: status words are sized for it
 constexpr int kMaxPasses = 8;
 constexpr int kMaxDigitBits = 9;             // digit width: ceil(bits / ceil(bits / 9))
 constexpr int kMaxBins = 1 << kMaxDigitBits;
@@ -329,7 +328,7 @@ struct BinLayout {
     size_t o = 0;
     auto take = [&](size_t bytes) { size_t a = align256(o); o = a + bytes; return a; };
     const size_t r = size_t(R > 0 ? R : 1);
-    const size_t sort_tiles = (r + kSortTile - 1) / kSortTile;
+    const size_t sort_tiles = (r + kSortTileMin - 1) / kSortTileMin;
     header = take(sizeof(BinHeader));
     keysA = take(r * 8);
     keysB = take(r * 8);
