@@ -63,9 +63,18 @@ struct BlendPixel {
   }
 };
 
-__global__ void __launch_bounds__(kBlendThreads, 2) blend_kernel(BlendArgs a) {
-  __shared__ TileWalkShared sm;
-  const int tile = int(a.order[blockIdx.x]);
+// Warps per CTA: 8 (one CTA per tile) or 4 (two CTAs per tile, upper and
+// lower eight rows; see tile_walk.cuh).
+constexpr int kBlendWarps = 4;
+constexpr int kBlendParts = 8 / kBlendWarps;  // CTAs per tile
+constexpr int kBlendCta = 32 * kBlendWarps;
+constexpr int kStagePer = kBatch / kBlendCta;  // entries each thread stages per batch
+static_assert(kBatch % kBlendCta == 0, "whole entries per thread");
+
+__global__ void __launch_bounds__(kBlendCta, 16 / kBlendWarps) blend_kernel(BlendArgs a) {
+  __shared__ TileWalkShared<kBlendWarps> sm;
+  const int part = int(blockIdx.x) % kBlendParts;
+  const int tile = int(a.order[blockIdx.x / kBlendParts]);
   // this tile's image: the call's, or its batch item's
   int W = a.W, H = a.H, ltile = tile;
   size_t pbase = 0;
@@ -79,7 +88,8 @@ __global__ void __launch_bounds__(kBlendThreads, 2) blend_kernel(BlendArgs a) {
     bg = it.bg;
   }
   const int gw = (W + kTile - 1) / kTile;
-  const TilePixel tp(ltile, gw);
+  const int warp = int(threadIdx.x >> 5), first_block = part * kBlendWarps;
+  const TilePixel tp(ltile, gw, first_block + warp);
   const bool inside = tp.px < W && tp.py < H;
   const uint2 range = a.ranges[tile];
   const int n = int(range.y - range.x);
@@ -88,22 +98,33 @@ __global__ void __launch_bounds__(kBlendThreads, 2) blend_kernel(BlendArgs a) {
   BlendPixel pix;
   pix.done = !inside;
   const int nb = (n + kBatch - 1) / kBatch;
-  Staged st;
+  Staged st[kStagePer];
+  auto load = [&](int base) {
+#pragma unroll
+    for (int r = 0; r < kStagePer; ++r) {
+      const int e = base + r * kBlendCta + int(threadIdx.x);
+      stage_load(st[r], a.record, a.point_list, range.x + e, e < n);
+    }
+  };
+  auto store = [&](int buf) {
+#pragma unroll
+    for (int r = 0; r < kStagePer; ++r)
+      stage_store(sm, buf, st[r], r * kBlendCta + int(threadIdx.x), tp.X0, tp.Y0, first_block);
+  };
   if (nb > 0) {
-    stage_load(st, a.record, a.point_list, range.x + threadIdx.x, int(threadIdx.x) < n);
-    stage_store(sm, 0, st, tp.X0, tp.Y0);
+    load(0);
+    store(0);
   }
   for (int b = 0; b < nb; ++b) {
     const int cur = b & 1;
     // barrier: batch b is staged; every warp has finished batch b-1
-    if (__syncthreads_count(pix.done ? 1 : 0) == kBlendThreads) break;
+    if (__syncthreads_count(pix.done ? 1 : 0) == kBlendCta) break;
     const int next_base = (b + 1) * kBatch;
-    if (b + 1 < nb) stage_load(st, a.record, a.point_list, range.x + next_base + threadIdx.x,
-                               next_base + int(threadIdx.x) < n);
+    if (b + 1 < nb) load(next_base);
     if (!__all_sync(0xffffffffu, pix.done)) {
       const float4* s = sm.rec[cur];
-      const int cnt = build_list(sm, cur, tp.warp, tp.lane);
-      const uint8_t* lst = sm.list[tp.warp];
+      const int cnt = build_list(sm, cur, warp, tp.lane);
+      const uint8_t* lst = sm.list[warp];
       const uint32_t base = uint32_t(b * kBatch) + 1u;
       for (int k0 = 0; k0 < cnt; k0 += kBlendIlp) {
         // kBlendIlp entries in flight: their Gaussian values are independent,
@@ -140,7 +161,7 @@ __global__ void __launch_bounds__(kBlendThreads, 2) blend_kernel(BlendArgs a) {
         if (__all_sync(0xffffffffu, pix.done)) break;
       }
     }
-    if (b + 1 < nb) stage_store(sm, cur ^ 1, st, tp.X0, tp.Y0);
+    if (b + 1 < nb) store(cur ^ 1);
   }
   if (inside) {
     const size_t q = size_t(tp.py) * W + tp.px;
@@ -154,15 +175,17 @@ __global__ void __launch_bounds__(kBlendThreads, 2) blend_kernel(BlendArgs a) {
     a.out_color[hw + cp] = fma(pix.T, bg[1], pix.C1);
     a.out_color[2 * hw + cp] = fma(pix.T, bg[2], pix.C2);
   }
-  // largest contributor count in the tile (the backward starts there)
-  __shared__ uint32_t s_max[kBlendThreads / 32];
+  // largest contributor count in the tile (the backward starts there); the
+  // tile's CTAs combine theirs (tile_max is cleared before the launch)
+  __shared__ uint32_t s_max[kBlendWarps];
   const uint32_t wm = __reduce_max_sync(0xffffffffu, pix.last);
-  if (tp.lane == 0) s_max[tp.warp] = wm;
+  if (tp.lane == 0) s_max[warp] = wm;
   __syncthreads();
   if (threadIdx.x == 0) {
-    uint32_t m = 0;
-    for (int w = 0; w < kBlendThreads / 32; ++w) m = max(m, s_max[w]);
-    a.tile_max[tile] = m;
+    uint32_t mx = 0;
+    for (int w = 0; w < kBlendWarps; ++w) mx = max(mx, s_max[w]);
+    if (kBlendParts == 1) a.tile_max[tile] = mx;
+    else atomicMax(&a.tile_max[tile], mx);
   }
 }
 
@@ -205,8 +228,9 @@ void launch_blend(const BlendArgs& a, cudaStream_t stream) {
   const int tiles = a.items ? a.total_tiles : ((a.W + kTile - 1) / kTile) * ((a.H + kTile - 1) / kTile);
   if (tiles <= 0) return;
   stage_begin(kStBlend, stream);
+  if (kBlendParts > 1) cudaMemsetAsync(a.tile_max, 0, sizeof(uint32_t) * size_t(tiles), stream);
   tile_order_kernel<<<1, 1024, 0, stream>>>(a.ranges, nullptr, tiles, a.order);
-  blend_kernel<<<tiles, kBlendThreads, 0, stream>>>(a);
+  blend_kernel<<<tiles * kBlendParts, kBlendCta, 0, stream>>>(a);
   // the backward's order: by the largest contributor count the blend just found
   tile_order_kernel<<<1, 1024, 0, stream>>>(nullptr, a.tile_max, tiles, a.order_bwd);
   stage_end(kStBlend, stream, 3);

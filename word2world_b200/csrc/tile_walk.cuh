@@ -103,28 +103,33 @@ __device__ __forceinline__ int pop_entry(uint32_t& bits) {
 }
 
 // ---------------------------------------------------------------------------
-// Cooperative batches (forward blend): the CTA stages kBatch entries at a time,
-// one per thread, double-buffered, with all 8 block bits computed once per
-// entry (block_mask); each warp expands its bits into an entry list
-// (build_list).  The blend walks far past most contributors (until every pixel
-// terminates), so sharing each entry's gather and test among the tile's warps
-// matters more there than letting warps run apart.
+// Cooperative batches (forward blend): the CTA stages kBatch entries at a time
+// (kBatch / blockDim.x per thread), double-buffered, with the block bits of the
+// CTA's kW warps computed once per entry (block_mask); each warp expands its
+// bits into an entry list (build_list).  The blend walks far past most
+// contributors (until every pixel terminates), so sharing each entry's gather
+// and test among warps matters more there than letting warps run apart.
+// kW = 8: one CTA per tile; kW = 4: two CTAs per tile (its upper and lower
+// eight rows), each staging the whole list, so that fewer warps wait at each
+// batch's barrier for the slowest of them.
 // ---------------------------------------------------------------------------
+template <int kW>
 struct TileWalkShared {
   float4 rec[2][kBatch * kRecVec];
   uint32_t id[2][kBatch];
-  uint32_t bal[2][8][8];  // [buffer][block][32-entry chunk]
-  uint8_t list[8][kBatch];  // per warp: its entries of the current batch, in order
+  uint32_t bal[2][kW][kBatch / 32];  // [buffer][warp's block][32-entry chunk]
+  uint8_t list[kW][kBatch];          // per warp: its entries of the current batch, in order
 };
 
-// Expand this warp's eight flag words into its entry list (in order); returns
-// the count.  Warp-collective.
-__device__ __forceinline__ int build_list(TileWalkShared& sm, int buf, int warp, int lane, int start = 0) {
+// Expand this warp's flag words into its entry list (in order); returns the
+// count.  Warp-collective.
+template <int kW>
+__device__ __forceinline__ int build_list(TileWalkShared<kW>& sm, int buf, int warp, int lane, int start = 0) {
   __syncwarp();  // the previous walk's reads of the list are done
   int count = 0;
   const uint32_t lt = (1u << lane) - 1u;
 #pragma unroll
-  for (int c = 0; c < 8; ++c) {
+  for (int c = 0; c < kBatch / 32; ++c) {
     uint32_t bits = sm.bal[buf][warp][c];
     const int lo = start - 32 * c;  // entries below `start` are dropped
     if (lo > 0) bits = lo >= 32 ? 0u : bits & (0xffffffffu << lo);
@@ -158,10 +163,14 @@ __device__ __forceinline__ void stage_load(Staged& st, const float* record, cons
   }
 }
 
-// Store the staged entry of thread j into buffer `buf` and publish the block
-// masks.  Every thread of the CTA must call this (the ballots are full-warp).
-__device__ __forceinline__ void stage_store(TileWalkShared& sm, int buf, const Staged& st, int X0, int Y0) {
-  const int j = threadIdx.x, lane = j & 31, chunk = j >> 5;
+// Store the staged entry j (slot j of the batch) into buffer `buf` and publish
+// the block masks of the CTA's kW blocks (the tile's blocks first_block ..
+// first_block + kW - 1).  Every thread of a warp must call this for the same
+// chunk (the ballots are full-warp).
+template <int kW>
+__device__ __forceinline__ void stage_store(TileWalkShared<kW>& sm, int buf, const Staged& st, int j, int X0, int Y0,
+                                            int first_block) {
+  const int lane = j & 31, chunk = j >> 5;
   uint32_t mask = 0;
   if (st.has) {
     float4* s = &sm.rec[buf][kRecVec * j];
@@ -169,15 +178,15 @@ __device__ __forceinline__ void stage_store(TileWalkShared& sm, int buf, const S
     s[1] = st.r1;
     s[2] = st.r2;
     sm.id[buf][j] = st.id;
-    mask = block_mask(st.r0.x, st.r0.y, st.r2.w, st.r3.x, st.r3.y, st.r3.z, st.r3.w, X0, Y0);
+    mask = block_mask(st.r0.x, st.r0.y, st.r2.w, st.r3.x, st.r3.y, st.r3.z, st.r3.w, X0, Y0) >> first_block;
   }
   uint32_t mine = 0;
 #pragma unroll
-  for (int b = 0; b < 8; ++b) {
+  for (int b = 0; b < kW; ++b) {
     const uint32_t w = __ballot_sync(0xffffffffu, (mask >> b) & 1u);
     if (lane == b) mine = w;
   }
-  if (lane < 8) sm.bal[buf][lane][chunk] = mine;
+  if (lane < kW) sm.bal[buf][lane][chunk] = mine;
 }
 
 }  // namespace w2w
