@@ -174,16 +174,18 @@ __device__ __forceinline__ float sqrt_approx(float x) {
 }
 
 // Bit b set: the Gaussian may reach alpha >= 1/255 in 8x4 block b of the tile
-// whose top-left pixel is (X0, Y0).  hy/beta/gamma/eps/vr as in CullParams.
+// whose top-left pixel is (X0, Y0) (kGroups rows of two blocks: the whole
+// 16x16 tile for kGroups = 4).  hy/beta/gamma/eps/vr as in CullParams.
+template <int kGroups = 4>
 __device__ __forceinline__ uint32_t block_mask(float mx, float my, float hy, float beta, float gamma, float eps,
                                                float vr, int X0, int Y0) {
-  if (!(hy >= 0.0f && hy < 1e30f)) return hy < 0.0f ? 0u : 0xffu;
+  if (!(hy >= 0.0f && hy < 1e30f)) return hy < 0.0f ? 0u : (1u << (2 * kGroups)) - 1u;
   const float ux = float(X0) - mx, vy = float(Y0) - my;
   const float ulo0 = ux - kCullPad, uhi0 = ux + (7.0f + kCullPad);
   const float ulo1 = ux + (8.0f - kCullPad), uhi1 = ux + (15.0f + kCullPad);
   uint32_t m = 0;
 #pragma unroll
-  for (int by = 0; by < 4; ++by) {
+  for (int by = 0; by < kGroups; ++by) {
     const float v0 = vy + (float(4 * by) - kCullPad), v1 = vy + (float(4 * by + 3) + kCullPad);
     const float a = fmaxf(v0, -hy), b = fminf(v1, hy);
     const float vR = fminf(fmaxf(vr, a), b), vL = fminf(fmaxf(-vr, a), b);

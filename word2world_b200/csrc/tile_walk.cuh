@@ -178,7 +178,9 @@ __device__ __forceinline__ void stage_store(TileWalkShared<kW>& sm, int buf, con
     s[1] = st.r1;
     s[2] = st.r2;
     sm.id[buf][j] = st.id;
-    mask = block_mask(st.r0.x, st.r0.y, st.r2.w, st.r3.x, st.r3.y, st.r3.z, st.r3.w, X0, Y0) >> first_block;
+    // the CTA's blocks are kW / 2 rows of two, starting at row group first_block / 2
+    mask = block_mask<kW / 2>(st.r0.x, st.r0.y, st.r2.w, st.r3.x, st.r3.y, st.r3.z, st.r3.w, X0,
+                              Y0 + kBlockH * (first_block / 2));
   }
   uint32_t mine = 0;
 #pragma unroll
