@@ -795,7 +795,10 @@ __device__ __forceinline__ void ref_gaussian(const BackwardArgs& a, int i, const
   a.dL_drotations[4 * i + 3] = dq.w;
 }
 
-__global__ void __launch_bounds__(kGaussThreads) gaussians_ref_kernel(BackwardArgs a) {
+// 8 CTAs per SM (64 registers, no spills; shared memory allows 9): more
+// Gaussians' loads in flight (0.452 -> 0.415 ms per 4-view step against the
+// default 6 CTAs at 80 registers).
+__global__ void __launch_bounds__(kGaussThreads, 8) gaussians_ref_kernel(BackwardArgs a) {
   __shared__ float s_sh[kGaussThreads / 32][32 * kShStride];
   // view, projection, camera position: shared memory is never aliased by the
   // outputs, so these stay in place across the output stores
