@@ -21,10 +21,13 @@ namespace {
 
 constexpr int kActThreads = 256;
 
+// kRow: floats per SH row, 3 (K + 1), when known at compile time (0: a.K's);
+// a constant row turns the element -> Gaussian division into a multiply.
+template <int kRow>
 __global__ void __launch_bounds__(kActThreads)
 activate_kernel(ActivateArgs a) {
   const long long P = a.P;
-  const int K = a.K;  // rest coefficients per Gaussian (sh_ac rows)
+  const int K = kRow > 0 ? kRow / 3 - 1 : a.K;  // rest coefficients per Gaussian (sh_ac rows)
   const int row = 3 * (K + 1);
   const long long stride = (long long)gridDim.x * blockDim.x;
   for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < P; i += stride) {
@@ -40,18 +43,20 @@ activate_kernel(ActivateArgs a) {
     a.rotations[4 * i + 3] = __fdiv_rn(z, n);
   }
   // shs[i] = [sh_dc[i], sh_ac[i]]: consecutive threads write consecutive floats
-  const long long total = P * row;
-  for (long long j = (long long)blockIdx.x * blockDim.x + threadIdx.x; j < total; j += stride) {
-    const long long i = j / row;
-    const int c = int(j - i * row);
-    a.shs[j] = c < 3 ? a.sh_dc[3 * i + c] : a.sh_ac[i * (3 * K) + (c - 3)];
+  // (32-bit indices: the host checks P * row < 2^31)
+  const uint32_t total = uint32_t(P) * uint32_t(row);
+  for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < total; j += uint32_t(stride)) {
+    const uint32_t i = j / uint32_t(row);
+    const uint32_t c = j - i * uint32_t(row);
+    a.shs[j] = c < 3u ? __ldg(a.sh_dc + 3u * i + c) : __ldg(a.sh_ac + i * uint32_t(3 * K) + (c - 3u));
   }
 }
 
+template <int kRow>
 __global__ void __launch_bounds__(kActThreads)
 activate_backward_kernel(ActivateBackwardArgs a) {
   const long long P = a.P;
-  const int K = a.K;
+  const int K = kRow > 0 ? kRow / 3 - 1 : a.K;
   const int row = 3 * (K + 1);
   const long long stride = (long long)gridDim.x * blockDim.x;
   for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < P; i += stride) {
@@ -74,13 +79,13 @@ activate_backward_kernel(ActivateBackwardArgs a) {
       for (int k = 0; k < 4; ++k) a.d_quat[4 * i + k] = g[k] * 1e12f;
     }
   }
-  const long long total = P * row;
-  for (long long j = (long long)blockIdx.x * blockDim.x + threadIdx.x; j < total; j += stride) {
-    const long long i = j / row;
-    const int c = int(j - i * row);
-    const float v = a.g_shs[j];
-    if (c < 3) a.d_sh_dc[3 * i + c] = v;
-    else a.d_sh_ac[i * (3 * K) + (c - 3)] = v;
+  const uint32_t total = uint32_t(P) * uint32_t(row);
+  for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < total; j += uint32_t(stride)) {
+    const uint32_t i = j / uint32_t(row);
+    const uint32_t c = j - i * uint32_t(row);
+    const float v = __ldg(a.g_shs + j);
+    if (c < 3u) a.d_sh_dc[3u * i + c] = v;
+    else a.d_sh_ac[i * uint32_t(3 * K) + (c - 3u)] = v;
   }
 }
 
@@ -88,22 +93,26 @@ int act_grid(long long P, int row) {
   int sms = 148;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, 0);
   const long long want = (P * row + kActThreads - 1) / kActThreads;
-  return int(want < 1 ? 1 : (want > (long long)sms * 16 ? (long long)sms * 16 : want));
+  return int(want < 1 ? 1 : (want > (long long)sms * 32 ? (long long)sms * 32 : want));
 }
 
 }  // namespace
 
 void launch_activate(const ActivateArgs& a, cudaStream_t stream) {
   if (a.P <= 0) return;
+  const int grid = act_grid(a.P, 3 * (a.K + 1));
   stage_begin(kStOther, stream);
-  activate_kernel<<<act_grid(a.P, 3 * (a.K + 1)), kActThreads, 0, stream>>>(a);
+  if (a.K == 15) activate_kernel<48><<<grid, kActThreads, 0, stream>>>(a);
+  else activate_kernel<0><<<grid, kActThreads, 0, stream>>>(a);
   stage_end(kStOther, stream, 1);
 }
 
 void launch_activate_backward(const ActivateBackwardArgs& a, cudaStream_t stream) {
   if (a.P <= 0) return;
+  const int grid = act_grid(a.P, 3 * (a.K + 1));
   stage_begin(kStOther, stream);
-  activate_backward_kernel<<<act_grid(a.P, 3 * (a.K + 1)), kActThreads, 0, stream>>>(a);
+  if (a.K == 15) activate_backward_kernel<48><<<grid, kActThreads, 0, stream>>>(a);
+  else activate_backward_kernel<0><<<grid, kActThreads, 0, stream>>>(a);
   stage_end(kStOther, stream, 1);
 }
 

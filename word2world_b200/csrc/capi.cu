@@ -451,6 +451,7 @@ int w2w_activate_forward(long long P, int K, const float* opacity_logit, const f
                          const float* sh_dc, const float* sh_ac, float* opacity, float* scales, float* rotations,
                          float* shs, w2w_stream_t stream) {
   if (P < 0 || K < 0) return W2W_ERR_INVALID;
+  if (P * 3 * (K + 1LL) >= (1LL << 31)) return W2W_ERR_CAPACITY;
   if (P == 0) return W2W_OK;
   if (!opacity_logit || !svec || !quaternion || !sh_dc || (K > 0 && !sh_ac) || !opacity || !scales ||
       !rotations || !shs)
@@ -465,6 +466,7 @@ int w2w_activate_backward(long long P, int K, const float* g_opacity, const floa
                           const float* quaternion, float* d_opacity_logit, float* d_svec, float* d_quaternion,
                           float* d_sh_dc, float* d_sh_ac, w2w_stream_t stream) {
   if (P < 0 || K < 0) return W2W_ERR_INVALID;
+  if (P * 3 * (K + 1LL) >= (1LL << 31)) return W2W_ERR_CAPACITY;
   if (P == 0) return W2W_OK;
   if (!g_opacity || !g_scales || !g_rotations || !g_shs || !opacity || !scales || !quaternion ||
       !d_opacity_logit || !d_svec || !d_quaternion || !d_sh_dc || (K > 0 && !d_sh_ac))
