@@ -274,6 +274,10 @@ unsigned long long w2w_launch_count(void);
  * milliseconds and kernel launches per stage (w2w_stage_count() stages,
  * named by w2w_stage_name) and resets the accumulators. */
 int w2w_stage_timing(int enable);
+/* The same for the stages whose bit is set in `mask` (bit i: stage i, named by
+ * w2w_stage_name); returns the previous mask.  Timing fewer stages keeps the
+ * host work between launches, and so the device's idle gaps, smaller. */
+unsigned w2w_stage_timing_mask(unsigned mask);
 int w2w_stage_count(void);
 const char* w2w_stage_name(int stage);
 int w2w_stage_times(double* ms, long long* launches, int max_stages);

@@ -421,6 +421,13 @@ PYBIND11_MODULE(TORCH_EXTENSION_NAME, m) {
   m.def("version", &w2w_version);
   m.def("launch_count", []() { return (unsigned long long)w2w_launch_count(); });
   m.def("stage_timing", [](bool on) { return w2w_stage_timing(on ? 1 : 0) != 0; });
+  m.def("stage_timing_only", [](const std::vector<std::string>& names) {
+    unsigned mask = 0;
+    for (const auto& nm : names)
+      for (int i = 0; i < w2w_stage_count(); ++i)
+        if (nm == w2w_stage_name(i)) mask |= 1u << i;
+    return w2w_stage_timing_mask(mask);
+  });
   m.def("stage_times", []() {
     const int n = w2w_stage_count();
     std::vector<double> ms(n);

@@ -194,7 +194,7 @@ __global__ void __launch_bounds__(kBlendCta, 16 / kBlendWarps) blend_kernel(Blen
 // Bucket sort of the tiles by decreasing list length (quarter-octave buckets;
 // order within a bucket is arbitrary).  One CTA.
 __global__ void __launch_bounds__(1024) tile_order_kernel(const uint2* ranges, const uint32_t* counts, int num_tiles,
-                                                          uint32_t* order) {
+                                                          uint32_t* order, uint32_t* zero) {
   constexpr int kBuckets = 130;
   __shared__ uint32_t s_cnt[kBuckets];
   __shared__ uint32_t s_pos[kBuckets];
@@ -205,6 +205,8 @@ __global__ void __launch_bounds__(1024) tile_order_kernel(const uint2* ranges, c
     return 1 + 4 * e + int(q);
   };
   for (int i = threadIdx.x; i < kBuckets; i += blockDim.x) s_cnt[i] = 0;
+  if (zero != nullptr)
+    for (int t = threadIdx.x; t < num_tiles; t += blockDim.x) zero[t] = 0u;
   __syncthreads();
   auto weight = [&](int t) -> uint32_t {
     if (counts) return counts[t];
@@ -228,11 +230,11 @@ void launch_blend(const BlendArgs& a, cudaStream_t stream) {
   const int tiles = a.items ? a.total_tiles : ((a.W + kTile - 1) / kTile) * ((a.H + kTile - 1) / kTile);
   if (tiles <= 0) return;
   stage_begin(kStBlend, stream);
-  if (kBlendParts > 1) cudaMemsetAsync(a.tile_max, 0, sizeof(uint32_t) * size_t(tiles), stream);
-  tile_order_kernel<<<1, 1024, 0, stream>>>(a.ranges, nullptr, tiles, a.order);
+  tile_order_kernel<<<1, 1024, 0, stream>>>(a.ranges, nullptr, tiles, a.order,
+                                            kBlendParts > 1 ? a.tile_max : nullptr);
   blend_kernel<<<tiles * kBlendParts, kBlendCta, 0, stream>>>(a);
   // the backward's order: by the largest contributor count the blend just found
-  tile_order_kernel<<<1, 1024, 0, stream>>>(nullptr, a.tile_max, tiles, a.order_bwd);
+  tile_order_kernel<<<1, 1024, 0, stream>>>(nullptr, a.tile_max, tiles, a.order_bwd, nullptr);
   stage_end(kStBlend, stream, 3);
 }
 

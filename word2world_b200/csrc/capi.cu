@@ -300,6 +300,11 @@ int w2w_forward_render(const w2w_settings* s, const void* geom_state, const w2w_
     so.num_tiles = T;
     so.tile_hist = at<uint32_t>(binning_state, BL.tile_hist);
     so.ranges = ranges;
+    // hist, tile_hist and the used status words are contiguous; the tile
+    // counters were cleared by write_bin_header
+    so.clear_span = at<void>(binning_state, BL.hist);
+    so.clear_bytes = BL.status - BL.hist + size_t(passes > 0 ? passes : 1) * kMaxBins * 4 *
+                     size_t((R + sort_tile_keys(kp.key64) - 1) / sort_tile_keys(kp.key64));
     launch_sort(so, st);
     point_list = valsA;
   }
@@ -868,6 +873,11 @@ int w2w_batch_forward_render(const w2w_batch_item* items, int n, const void* geo
     so.num_tiles = T;
     so.tile_hist = at<uint32_t>(binning_state, BL.tile_hist);
     so.ranges = ranges;
+    // hist, tile_hist and the used status words are contiguous; the tile
+    // counters were cleared by write_bin_header
+    so.clear_span = at<void>(binning_state, BL.hist);
+    so.clear_bytes = BL.status - BL.hist + size_t(passes > 0 ? passes : 1) * kMaxBins * 4 *
+                     size_t((R + sort_tile_keys(kp.key64) - 1) / sort_tile_keys(kp.key64));
     launch_sort(so, st);
     point_list = valsA;
   }

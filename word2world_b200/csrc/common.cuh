@@ -336,9 +336,11 @@ struct BinLayout {
     keysB = take(r * 8);
     valsA = take(r * 4);
     valsB = take(r * 4);
+    // hist, tile_hist, then status: one memset clears them and the used
+    // passes' status words
     hist = take(size_t(kMaxPasses) * kMaxBins * 4);
-    status = take(size_t(kMaxPasses) * sort_tiles * kMaxBins * 4);
     tile_hist = take(size_t(num_tiles > 0 ? num_tiles : 1) * 4);
+    status = take(size_t(kMaxPasses) * sort_tiles * kMaxBins * 4);
     total = align256(o);
   }
 };

@@ -122,8 +122,14 @@ struct SortArgs {
   int num_tiles;
   uint32_t* tile_hist;
   uint2* ranges;
+  // optional: one span to zero instead of the four buffers above (hist, the
+  // used status words, counters, tile_hist), when the caller's layout makes
+  // them contiguous
+  void* clear_span;
+  size_t clear_bytes;
 };
 int sort_passes(int bits);
+long long sort_tile_keys(int key64);  // keys per onesweep tile for the key width
 int sort_digit_bits(int bits);
 void launch_sort(const SortArgs& a, cudaStream_t stream);
 size_t sort_status_words(long long n);

@@ -388,7 +388,15 @@ void launch_onesweep_w(int tiles, cudaStream_t stream, const K* kin, const uint3
                        long long n, int shift, const uint32_t* digit_base, uint32_t* status, uint32_t* counter,
                        uint32_t* err) {
   const size_t dyn = (sizeof(K) + sizeof(uint32_t)) * size_t(onesweep_tile<K>());
-  cudaFuncSetAttribute(onesweep_kernel<K, kWidth>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(dyn));
+  // the shared-memory opt-in is set once per device (a driver call per launch
+  // would widen the gap the device waits between launches)
+  static bool opted[64] = {false};
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (dev < 0 || dev >= 64 || !opted[dev]) {
+    cudaFuncSetAttribute(onesweep_kernel<K, kWidth>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(dyn));
+    if (dev >= 0 && dev < 64) opted[dev] = true;
+  }
   onesweep_kernel<K, kWidth><<<tiles, kSortThreads, dyn, stream>>>(kin, vin, kout, vout, n, shift, digit_base,
                                                                     status, counter, err);
 }
@@ -417,11 +425,15 @@ void run_sort(const SortArgs& a, cudaStream_t stream) {
   const long long n = a.n;
   if (n <= 0) return;
   const long long tiles = (n + onesweep_tile<K>() - 1) / onesweep_tile<K>();
-  cudaMemsetAsync(a.hist, 0, sizeof(uint32_t) * kMaxBins * kMaxPasses, stream);
-  cudaMemsetAsync(a.counters, 0, sizeof(uint32_t) * kMaxPasses, stream);
-  cudaMemsetAsync(a.status, 0, sizeof(uint32_t) * kMaxBins * size_t(tiles) * size_t(passes > 0 ? passes : 1),
-                  stream);
-  if (a.tile_hist) cudaMemsetAsync(a.tile_hist, 0, sizeof(uint32_t) * size_t(a.num_tiles), stream);
+  if (a.clear_span != nullptr) {  // the caller's layout puts everything to clear in one span
+    cudaMemsetAsync(a.clear_span, 0, a.clear_bytes, stream);
+  } else {
+    cudaMemsetAsync(a.hist, 0, sizeof(uint32_t) * kMaxBins * kMaxPasses, stream);
+    cudaMemsetAsync(a.counters, 0, sizeof(uint32_t) * kMaxPasses, stream);
+    cudaMemsetAsync(a.status, 0, sizeof(uint32_t) * kMaxBins * size_t(tiles) * size_t(passes > 0 ? passes : 1),
+                    stream);
+    if (a.tile_hist) cudaMemsetAsync(a.tile_hist, 0, sizeof(uint32_t) * size_t(a.num_tiles), stream);
+  }
   if (passes > 0 || a.tile_hist) {
     int sms = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, 0);
@@ -461,6 +473,8 @@ void run_sort(const SortArgs& a, cudaStream_t stream) {
 }
 
 }  // namespace
+
+long long sort_tile_keys(int key64) { return key64 ? onesweep_tile<uint64_t>() : onesweep_tile<uint32_t>(); }
 
 int sort_passes(int bits) { return bits <= 0 ? 0 : (bits + kMaxDigitBits - 1) / kMaxDigitBits; }
 

@@ -51,7 +51,10 @@ struct TilePixel {
 // lists the tiles by decreasing weight (tile_order_kernel: the list length
 // from `ranges`, or `counts` when given), so the heaviest start in the first
 // wave instead of wherever the raster order puts them.
-__global__ void tile_order_kernel(const uint2* ranges, const uint32_t* counts, int num_tiles, uint32_t* order);
+// `zero`, when given, is cleared over num_tiles entries on the way (the
+// blend's per-tile maximum, which its CTAs then combine).
+__global__ void tile_order_kernel(const uint2* ranges, const uint32_t* counts, int num_tiles, uint32_t* order,
+                                  uint32_t* zero);
 
 // One entry's record held in registers between its gather and its store.
 struct ChunkLoad {

@@ -18,7 +18,7 @@ const char* kStageNames[kNumStages] = {"preprocess", "duplicate", "sort_histogra
                                        "backward_render", "backward_gaussians", "scan", "other"};
 
 std::atomic<unsigned long long> g_launches{0};
-std::atomic<int> g_enabled{0};
+std::atomic<unsigned> g_mask{0};  // bit s: stage s records events
 
 struct Pending {
   int stage;
@@ -48,15 +48,14 @@ cudaEvent_t take_event() {
 }  // namespace
 
 void stage_begin(int stage, cudaStream_t s) {
-  (void)stage;
-  if (!g_enabled.load(std::memory_order_relaxed)) return;
+  if (!((g_mask.load(std::memory_order_relaxed) >> stage) & 1u)) return;
   t_start = take_event();
   cudaEventRecord(t_start, s);
 }
 
 void stage_end(int stage, cudaStream_t s, int kernels) {
   g_launches.fetch_add(static_cast<unsigned long long>(kernels), std::memory_order_relaxed);
-  if (!g_enabled.load(std::memory_order_relaxed) || t_start == nullptr) return;
+  if (!((g_mask.load(std::memory_order_relaxed) >> stage) & 1u) || t_start == nullptr) return;
   cudaEvent_t stop = take_event();
   cudaEventRecord(stop, s);
   std::lock_guard<std::mutex> lk(g_mu);
@@ -70,7 +69,13 @@ extern "C" {
 
 unsigned long long w2w_launch_count(void) { return w2w::g_launches.load(); }
 
-int w2w_stage_timing(int enable) { return w2w::g_enabled.exchange(enable ? 1 : 0); }
+int w2w_stage_timing(int enable) {
+  return w2w::g_mask.exchange(enable ? (1u << w2w::kNumStages) - 1u : 0u) != 0u;
+}
+
+unsigned w2w_stage_timing_mask(unsigned mask) {
+  return w2w::g_mask.exchange(mask & ((1u << w2w::kNumStages) - 1u));
+}
 
 int w2w_stage_count(void) { return w2w::kNumStages; }
 
