@@ -45,6 +45,7 @@ activate_kernel(ActivateArgs a) {
   // shs[i] = [sh_dc[i], sh_ac[i]]: consecutive threads write consecutive floats
   // (32-bit indices: the host checks P * row < 2^31)
   const uint32_t total = uint32_t(P) * uint32_t(row);
+#pragma unroll 4
   for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < total; j += uint32_t(stride)) {
     const uint32_t i = j / uint32_t(row);
     const uint32_t c = j - i * uint32_t(row);
@@ -80,6 +81,7 @@ activate_backward_kernel(ActivateBackwardArgs a) {
     }
   }
   const uint32_t total = uint32_t(P) * uint32_t(row);
+#pragma unroll 4
   for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < total; j += uint32_t(stride)) {
     const uint32_t i = j / uint32_t(row);
     const uint32_t c = j - i * uint32_t(row);
@@ -93,7 +95,7 @@ int act_grid(long long P, int row) {
   int sms = 148;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, 0);
   const long long want = (P * row + kActThreads - 1) / kActThreads;
-  return int(want < 1 ? 1 : (want > (long long)sms * 32 ? (long long)sms * 32 : want));
+  return int(want < 1 ? 1 : (want > (long long)sms * 16 ? (long long)sms * 16 : want));
 }
 
 }  // namespace
