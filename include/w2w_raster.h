@@ -195,6 +195,15 @@ int w2w_voxel_field(const float* means, const float* covs, const float* opacitie
 int w2w_compute_voxel_field(float* h_occ, const float* h_means, const float* h_covs, const float* h_opacities,
                             int n, int resolution, int num_blocks, float relax_ratio);
 
+/* Per-group sums of a batched call's per-element gradient rows (width floats
+ * per row): output row r of group g = the sum over g's items, in list order,
+ * of row (item's first element + r).  `tables` (device) holds group_base[G+1]
+ * (the groups' first output rows, then the total), item_ptr[G+1] (CSR offsets
+ * into the next array) and item_elem[num_items] (each item's first element
+ * row).  No counterpart in the reference, which renders one view per call. */
+int w2w_group_sum(const float* src, int width, int num_groups, const uint32_t* tables, int num_items, float* dst,
+                  long long total_rows, w2w_stream_t stream);
+
 /* Densification statistics of the training loop (gaussians_handler.py:116-118):
  * for every Gaussian with radii[i] > 0, counter[i] += 1 and accum[i] +=
  * |dL/dmean2D[i, 0:2]| (dL_dmeans2D [P,3], accum and counter [P], updated in

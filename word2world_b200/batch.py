@@ -314,30 +314,44 @@ class BatchRenderer:
                                     p(st["radii"]), p(st["alpha"]), p(dlc), p(dld), p(dla), self.grad_mode,
                                     p(scratch), ctypes.c_size_t(scratch.numel()), p(g_m2), p(g_col), p(g_op),
                                     p(g_m3), p(g_cov), p(g_sh), p(g_sc), p(g_rot), stream), "batch backward")
-        # per-group sums of the items' element ranges (one index_add per tensor)
+        # per-group sums of the items' element ranges: one deterministic
+        # reduction launch per tensor (w2w_group_sum)
         gid = [groups[v] if groups is not None else views[v].scene for v in range(n)]
-        order, base, total = [], {}, 0
-        for v in range(n):
-            if gid[v] not in base:
-                base[gid[v]] = total
-                order.append(gid[v])
-                total += scenes[views[v].scene].P
-        # element e of item v goes to row base[group of v] + (e - first element of v)
-        idx = self.ws.i64("idx", E) if self.ws is not None else torch.empty(E, dtype=torch.int64, device=dev)
-        torch.arange(E, out=idx)
-        e0 = 0
+        order, base, total, members = [], {}, 0, {}
+        ebase, e0 = [], 0
         for v in range(n):
             P = scenes[views[v].scene].P
-            if base[gid[v]] != e0:
-                idx[e0:e0 + P] += base[gid[v]] - e0
+            ebase.append(e0)
             e0 += P
-        size = {gid[v]: scenes[views[v].scene].P for v in range(n)}
+            g = gid[v]
+            if g not in base:
+                base[g] = total
+                order.append(g)
+                members[g] = []
+                total += P
+            elif scenes[views[members[g][0]].scene].P != P:
+                raise ValueError(f"group {g!r} mixes scenes of different sizes")
+            members[g].append(v)
+        size = {g: scenes[views[members[g][0]].scene].P for g in order}
+        G = len(order)
+        tab = np.empty(2 * (G + 1) + n, dtype=np.uint32)
+        tab[:G] = [base[g] for g in order]
+        tab[G] = total
+        ptr, items = [0], []
+        for g in order:
+            items += [ebase[v] for v in members[g]]
+            ptr.append(len(items))
+        tab[G + 1:2 * (G + 1)] = ptr
+        tab[2 * (G + 1):] = items
+        tables = self._u8("group_tables", tab.nbytes)
+        tables.copy_(torch.from_numpy(tab.view(np.uint8)))
         out = {"groups": order}
         for name, t in (("means3D", g_m3), ("opacities", g_op), ("scales", g_sc), ("rotations", g_rot),
                         ("shs", g_sh)):
+            width = int(np.prod(t.shape[1:]))
             acc = self._f32("acc_" + name, total, *t.shape[1:])
-            acc.zero_()
-            acc.index_add_(0, idx, t[:E])
+            _check(L.w2w_group_sum(p(t), width, G, p(tables), n, p(acc), ctypes.c_longlong(total), stream),
+                   "group sum")
             out[name] = [acc[base[g]:base[g] + size[g]] for g in order]
         e = 0
         out["means2D"] = []

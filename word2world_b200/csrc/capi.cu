@@ -590,6 +590,15 @@ int w2w_compute_voxel_field(float* h_occ, const float* h_means, const float* h_c
   return rc;
 }
 
+int w2w_group_sum(const float* src, int width, int num_groups, const uint32_t* tables, int num_items, float* dst,
+                  long long total_rows, w2w_stream_t stream) {
+  if (width <= 0 || num_groups < 0 || num_items < 0 || total_rows < 0) return W2W_ERR_INVALID;
+  if (num_groups == 0 || total_rows == 0) return W2W_OK;
+  if (!src || !tables || !dst) return W2W_ERR_INVALID;
+  launch_group_sum(src, width, num_groups, tables, num_items, dst, total_rows, S(stream));
+  return check_launch();
+}
+
 int w2w_densification_stats(long long P, const float* dL_dmeans2D, const int* radii, float* accum, float* counter,
                             w2w_stream_t stream) {
   if (P < 0) return W2W_ERR_INVALID;

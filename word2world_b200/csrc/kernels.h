@@ -245,6 +245,12 @@ struct VoxelArgs {
 void launch_voxel_prepare(const VoxelArgs& a, cudaStream_t stream);
 void launch_voxel_emit(const VoxelArgs& a, cudaStream_t stream);
 void launch_voxel_field(const VoxelArgs& a, const uint32_t* list, const uint2* ranges, cudaStream_t stream);
+// Per-group sums of element rows (groupsum.cu).  tables: group_base[G + 1]
+// (first output row of each group; the last entry is the total),
+// item_ptr[G + 1] (CSR into item_elem), item_elem[num_items] (each item's
+// first element row).
+void launch_group_sum(const float* src, int width, int num_groups, const uint32_t* tables, int num_items,
+                      float* dst, long long total_rows, cudaStream_t stream);
 // Densification statistics (densify.cu).
 void launch_densify_stats(long long P, const float* dL_dmeans2D, const int* radii, float* accum, float* counter,
                           cudaStream_t stream);
