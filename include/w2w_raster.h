@@ -165,6 +165,28 @@ int w2w_scan_u32(const uint32_t* in, uint32_t* out, long long n, int exclusive, 
 #define W2W_SCAN_NOALLOC_MAX (1LL << 24)
 int w2w_scan_u32_noalloc(const uint32_t* in, uint32_t* out, long long n, int exclusive, w2w_stream_t stream);
 
+/* Renderer.render's path on its raw parameters (Renderer.py:164-192): the
+ * activation preamble (sigmoid opacity, exp scales, normalised quaternion,
+ * concatenated SH; bit-identical to the reference's torch operations) runs
+ * inside the projection pass, so the activated tensors never exist.
+ * w2w_forward_geometry_raw takes mean [P,3], svec [P,3], quaternion [P,4],
+ * opacity logits [P], sh_dc [P,1,3] and sh_ac [P,M-1,3] (1 <= M <= 16) and is
+ * otherwise w2w_forward_geometry (w2w_forward_render follows unchanged).
+ * w2w_backward_raw is w2w_backward in reference mode whose per-Gaussian pass
+ * chains through the activations: it writes d/dsvec, d/dquaternion,
+ * d/dlogit and the SH gradient split as sh_dc / sh_ac. */
+int w2w_forward_geometry_raw(const w2w_settings* s, const float* means3D, const float* svec, const float* quaternion,
+                             const float* opacity_logit, const float* sh_dc, const float* sh_ac, int* radii,
+                             void* geom_state, w2w_geometry_info* info, w2w_stream_t stream);
+int w2w_backward_raw(const w2w_settings* s, const float* means3D, const float* svec, const float* quaternion,
+                     const float* opacity_logit, const float* sh_dc, const float* sh_ac, const int* radii,
+                     const void* geom_state, long long num_rendered, const void* binning_state,
+                     const void* image_state, const float* out_alpha, const float* dL_dcolor, const float* dL_ddepth,
+                     const float* dL_dalpha, void* scratch, size_t scratch_bytes, float* dL_dmeans2D,
+                     float* dL_dcolors, float* dL_dopacity_logit, float* dL_dmeans3D, float* dL_dcov3D,
+                     float* dL_dsh_dc, float* dL_dsh_ac, float* dL_dsvec, float* dL_dquaternion,
+                     w2w_stream_t stream);
+
 /* The activation preamble of Renderer.render (Renderer.py:164-167) in one
  * pass: opacity = sigmoid(logit) [P], scales = exp(svec) [P,3], rotations =
  * normalize(quaternion) [P,4], shs = cat(sh_dc [P,1,3], sh_ac [P,K,3]) [P,K+1,3];

@@ -31,16 +31,14 @@ activate_kernel(ActivateArgs a) {
   const int row = 3 * (K + 1);
   const long long stride = (long long)gridDim.x * blockDim.x;
   for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < P; i += stride) {
-    a.opacity[i] = __fdiv_rn(1.f, __fadd_rn(1.f, expf(-a.opacity_logit[i])));
+    a.opacity[i] = act_sigmoid(a.opacity_logit[i]);
 #pragma unroll
     for (int k = 0; k < 3; ++k) a.scales[3 * i + k] = expf(a.svec[3 * i + k]);
-    const float w = a.quat[4 * i], x = a.quat[4 * i + 1], y = a.quat[4 * i + 2], z = a.quat[4 * i + 3];
-    const float ss = __fadd_rn(__fadd_rn(__fmul_rn(w, w), __fmul_rn(y, y)), __fadd_rn(__fmul_rn(x, x), __fmul_rn(z, z)));
-    const float n = fmaxf(__fsqrt_rn(ss), 1e-12f);
-    a.rotations[4 * i] = __fdiv_rn(w, n);
-    a.rotations[4 * i + 1] = __fdiv_rn(x, n);
-    a.rotations[4 * i + 2] = __fdiv_rn(y, n);
-    a.rotations[4 * i + 3] = __fdiv_rn(z, n);
+    const float4 r = act_normalize(a.quat[4 * i], a.quat[4 * i + 1], a.quat[4 * i + 2], a.quat[4 * i + 3]);
+    a.rotations[4 * i] = r.x;
+    a.rotations[4 * i + 1] = r.y;
+    a.rotations[4 * i + 2] = r.z;
+    a.rotations[4 * i + 3] = r.w;
   }
   // shs[i] = [sh_dc[i], sh_ac[i]]: consecutive threads write consecutive floats
   // (32-bit indices: the host checks P * row < 2^31)
@@ -61,10 +59,13 @@ activate_backward_kernel(ActivateBackwardArgs a) {
   const int row = 3 * (K + 1);
   const long long stride = (long long)gridDim.x * blockDim.x;
   for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < P; i += stride) {
-    const float y = a.opacity[i];
+    // activated opacity and scales: kept by the forward, or recomputed from
+    // the raw parameters (the fused-preamble path keeps none)
+    const float y = a.opacity != nullptr ? a.opacity[i] : act_sigmoid(a.opacity_logit[i]);
     a.d_opacity_logit[i] = a.g_opacity[i] * (1.f - y) * y;
 #pragma unroll
-    for (int k = 0; k < 3; ++k) a.d_svec[3 * i + k] = a.g_scales[3 * i + k] * a.scales[3 * i + k];
+    for (int k = 0; k < 3; ++k)
+      a.d_svec[3 * i + k] = a.g_scales[3 * i + k] * (a.scales != nullptr ? a.scales[3 * i + k] : expf(a.svec[3 * i + k]));
     const float q[4] = {a.quat[4 * i], a.quat[4 * i + 1], a.quat[4 * i + 2], a.quat[4 * i + 3]};
     const float g[4] = {a.g_rotations[4 * i], a.g_rotations[4 * i + 1], a.g_rotations[4 * i + 2],
                         a.g_rotations[4 * i + 3]};

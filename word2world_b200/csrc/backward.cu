@@ -566,6 +566,70 @@ __device__ __forceinline__ void sh_store_outer(float* dsh, int M, int i0, int n,
   }
 }
 
+// The raw path's SH rows: coefficient 0 from sh_dc ([P, 1, 3]), the rest from
+// sh_ac ([P, M - 1, 3]).  Same staging as sh_stage_in.  Warp-collective.
+__device__ __forceinline__ void sh_stage_in_raw(const float* dc, const float* ac, int M, int i0, int n, float* s,
+                                                int stride) {
+  constexpr int kInFlight = 8;
+  const int rs = 3 * (M < 16 ? M : 16), ra = 3 * (M - 1), lane = threadIdx.x & 31;
+  if (rs > 0) {
+    const int total = n * rs;
+    int g = 0, c = lane;
+    while (c >= rs) { c -= rs; ++g; }
+    for (int e0 = 0; e0 < total; e0 += 32 * kInFlight) {
+      float v[kInFlight];
+      int dst[kInFlight];
+#pragma unroll
+      for (int k = 0; k < kInFlight; ++k) {
+        const bool ok = e0 + 32 * k + lane < total;
+        v[k] = !ok ? 0.f : c < 3 ? __ldg(dc + size_t(i0 + g) * 3 + c) : __ldg(ac + size_t(i0 + g) * ra + (c - 3));
+        dst[k] = ok ? g * stride + c : -1;
+        c += 32;
+        while (c >= rs) { c -= rs; ++g; }
+      }
+#pragma unroll
+      for (int k = 0; k < kInFlight; ++k)
+        if (dst[k] >= 0) s[dst[k]] = v[k];
+    }
+  }
+  __syncwarp();
+}
+
+// sh_store_outer for the raw path: coefficient 0 to ddc, the rest to dac.
+__device__ __forceinline__ void sh_store_outer_raw(float* ddc, float* dac, int M, int i0, int n, float* s,
+                                                   const float (&basis)[16], const float (&cf)[3], bool active) {
+  constexpr int kRow = 21;
+  const int lane = threadIdx.x & 31, rg = 3 * M, ra = 3 * (M - 1);
+  __syncwarp();
+#pragma unroll
+  for (int k = 0; k < 16; ++k) s[lane * kRow + k] = active ? basis[k] : 0.f;
+#pragma unroll
+  for (int ch = 0; ch < 3; ++ch) s[lane * kRow + 16 + ch] = active ? cf[ch] : 0.f;
+  __syncwarp();
+  if (rg > 0) {
+    constexpr int kInFlight = 8;
+    const int total = n * rg;
+    int g = 0, c = lane;
+    while (c >= rg) { c -= rg; ++g; }
+    for (int e0 = 0; e0 < total; e0 += 32 * kInFlight) {
+      float v[kInFlight];
+      float* dst[kInFlight];
+#pragma unroll
+      for (int q = 0; q < kInFlight; ++q) {
+        const int k = c / 3, ch = c - 3 * k;
+        const bool ok = e0 + 32 * q + lane < total;
+        v[q] = ok && k < 16 ? s[g * kRow + k] * s[g * kRow + 16 + ch] : 0.f;
+        dst[q] = !ok ? nullptr : c < 3 ? ddc + size_t(i0 + g) * 3 + c : dac + size_t(i0 + g) * ra + (c - 3);
+        c += 32;
+        while (c >= rg) { c -= rg; ++g; }
+      }
+#pragma unroll
+      for (int q = 0; q < kInFlight; ++q)
+        if (dst[q] != nullptr) *dst[q] = v[q];
+    }
+  }
+}
+
 // Per-Gaussian, reference formulas (backward.cu:27-227 then :229-519)
 __constant__ float kSH_C2[5] = {1.0925484305920792f, -1.0925484305920792f, 0.31539156525252005f,
                                 -1.0925484305920792f, 0.5462742152960396f};
@@ -582,6 +646,20 @@ struct GView {
   int gi;             // index within the scene
   int W, degree;
   float h_x, h_y, tan_fovx, tan_fovy, focal_x, scale_modifier;
+  const float* svec = nullptr;  // raw scales / quaternions (then scales / rotations are unused)
+  const float* quat = nullptr;
+
+  // the activated scale k and rotation (w, x, y, z)
+  __device__ __forceinline__ float scale(int k) const {
+    return svec != nullptr ? expf(__ldg(&svec[3 * gi + k])) : __ldg(&scales[3 * gi + k]);
+  }
+  __device__ __forceinline__ float4 rotation() const {
+    if (quat != nullptr)
+      return act_normalize(__ldg(&quat[4 * gi]), __ldg(&quat[4 * gi + 1]), __ldg(&quat[4 * gi + 2]),
+                           __ldg(&quat[4 * gi + 3]));
+    return make_float4(__ldg(&rotations[4 * gi]), __ldg(&rotations[4 * gi + 1]), __ldg(&rotations[4 * gi + 2]),
+                       __ldg(&rotations[4 * gi + 3]));
+  }
 };
 
 __device__ __forceinline__ GView make_gview(const BackwardArgs& a, int i, const float* s_mats) {
@@ -589,6 +667,8 @@ __device__ __forceinline__ GView make_gview(const BackwardArgs& a, int i, const 
   if (a.items == nullptr) {
     g = GView{a.means3D, a.scales, a.rotations, s_mats, i, a.W, a.degree, a.h_x, a.h_y, a.tan_fovx, a.tan_fovy,
               a.focal_x, a.scale_modifier};
+    g.svec = a.svec;
+    g.quat = a.quat;
   } else {
     const BatchItem& it = a.items[find_item_elem(a.items, a.num_items, uint32_t(i))];
     g = GView{it.means3D, it.scales, it.rotations, it.view, i - int(it.elem_base), it.W, it.degree, it.h_x, it.h_y,
@@ -761,13 +841,13 @@ __device__ __forceinline__ void ref_gaussian(const BackwardArgs& a, int i, const
   a.dL_dmeans3D[3 * i + 2] = sd[2];
 
   // ---- scale / rotation (backward.cu:446-518) ----
-  const float qw = __ldg(&gv.rotations[4 * gv.gi]), qx = __ldg(&gv.rotations[4 * gv.gi + 1]), qy = __ldg(&gv.rotations[4 * gv.gi + 2]),
-              qz = __ldg(&gv.rotations[4 * gv.gi + 3]);
+  const float4 qr = gv.rotation();
+  const float qw = qr.x, qx = qr.y, qy = qr.z, qz = qr.w;
   const float xx = qx * qx, yy = qy * qy, zz = qz * qz;
   const float qxy = qx * qy, qxz = qx * qz, qyz = qy * qz;
   const float xw = qx * qw, yw = qy * qw, zw = qz * qw;
-  const float sx = gv.scale_modifier * __ldg(&gv.scales[3 * gv.gi]), sy = gv.scale_modifier * __ldg(&gv.scales[3 * gv.gi + 1]),
-              sz = gv.scale_modifier * __ldg(&gv.scales[3 * gv.gi + 2]);
+  const float sx = gv.scale_modifier * gv.scale(0), sy = gv.scale_modifier * gv.scale(1),
+              sz = gv.scale_modifier * gv.scale(2);
   const float m11 = sx * (1.f - 2.f * (yy + zz)), m12 = sx * 2.f * (qxy - zw), m13 = sx * 2.f * (qxz + yw);
   const float m21 = sy * 2.f * (qxy + zw), m22 = sy * (1.f - 2.f * (xx + zz)), m23 = sy * 2.f * (qyz - xw);
   const float m31 = sz * 2.f * (qxz - yw), m32 = sz * 2.f * (qyz + xw), m33 = sz * (1.f - 2.f * (xx + yy));
@@ -781,14 +861,32 @@ __device__ __forceinline__ void ref_gaussian(const BackwardArgs& a, int i, const
   const float a31 = 2.f * (m31 * g11 + m32 * g12 + m33 * g13);
   const float a32 = 2.f * (m31 * g12 + m32 * g22 + m33 * g23);
   const float a33 = 2.f * (m31 * g13 + m32 * g23 + m33 * g33);
-  a.dL_dscales[3 * i] = (1.f - 2.f * (yy + zz)) * a11 + 2.f * (qxy - zw) * a12 + 2.f * (qxz + yw) * a13;
-  a.dL_dscales[3 * i + 1] = 2.f * (qxy + zw) * a21 + (1.f - 2.f * (xx + zz)) * a22 + 2.f * (qyz - xw) * a23;
-  a.dL_dscales[3 * i + 2] = 2.f * (qxz - yw) * a31 + 2.f * (qyz + xw) * a32 + (1.f - 2.f * (xx + yy)) * a33;
+  float ds[3] = {(1.f - 2.f * (yy + zz)) * a11 + 2.f * (qxy - zw) * a12 + 2.f * (qxz + yw) * a13,
+                 2.f * (qxy + zw) * a21 + (1.f - 2.f * (xx + zz)) * a22 + 2.f * (qyz - xw) * a23,
+                 2.f * (qxz - yw) * a31 + 2.f * (qyz + xw) * a32 + (1.f - 2.f * (xx + yy)) * a33};
+  if (gv.svec != nullptr)  // raw path: scales = exp(svec)
+    for (int k = 0; k < 3; ++k) ds[k] = ds[k] * gv.scale(k);
+  a.dL_dscales[3 * i] = ds[0];
+  a.dL_dscales[3 * i + 1] = ds[1];
+  a.dL_dscales[3 * i + 2] = ds[2];
   float4 dq;
   dq.x = 4.f * (-sz * (a31 * yw - a32 * xw + a33 * qxy) + sy * (a21 * zw - a22 * qxz + a23 * yy) + sx * (a12 * zw - a13 * yw - a11 * qyz));
   dq.y = 4.f * (sz * (a31 * zw + a32 * zz - a33 * qyz) - sy * (a21 * yw + a22 * qxy + a23 * xx) + sx * (a12 * yy + a13 * zw + a11 * qxz));
   dq.z = 4.f * (-sz * (a31 * xx + a32 * xw + a33 * qxz) + sy * (a21 * zw + a22 * yy + a23 * yw) - sx * (a12 * xw + a13 * xx + a11 * qxy));
   dq.w = 4.f * (sz * (a31 * xw - a32 * xx + a33 * qxy) - sy * (a21 * qxz - a22 * zw + a23 * qyz) + sx * (a12 * qyz - a13 * zz + a11 * yy));
+  if (gv.quat != nullptr) {  // raw path: rotation = q / max(|q|, 1e-12)
+    const float q0 = __ldg(&gv.quat[4 * gv.gi]), q1 = __ldg(&gv.quat[4 * gv.gi + 1]),
+                q2 = __ldg(&gv.quat[4 * gv.gi + 2]), q3 = __ldg(&gv.quat[4 * gv.gi + 3]);
+    const float n = sqrtf(q0 * q0 + q1 * q1 + q2 * q2 + q3 * q3);
+    if (n > 1e-12f) {  // (g - r (r . g)) / n with r = q / n
+      const float inv = 1.f / n;
+      const float rg = (q0 * dq.x + q1 * dq.y + q2 * dq.z + q3 * dq.w) * inv;
+      dq = make_float4((dq.x - q0 * inv * rg) * inv, (dq.y - q1 * inv * rg) * inv, (dq.z - q2 * inv * rg) * inv,
+                       (dq.w - q3 * inv * rg) * inv);
+    } else {  // the norm is clamped to 1e-12 there: q / 1e-12 is linear in q
+      dq = make_float4(dq.x * 1e12f, dq.y * 1e12f, dq.z * 1e12f, dq.w * 1e12f);
+    }
+  }
   a.dL_drotations[4 * i] = dq.x;
   a.dL_drotations[4 * i + 1] = dq.y;
   a.dL_drotations[4 * i + 2] = dq.z;
@@ -818,7 +916,8 @@ __global__ void __launch_bounds__(kGaussThreads, 8) gaussians_ref_kernel(Backwar
   const int stride = sh_stride(a.M);
   const GView gv = make_gview(a, lane < n ? i : i0, s_mats);
   if (a.items == nullptr) {
-    sh_stage_in(a.shs, a.M, i0, n, sw, stride);
+    if (a.sh_dc != nullptr) sh_stage_in_raw(a.sh_dc, a.sh_ac, a.M, i0, n, sw, stride);
+    else sh_stage_in(a.shs, a.M, i0, n, sw, stride);
   } else {  // a warp's elements may belong to different scenes: each thread its own row
     const int rs = 3 * (a.M < 16 ? a.M : 16);
     if (lane < n) {
@@ -837,8 +936,14 @@ __global__ void __launch_bounds__(kGaussThreads, 8) gaussians_ref_kernel(Backwar
     for (int k = 0; k < 3; ++k) a.dL_dscales[3 * i + k] = 0.f;
     for (int k = 0; k < 4; ++k) a.dL_drotations[4 * i + k] = 0.f;
   }
+  // raw path: the accumulated opacity gradient through opacity = sigmoid(logit)
+  if (a.logit != nullptr && lane < n) {
+    const float y = act_sigmoid(__ldg(&a.logit[i]));
+    a.dL_dopacity[i] = a.dL_dopacity[i] * (1.f - y) * y;
+  }
   // dL_dsh[k][ch] = basis[k] * cf[ch] for the first min(M, 16) bands, 0 beyond
-  sh_store_outer(a.dL_dsh, a.M, i0, n, sw, basis, cf, active);
+  if (a.dL_dsh_dc != nullptr) sh_store_outer_raw(a.dL_dsh_dc, a.dL_dsh_ac, a.M, i0, n, sw, basis, cf, active);
+  else sh_store_outer(a.dL_dsh, a.M, i0, n, sw, basis, cf, active);
 }
 
 // Per-Gaussian, exact derivative of the forward.
@@ -917,11 +1022,12 @@ __device__ __forceinline__ void exact_gaussian(const BackwardArgs& a, int i, con
   for (int c = 0; c < 3; ++c)
     for (int r = 0; r < 3; ++r) gm[c] += V[4 * c + r] * gt[r];
   // Sigma = M M^T, M = R diag(s)
-  const float w = __ldg(&gv.rotations[4 * gv.gi]), x = __ldg(&gv.rotations[4 * gv.gi + 1]), y = __ldg(&gv.rotations[4 * gv.gi + 2]), z = __ldg(&gv.rotations[4 * gv.gi + 3]);
+  const float4 qr = gv.rotation();
+  const float w = qr.x, x = qr.y, y = qr.z, z = qr.w;
   const float R[3][3] = {{1.f - 2.f * (y * y + z * z), 2.f * (x * y - w * z), 2.f * (x * z + w * y)},
                          {2.f * (x * y + w * z), 1.f - 2.f * (x * x + z * z), 2.f * (y * z - w * x)},
                          {2.f * (x * z - w * y), 2.f * (y * z + w * x), 1.f - 2.f * (x * x + y * y)}};
-  const float s[3] = {__ldg(&gv.scales[3 * gv.gi]), __ldg(&gv.scales[3 * gv.gi + 1]), __ldg(&gv.scales[3 * gv.gi + 2])};
+  const float s[3] = {gv.scale(0), gv.scale(1), gv.scale(2)};
   float dM[3][3];
   for (int p = 0; p < 3; ++p)
     for (int k = 0; k < 3; ++k) {

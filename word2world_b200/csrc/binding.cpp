@@ -218,6 +218,117 @@ std::tuple<Tensor, Tensor> sort_pairs_u64(const Tensor& keys, const Tensor& vals
   return std::make_tuple(ko, vo);
 }
 
+// Renderer.render on raw parameters (Renderer.py:164-192): the activation
+// preamble runs inside the projection pass; outputs as rasterize_gaussians.
+std::tuple<int64_t, Tensor, Tensor, Tensor, Tensor, Tensor, Tensor, Tensor> rasterize_gaussians_raw(
+    const Tensor& means3D, const Tensor& sh_dc, const Tensor& sh_ac, const Tensor& opacity_logit, const Tensor& svec,
+    const Tensor& quaternion, const Tensor& viewmatrix, const Tensor& projmatrix, const Tensor& campos,
+    double focal_x, int64_t degree, int64_t image_height, int64_t image_width, const c10::optional<Tensor>& background,
+    bool compat_spill) {
+  TORCH_CHECK(means3D.dim() == 2 && means3D.size(1) == 3, "means3D must be [P, 3]");
+  const auto dev = means3D.device();
+  const int64_t P = means3D.size(0);
+  c10::cuda::CUDAGuard guard(dev);
+  Tensor m = f32(means3D, "means3D", dev), dc = f32(sh_dc, "sh_dc", dev), ac = f32(sh_ac, "sh_ac", dev);
+  Tensor lo = f32(opacity_logit, "opacity", dev), sv = f32(svec, "svec", dev), q = f32(quaternion, "quaternion", dev);
+  TORCH_CHECK(dc.numel() == 3 * P && ac.dim() == 3 && ac.size(0) == P && ac.size(2) == 3 && ac.size(1) <= 15,
+              "sh_dc [P,1,3] and sh_ac [P,K,3] (K <= 15) expected");
+  TORCH_CHECK(lo.numel() == P && sv.numel() == 3 * P && q.numel() == 4 * P, "opacity [P,1], svec [P,3], quaternion [P,4]");
+  TORCH_CHECK(image_height > 0 && image_width > 0 && degree >= 0 && degree <= 3, "bad image size or degree");
+  const int64_t M = ac.size(1) + 1;
+  Camera cam = camera(viewmatrix, projmatrix, campos, background, dev);
+  const auto fopt = torch::TensorOptions().dtype(torch::kFloat32).device(dev);
+  const auto bopt = torch::TensorOptions().dtype(torch::kUInt8).device(dev);
+  const int W = int(image_width), H = int(image_height);
+  Tensor color = torch::empty({3, H, W}, fopt), depth = torch::empty({1, H, W}, fopt), alpha = torch::empty({1, H, W}, fopt);
+  Tensor radii = torch::empty({P}, torch::TensorOptions().dtype(torch::kInt32).device(dev));
+  Tensor geom = torch::empty({int64_t(w2w_geometry_state_bytes(int(P)))}, bopt);
+  Tensor img = torch::empty({int64_t(w2w_image_state_bytes(W, H))}, bopt);
+  w2w_settings st{};
+  st.P = int(P); st.degree = int(degree); st.M = int(M); st.width = W; st.height = H;
+  st.focal_x = float(focal_x);
+  st.tan_fovx = st.tan_fovy = 1.0f;
+  st.scale_modifier = 1.0f;
+  st.compat_spill = compat_spill ? 1 : 0;
+  st.viewmatrix = cam.view.data_ptr<float>(); st.projmatrix = cam.proj.data_ptr<float>();
+  st.campos = cam.campos.data_ptr<float>(); st.background = cam.bg.data_ptr<float>();
+  w2w_geometry_info info{};
+  const w2w_stream_t stream = cur_stream();
+  {
+    pybind11::gil_scoped_release nogil;
+    check(w2w_forward_geometry_raw(&st, m.data_ptr<float>(), sv.data_ptr<float>(), q.data_ptr<float>(),
+                                   lo.data_ptr<float>(), dc.data_ptr<float>(), ac.data_ptr<float>(),
+                                   radii.data_ptr<int>(), geom.data_ptr(), &info, stream),
+          "w2w_forward_geometry_raw");
+  }
+  const int64_t R = info.num_rendered;
+  Tensor bin = torch::empty({int64_t(w2w_binning_state_bytes(R, W, H))}, bopt);
+  {
+    pybind11::gil_scoped_release nogil;
+    check(w2w_forward_render(&st, geom.data_ptr(), &info, bin.data_ptr(), img.data_ptr(), color.data_ptr<float>(),
+                             depth.data_ptr<float>(), alpha.data_ptr<float>(), stream),
+          "w2w_forward_render");
+  }
+  return std::make_tuple(R, color, depth, alpha, radii, geom, bin, img);
+}
+
+// Gradients of rasterize_gaussians_raw's outputs with respect to its raw
+// parameters (reference formulas): (means2D, means3D, sh_dc, sh_ac, opacity
+// logits, svec, quaternion).
+std::tuple<Tensor, Tensor, Tensor, Tensor, Tensor, Tensor, Tensor> rasterize_gaussians_backward_raw(
+    const Tensor& background, const Tensor& means3D, const Tensor& sh_dc, const Tensor& sh_ac,
+    const Tensor& opacity_logit, const Tensor& svec, const Tensor& quaternion, const Tensor& radii,
+    const Tensor& viewmatrix, const Tensor& projmatrix, const Tensor& campos, double tan_fovx, double tan_fovy,
+    int64_t degree, const Tensor& dL_dout_color, const Tensor& dL_dout_depth, const Tensor& dL_dout_alpha,
+    const Tensor& geomBuffer, int64_t R, const Tensor& binningBuffer, const Tensor& imageBuffer, const Tensor& alpha) {
+  const auto dev = means3D.device();
+  c10::cuda::CUDAGuard guard(dev);
+  const int64_t P = means3D.size(0);
+  Tensor m = f32(means3D, "means3D", dev), dc = f32(sh_dc, "sh_dc", dev), ac = f32(sh_ac, "sh_ac", dev);
+  Tensor lo = f32(opacity_logit, "opacity", dev), sv = f32(svec, "svec", dev), q = f32(quaternion, "quaternion", dev);
+  Tensor g = f32(dL_dout_color, "dL_dout_color", dev);
+  TORCH_CHECK(g.dim() == 3 && g.size(0) == 3, "dL_dout_color must be [3, H, W]");
+  const int H = int(g.size(1)), W = int(g.size(2));
+  Tensor gd = f32(dL_dout_depth, "dL_dout_depth", dev), ga = f32(dL_dout_alpha, "dL_dout_alpha", dev);
+  Tensor al = f32(alpha, "alpha", dev);
+  TORCH_CHECK(gd.numel() == int64_t(H) * W && ga.numel() == int64_t(H) * W && al.numel() == int64_t(H) * W,
+              "depth / alpha gradients and alpha must be [1, H, W]");
+  TORCH_CHECK(radii.is_cuda() && radii.scalar_type() == torch::kInt32 && radii.numel() == P, "radii must be int32 [P]");
+  TORCH_CHECK(geomBuffer.numel() >= int64_t(w2w_geometry_state_bytes(int(P))), "geomBuffer does not match P");
+  TORCH_CHECK(imageBuffer.numel() >= int64_t(w2w_image_state_bytes(W, H)), "imageBuffer does not match H, W");
+  TORCH_CHECK(binningBuffer.numel() >= int64_t(w2w_binning_state_bytes(R, W, H)), "binningBuffer does not match R");
+  Tensor rad = radii.contiguous();
+  const int64_t K = ac.size(1);
+  Camera cam = camera(viewmatrix, projmatrix, campos, background, dev);
+  const auto fopt = torch::TensorOptions().dtype(torch::kFloat32).device(dev);
+  Tensor dmean2D = torch::empty({P, 3}, fopt), dcolors = torch::empty({P, 3}, fopt),
+         dlogit = torch::empty({P, 1}, fopt), dmean3D = torch::empty({P, 3}, fopt),
+         dcov3D = torch::empty({P, 6}, fopt), ddc = torch::empty({P, 1, 3}, fopt), dac = torch::empty({P, K, 3}, fopt),
+         dsvec = torch::empty({P, 3}, fopt), dquat = torch::empty({P, 4}, fopt);
+  Tensor scratch = torch::empty({int64_t(w2w_backward_scratch_bytes(int(P)))},
+                                torch::TensorOptions().dtype(torch::kUInt8).device(dev));
+  w2w_settings st{};
+  st.P = int(P); st.degree = int(degree); st.M = int(K + 1); st.width = W; st.height = H;
+  st.tan_fovx = float(tan_fovx); st.tan_fovy = float(tan_fovy);
+  st.focal_x = float(W / (2.0 * tan_fovx));
+  st.scale_modifier = 1.0f;
+  st.viewmatrix = cam.view.data_ptr<float>(); st.projmatrix = cam.proj.data_ptr<float>();
+  st.campos = cam.campos.data_ptr<float>(); st.background = cam.bg.data_ptr<float>();
+  const w2w_stream_t stream = cur_stream();
+  {
+    pybind11::gil_scoped_release nogil;
+    check(w2w_backward_raw(&st, m.data_ptr<float>(), sv.data_ptr<float>(), q.data_ptr<float>(), lo.data_ptr<float>(),
+                           dc.data_ptr<float>(), ac.data_ptr<float>(), rad.data_ptr<int>(), geomBuffer.data_ptr(), R,
+                           binningBuffer.data_ptr(), imageBuffer.data_ptr(), al.data_ptr<float>(), g.data_ptr<float>(),
+                           gd.data_ptr<float>(), ga.data_ptr<float>(), scratch.data_ptr(), size_t(scratch.numel()),
+                           dmean2D.data_ptr<float>(), dcolors.data_ptr<float>(), dlogit.data_ptr<float>(),
+                           dmean3D.data_ptr<float>(), dcov3D.data_ptr<float>(), ddc.data_ptr<float>(),
+                           dac.data_ptr<float>(), dsvec.data_ptr<float>(), dquat.data_ptr<float>(), stream),
+          "w2w_backward_raw");
+  }
+  return std::make_tuple(dmean2D, dmean3D, ddc, dac, dlogit, dsvec, dquat);
+}
+
 // Renderer.render's activation preamble (Renderer.py:164-167), fused.
 std::tuple<Tensor, Tensor, Tensor, Tensor> activate(const Tensor& opacity_logit, const Tensor& svec,
                                                     const Tensor& quaternion, const Tensor& sh_dc,
@@ -388,6 +499,8 @@ PYBIND11_MODULE(TORCH_EXTENSION_NAME, m) {
   m.def("sort_pairs_u64", &sort_pairs_u64);
   m.def("scan_u32", &scan_u32);
   m.def("activate", &activate);
+  m.def("rasterize_gaussians_raw", &rasterize_gaussians_raw);
+  m.def("rasterize_gaussians_backward_raw", &rasterize_gaussians_backward_raw);
   m.def("densification_stats", &densification_stats);
   m.def("voxel_field", &voxel_field);
   m.def("activate_backward", &activate_backward);

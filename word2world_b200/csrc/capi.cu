@@ -199,12 +199,14 @@ size_t w2w_binning_offset(long long R, int W, int H, const char* name) {
   return size_t(-1);
 }
 
-int w2w_forward_geometry(const w2w_settings* s, const float* means3D, const float* scales, const float* rotations,
-                         const float* opacities, const float* shs, int* radii, void* geom_state,
-                         w2w_geometry_info* info, w2w_stream_t stream) {
-  if (!settings_ok(s) || !info || (s->P > 0 && (!means3D || !scales || !rotations || !opacities || !radii ||
-                                                !geom_state || (s->M > 0 && !shs))))
-    return W2W_ERR_INVALID;
+// raw != null: Renderer.render's raw parameters, activated by preprocess
+struct RawParams {
+  const float *svec, *quat, *logit, *sh_dc, *sh_ac;
+};
+
+static int forward_geometry(const w2w_settings* s, const float* means3D, const float* scales, const float* rotations,
+                            const float* opacities, const float* shs, const RawParams* raw, int* radii,
+                            void* geom_state, w2w_geometry_info* info, w2w_stream_t stream) {
   std::memset(info, 0, sizeof(*info));
   if (s->P == 0) return W2W_OK;
   const GeomLayout L(s->P);
@@ -231,6 +233,9 @@ int w2w_forward_geometry(const w2w_settings* s, const float* means3D, const floa
   a.prev_reach = at<uint32_t>(geom_state, L.prev_reach);
   a.record = at<float>(geom_state, L.record);
   a.bwd_record = at<float>(geom_state, L.bwd_record);
+  if (raw != nullptr) {
+    a.svec = raw->svec; a.quat = raw->quat; a.logit = raw->logit; a.sh_dc = raw->sh_dc; a.sh_ac = raw->sh_ac;
+  }
   launch_preprocess(a, st);
   int rc = check_launch();
   if (rc) return rc;
@@ -245,6 +250,26 @@ int w2w_forward_geometry(const w2w_settings* s, const float* means3D, const floa
   if (h.error & kErrTimeout) return W2W_ERR_TIMEOUT;
   if (h.error & kErrCapacity) return W2W_ERR_CAPACITY;
   return W2W_OK;
+}
+
+int w2w_forward_geometry(const w2w_settings* s, const float* means3D, const float* scales, const float* rotations,
+                         const float* opacities, const float* shs, int* radii, void* geom_state,
+                         w2w_geometry_info* info, w2w_stream_t stream) {
+  if (!settings_ok(s) || !info || (s->P > 0 && (!means3D || !scales || !rotations || !opacities || !radii ||
+                                                !geom_state || (s->M > 0 && !shs))))
+    return W2W_ERR_INVALID;
+  return forward_geometry(s, means3D, scales, rotations, opacities, shs, nullptr, radii, geom_state, info, stream);
+}
+
+int w2w_forward_geometry_raw(const w2w_settings* s, const float* means3D, const float* svec, const float* quaternion,
+                             const float* opacity_logit, const float* sh_dc, const float* sh_ac, int* radii,
+                             void* geom_state, w2w_geometry_info* info, w2w_stream_t stream) {
+  if (!settings_ok(s) || !info || s->M < 1 || s->M > 16 ||
+      (s->P > 0 && (!means3D || !svec || !quaternion || !opacity_logit || !sh_dc || (s->M > 1 && !sh_ac) ||
+                    !radii || !geom_state)))
+    return W2W_ERR_INVALID;
+  const RawParams raw{svec, quaternion, opacity_logit, sh_dc, sh_ac};
+  return forward_geometry(s, means3D, nullptr, nullptr, nullptr, nullptr, &raw, radii, geom_state, info, stream);
 }
 
 int w2w_forward_render(const w2w_settings* s, const void* geom_state, const w2w_geometry_info* info,
@@ -334,20 +359,19 @@ int w2w_state_error(const void* state, int which, w2w_stream_t stream) {
   return int(e);
 }
 
-int w2w_backward(const w2w_settings* s, const float* means3D, const float* scales, const float* rotations,
-                 const float* shs, const int* radii, const void* geom_state,
-                 long long R, const void* binning_state, const void* image_state, const float* out_alpha,
-                 const float* dL_dcolor, const float* dL_ddepth, const float* dL_dalpha, int grad_mode,
-                 void* scratch, size_t scratch_bytes, float* dL_dmeans2D, float* dL_dcolors, float* dL_dopacity,
-                 float* dL_dmeans3D, float* dL_dcov3D, float* dL_dsh, float* dL_dscales, float* dL_drotations,
-                 w2w_stream_t stream) {
-  if (!settings_ok(s) || (grad_mode != 0 && grad_mode != 1)) return W2W_ERR_INVALID;
+struct RawGrads {
+  const float *svec, *quat, *logit, *sh_dc, *sh_ac;
+  float *d_sh_dc, *d_sh_ac;
+};
+
+static int backward_impl(const w2w_settings* s, const float* means3D, const float* scales, const float* rotations,
+                         const float* shs, const RawGrads* raw, const int* radii, const void* geom_state,
+                         long long R, const void* binning_state, const void* image_state, const float* out_alpha,
+                         const float* dL_dcolor, const float* dL_ddepth, const float* dL_dalpha, int grad_mode,
+                         void* scratch, size_t scratch_bytes, float* dL_dmeans2D, float* dL_dcolors,
+                         float* dL_dopacity, float* dL_dmeans3D, float* dL_dcov3D, float* dL_dsh, float* dL_dscales,
+                         float* dL_drotations, w2w_stream_t stream) {
   const int P = s->P;
-  if (P == 0) return W2W_OK;
-  if (!means3D || !scales || !rotations || !radii || !geom_state || !image_state || !out_alpha ||
-      !dL_dcolor || !dL_ddepth || !dL_dalpha || !dL_dmeans2D || !dL_dcolors || !dL_dopacity || !dL_dmeans3D ||
-      !dL_dcov3D || !dL_dscales || !dL_drotations || (s->M > 0 && (!shs || !dL_dsh)) || (R > 0 && !binning_state))
-    return W2W_ERR_INVALID;
   if (!scratch || scratch_bytes < w2w_backward_scratch_bytes(P)) return W2W_ERR_SCRATCH;
   cudaStream_t st = S(stream);
   const int W = s->width, H = s->height;
@@ -385,9 +409,55 @@ int w2w_backward(const w2w_settings* s, const float* means3D, const float* scale
   a.acc_depth = acc_depth;
   a.dL_dmeans3D = dL_dmeans3D; a.dL_dcov3D = dL_dcov3D; a.dL_dsh = dL_dsh; a.dL_dscales = dL_dscales;
   a.dL_drotations = dL_drotations;
+  if (raw != nullptr) {
+    a.svec = raw->svec; a.quat = raw->quat; a.logit = raw->logit; a.sh_dc = raw->sh_dc; a.sh_ac = raw->sh_ac;
+    a.dL_dsh_dc = raw->d_sh_dc; a.dL_dsh_ac = raw->d_sh_ac;
+  }
   if (R > 0) launch_backward_render(a, st);
   launch_backward_gaussians(a, st);
   return check_launch();
+}
+
+int w2w_backward(const w2w_settings* s, const float* means3D, const float* scales, const float* rotations,
+                 const float* shs, const int* radii, const void* geom_state,
+                 long long R, const void* binning_state, const void* image_state, const float* out_alpha,
+                 const float* dL_dcolor, const float* dL_ddepth, const float* dL_dalpha, int grad_mode,
+                 void* scratch, size_t scratch_bytes, float* dL_dmeans2D, float* dL_dcolors, float* dL_dopacity,
+                 float* dL_dmeans3D, float* dL_dcov3D, float* dL_dsh, float* dL_dscales, float* dL_drotations,
+                 w2w_stream_t stream) {
+  if (!settings_ok(s) || (grad_mode != 0 && grad_mode != 1)) return W2W_ERR_INVALID;
+  const int P = s->P;
+  if (P == 0) return W2W_OK;
+  if (!means3D || !scales || !rotations || !radii || !geom_state || !image_state || !out_alpha ||
+      !dL_dcolor || !dL_ddepth || !dL_dalpha || !dL_dmeans2D || !dL_dcolors || !dL_dopacity || !dL_dmeans3D ||
+      !dL_dcov3D || !dL_dscales || !dL_drotations || (s->M > 0 && (!shs || !dL_dsh)) || (R > 0 && !binning_state))
+    return W2W_ERR_INVALID;
+  return backward_impl(s, means3D, scales, rotations, shs, nullptr, radii, geom_state, R, binning_state,
+                       image_state, out_alpha, dL_dcolor, dL_ddepth, dL_dalpha, grad_mode, scratch, scratch_bytes,
+                       dL_dmeans2D, dL_dcolors, dL_dopacity, dL_dmeans3D, dL_dcov3D, dL_dsh, dL_dscales,
+                       dL_drotations, stream);
+}
+
+int w2w_backward_raw(const w2w_settings* s, const float* means3D, const float* svec, const float* quaternion,
+                     const float* opacity_logit, const float* sh_dc, const float* sh_ac, const int* radii,
+                     const void* geom_state, long long R, const void* binning_state, const void* image_state,
+                     const float* out_alpha, const float* dL_dcolor, const float* dL_ddepth, const float* dL_dalpha,
+                     void* scratch, size_t scratch_bytes, float* dL_dmeans2D, float* dL_dcolors,
+                     float* dL_dopacity_logit, float* dL_dmeans3D, float* dL_dcov3D, float* dL_dsh_dc,
+                     float* dL_dsh_ac, float* dL_dsvec, float* dL_dquaternion, w2w_stream_t stream) {
+  if (!settings_ok(s) || s->M < 1 || s->M > 16) return W2W_ERR_INVALID;
+  const int P = s->P;
+  if (P == 0) return W2W_OK;
+  if (!means3D || !svec || !quaternion || !opacity_logit || !sh_dc || (s->M > 1 && (!sh_ac || !dL_dsh_ac)) ||
+      !radii || !geom_state || !image_state || !out_alpha || !dL_dcolor || !dL_ddepth || !dL_dalpha ||
+      !dL_dmeans2D || !dL_dcolors || !dL_dopacity_logit || !dL_dmeans3D || !dL_dcov3D || !dL_dsh_dc || !dL_dsvec ||
+      !dL_dquaternion || (R > 0 && !binning_state))
+    return W2W_ERR_INVALID;
+  const RawGrads raw{svec, quaternion, opacity_logit, sh_dc, sh_ac, dL_dsh_dc, dL_dsh_ac};
+  return backward_impl(s, means3D, nullptr, nullptr, nullptr, &raw, radii, geom_state, R, binning_state, image_state,
+                       out_alpha, dL_dcolor, dL_ddepth, dL_dalpha, 0, scratch, scratch_bytes, dL_dmeans2D,
+                       dL_dcolors, dL_dopacity_logit, dL_dmeans3D, dL_dcov3D, nullptr, dL_dsvec, dL_dquaternion,
+                       stream);
 }
 
 size_t w2w_sort_scratch_bytes(long long n) {

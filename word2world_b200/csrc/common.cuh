@@ -173,6 +173,17 @@ __device__ __forceinline__ float sqrt_approx(float x) {
   return y;
 }
 
+// Renderer.render's activations (Renderer.py:164-167), bit-identical to the
+// torch operations the reference runs on a B200 (checked over 2^24 inputs):
+// sigmoid = 1 / (1 + exp(-x)) with IEEE division; exp; the quaternion divided
+// by max(sqrt((w*w + y*y) + (x*x + z*z)), 1e-12) with every product rounded.
+__device__ __forceinline__ float act_sigmoid(float x) { return __fdiv_rn(1.f, __fadd_rn(1.f, expf(-x))); }
+__device__ __forceinline__ float4 act_normalize(float w, float x, float y, float z) {
+  const float ss = __fadd_rn(__fadd_rn(__fmul_rn(w, w), __fmul_rn(y, y)), __fadd_rn(__fmul_rn(x, x), __fmul_rn(z, z)));
+  const float n = fmaxf(__fsqrt_rn(ss), 1e-12f);
+  return make_float4(__fdiv_rn(w, n), __fdiv_rn(x, n), __fdiv_rn(y, n), __fdiv_rn(z, n));
+}
+
 // Bit b set: the Gaussian may reach alpha >= 1/255 in 8x4 block b of the tile
 // whose top-left pixel is (X0, Y0) (kGroups rows of two blocks: the whole
 // 16x16 tile for kGroups = 4).  hy/beta/gamma/eps/vr as in CullParams.

@@ -75,6 +75,11 @@ struct PreprocessArgs {
   uint32_t* prev_reach;
   float* record;      // BlendRecord[P]
   float* bwd_record;  // BackwardRecord[P]
+  // raw parameters (Renderer.render's, single-view calls only): when svec is
+  // set, scales = exp(svec), rotations = normalize(quat), opacity =
+  // sigmoid(logit) and the SH row is sh_dc followed by sh_ac, computed here
+  // as the reference's torch preamble computes them
+  const float *svec, *quat, *logit, *sh_dc, *sh_ac;
 };
 void launch_preprocess(const PreprocessArgs& a, cudaStream_t stream);
 
@@ -198,6 +203,13 @@ struct BackwardArgs {
   float* dL_dsh;
   float* dL_dscales;
   float* dL_drotations;
+  // raw parameters (the fused-preamble path, reference mode, single view):
+  // when svec is set the per-Gaussian pass activates svec / quat itself, reads
+  // the SH rows from sh_dc and sh_ac, and writes the raw parameters' gradients
+  // (dL_dscales then holds d/dsvec, dL_drotations d/dquat, dL_dopacity
+  // d/dlogit, and dL_dsh_dc / dL_dsh_ac the SH rows split as the inputs)
+  const float *svec, *quat, *logit, *sh_dc, *sh_ac;
+  float *dL_dsh_dc, *dL_dsh_ac;
 };
 void launch_backward_render(const BackwardArgs& a, cudaStream_t stream);
 void launch_backward_gaussians(const BackwardArgs& a, cudaStream_t stream);
@@ -225,8 +237,9 @@ struct ActivateBackwardArgs {
   long long P;
   int K;
   const float *g_opacity, *g_scales, *g_rotations, *g_shs;  // gradients of the activated tensors
-  const float *opacity, *scales, *quat;                      // activated opacity and scales, raw quaternion
+  const float *opacity, *scales, *quat;                      // activated opacity and scales (or null), raw quaternion
   float *d_opacity_logit, *d_svec, *d_quat, *d_sh_dc, *d_sh_ac;
+  const float *opacity_logit, *svec;                         // raw, read when opacity / scales are null
 };
 void launch_activate(const ActivateArgs& a, cudaStream_t stream);
 void launch_activate_backward(const ActivateBackwardArgs& a, cudaStream_t stream);

@@ -229,8 +229,9 @@ __device__ __forceinline__ void sh_colour(const float* __restrict__ sh, int M, i
   for (int k = 0; k < 3; ++k) clamped[k] = rgb[k] < 0.0f ? 1 : 0;
 }
 
-template <bool kSh16>
-// 4 CTAs per SM (64 registers, a few spilled): measured 2 % faster than 3 at 80
+// 4 CTAs per SM (64 registers, a few spilled): measured 2 % faster than 3 at 80.
+// kRaw: the raw parameters of Renderer.render, activated here (PreprocessArgs).
+template <bool kSh16, bool kRaw>
 __global__ void __launch_bounds__(kPreThreads, 4)
 preprocess_kernel(PreprocessArgs a) {
   __shared__ uint32_t s_tile;
@@ -264,10 +265,21 @@ preprocess_kernel(PreprocessArgs a) {
   uint32_t depth_bits = 0;
   if (i < P) {
     const float px = means3D[3 * gi], py = means3D[3 * gi + 1], pz = means3D[3 * gi + 2];
-    const float sx = scales[3 * gi], sy = scales[3 * gi + 1], sz = scales[3 * gi + 2];
-    const float4 q = make_float4(rotations[4 * gi], rotations[4 * gi + 1], rotations[4 * gi + 2],
-                                 rotations[4 * gi + 3]);
-    const float opacity = opacities[gi];
+    float sx, sy, sz, opacity;
+    float4 q;
+    if constexpr (kRaw) {
+      sx = expf(a.svec[3 * gi]);
+      sy = expf(a.svec[3 * gi + 1]);
+      sz = expf(a.svec[3 * gi + 2]);
+      q = act_normalize(a.quat[4 * gi], a.quat[4 * gi + 1], a.quat[4 * gi + 2], a.quat[4 * gi + 3]);
+      opacity = act_sigmoid(a.logit[gi]);
+    } else {
+      sx = scales[3 * gi];
+      sy = scales[3 * gi + 1];
+      sz = scales[3 * gi + 2];
+      q = make_float4(rotations[4 * gi], rotations[4 * gi + 1], rotations[4 * gi + 2], rotations[4 * gi + 3]);
+      opacity = opacities[gi];
+    }
     Geometry g;
     project(view, proj, focal, float(Wd), float(Hd), px, py, pz, sx, sy, sz, q, g);
     float* cov3 = a.cov3D + 6 * size_t(i);
@@ -277,8 +289,17 @@ preprocess_kernel(PreprocessArgs a) {
     // SH colour
     float rgb[3];
     uint8_t clampf[3];
-    const float* shp = shs + size_t(gi) * M * 3;
-    if constexpr (kSh16) {
+    const float* shp = kRaw ? nullptr : shs + size_t(gi) * M * 3;
+    if constexpr (kRaw) {  // the row is sh_dc (3 floats) then sh_ac (3 (M - 1) floats); M <= 16
+      float buf[48];
+      const float* dc = a.sh_dc + 3 * size_t(gi);
+      const float* ac = a.sh_ac + size_t(gi) * 3 * (M - 1);
+#pragma unroll
+      for (int k = 0; k < 3; ++k) buf[k] = __ldg(dc + k);
+#pragma unroll
+      for (int k = 3; k < 48; ++k) buf[k] = k < 3 * M ? __ldg(ac + (k - 3)) : 0.f;
+      sh_colour(buf, M, degree, px, py, pz, campos, rgb, clampf);
+    } else if constexpr (kSh16) {
       float buf[48];
       const float4* s4 = reinterpret_cast<const float4*>(shp);
 #pragma unroll
@@ -503,8 +524,9 @@ void launch_preprocess(const PreprocessArgs& a, cudaStream_t stream) {
   if (blocks == 0) return;
   const bool sh16 = a.M == 16 && (reinterpret_cast<uintptr_t>(a.shs) & 15) == 0;
   stage_begin(kStPreprocess, stream);
-  if (sh16) preprocess_kernel<true><<<blocks, kPreThreads, 0, stream>>>(a);
-  else preprocess_kernel<false><<<blocks, kPreThreads, 0, stream>>>(a);
+  if (a.svec != nullptr) preprocess_kernel<false, true><<<blocks, kPreThreads, 0, stream>>>(a);
+  else if (sh16) preprocess_kernel<true, false><<<blocks, kPreThreads, 0, stream>>>(a);
+  else preprocess_kernel<false, false><<<blocks, kPreThreads, 0, stream>>>(a);
   stage_end(kStPreprocess, stream, 1);
 }
 

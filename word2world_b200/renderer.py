@@ -119,6 +119,40 @@ def activate(opacity_logit, svec, quaternion, sh_dc, sh_ac):
     return _Activate.apply(opacity_logit, svec, quaternion, sh_dc, sh_ac)
 
 
+class _RasterizeRaw(torch.autograd.Function):
+    """``Renderer.render``'s preamble and rasterization in one forward and one
+    backward call on the raw parameters (opacity logits, log-scales,
+    unnormalised quaternions, split SH): the projection pass activates them
+    as it reads them, with the same arithmetic as ``activate`` (the image is
+    bit-identical to ``activate`` followed by ``_render_gaussians_inline``),
+    and the per-Gaussian backward applies the activations' chain rule before
+    it stores.  Reference-formula gradients only."""
+
+    @staticmethod
+    def forward(ctx, means3D, means2D, sh_dc, sh_ac, opacity_logit, svec, quaternion, bg, viewmatrix, projmatrix,
+                tanfovx, tanfovy, sh_degree, campos, image_height, image_width, compat_spill):
+        focal_x = image_width / (2.0 * tanfovx)
+        num_rend, color, depth, alpha, radii, geom, binb, img = _C.rasterize_gaussians_raw(
+            means3D, sh_dc, sh_ac, opacity_logit, svec, quaternion, viewmatrix, projmatrix, campos, focal_x,
+            sh_degree, image_height, image_width, bg, compat_spill)
+        ctx.num_rend = num_rend
+        ctx.bg, ctx.vmat, ctx.pmat, ctx.campos = bg, viewmatrix, projmatrix, campos
+        ctx.fx, ctx.fy, ctx.sh_deg = tanfovx, tanfovy, sh_degree
+        ctx.save_for_backward(means3D, sh_dc, sh_ac, opacity_logit, svec, quaternion, radii, geom, binb, img, alpha)
+        ctx.mark_non_differentiable(radii)
+        return color, radii, depth, alpha
+
+    @staticmethod
+    def backward(ctx, g_color, g_radii, g_depth, g_alpha):
+        means3D, sh_dc, sh_ac, opacity_logit, svec, quaternion, radii, geom, binb, img, alpha = ctx.saved_tensors
+        g_means2D, g_means3D, g_dc, g_ac, g_logit, g_svec, g_quat = _C.rasterize_gaussians_backward_raw(
+            ctx.bg, means3D, sh_dc, sh_ac, opacity_logit, svec, quaternion, radii, ctx.vmat, ctx.pmat, ctx.campos,
+            ctx.fx, ctx.fy, ctx.sh_deg, g_color.contiguous(), g_depth.contiguous(), g_alpha.contiguous(), geom,
+            ctx.num_rend, binb, img, alpha)
+        return (g_means3D, g_means2D, g_dc, g_ac, g_logit, g_svec, g_quat,
+                None, None, None, None, None, None, None, None, None, None)
+
+
 @dataclass
 class GaussianParams:
     """Raw per-Gaussian parameters as structure-of-arrays tensors (the
@@ -195,10 +229,20 @@ class Renderer:
         accum_grads.retain_grad()
         tanfovx = math.tan(float(FoVx) * 0.5)
         tanfovy = math.tan(float(FoVy) * 0.5)
+        bg = torch.ones(3, dtype=torch.float32, device=p.mean.device)
+        if self.grad_mode == "reference":
+            # activation preamble (Renderer.py:164-167) folded into the projection
+            # pass and the per-Gaussian backward
+            image, radii, _, _ = _RasterizeRaw.apply(
+                p.mean, accum_grads, p.sh_dc, p.sh_ac, p.opacity, p.svec, p.quaternion, bg, world_view_transform,
+                full_proj_transform, tanfovx, tanfovy, self.sh_degree, camera_center, int(image_height),
+                int(image_width), bool(self.compat_spill))
+            available = radii > 0
+            return {"image": image, "accum_grads": accum_grads, "avaialble_pts": available,
+                    "available_pts": available}
         # activation preamble (Renderer.py:164-167), one fused kernel each way
         activated_opacity, activated_scales, rotations, shs = activate(p.opacity, p.svec, p.quaternion, p.sh_dc,
                                                                        p.sh_ac)
-        bg = torch.ones(3, dtype=torch.float32, device=p.mean.device)
         image, radii, _, _ = _render_gaussians_inline(
             p.mean, accum_grads, shs, None, activated_opacity, activated_scales, rotations, None, bg, 1,
             world_view_transform, full_proj_transform, tanfovx, tanfovy, self.sh_degree, camera_center, False,
