@@ -232,14 +232,16 @@ struct LookbackWindow {
 
 // Tile shape per key type: keys per thread and resident CTAs per SM (the
 // register budget).  Every tile holds at least kSortTileMin keys.  Measured on
-// a B200: 32-bit keys (the rasterizer's, 5.9M) 16 items at 3 CTAs/SM beat 20
-// and 24 at 2 (0.181 vs 0.184, 0.186 ms per 3 passes); 64-bit keys (20M, 5
-// passes) 20 items at 2 CTAs/SM beat 16 (1.139 vs 1.172 ms).
+// a B200, one 9-bit pass: 32-bit keys (the rasterizer's, 5.9M pairs) 24 items
+// at 2 CTAs/SM 51.7 us, against 20 / 22 / 26 / 28 / 32 at 2 (57.9, 55.6, 55.8,
+// 59.7, 68.0 us) and 16 at 3 (59.8 us); 64-bit keys (20M pairs) 20 items at 2
+// CTAs/SM 174.5 us, against 16 / 24 at 2 (186.8, 203.0 us) and 12 / 16 at 3
+// (218.7, 211.2 us).
 template <typename K>
 struct OnesweepShape;
 template <>
 struct OnesweepShape<uint32_t> {
-  static constexpr int kItems = 16, kMinBlocks = 3;
+  static constexpr int kItems = 24, kMinBlocks = 2;
 };
 template <>
 struct OnesweepShape<uint64_t> {
@@ -250,96 +252,91 @@ __host__ __device__ constexpr int onesweep_tile() { return kSortThreads * Oneswe
 static_assert(onesweep_tile<uint32_t>() >= kSortTileMin && onesweep_tile<uint64_t>() >= kSortTileMin,
               "scratch is sized for tiles of at least kSortTileMin keys");
 
-// kWidth: this pass's digit width (compile-time, so the per-bit ballots unroll).
-template <typename K, int kWidth>
-__global__ void __launch_bounds__(kSortThreads, OnesweepShape<K>::kMinBlocks)
-onesweep_kernel(const K* __restrict__ kin, const uint32_t* __restrict__ vin, K* __restrict__ kout,
-                uint32_t* __restrict__ vout, long long n, int shift,
-                const uint32_t* __restrict__ digit_base, uint32_t* status, uint32_t* counter, uint32_t* err) {
-  constexpr int kWarps = kSortThreads / 32;
-  constexpr int kSortItems = OnesweepShape<K>::kItems;
-  constexpr int kSortTile = onesweep_tile<K>();
-  static_assert(kSortThreads * 2 >= kMaxBins, "at most two digits per thread");
-  __shared__ uint32_t s_wcnt[kWarps][kMaxBins];
-  __shared__ uint32_t s_excl[kMaxBins];
-  __shared__ uint32_t s_gofs[kMaxBins];
-  __shared__ uint32_t s_warp[32];
-  __shared__ uint32_t s_tile;
-  extern __shared__ __align__(16) unsigned char s_dyn[];
-  K* s_keys = reinterpret_cast<K*>(s_dyn);
-  uint32_t* s_vals = reinterpret_cast<uint32_t*>(s_dyn + sizeof(K) * kSortTile);
+template <typename K>
+struct OnesweepShared {
+  uint32_t wcnt[kSortThreads / 32][kMaxBins];  // per-warp digit counts, then each warp's base within the digit
+  uint32_t excl[kMaxBins];                     // digit's first slot in the tile
+  uint32_t gofs[kMaxBins];                     // output index of the digit's slot 0 (mod 2^32)
+  uint32_t warp_sums[32];
+  uint32_t tile;
+};
 
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+// One tile of a pass.  kFull: every key of the tile exists (all tiles but the
+// last), so the per-key bounds checks drop out.  Indices are 32-bit (n < 2^30).
+template <typename K, int kWidth, bool kFull>
+__device__ __forceinline__ void onesweep_tile_pass(const K* __restrict__ kin, const uint32_t* __restrict__ vin,
+                                                   K* __restrict__ kout, uint32_t* __restrict__ vout, uint32_t n,
+                                                   int shift, const uint32_t* __restrict__ digit_base,
+                                                   uint32_t* status, uint32_t* err, uint32_t tile,
+                                                   OnesweepShared<K>& sm, K* s_keys, uint32_t* s_vals) {
+  constexpr int kWarps = kSortThreads / 32;
+  constexpr int kItems = OnesweepShape<K>::kItems;
+  constexpr int kTile = onesweep_tile<K>();
   constexpr int bins = 1 << kWidth;
   const uint32_t dmask = uint32_t(bins) - 1u;
-  if (tid == 0) s_tile = atomicAdd(counter, 1u);
-  for (int i = tid; i < kWarps * kMaxBins; i += kSortThreads) (&s_wcnt[0][0])[i] = 0u;
-  __syncthreads();
-  const long long tile = s_tile;
-  const long long base = tile * kSortTile;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const uint32_t base = tile * uint32_t(kTile);
+  const uint32_t wbase = base + uint32_t(warp * 32 * kItems + lane);  // item i: wbase + 32 i
 
-  K k[kSortItems];
-  uint32_t v[kSortItems];
-  uint32_t rank[kSortItems];
+  K k[kItems];
+  uint32_t v[kItems];
+  uint32_t rank[kItems];
   const uint32_t lt = lanemask_lt();
 #pragma unroll
-  for (int i = 0; i < kSortItems; ++i) {
-    const long long idx = base + warp * (32 * kSortItems) + i * 32 + lane;
-    const bool valid = idx < n;
-    k[i] = valid ? kin[idx] : K(0);
-    v[i] = valid ? vin[idx] : 0u;
+  for (int i = 0; i < kItems; ++i) {
+    const uint32_t idx = wbase + uint32_t(i * 32);
+    if (kFull || idx < n) {
+      k[i] = __ldg(kin + idx);
+      v[i] = __ldg(vin + idx);
+    } else {
+      k[i] = K(0);
+      v[i] = 0u;
+    }
   }
   // early counts: per-warp digit histograms, so the tile's counts are
   // published before the ranking and successors find them sooner
 #pragma unroll
-  for (int i = 0; i < kSortItems; ++i) {
-    const long long idx = base + warp * (32 * kSortItems) + i * 32 + lane;
-    if (idx < n) atomicAdd(&s_wcnt[warp][uint32_t(k[i] >> shift) & dmask], 1u);
-  }
+  for (int i = 0; i < kItems; ++i)
+    if (kFull || wbase + uint32_t(i * 32) < n) atomicAdd(&sm.wcnt[warp][uint32_t(k[i] >> shift) & dmask], 1u);
   __syncthreads();
 
   // two adjacent digits per thread: exclusive over warps (each warp's base
   // within the digit), tile counts, publish
-  const int d0 = 2 * tid, d1 = 2 * tid + 1;
+  const int d0 = 2 * tid;
   uint32_t c0 = 0, c1 = 0;
   if (d0 < bins) {
 #pragma unroll
     for (int w = 0; w < kWarps; ++w) {
-      const uint32_t x0 = s_wcnt[w][d0], x1 = s_wcnt[w][d1];
-      s_wcnt[w][d0] = c0;
-      s_wcnt[w][d1] = c1;
-      c0 += x0;
-      c1 += x1;
+      uint2* p = reinterpret_cast<uint2*>(&sm.wcnt[w][d0]);
+      const uint2 x = *p;
+      *p = make_uint2(c0, c1);
+      c0 += x.x;
+      c1 += x.y;
     }
     const uint32_t flag = tile == 0 ? kStatInc : kStatAgg;
-    st_relaxed64(reinterpret_cast<unsigned long long*>(status + tile * kMaxBins + d0),
+    st_relaxed64(reinterpret_cast<unsigned long long*>(status + size_t(tile) * kMaxBins + d0),
                  (uint64_t(flag | c1) << 32) | (flag | c0));
   }
-  const uint32_t excl = block_exclusive_scan(c0 + c1, s_warp, nullptr);  // ends with a barrier
-  if (d0 < bins) {
-    s_excl[d0] = excl;
-    s_excl[d1] = excl + c0;
-  }
+  const uint32_t excl = block_exclusive_scan(c0 + c1, sm.warp_sums, nullptr);  // ends with a barrier
+  if (d0 < bins) *reinterpret_cast<uint2*>(sm.excl + d0) = make_uint2(excl, excl + c0);
 
   // stable rank within the tile's digit: warp base + earlier items of the warp
   // + earlier lanes of this item holding the same digit (one ballot per digit
   // bit: constant cost whatever the number of distinct digits)
 #pragma unroll
-  for (int i = 0; i < kSortItems; ++i) {
-    const long long idx = base + warp * (32 * kSortItems) + i * 32 + lane;
-    const bool valid = idx < n;
+  for (int i = 0; i < kItems; ++i) {
     const uint32_t d = uint32_t(k[i] >> shift) & dmask;
-    uint32_t pm = __ballot_sync(0xffffffffu, valid);
+    const bool valid = kFull || wbase + uint32_t(i * 32) < n;
+    uint32_t pm = kFull ? 0xffffffffu : __ballot_sync(0xffffffffu, valid);
 #pragma unroll
     for (int bt = 0; bt < kWidth; ++bt) {
-      const bool bit = (d >> bt) & 1u;
-      const uint32_t bal = __ballot_sync(0xffffffffu, bit);
-      pm &= bit ? bal : ~bal;
+      const uint32_t bal = __ballot_sync(0xffffffffu, (d >> bt) & 1u);
+      pm &= ((d >> bt) & 1u) ? bal : ~bal;
     }
-    const uint32_t before = valid ? s_wcnt[warp][d] : 0u;
+    const uint32_t before = valid ? sm.wcnt[warp][d] : 0u;
     rank[i] = before + __popc(pm & lt);
     __syncwarp();
-    if (valid && lane == __ffs(pm) - 1) s_wcnt[warp][d] = before + __popc(pm);
+    if (valid && lane == __ffs(pm) - 1) sm.wcnt[warp][d] = before + __popc(pm);
     __syncwarp();
   }
 
@@ -351,36 +348,63 @@ onesweep_kernel(const K* __restrict__ kin, const uint32_t* __restrict__ vin, K* 
       const uint2 a = lookback_pair<LookbackWindow<K>::value>(status, tile, d0, err);
       a0 = a.x;
       a1 = a.y;
-      st_relaxed64(reinterpret_cast<unsigned long long*>(status + tile * kMaxBins + d0),
+      st_relaxed64(reinterpret_cast<unsigned long long*>(status + size_t(tile) * kMaxBins + d0),
                    (uint64_t(kStatInc | (a1 + c1)) << 32) | (kStatInc | (a0 + c0)));
     }
-    s_gofs[d0] = digit_base[d0] + a0;
-    s_gofs[d1] = digit_base[d1] + a1;
+    const uint2 ex = *reinterpret_cast<const uint2*>(sm.excl + d0);
+    // sorted slot j of digit d goes to gofs[d] + j
+    *reinterpret_cast<uint2*>(sm.gofs + d0) = make_uint2(digit_base[d0] + a0 - ex.x, digit_base[d0 + 1] + a1 - ex.y);
   }
   __syncthreads();
 #pragma unroll
-  for (int i = 0; i < kSortItems; ++i) {
-    const long long idx = base + warp * (32 * kSortItems) + i * 32 + lane;
-    if (idx < n) {
-      const uint32_t d = uint32_t(k[i] >> shift) & dmask;
-      const uint32_t pos = s_excl[d] + rank[i];
+  for (int i = 0; i < kItems; ++i) {
+    if (kFull || wbase + uint32_t(i * 32) < n) {
+      const uint32_t pos = sm.excl[uint32_t(k[i] >> shift) & dmask] + rank[i];
       s_keys[pos] = k[i];
       s_vals[pos] = v[i];
     }
   }
   __syncthreads();
-  const int nvalid = int(min((long long)kSortTile, n - base));
+  const int nvalid = kFull ? kTile : int(min(uint32_t(kTile), n - base));
+#pragma unroll 4
   for (int j = tid; j < nvalid; j += kSortThreads) {
     const K key = s_keys[j];
-    const uint32_t d = uint32_t(key >> shift) & dmask;
-    const long long out = (long long)s_gofs[d] + (j - (long long)s_excl[d]);
-    if (out >= 0 && out < n) {
+    const uint32_t out = sm.gofs[uint32_t(key >> shift) & dmask] + uint32_t(j);
+    if (out < n) {
       kout[out] = key;
       vout[out] = s_vals[j];
     } else {
       atomicOr(err, kErrRange);
     }
   }
+}
+
+// kWidth: this pass's digit width (compile-time, so the per-bit ballots unroll).
+template <typename K, int kWidth>
+__global__ void __launch_bounds__(kSortThreads, OnesweepShape<K>::kMinBlocks)
+onesweep_kernel(const K* __restrict__ kin, const uint32_t* __restrict__ vin, K* __restrict__ kout,
+                uint32_t* __restrict__ vout, long long n, int shift,
+                const uint32_t* __restrict__ digit_base, uint32_t* status, uint32_t* counter, uint32_t* err) {
+  constexpr int kTile = onesweep_tile<K>();
+  static_assert(kSortThreads * 2 >= kMaxBins, "at most two digits per thread");
+  __shared__ __align__(16) OnesweepShared<K> sm;
+  extern __shared__ __align__(16) unsigned char s_dyn[];
+  K* s_keys = reinterpret_cast<K*>(s_dyn);
+  uint32_t* s_vals = reinterpret_cast<uint32_t*>(s_dyn + sizeof(K) * kTile);
+  if (threadIdx.x == 0) sm.tile = atomicAdd(counter, 1u);
+  {
+    uint4* z = reinterpret_cast<uint4*>(&sm.wcnt[0][0]);
+    for (int i = threadIdx.x; i < int(sizeof(sm.wcnt) / 16); i += kSortThreads) z[i] = make_uint4(0u, 0u, 0u, 0u);
+  }
+  __syncthreads();
+  const uint32_t tile = sm.tile;
+  const uint32_t nn = uint32_t(n);  // n < 2^30 (checked by every caller)
+  if ((unsigned long long)(tile + 1) * kTile <= nn)
+    onesweep_tile_pass<K, kWidth, true>(kin, vin, kout, vout, nn, shift, digit_base, status, err, tile, sm, s_keys,
+                                        s_vals);
+  else
+    onesweep_tile_pass<K, kWidth, false>(kin, vin, kout, vout, nn, shift, digit_base, status, err, tile, sm, s_keys,
+                                         s_vals);
 }
 
 template <typename K, int kWidth>
