@@ -299,8 +299,9 @@ def run_e2e(a, sc, cams, device, world):
     h2d = sum(g.numel() * 4 for g in host_g) + sum(sum(x.numel() * 4 for x in c) for c in host_c)
     loss_host = torch.empty(a.views, dtype=torch.float32).pin_memory()
 
-    # the step's inputs are copied on a side stream, all views' at the step's
-    # start, so that view v's copy overlaps the rendering of views < v
+    # the step's inputs are copied on a side stream at the step's start: all
+    # cameras first (a view's render needs only its camera), then the image
+    # gradients (needed only by its loss), so every copy overlaps rendering
     copy_stream = torch.cuda.Stream(device=device)
     main_stream = torch.cuda.current_stream(device)
 
@@ -308,21 +309,28 @@ def run_e2e(a, sc, cams, device, world):
         for p_ in params.parameters():
             p_.grad = None
         copy_stream.wait_stream(main_stream)  # the previous step is done with the buffers
-        staged = []
+        cams_dev, grads_dev = [], []
         with torch.cuda.stream(copy_stream):
             for v in range(len(cams)):
-                g = host_g[v].to(device, non_blocking=True)
                 VPC = tuple(x.to(device, non_blocking=True) for x in host_c[v])
                 ev = torch.cuda.Event()
                 ev.record(copy_stream)
-                staged.append((g, VPC, ev))
+                cams_dev.append((VPC, ev))
+            for v in range(len(cams)):
+                g = host_g[v].to(device, non_blocking=True)
+                ev = torch.cuda.Event()
+                ev.record(copy_stream)
+                grads_dev.append((g, ev))
         losses = []
         for v, c in enumerate(cams):
-            g, (V, Pm, C), ev = staged[v]
-            main_stream.wait_event(ev)
-            for x in (g, V, Pm, C):
+            (V, Pm, C), ev_c = cams_dev[v]
+            g, ev_g = grads_dev[v]
+            main_stream.wait_event(ev_c)
+            for x in (V, Pm, C):
                 x.record_stream(main_stream)
             out = r.render(c.fovx, c.fovy, V, Pm, C, a.res, a.res)
+            main_stream.wait_event(ev_g)
+            g.record_stream(main_stream)
             loss = (out["image"] * g).sum()
             loss.backward()
             losses.append(loss.detach())

@@ -221,6 +221,7 @@ class Renderer:
         self.sh_degree = sh_degree
         self.grad_mode = grad_mode
         self.compat_spill = compat_spill
+        self._bg = None  # the white background (Renderer.py:169), kept across calls
 
     def render(self, FoVx, FoVy, world_view_transform, full_proj_transform, camera_center, image_width,
                image_height):
@@ -229,7 +230,9 @@ class Renderer:
         accum_grads.retain_grad()
         tanfovx = math.tan(float(FoVx) * 0.5)
         tanfovy = math.tan(float(FoVy) * 0.5)
-        bg = torch.ones(3, dtype=torch.float32, device=p.mean.device)
+        if self._bg is None or self._bg.device != p.mean.device:
+            self._bg = torch.ones(3, dtype=torch.float32, device=p.mean.device)
+        bg = self._bg
         if self.grad_mode == "reference":
             # activation preamble (Renderer.py:164-167) folded into the projection
             # pass and the per-Gaussian backward
