@@ -649,14 +649,20 @@ struct GView {
   const float* svec = nullptr;  // raw scales / quaternions (then scales / rotations are unused)
   const float* quat = nullptr;
 
-  // the activated scale k and rotation (w, x, y, z)
+  // the activated scale k and rotation (w, x, y, z).  The raw path's
+  // rotation multiplies by the reciprocal of the clamped norm (the forward
+  // divides, bit-exact with torch; here it only enters gradients, and the two
+  // differ by at most an ulp)
   __device__ __forceinline__ float scale(int k) const {
     return svec != nullptr ? expf(__ldg(&svec[3 * gi + k])) : __ldg(&scales[3 * gi + k]);
   }
   __device__ __forceinline__ float4 rotation() const {
-    if (quat != nullptr)
-      return act_normalize(__ldg(&quat[4 * gi]), __ldg(&quat[4 * gi + 1]), __ldg(&quat[4 * gi + 2]),
-                           __ldg(&quat[4 * gi + 3]));
+    if (quat != nullptr) {
+      const float w = __ldg(&quat[4 * gi]), x = __ldg(&quat[4 * gi + 1]), y = __ldg(&quat[4 * gi + 2]),
+                  z = __ldg(&quat[4 * gi + 3]);
+      const float inv = __frcp_rn(fmaxf(sqrtf((w * w + y * y) + (x * x + z * z)), 1e-12f));
+      return make_float4(w * inv, x * inv, y * inv, z * inv);
+    }
     return make_float4(__ldg(&rotations[4 * gi]), __ldg(&rotations[4 * gi + 1]), __ldg(&rotations[4 * gi + 2]),
                        __ldg(&rotations[4 * gi + 3]));
   }
@@ -846,8 +852,8 @@ __device__ __forceinline__ void ref_gaussian(const BackwardArgs& a, int i, const
   const float xx = qx * qx, yy = qy * qy, zz = qz * qz;
   const float qxy = qx * qy, qxz = qx * qz, qyz = qy * qz;
   const float xw = qx * qw, yw = qy * qw, zw = qz * qw;
-  const float sx = gv.scale_modifier * gv.scale(0), sy = gv.scale_modifier * gv.scale(1),
-              sz = gv.scale_modifier * gv.scale(2);
+  const float sc[3] = {gv.scale(0), gv.scale(1), gv.scale(2)};
+  const float sx = gv.scale_modifier * sc[0], sy = gv.scale_modifier * sc[1], sz = gv.scale_modifier * sc[2];
   const float m11 = sx * (1.f - 2.f * (yy + zz)), m12 = sx * 2.f * (qxy - zw), m13 = sx * 2.f * (qxz + yw);
   const float m21 = sy * 2.f * (qxy + zw), m22 = sy * (1.f - 2.f * (xx + zz)), m23 = sy * 2.f * (qyz - xw);
   const float m31 = sz * 2.f * (qxz - yw), m32 = sz * 2.f * (qyz + xw), m33 = sz * (1.f - 2.f * (xx + yy));
@@ -865,7 +871,7 @@ __device__ __forceinline__ void ref_gaussian(const BackwardArgs& a, int i, const
                  2.f * (qxy + zw) * a21 + (1.f - 2.f * (xx + zz)) * a22 + 2.f * (qyz - xw) * a23,
                  2.f * (qxz - yw) * a31 + 2.f * (qyz + xw) * a32 + (1.f - 2.f * (xx + yy)) * a33};
   if (gv.svec != nullptr)  // raw path: scales = exp(svec)
-    for (int k = 0; k < 3; ++k) ds[k] = ds[k] * gv.scale(k);
+    for (int k = 0; k < 3; ++k) ds[k] = ds[k] * sc[k];
   a.dL_dscales[3 * i] = ds[0];
   a.dL_dscales[3 * i + 1] = ds[1];
   a.dL_dscales[3 * i + 2] = ds[2];
@@ -879,7 +885,7 @@ __device__ __forceinline__ void ref_gaussian(const BackwardArgs& a, int i, const
                 q2 = __ldg(&gv.quat[4 * gv.gi + 2]), q3 = __ldg(&gv.quat[4 * gv.gi + 3]);
     const float n = sqrtf(q0 * q0 + q1 * q1 + q2 * q2 + q3 * q3);
     if (n > 1e-12f) {  // (g - r (r . g)) / n with r = q / n
-      const float inv = 1.f / n;
+      const float inv = __frcp_rn(n);
       const float rg = (q0 * dq.x + q1 * dq.y + q2 * dq.z + q3 * dq.w) * inv;
       dq = make_float4((dq.x - q0 * inv * rg) * inv, (dq.y - q1 * inv * rg) * inv, (dq.z - q2 * inv * rg) * inv,
                        (dq.w - q3 * inv * rg) * inv);
@@ -938,7 +944,7 @@ __global__ void __launch_bounds__(kGaussThreads, 8) gaussians_ref_kernel(Backwar
   }
   // raw path: the accumulated opacity gradient through opacity = sigmoid(logit)
   if (a.logit != nullptr && lane < n) {
-    const float y = act_sigmoid(__ldg(&a.logit[i]));
+    const float y = __frcp_rn(1.f + expf(-__ldg(&a.logit[i])));  // sigmoid, within an ulp of the forward's
     a.dL_dopacity[i] = a.dL_dopacity[i] * (1.f - y) * y;
   }
   // dL_dsh[k][ch] = basis[k] * cf[ch] for the first min(M, 16) bands, 0 beyond
