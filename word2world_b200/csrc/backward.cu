@@ -504,9 +504,56 @@ __device__ __forceinline__ int sh_stride(int M) {
 
 // Rows [i0, i0 + n) of shs ([P, M, 3]), first min(M, 16) coefficients, into
 // s (row g at g * stride).  Warp-collective.
+__device__ __forceinline__ bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0u; }
+
+// Vector forms for a full warp of degree-3 rows (M == 16): the warp's rows are
+// one contiguous span, moved as float4s (coalesced 16-byte accesses; the span
+// starts on a 16-byte boundary when the tensor does, since i0 is a multiple of
+// 32), each float4's four elements placed by one division per float4.
+constexpr int kVecBatch = 4;  // float4 loads in flight per lane
+
+// Scatter float4 number f of a span of rows of `len` floats (row g's element c
+// to s[g * stride + off + c]).
+__device__ __forceinline__ void scatter4(float* s, int stride, int len, int off, int f, float4 v) {
+  int g = (4 * f) / len, c = 4 * f - g * len;
+  const float x[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+  for (int w = 0; w < 4; ++w) {
+    s[g * stride + off + c] = x[w];
+    if (++c == len) {
+      c = 0;
+      ++g;
+    }
+  }
+}
+
+// Stage the span of 32 rows of `len` floats at src (nf = 8 len float4s).
+__device__ __forceinline__ void stage_span(const float* src, int len, float* s, int stride, int off) {
+  const int lane = threadIdx.x & 31, nf = 8 * len;
+  const float4* q = reinterpret_cast<const float4*>(src);
+  for (int f0 = 0; f0 < nf; f0 += 32 * kVecBatch) {
+    float4 v[kVecBatch];
+#pragma unroll
+    for (int u = 0; u < kVecBatch; ++u) {
+      const int f = f0 + 32 * u + lane;
+      v[u] = f < nf ? __ldg(q + f) : make_float4(0.f, 0.f, 0.f, 0.f);
+    }
+#pragma unroll
+    for (int u = 0; u < kVecBatch; ++u) {
+      const int f = f0 + 32 * u + lane;
+      if (f < nf) scatter4(s, stride, len, off, f, v[u]);
+    }
+  }
+}
+
 __device__ __forceinline__ void sh_stage_in(const float* shs, int M, int i0, int n, float* s, int stride) {
   constexpr int kInFlight = 8;  // loads issued before their stores
   const int rs = 3 * (M < 16 ? M : 16), rg = 3 * M, lane = threadIdx.x & 31;
+  if (M == 16 && n == 32 && aligned16(shs)) {
+    stage_span(shs + size_t(i0) * 48, 48, s, stride, 0);
+    __syncwarp();
+    return;
+  }
   if (rs > 0) {
     const int total = n * rs;
     int g = 0, c = lane;
@@ -530,6 +577,28 @@ __device__ __forceinline__ void sh_stage_in(const float* shs, int M, int i0, int
   __syncwarp();
 }
 
+// Write the span of 32 rows of `len` floats at dst: row g's element c is
+// coefficient (c + off) / 3, channel (c + off) % 3 of Gaussian g, the product of
+// its basis value and colour factor in s (row g at g * 21: 16 basis, 3 factors).
+__device__ __forceinline__ void store_span(float* dst, int len, const float* s, int off) {
+  const int lane = threadIdx.x & 31, nf = 8 * len;
+  float4* q = reinterpret_cast<float4*>(dst);
+  for (int f = lane; f < nf; f += 32) {
+    int g = (4 * f) / len, c = 4 * f - g * len;
+    float o[4];
+#pragma unroll
+    for (int w = 0; w < 4; ++w) {
+      const int e = c + off, k = e / 3, ch = e - 3 * k;
+      o[w] = s[g * 21 + k] * s[g * 21 + 16 + ch];
+      if (++c == len) {
+        c = 0;
+        ++g;
+      }
+    }
+    q[f] = make_float4(o[0], o[1], o[2], o[3]);
+  }
+}
+
 // dsh rows [i0, i0 + n) ([P, M, 3]) = basis[k] * cf[ch] (k < 16; 0 beyond),
 // written contiguously; each thread's factors pass through s.  Warp-collective.
 __device__ __forceinline__ void sh_store_outer(float* dsh, int M, int i0, int n, float* s, const float (&basis)[16],
@@ -542,6 +611,10 @@ __device__ __forceinline__ void sh_store_outer(float* dsh, int M, int i0, int n,
 #pragma unroll
   for (int ch = 0; ch < 3; ++ch) s[lane * kRow + 16 + ch] = active ? cf[ch] : 0.f;
   __syncwarp();
+  if (M == 16 && n == 32 && aligned16(dsh)) {
+    store_span(dsh + size_t(i0) * 48, 48, s, 0);
+    return;
+  }
   if (rg > 0) {
     constexpr int kInFlight = 8;
     const int total = n * rg;
@@ -572,6 +645,12 @@ __device__ __forceinline__ void sh_stage_in_raw(const float* dc, const float* ac
                                                 int stride) {
   constexpr int kInFlight = 8;
   const int rs = 3 * (M < 16 ? M : 16), ra = 3 * (M - 1), lane = threadIdx.x & 31;
+  if (M == 16 && n == 32 && aligned16(dc) && aligned16(ac)) {
+    stage_span(dc + size_t(i0) * 3, 3, s, stride, 0);
+    stage_span(ac + size_t(i0) * 45, 45, s, stride, 3);
+    __syncwarp();
+    return;
+  }
   if (rs > 0) {
     const int total = n * rs;
     int g = 0, c = lane;
@@ -606,6 +685,11 @@ __device__ __forceinline__ void sh_store_outer_raw(float* ddc, float* dac, int M
 #pragma unroll
   for (int ch = 0; ch < 3; ++ch) s[lane * kRow + 16 + ch] = active ? cf[ch] : 0.f;
   __syncwarp();
+  if (M == 16 && n == 32 && aligned16(ddc) && aligned16(dac)) {
+    store_span(ddc + size_t(i0) * 3, 3, s, 0);
+    store_span(dac + size_t(i0) * 45, 45, s, 3);
+    return;
+  }
   if (rg > 0) {
     constexpr int kInFlight = 8;
     const int total = n * rg;
