@@ -495,7 +495,6 @@ __global__ void __launch_bounds__(kBlendThreads, 2) render_exact_kernel(Backward
 // 192-byte-strided row per thread.
 // ---------------------------------------------------------------------------
 constexpr int kGaussThreads = 128;
-constexpr int kShStride = 49;  // odd row stride: row reads by 32 threads hit 32 banks
 
 __device__ __forceinline__ int sh_stride(int M) {
   const int r = 3 * (M < 16 ? M : 16);
@@ -504,48 +503,6 @@ __device__ __forceinline__ int sh_stride(int M) {
 
 // Rows [i0, i0 + n) of shs ([P, M, 3]), first min(M, 16) coefficients, into
 // s (row g at g * stride).  Warp-collective.
-__device__ __forceinline__ bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0u; }
-
-// Vector forms for a full warp of degree-3 rows (M == 16): the warp's rows are
-// one contiguous span, moved as float4s (coalesced 16-byte accesses; the span
-// starts on a 16-byte boundary when the tensor does, since i0 is a multiple of
-// 32), each float4's four elements placed by one division per float4.
-constexpr int kVecBatch = 4;  // float4 loads in flight per lane
-
-// Scatter float4 number f of a span of rows of `len` floats (row g's element c
-// to s[g * stride + off + c]).
-__device__ __forceinline__ void scatter4(float* s, int stride, int len, int off, int f, float4 v) {
-  int g = (4 * f) / len, c = 4 * f - g * len;
-  const float x[4] = {v.x, v.y, v.z, v.w};
-#pragma unroll
-  for (int w = 0; w < 4; ++w) {
-    s[g * stride + off + c] = x[w];
-    if (++c == len) {
-      c = 0;
-      ++g;
-    }
-  }
-}
-
-// Stage the span of 32 rows of `len` floats at src (nf = 8 len float4s).
-__device__ __forceinline__ void stage_span(const float* src, int len, float* s, int stride, int off) {
-  const int lane = threadIdx.x & 31, nf = 8 * len;
-  const float4* q = reinterpret_cast<const float4*>(src);
-  for (int f0 = 0; f0 < nf; f0 += 32 * kVecBatch) {
-    float4 v[kVecBatch];
-#pragma unroll
-    for (int u = 0; u < kVecBatch; ++u) {
-      const int f = f0 + 32 * u + lane;
-      v[u] = f < nf ? __ldg(q + f) : make_float4(0.f, 0.f, 0.f, 0.f);
-    }
-#pragma unroll
-    for (int u = 0; u < kVecBatch; ++u) {
-      const int f = f0 + 32 * u + lane;
-      if (f < nf) scatter4(s, stride, len, off, f, v[u]);
-    }
-  }
-}
-
 __device__ __forceinline__ void sh_stage_in(const float* shs, int M, int i0, int n, float* s, int stride) {
   constexpr int kInFlight = 8;  // loads issued before their stores
   const int rs = 3 * (M < 16 ? M : 16), rg = 3 * M, lane = threadIdx.x & 31;

@@ -231,12 +231,18 @@ __device__ __forceinline__ void sh_colour(const float* __restrict__ sh, int M, i
 
 // 4 CTAs per SM (64 registers, a few spilled): measured 2 % faster than 3 at 80.
 // kRaw: the raw parameters of Renderer.render, activated here (PreprocessArgs).
-template <bool kSh16, bool kRaw>
+// kStage: degree-3 rows (M == 16) of a full warp are staged through shared
+// memory as coalesced float4 spans (dynamic shared memory, kStageBytes) instead
+// of each thread gathering its own 192-byte row.
+constexpr int kStageBytes = kPreThreads * kShStride * 4;
+
+template <bool kSh16, bool kRaw, bool kStage>
 __global__ void __launch_bounds__(kPreThreads, 4)
 preprocess_kernel(PreprocessArgs a) {
   __shared__ uint32_t s_tile;
   __shared__ Pair s_warp[kPreThreads / 32];
   __shared__ Pair s_prefix;
+  extern __shared__ __align__(16) float s_rows[];
   GeomHeader* hdr = a.header;
   if (threadIdx.x == 0) s_tile = atomicAdd(&hdr->scan_tile_counter, 1u);
   __syncthreads();
@@ -260,6 +266,22 @@ preprocess_kernel(PreprocessArgs a) {
     focal = it.focal_x;
   }
   const int gw = (Wd + kTile - 1) / kTile, gh = (Hd + kTile - 1) / kTile;
+
+  // this warp's SH rows, staged when all 32 of its Gaussians exist
+  const int i0 = int(tile) * kPreThreads + int(threadIdx.x & ~31u);
+  const bool staged = kStage && i0 + 32 <= P;  // warp-uniform
+  const float* srow = s_rows + int(threadIdx.x >> 5) * 32 * kShStride;
+  if (staged) {
+    float* w = s_rows + int(threadIdx.x >> 5) * 32 * kShStride;
+    if (kRaw) {
+      stage_span(a.sh_dc + size_t(i0) * 3, 3, w, kShStride, 0);
+      stage_span(a.sh_ac + size_t(i0) * 45, 45, w, kShStride, 3);
+    } else {
+      stage_span(a.shs + size_t(i0) * 48, 48, w, kShStride, 0);
+    }
+    __syncwarp();
+  }
+  srow += int(threadIdx.x & 31) * kShStride;
 
   uint32_t alloc = 0, emit = 0;
   uint32_t depth_bits = 0;
@@ -290,14 +312,18 @@ preprocess_kernel(PreprocessArgs a) {
     float rgb[3];
     uint8_t clampf[3];
     const float* shp = kRaw ? nullptr : shs + size_t(gi) * M * 3;
-    if constexpr (kRaw) {  // the row is sh_dc (3 floats) then sh_ac (3 (M - 1) floats); M <= 16
+    if (staged) {
+      sh_colour(srow, 16, degree, px, py, pz, campos, rgb, clampf);
+    } else if constexpr (kRaw) {  // the row is sh_dc (3 floats) then sh_ac (3 (M - 1) floats); M <= 16
       float buf[48];
       const float* dc = a.sh_dc + 3 * size_t(gi);
       const float* ac = a.sh_ac + size_t(gi) * 3 * (M - 1);
+      // only the coefficients the degree uses: (degree + 1)^2 of the M stored
+      const int used = 3 * min(M, (degree + 1) * (degree + 1));
 #pragma unroll
       for (int k = 0; k < 3; ++k) buf[k] = __ldg(dc + k);
 #pragma unroll
-      for (int k = 3; k < 48; ++k) buf[k] = k < 3 * M ? __ldg(ac + (k - 3)) : 0.f;
+      for (int k = 3; k < 48; ++k) buf[k] = k < used ? __ldg(ac + (k - 3)) : 0.f;
       sh_colour(buf, M, degree, px, py, pz, campos, rgb, clampf);
     } else if constexpr (kSh16) {
       float buf[48];
@@ -522,11 +548,29 @@ preprocess_kernel(PreprocessArgs a) {
 void launch_preprocess(const PreprocessArgs& a, cudaStream_t stream) {
   const int blocks = (a.P + kPreThreads - 1) / kPreThreads;
   if (blocks == 0) return;
-  const bool sh16 = a.M == 16 && (reinterpret_cast<uintptr_t>(a.shs) & 15) == 0;
+  // degree 3 with 16 stored coefficients reads whole rows: staged spans; a
+  // lower degree reads only its first (degree + 1)^2 coefficients per thread
+  const bool raw = a.svec != nullptr;
+  const bool full_rows = a.items == nullptr && a.M == 16 && a.degree == 3;
+  const bool stage = full_rows && (raw ? aligned16(a.sh_dc) && aligned16(a.sh_ac) : aligned16(a.shs));
+  const bool sh16 = !raw && a.M == 16 && a.degree == 3 && aligned16(a.shs);
+  // the dynamic shared-memory opt-in of the staging kernels, once per device
+  static bool opted[64] = {false};
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (stage && (dev < 0 || dev >= 64 || !opted[dev])) {
+    cudaFuncSetAttribute(preprocess_kernel<true, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         kStageBytes);
+    cudaFuncSetAttribute(preprocess_kernel<false, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         kStageBytes);
+    if (dev >= 0 && dev < 64) opted[dev] = true;
+  }
   stage_begin(kStPreprocess, stream);
-  if (a.svec != nullptr) preprocess_kernel<false, true><<<blocks, kPreThreads, 0, stream>>>(a);
-  else if (sh16) preprocess_kernel<true, false><<<blocks, kPreThreads, 0, stream>>>(a);
-  else preprocess_kernel<false, false><<<blocks, kPreThreads, 0, stream>>>(a);
+  if (raw && stage) preprocess_kernel<false, true, true><<<blocks, kPreThreads, kStageBytes, stream>>>(a);
+  else if (raw) preprocess_kernel<false, true, false><<<blocks, kPreThreads, 0, stream>>>(a);
+  else if (stage) preprocess_kernel<true, false, true><<<blocks, kPreThreads, kStageBytes, stream>>>(a);
+  else if (sh16) preprocess_kernel<true, false, false><<<blocks, kPreThreads, 0, stream>>>(a);
+  else preprocess_kernel<false, false, false><<<blocks, kPreThreads, 0, stream>>>(a);
   stage_end(kStPreprocess, stream, 1);
 }
 
