@@ -4,8 +4,11 @@ Workload (the single-scene drop-in configuration): 500,000 Gaussians
 uniformly in a radius-0.6 ball, SH degree 3, 4 orbit views at 512x512,
 fp32 forward + backward through the torch.autograd.Function
 (_render_gaussians_inline) with synthetic N(0,1) upstream image gradients.
-A step renders and back-propagates all 4 views.  N GPUs run N replicas
-(no exchange step exists on this path), each its own 4 views.
+A step renders and back-propagates all 4 views, each on its own CUDA stream
+(the binding launches on the current stream and waits only on it), so the
+views' kernels overlap; `--single-stream` runs them one after another, and
+the JSON line carries that figure too ("single_stream").  N GPUs run N
+replicas (no exchange step exists on this path), each its own 4 views.
 
 Prints one JSON line (rank 0).  `--impl reference` times the reference's
 path on the host cores instead (see run_reference).
@@ -48,6 +51,8 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--no-batched", action="store_true", help="skip the batched-call measurement of the workload")
+    ap.add_argument("--single-stream", action="store_true",
+                    help="run a step's views one after another on one stream (default: one stream per view)")
     ap.add_argument("--config", default="single", choices=["single", "multiscene", "serve", "sortscan"],
                     help="single: the 500k / 512^2 drop-in workload (default); multiscene: 64 scenes, batched "
                          "calls vs sequential single-view calls; serve: Poisson requests over the 64 resident "
@@ -64,7 +69,17 @@ def workload_config(a):
                         f"SH degree 3, fp32 forward+backward through the autograd Function",
             "gaussians": a.P, "views_per_gpu": a.views, "resolution": a.res, "sh_degree": 3,
             "grad_mode": a.grad_mode, "compat_spill": True,
+            "streams": "one per view" if not a.single_stream else "one",
             "l2": "inputs larger than L2 (about 1 GB of parameters, state and images touched per step)"}
+
+
+def quiet_stream_mismatch():
+    """Leaf gradients of a step accumulate from several views' streams on
+    purpose; torch warns about that stream mismatch, which is expected here."""
+    import torch
+    f = getattr(torch.autograd.graph, "set_warn_on_accumulate_grad_stream_mismatch", None)
+    if f is not None:
+        f(False)
 
 
 def peaks():
@@ -168,18 +183,35 @@ def run_ours(a):
     sc, cams, L, grads, cam_t = build_inputs(a, device)
     bg = torch.ones(3, device=device)
     means2D = torch.zeros_like(L["means3D"], requires_grad=True)
+    # each view of a step on its own stream: the binding launches on the
+    # current stream and waits only on it (for the instance count), so one
+    # view's kernels fill the SMs another view's heaviest tiles leave idle
+    main = torch.cuda.current_stream(device)
+    vstreams = [torch.cuda.Stream(device=device) for _ in range(a.views)]
+    quiet_stream_mismatch()
 
-    def step():
+    def one_view(v):
+        c = cam_t[v]
+        color, radii, depth, alpha = _render_gaussians_inline(
+            L["means3D"], means2D, L["shs"], None, L["opacity"], L["scales"], L["rotations"], None, bg, 1,
+            c["view"], c["proj"], c["tanx"], c["tany"], 3, c["campos"], image_height=a.res, image_width=a.res,
+            grad_mode=a.grad_mode)
+        torch.autograd.backward([color], [grads[v]])
+
+    def step(per_view_streams=not a.single_stream):
         for k in L:
             L[k].grad = None
         means2D.grad = None
+        if not per_view_streams:
+            for v in range(a.views):
+                one_view(v)
+            return
         for v in range(a.views):
-            c = cam_t[v]
-            color, radii, depth, alpha = _render_gaussians_inline(
-                L["means3D"], means2D, L["shs"], None, L["opacity"], L["scales"], L["rotations"], None, bg, 1,
-                c["view"], c["proj"], c["tanx"], c["tany"], 3, c["campos"], image_height=a.res, image_width=a.res,
-                grad_mode=a.grad_mode)
-            torch.autograd.backward([color], [grads[v]])
+            vstreams[v].wait_stream(main)
+            with torch.cuda.stream(vstreams[v]):
+                one_view(v)
+        for vs in vstreams:
+            main.wait_stream(vs)
 
     # per-view instance counts and sort plan (for the roofline's algorithmic bytes)
     plans = []
@@ -220,11 +252,34 @@ def run_ours(a):
         dist.barrier()
     ms_max = wd.max_over_ranks(ms, device=device)
     value = world * a.views * a.steps / (ms_max / 1e3)
-    # every stage's time, from separate untimed steps
+    # the same steps with every view on the one stream, for comparison; the
+    # roofline kernel's launches are timed here, where each runs alone on the
+    # device (in the timed steps above it shares the SMs with other views')
+    single = None
+    concurrent_stages = None
+    if not a.single_stream:
+        concurrent_stages = timed_stages
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+        _C.stage_times()
+        _C.stage_timing_only(["sort_onesweep"])
+        s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s0.record(stream)
+        for _ in range(a.steps):
+            step(False)
+        s1.record(stream)
+        torch.cuda.synchronize()
+        _C.stage_timing(False)
+        timed_stages = _C.stage_times()
+        sms = wd.max_over_ranks(s0.elapsed_time(s1), device=device)
+        single = {"value": round(world * a.views * a.steps / (sms / 1e3), 3), "ms_per_step": round(sms / a.steps, 4)}
+    # every stage's time, from separate untimed steps on one stream (stages
+    # of concurrent views would overlap)
     stage_steps = max(10, a.steps // 10)
     _C.stage_timing(True)
     for _ in range(stage_steps):
-        step()
+        step(False)
     torch.cuda.synchronize()
     _C.stage_timing(False)
     stages = _C.stage_times()
@@ -258,7 +313,14 @@ def run_ours(a):
                     "traffic": NCU_TRAFFIC_500K_512.get(dom) if (a.P, a.res) == (500_000, 512) else None,
                     "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum per launch "
                                       "(profiles/dram_traffic_500k_512x512.md)",
-                    "algorithmic_bytes_per_launch": int(alg_bytes[dom]), "avg_launch_ms": round(per_launch_ms, 4)}
+                    "algorithmic_bytes_per_launch": int(alg_bytes[dom]), "avg_launch_ms": round(per_launch_ms, 4),
+                    "timed_in": "timed steps" if single is None else "single-stream timed steps"}
+        cs = (concurrent_stages or {}).get(dom, (0, 0))
+        if cs[1]:
+            cms = cs[0] / cs[1]
+            roofline["concurrent"] = {"achieved": round(alg_bytes[dom] / (cms / 1e3) / 1e9, 1),
+                                      "avg_launch_ms": round(cms, 4),
+                                      "note": "launches timed in the per-view-stream steps, sharing the SMs"}
     stage_report = {k: {"ms_per_step": round(stage_ms[k] / stage_steps, 4),
                         "launches_per_step": stage_n[k] / stage_steps,
                         "share": round(stage_ms[k] / total_stage, 4)} for k in stage_ms if stage_n[k]}
@@ -269,6 +331,8 @@ def run_ours(a):
               "config": dict(workload_config(a), parallelism=f"replicas x{world}", num_rendered_per_view=int(Rm),
                              sort_key_bytes=kb, sort_passes=plans[0].get("passes")),
               "gpu_launches": int(launches), "clocks": clk.summary(), "roofline": roofline, "stages": stage_report}
+    if single is not None:
+        result["single_stream"] = single
 
     if not a.no_batched:
         result["batched"] = run_batched_single(a, sc, cams, device, world, value)
@@ -304,6 +368,9 @@ def run_e2e(a, sc, cams, device, world):
     # gradients (needed only by its loss), so every copy overlaps rendering
     copy_stream = torch.cuda.Stream(device=device)
     main_stream = torch.cuda.current_stream(device)
+    # each view renders and back-propagates on its own stream (as run_ours)
+    vstreams = [torch.cuda.Stream(device=device) for _ in cams] if not a.single_stream else None
+    quiet_stream_mismatch()
 
     def step():
         for p_ in params.parameters():
@@ -325,15 +392,24 @@ def run_e2e(a, sc, cams, device, world):
         for v, c in enumerate(cams):
             (V, Pm, C), ev_c = cams_dev[v]
             g, ev_g = grads_dev[v]
-            main_stream.wait_event(ev_c)
-            for x in (V, Pm, C):
+            vs = vstreams[v] if vstreams else main_stream
+            if vstreams:
+                vs.wait_stream(main_stream)
+            with torch.cuda.stream(vs):
+                vs.wait_event(ev_c)
+                for x in (V, Pm, C):
+                    x.record_stream(vs)
+                out = r.render(c.fovx, c.fovy, V, Pm, C, a.res, a.res)
+                vs.wait_event(ev_g)
+                g.record_stream(vs)
+                loss = (out["image"] * g).sum()
+                loss.backward()
+                losses.append(loss.detach())
+        if vstreams:
+            for vs in vstreams:
+                main_stream.wait_stream(vs)
+            for x in losses:
                 x.record_stream(main_stream)
-            out = r.render(c.fovx, c.fovy, V, Pm, C, a.res, a.res)
-            main_stream.wait_event(ev_g)
-            g.record_stream(main_stream)
-            loss = (out["image"] * g).sum()
-            loss.backward()
-            losses.append(loss.detach())
         loss_host.copy_(torch.stack(losses), non_blocking=True)
         torch.cuda.current_stream().synchronize()
         return loss_host
