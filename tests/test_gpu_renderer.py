@@ -183,3 +183,55 @@ def test_ply_round_trip_renders_identically(tmp_path):
     assert torch.equal(img0, img1)
     res = BatchRenderer().forward([Scene.from_ply(path, device=DEV)], [View(0, cam)])
     assert parity.bit_mismatch(res.color[0].cpu().numpy(), img0.cpu().numpy()) == 0
+
+
+def test_views_on_separate_streams_match_one_stream():
+    """The binding launches on the current stream and waits only on it, so the
+    views of a step may run on separate streams: the images are the
+    single-stream images bit for bit and the accumulated leaf gradients agree
+    up to the order of the atomic additions."""
+    sc, cam0, t = _setup(seed=6)
+    from word2world_b200 import camera
+    cams = camera.orbit_views(3, 2.5, cam0.width, cam0.height)
+    m, o, s, q, sh = sc.activate()
+    leaves = [t(x).requires_grad_(True) for x in (m, sh, o, s, q)]
+    means3D, shs, opac, scales, rots = leaves
+    means2D = torch.zeros_like(means3D, requires_grad=True)
+    bg = torch.ones(3, device=DEV)
+    S = cam0.width
+    gen = torch.Generator(device=DEV).manual_seed(7)
+    gs = [torch.randn(3, S, S, device=DEV, generator=gen) for _ in cams]
+    ct = [(t(c.viewmatrix), t(c.projmatrix), t(c.campos), c.tanfovx, c.tanfovy) for c in cams]
+
+    def view(v):
+        V, Pm, C, tx, ty = ct[v]
+        color, _, _, _ = _render_gaussians_inline(means3D, means2D, shs, None, opac, scales, rots, None, bg, 1.0, V,
+                                                  Pm, tx, ty, 3, C, image_height=S, image_width=S)
+        torch.autograd.backward([color], [gs[v]])
+        return color.detach()
+
+    def run(streams):
+        for x in leaves + [means2D]:
+            x.grad = None
+        main = torch.cuda.current_stream()
+        imgs = []
+        for v in range(len(cams)):
+            if streams is None:
+                imgs.append(view(v))
+                continue
+            streams[v].wait_stream(main)
+            with torch.cuda.stream(streams[v]):
+                imgs.append(view(v))
+        if streams is not None:
+            for st in streams:
+                main.wait_stream(st)
+        torch.cuda.synchronize()
+        return [i.cpu().numpy() for i in imgs], [x.grad.cpu().numpy() for x in leaves + [means2D]]
+
+    img1, g1 = run(None)
+    img2, g2 = run([torch.cuda.Stream() for _ in cams])
+    for a_, b_ in zip(img1, img2):
+        assert parity.bit_mismatch(a_, b_) == 0
+    for name, a_, b_ in zip(("means3D", "shs", "opacity", "scales", "rotations", "means2D"), g1, g2):
+        chk = parity.grad_check(a_, b_)
+        assert chk["norm_rel"] <= 1e-5 and chk["n_bad"] == 0, (name, chk)
