@@ -121,7 +121,9 @@ int w2w_state_error(const void* state, int which /* 0 geometry, 1 binning */, w2
  * backward (gradientPass.cu:26-207).  grad_mode 0 = the reference's formulas,
  * 1 = the exact derivative of the forward.  All eight outputs are fully
  * written (no pre-zeroing needed); dL_dmeans2D is [P,3] with the third
- * component 0; dL_dcov3D is [P,6]; dL_dsh is [P,M,3]. */
+ * component 0; dL_dcov3D is [P,6]; dL_dsh is [P,M,3].  dL_ddepth and
+ * dL_dalpha may be NULL: no loss on depth / alpha (the reference always
+ * passes buffers, zero-filled by autograd when unused). */
 int w2w_backward(const w2w_settings* s, const float* means3D, const float* scales, const float* rotations,
                  const float* shs, const int* radii, const void* geom_state,
                  long long num_rendered, const void* binning_state, const void* image_state,

@@ -134,8 +134,8 @@ struct BwdPixel {
       dLp0 = a.dL_dcolor[cp];
       dLp1 = a.dL_dcolor[hw + cp];
       dLp2 = a.dL_dcolor[2 * hw + cp];
-      dLd = a.dL_ddepth[pix];
-      dLa = a.dL_dalpha[pix];
+      dLd = a.dL_ddepth != nullptr ? a.dL_ddepth[pix] : 0.f;  // absent: no loss on depth / alpha
+      dLa = a.dL_dalpha != nullptr ? a.dL_dalpha[pix] : 0.f;
     }
   }
 };

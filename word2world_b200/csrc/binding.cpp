@@ -148,8 +148,10 @@ std::tuple<Tensor, Tensor, Tensor, Tensor, Tensor, Tensor, Tensor, Tensor> raste
   Tensor gd = f32(dL_dout_depth, "dL_dout_depth", dev);
   Tensor ga = f32(dL_dout_alpha, "dL_dout_alpha", dev);
   Tensor al = f32(alpha, "alpha", dev);
-  TORCH_CHECK(gd.numel() == int64_t(H) * W && ga.numel() == int64_t(H) * W && al.numel() == int64_t(H) * W,
-              "depth / alpha gradients and alpha must be [1, H, W]");
+  // an empty depth / alpha gradient means none (no loss on that output)
+  TORCH_CHECK((gd.numel() == 0 || gd.numel() == int64_t(H) * W) && (ga.numel() == 0 || ga.numel() == int64_t(H) * W) &&
+                  al.numel() == int64_t(H) * W,
+              "depth / alpha gradients (or empty) and alpha must be [1, H, W]");
   TORCH_CHECK(radii.is_cuda() && radii.scalar_type() == torch::kInt32 && radii.numel() == P, "radii must be int32 [P]");
   Tensor rad = radii.contiguous();
   int64_t M = 0;
@@ -185,7 +187,8 @@ std::tuple<Tensor, Tensor, Tensor, Tensor, Tensor, Tensor, Tensor, Tensor> raste
     check(w2w_backward(&st, m.data_ptr<float>(), s.data_ptr<float>(), r.data_ptr<float>(),
                        M > 0 ? shc.data_ptr<float>() : nullptr, rad.data_ptr<int>(), geomBuffer.data_ptr(), R,
                        binningBuffer.data_ptr(), imageBuffer.data_ptr(), al.data_ptr<float>(), g.data_ptr<float>(),
-                       gd.data_ptr<float>(), ga.data_ptr<float>(), int(grad_mode), scratch.data_ptr(),
+                       gd.numel() ? gd.data_ptr<float>() : nullptr, ga.numel() ? ga.data_ptr<float>() : nullptr,
+                       int(grad_mode), scratch.data_ptr(),
                        size_t(scratch.numel()), dmean2D.data_ptr<float>(), dcolors.data_ptr<float>(),
                        dopac.data_ptr<float>(), dmean3D.data_ptr<float>(), dcov3D.data_ptr<float>(),
                        M > 0 ? dsh.data_ptr<float>() : nullptr, dscales.data_ptr<float>(), drot.data_ptr<float>(),
@@ -291,8 +294,10 @@ std::tuple<Tensor, Tensor, Tensor, Tensor, Tensor, Tensor, Tensor> rasterize_gau
   const int H = int(g.size(1)), W = int(g.size(2));
   Tensor gd = f32(dL_dout_depth, "dL_dout_depth", dev), ga = f32(dL_dout_alpha, "dL_dout_alpha", dev);
   Tensor al = f32(alpha, "alpha", dev);
-  TORCH_CHECK(gd.numel() == int64_t(H) * W && ga.numel() == int64_t(H) * W && al.numel() == int64_t(H) * W,
-              "depth / alpha gradients and alpha must be [1, H, W]");
+  // an empty depth / alpha gradient means none (no loss on that output)
+  TORCH_CHECK((gd.numel() == 0 || gd.numel() == int64_t(H) * W) && (ga.numel() == 0 || ga.numel() == int64_t(H) * W) &&
+                  al.numel() == int64_t(H) * W,
+              "depth / alpha gradients (or empty) and alpha must be [1, H, W]");
   TORCH_CHECK(radii.is_cuda() && radii.scalar_type() == torch::kInt32 && radii.numel() == P, "radii must be int32 [P]");
   TORCH_CHECK(geomBuffer.numel() >= int64_t(w2w_geometry_state_bytes(int(P))), "geomBuffer does not match P");
   TORCH_CHECK(imageBuffer.numel() >= int64_t(w2w_image_state_bytes(W, H)), "imageBuffer does not match H, W");
@@ -320,7 +325,8 @@ std::tuple<Tensor, Tensor, Tensor, Tensor, Tensor, Tensor, Tensor> rasterize_gau
     check(w2w_backward_raw(&st, m.data_ptr<float>(), sv.data_ptr<float>(), q.data_ptr<float>(), lo.data_ptr<float>(),
                            dc.data_ptr<float>(), ac.data_ptr<float>(), rad.data_ptr<int>(), geomBuffer.data_ptr(), R,
                            binningBuffer.data_ptr(), imageBuffer.data_ptr(), al.data_ptr<float>(), g.data_ptr<float>(),
-                           gd.data_ptr<float>(), ga.data_ptr<float>(), scratch.data_ptr(), size_t(scratch.numel()),
+                           gd.numel() ? gd.data_ptr<float>() : nullptr, ga.numel() ? ga.data_ptr<float>() : nullptr,
+                           scratch.data_ptr(), size_t(scratch.numel()),
                            dmean2D.data_ptr<float>(), dcolors.data_ptr<float>(), dlogit.data_ptr<float>(),
                            dmean3D.data_ptr<float>(), dcov3D.data_ptr<float>(), ddc.data_ptr<float>(),
                            dac.data_ptr<float>(), dsvec.data_ptr<float>(), dquat.data_ptr<float>(), stream),

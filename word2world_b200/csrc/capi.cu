@@ -429,7 +429,7 @@ int w2w_backward(const w2w_settings* s, const float* means3D, const float* scale
   const int P = s->P;
   if (P == 0) return W2W_OK;
   if (!means3D || !scales || !rotations || !radii || !geom_state || !image_state || !out_alpha ||
-      !dL_dcolor || !dL_ddepth || !dL_dalpha || !dL_dmeans2D || !dL_dcolors || !dL_dopacity || !dL_dmeans3D ||
+      !dL_dcolor || !dL_dmeans2D || !dL_dcolors || !dL_dopacity || !dL_dmeans3D ||
       !dL_dcov3D || !dL_dscales || !dL_drotations || (s->M > 0 && (!shs || !dL_dsh)) || (R > 0 && !binning_state))
     return W2W_ERR_INVALID;
   return backward_impl(s, means3D, scales, rotations, shs, nullptr, radii, geom_state, R, binning_state,
@@ -449,7 +449,7 @@ int w2w_backward_raw(const w2w_settings* s, const float* means3D, const float* s
   const int P = s->P;
   if (P == 0) return W2W_OK;
   if (!means3D || !svec || !quaternion || !opacity_logit || !sh_dc || (s->M > 1 && (!sh_ac || !dL_dsh_ac)) ||
-      !radii || !geom_state || !image_state || !out_alpha || !dL_dcolor || !dL_ddepth || !dL_dalpha ||
+      !radii || !geom_state || !image_state || !out_alpha || !dL_dcolor ||
       !dL_dmeans2D || !dL_dcolors || !dL_dopacity_logit || !dL_dmeans3D || !dL_dcov3D || !dL_dsh_dc || !dL_dsvec ||
       !dL_dquaternion || (R > 0 && !binning_state))
     return W2W_ERR_INVALID;

@@ -35,6 +35,17 @@ def fill_missing_attributes(means3D, shs, colors_precomp, scales, rotations, cov
             cov3D_precomp if cov3D_precomp is not None else empty())
 
 
+def _image_grads(g_color, g_depth, g_alpha, alpha):
+    """The upstream image gradients as the binding takes them: colour always
+    (zeros when only depth / alpha carry a loss), depth and alpha empty when
+    no loss reaches them (read as zero by the kernels, no zero-filled planes)."""
+    empty = alpha.new_empty(0)
+    H, W = alpha.shape[-2], alpha.shape[-1]
+    g_color = g_color.contiguous() if g_color is not None else alpha.new_zeros(3, H, W)
+    return (g_color, g_depth.contiguous() if g_depth is not None else empty,
+            g_alpha.contiguous() if g_alpha is not None else empty)
+
+
 class _RasterizeGaussians(torch.autograd.Function):
     @staticmethod
     def forward(ctx, means3D, means2D, sh, colors_precomp, opacities, scales, rotations, cov3Ds_precomp, bg,
@@ -59,15 +70,17 @@ class _RasterizeGaussians(torch.autograd.Function):
         ctx.save_for_backward(colors_precomp, means3D, scales, rotations, cov3Ds_precomp, radii, sh, geom, binb, img,
                               alpha)
         ctx.mark_non_differentiable(radii)
+        ctx.set_materialize_grads(False)  # an output without a gradient reaches the kernels as none
         return color, radii, depth, alpha
 
     @staticmethod
     def backward(ctx, g_color, g_radii, g_depth, g_alpha):
         (colors_precomp, means3D, scales, rotations, cov3Ds_precomp, radii, sh, geom, binb, img,
          alpha) = ctx.saved_tensors
+        g_color, g_depth, g_alpha = _image_grads(g_color, g_depth, g_alpha, alpha)
         g_means2D, g_colors, g_opac, g_means3D, g_cov3D, g_sh, g_scales, g_rots = _C.rasterize_gaussians_backward(
             ctx.bg, means3D, radii, colors_precomp, scales, rotations, ctx.scale_mod, cov3Ds_precomp, ctx.vmat,
-            ctx.pmat, ctx.fx, ctx.fy, g_color.contiguous(), g_depth.contiguous(), g_alpha.contiguous(), sh,
+            ctx.pmat, ctx.fx, ctx.fy, g_color, g_depth, g_alpha, sh,
             ctx.sh_deg, ctx.campos, geom, ctx.num_rend, binb, img, alpha, ctx.debug, ctx.grad_mode)
         return (g_means3D, g_means2D, g_sh, None if colors_precomp.numel() == 0 else g_colors, g_opac, g_scales,
                 g_rots, None if cov3Ds_precomp.numel() == 0 else g_cov3D,
@@ -140,14 +153,16 @@ class _RasterizeRaw(torch.autograd.Function):
         ctx.fx, ctx.fy, ctx.sh_deg = tanfovx, tanfovy, sh_degree
         ctx.save_for_backward(means3D, sh_dc, sh_ac, opacity_logit, svec, quaternion, radii, geom, binb, img, alpha)
         ctx.mark_non_differentiable(radii)
+        ctx.set_materialize_grads(False)
         return color, radii, depth, alpha
 
     @staticmethod
     def backward(ctx, g_color, g_radii, g_depth, g_alpha):
         means3D, sh_dc, sh_ac, opacity_logit, svec, quaternion, radii, geom, binb, img, alpha = ctx.saved_tensors
+        g_color, g_depth, g_alpha = _image_grads(g_color, g_depth, g_alpha, alpha)
         g_means2D, g_means3D, g_dc, g_ac, g_logit, g_svec, g_quat = _C.rasterize_gaussians_backward_raw(
             ctx.bg, means3D, sh_dc, sh_ac, opacity_logit, svec, quaternion, radii, ctx.vmat, ctx.pmat, ctx.campos,
-            ctx.fx, ctx.fy, ctx.sh_deg, g_color.contiguous(), g_depth.contiguous(), g_alpha.contiguous(), geom,
+            ctx.fx, ctx.fy, ctx.sh_deg, g_color, g_depth, g_alpha, geom,
             ctx.num_rend, binb, img, alpha)
         return (g_means3D, g_means2D, g_dc, g_ac, g_logit, g_svec, g_quat,
                 None, None, None, None, None, None, None, None, None, None)
