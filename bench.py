@@ -357,10 +357,18 @@ def run_e2e(a, sc, cams, device, world):
     from word2world_b200.renderer import GaussianParams, Renderer
     params = GaussianParams.from_scene(sc, device=device)
     r = Renderer(params, sh_degree=3, grad_mode=a.grad_mode)
-    host_g = [torch.from_numpy(g).pin_memory() for g in scenes.upstream_grads(a.views, a.res, a.res, seed=a.seed + 1)]
-    host_c = [(torch.from_numpy(c.viewmatrix).pin_memory(), torch.from_numpy(c.projmatrix).pin_memory(),
-               torch.from_numpy(c.campos).pin_memory()) for c in cams]
-    h2d = sum(g.numel() * 4 for g in host_g) + sum(sum(x.numel() * 4 for x in c) for c in host_c)
+    # a step's inputs in two pinned buffers: every view's camera (view matrix,
+    # projection matrix, position, at float offsets 0, 16 and 32 of a 48-float
+    # row), then every view's image gradient
+    grads_np = scenes.upstream_grads(a.views, a.res, a.res, seed=a.seed + 1)
+    host_g = torch.from_numpy(np.stack([np.asarray(g, np.float32) for g in grads_np])).pin_memory()
+    cam_rows = np.zeros((len(cams), 48), np.float32)
+    for v, c in enumerate(cams):
+        cam_rows[v, :16] = np.asarray(c.viewmatrix, np.float32).ravel()
+        cam_rows[v, 16:32] = np.asarray(c.projmatrix, np.float32).ravel()
+        cam_rows[v, 32:35] = np.asarray(c.campos, np.float32).ravel()
+    host_c = torch.from_numpy(cam_rows).pin_memory()
+    h2d = host_g.numel() * 4 + host_c.numel() * 4
     loss_host = torch.empty(a.views, dtype=torch.float32).pin_memory()
 
     # the step's inputs are copied on a side stream at the step's start: all
@@ -376,32 +384,27 @@ def run_e2e(a, sc, cams, device, world):
         for p_ in params.parameters():
             p_.grad = None
         copy_stream.wait_stream(main_stream)  # the previous step is done with the buffers
-        cams_dev, grads_dev = [], []
         with torch.cuda.stream(copy_stream):
-            for v in range(len(cams)):
-                VPC = tuple(x.to(device, non_blocking=True) for x in host_c[v])
-                ev = torch.cuda.Event()
-                ev.record(copy_stream)
-                cams_dev.append((VPC, ev))
-            for v in range(len(cams)):
-                g = host_g[v].to(device, non_blocking=True)
-                ev = torch.cuda.Event()
-                ev.record(copy_stream)
-                grads_dev.append((g, ev))
+            cams_dev = host_c.to(device, non_blocking=True)
+            ev_c = torch.cuda.Event()
+            ev_c.record(copy_stream)
+            grads_dev = host_g.to(device, non_blocking=True)
+            ev_g = torch.cuda.Event()
+            ev_g.record(copy_stream)
         losses = []
         for v, c in enumerate(cams):
-            (V, Pm, C), ev_c = cams_dev[v]
-            g, ev_g = grads_dev[v]
             vs = vstreams[v] if vstreams else main_stream
             if vstreams:
                 vs.wait_stream(main_stream)
             with torch.cuda.stream(vs):
                 vs.wait_event(ev_c)
-                for x in (V, Pm, C):
-                    x.record_stream(vs)
+                cams_dev.record_stream(vs)
+                row = cams_dev[v]
+                V, Pm, C = row[:16].view(4, 4), row[16:32].view(4, 4), row[32:35]
                 out = r.render(c.fovx, c.fovy, V, Pm, C, a.res, a.res)
                 vs.wait_event(ev_g)
-                g.record_stream(vs)
+                grads_dev.record_stream(vs)
+                g = grads_dev[v]
                 loss = (out["image"] * g).sum()
                 loss.backward()
                 losses.append(loss.detach())
