@@ -4,10 +4,12 @@ Workload (the single-scene drop-in configuration): 500,000 Gaussians
 uniformly in a radius-0.6 ball, SH degree 3, 4 orbit views at 512x512,
 fp32 forward + backward through the torch.autograd.Function
 (_render_gaussians_inline) with synthetic N(0,1) upstream image gradients.
-A step renders and back-propagates all 4 views, each on its own CUDA stream
-(the binding launches on the current stream and waits only on it), so the
-views' kernels overlap; `--single-stream` runs them one after another, and
-the JSON line carries that figure too ("single_stream").  N GPUs run N
+A step renders all 4 views, each on its own CUDA stream (the binding
+launches on the current stream and waits only on it), then back-propagates
+them with one backward call (as the reference's trainer does; each view's
+backward runs on its forward's stream), so the views' kernels overlap;
+`--single-stream` renders and back-propagates them one after another on one
+stream, and the JSON line carries that figure too ("single_stream").  N GPUs run N
 replicas (no exchange step exists on this path), each its own 4 views.
 
 Prints one JSON line (rank 0).  `--impl reference` times the reference's
@@ -190,13 +192,16 @@ def run_ours(a):
     vstreams = [torch.cuda.Stream(device=device) for _ in range(a.views)]
     quiet_stream_mismatch()
 
-    def one_view(v):
+    def render_view(v):
         c = cam_t[v]
         color, radii, depth, alpha = _render_gaussians_inline(
             L["means3D"], means2D, L["shs"], None, L["opacity"], L["scales"], L["rotations"], None, bg, 1,
             c["view"], c["proj"], c["tanx"], c["tany"], 3, c["campos"], image_height=a.res, image_width=a.res,
             grad_mode=a.grad_mode)
-        torch.autograd.backward([color], [grads[v]])
+        return color
+
+    def one_view(v):
+        torch.autograd.backward([render_view(v)], [grads[v]])
 
     def step(per_view_streams=not a.single_stream):
         for k in L:
@@ -206,10 +211,14 @@ def run_ours(a):
             for v in range(a.views):
                 one_view(v)
             return
+        # every view's forward on its stream, then one backward over all views
+        # (each view's backward runs on the stream its forward ran on)
+        colors = []
         for v in range(a.views):
             vstreams[v].wait_stream(main)
             with torch.cuda.stream(vstreams[v]):
-                one_view(v)
+                colors.append(render_view(v))
+        torch.autograd.backward(colors, grads)
         for vs in vstreams:
             main.wait_stream(vs)
 
@@ -406,8 +415,12 @@ def run_e2e(a, sc, cams, device, world):
                 grads_dev.record_stream(vs)
                 g = grads_dev[v]
                 loss = (out["image"] * g).sum()
-                loss.backward()
-                losses.append(loss.detach())
+                if not vstreams:
+                    loss.backward()
+                losses.append(loss)
+        if vstreams:  # one backward over all views (each on its forward's stream)
+            torch.autograd.backward(losses)
+        losses = [x.detach() for x in losses]
         if vstreams:
             for vs in vstreams:
                 main_stream.wait_stream(vs)
