@@ -671,6 +671,28 @@ __device__ __forceinline__ void sh_store_outer_raw(float* ddc, float* dac, int M
   }
 }
 
+// A batched call's SH rows of the warp's elements [i0, i0 + n): one scene's
+// contiguous rows when all n belong to one item (sh_stage_in's spans), else
+// each thread its own row (the warp spans scenes).  Warp-collective.
+__device__ __forceinline__ void batch_sh_stage_in(const BackwardArgs& a, int i0, int n, float* s, int stride) {
+  const int lane = threadIdx.x & 31;
+  const int first = find_item_elem(a.items, a.num_items, uint32_t(i0));
+  const int last = find_item_elem(a.items, a.num_items, uint32_t(i0 + n - 1));
+  if (first == last) {
+    const BatchItem& it = a.items[first];
+    sh_stage_in(it.shs, a.M, i0 - int(it.elem_base), n, s, stride);
+    return;
+  }
+  const int rs = 3 * (a.M < 16 ? a.M : 16);
+  if (lane < n) {
+    const int i = i0 + lane;
+    const BatchItem& it = a.items[find_item_elem(a.items, a.num_items, uint32_t(i))];
+    const float* row = it.shs + size_t(i - int(it.elem_base)) * 3 * a.M;
+    for (int c = 0; c < rs; ++c) s[lane * stride + c] = __ldg(row + c);
+  }
+  __syncwarp();
+}
+
 // Per-Gaussian, reference formulas (backward.cu:27-227 then :229-519)
 __constant__ float kSH_C2[5] = {1.0925484305920792f, -1.0925484305920792f, 0.31539156525252005f,
                                 -1.0925484305920792f, 0.5462742152960396f};
@@ -965,13 +987,8 @@ __global__ void __launch_bounds__(kGaussThreads, 8) gaussians_ref_kernel(Backwar
   if (a.items == nullptr) {
     if (a.sh_dc != nullptr) sh_stage_in_raw(a.sh_dc, a.sh_ac, a.M, i0, n, sw, stride);
     else sh_stage_in(a.shs, a.M, i0, n, sw, stride);
-  } else {  // a warp's elements may belong to different scenes: each thread its own row
-    const int rs = 3 * (a.M < 16 ? a.M : 16);
-    if (lane < n) {
-      const float* row = a.items[find_item_elem(a.items, a.num_items, uint32_t(i))].shs + size_t(gv.gi) * 3 * a.M;
-      for (int c = 0; c < rs; ++c) sw[lane * stride + c] = __ldg(row + c);
-    }
-    __syncwarp();
+  } else {
+    batch_sh_stage_in(a, i0, n, sw, stride);
   }
   float basis[16], cf[3] = {0.f, 0.f, 0.f};
   const bool active = lane < n && a.radii[i] > 0;
@@ -1170,13 +1187,8 @@ __global__ void __launch_bounds__(kGaussThreads) gaussians_exact_kernel(Backward
   const GView gv = make_gview(a, lane < n ? i : i0, s_mats);
   if (a.items == nullptr) {
     sh_stage_in(a.shs, a.M, i0, n, sw, stride);
-  } else {  // a warp's elements may belong to different scenes: each thread its own row
-    const int rs = 3 * (a.M < 16 ? a.M : 16);
-    if (lane < n) {
-      const float* row = a.items[find_item_elem(a.items, a.num_items, uint32_t(i))].shs + size_t(gv.gi) * 3 * a.M;
-      for (int c = 0; c < rs; ++c) sw[lane * stride + c] = __ldg(row + c);
-    }
-    __syncwarp();
+  } else {
+    batch_sh_stage_in(a, i0, n, sw, stride);
   }
   float basis[16], cf[3] = {0.f, 0.f, 0.f};
   const bool active = lane < n && a.radii[i] > 0;
