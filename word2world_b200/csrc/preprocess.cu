@@ -267,9 +267,16 @@ preprocess_kernel(PreprocessArgs a) {
   }
   const int gw = (Wd + kTile - 1) / kTile, gh = (Hd + kTile - 1) / kTile;
 
-  // this warp's SH rows, staged when all 32 of its Gaussians exist
+  // this warp's SH rows, staged when all 32 of its Gaussians exist (and, in a
+  // batched call, belong to one scene with 16 coefficients)
   const int i0 = int(tile) * kPreThreads + int(threadIdx.x & ~31u);
-  const bool staged = kStage && i0 + 32 <= P;  // warp-uniform
+  bool staged = kStage && i0 + 32 <= P;  // warp-uniform
+  const float* span = kRaw ? nullptr : a.shs + size_t(i0) * 48;  // the warp's first row
+  if (staged && a.items != nullptr) {
+    const int f = find_item_elem(a.items, a.num_items, uint32_t(i0));
+    staged = f == find_item_elem(a.items, a.num_items, uint32_t(i0 + 31)) && a.items[f].M == 16;
+    span = a.items[f].shs + size_t(i0 - int(a.items[f].elem_base)) * 48;
+  }
   const float* srow = s_rows + int(threadIdx.x >> 5) * 32 * kShStride;
   if (staged) {
     float* w = s_rows + int(threadIdx.x >> 5) * 32 * kShStride;
@@ -277,7 +284,7 @@ preprocess_kernel(PreprocessArgs a) {
       stage_span(a.sh_dc + size_t(i0) * 3, 3, w, kShStride, 0);
       stage_span(a.sh_ac + size_t(i0) * 45, 45, w, kShStride, 3);
     } else {
-      stage_span(a.shs + size_t(i0) * 48, 48, w, kShStride, 0);
+      stage_span(span, 48, w, kShStride, 0);
     }
     __syncwarp();
   }
@@ -550,10 +557,13 @@ void launch_preprocess(const PreprocessArgs& a, cudaStream_t stream) {
   if (blocks == 0) return;
   // degree 3 with 16 stored coefficients reads whole rows: staged spans; a
   // lower degree reads only its first (degree + 1)^2 coefficients per thread
+  // (a batched call sets M = 16 and shs non-null when every scene's rows are
+  // 16-byte aligned with 16 coefficients; its degrees are per scene)
   const bool raw = a.svec != nullptr;
-  const bool full_rows = a.items == nullptr && a.M == 16 && a.degree == 3;
+  const bool batched = a.items != nullptr;
+  const bool full_rows = a.M == 16 && (batched ? a.shs != nullptr : a.degree == 3);
   const bool stage = full_rows && (raw ? aligned16(a.sh_dc) && aligned16(a.sh_ac) : aligned16(a.shs));
-  const bool sh16 = !raw && a.M == 16 && a.degree == 3 && aligned16(a.shs);
+  const bool sh16 = !raw && full_rows && aligned16(a.shs);
   // the dynamic shared-memory opt-in of the staging kernels, once per device
   static bool opted[64] = {false};
   int dev = 0;
