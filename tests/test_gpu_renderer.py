@@ -67,8 +67,8 @@ def test_autograd_function_matches_binding(grad_mode):
         assert chk["norm_rel"] <= 1e-5 and chk["n_bad"] == 0, (k, chk)
 
 
-@pytest.mark.parametrize("grad_mode", ["reference", "exact"])
-def test_renderer_render_is_preamble_plus_function(grad_mode):
+@pytest.mark.parametrize("grad_mode,degree", [("reference", 3), ("exact", 3), ("reference", 0)])
+def test_renderer_render_is_preamble_plus_function(grad_mode, degree):
     """In "reference" mode ``Renderer.render`` runs the raw-parameter Function
     (preamble folded into the projection and the per-Gaussian backward); in
     "exact" mode the fused activation kernels and the plain Function."""
@@ -78,7 +78,7 @@ def test_renderer_render_is_preamble_plus_function(grad_mode):
     with torch.no_grad():  # a few degenerate quaternions: the normalisation's 1e-12 floor
         params.quaternion[:7] = 0.0
         params.quaternion[7:14] *= 1e-20
-    r = Renderer(params, sh_degree=3, grad_mode=grad_mode)
+    r = Renderer(params, sh_degree=degree, grad_mode=grad_mode)
     out = r.render(cam.fovx, cam.fovy, t(cam.viewmatrix), t(cam.projmatrix), t(cam.campos), S, S)
     assert set(out) >= {"image", "accum_grads", "avaialble_pts", "available_pts"}
     g = torch.randn(3, S, S, device=DEV, generator=torch.Generator(device=DEV).manual_seed(2))
@@ -93,7 +93,7 @@ def test_renderer_render_is_preamble_plus_function(grad_mode):
     image, radii, _, _ = _render_gaussians_inline(
         mean, means2D, shs, None, torch.sigmoid(opac_l), torch.exp(svec), torch.nn.functional.normalize(quat), None,
         torch.ones(3, device=DEV), 1, t(cam.viewmatrix), t(cam.projmatrix), np.tan(cam.fovx / 2),
-        np.tan(cam.fovy / 2), 3, t(cam.campos), image_height=S, image_width=S, grad_mode=grad_mode)
+        np.tan(cam.fovy / 2), degree, t(cam.campos), image_height=S, image_width=S, grad_mode=grad_mode)
     assert parity.bit_mismatch(out["image"].detach().cpu().numpy(), image.detach().cpu().numpy()) == 0
     assert torch.equal(out["available_pts"], radii > 0)
     (image * g).sum().backward()
@@ -108,7 +108,7 @@ def test_renderer_render_is_preamble_plus_function(grad_mode):
     n = lambda x: x.detach().cpu().numpy()
     m, o, s, q, sh = (n(mean), n(torch.sigmoid(opac_l)), n(torch.exp(svec)),
                       n(torch.nn.functional.normalize(quat)), n(shs))
-    f = oracle.forward(oracle.RasterSettings.from_camera(cam), m, s, q, o, sh)
+    f = oracle.forward(oracle.RasterSettings.from_camera(cam, degree=degree), m, s, q, o, sh)
     np.testing.assert_allclose(out["image"].detach().cpu().numpy(), f["color"], rtol=1e-4, atol=1e-5)
 
 
