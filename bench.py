@@ -34,7 +34,7 @@ UNIT = "views/s"
 PEAKS_FILE = os.path.join(ROOT, "MEASURED_PEAKS.json")
 FALLBACK_HBM_GBS = 6650.0
 # DRAM bytes (read + write) per launch, from one ncu capture of the default
-# workload (500k Gaussians, 512x512; profiles/dram_traffic_500k_512x512.md)
+# workload (500k Gaussians, 512x512; dram__bytes_read.sum + dram__bytes_write.sum)
 NCU_TRAFFIC_500K_512 = {"sort_onesweep": 49.0e6, "preprocess": 181.2e6, "duplicate": 12.2e6,
                         "sort_histogram": 23.7e6, "backward_gaussians": 232.4e6}
 
@@ -715,7 +715,7 @@ def run_sortscan(a):
                            "frac": round(sort_gbs / peak, 4), "peak_source": src,
                            "bytes_per_key": pass_bytes,
                            # DRAM bytes of one sort call (histogram + 5 passes), one ncu capture of this
-                           # workload (profiles/sort_scan_20M_2M.md); algorithmic: 128 B x 20M = 2.56 GB
+                           # workload; algorithmic: 128 B x 20M = 2.56 GB
                            "traffic": 2.35e9, "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum"},
               "sort": {"ms": round(ms_sort, 4), "ms_all": [round(x, 4) for x in all_sort],
                        "gkeys_per_s": round(n_sort / (ms_sort * 1e-3) / 1e9, 3),
