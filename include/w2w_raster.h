@@ -19,6 +19,21 @@
  *   position; image outputs are CHW float32; radii int32[P].
  *
  * Status codes: 0 ok, otherwise a W2W_ERR_* value (w2w_status_string()).
+ *
+ * Device-side failures.  The sort's and the scans' single-pass lookbacks wait
+ * on their predecessors with an iteration limit; a wait that runs out, or an
+ * instance count beyond the state's capacity, sets bits in a device error
+ * word instead of hanging or faulting.  w2w_forward_geometry(_raw) and
+ * w2w_batch_forward_geometry read their word back (they synchronise anyway)
+ * and return W2W_ERR_TIMEOUT / W2W_ERR_CAPACITY.  The other entry points with
+ * such waits (w2w_forward_render, w2w_batch_forward_render, w2w_sort_pairs_u64,
+ * w2w_scan_u32, w2w_scan_u32_noalloc) return once their work is enqueued, so
+ * by default their status covers the launches only and the word is left for
+ * the caller: w2w_state_error(binning_state, 1, stream) after a render,
+ * w2w_scratch_error(scratch, stream) after a sort or scan,
+ * w2w_scan_noalloc_error(stream) after the allocation-free scan.  With
+ * w2w_set_error_check(1) those entry points synchronise their stream before
+ * returning and return W2W_ERR_TIMEOUT / W2W_ERR_CAPACITY themselves.
  */
 #ifndef W2W_RASTER_H
 #define W2W_RASTER_H
@@ -69,6 +84,16 @@ typedef struct {
 int w2w_version(void);
 const char* w2w_status_string(int status);
 
+/* Error-word checking of the entry points that return before their device
+ * waits finish (see above): 0 = leave the word for the caller (default),
+ * 1 = synchronise the stream and return the word's status.  Process-wide;
+ * returns the previous mode.  No counterpart in the reference, which checks
+ * nothing (rasterize_points.cu). */
+int w2w_set_error_check(int mode);
+/* Status of the error word of a sort or scan scratch buffer (the 32-bit word
+ * at byte 4 of every stage scratch); synchronises `stream`. */
+int w2w_scratch_error(const void* scratch, w2w_stream_t stream);
+
 /* ---- state buffer sizes (bytes; caller allocates device memory) ------------
  * Replace the resize callbacks of rasterize_points.cu:81-87 and the
  * cudaMalloc'd temporaries of gaussianRasterizer.cu:209-212. */
@@ -108,7 +133,9 @@ int w2w_forward_geometry(const w2w_settings* s, const float* means3D, const floa
  * compat_spill=1 keys are emitted over the reference's emission rectangle;
  * where that writes past a Gaussian's allocation the lowest-index writer owns
  * each slot (the reference leaves this to a race).  Outputs: color [3,H,W],
- * depth [1,H,W], alpha [1,H,W] (sum of alpha*T, as the reference). */
+ * depth [1,H,W], alpha [1,H,W] (sum of alpha*T, as the reference).  The
+ * sort's error word is the binning state's (w2w_state_error(binning_state,
+ * 1, ...)), returned here in checked mode (w2w_set_error_check). */
 int w2w_forward_render(const w2w_settings* s, const void* geom_state, const w2w_geometry_info* info,
                        void* binning_state, void* image_state, float* out_color, float* out_depth,
                        float* out_alpha, w2w_stream_t stream);
@@ -158,14 +185,19 @@ int w2w_scan_u32(const uint32_t* in, uint32_t* out, long long n, int exclusive, 
  * device array inside the library (about 32 KB, held by every GPU that loads
  * the library until the process exits), so the caller passes only the input
  * and output.  At most W2W_SCAN_NOALLOC_MAX elements; larger n returns
- * W2W_ERR_CAPACITY without launching anything.  The first call on a device
- * looks up the array's device address (done once per device, with that
- * device current), so make that first call before any stream capture on the
- * device.  All calls share the one array and each clears the parts it needs
+ * W2W_ERR_CAPACITY without launching anything.  Every call looks up the
+ * array's address in the caller's current CUDA context (a host-side lookup,
+ * right for any context, including one re-created after cudaDeviceReset); the
+ * first call in a context also loads the library's device code into it, so
+ * make that first call before any stream capture on the device.  All calls share the one array and each clears the parts it needs
  * before use; calls that overlap on the GPU (other streams, other threads)
  * race on it, so serialise them.  Never calls cudaMalloc or cudaFree. */
 #define W2W_SCAN_NOALLOC_MAX (1LL << 24)
 int w2w_scan_u32_noalloc(const uint32_t* in, uint32_t* out, long long n, int exclusive, w2w_stream_t stream);
+/* Status of the allocation-free scan's error word (inside the library's
+ * fixed array): W2W_ERR_TIMEOUT if a lookback wait of the last call ran out
+ * (its output is then invalid).  Synchronises `stream`. */
+int w2w_scan_noalloc_error(w2w_stream_t stream);
 
 /* Renderer.render's path on its raw parameters (Renderer.py:164-192): the
  * activation preamble (sigmoid opacity, exp scales, normalised quaternion,
@@ -314,6 +346,27 @@ unsigned w2w_stage_timing_mask(unsigned mask);
 int w2w_stage_count(void);
 const char* w2w_stage_name(int stage);
 int w2w_stage_times(double* ms, long long* launches, int max_stages);
+/* Arithmetic throughput probe (no counterpart in the reference): kind 0 runs
+ * FP32 fused multiply-adds, kind 1 SFU base-2 exponentials, on `blocks` CTAs
+ * of 256 threads, `iters` steps of 8 independent chains per thread.  *ops
+ * receives the instruction count (blocks * 256 * iters * 8); time the launch
+ * with events on `stream` to get the GPU's issue rate, the denominator of the
+ * per-pixel passes' roofline.  `out` (>= 256 floats, device) is never
+ * written in practice; it keeps the chains from being optimised away. */
+int w2w_throughput_probe(int kind, long long iters, int blocks, float* out, long long* ops, w2w_stream_t stream);
+
+/* ---- test hooks --------------------------------------------------------------
+ * For tests of the failure path (no counterpart in the reference).
+ * w2w_test_set_spin_limit: the iteration limit of every bounded device wait
+ * (0 restores the default, 2^22 polls: a second or two); returns the previous
+ * limit.  w2w_test_unpublished_tile: the CTA of tile `tile` of a stage (0: the
+ * stand-alone scans, 1: the first pass of every sort, 2: the scan fused into
+ * w2w_forward_geometry) skips publishing its status, so that the waits behind
+ * it run out and the call reports W2W_ERR_TIMEOUT; -1 turns it off.  Returns
+ * the previous tile (-2 for an unknown stage).  Nothing faults or hangs: every
+ * wait ends at its limit.  Process-wide settings read at launch. */
+unsigned w2w_test_set_spin_limit(unsigned limit);
+long long w2w_test_unpublished_tile(int stage, long long tile);
 
 #ifdef __cplusplus
 }

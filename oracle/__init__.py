@@ -90,6 +90,17 @@ def set_variants(variants: dict):
         L.orc_set_variant(VARIANT_NAMES.index(k), int(v))
 
 
+def set_threads(n: int) -> None:
+    """Threads of the oracle's per-pixel and per-Gaussian loops (default 1).
+    Results do not depend on it, except the backward's per-Gaussian sums,
+    whose order of addition (in double) follows the thread schedule."""
+    lib().orc_set_threads(int(n))
+
+
+def get_threads() -> int:
+    return int(lib().orc_get_threads())
+
+
 def get_variants() -> dict:
     L = lib()
     return {n: L.orc_get_variant(i) for i, n in enumerate(VARIANT_NAMES)}
@@ -251,9 +262,15 @@ def blend(s: RasterSettings, geom: dict, ranges, point_list, precision: str = "f
 
 
 def backward(fwd: dict, dL_dcolor, dL_ddepth=None, dL_dalpha=None, mode: str = "reference",
-             tan_fovx: float | None = None, tan_fovy: float | None = None, scale_modifier: float = 1.0) -> dict:
+             tan_fovx: float | None = None, tan_fovy: float | None = None, scale_modifier: float = 1.0,
+             error_bounds: bool = True) -> dict:
     """Gradients for the forward ``fwd``.  Returns the eight tensors of
-    ``rasterize_gaussians_backward`` (rasterize_points.cu:139-148) by name."""
+    ``rasterize_gaussians_backward`` (rasterize_points.cu:139-148) by name.
+    ``error_bounds`` (reference mode): also return ``abs_<name>``, the sums of
+    absolute per-pair contributions behind each gradient (the scale of fp32
+    accumulation-order error), which costs nine extra per-Gaussian passes;
+    the timed CPU baseline turns it off, as the reference computes no such
+    thing."""
     L = lib()
     s: RasterSettings = fwd["settings"]
     prec = fwd["precision"]
@@ -272,12 +289,12 @@ def backward(fwd: dict, dL_dcolor, dL_ddepth=None, dL_dalpha=None, mode: str = "
              dL_dscales=np.zeros((P, 3), R_), dL_drotations=np.zeros((P, 4), R_))
     if mode == "reference":
         dm2 = np.zeros((P, 3)); dcon = np.zeros((P, 4)); dop = np.zeros(P); dcol = np.zeros((P, 3)); ddep = np.zeros(P)
-        abs_sum = np.zeros((P, 10))
+        abs_sum = np.zeros((P, 10)) if error_bounds else None
         getattr(L, "orc_backward_render" + sfx)(
-            ctypes.byref(cfg), _p(fwd["ranges"]), _p(pl), _p(fwd["means2D"]), _p(fwd["conic_opac"]),
+            ctypes.byref(cfg), ctypes.c_int(P), _p(fwd["ranges"]), _p(pl), _p(fwd["means2D"]), _p(fwd["conic_opac"]),
             _p(fwd["rgb"]), _p(fwd["depth"]), _p(np.ascontiguousarray(fwd["alpha"].reshape(-1))),
             _p(np.ascontiguousarray(fwd["n_contrib"].reshape(-1))), _p(dLc), _p(dLd), _p(dLa),
-            _p(dm2), _p(dcon), _p(dop), _p(dcol), _p(ddep), _p(abs_sum))
+            _p(dm2), _p(dcon), _p(dop), _p(dcol), _p(ddep), _p(abs_sum) if error_bounds else None)
         tfx = s.tan_fovx if tan_fovx is None else tan_fovx
         tfy = s.tan_fovy if tan_fovy is None else tan_fovy
         h_x = np.float32(W) / (np.float32(2.0) * np.float32(tfx))
@@ -300,6 +317,8 @@ def backward(fwd: dict, dL_dcolor, dL_ddepth=None, dL_dalpha=None, mode: str = "
             _p(g["dL_dmeans3D"]), _p(g["dL_dsh"]), _p(g["dL_dscales"]), _p(g["dL_drotations"]))
         g["dL_dconic"] = dconR
         g["dL_ddepths"] = ddepR
+        if not error_bounds:
+            return g
         # sums of |per-pair contribution|: the scale of fp32 accumulation-order error
         g["abs_dL_dcolors"] = abs_sum[:, 0:3]
         g["abs_dL_dmeans2D"] = np.concatenate([abs_sum[:, 4:6], np.zeros((P, 1))], axis=1)

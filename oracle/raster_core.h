@@ -333,15 +333,56 @@ static void SFX(sh_one)(const float* mean, const float* campos, const float* sh,
 
 /* Whole per-Gaussian preprocessing for P Gaussians.  Arrays are float32 in
  * both instantiations except the REAL outputs. */
-void SFX(orc_preprocess)(const orc_cfg* cfg, int P,
-                         const float* means3D, const float* scales, const float* rots,
-                         const float* opac, const float* sh,
-                         REAL* cov3D, REAL* cov2D, REAL* det, REAL* conic_opac,
-                         REAL* means2D, REAL* depth, int32_t* radii, uint32_t* tiles,
-                         int32_t* rects, REAL* rgb, uint8_t* clamped,
-                         uint8_t* visible, uint8_t* clamp_hit, double* adr_margin)
+typedef struct {
+    const orc_cfg* cfg;
+    int P;
+    const float* means3D;
+    const float* scales;
+    const float* rots;
+    const float* opac;
+    const float* sh;
+    REAL* cov3D;
+    REAL* cov2D;
+    REAL* det;
+    REAL* conic_opac;
+    REAL* means2D;
+    REAL* depth;
+    int32_t* radii;
+    uint32_t* tiles;
+    int32_t* rects;
+    REAL* rgb;
+    uint8_t* clamped;
+    uint8_t* visible;
+    uint8_t* clamp_hit;
+    double* adr_margin;
+} SFX(orc_preprocess_ctx);
+static void SFX(orc_preprocess_part)(void* vc_, long long lo_, long long hi_, int tid_)
 {
-    for (int i = 0; i < P; ++i) {
+    SFX(orc_preprocess_ctx)* c_ = (SFX(orc_preprocess_ctx)*)vc_;
+    const orc_cfg* cfg = c_->cfg;
+    (void)c_->P;
+    const float* means3D = c_->means3D;
+    const float* scales = c_->scales;
+    const float* rots = c_->rots;
+    const float* opac = c_->opac;
+    const float* sh = c_->sh;
+    REAL* cov3D = c_->cov3D;
+    REAL* cov2D = c_->cov2D;
+    REAL* det = c_->det;
+    REAL* conic_opac = c_->conic_opac;
+    REAL* means2D = c_->means2D;
+    REAL* depth = c_->depth;
+    int32_t* radii = c_->radii;
+    uint32_t* tiles = c_->tiles;
+    int32_t* rects = c_->rects;
+    REAL* rgb = c_->rgb;
+    uint8_t* clamped = c_->clamped;
+    uint8_t* visible = c_->visible;
+    uint8_t* clamp_hit = c_->clamp_hit;
+    double* adr_margin = c_->adr_margin;
+    (void)tid_;
+
+    for (int i = (int)lo_; i < (int)hi_; ++i) {
         int ch = 0;
         for (int k = 0; k < 6; ++k) cov3D[6 * i + k] = 0;
         for (int k = 0; k < 4; ++k) conic_opac[4 * i + k] = 0;
@@ -362,6 +403,19 @@ void SFX(orc_preprocess)(const orc_cfg* cfg, int P,
                     rgb + 3 * i, clamped + 3 * i);
     }
 }
+
+void SFX(orc_preprocess)(const orc_cfg* cfg, int P,
+                         const float* means3D, const float* scales, const float* rots,
+                         const float* opac, const float* sh,
+                         REAL* cov3D, REAL* cov2D, REAL* det, REAL* conic_opac,
+                         REAL* means2D, REAL* depth, int32_t* radii, uint32_t* tiles,
+                         int32_t* rects, REAL* rgb, uint8_t* clamped,
+                         uint8_t* visible, uint8_t* clamp_hit, double* adr_margin)
+{
+    SFX(orc_preprocess_ctx) c_ = {cfg, P, means3D, scales, rots, opac, sh, cov3D, cov2D, det, conic_opac, means2D, depth, radii, tiles, rects, rgb, clamped, visible, clamp_hit, adr_margin};
+    orc_parallel_for(P, 4096, SFX(orc_preprocess_part), &c_);
+}
+
 
 /* ------------------------------------------------------------------------ */
 /* Forward: key emission (prepareSort.cu:178-205, 239-301)                  */
@@ -450,15 +504,46 @@ static inline REAL SFX(blend_det)(const REAL* cov2D) {
  * pixel from its threshold.  sig[H*W] (may be NULL): a hash of the pixel's
  * blend decisions (which entries were blended, which hit the 0.99 clamp),
  * so callers can tell when a perturbation changed a discrete decision. */
-void SFX(orc_blend)(const orc_cfg* cfg, const uint32_t* ranges, const uint32_t* point_list,
-                    const REAL* means2D, const REAL* cov2D, const REAL* conic_opac,
-                    const REAL* rgb, const REAL* depth,
-                    REAL* out_color, REAL* out_depth, REAL* out_alpha, uint32_t* n_contrib,
-                    REAL* out_T, double* margin, uint64_t* sig)
+typedef struct {
+    const orc_cfg* cfg;
+    const uint32_t* ranges;
+    const uint32_t* point_list;
+    const REAL* means2D;
+    const REAL* cov2D;
+    const REAL* conic_opac;
+    const REAL* rgb;
+    const REAL* depth;
+    REAL* out_color;
+    REAL* out_depth;
+    REAL* out_alpha;
+    uint32_t* n_contrib;
+    REAL* out_T;
+    double* margin;
+    uint64_t* sig;
+} SFX(orc_blend_ctx);
+static void SFX(orc_blend_part)(void* vc_, long long lo_, long long hi_, int tid_)
 {
+    SFX(orc_blend_ctx)* c_ = (SFX(orc_blend_ctx)*)vc_;
+    const orc_cfg* cfg = c_->cfg;
+    const uint32_t* ranges = c_->ranges;
+    const uint32_t* point_list = c_->point_list;
+    const REAL* means2D = c_->means2D;
+    const REAL* cov2D = c_->cov2D;
+    const REAL* conic_opac = c_->conic_opac;
+    const REAL* rgb = c_->rgb;
+    const REAL* depth = c_->depth;
+    REAL* out_color = c_->out_color;
+    REAL* out_depth = c_->out_depth;
+    REAL* out_alpha = c_->out_alpha;
+    uint32_t* n_contrib = c_->n_contrib;
+    REAL* out_T = c_->out_T;
+    double* margin = c_->margin;
+    uint64_t* sig = c_->sig;
+    (void)tid_;
+
     const int W = cfg->W, H = cfg->H, gw = (W + 15) / 16;
     const REAL min_alpha = (REAL)(1.0f / 255.0f), min_T = (REAL)0.0001f, max_alpha = (REAL)0.99f;
-    for (int py = 0; py < H; ++py) {
+    for (int py = (int)lo_; py < (int)hi_; ++py) {
         for (int px = 0; px < W; ++px) {
             int tile = (py / 16) * gw + (px / 16);
             uint32_t s = ranges[2 * tile], e = ranges[2 * tile + 1];
@@ -508,6 +593,17 @@ void SFX(orc_blend)(const orc_cfg* cfg, const uint32_t* ranges, const uint32_t* 
     }
 }
 
+void SFX(orc_blend)(const orc_cfg* cfg, const uint32_t* ranges, const uint32_t* point_list,
+                    const REAL* means2D, const REAL* cov2D, const REAL* conic_opac,
+                    const REAL* rgb, const REAL* depth,
+                    REAL* out_color, REAL* out_depth, REAL* out_alpha, uint32_t* n_contrib,
+                    REAL* out_T, double* margin, uint64_t* sig)
+{
+    SFX(orc_blend_ctx) c_ = {cfg, ranges, point_list, means2D, cov2D, conic_opac, rgb, depth, out_color, out_depth, out_alpha, n_contrib, out_T, margin, sig};
+    orc_parallel_for(cfg->H, 1, SFX(orc_blend_part), &c_);
+}
+
+
 /* ------------------------------------------------------------------------ */
 /* Backward: per-pixel gradients, back to front (backward.cu:521-665)       */
 /* ------------------------------------------------------------------------ */
@@ -517,20 +613,39 @@ void SFX(orc_blend)(const orc_cfg* cfg, const uint32_t* ranges, const uint32_t* 
  *   dcolor[P*3], ddepth[P].
  * The pixel-to-NDC factors 0.5*W and 0.5*H come from the gradient image size
  * (backward.cu:586-587). */
-void SFX(orc_backward_render)(const orc_cfg* cfg, const uint32_t* ranges, const uint32_t* point_list,
-                              const REAL* means2D, const REAL* conic_opac, const REAL* rgb,
-                              const REAL* depth, const REAL* out_alpha, const uint32_t* n_contrib,
-                              const float* dL_dpix, const float* dL_ddepth, const float* dL_dalpha,
-                              double* dmean2D, double* dconic, double* dopac, double* dcolor,
-                              double* ddepth, double* abs_sum)
+typedef struct {
+    const orc_cfg* cfg; int P; const uint32_t* ranges; const uint32_t* point_list;
+    const REAL* means2D; const REAL* conic_opac; const REAL* rgb; const REAL* depth; const REAL* out_alpha;
+    const uint32_t* n_contrib; const float* dL_dpix; const float* dL_ddepth; const float* dL_dalpha;
+    double* dmean2D; double* dconic; double* dopac; double* dcolor; double* ddepth; double* abs_sum;
+    double* priv; size_t stride;
+} SFX(orc_backward_render_ctx);
+
+/* Rows [lo_, hi_) of the per-pixel backward.  With several threads each
+ * accumulates into its own zeroed copy of the outputs (priv), summed in
+ * thread order at the end. */
+static void SFX(orc_backward_render_part)(void* vc_, long long lo_, long long hi_, int tid_)
 {
+    SFX(orc_backward_render_ctx)* c_ = (SFX(orc_backward_render_ctx)*)vc_;
+    const orc_cfg* cfg = c_->cfg; const uint32_t* ranges = c_->ranges; const uint32_t* point_list = c_->point_list;
+    const REAL* means2D = c_->means2D; const REAL* conic_opac = c_->conic_opac; const REAL* rgb = c_->rgb;
+    const REAL* depth = c_->depth; const REAL* out_alpha = c_->out_alpha; const uint32_t* n_contrib = c_->n_contrib;
+    const float* dL_dpix = c_->dL_dpix; const float* dL_ddepth = c_->dL_ddepth; const float* dL_dalpha = c_->dL_dalpha;
+    double *m2 = c_->dmean2D, *cn = c_->dconic, *op = c_->dopac, *cl = c_->dcolor, *dp = c_->ddepth, *as_ = c_->abs_sum;
+    if (c_->priv) {
+        const size_t P = (size_t)c_->P;
+        double* b = c_->priv + (size_t)tid_ * P * c_->stride;
+        m2 = b; cn = b + 3 * P; op = b + 7 * P; cl = b + 8 * P; dp = b + 11 * P;
+        as_ = c_->abs_sum ? b + 12 * P : NULL;
+    }
+
     /* abs_sum[P*10] (may be NULL): per Gaussian, the sum of |contribution| of
      * each accumulated value (colour r,g,b, depth, mean2D x,y, conic x,y,w,
      * opacity) -- the scale of fp32 accumulation-order error */
     const int W = cfg->W, H = cfg->H, gw = (W + 15) / 16;
     const REAL ddelx_dx = (REAL)(0.5 * W), ddely_dy = (REAL)(0.5 * H);
     const REAL bg[3] = {cfg->bg[0], cfg->bg[1], cfg->bg[2]};
-    for (int py = 0; py < H; ++py) {
+    for (int py = (int)lo_; py < (int)hi_; ++py) {
         for (int px = 0; px < W; ++px) {
             int tile = (py / 16) * gw + (px / 16);
             uint32_t s = ranges[2 * tile], e = ranges[2 * tile + 1];
@@ -567,13 +682,13 @@ void SFX(orc_backward_render)(const orc_cfg* cfg, const uint32_t* ranges, const 
                     acc[c] = last_a * last_c[c] + ((REAL)1 - last_a) * acc[c];
                     last_c[c] = col;
                     dLdo = dLdo + (col - acc[c]) * dLp[c];
-                    dcolor[3 * id + c] += (double)(dchdc * dLp[c]);
+                    cl[3 * id + c] += (double)(dchdc * dLp[c]);
                 }
                 REAL cd = depth[id];
                 accd = last_a * last_d + ((REAL)1 - last_a) * accd;
                 last_d = cd;
                 dLdo = dLdo + (cd - accd) * dLd;
-                ddepth[id] += (double)(a * T * dLd);
+                dp[id] += (double)(a * T * dLd);
                 acca = last_a + ((REAL)1 - last_a) * acca;
                 dLdo = dLdo + ((REAL)1 - acca) * dLa;
                 dLdo = dLdo * T;
@@ -583,14 +698,14 @@ void SFX(orc_backward_render)(const orc_cfg* cfg, const uint32_t* ranges, const 
                 REAL gdx = G * dx, gdy = G * dy;
                 REAL dGdx = -gdx * co[0] - gdy * co[1];
                 REAL dGdy = -gdy * co[2] - gdx * co[1];
-                dmean2D[3 * id] += (double)(dLdG * dGdx * ddelx_dx);
-                dmean2D[3 * id + 1] += (double)(dLdG * dGdy * ddely_dy);
-                dconic[4 * id] += (double)((REAL)-0.5 * gdx * dx * dLdG);
-                dconic[4 * id + 1] += (double)((REAL)-0.5 * gdx * dy * dLdG);
-                dconic[4 * id + 3] += (double)((REAL)-0.5 * gdy * dy * dLdG);
-                dopac[id] += (double)(G * dLdo);
-                if (abs_sum) {
-                    double* as = abs_sum + 10 * (size_t)id;
+                m2[3 * id] += (double)(dLdG * dGdx * ddelx_dx);
+                m2[3 * id + 1] += (double)(dLdG * dGdy * ddely_dy);
+                cn[4 * id] += (double)((REAL)-0.5 * gdx * dx * dLdG);
+                cn[4 * id + 1] += (double)((REAL)-0.5 * gdx * dy * dLdG);
+                cn[4 * id + 3] += (double)((REAL)-0.5 * gdy * dy * dLdG);
+                op[id] += (double)(G * dLdo);
+                if (as_) {
+                    double* as = as_ + 10 * (size_t)id;
                     for (int c = 0; c < 3; ++c) as[c] += fabs((double)(dchdc * dLp[c]));
                     as[3] += fabs((double)(a * T * dLd));
                     as[4] += fabs((double)(dLdG * dGdx * ddelx_dx));
@@ -605,17 +720,79 @@ void SFX(orc_backward_render)(const orc_cfg* cfg, const uint32_t* ranges, const 
     }
 }
 
+void SFX(orc_backward_render)(const orc_cfg* cfg, int P, const uint32_t* ranges, const uint32_t* point_list,
+                              const REAL* means2D, const REAL* conic_opac, const REAL* rgb,
+                              const REAL* depth, const REAL* out_alpha, const uint32_t* n_contrib,
+                              const float* dL_dpix, const float* dL_ddepth, const float* dL_dalpha,
+                              double* dmean2D, double* dconic, double* dopac, double* dcolor,
+                              double* ddepth, double* abs_sum)
+{
+    /* abs_sum[P*10] (may be NULL): per Gaussian, the sum of |contribution| of
+     * each accumulated value (colour r,g,b, depth, mean2D x,y, conic x,y,w,
+     * opacity) -- the scale of fp32 accumulation-order error */
+    const int nt = orc_threads > 1 ? orc_threads : 1;
+    const size_t stride = abs_sum ? 22 : 12;
+    double* priv = nt > 1 ? (double*)calloc((size_t)nt * (size_t)P * stride, sizeof(double)) : NULL;
+    SFX(orc_backward_render_ctx) c_ = {cfg, P, ranges, point_list, means2D, conic_opac, rgb, depth, out_alpha,
+                                       n_contrib, dL_dpix, dL_ddepth, dL_dalpha, dmean2D, dconic, dopac, dcolor,
+                                       ddepth, abs_sum, priv, stride};
+    if (priv == NULL) {
+        SFX(orc_backward_render_part)(&c_, 0, cfg->H, 0);
+        return;
+    }
+    orc_parallel_for(cfg->H, 1, SFX(orc_backward_render_part), &c_);
+    for (int t = 0; t < nt; ++t) {
+        const double* b = priv + (size_t)t * (size_t)P * stride;
+        const size_t Pz = (size_t)P;
+        for (size_t i = 0; i < 3 * Pz; ++i) dmean2D[i] += b[i];
+        for (size_t i = 0; i < 4 * Pz; ++i) dconic[i] += b[3 * Pz + i];
+        for (size_t i = 0; i < Pz; ++i) dopac[i] += b[7 * Pz + i];
+        for (size_t i = 0; i < 3 * Pz; ++i) dcolor[i] += b[8 * Pz + i];
+        for (size_t i = 0; i < Pz; ++i) ddepth[i] += b[11 * Pz + i];
+        if (abs_sum)
+            for (size_t i = 0; i < 10 * Pz; ++i) abs_sum[i] += b[12 * Pz + i];
+    }
+    free(priv);
+}
+
 /* ------------------------------------------------------------------------ */
 /* Backward: dL/dconic -> dL/dcov3D and the Jacobian part of dL/dmean3D     */
 /* (backward.cu:27-227)                                                     */
 /* ------------------------------------------------------------------------ */
 /* h_x, h_y = W/(2 tan_fovx), H/(2 tan_fovy) (gradientPass.cu:119-120).
  * ASSIGNS dmean3D for visible Gaussians (backward.cu:226). */
-void SFX(orc_backward_cov2d)(int P, const float* means3D, const int32_t* radii, const REAL* cov3D,
-                             REAL h_x, REAL h_y, REAL tan_fovx, REAL tan_fovy, const float* view,
-                             const REAL* dconic, REAL* dcov3D, REAL* dmean3D)
+typedef struct {
+    int P;
+    const float* means3D;
+    const int32_t* radii;
+    const REAL* cov3D;
+    REAL h_x;
+    REAL h_y;
+    REAL tan_fovx;
+    REAL tan_fovy;
+    const float* view;
+    const REAL* dconic;
+    REAL* dcov3D;
+    REAL* dmean3D;
+} SFX(orc_backward_cov2d_ctx);
+static void SFX(orc_backward_cov2d_part)(void* vc_, long long lo_, long long hi_, int tid_)
 {
-    for (int i = 0; i < P; ++i) {
+    SFX(orc_backward_cov2d_ctx)* c_ = (SFX(orc_backward_cov2d_ctx)*)vc_;
+    (void)c_->P;
+    const float* means3D = c_->means3D;
+    const int32_t* radii = c_->radii;
+    const REAL* cov3D = c_->cov3D;
+    REAL h_x = c_->h_x;
+    REAL h_y = c_->h_y;
+    REAL tan_fovx = c_->tan_fovx;
+    REAL tan_fovy = c_->tan_fovy;
+    const float* view = c_->view;
+    const REAL* dconic = c_->dconic;
+    REAL* dcov3D = c_->dcov3D;
+    REAL* dmean3D = c_->dmean3D;
+    (void)tid_;
+
+    for (int i = (int)lo_; i < (int)hi_; ++i) {
         if (!(radii[i] > 0)) continue;
         const REAL* pc = cov3D + 6 * i;
         REAL cx = means3D[3 * i], cy = means3D[3 * i + 1], cz = means3D[3 * i + 2];
@@ -689,24 +866,73 @@ void SFX(orc_backward_cov2d)(int P, const float* means3D, const int32_t* radii, 
     }
 }
 
+void SFX(orc_backward_cov2d)(int P, const float* means3D, const int32_t* radii, const REAL* cov3D,
+                             REAL h_x, REAL h_y, REAL tan_fovx, REAL tan_fovy, const float* view,
+                             const REAL* dconic, REAL* dcov3D, REAL* dmean3D)
+{
+    SFX(orc_backward_cov2d_ctx) c_ = {P, means3D, radii, cov3D, h_x, h_y, tan_fovx, tan_fovy, view, dconic, dcov3D, dmean3D};
+    orc_parallel_for(P, 4096, SFX(orc_backward_cov2d_part), &c_);
+}
+
+
 /* ------------------------------------------------------------------------ */
 /* Backward: mean2D/depth -> mean3D, SH, scale and rotation gradients       */
 /* (backward.cu:229-519)                                                    */
 /* ------------------------------------------------------------------------ */
-void SFX(orc_backward_preprocess)(int P, int M, const float* means3D, const int32_t* radii,
-                                  const float* sh, const uint8_t* clamped, const float* scales,
-                                  const float* rots, REAL scale_mod, const float* view,
-                                  const float* proj, const float* campos, const REAL* dmean2D,
-                                  const REAL* dcolor, const REAL* ddepth, const REAL* dcov3D,
-                                  REAL* dmean3D, REAL* dsh, REAL* dscale, REAL* drot)
+typedef struct {
+    int P;
+    int M;
+    const float* means3D;
+    const int32_t* radii;
+    const float* sh;
+    const uint8_t* clamped;
+    const float* scales;
+    const float* rots;
+    REAL scale_mod;
+    const float* view;
+    const float* proj;
+    const float* campos;
+    const REAL* dmean2D;
+    const REAL* dcolor;
+    const REAL* ddepth;
+    const REAL* dcov3D;
+    REAL* dmean3D;
+    REAL* dsh;
+    REAL* dscale;
+    REAL* drot;
+} SFX(orc_backward_preprocess_ctx);
+static void SFX(orc_backward_preprocess_part)(void* vc_, long long lo_, long long hi_, int tid_)
 {
+    SFX(orc_backward_preprocess_ctx)* c_ = (SFX(orc_backward_preprocess_ctx)*)vc_;
+    (void)c_->P;
+    int M = c_->M;
+    const float* means3D = c_->means3D;
+    const int32_t* radii = c_->radii;
+    const float* sh = c_->sh;
+    const uint8_t* clamped = c_->clamped;
+    const float* scales = c_->scales;
+    const float* rots = c_->rots;
+    REAL scale_mod = c_->scale_mod;
+    const float* view = c_->view;
+    const float* proj = c_->proj;
+    const float* campos = c_->campos;
+    const REAL* dmean2D = c_->dmean2D;
+    const REAL* dcolor = c_->dcolor;
+    const REAL* ddepth = c_->ddepth;
+    const REAL* dcov3D = c_->dcov3D;
+    REAL* dmean3D = c_->dmean3D;
+    REAL* dsh = c_->dsh;
+    REAL* dscale = c_->dscale;
+    REAL* drot = c_->drot;
+    (void)tid_;
+
     static const REAL C0 = (REAL)0.28209479177387814f, C1 = (REAL)0.4886025119029199f;
     static const REAL C2[5] = {(REAL)1.0925484305920792f, (REAL)-1.0925484305920792f, (REAL)0.31539156525252005f,
                                (REAL)-1.0925484305920792f, (REAL)0.5462742152960396f};
     static const REAL C3[7] = {(REAL)-0.5900435899266435f, (REAL)2.890611442640554f, (REAL)-0.4570457994644658f,
                                (REAL)0.3731763325901154f, (REAL)-0.4570457994644658f, (REAL)1.445305721320277f,
                                (REAL)-0.5900435899266435f};
-    for (int i = 0; i < P; ++i) {
+    for (int i = (int)lo_; i < (int)hi_; ++i) {
         if (radii[i] <= 0) continue;
         REAL wx = means3D[3 * i], wy = means3D[3 * i + 1], wz = means3D[3 * i + 2];
         const float* m = proj;
@@ -818,6 +1044,18 @@ void SFX(orc_backward_preprocess)(int P, int M, const float* means3D, const int3
         drot[4 * i + 3] = (REAL)4 * (sz * (a31 * xw - a32 * xx + a33 * qxy) - sy * (a21 * qxz - a22 * zw + a23 * qyz) + sx * (a12 * qyz - a13 * zz + a11 * yy));
     }
 }
+
+void SFX(orc_backward_preprocess)(int P, int M, const float* means3D, const int32_t* radii,
+                                  const float* sh, const uint8_t* clamped, const float* scales,
+                                  const float* rots, REAL scale_mod, const float* view,
+                                  const float* proj, const float* campos, const REAL* dmean2D,
+                                  const REAL* dcolor, const REAL* ddepth, const REAL* dcov3D,
+                                  REAL* dmean3D, REAL* dsh, REAL* dscale, REAL* drot)
+{
+    SFX(orc_backward_preprocess_ctx) c_ = {P, M, means3D, radii, sh, clamped, scales, rots, scale_mod, view, proj, campos, dmean2D, dcolor, ddepth, dcov3D, dmean3D, dsh, dscale, drot};
+    orc_parallel_for(P, 4096, SFX(orc_backward_preprocess_part), &c_);
+}
+
 
 /* ------------------------------------------------------------------------ */
 /* Backward, exact mode: the true derivative of the forward restated above. */

@@ -13,12 +13,13 @@
  * The per-element arithmetic lives in raster_core.h, instantiated for float
  * (bit-level restatement) and double (fp64 re-evaluation).
  *
- * Build: gcc -O2 -ffp-contract=off -fno-fast-math -fPIC -shared (see Makefile).
+ * Build: gcc -O2 -ffp-contract=off -fno-fast-math -pthread -fPIC -shared (see Makefile).
  */
 #include <math.h>
 #include <stdint.h>
 #include <stdlib.h>
 #include <string.h>
+#include <pthread.h>
 
 typedef struct {
     int W, H;          /* image size */
@@ -51,6 +52,56 @@ enum {
     V_COUNT
 };
 static int orc_var[V_COUNT];
+
+/* Threads of the per-pixel and per-Gaussian loops (1 = serial, the default:
+ * the tests' results are then independent of the machine).  Only the timed
+ * CPU baseline raises it. */
+static int orc_threads = 1;
+void orc_set_threads(int n) { orc_threads = n > 1 ? (n < 1024 ? n : 1024) : 1; }
+int orc_get_threads(void) { return orc_threads; }
+
+/* Parallel loop over [0, n): workers take `chunk` indices at a time from a
+ * shared counter and call fn(ctx, lo, hi, worker).  Worker 0 is the calling
+ * thread; if a thread cannot be started its share is taken by the others. */
+typedef void (*orc_part_fn)(void* ctx, long long lo, long long hi, int tid);
+typedef struct {
+    orc_part_fn fn;
+    void* ctx;
+    long long n, chunk, next;
+} orc_job;
+typedef struct {
+    orc_job* job;
+    int tid;
+} orc_worker_arg;
+
+static void* orc_worker(void* p) {
+    orc_worker_arg* w = (orc_worker_arg*)p;
+    orc_job* j = w->job;
+    for (;;) {
+        const long long lo = __atomic_fetch_add(&j->next, j->chunk, __ATOMIC_RELAXED);
+        if (lo >= j->n) break;
+        const long long hi = lo + j->chunk < j->n ? lo + j->chunk : j->n;
+        j->fn(j->ctx, lo, hi, w->tid);
+    }
+    return NULL;
+}
+
+static void orc_parallel_for(long long n, long long chunk, orc_part_fn fn, void* ctx) {
+    const int nt = orc_threads;
+    if (nt <= 1 || n <= chunk) {
+        if (n > 0) fn(ctx, 0, n, 0);
+        return;
+    }
+    orc_job job = {fn, ctx, n, chunk, 0};
+    pthread_t th[1024];
+    orc_worker_arg arg[1024];
+    int started[1024];
+    for (int t = 0; t < nt; ++t) { arg[t].job = &job; arg[t].tid = t; started[t] = 0; }
+    for (int t = 1; t < nt; ++t) started[t] = pthread_create(&th[t], NULL, orc_worker, &arg[t]) == 0;
+    orc_worker(&arg[0]);
+    for (int t = 1; t < nt; ++t)
+        if (started[t]) pthread_join(th[t], NULL);
+}
 
 void orc_set_variant(int k, int v) { if (k >= 0 && k < V_COUNT) orc_var[k] = v; }
 int orc_get_variant(int k) { return (k >= 0 && k < V_COUNT) ? orc_var[k] : -1; }

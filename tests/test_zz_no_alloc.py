@@ -30,7 +30,13 @@ def _lib():
     lib.w2w_scan_u32_noalloc.argtypes = [vp, vp, ll, ctypes.c_int, vp]
     lib.w2w_scan_scratch_bytes.argtypes = [ll]
     lib.w2w_scan_scratch_bytes.restype = sz
+    lib.w2w_scan_noalloc_error.argtypes = [vp]
     return lib
+
+
+def _cumsum(host, exclusive):
+    inc = np.cumsum(host, dtype=np.uint64).astype(np.uint32)
+    return np.concatenate([[0], inc[:-1]]).astype(np.uint32) if exclusive else inc
 
 
 def test_noalloc_scan_matches_scratch_entry_point():
@@ -49,10 +55,29 @@ def test_noalloc_scan_matches_scratch_entry_point():
         assert lib.w2w_scan_u32_noalloc(x.data_ptr(), got.data_ptr(), n, exclusive, stream) == 0
         torch.cuda.synchronize()
         assert torch.equal(got, expect)
-        host = x.cpu().numpy().view(np.uint32)
-        inc = np.cumsum(host, dtype=np.uint64).astype(np.uint32)
-        want = np.concatenate([[0], inc[:-1]]).astype(np.uint32) if exclusive else inc
-        assert np.array_equal(got.cpu().numpy().view(np.uint32), want)
+        assert np.array_equal(got.cpu().numpy().view(np.uint32), _cumsum(x.cpu().numpy().view(np.uint32), exclusive))
+    assert lib.w2w_scan_noalloc_error(stream) == 0
+
+
+def test_noalloc_scan_back_to_back_after_a_larger_call():
+    """Calls queued on one stream with no synchronisation between them, the
+    first at the maximum size: each later, smaller call must clear the shared
+    array's words it uses, whatever the larger call left beyond them."""
+    lib = _lib()
+    stream = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    rng = np.random.default_rng(11)
+    sizes = [MAX_N, 1, 4096, 4097, 12289, 1]  # 4096 elements per scan tile
+    xs, outs = [], []
+    for k, n in enumerate(sizes):
+        x = torch.from_numpy(rng.integers(0, 1 << 20, size=n).astype(np.uint32).view(np.int32)).cuda()
+        out = torch.full_like(x, -1)
+        assert lib.w2w_scan_u32_noalloc(x.data_ptr(), out.data_ptr(), n, k % 2, stream) == 0
+        xs.append(x)
+        outs.append(out)
+    torch.cuda.synchronize()
+    assert lib.w2w_scan_noalloc_error(stream) == 0
+    for k, (x, out) in enumerate(zip(xs, outs)):
+        assert np.array_equal(out.cpu().numpy().view(np.uint32), _cumsum(x.cpu().numpy().view(np.uint32), k % 2)), k
 
 
 def test_noalloc_scan_rejects_oversize():

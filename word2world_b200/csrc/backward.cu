@@ -226,21 +226,22 @@ __device__ __forceinline__ bool ref_eval(float4 q0, float4 q1, float4 q2, float 
 // hi) handles one staged chunk whose entry j is list position hi - 1 - j and
 // whose set bits are the entries that may reach this warp's block.
 template <typename Body>
-__device__ __forceinline__ void walk_back(const float* records, const uint32_t* point_list, uint32_t base, int lo,
-                                          int top, WarpChunk& wc, const TilePixel& tp, Body&& body) {
+__device__ __forceinline__ void walk_back(const float* records, const uint32_t* point_list, uint32_t num_records,
+                                          uint32_t base, int lo, int top, WarpChunk& wc, const TilePixel& tp,
+                                          Body&& body) {
   const int len = top - lo;
   const int nc = len > 0 ? (len + kChunk - 1) / kChunk : 0;
   ChunkLoad ld;
   uint32_t reach = 0;
   if (nc > 0) {
-    chunk_load(ld, records, point_list, base + top - 1 - tp.lane, tp.lane < len);
+    chunk_load(ld, records, point_list, base + top - 1 - tp.lane, tp.lane < len, num_records);
     reach = chunk_store(wc, ld, tp.bx, tp.by);
   }
   for (int c = 0; c < nc; ++c) {
     const int hi = top - c * kChunk;
     const int hn = hi - kChunk;
     const bool more = c + 1 < nc;
-    if (more) chunk_load(ld, records, point_list, base + hn - 1 - tp.lane, hn - 1 - tp.lane >= lo);
+    if (more) chunk_load(ld, records, point_list, base + hn - 1 - tp.lane, hn - 1 - tp.lane >= lo, num_records);
     body(reach, hi);
     if (more) {
       __syncwarp();
@@ -325,13 +326,13 @@ __global__ void __launch_bounds__(kBlendThreads, 2) render_ref_kernel(BackwardAr
     }
   };
   if (role < 0) {
-    walk_back(a.bwd_record, a.point_list, p.range.x, 0, p.walk, wc, p.tp, full);
+    walk_back(a.bwd_record, a.point_list, uint32_t(a.P), p.range.x, 0, p.walk, wc, p.tp, full);
   } else {
     int lo, hi;
     segment_of(p.walk, role, lo, hi);
-    walk_back(a.bwd_record, a.point_list, p.range.x, hi, p.walk, wc, p.tp, state_only);
+    walk_back(a.bwd_record, a.point_list, uint32_t(a.P), p.range.x, hi, p.walk, wc, p.tp, state_only);
     __syncwarp();
-    walk_back(a.bwd_record, a.point_list, p.range.x, lo, hi, wc, p.tp, full);
+    walk_back(a.bwd_record, a.point_list, uint32_t(a.P), p.range.x, lo, hi, wc, p.tp, full);
   }
 }
 
@@ -478,13 +479,13 @@ __global__ void __launch_bounds__(kBlendThreads, 2) render_exact_kernel(Backward
     }
   };
   if (role < 0) {
-    walk_back(a.record, a.point_list, p.range.x, 0, p.walk, wc, p.tp, full);
+    walk_back(a.record, a.point_list, uint32_t(a.P), p.range.x, 0, p.walk, wc, p.tp, full);
   } else {
     int lo, hi;
     segment_of(p.walk, role, lo, hi);
-    walk_back(a.record, a.point_list, p.range.x, hi, p.walk, wc, p.tp, state_only);
+    walk_back(a.record, a.point_list, uint32_t(a.P), p.range.x, hi, p.walk, wc, p.tp, state_only);
     __syncwarp();
-    walk_back(a.record, a.point_list, p.range.x, lo, hi, wc, p.tp, full);
+    walk_back(a.record, a.point_list, uint32_t(a.P), p.range.x, lo, hi, wc, p.tp, full);
   }
 }
 

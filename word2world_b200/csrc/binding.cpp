@@ -8,9 +8,14 @@
 #include <c10/cuda/CUDAStream.h>
 #include <torch/extension.h>
 
+#include <cuda_runtime.h>
+
+#include <mutex>
 #include <sstream>
 #include <stdexcept>
+#include <string>
 #include <tuple>
+#include <vector>
 
 #include "../../include/w2w_raster.h"
 
@@ -35,6 +40,92 @@ Tensor f32(const Tensor& t, const char* name, const torch::Device& dev) {
 
 w2w_stream_t cur_stream() {
   return reinterpret_cast<w2w_stream_t>(c10::cuda::getCurrentCUDAStream().stream());
+}
+
+// Deferred device error checks.  A render returns before its sort has run,
+// so the sort's error word (a lookback wait that ran out, an index out of
+// range) cannot be read without stalling the host.  Instead, each render
+// enqueues a 4-byte copy of the word into a pinned host slot on its own stream,
+// followed by an event; every later call into this module polls the finished
+// events without blocking and raises if a word was set, and
+// check_device_errors() waits for all of them first.
+class DeferredChecks {
+ public:
+  void add(const void* dev_word, cudaStream_t st, const char* what) {
+    std::lock_guard<std::mutex> lk(mu_);
+    if (free_.empty()) grow();
+    Entry e = free_.back();
+    free_.pop_back();
+    *e.slot = 0u;
+    if (cudaMemcpyAsync(e.slot, dev_word, 4, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+        cudaEventRecord(e.ev, st) != cudaSuccess) {
+      free_.push_back(e);
+      throw std::runtime_error(std::string(what) + ": could not enqueue the error-word read");
+    }
+    e.what = what;
+    pending_.push_back(e);
+  }
+
+  // Raises on the first finished entry whose word is set (wait: finish all first).
+  void poll(bool wait) {
+    std::string msg;
+    {
+      std::lock_guard<std::mutex> lk(mu_);
+      std::vector<Entry> keep;
+      for (Entry& e : pending_) {
+        const cudaError_t q = wait ? cudaEventSynchronize(e.ev) : cudaEventQuery(e.ev);
+        if (q == cudaErrorNotReady) {
+          keep.push_back(e);
+          continue;
+        }
+        if (q != cudaSuccess) {
+          cudaGetLastError();
+          if (msg.empty()) msg = e.what + ": CUDA error while reading the device error word";
+        } else if (*e.slot != 0u && msg.empty()) {
+          const uint32_t w = *e.slot;
+          msg = e.what + ": device error word " + std::to_string(w) +
+                ((w & 2u) ? " (a bounded device wait timed out; results invalid)"
+                          : " (capacity exceeded or an index out of range; results invalid)");
+        }
+        free_.push_back(e);
+      }
+      pending_.swap(keep);
+    }
+    if (!msg.empty()) throw std::runtime_error(msg);
+  }
+
+ private:
+  struct Entry {
+    uint32_t* slot;
+    cudaEvent_t ev;
+    std::string what;
+  };
+  void grow() {
+    constexpr int kSlots = 256;
+    void* p = nullptr;
+    if (cudaHostAlloc(&p, kSlots * sizeof(uint32_t), cudaHostAllocDefault) != cudaSuccess)
+      throw std::runtime_error("could not allocate pinned error-word slots");
+    for (int i = 0; i < kSlots; ++i) {
+      Entry e{static_cast<uint32_t*>(p) + i, nullptr, std::string()};
+      if (cudaEventCreateWithFlags(&e.ev, cudaEventDisableTiming) != cudaSuccess)
+        throw std::runtime_error("could not create an event for the error-word read");
+      free_.push_back(e);
+    }
+  }
+  std::mutex mu_;
+  std::vector<Entry> pending_, free_;
+};
+
+DeferredChecks& deferred() {
+  static DeferredChecks* d = new DeferredChecks();  // lives until exit (its pinned slots too)
+  return *d;
+}
+
+// The binning state's error word, read after the render (deferred).
+void defer_bin_check(const Tensor& bin, int64_t R, int W, int H, cudaStream_t st, const char* what) {
+  if (R <= 0) return;
+  const size_t off = w2w_binning_offset(R, W, H, "header");  // the header starts with the error word
+  deferred().add(static_cast<const unsigned char*>(bin.data_ptr()) + off, st, what);
 }
 
 struct Camera {
@@ -64,6 +155,7 @@ std::tuple<int64_t, Tensor, Tensor, Tensor, Tensor, Tensor, Tensor, Tensor> rast
     double focal_x, int64_t image_height, int64_t image_width, const c10::optional<Tensor>& background,
     bool compat_spill) {
   (void)focal_y;  // the reference forward uses focal_x on both axes (projection.cu:100-101)
+  deferred().poll(false);
   TORCH_CHECK(means3D.dim() == 2 && means3D.size(1) == 3, "means3D must be [P, 3]");
   const auto dev = means3D.device();
   const int64_t P = means3D.size(0);
@@ -121,6 +213,7 @@ std::tuple<int64_t, Tensor, Tensor, Tensor, Tensor, Tensor, Tensor, Tensor> rast
                              depth.data_ptr<float>(), alpha.data_ptr<float>(), stream),
           "w2w_forward_render");
   }
+  defer_bin_check(bin, R, W, H, reinterpret_cast<cudaStream_t>(stream), "w2w_forward_render");
   return std::make_tuple(R, color, depth, alpha, radii, geom, bin, img);
 }
 
@@ -136,6 +229,7 @@ std::tuple<Tensor, Tensor, Tensor, Tensor, Tensor, Tensor, Tensor, Tensor> raste
               "precomputed colours / covariances are not supported: the forward always derives them from "
               "SH coefficients, scales and rotations (as the reference forward does)");
   TORCH_CHECK(grad_mode == 0 || grad_mode == 1, "grad_mode must be 0 (reference) or 1 (exact)");
+  deferred().poll(debug);
   const auto dev = means3D.device();
   c10::cuda::CUDAGuard guard(dev);
   const int64_t P = means3D.size(0);
@@ -204,7 +298,9 @@ std::tuple<Tensor, Tensor, Tensor, Tensor, Tensor, Tensor, Tensor, Tensor> raste
 
 // ---- stages ---------------------------------------------------------------
 
-std::tuple<Tensor, Tensor> sort_pairs_u64(const Tensor& keys, const Tensor& vals, int64_t begin_bit, int64_t end_bit) {
+// check_errors: read the scratch's error word back (synchronises the stream).
+std::tuple<Tensor, Tensor> sort_pairs_u64(const Tensor& keys, const Tensor& vals, int64_t begin_bit, int64_t end_bit,
+                                          bool check_errors) {
   TORCH_CHECK(keys.is_cuda() && keys.scalar_type() == torch::kInt64, "keys must be a CUDA int64 tensor (raw u64 bits)");
   TORCH_CHECK(vals.is_cuda() && vals.scalar_type() == torch::kInt32 && vals.numel() == keys.numel(),
               "vals must be a CUDA int32 tensor with one value per key");
@@ -218,6 +314,7 @@ std::tuple<Tensor, Tensor> sort_pairs_u64(const Tensor& keys, const Tensor& vals
                            reinterpret_cast<uint64_t*>(ko.data_ptr<int64_t>()), reinterpret_cast<uint32_t*>(vo.data_ptr<int>()),
                            n, int(begin_bit), int(end_bit), scratch.data_ptr(), size_t(scratch.numel()), cur_stream()),
         "w2w_sort_pairs_u64");
+  if (check_errors && n > 0) check(w2w_scratch_error(scratch.data_ptr(), cur_stream()), "w2w_sort_pairs_u64");
   return std::make_tuple(ko, vo);
 }
 
@@ -228,6 +325,7 @@ std::tuple<int64_t, Tensor, Tensor, Tensor, Tensor, Tensor, Tensor, Tensor> rast
     const Tensor& quaternion, const Tensor& viewmatrix, const Tensor& projmatrix, const Tensor& campos,
     double focal_x, int64_t degree, int64_t image_height, int64_t image_width, const c10::optional<Tensor>& background,
     bool compat_spill) {
+  deferred().poll(false);
   TORCH_CHECK(means3D.dim() == 2 && means3D.size(1) == 3, "means3D must be [P, 3]");
   const auto dev = means3D.device();
   const int64_t P = means3D.size(0);
@@ -272,6 +370,7 @@ std::tuple<int64_t, Tensor, Tensor, Tensor, Tensor, Tensor, Tensor, Tensor> rast
                              depth.data_ptr<float>(), alpha.data_ptr<float>(), stream),
           "w2w_forward_render");
   }
+  defer_bin_check(bin, R, W, H, reinterpret_cast<cudaStream_t>(stream), "w2w_forward_render");
   return std::make_tuple(R, color, depth, alpha, radii, geom, bin, img);
 }
 
@@ -284,6 +383,7 @@ std::tuple<Tensor, Tensor, Tensor, Tensor, Tensor, Tensor, Tensor> rasterize_gau
     const Tensor& viewmatrix, const Tensor& projmatrix, const Tensor& campos, double tan_fovx, double tan_fovy,
     int64_t degree, const Tensor& dL_dout_color, const Tensor& dL_dout_depth, const Tensor& dL_dout_alpha,
     const Tensor& geomBuffer, int64_t R, const Tensor& binningBuffer, const Tensor& imageBuffer, const Tensor& alpha) {
+  deferred().poll(false);
   const auto dev = means3D.device();
   c10::cuda::CUDAGuard guard(dev);
   const int64_t P = means3D.size(0);
@@ -417,7 +517,8 @@ Tensor voxel_field(const Tensor& means, const Tensor& covs, const Tensor& opacit
   return occ;
 }
 
-Tensor scan_u32(const Tensor& x, bool exclusive) {
+// check_errors: read the scratch's error word back (synchronises the stream).
+Tensor scan_u32(const Tensor& x, bool exclusive, bool check_errors) {
   TORCH_CHECK(x.is_cuda() && x.scalar_type() == torch::kInt32, "x must be a CUDA int32 tensor (raw u32 bits)");
   c10::cuda::CUDAGuard guard(x.device());
   Tensor xi = x.contiguous();
@@ -427,6 +528,7 @@ Tensor scan_u32(const Tensor& x, bool exclusive) {
   check(w2w_scan_u32(reinterpret_cast<const uint32_t*>(xi.data_ptr<int>()), reinterpret_cast<uint32_t*>(out.data_ptr<int>()),
                      n, exclusive ? 1 : 0, scratch.data_ptr(), size_t(scratch.numel()), cur_stream()),
         "w2w_scan_u32");
+  if (check_errors && n > 0) check(w2w_scratch_error(scratch.data_ptr(), cur_stream()), "w2w_scan_u32");
   return out;
 }
 
@@ -502,8 +604,20 @@ PYBIND11_MODULE(TORCH_EXTENSION_NAME, m) {
         py::arg("dL_dout_alpha"), py::arg("sh"), py::arg("degree"), py::arg("campos"), py::arg("geomBuffer"),
         py::arg("R"), py::arg("binningBuffer"), py::arg("imageBuffer"), py::arg("alpha"), py::arg("debug"),
         py::arg("grad_mode") = 0);
-  m.def("sort_pairs_u64", &sort_pairs_u64);
-  m.def("scan_u32", &scan_u32);
+  m.def("sort_pairs_u64", &sort_pairs_u64, py::arg("keys"), py::arg("vals"), py::arg("begin_bit"), py::arg("end_bit"),
+        py::arg("check_errors") = true);
+  m.def("scan_u32", &scan_u32, py::arg("x"), py::arg("exclusive"), py::arg("check_errors") = true);
+  m.def("check_device_errors", []() {
+    // waits for every pending error-word read of earlier renders; raises on a set word
+    pybind11::gil_scoped_release nogil;
+    deferred().poll(true);
+  });
+  m.def("poll_device_errors", []() { deferred().poll(false); });
+  m.def("test_set_spin_limit", [](int64_t limit) { return int64_t(w2w_test_set_spin_limit(unsigned(limit))); });
+  m.def("test_unpublished_tile", [](int64_t stage, int64_t tile) {
+    return int64_t(w2w_test_unpublished_tile(int(stage), tile));
+  });
+  m.def("set_error_check", [](bool on) { return w2w_set_error_check(on ? 1 : 0) != 0; });
   m.def("activate", &activate);
   m.def("rasterize_gaussians_raw", &rasterize_gaussians_raw);
   m.def("rasterize_gaussians_backward_raw", &rasterize_gaussians_backward_raw);
@@ -536,6 +650,14 @@ PYBIND11_MODULE(TORCH_EXTENSION_NAME, m) {
     const uint32_t* u = reinterpret_cast<const uint32_t*>(h.data_ptr());
     d["key64"] = u[1]; d["depth_bits"] = u[2]; d["tile_bits"] = u[4]; d["passes"] = u[5];
     return d;
+  });
+  m.def("throughput_probe", [](int64_t kind, int64_t iters, int64_t blocks, const Tensor& out) {
+    // enqueues the probe on the current stream; returns its instruction count
+    c10::cuda::CUDAGuard guard(out.device());
+    long long ops = 0;
+    check(w2w_throughput_probe(int(kind), iters, int(blocks), out.data_ptr<float>(), &ops, cur_stream()),
+          "w2w_throughput_probe");
+    return int64_t(ops);
   });
   m.def("version", &w2w_version);
   m.def("launch_count", []() { return (unsigned long long)w2w_launch_count(); });

@@ -103,7 +103,7 @@ __global__ void __launch_bounds__(kBlendCta, 16 / kBlendWarps) blend_kernel(Blen
 #pragma unroll
     for (int r = 0; r < kStagePer; ++r) {
       const int e = base + r * kBlendCta + int(threadIdx.x);
-      stage_load(st[r], a.record, a.point_list, range.x + e, e < n);
+      stage_load(st[r], a.record, a.point_list, range.x + e, e < n, a.num_records);
     }
   };
   auto store = [&](int buf) {

@@ -1,7 +1,9 @@
 // C ABI of the rasterizer (declared in include/w2w_raster.h): host
 // orchestration of the kernels, state-buffer layouts and argument checks.
-// The library never allocates device memory; every buffer comes from the
-// caller.  All work is enqueued on the caller's stream.
+// The rasterizer entry points never allocate device memory: every buffer
+// comes from the caller (w2w_voxel_field alone takes its temporaries from the
+// stream-ordered allocator).  All work is enqueued on the caller's stream.
+#include <atomic>
 #include <cstdio>
 #include <cstring>
 #include <vector>
@@ -120,13 +122,42 @@ size_t sort_scratch_layout(long long n, size_t* keys_tmp, size_t* vals_tmp, size
   size_t o = 0;
   auto take = [&](size_t bytes) { size_t a = align256(o); o = a + bytes; return a; };
   const size_t nn = size_t(n > 0 ? n : 1);
+  // the error word sits at byte 4 of every stage scratch (sort and scan), where
+  // w2w_scratch_error reads it
+  *err = take(256) + 4;
   *keys_tmp = take(nn * 8);
   *vals_tmp = take(nn * 4);
   *hist = take(size_t(kMaxPasses) * kMaxBins * 4);
   *status = take(sort_status_words(n) * 4);
   *counters = take(kMaxPasses * 4);
-  *err = take(4);
   return align256(o);
+}
+
+// Whether entry points with bounded device waits read their error word back
+// before returning (w2w_set_error_check).
+std::atomic<int> g_error_check{0};
+
+int status_of(uint32_t err) {
+  if (err & kErrTimeout) return W2W_ERR_TIMEOUT;
+  if (err & (kErrCapacity | kErrRange)) return W2W_ERR_CAPACITY;
+  return W2W_OK;
+}
+
+// Synchronises `st` and maps the device error word at `word` to a status.
+int read_error_word(const void* word, cudaStream_t st) {
+  uint32_t e = 0;
+  if (cudaMemcpyAsync(&e, word, 4, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+      cudaStreamSynchronize(st) != cudaSuccess)
+    return W2W_ERR_CUDA;
+  return status_of(e);
+}
+
+// After a launch sequence: the launch status, then (in checked mode) the
+// error word's.
+int finish(const void* err_word, cudaStream_t st) {
+  const int rc = check_launch();
+  if (rc != W2W_OK || err_word == nullptr || g_error_check.load(std::memory_order_relaxed) == 0) return rc;
+  return read_error_word(err_word, st);
 }
 
 }  // namespace
@@ -134,6 +165,20 @@ size_t sort_scratch_layout(long long n, size_t* keys_tmp, size_t* vals_tmp, size
 extern "C" {
 
 int w2w_version(void) { return 1; }
+
+int w2w_set_error_check(int mode) { return g_error_check.exchange(mode ? 1 : 0); }
+
+int w2w_scratch_error(const void* scratch, w2w_stream_t stream) {
+  if (!scratch) return W2W_ERR_INVALID;
+  return read_error_word(static_cast<const unsigned char*>(scratch) + 4, S(stream));
+}
+
+int w2w_scan_noalloc_error(w2w_stream_t stream) {
+  int rc = 0;
+  void* scratch = scan_noalloc_scratch(&rc);
+  if (rc != 0 || scratch == nullptr) return W2W_ERR_CUDA;
+  return read_error_word(static_cast<const unsigned char*>(scratch) + 4, S(stream));
+}
 
 const char* w2w_status_string(int status) {
   switch (status) {
@@ -233,6 +278,8 @@ static int forward_geometry(const w2w_settings* s, const float* means3D, const f
   a.prev_reach = at<uint32_t>(geom_state, L.prev_reach);
   a.record = at<float>(geom_state, L.record);
   a.bwd_record = at<float>(geom_state, L.bwd_record);
+  a.spin_limit = spin_limit();
+  a.unpublished_tile = unpublished_tile(kWaitPreprocess);
   if (raw != nullptr) {
     a.svec = raw->svec; a.quat = raw->quat; a.logit = raw->logit; a.sh_dc = raw->sh_dc; a.sh_ac = raw->sh_ac;
   }
@@ -284,6 +331,7 @@ int w2w_forward_render(const w2w_settings* s, const void* geom_state, const w2w_
   const ImageLayout IL(W, H);
   uint2* ranges = at<uint2>(image_state, IL.ranges);
   const uint32_t* point_list = nullptr;
+  const void* err_word = nullptr;  // the binning header's error word
   if (R == 0) {
     cudaMemsetAsync(ranges, 0, sizeof(uint2) * size_t(T), st);
   } else {
@@ -292,6 +340,7 @@ int w2w_forward_render(const w2w_settings* s, const void* geom_state, const w2w_
     const KeyPlan kp = plan_keys(*info, W, H);
     const int passes = sort_passes(kp.bits);
     BinHeader* bh = at<BinHeader>(binning_state, BL.header);
+    err_word = &bh->error;
     stage_begin(kStOther, st);
     write_bin_header<<<1, 1, 0, st>>>(bh, kp, uint32_t(R), uint32_t(passes));
     stage_end(kStOther, st, 1);
@@ -330,6 +379,8 @@ int w2w_forward_render(const w2w_settings* s, const void* geom_state, const w2w_
     so.clear_span = at<void>(binning_state, BL.hist);
     so.clear_bytes = BL.status - BL.hist + size_t(passes > 0 ? passes : 1) * kMaxBins * 4 *
                      size_t((R + sort_tile_keys(kp.key64) - 1) / sort_tile_keys(kp.key64));
+    so.spin_limit = spin_limit();
+    so.unpublished_tile = unpublished_tile(kWaitSort);
     launch_sort(so, st);
     point_list = valsA;
   }
@@ -338,6 +389,7 @@ int w2w_forward_render(const w2w_settings* s, const void* geom_state, const w2w_
   b.ranges = ranges;
   b.point_list = point_list;
   b.record = R > 0 ? at<float>(geom_state, GeomLayout(s->P).record) : nullptr;
+  b.num_records = uint32_t(s->P);
   b.bg = s->background;
   b.out_color = out_color; b.out_depth = out_depth; b.out_alpha = out_alpha;
   b.n_contrib = at<uint32_t>(image_state, IL.n_contrib);
@@ -346,7 +398,7 @@ int w2w_forward_render(const w2w_settings* s, const void* geom_state, const w2w_
   b.order = at<uint32_t>(image_state, IL.order);
   b.order_bwd = at<uint32_t>(image_state, IL.order_bwd);
   launch_blend(b, st);
-  return check_launch();
+  return finish(err_word, st);
 }
 
 int w2w_state_error(const void* state, int which, w2w_stream_t stream) {
@@ -488,8 +540,10 @@ int w2w_sort_pairs_u64(const uint64_t* keys_in, const uint32_t* vals_in, uint64_
   so.counters = at<uint32_t>(scratch, ct);
   so.error = at<uint32_t>(scratch, er);
   so.tile_shift = 0; so.num_tiles = 0; so.tile_hist = nullptr; so.ranges = nullptr;
+  so.spin_limit = spin_limit();
+  so.unpublished_tile = unpublished_tile(kWaitSort);
   launch_sort(so, st);
-  return check_launch();
+  return finish(so.error, st);
 }
 
 size_t w2w_scan_scratch_bytes(long long n) { return align256(scan_scratch_bytes(n)); }
@@ -501,7 +555,7 @@ int w2w_scan_u32(const uint32_t* in, uint32_t* out, long long n, int exclusive, 
   if (!in || !out) return W2W_ERR_INVALID;
   if (!scratch || scratch_bytes < w2w_scan_scratch_bytes(n)) return W2W_ERR_SCRATCH;
   launch_scan(in, out, n, exclusive, scratch, S(stream));
-  return check_launch();
+  return finish(static_cast<unsigned char*>(scratch) + 4, S(stream));
 }
 
 int w2w_scan_u32_noalloc(const uint32_t* in, uint32_t* out, long long n, int exclusive, w2w_stream_t stream) {
@@ -519,7 +573,7 @@ int w2w_scan_u32_noalloc(const uint32_t* in, uint32_t* out, long long n, int exc
   void* scratch = scan_noalloc_scratch(&rc);
   if (rc != 0 || scratch == nullptr) return W2W_ERR_CUDA;
   launch_scan(in, out, n, exclusive, scratch, S(stream));
-  return check_launch();
+  return finish(static_cast<unsigned char*>(scratch) + 4, S(stream));
 }
 
 int w2w_activate_forward(long long P, int K, const float* opacity_logit, const float* svec, const float* quaternion,
@@ -623,6 +677,8 @@ int w2w_voxel_field(const float* means, const float* covs, const float* opacitie
   so.hist = at<uint32_t>(sort_scratch, hi); so.status = at<uint32_t>(sort_scratch, stt);
   so.counters = at<uint32_t>(sort_scratch, ct); so.error = at<uint32_t>(sort_scratch, er);
   so.tile_shift = 0; so.num_tiles = nblocks; so.tile_hist = tile_hist; so.ranges = ranges;
+  so.spin_limit = spin_limit();
+  so.unpublished_tile = unpublished_tile(kWaitSort);
   launch_sort(so, st);
   launch_voxel_field(a, vals_out, ranges, st);
   uint32_t err = 0;
@@ -708,6 +764,7 @@ int w2w_blend(const w2w_settings* s, const void* geom_state, const uint32_t* ran
   b.ranges = own;
   b.point_list = point_list;
   b.record = at<float>(geom_state, GeomLayout(s->P).record);
+  b.num_records = uint32_t(s->P);
   b.bg = s->background;
   b.out_color = out_color; b.out_depth = out_depth; b.out_alpha = out_alpha;
   b.n_contrib = at<uint32_t>(image_state, IL.n_contrib);
@@ -880,6 +937,8 @@ int w2w_batch_forward_geometry(const w2w_batch_item* items, int n, int compat_sp
   a.prev_reach = at<uint32_t>(geom_state, L.prev_reach);
   a.record = at<float>(geom_state, L.record);
   a.bwd_record = at<float>(geom_state, L.bwd_record);
+  a.spin_limit = spin_limit();
+  a.unpublished_tile = unpublished_tile(kWaitPreprocess);
   launch_preprocess(a, st);
   int rc = check_launch();
   if (rc) return rc;
@@ -912,6 +971,7 @@ int w2w_batch_forward_render(const w2w_batch_item* items, int n, const void* geo
   const BatchItem* dev_items = at<BatchItem>(geom_state, BGL.items);
   uint2* ranges = at<uint2>(image_state, IL.ranges);
   const uint32_t* point_list = nullptr;
+  const void* err_word = nullptr;  // the binning header's error word
   if (R == 0) {
     cudaMemsetAsync(ranges, 0, sizeof(uint2) * size_t(T), st);
   } else {
@@ -920,6 +980,7 @@ int w2w_batch_forward_render(const w2w_batch_item* items, int n, const void* geo
     const KeyPlan kp = plan_keys_tiles(*info, T);
     const int passes = sort_passes(kp.bits);
     BinHeader* bh = at<BinHeader>(binning_state, BL.header);
+    err_word = &bh->error;
     stage_begin(kStOther, st);
     write_bin_header<<<1, 1, 0, st>>>(bh, kp, uint32_t(R), uint32_t(passes));
     stage_end(kStOther, st, 1);
@@ -957,6 +1018,8 @@ int w2w_batch_forward_render(const w2w_batch_item* items, int n, const void* geo
     so.clear_span = at<void>(binning_state, BL.hist);
     so.clear_bytes = BL.status - BL.hist + size_t(passes > 0 ? passes : 1) * kMaxBins * 4 *
                      size_t((R + sort_tile_keys(kp.key64) - 1) / sort_tile_keys(kp.key64));
+    so.spin_limit = spin_limit();
+    so.unpublished_tile = unpublished_tile(kWaitSort);
     launch_sort(so, st);
     point_list = valsA;
   }
@@ -966,6 +1029,7 @@ int w2w_batch_forward_render(const w2w_batch_item* items, int n, const void* geo
   b.ranges = ranges;
   b.point_list = point_list;
   b.record = R > 0 ? at<float>(geom_state, GeomLayout(E).record) : nullptr;
+  b.num_records = uint32_t(E);
   b.bg = nullptr;
   b.out_color = out_color; b.out_depth = out_depth; b.out_alpha = out_alpha;
   b.n_contrib = at<uint32_t>(image_state, IL.n_contrib);
@@ -974,7 +1038,7 @@ int w2w_batch_forward_render(const w2w_batch_item* items, int n, const void* geo
   b.order = at<uint32_t>(image_state, IL.order);
   b.order_bwd = at<uint32_t>(image_state, IL.order_bwd);
   launch_blend(b, st);
-  return check_launch();
+  return finish(err_word, st);
 }
 
 int w2w_batch_backward(const w2w_batch_item* items, int n, const void* geom_state, long long R,

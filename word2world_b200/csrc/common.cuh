@@ -407,7 +407,7 @@ struct BinLayout {
 // ---------------------------------------------------------------------------
 // Bounded waits and release/acquire helpers
 // ---------------------------------------------------------------------------
-constexpr uint32_t kSpinLimit = 1u << 22;   // per wait; a few ms at most
+constexpr uint32_t kSpinLimit = 1u << 22;   // per wait; each poll is an L2 round trip, so 1-2 s at most
 
 __device__ __forceinline__ uint32_t ld_acquire(const uint32_t* p) {
   uint32_t v;

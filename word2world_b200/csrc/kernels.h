@@ -80,6 +80,8 @@ struct PreprocessArgs {
   // sigmoid(logit) and the SH row is sh_dc followed by sh_ac, computed here
   // as the reference's torch preamble computes them
   const float *svec, *quat, *logit, *sh_dc, *sh_ac;
+  uint32_t spin_limit = kSpinLimit;  // bounded waits (spin_limit())
+  long long unpublished_tile = -1;   // fused scan: tile that skips publishing (tests; -1 = none)
 };
 void launch_preprocess(const PreprocessArgs& a, cudaStream_t stream);
 
@@ -123,6 +125,8 @@ struct SortArgs {
   uint32_t* status;      // [kMaxPasses * sort_tiles * kMaxBins]
   uint32_t* counters;    // [kMaxPasses]
   uint32_t* error;
+  uint32_t spin_limit = kSpinLimit;  // bounded waits (spin_limit())
+  long long unpublished_tile = -1;   // first pass: tile that skips publishing (tests; -1 = none)
   int tile_shift;
   int num_tiles;
   uint32_t* tile_hist;
@@ -146,6 +150,7 @@ struct BlendArgs {
   const uint2* ranges;
   const uint32_t* point_list;
   const float* record;
+  uint32_t num_records;  // records (Gaussians, or batch elements); larger ids in the list are skipped
   const float* bg;
   float* out_color;
   float* out_depth;
@@ -269,6 +274,15 @@ void launch_densify_stats(long long P, const float* dL_dmeans2D, const int* radi
                           cudaStream_t stream);
 
 size_t scan_status_words(long long n);
+// Bounded device waits.  spin_limit(): the iteration limit of every lookback
+// wait (kSpinLimit unless a test lowered it).  unpublished_tile(stage): a
+// tile of that stage whose CTA skips publishing its status, so that the waits
+// behind it run out and report kErrTimeout (tests only; -1 = none).  Both are
+// host-side settings read when a kernel is launched.
+enum WaitStage { kWaitScan = 0, kWaitSort = 1, kWaitPreprocess = 2, kNumWaitStages = 3 };
+uint32_t spin_limit();
+long long unpublished_tile(int stage);
+
 size_t scan_scratch_bytes(long long n);
 void launch_scan(const uint32_t* in, uint32_t* out, long long n, int exclusive, void* scratch, cudaStream_t stream);
 long long scan_noalloc_max();

@@ -481,13 +481,14 @@ preprocess_kernel(PreprocessArgs a) {
   // left); a serial walk would cost one L2 round trip per tile.
   if (warp == 0) {
     unsigned long long* status = a.scan_status;
+    const bool publish = (long long)tile != a.unpublished_tile;
     if (tile == 0) {
       if (lane == 0) {
-        st_relaxed64(status + tile, pack(kFlagInc, block_total));
+        if (publish) st_relaxed64(status + tile, pack(kFlagInc, block_total));
         s_prefix = Pair{0, 0, 0};
       }
     } else {
-      if (lane == 0) st_relaxed64(status + tile, pack(kFlagAgg, block_total));
+      if (lane == 0 && publish) st_relaxed64(status + tile, pack(kFlagAgg, block_total));
       // (0, 0, 0) is an identity on both sides for every pair that occurs
       Pair ex{0, 0, 0};
       long long t = int(tile) - 1;
@@ -500,7 +501,7 @@ preprocess_kernel(PreprocessArgs a) {
         const uint32_t ready = __ballot_sync(0xffffffffu, flag != 0ull);
         const uint32_t need = inc ? ((inc & (0u - inc)) << 1) - 1u : 0xffffffffu;
         if ((ready & need) != need) {
-          if (++spins > kSpinLimit) {
+          if (++spins > a.spin_limit) {
             if (lane == 0) atomicOr(&hdr->error, kErrTimeout);
             break;
           }
@@ -521,7 +522,7 @@ preprocess_kernel(PreprocessArgs a) {
       }
       if (lane == 0) {
         s_prefix = ex;
-        st_relaxed64(status + tile, pack(kFlagInc, combine(ex, block_total)));
+        if (publish) st_relaxed64(status + tile, pack(kFlagInc, combine(ex, block_total)));
       }
     }
   }

@@ -3,8 +3,6 @@
 // which allocates, frees and synchronises the device at every level).  The
 // rasterizer itself fuses its scan into the preprocess kernel; this entry
 // point serves the isolated-stage workload and callers that scan alone.
-#include <mutex>
-
 #include "common.cuh"
 #include "kernels.h"
 
@@ -20,7 +18,8 @@ constexpr unsigned long long kAgg = 1ull << 62, kInc = 2ull << 62, kFlags = 3ull
 // wraps modulo 2^32, as the reference's uint32 scan does) in the low bits.
 __global__ void __launch_bounds__(kScanThreads)
 scan_kernel(const uint32_t* __restrict__ in, uint32_t* __restrict__ out, long long n, int exclusive,
-            unsigned long long* status, uint32_t* counter, uint32_t* err) {
+            unsigned long long* status, uint32_t* counter, uint32_t* err, uint32_t spin_limit,
+            long long unpublished_tile) {
   __shared__ uint32_t s_tile, s_prefix;
   __shared__ uint32_t s_warp[kScanThreads / 32];
   __shared__ uint32_t s_data[kScanTile];
@@ -67,13 +66,14 @@ scan_kernel(const uint32_t* __restrict__ in, uint32_t* __restrict__ out, long lo
   // word carries its flag and count together and nothing else written by its
   // tile is read, so relaxed accesses suffice.
   if (warp == 0) {
+    const bool publish = tile != unpublished_tile;
     if (tile == 0) {
       if (lane == 0) {
-        st_relaxed64(status, kInc | total);
+        if (publish) st_relaxed64(status, kInc | total);
         s_prefix = 0;
       }
     } else {
-      if (lane == 0) st_relaxed64(status + tile, kAgg | total);
+      if (lane == 0 && publish) st_relaxed64(status + tile, kAgg | total);
       uint32_t acc = 0, spins = 0;
       long long t = tile - 1;
       while (true) {
@@ -84,7 +84,7 @@ scan_kernel(const uint32_t* __restrict__ in, uint32_t* __restrict__ out, long lo
         const uint32_t ready = __ballot_sync(0xffffffffu, flag != 0ull);
         const uint32_t need = inc ? ((inc & (0u - inc)) << 1) - 1u : 0xffffffffu;  // lanes up to the nearest inclusive
         if ((ready & need) != need) {
-          if (++spins > kSpinLimit) {
+          if (++spins > spin_limit) {
             if (lane == 0) atomicOr(err, kErrTimeout);
             break;
           }
@@ -99,7 +99,7 @@ scan_kernel(const uint32_t* __restrict__ in, uint32_t* __restrict__ out, long lo
       }
       if (lane == 0) {
         s_prefix = acc;
-        st_relaxed64(status + tile, kInc | uint32_t(acc + total));
+        if (publish) st_relaxed64(status + tile, kInc | uint32_t(acc + total));
       }
     }
   }
@@ -133,29 +133,23 @@ size_t scan_scratch_bytes(long long n) { return 256 + scan_status_words(n) * 8; 
 
 long long scan_noalloc_max() { return kScanNoAllocMax; }
 
-// Device address of g_scan_scratch on the current device.  Host code may not
-// use the symbol itself (on the host it is only a stand-in), so the address is
-// looked up once per device, with that device current, and cached.
+// Device address of g_scan_scratch in the current CUDA context.  Host code
+// may not use the symbol itself (on the host it is only a stand-in), so the
+// address is looked up with the caller's device and context current, at every
+// call: the lookup is a host-side table read, and it stays right for any
+// context the caller makes current (several driver-API contexts on one
+// device, or a context re-created after cudaDeviceReset), where an address
+// cached per device would not.  The first lookup in a context also loads the
+// library's device code into it.
 void* scan_noalloc_scratch(int* status) {
-  static std::mutex mu;
-  static void* addr[128] = {nullptr};
-  int dev = 0;
-  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 128) {
+  void* p = nullptr;
+  const cudaError_t e = cudaGetSymbolAddress(&p, g_scan_scratch);
+  if (e != cudaSuccess || p == nullptr) {
     *status = 2;
     return nullptr;
   }
-  std::lock_guard<std::mutex> lk(mu);
-  if (addr[dev] == nullptr) {
-    void* p = nullptr;
-    const cudaError_t e = cudaGetSymbolAddress(&p, g_scan_scratch);
-    if (e != cudaSuccess || p == nullptr) {
-      *status = 2;
-      return nullptr;
-    }
-    addr[dev] = p;
-  }
   *status = 0;
-  return addr[dev];
+  return p;
 }
 
 // scratch: [tile counter u32, error word u32, pad to 256 B][one 64-bit status
@@ -168,7 +162,8 @@ void launch_scan(const uint32_t* in, uint32_t* out, long long n, int exclusive, 
   uint32_t* counter = reinterpret_cast<uint32_t*>(b);
   unsigned long long* status = reinterpret_cast<unsigned long long*>(b + 256);
   stage_begin(kStScan, stream);
-  scan_kernel<<<int(tiles), kScanThreads, 0, stream>>>(in, out, n, exclusive, status, counter, counter + 1);
+  scan_kernel<<<int(tiles), kScanThreads, 0, stream>>>(in, out, n, exclusive, status, counter, counter + 1,
+                                                       spin_limit(), unpublished_tile(kWaitScan));
   stage_end(kStScan, stream, 1);
 }
 

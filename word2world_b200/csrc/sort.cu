@@ -185,7 +185,8 @@ offsets_kernel(uint32_t* hist, int passes, const uint32_t* tile_hist, int num_ti
 // runs) and each step costs an L2 round trip (about 0.45 us measured), so a
 // step reads several tiles.  Bounded wait.
 template <int kLook>
-__device__ __forceinline__ uint2 lookback_pair(const uint32_t* status, long long tile, int d, uint32_t* err) {
+__device__ __forceinline__ uint2 lookback_pair(const uint32_t* status, long long tile, int d, uint32_t* err,
+                                               uint32_t spin_limit) {
   const unsigned long long* st = reinterpret_cast<const unsigned long long*>(status + d);
   constexpr unsigned long long kIncPair = (unsigned long long)(kStatInc) << 32 | kStatInc;
   uint32_t a0 = 0, a1 = 0, spins = 0;
@@ -211,7 +212,7 @@ __device__ __forceinline__ uint2 lookback_pair(const uint32_t* status, long long
       }
     }
     if (done) break;
-    if (used == 0 && ++spins > kSpinLimit) {
+    if (used == 0 && ++spins > spin_limit) {
       atomicOr(err, kErrTimeout);
       break;
     }
@@ -268,7 +269,8 @@ __device__ __forceinline__ void onesweep_tile_pass(const K* __restrict__ kin, co
                                                    K* __restrict__ kout, uint32_t* __restrict__ vout, uint32_t n,
                                                    int shift, const uint32_t* __restrict__ digit_base,
                                                    uint32_t* status, uint32_t* err, uint32_t tile,
-                                                   OnesweepShared<K>& sm, K* s_keys, uint32_t* s_vals) {
+                                                   uint32_t spin_limit, bool publish, OnesweepShared<K>& sm,
+                                                   K* s_keys, uint32_t* s_vals) {
   constexpr int kWarps = kSortThreads / 32;
   constexpr int kItems = OnesweepShape<K>::kItems;
   constexpr int kTile = onesweep_tile<K>();
@@ -314,8 +316,9 @@ __device__ __forceinline__ void onesweep_tile_pass(const K* __restrict__ kin, co
       c1 += x.y;
     }
     const uint32_t flag = tile == 0 ? kStatInc : kStatAgg;
-    st_relaxed64(reinterpret_cast<unsigned long long*>(status + size_t(tile) * kMaxBins + d0),
-                 (uint64_t(flag | c1) << 32) | (flag | c0));
+    if (publish)
+      st_relaxed64(reinterpret_cast<unsigned long long*>(status + size_t(tile) * kMaxBins + d0),
+                   (uint64_t(flag | c1) << 32) | (flag | c0));
   }
   const uint32_t excl = block_exclusive_scan(c0 + c1, sm.warp_sums, nullptr);  // ends with a barrier
   if (d0 < bins) *reinterpret_cast<uint2*>(sm.excl + d0) = make_uint2(excl, excl + c0);
@@ -345,11 +348,12 @@ __device__ __forceinline__ void onesweep_tile_pass(const K* __restrict__ kin, co
   if (d0 < bins) {
     uint32_t a0 = 0, a1 = 0;
     if (tile > 0) {
-      const uint2 a = lookback_pair<LookbackWindow<K>::value>(status, tile, d0, err);
+      const uint2 a = lookback_pair<LookbackWindow<K>::value>(status, tile, d0, err, spin_limit);
       a0 = a.x;
       a1 = a.y;
-      st_relaxed64(reinterpret_cast<unsigned long long*>(status + size_t(tile) * kMaxBins + d0),
-                   (uint64_t(kStatInc | (a1 + c1)) << 32) | (kStatInc | (a0 + c0)));
+      if (publish)
+        st_relaxed64(reinterpret_cast<unsigned long long*>(status + size_t(tile) * kMaxBins + d0),
+                     (uint64_t(kStatInc | (a1 + c1)) << 32) | (kStatInc | (a0 + c0)));
     }
     const uint2 ex = *reinterpret_cast<const uint2*>(sm.excl + d0);
     // sorted slot j of digit d goes to gofs[d] + j
@@ -384,7 +388,8 @@ template <typename K, int kWidth>
 __global__ void __launch_bounds__(kSortThreads, OnesweepShape<K>::kMinBlocks)
 onesweep_kernel(const K* __restrict__ kin, const uint32_t* __restrict__ vin, K* __restrict__ kout,
                 uint32_t* __restrict__ vout, long long n, int shift,
-                const uint32_t* __restrict__ digit_base, uint32_t* status, uint32_t* counter, uint32_t* err) {
+                const uint32_t* __restrict__ digit_base, uint32_t* status, uint32_t* counter, uint32_t* err,
+                uint32_t spin_limit, long long unpublished_tile) {
   constexpr int kTile = onesweep_tile<K>();
   static_assert(kSortThreads * 2 >= kMaxBins, "at most two digits per thread");
   __shared__ __align__(16) OnesweepShared<K> sm;
@@ -399,18 +404,19 @@ onesweep_kernel(const K* __restrict__ kin, const uint32_t* __restrict__ vin, K* 
   __syncthreads();
   const uint32_t tile = sm.tile;
   const uint32_t nn = uint32_t(n);  // n < 2^30 (checked by every caller)
+  const bool publish = (long long)tile != unpublished_tile;
   if ((unsigned long long)(tile + 1) * kTile <= nn)
-    onesweep_tile_pass<K, kWidth, true>(kin, vin, kout, vout, nn, shift, digit_base, status, err, tile, sm, s_keys,
-                                        s_vals);
+    onesweep_tile_pass<K, kWidth, true>(kin, vin, kout, vout, nn, shift, digit_base, status, err, tile, spin_limit,
+                                        publish, sm, s_keys, s_vals);
   else
-    onesweep_tile_pass<K, kWidth, false>(kin, vin, kout, vout, nn, shift, digit_base, status, err, tile, sm, s_keys,
-                                         s_vals);
+    onesweep_tile_pass<K, kWidth, false>(kin, vin, kout, vout, nn, shift, digit_base, status, err, tile, spin_limit,
+                                         publish, sm, s_keys, s_vals);
 }
 
 template <typename K, int kWidth>
 void launch_onesweep_w(int tiles, cudaStream_t stream, const K* kin, const uint32_t* vin, K* kout, uint32_t* vout,
                        long long n, int shift, const uint32_t* digit_base, uint32_t* status, uint32_t* counter,
-                       uint32_t* err) {
+                       uint32_t* err, uint32_t spin_limit, long long unpublished) {
   const size_t dyn = (sizeof(K) + sizeof(uint32_t)) * size_t(onesweep_tile<K>());
   // the shared-memory opt-in is set once per device (a driver call per launch
   // would widen the gap the device waits between launches)
@@ -422,17 +428,18 @@ void launch_onesweep_w(int tiles, cudaStream_t stream, const K* kin, const uint3
     if (dev >= 0 && dev < 64) opted[dev] = true;
   }
   onesweep_kernel<K, kWidth><<<tiles, kSortThreads, dyn, stream>>>(kin, vin, kout, vout, n, shift, digit_base,
-                                                                    status, counter, err);
+                                                                    status, counter, err, spin_limit, unpublished);
 }
 
 template <typename K>
 void launch_onesweep(int width, int tiles, cudaStream_t stream, const K* kin, const uint32_t* vin, K* kout,
                      uint32_t* vout, long long n, int shift, const uint32_t* digit_base, uint32_t* status,
-                     uint32_t* counter, uint32_t* err) {
+                     uint32_t* counter, uint32_t* err, uint32_t spin_limit, long long unpublished) {
   switch (width) {
-#define W2W_ONESWEEP_CASE(W)                                                                                  \
-  case W:                                                                                                     \
-    launch_onesweep_w<K, W>(tiles, stream, kin, vin, kout, vout, n, shift, digit_base, status, counter, err); \
+#define W2W_ONESWEEP_CASE(W)                                                                                      \
+  case W:                                                                                                         \
+    launch_onesweep_w<K, W>(tiles, stream, kin, vin, kout, vout, n, shift, digit_base, status, counter, err,      \
+                            spin_limit, unpublished);                                                             \
     break;
     W2W_ONESWEEP_CASE(1) W2W_ONESWEEP_CASE(2) W2W_ONESWEEP_CASE(3) W2W_ONESWEEP_CASE(4) W2W_ONESWEEP_CASE(5)
     W2W_ONESWEEP_CASE(6) W2W_ONESWEEP_CASE(7) W2W_ONESWEEP_CASE(8) W2W_ONESWEEP_CASE(9)
@@ -485,7 +492,8 @@ void run_sort(const SortArgs& a, cudaStream_t stream) {
     stage_begin(kStSortPass, stream);
     launch_onesweep<K>(pass_width(p, dbits, a.bits), int(tiles), stream, kin, vin, kout, vout, n,
                        a.begin_bit + dbits * p, a.hist + kMaxBins * p,
-                       a.status + size_t(p) * kMaxBins * size_t(tiles), a.counters + p, a.error);
+                       a.status + size_t(p) * kMaxBins * size_t(tiles), a.counters + p, a.error,
+                       a.spin_limit, p == 0 ? a.unpublished_tile : -1LL);
     stage_end(kStSortPass, stream, 1);
     kin = kout;
     vin = vout;

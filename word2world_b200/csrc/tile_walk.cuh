@@ -64,13 +64,19 @@ struct ChunkLoad {
 };
 
 // Gather entry `pos` of the point list (when `has`).  Records are four float4s;
-// r2.w and r3 hold the culling parameters (hy; beta, gamma, eps, vr).
+// r2.w and r3 hold the culling parameters (hy; beta, gamma, eps, vr).  An id
+// of num_records or more (a list left inconsistent by a sort whose bounded
+// wait ran out, which its error word reports) is skipped, never read.
 __device__ __forceinline__ void chunk_load(ChunkLoad& st, const float* record, const uint32_t* point_list, size_t pos,
-                                           bool has) {
-  st.has = has;
+                                           bool has, uint32_t num_records) {
+  st.has = false;
   if (has) {
     const float4* rec = reinterpret_cast<const float4*>(record);
     st.id = point_list[pos];
+    st.has = st.id < num_records;
+  }
+  if (st.has) {
+    const float4* rec = reinterpret_cast<const float4*>(record);
     const float4* r = rec + 4 * size_t(st.id);
     st.r0 = __ldg(r);
     st.r1 = __ldg(r + 1);
@@ -151,13 +157,17 @@ struct Staged {
 };
 
 // Gather entry `pos` of the point list (when `has`).  Records are four float4s;
-// r2.w and r3 hold the culling parameters (hy; beta, gamma, eps, vr).
+// r2.w and r3 hold the culling parameters (hy; beta, gamma, eps, vr).  Ids of
+// num_records or more are skipped (see chunk_load).
 __device__ __forceinline__ void stage_load(Staged& st, const float* record, const uint32_t* point_list, size_t pos,
-                                           bool has) {
-  st.has = has;
+                                           bool has, uint32_t num_records) {
+  st.has = false;
   if (has) {
-    const float4* rec = reinterpret_cast<const float4*>(record);
     st.id = point_list[pos];
+    st.has = st.id < num_records;
+  }
+  if (st.has) {
+    const float4* rec = reinterpret_cast<const float4*>(record);
     const float4* r = rec + 4 * size_t(st.id);
     st.r0 = __ldg(r);
     st.r1 = __ldg(r + 1);

@@ -63,9 +63,27 @@ void stage_end(int stage, cudaStream_t s, int kernels) {
   t_start = nullptr;
 }
 
+std::atomic<uint32_t> g_spin_limit{kSpinLimit};
+std::atomic<long long> g_unpublished[kNumWaitStages] = {{-1}, {-1}, {-1}};
+
+uint32_t spin_limit() { return g_spin_limit.load(std::memory_order_relaxed); }
+
+long long unpublished_tile(int stage) {
+  return (stage >= 0 && stage < kNumWaitStages) ? g_unpublished[stage].load(std::memory_order_relaxed) : -1;
+}
+
 }  // namespace w2w
 
 extern "C" {
+
+unsigned w2w_test_set_spin_limit(unsigned limit) {
+  return w2w::g_spin_limit.exchange(limit == 0u ? w2w::kSpinLimit : limit);
+}
+
+long long w2w_test_unpublished_tile(int stage, long long tile) {
+  if (stage < 0 || stage >= w2w::kNumWaitStages) return -2;
+  return w2w::g_unpublished[stage].exchange(tile < 0 ? -1 : tile);
+}
 
 unsigned long long w2w_launch_count(void) { return w2w::g_launches.load(); }
 
@@ -115,3 +133,66 @@ int w2w_stage_times(double* ms, long long* launches, int n) {
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Arithmetic throughput probe: the FP32 and SFU issue rates of this GPU, the
+// denominators of the per-pixel passes' roofline (their unit is an evaluated
+// Gaussian-pixel pair: FP32 instructions plus one exponential and one
+// division each).  Every thread runs kChains independent dependency chains,
+// so each warp scheduler always has independent instructions to issue.
+// ---------------------------------------------------------------------------
+namespace w2w {
+namespace {
+
+constexpr int kChains = 8;
+
+__global__ void __launch_bounds__(256) fma_probe_kernel(long long iters, float a, float* out) {
+  float x[kChains];
+#pragma unroll
+  for (int c = 0; c < kChains; ++c) x[c] = float(threadIdx.x + c);
+  for (long long i = 0; i < iters; ++i) {
+#pragma unroll
+    for (int c = 0; c < kChains; ++c) x[c] = __fmaf_rn(x[c], a, 0.5f);
+  }
+  float s = 0.f;
+#pragma unroll
+  for (int c = 0; c < kChains; ++c) s += x[c];
+  if (s == 1234.5f) out[threadIdx.x] = s;  // keeps the chains live; never true for the probe's inputs
+}
+
+__device__ __forceinline__ float ex2_approx(float v) {
+  float r;
+  asm volatile("ex2.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(v));
+  return r;
+}
+
+__global__ void __launch_bounds__(256) sfu_probe_kernel(long long iters, float a, float* out) {
+  float x[kChains];
+#pragma unroll
+  for (int c = 0; c < kChains; ++c) x[c] = a * 1e-3f * float(threadIdx.x + c);
+  for (long long i = 0; i < iters; ++i) {
+    // x stays in [0.5, 1]: one MUFU instruction per step (the sign is an operand modifier)
+#pragma unroll
+    for (int c = 0; c < kChains; ++c) x[c] = ex2_approx(-x[c]);
+  }
+  float s = 0.f;
+#pragma unroll
+  for (int c = 0; c < kChains; ++c) s += x[c];
+  if (s == 1234.5f) out[threadIdx.x] = s;
+}
+
+}  // namespace
+}  // namespace w2w
+
+extern "C" int w2w_throughput_probe(int kind, long long iters, int blocks, float* out, long long* ops,
+                                    w2w_stream_t stream) {
+  using namespace w2w;
+  if ((kind != 0 && kind != 1) || iters <= 0 || blocks <= 0 || !out) return W2W_ERR_INVALID;
+  cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+  // a multiplier just below 1 keeps the chains finite and normal
+  if (kind == 0) fma_probe_kernel<<<blocks, 256, 0, st>>>(iters, 0.999999f, out);
+  else sfu_probe_kernel<<<blocks, 256, 0, st>>>(iters, 0.999999f, out);
+  g_launches.fetch_add(1, std::memory_order_relaxed);
+  if (ops) *ops = (long long)blocks * 256 * iters * kChains;
+  return cudaGetLastError() == cudaSuccess ? W2W_OK : W2W_ERR_CUDA;
+}
