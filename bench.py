@@ -36,7 +36,14 @@ FALLBACK_HBM_GBS = 6650.0
 # DRAM bytes (read + write) per launch, from one ncu capture of the default
 # workload (500k Gaussians, 512x512; dram__bytes_read.sum + dram__bytes_write.sum)
 NCU_TRAFFIC_500K_512 = {"sort_onesweep": 49.0e6, "preprocess": 181.2e6, "duplicate": 12.2e6,
-                        "sort_histogram": 23.7e6, "backward_gaussians": 232.4e6}
+                        "sort_histogram": 23.7e6, "backward_gaussians": 232.4e6, "backward_render": 35.2e6,
+                        "blend": 17.0e6}
+# Algorithmic work of the per-pixel passes per evaluated Gaussian-pixel pair
+# (the pairs are the reference's: sum over pixels of the contributor count):
+# FP32 instructions (an add, multiply or fused multiply-add each counts once)
+# and SFU operations (one exponential and one division's reciprocal).
+PAIR_OPS = {"blend": 20, "backward_render": 60}
+PAIR_SFU = 2
 
 
 def parse():
@@ -53,6 +60,8 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--no-batched", action="store_true", help="skip the batched-call measurement of the workload")
+    ap.add_argument("--no-autotune", action="store_true",
+                    help="keep the default launch shapes instead of tuning them on the workload first")
     ap.add_argument("--single-stream", action="store_true",
                     help="run a step's views one after another on one stream (default: one stream per view)")
     ap.add_argument("--config", default="single", choices=["single", "multiscene", "serve", "sortscan"],
@@ -150,6 +159,33 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(rows)}
 
 
+def arithmetic_peaks(device):
+    """FP32 and SFU issue rates of this GPU, measured with the library's
+    throughput probe (w2w_throughput_probe: independent FMA / ex2 chains on
+    every SM at full occupancy), best of three 20-40 ms launches each, CUDA
+    events on the launching stream, SM clocks sampled meanwhile."""
+    import torch
+    from word2world_b200 import _C
+    sms = torch.cuda.get_device_properties(device).multi_processor_count
+    out = torch.zeros(256, device=device)
+    stream = torch.cuda.current_stream(device)
+    res = {}
+    with ClockSampler(device.index if device.index is not None else 0) as clk:
+        for kind, name, iters in ((0, "fp32_fma", 40000), (1, "sfu_ex2", 4000)):
+            _C.throughput_probe(kind, 100, sms * 8, out)
+            best = 0.0
+            for _ in range(3):
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                ops = _C.throughput_probe(kind, iters, sms * 8, out)
+                e1.record(stream)
+                torch.cuda.synchronize()
+                best = max(best, ops / (e0.elapsed_time(e1) / 1e3))
+            res[name] = best / 1e9  # Gop/s
+    res["clocks"] = clk.summary()
+    return res
+
+
 # ---------------------------------------------------------------------------
 # this implementation
 # ---------------------------------------------------------------------------
@@ -231,8 +267,23 @@ def run_ours(a):
                                          L["opacity"], L["rotations"], c["campos"], c["view"],
                                          a.res / (2 * c["tanx"]), a.res, a.res, bg, True)
             info = _C.binning_info(out[6], out[0], a.res, a.res)
-            plans.append(dict(R=int(out[0]), **{k: int(x) for k, x in info.items()}))
+            # evaluated pairs of the view: the sum over pixels of the contributor count
+            off = _C.image_offset(a.res, a.res, "n_contrib")
+            nc = out[7][off:off + 4 * a.res * a.res].view(torch.int32)
+            pairs = int(nc.to(torch.int64).sum())
+            d = dict(R=int(out[0]), pairs=pairs, **{k: int(x) for k, x in info.items()})
+            d["depth_passes"] = -(-d.get("depth_bits", 18) // 9)
+            plans.append(d)
             del out
+    tuning = None
+    if not a.no_autotune:
+        # launch shapes tuned on this workload's own step (word2world_b200.autotune)
+        from word2world_b200 import autotune
+        tuner = autotune.Autotuner(reps=3, warmup=1)
+        key = autotune.bucket_key(a.res, a.res, a.P, a.grad_mode, device)
+        knobs = tuner.tune(key, step)
+        tuning = {"knobs": knobs, "bucket": key,
+                  "trials": [{"knobs": k, "ms_per_step": round(ms, 4)} for k, ms in tuner.log]}
     for _ in range(max(a.warmup, 1)):
         step()
     torch.cuda.synchronize()
@@ -272,7 +323,7 @@ def run_ours(a):
         if world > 1:
             dist.barrier()
         _C.stage_times()
-        _C.stage_timing_only(["sort_onesweep"])
+        _C.stage_timing_only(["sort_onesweep", "backward_render", "blend"])
         s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         s0.record(stream)
         for _ in range(a.steps):
@@ -293,43 +344,94 @@ def run_ours(a):
     _C.stage_timing(False)
     stages = _C.stage_times()
 
-    # roofline of the dominant HBM-bound stage (per-launch algorithmic bytes / average launch time)
+    # rooflines.  The per-pixel passes (the step's dominant kernels) are bound
+    # by FP32 issue: work = evaluated pairs x FP32 instructions per pair,
+    # against the FP32 rate measured on this GPU.  The other stages are bound
+    # by HBM: per-launch algorithmic bytes / average launch time.
     P, M = a.P, 16
     Rm = statistics.mean(p["R"] for p in plans)
+    pairs = statistics.mean(p["pairs"] for p in plans)
     kb = 8 if any(p["key64"] for p in plans) else 4
     alg_bytes = {
-        "preprocess": P * (12 + 12 + 16 + 4 + 12 * M + 24 + 12 + 3 + 16 + 8 + 4 + 4 + 4 + 8 + 64 + 48 + 4 + 4),
+        # projection + SH read, geometry state written (the survey's 323 B per Gaussian per view)
+        "preprocess": P * 323,
+        # the depth order: one 4-byte key and id read and written per digit pass, a histogram read,
+        # the owned-count gather (id, offset, count, rectangle, reach read; count written)
+        "depth_sort": P * (16 * max(1, plans[0].get("depth_passes", 2)) + 4 + 28),
+        # binning: two walks over the depth-ordered Gaussians (id, prefix, offset, count, rectangle,
+        # reach, depth: 32 B each) and the sorted keys and ids written once
+        "binning": P * 2 * 32 + Rm * (kb + 4),
         "duplicate": Rm * (kb + 4) + P * 24,
         "sort_histogram": Rm * kb,
         "sort_onesweep": Rm * 2 * (kb + 4),
         "backward_gaussians": P * (12 + 4 + 24 + 16 + 12 + 12 + 4 + 3 + 12 * M + 12 + 16 + 12 + 24 + 12 * M + 12 + 16),
     }
+    # bytes this build moves for preprocess, including its per-pixel records (blend 64 B, backward 64 B)
+    preprocess_bytes_built = P * (12 + 12 + 16 + 4 + 12 * M + 24 + 12 + 3 + 16 + 8 + 4 + 4 + 4 + 8 + 64 + 48 + 4 + 4)
     stage_ms = {k: v[0] for k, v in stages.items()}
     stage_n = {k: v[1] for k, v in stages.items()}
     total_stage = sum(stage_ms.values()) or 1.0
     hbm, peak_kind = peaks()
+    ap = arithmetic_peaks(device)
+
+    def launch_ms(k):
+        # a stage's launches as timed in the single-stream timed steps when it
+        # was recorded there, else from the untimed stage steps
+        src = timed_stages.get(k, (0, 0))
+        if src[1]:
+            return src[0] / src[1], "single-stream timed steps"
+        return (stage_ms[k] / stage_n[k], "untimed stage steps") if stage_n.get(k) else (None, None)
+
+    def fp32_line(k):
+        ms, where = launch_ms(k)
+        if ms is None:
+            return None
+        ops = pairs * PAIR_OPS[k]
+        ach = ops / (ms / 1e3) / 1e9
+        sfu = pairs * PAIR_SFU / (ms / 1e3) / 1e9
+        line = {"kernel": k, "bound": "fp32", "achieved": round(ach, 1), "peak": round(ap["fp32_fma"], 1),
+                "unit": "Gop/s", "frac": round(ach / ap["fp32_fma"], 4),
+                "peak_source": "measured here: FP32 FMA issue rate (w2w_throughput_probe)",
+                "ops_per_pair": PAIR_OPS[k], "pairs_per_launch": int(pairs), "avg_launch_ms": round(ms, 4),
+                "sfu": {"achieved": round(sfu, 1), "peak": round(ap["sfu_ex2"], 1), "unit": "Gop/s",
+                        "frac": round(sfu / ap["sfu_ex2"], 4), "ops_per_pair": PAIR_SFU},
+                "traffic": NCU_TRAFFIC_500K_512.get(k) if (a.P, a.res) == (500_000, 512) else None,
+                "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum per launch, one capture "
+                                  "of this workload",
+                "timed_in": where}
+        return line
+
+    roofline = fp32_line("backward_render")
+    roofline_blend = fp32_line("blend")
     hbm_stages = {k: stage_ms[k] for k in alg_bytes if stage_n.get(k)}
     dom = max(hbm_stages, key=hbm_stages.get) if hbm_stages else None
-    roofline = None
+    roofline_hbm = None
     if dom:
-        # the dominant kernel's launches as timed inside the timed region when
-        # it is the one recorded there, else from the untimed stage steps
-        src_ms, src_n = (timed_stages[dom] if timed_stages.get(dom, (0, 0))[1] else (stage_ms[dom], stage_n[dom]))
-        per_launch_ms = src_ms / src_n * (2 if dom == "sort_histogram" else 1)
+        per_launch_ms, where = launch_ms(dom)
+        if dom == "sort_histogram" and where == "untimed stage steps":
+            per_launch_ms *= 2  # the stage brackets the histogram and the offsets kernels
         ach = alg_bytes[dom] / (per_launch_ms / 1e3) / 1e9
-        roofline = {"kernel": dom, "bound": "hbm", "achieved": round(ach, 1), "peak": hbm, "unit": "GB/s",
-                    "frac": round(ach / hbm, 4), "peak_source": peak_kind,
-                    "traffic": NCU_TRAFFIC_500K_512.get(dom) if (a.P, a.res) == (500_000, 512) else None,
-                    "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum per launch "
-                                      "(profiles/dram_traffic_500k_512x512.md)",
-                    "algorithmic_bytes_per_launch": int(alg_bytes[dom]), "avg_launch_ms": round(per_launch_ms, 4),
-                    "timed_in": "timed steps" if single is None else "single-stream timed steps"}
+        roofline_hbm = {"kernel": dom, "bound": "hbm", "achieved": round(ach, 1), "peak": hbm, "unit": "GB/s",
+                        "frac": round(ach / hbm, 4), "peak_source": peak_kind,
+                        "traffic": NCU_TRAFFIC_500K_512.get(dom) if (a.P, a.res) == (500_000, 512) else None,
+                        "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum per launch, one capture "
+                                          "of this workload",
+                        "algorithmic_bytes_per_launch": int(alg_bytes[dom]), "avg_launch_ms": round(per_launch_ms, 4),
+                        "timed_in": where}
         cs = (concurrent_stages or {}).get(dom, (0, 0))
         if cs[1]:
             cms = cs[0] / cs[1]
-            roofline["concurrent"] = {"achieved": round(alg_bytes[dom] / (cms / 1e3) / 1e9, 1),
-                                      "avg_launch_ms": round(cms, 4),
-                                      "note": "launches timed in the per-view-stream steps, sharing the SMs"}
+            roofline_hbm["concurrent"] = {"achieved": round(alg_bytes[dom] / (cms / 1e3) / 1e9, 1),
+                                          "avg_launch_ms": round(cms, 4),
+                                          "note": "launches timed in the per-view-stream steps, sharing the SMs"}
+    if stage_n.get("preprocess"):
+        pms = stage_ms["preprocess"] / stage_n["preprocess"]
+        preprocess_hbm = {"algorithmic_gbs": round(alg_bytes["preprocess"] / (pms / 1e3) / 1e9, 1),
+                          "built_bytes_gbs": round(preprocess_bytes_built / (pms / 1e3) / 1e9, 1),
+                          "avg_launch_ms": round(pms, 4), "peak": hbm,
+                          "note": "algorithmic: 323 B per Gaussian; built: also this build's per-pixel records"}
+    else:
+        preprocess_hbm = None
     stage_report = {k: {"ms_per_step": round(stage_ms[k] / stage_steps, 4),
                         "launches_per_step": stage_n[k] / stage_steps,
                         "share": round(stage_ms[k] / total_stage, 4)} for k in stage_ms if stage_n[k]}
@@ -338,8 +440,14 @@ def run_ours(a):
               "warmup": a.warmup, "ms_per_step": round(ms_max / a.steps, 4), "higher_is_better": True,
               "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded scene, N(0,1) dL/dimage)",
               "config": dict(workload_config(a), parallelism=f"replicas x{world}", num_rendered_per_view=int(Rm),
-                             sort_key_bytes=kb, sort_passes=plans[0].get("passes")),
-              "gpu_launches": int(launches), "clocks": clk.summary(), "roofline": roofline, "stages": stage_report}
+                             sort_key_bytes=kb,
+                             binning=("depth-ordered Gaussians, one counting placement by tile"
+                                      if plans[0].get("passes") == 0 else
+                                      f"key emission + {plans[0].get('passes')}-pass radix sort")),
+              "gpu_launches": int(launches), "clocks": clk.summary(), "roofline": roofline,
+              "roofline_blend": roofline_blend, "roofline_hbm": roofline_hbm, "preprocess_hbm": preprocess_hbm,
+              "arithmetic_peaks": ap, "pairs_per_view": int(pairs), "stages": stage_report,
+              "autotune": tuning}
     if single is not None:
         result["single_stream"] = single
 
@@ -595,7 +703,7 @@ def run_serve(a):
     srv = sv.Server(scs, hbm_budget_bytes=150e9, grad_mode=a.grad_mode)
 
     def release():  # hand the served loop's workspace back, so each path starts from a clean allocator
-        srv.renderer.ws.bufs.clear()
+        srv.release_workspaces()
         torch.cuda.synchronize()
         torch.cuda.empty_cache()
 
@@ -620,14 +728,15 @@ def run_serve(a):
         warm_served()
         reqs = sv.poisson_requests(a.requests, rate, scs, seed=a.seed + 3, device=device)
         srv.batch_ms = []
-        grown = srv.renderer.ws.grown
+        grown = srv.workspace_growths()
         info = srv.serve(reqs, realtime=True)
         bm = np.array(srv.batch_ms)
         served = dict(sv.latency_stats(reqs), batches=info["batches"],
-                      workspace_growths=srv.renderer.ws.grown - grown,
+                      workspace_growths=srv.workspace_growths() - grown,
                       batch_ms_p50=round(float(np.percentile(bm, 50)), 3),
                       batch_ms_p99=round(float(np.percentile(bm, 99)), 3),
-                      workspace_gb=round(srv.renderer.ws.bytes / 1e9, 2))
+                      workspace_gb=round(srv.workspace_bytes() / 1e9, 2),
+                      overlapping_batches=sv.overlapping_batches(srv.batch_log))
         del reqs
         runs[f"{rate:g}"] = {"served": served, "plain": plain,
                              "served_vs_plain_throughput": round(served["views_per_s"] / plain["views_per_s"], 3)}

@@ -117,17 +117,25 @@ size_t w2w_binning_offset(long long num_rendered, int width, int height, const c
  * gaussianForwardPass.cu calcColour and the scan of gaussianRasterizer.cu:233,
  * i.e. gaussianForwardPass, gaussianRasterizer.cu:118-237): one fused kernel.  Writes radii and
  * the geometry state, then reads the instance count and depth-bit range back
- * into *info (synchronising `stream` once). */
+ * into *info (synchronising `stream` once).  For images of at most 4096
+ * tiles it then enqueues the per-Gaussian half of the binning (the Gaussians
+ * sorted stably by depth bits, and the prefix of their owned instance counts
+ * in that order) into the geometry state. */
 int w2w_forward_geometry(const w2w_settings* s, const float* means3D, const float* scales,
                          const float* rotations, const float* opacities, const float* shs,
                          int* radii, void* geom_state, w2w_geometry_info* info, w2w_stream_t stream);
 
 /* Phase 2 (replaces prepareAndSort, prepareSort.cu:362-435, gaussianTiles,
  * gaussianTiles.cu:6-33, and pixelGaussiansFull, pixelGaussiansFull.cu:99-122):
- * key emission, onesweep radix sort, tile ranges, blending.  binning_state
- * must be w2w_binning_state_bytes(info->num_rendered, W, H) long.  Sort keys
- * keep only the bits in which keys can differ (tile bits and the low depth
- * bits below the depths' common prefix), packed into 32 bits when they fit;
+ * the sorted instance list and tile ranges, then blending.  binning_state
+ * must be w2w_binning_state_bytes(info->num_rendered, W, H) long.  Images of
+ * at most 4096 tiles: every instance is placed once, by tile, walking the
+ * Gaussians in the depth order phase 1 prepared (a counting sort whose keys
+ * are generated, not stored); larger images: key emission and an onesweep
+ * radix sort.  Either way the list is the reference's: sorted by tile, then
+ * depth bits, ties in slot order.  The sorted keys are kept in the binning
+ * state, packed: only the bits in which keys can differ (tile bits and the
+ * low depth bits below the depths' common prefix), in 32 bits when they fit;
  * the order equals that of the reference's 64-bit (tile << 32 | depth bits)
  * keys.  With
  * compat_spill=1 keys are emitted over the reference's emission rectangle;
@@ -354,6 +362,23 @@ int w2w_stage_times(double* ms, long long* launches, int max_stages);
  * per-pixel passes' roofline.  `out` (>= 256 floats, device) is never
  * written in practice; it keeps the chains from being optimised away. */
 int w2w_throughput_probe(int kind, long long iters, int blocks, float* out, long long* ops, w2w_stream_t stream);
+
+/* ---- launch-shape tuning -----------------------------------------------------
+ * Process-wide knobs read at every launch, set by the autotuner
+ * (word2world_b200/autotune.py) from timings of the caller's workload.  No
+ * counterpart in the reference, whose launch shapes are fixed
+ * (pixelGaussiansFull.cu:99-122).  Knobs (w2w_tune_name): 0 "blend_warps"
+ * (4: two 4-warp CTAs per tile, 8: one 8-warp CTA; default 4), 1
+ * "backward_split" (the per-pixel backward splits its heaviest tiles, up to
+ * this many quarters of the SM count, across CTAs; 0..16, default 4), 2
+ * "backward_ways" (segments per split tile, 2 or 3; default 2).  Results do
+ * not depend on them beyond the order of float atomic additions.
+ * w2w_tune_set returns the previous value, or -1 (and changes nothing) for an
+ * unknown knob or value. */
+int w2w_tune_count(void);
+const char* w2w_tune_name(int knob);
+int w2w_tune_get(int knob);
+int w2w_tune_set(int knob, int value);
 
 /* ---- test hooks --------------------------------------------------------------
  * For tests of the failure path (no counterpart in the reference).

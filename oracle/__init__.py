@@ -174,9 +174,12 @@ def preprocess(s: RasterSettings, means3D, scales, rotations, opacities, shs, pr
     return out
 
 
-def forward(s: RasterSettings, means3D, scales, rotations, opacities, shs, precision: str = "f32") -> dict:
+def forward(s: RasterSettings, means3D, scales, rotations, opacities, shs, precision: str = "f32",
+            only_tiles=None) -> dict:
     """Full forward.  Returns every intermediate the reference keeps
-    (geometry, binning and image state) plus the images."""
+    (geometry, binning and image state) plus the images.  ``only_tiles``
+    (tile indices): blend only those tiles (the others render as empty),
+    for callers that read a window of the image."""
     L = lib()
     sfx = "_f32" if precision == "f32" else "_f64"
     R_ = np.float32 if precision == "f32" else np.float64
@@ -213,6 +216,11 @@ def forward(s: RasterSettings, means3D, scales, rotations, opacities, shs, preci
     gw, gh = (s.W + 15) // 16, (s.H + 15) // 16
     ranges = np.zeros((gw * gh, 2), np.uint32)
     L.orc_tile_ranges(_p(keys), ctypes.c_longlong(R), _p(ranges), ctypes.c_int(gw * gh))
+    blend_ranges = ranges
+    if only_tiles is not None:
+        blend_ranges = np.zeros_like(ranges)
+        sel = np.asarray(only_tiles, np.int64)
+        blend_ranges[sel] = ranges[sel]
     HW = s.H * s.W
     color = np.zeros((3, s.H, s.W), R_)
     depth_img = np.zeros((1, s.H, s.W), R_)
@@ -222,7 +230,7 @@ def forward(s: RasterSettings, means3D, scales, rotations, opacities, shs, preci
     margin = np.zeros(HW, np.float64)
     sig = np.zeros(HW, np.uint64)
     getattr(L, "orc_blend" + sfx)(
-        ctypes.byref(cfg), _p(ranges), _p(vals if R else np.zeros(1, np.uint32)), _p(out["means2D"]),
+        ctypes.byref(cfg), _p(blend_ranges), _p(vals if R else np.zeros(1, np.uint32)), _p(out["means2D"]),
         _p(out["cov2D"]), _p(out["conic_opac"]), _p(out["rgb"]), _p(out["depth"]), _p(color), _p(depth_img),
         _p(alpha), _p(n_contrib), _p(T_final), _p(margin), _p(sig))
     out.update(offsets=offsets, num_rendered=R, unsorted_keys=unsorted_keys, unsorted_vals=unsorted_vals,

@@ -15,7 +15,8 @@ points ``rasterize_gaussians`` / ``rasterize_gaussians_backward``
 (``cudaForwardBackwardRenderer/ext.cpp:5-7``).  It is loaded only by the GPU
 parity tests, the golden-fixture generator and ``bench.py --impl reference``.
 
-Usage: python oracle/build_ref.py [--ref-root PATH]
+Usage: python oracle/build_ref.py [--ref-root PATH]; the default location of
+the reference checkout is $W2W_REFERENCE_ROOT, else /root/reference.
 """
 import argparse
 import os
@@ -23,6 +24,7 @@ import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 OUT = os.path.join(HERE, "_ref")
+REFERENCE_ROOT = os.environ.get("W2W_REFERENCE_ROOT", "/root/reference")
 MODULE_NAME = "w2w_reference_C"
 SOURCES = [
     "gaussianRasterizer.cu", "gaussianForwardPass.cu", "backward.cu",
@@ -32,7 +34,7 @@ SOURCES = [
 ]
 
 
-def build(ref_root="/root/reference", verbose=False):
+def build(ref_root=REFERENCE_ROOT, verbose=False):
     src_dir = os.path.join(ref_root, "cudaForwardBackwardRenderer")
     if not os.path.isdir(src_dir):
         raise FileNotFoundError(f"reference sources not found at {src_dir}")
@@ -57,7 +59,7 @@ def so_path():
 VOXEL_SO = os.path.join(OUT, "compute_voxel_field.so")
 
 
-def build_voxel(ref_root="/root/reference"):
+def build_voxel(ref_root=REFERENCE_ROOT):
     """The reference's voxel-field kernel (``compute_voxel_field.cu``) as a
     shared library exporting ``compute_voxel_field_cuda``, compiled from its
     one source file where it lies.  The source marks the export with the
@@ -75,7 +77,7 @@ def build_voxel(ref_root="/root/reference"):
 
 if __name__ == "__main__":
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref-root", default="/root/reference")
+    ap.add_argument("--ref-root", default=REFERENCE_ROOT)
     ap.add_argument("-v", action="store_true")
     a = ap.parse_args()
     build(a.ref_root, a.v)

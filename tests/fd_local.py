@@ -26,7 +26,7 @@ def tile_grid(st):
     return (st.W + 15) // 16, (st.H + 15) // 16
 
 
-def neighbourhood(base: dict, i: int, margin: int = 1):
+def neighbourhood(base: dict, i: int, margin: int = 0):
     """Tile rectangle [x0, x1) x [y0, y1) around Gaussian i's rectangle."""
     gw, gh = tile_grid(base["settings"])
     x0, y0, x1, y1 = (int(v) for v in base["rects"][i])
@@ -50,10 +50,16 @@ def box_pixels(st, box):
     return slice(16 * y0, min(st.H, 16 * y1)), slice(16 * x0, min(st.W, 16 * x1))
 
 
-def local_render(st, params: dict, subset: np.ndarray, precision="f64") -> dict:
+def box_tiles(st, box) -> np.ndarray:
+    gw, _ = tile_grid(st)
+    x0, y0, x1, y1 = box
+    return np.array([ty * gw + tx for ty in range(y0, y1) for tx in range(x0, x1)], np.int64)
+
+
+def local_render(st, params: dict, subset: np.ndarray, box, precision="f64") -> dict:
     p = {k: np.ascontiguousarray(np.asarray(v)[subset]) for k, v in params.items()}
     return oracle.forward(st, p["means3D"], p["scales"], p["rotations"], p["opacities"], p["shs"],
-                          precision=precision)
+                          precision=precision, only_tiles=box_tiles(st, box))
 
 
 def central_difference(st, params: dict, base: dict, dL_dcolor, name: str, idx: tuple, rel_h: float = 1e-3):
@@ -73,7 +79,8 @@ def central_difference(st, params: dict, base: dict, dL_dcolor, name: str, idx: 
         li = (k,) + tuple(idx[1:])
         local[name][li] = np.float32(float(arr[idx]) + sign * h)
         renders.append((oracle.forward(st, local["means3D"], local["scales"], local["rotations"],
-                                       local["opacities"], local["shs"], precision="f64"), float(local[name][li])))
+                                       local["opacities"], local["shs"], precision="f64",
+                                       only_tiles=box_tiles(st, box)), float(local[name][li])))
     (fp, vp), (fm, vm) = renders
     hh = (vp - vm) / 2.0
     # the perturbed Gaussian must stay inside the neighbourhood
@@ -82,8 +89,10 @@ def central_difference(st, params: dict, base: dict, dL_dcolor, name: str, idx: 
         if f["radii"][k] > 0 and (x0 < box[0] or y0 < box[1] or x1 > box[2] or y1 > box[3]):
             return None, "left the neighbourhood", hh
     rows, cols = box_pixels(st, box)
+    tiles = box_tiles(st, box)
+    lists = lambda f: [f["point_list"][f["ranges"][t][0]:f["ranges"][t][1]] for t in tiles]
     if not (np.array_equal(fp["blend_signature"][rows, cols], fm["blend_signature"][rows, cols])
-            and np.array_equal(fp["point_list"], fm["point_list"])):
+            and all(np.array_equal(a, b) for a, b in zip(lists(fp), lists(fm)))):
         return None, "blend decision changed", hh
     g = np.asarray(dL_dcolor, np.float64)[:, rows, cols]
     dl = float(np.sum((np.asarray(fp["color"], np.float64)[:, rows, cols] -

@@ -72,7 +72,38 @@ def test_request_same_alone_and_in_the_mix():
     st = sv.latency_stats(reqs)
     assert st["requests"] == 10 and st["p99_ms"] >= st["p50_ms"] > 0
     # the same stream again: the workspace already holds the largest batch
-    grown = srv.renderer.ws.grown
+    grown = srv.workspace_growths()
     srv.serve(sv.poisson_requests(10, rate=1000.0, scenes=scs, seed=5, views=(1, 3), res=(64, 96, 128)),
               realtime=False)
-    assert srv.renderer.ws.grown == grown
+    assert srv.workspace_growths() == grown
+
+
+@pytest.mark.gpu
+@pytest.mark.skipif(not torch.cuda.is_available(), reason="needs a GPU")
+def test_batches_overlap_on_the_device():
+    """With two slots, a batch admitted while another is running starts on the
+    device before that one ends (CUDA events on the slots' streams), and the
+    overlapped results equal each request run alone."""
+    import parity
+    from word2world_b200 import scenes as S
+    from word2world_b200.batch import Scene
+    scs = [Scene.from_arrays(S.make_scene(P, seed=40 + k, layout="ball").activate(), "cuda")
+           for k, P in enumerate((60000, 30000))]
+    reqs = sv.poisson_requests(8, rate=1000.0, scenes=scs, seed=9, views=(2, 2), res=(256,))
+    # at most one request per batch: eight batches through two slots
+    srv = sv.Server(scs, keep_results=True, max_batch_work=1.0, slots=2)
+    info = srv.serve(reqs, realtime=False)
+    assert info["batches"] == 8 and len(srv.batch_log) == 8
+    assert sv.overlapping_batches(srv.batch_log) >= 1, srv.batch_log
+    for r in reqs:
+        assert r.done > r.start >= 0.0
+    for r in (reqs[1], reqs[6]):
+        alone = sv.Request(r.rid, r.scene, r.cameras, r.grads)
+        srv.run_batch([alone])
+        torch.cuda.synchronize()
+        for a, b in zip(alone.color, r.color):
+            assert parity.bit_mismatch(a.cpu().numpy(), b.cpu().numpy()) == 0
+        for ga, gb in zip(alone.scene_grads["per_item"], r.scene_grads["per_item"]):
+            for name, x, y in zip(parity.GRAD_NAMES, ga, gb):
+                chk = parity.grad_check(x.cpu().numpy(), y.cpu().numpy())
+                assert chk["norm_rel"] <= 1e-5 and chk["n_bad"] == 0, (r.rid, name, chk)

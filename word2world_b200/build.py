@@ -24,7 +24,7 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 BUILD = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libw2w_raster.so")
-CUDA_SOURCES = ["preprocess.cu", "duplicate.cu", "sort.cu", "blend.cu", "backward.cu", "scan.cu", "activate.cu",
+CUDA_SOURCES = ["preprocess.cu", "duplicate.cu", "sort.cu", "binning.cu", "blend.cu", "backward.cu", "scan.cu", "activate.cu",
                 "densify.cu", "voxel.cu", "groupsum.cu", "capi.cu", "timing.cu"]
 HEADERS = ["common.cuh", "kernels.h", "pinned_fp.h", "tile_walk.cuh"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")

@@ -93,8 +93,9 @@ activate_backward_kernel(ActivateBackwardArgs a) {
 }
 
 int act_grid(long long P, int row) {
-  int sms = 148;
-  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, 0);
+  int sms = 148, dev = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   const long long want = (P * row + kActThreads - 1) / kActThreads;
   return int(want < 1 ? 1 : (want > (long long)sms * 16 ? (long long)sms * 16 : want));
 }

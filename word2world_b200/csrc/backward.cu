@@ -34,11 +34,14 @@ constexpr int kValues = 10;
 // exactly the state a single walk would have reached; only the order of the
 // atomic additions changes.  Segment lengths (from the back) make the
 // segments' work equal: L_0 = W, L_i = W - kReplayCost * (L_0 + ... + L_{i-1}).
-constexpr int kSplitWays = 2;
+// kSplitWays (2 or 3) and the number of split tiles are run-time tuning
+// knobs (W2W_TUNE_BWD_WAYS, W2W_TUNE_BWD_SPLIT); only the order of the atomic
+// additions depends on them.
 constexpr float kReplayCost = 0.22f;
 
 // List positions [lo, hi) of segment k (0 = the back-most) of a walk of
 // length `walk`.
+template <int kSplitWays>
 __device__ __forceinline__ void segment_of(int walk, int k, int& lo, int& hi) {
   float len[kSplitWays], before = 0.f, total = 0.f;
 #pragma unroll
@@ -265,6 +268,7 @@ __device__ __forceinline__ BwdPixel make_bwd_pixel(const BackwardArgs& a, int ti
   return BwdPixel(a, tile, tile - int(it.tile_base), it.W, it.H, size_t(it.pix_base), it.bg);
 }
 
+template <int kSplitWays>
 __device__ __forceinline__ int cta_tile(const BackwardArgs& a, int& seg) {
   const int b = int(blockIdx.x);
   if (b < kSplitWays * a.split) {
@@ -275,10 +279,11 @@ __device__ __forceinline__ int cta_tile(const BackwardArgs& a, int& seg) {
   return int(a.order_bwd[b - (kSplitWays - 1) * a.split]);
 }
 
+template <int kSplitWays>
 __global__ void __launch_bounds__(kBlendThreads, 2) render_ref_kernel(BackwardArgs a) {
   __shared__ WarpChunk s_chunk[kBlendThreads / 32];
   int role;
-  const int gtile = cta_tile(a, role);
+  const int gtile = cta_tile<kSplitWays>(a, role);
   const float* bgp;
   const BwdPixel p = make_bwd_pixel(a, gtile, bgp);
   RefChain ch;
@@ -329,7 +334,7 @@ __global__ void __launch_bounds__(kBlendThreads, 2) render_ref_kernel(BackwardAr
     walk_back(a.bwd_record, a.point_list, uint32_t(a.P), p.range.x, 0, p.walk, wc, p.tp, full);
   } else {
     int lo, hi;
-    segment_of(p.walk, role, lo, hi);
+    segment_of<kSplitWays>(p.walk, role, lo, hi);
     walk_back(a.bwd_record, a.point_list, uint32_t(a.P), p.range.x, hi, p.walk, wc, p.tp, state_only);
     __syncwarp();
     walk_back(a.bwd_record, a.point_list, uint32_t(a.P), p.range.x, lo, hi, wc, p.tp, full);
@@ -408,10 +413,11 @@ struct ExactChain {
   }
 };
 
+template <int kSplitWays>
 __global__ void __launch_bounds__(kBlendThreads, 2) render_exact_kernel(BackwardArgs a) {
   __shared__ WarpChunk s_chunk[kBlendThreads / 32];
   int role;
-  const int gtile = cta_tile(a, role);
+  const int gtile = cta_tile<kSplitWays>(a, role);
   const float* bgp;
   const BwdPixel p = make_bwd_pixel(a, gtile, bgp);
   ExactChain ch;
@@ -482,7 +488,7 @@ __global__ void __launch_bounds__(kBlendThreads, 2) render_exact_kernel(Backward
     walk_back(a.record, a.point_list, uint32_t(a.P), p.range.x, 0, p.walk, wc, p.tp, full);
   } else {
     int lo, hi;
-    segment_of(p.walk, role, lo, hi);
+    segment_of<kSplitWays>(p.walk, role, lo, hi);
     walk_back(a.record, a.point_list, uint32_t(a.P), p.range.x, hi, p.walk, wc, p.tp, state_only);
     __syncwarp();
     walk_back(a.record, a.point_list, uint32_t(a.P), p.range.x, lo, hi, wc, p.tp, full);
@@ -1210,13 +1216,21 @@ void launch_backward_render(const BackwardArgs& a, cudaStream_t stream) {
   const int tiles = a.items ? a.total_tiles : ((a.W + kTile - 1) / kTile) * ((a.H + kTile - 1) / kTile);
   if (tiles <= 0) return;
   BackwardArgs b = a;
-  int sms = 148;
-  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, 0);
-  b.split = min(tiles / 4, sms);  // the heaviest tiles by largest contributor count
+  int sms = 148, dev = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  // the heaviest tiles by largest contributor count: knob quarters of the SM count
+  b.split = min(tiles / 4, sms * tune_value(kTuneBwdSplit) / 4);
+  const int ways = tune_value(kTuneBwdWays);
   stage_begin(kStBwdRender, stream);
-  const int grid = tiles + (kSplitWays - 1) * b.split;
-  if (a.grad_mode == 1) render_exact_kernel<<<grid, kBlendThreads, 0, stream>>>(b);
-  else render_ref_kernel<<<grid, kBlendThreads, 0, stream>>>(b);
+  const int grid = tiles + (ways - 1) * b.split;
+  if (ways == 3) {
+    if (a.grad_mode == 1) render_exact_kernel<3><<<grid, kBlendThreads, 0, stream>>>(b);
+    else render_ref_kernel<3><<<grid, kBlendThreads, 0, stream>>>(b);
+  } else {
+    if (a.grad_mode == 1) render_exact_kernel<2><<<grid, kBlendThreads, 0, stream>>>(b);
+    else render_ref_kernel<2><<<grid, kBlendThreads, 0, stream>>>(b);
+  }
   stage_end(kStBwdRender, stream, 1);
 }
 

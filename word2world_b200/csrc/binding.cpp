@@ -618,6 +618,20 @@ PYBIND11_MODULE(TORCH_EXTENSION_NAME, m) {
     return int64_t(w2w_test_unpublished_tile(int(stage), tile));
   });
   m.def("set_error_check", [](bool on) { return w2w_set_error_check(on ? 1 : 0) != 0; });
+  m.def("tune_knobs", []() {
+    py::dict d;
+    for (int k = 0; k < w2w_tune_count(); ++k) d[py::str(w2w_tune_name(k))] = w2w_tune_get(k);
+    return d;
+  });
+  m.def("tune_set", [](const std::string& name, int64_t value) {
+    for (int k = 0; k < w2w_tune_count(); ++k)
+      if (name == w2w_tune_name(k)) {
+        const int prev = w2w_tune_set(k, int(value));
+        if (prev < 0) throw std::invalid_argument("invalid value for tuning knob " + name);
+        return int64_t(prev);
+      }
+    throw std::invalid_argument("unknown tuning knob " + name);
+  });
   m.def("activate", &activate);
   m.def("rasterize_gaussians_raw", &rasterize_gaussians_raw);
   m.def("rasterize_gaussians_backward_raw", &rasterize_gaussians_backward_raw);

@@ -63,15 +63,15 @@ struct BlendPixel {
   }
 };
 
-// Warps per CTA: 8 (one CTA per tile) or 4 (two CTAs per tile, upper and
-// lower eight rows; see tile_walk.cuh).
-constexpr int kBlendWarps = 4;
-constexpr int kBlendParts = 8 / kBlendWarps;  // CTAs per tile
-constexpr int kBlendCta = 32 * kBlendWarps;
-constexpr int kStagePer = kBatch / kBlendCta;  // entries each thread stages per batch
-static_assert(kBatch % kBlendCta == 0, "whole entries per thread");
-
-__global__ void __launch_bounds__(kBlendCta, 16 / kBlendWarps) blend_kernel(BlendArgs a) {
+// Warps per CTA, kBlendWarps: 8 (one CTA per tile) or 4 (two CTAs per tile,
+// upper and lower eight rows; see tile_walk.cuh), chosen at run time (the
+// tuning knob W2W_TUNE_BLEND_WARPS).  Results are identical either way.
+template <int kBlendWarps>
+__global__ void __launch_bounds__(32 * kBlendWarps, 16 / kBlendWarps) blend_kernel(BlendArgs a) {
+  constexpr int kBlendParts = 8 / kBlendWarps;  // CTAs per tile
+  constexpr int kBlendCta = 32 * kBlendWarps;
+  constexpr int kStagePer = kBatch / kBlendCta;  // entries each thread stages per batch
+  static_assert(kBatch % kBlendCta == 0, "whole entries per thread");
   __shared__ TileWalkShared<kBlendWarps> sm;
   const int part = int(blockIdx.x) % kBlendParts;
   const int tile = int(a.order[blockIdx.x / kBlendParts]);
@@ -229,13 +229,19 @@ __global__ void __launch_bounds__(1024) tile_order_kernel(const uint2* ranges, c
 void launch_blend(const BlendArgs& a, cudaStream_t stream) {
   const int tiles = a.items ? a.total_tiles : ((a.W + kTile - 1) / kTile) * ((a.H + kTile - 1) / kTile);
   if (tiles <= 0) return;
+  const int warps = tune_value(kTuneBlendWarps);
+  stage_begin(kStOther, stream);
+  // with two CTAs per tile they combine their maxima with atomics: clear first
+  tile_order_kernel<<<1, 1024, 0, stream>>>(a.ranges, nullptr, tiles, a.order, warps == 4 ? a.tile_max : nullptr);
+  stage_end(kStOther, stream, 1);
   stage_begin(kStBlend, stream);
-  tile_order_kernel<<<1, 1024, 0, stream>>>(a.ranges, nullptr, tiles, a.order,
-                                            kBlendParts > 1 ? a.tile_max : nullptr);
-  blend_kernel<<<tiles * kBlendParts, kBlendCta, 0, stream>>>(a);
+  if (warps == 4) blend_kernel<4><<<tiles * 2, 128, 0, stream>>>(a);
+  else blend_kernel<8><<<tiles, 256, 0, stream>>>(a);
+  stage_end(kStBlend, stream, 1);
   // the backward's order: by the largest contributor count the blend just found
+  stage_begin(kStOther, stream);
   tile_order_kernel<<<1, 1024, 0, stream>>>(nullptr, a.tile_max, tiles, a.order_bwd, nullptr);
-  stage_end(kStBlend, stream, 3);
+  stage_end(kStOther, stream, 1);
 }
 
 }  // namespace w2w

@@ -86,8 +86,12 @@ KeyPlan plan_keys(const w2w_geometry_info& info, int W, int H) {
   return k;
 }
 
-__global__ void write_bin_header(BinHeader* h, KeyPlan k, uint32_t R, uint32_t passes) {
-  h->error = 0;
+// fold0 / fold1 (may be null): error words of earlier work on the same data
+// (the depth sort and prefix scan of the binning path), carried into the
+// binning state's word, which the caller reads.
+__global__ void write_bin_header(BinHeader* h, KeyPlan k, uint32_t R, uint32_t passes, const uint32_t* fold0,
+                                 const uint32_t* fold1) {
+  h->error = (fold0 != nullptr ? *fold0 : 0u) | (fold1 != nullptr ? *fold1 : 0u);
   h->key64 = k.key64;
   h->depth_bits = k.depth_bits;
   h->depth_prefix = k.prefix;
@@ -244,6 +248,59 @@ size_t w2w_binning_offset(long long R, int W, int H, const char* name) {
   return size_t(-1);
 }
 
+// Single-view calls with at most kMaxBinTiles tiles bin their instances from
+// the depth-ordered Gaussians (binning.cu); others emit keys and sort them.
+inline bool use_binning(int P, int W, int H) { return P > 0 && num_tiles(W, H) <= kMaxBinTiles; }
+
+// The binning path's per-Gaussian half, after the projection pass: the
+// Gaussians sorted stably by the depth bits their keys keep, and the prefix of
+// their owned instance counts in that order.  Errors land in the geometry
+// header's word and the prefix scan's scratch word (read back by the render).
+static void launch_depth_order(const w2w_settings* s, void* geom_state, const w2w_geometry_info& info,
+                               cudaStream_t st) {
+  const int P = s->P;
+  const GeomLayout L(P);
+  const KeyPlan kp = plan_keys(info, s->width, s->height);
+  uint32_t* order = at<uint32_t>(geom_state, L.dorder);
+  if (kp.depth_bits == 0) {
+    launch_iota(order, P, st);  // one depth: Gaussian order
+  } else {
+    SortArgs so{};
+    so.n = P; so.key64 = 0; so.begin_bit = 0; so.bits = kp.depth_bits;
+    so.keys_in = at<uint32_t>(geom_state, L.depth);  // the depths' float bits
+    so.vals_in = nullptr;                            // values: the Gaussian ids
+    so.keys_out = at<uint32_t>(geom_state, L.dkeys); so.vals_out = order;
+    so.keys_tmp = at<uint32_t>(geom_state, L.dtmp_keys); so.vals_tmp = at<uint32_t>(geom_state, L.dtmp_vals);
+    so.hist = at<uint32_t>(geom_state, L.dsort_hist);
+    so.counters = at<uint32_t>(geom_state, L.dsort_counters);
+    so.status = at<uint32_t>(geom_state, L.dsort_status);
+    so.error = &at<GeomHeader>(geom_state, L.header)->error;
+    so.tile_shift = 0; so.num_tiles = 0; so.tile_hist = nullptr; so.ranges = nullptr;
+    const int passes = sort_passes(kp.depth_bits);
+    so.clear_span = at<void>(geom_state, L.dsort_hist);
+    so.clear_bytes = L.dsort_status - L.dsort_hist +
+                     size_t(passes) * kMaxBins * 4 * size_t((P + sort_tile_keys(0) - 1) / sort_tile_keys(0));
+    so.spin_limit = spin_limit();
+    so.unpublished_tile = unpublished_tile(kWaitSort);
+    so.stage_hist = so.stage_pass = kStDepthSort;
+    launch_sort(so, st);
+  }
+  BinArgs b{};
+  b.P = P; b.R = uint32_t(info.num_rendered);
+  b.order = order;
+  b.tiles = at<uint32_t>(geom_state, L.tiles);
+  b.offsets = at<uint32_t>(geom_state, L.offsets);
+  b.rect = at<uint32_t>(geom_state, L.rect);
+  b.prev_reach = at<uint32_t>(geom_state, L.prev_reach);
+  uint32_t* count = at<uint32_t>(geom_state, L.dtmp_vals);  // free once the sort is done
+  uint32_t* dprefix = at<uint32_t>(geom_state, L.dprefix);
+  stage_begin(kStDepthSort, st);
+  launch_owned_counts(b, count, st);
+  cudaMemsetAsync(dprefix, 0, 4, st);
+  stage_end(kStDepthSort, st, 1);
+  launch_scan(count, dprefix + 1, P, 0, at<void>(geom_state, L.dscan), st);
+}
+
 // raw != null: Renderer.render's raw parameters, activated by preprocess
 struct RawParams {
   const float *svec, *quat, *logit, *sh_dc, *sh_ac;
@@ -296,6 +353,10 @@ static int forward_geometry(const w2w_settings* s, const float* means3D, const f
   info->error = h.error;
   if (h.error & kErrTimeout) return W2W_ERR_TIMEOUT;
   if (h.error & kErrCapacity) return W2W_ERR_CAPACITY;
+  if (h.num_rendered > 0 && use_binning(s->P, s->width, s->height)) {
+    launch_depth_order(s, geom_state, *info, st);
+    return check_launch();
+  }
   return W2W_OK;
 }
 
@@ -334,6 +395,35 @@ int w2w_forward_render(const w2w_settings* s, const void* geom_state, const w2w_
   const void* err_word = nullptr;  // the binning header's error word
   if (R == 0) {
     cudaMemsetAsync(ranges, 0, sizeof(uint2) * size_t(T), st);
+  } else if (use_binning(s->P, W, H)) {
+    const GeomLayout GL(s->P);
+    const BinLayout BL(R, T);
+    const KeyPlan kp = plan_keys(*info, W, H);
+    BinHeader* bh = at<BinHeader>(binning_state, BL.header);
+    err_word = &bh->error;
+    stage_begin(kStOther, st);
+    write_bin_header<<<1, 1, 0, st>>>(bh, kp, uint32_t(R), 0u, &at<GeomHeader>(geom_state, GL.header)->error,
+                                      at<uint32_t>(geom_state, GL.dscan + 4));
+    stage_end(kStOther, st, 1);
+    BinArgs b{};
+    b.P = s->P; b.R = uint32_t(R); b.gw = tiles_x(W); b.T = T;
+    b.key64 = kp.key64; b.depth_bits = uint32_t(kp.depth_bits);
+    b.order = at<uint32_t>(geom_state, GL.dorder);
+    b.dprefix = at<uint32_t>(geom_state, GL.dprefix);
+    b.tiles = at<uint32_t>(geom_state, GL.tiles);
+    b.offsets = at<uint32_t>(geom_state, GL.offsets);
+    b.rect = at<uint32_t>(geom_state, GL.rect);
+    b.prev_reach = at<uint32_t>(geom_state, GL.prev_reach);
+    b.depth = at<float>(geom_state, GL.depth);
+    b.warp_start = at<uint32_t>(binning_state, BL.warp_start);
+    b.counts = at<uint32_t>(binning_state, BL.bin_counts);
+    b.tile_total = at<uint32_t>(binning_state, BL.tile_hist);
+    b.ranges = ranges;
+    b.keys = at<void>(binning_state, BL.keysA);
+    b.vals = at<uint32_t>(binning_state, BL.valsA);
+    b.error = &bh->error;
+    launch_binning(b, st);
+    point_list = b.vals;
   } else {
     const GeomLayout GL(s->P);
     const BinLayout BL(R, T);
@@ -342,7 +432,7 @@ int w2w_forward_render(const w2w_settings* s, const void* geom_state, const w2w_
     BinHeader* bh = at<BinHeader>(binning_state, BL.header);
     err_word = &bh->error;
     stage_begin(kStOther, st);
-    write_bin_header<<<1, 1, 0, st>>>(bh, kp, uint32_t(R), uint32_t(passes));
+    write_bin_header<<<1, 1, 0, st>>>(bh, kp, uint32_t(R), uint32_t(passes), nullptr, nullptr);
     stage_end(kStOther, st, 1);
     // the sort result lands in (keysA, valsA); key emission targets the
     // buffer that makes the ping-pong end there
@@ -982,7 +1072,7 @@ int w2w_batch_forward_render(const w2w_batch_item* items, int n, const void* geo
     BinHeader* bh = at<BinHeader>(binning_state, BL.header);
     err_word = &bh->error;
     stage_begin(kStOther, st);
-    write_bin_header<<<1, 1, 0, st>>>(bh, kp, uint32_t(R), uint32_t(passes));
+    write_bin_header<<<1, 1, 0, st>>>(bh, kp, uint32_t(R), uint32_t(passes), nullptr, nullptr);
     stage_end(kStOther, st, 1);
     const bool odd = (passes % 2) == 1;
     void* keysA = at<void>(binning_state, BL.keysA);

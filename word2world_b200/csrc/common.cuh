@@ -320,9 +320,24 @@ __device__ __forceinline__ void stage_span(const float* src, int len, float* s, 
 }
 
 
+constexpr int kSortTileMin = 4096;  // smallest onesweep tile of any key type: status words are sized for it
+constexpr int kMaxPasses = 8;
+constexpr int kMaxDigitBits = 9;             // digit width: ceil(bits / ceil(bits / 9))
+constexpr int kMaxBins = 1 << kMaxDigitBits;
+
+// Instance binning from depth-ordered Gaussians (binning.cu)
+constexpr int kBinChunk = 4096;     // instance positions per CTA of the count / scatter kernels
+constexpr int kBinShare = kBinChunk / 8;  // positions per warp of a chunk
+constexpr int kMaxBinTiles = 4096;  // tile counts up to this use the binning path (1024 x 1024 at 16 x 16)
+constexpr int kScanTileElems = 4096;  // elements per CTA of the stand-alone scan
+
 struct GeomLayout {
   size_t header, scan_status, depth, clamped, means2D, cov3D, conic, rgb, tiles, offsets, rect, prev_reach,
       record, bwd_record, total;
+  // the Gaussians by depth (single-view calls): sorted ids and keys, the
+  // sort's ping-pong buffers, its histograms / counters / status words (one
+  // span, cleared together), the owned-instance prefix and its scan scratch
+  size_t dorder, dkeys, dtmp_keys, dtmp_vals, dprefix, dsort_hist, dsort_counters, dsort_status, dscan;
   // header and scan_status are adjacent so one memset clears both
   __host__ __device__ explicit GeomLayout(long long P) {
     size_t o = 0;
@@ -342,6 +357,15 @@ struct GeomLayout {
     prev_reach = take(p * 4);
     record = take(p * sizeof(BlendRecord));
     bwd_record = take(p * sizeof(BackwardRecord));
+    dorder = take(p * 4);
+    dkeys = take(p * 4);
+    dtmp_keys = take(p * 4);
+    dtmp_vals = take(p * 4);
+    dprefix = take((p + 1) * 4);
+    dsort_hist = take(size_t(kMaxPasses) * kMaxBins * 4);
+    dsort_counters = take(size_t(kMaxPasses) * 4);
+    dsort_status = take(size_t(kMaxPasses) * kMaxBins * ((p + kSortTileMin - 1) / kSortTileMin + 1) * 4);
+    dscan = take(256 + ((p + kScanTileElems - 1) / kScanTileElems + 1) * 8);
     total = align256(o);
   }
 };
@@ -378,13 +402,9 @@ struct BinHeader {
 };
 
 constexpr int kSortThreads = 256;
-constexpr int kSortTileMin = 4096;  // smallest onesweep tile of any key type: status words are sized for it
-constexpr int kMaxPasses = 8;
-constexpr int kMaxDigitBits = 9;             // digit width: ceil(bits / ceil(bits / 9))
-constexpr int kMaxBins = 1 << kMaxDigitBits;
 
 struct BinLayout {
-  size_t header, keysA, keysB, valsA, valsB, hist, status, tile_hist, total;
+  size_t header, keysA, keysB, valsA, valsB, hist, status, tile_hist, bin_counts, warp_start, total;
   __host__ __device__ BinLayout(long long R, int num_tiles) {
     size_t o = 0;
     auto take = [&](size_t bytes) { size_t a = align256(o); o = a + bytes; return a; };
@@ -400,6 +420,11 @@ struct BinLayout {
     hist = take(size_t(kMaxPasses) * kMaxBins * 4);
     tile_hist = take(size_t(num_tiles > 0 ? num_tiles : 1) * 4);
     status = take(size_t(kMaxPasses) * sort_tiles * kMaxBins * 4);
+    // binning path (tile counts up to kMaxBinTiles): the chunk x tile matrix
+    // and every warp share's first depth-order index
+    const size_t chunks = num_tiles > 0 && num_tiles <= kMaxBinTiles ? (r + kBinChunk - 1) / kBinChunk : 0;
+    bin_counts = take(chunks * size_t(num_tiles > 0 ? num_tiles : 0) * 4);
+    warp_start = take(chunks ? ((r + kBinShare - 1) / kBinShare + 1) * 4 : 0);
     total = align256(o);
   }
 };

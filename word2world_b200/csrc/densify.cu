@@ -33,8 +33,9 @@ densify_stats_kernel(long long P, const float* __restrict__ dL_dmeans2D, const i
 void launch_densify_stats(long long P, const float* dL_dmeans2D, const int* radii, float* accum, float* counter,
                           cudaStream_t stream) {
   if (P <= 0) return;
-  int sms = 148;
-  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, 0);
+  int sms = 148, dev = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   const long long want = (P + 255) / 256;
   const int grid = int(want > (long long)sms * 8 ? (long long)sms * 8 : want);
   stage_begin(kStOther, stream);

@@ -47,8 +47,9 @@ void launch_group_sum(const float* src, int width, int num_groups, const uint32_
   const uint32_t* item_ptr = tables + (num_groups + 1);
   const uint32_t* item_elem = item_ptr + (num_groups + 1);
   (void)num_items;
-  int sms = 148;
-  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, 0);
+  int sms = 148, dev = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   const long long want = (total + kGroupThreads - 1) / kGroupThreads;
   const int grid = int(want > (long long)sms * 16 ? (long long)sms * 16 : want);
   stage_begin(kStOther, stream);

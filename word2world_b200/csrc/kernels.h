@@ -127,6 +127,7 @@ struct SortArgs {
   uint32_t* error;
   uint32_t spin_limit = kSpinLimit;  // bounded waits (spin_limit())
   long long unpublished_tile = -1;   // first pass: tile that skips publishing (tests; -1 = none)
+  int stage_hist = -1, stage_pass = -1;  // timing stages (default: the sort's own)
   int tile_shift;
   int num_tiles;
   uint32_t* tile_hist;
@@ -219,6 +220,37 @@ struct BackwardArgs {
 void launch_backward_render(const BackwardArgs& a, cudaStream_t stream);
 void launch_backward_gaussians(const BackwardArgs& a, cudaStream_t stream);
 
+// Instance binning from depth-ordered Gaussians (binning.cu): a single-view
+// call's sorted instance list and tile ranges without key emission or an
+// R-sized sort.  `order` is the Gaussians sorted stably by their depth bits,
+// `dprefix` the exclusive prefix (P + 1 entries) of their owned instance
+// counts in that order.
+struct BinArgs {
+  int P;
+  uint32_t R;
+  int gw, T;
+  int key64;
+  uint32_t depth_bits;
+  const uint32_t* order;       // [P]
+  const uint32_t* dprefix;     // [P + 1]
+  const uint32_t* tiles;       // geometry state: allocation counts, inclusive offsets, emission rectangles,
+  const uint32_t* offsets;     // earlier Gaussians' reach and depths
+  const uint32_t* rect;
+  const uint32_t* prev_reach;
+  const float* depth;
+  uint32_t* warp_start;        // [ceil(R / kBinShare)] depth-order index at each warp share's start
+  uint32_t* counts;            // [ceil(R / kBinChunk)][T]: chunk counts, then each chunk's first slot per tile
+  uint32_t* tile_total;        // [T]
+  uint2* ranges;               // [T]
+  void* keys;                  // sorted packed keys (tile << depth_bits | low depth bits), 32 or 64 bit
+  uint32_t* vals;              // sorted Gaussian ids (the point list)
+  uint32_t* error;
+};
+size_t bin_smem_bytes(int tiles);
+void launch_iota(uint32_t* out, int n, cudaStream_t stream);
+void launch_owned_counts(const BinArgs& a, uint32_t* count, cudaStream_t stream);
+void launch_binning(const BinArgs& a, cudaStream_t stream);
+
 }  // namespace w2w
 
 namespace w2w {
@@ -226,7 +258,7 @@ namespace w2w {
 // of one logical step; `kernels` is how many kernels the stage launched.
 enum Stage {
   kStPreprocess, kStDuplicate, kStSortHist, kStSortPass, kStBlend, kStBwdRender, kStBwdGaussians, kStScan,
-  kStOther, kNumStages
+  kStOther, kStDepthSort, kStBinning, kNumStages
 };
 void stage_begin(int stage, cudaStream_t s);
 void stage_end(int stage, cudaStream_t s, int kernels);
@@ -282,6 +314,14 @@ size_t scan_status_words(long long n);
 enum WaitStage { kWaitScan = 0, kWaitSort = 1, kWaitPreprocess = 2, kNumWaitStages = 3 };
 uint32_t spin_limit();
 long long unpublished_tile(int stage);
+
+// Run-time launch shapes chosen by the autotuner (w2w_tune_set): warps per
+// blend CTA (4: two CTAs per tile, 8: one), how many of the heaviest tiles the
+// per-pixel backward splits (in quarters of the SM count) and into how many
+// segments.  None of them changes a result beyond the order of float atomic
+// additions.
+enum TuneKnob { kTuneBlendWarps = 0, kTuneBwdSplit = 1, kTuneBwdWays = 2, kNumTuneKnobs = 3 };
+int tune_value(int knob);
 
 size_t scan_scratch_bytes(long long n);
 void launch_scan(const uint32_t* in, uint32_t* out, long long n, int exclusive, void* scratch, cudaStream_t stream);

@@ -12,6 +12,7 @@ namespace {
 constexpr int kScanThreads = 256;
 constexpr int kScanItems = 16;
 constexpr int kScanTile = kScanThreads * kScanItems;
+static_assert(kScanTile == kScanTileElems, "scratch layouts assume kScanTileElems elements per tile");
 constexpr unsigned long long kAgg = 1ull << 62, kInc = 2ull << 62, kFlags = 3ull << 62;
 
 // 64-bit status words: flag in the top two bits, a uint32 partial sum (which

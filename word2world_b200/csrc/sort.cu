@@ -289,7 +289,7 @@ __device__ __forceinline__ void onesweep_tile_pass(const K* __restrict__ kin, co
     const uint32_t idx = wbase + uint32_t(i * 32);
     if (kFull || idx < n) {
       k[i] = __ldg(kin + idx);
-      v[i] = __ldg(vin + idx);
+      v[i] = vin != nullptr ? __ldg(vin + idx) : idx;  // no values: the keys' positions
     } else {
       k[i] = K(0);
       v[i] = 0u;
@@ -466,8 +466,9 @@ void run_sort(const SortArgs& a, cudaStream_t stream) {
     if (a.tile_hist) cudaMemsetAsync(a.tile_hist, 0, sizeof(uint32_t) * size_t(a.num_tiles), stream);
   }
   if (passes > 0 || a.tile_hist) {
-    int sms = 148;
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, 0);
+    int sms = 148, dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     // a few blocks per SM: each block's flush is passes * kMaxBins global atomics
     const long long want = (n + kHistThreads * kHistRun * 4 - 1) / (kHistThreads * kHistRun * 4);
     const int grid = int(max(1LL, min(want, (long long)sms * 2)));
@@ -476,12 +477,13 @@ void run_sort(const SortArgs& a, cudaStream_t stream) {
         sizeof(uint32_t) * (size_t(passes) * kMaxBins + (tiles_in_smem ? size_t(a.num_tiles) : 0));
     if (smem > 48 * 1024)
       cudaFuncSetAttribute(hist_kernel<K>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
-    stage_begin(kStSortHist, stream);
+    const int st_hist = a.stage_hist >= 0 ? a.stage_hist : kStSortHist;
+    stage_begin(st_hist, stream);
     hist_kernel<K><<<grid, kHistThreads, smem, stream>>>(reinterpret_cast<const K*>(a.keys_in), n, a.begin_bit,
                                                          passes, dbits, a.bits, a.hist, a.tile_shift,
                                                          a.num_tiles, a.tile_hist);
     offsets_kernel<<<1, 1024, 0, stream>>>(a.hist, passes, a.tile_hist, a.num_tiles, a.ranges);
-    stage_end(kStSortHist, stream, 2);
+    stage_end(st_hist, stream, 2);
   }
   const K* kin = reinterpret_cast<const K*>(a.keys_in);
   const uint32_t* vin = a.vals_in;
@@ -489,12 +491,13 @@ void run_sort(const SortArgs& a, cudaStream_t stream) {
     const bool to_out = ((passes - 1 - p) % 2) == 0;
     K* kout = reinterpret_cast<K*>(to_out ? a.keys_out : a.keys_tmp);
     uint32_t* vout = to_out ? a.vals_out : a.vals_tmp;
-    stage_begin(kStSortPass, stream);
+    const int st_pass = a.stage_pass >= 0 ? a.stage_pass : kStSortPass;
+    stage_begin(st_pass, stream);
     launch_onesweep<K>(pass_width(p, dbits, a.bits), int(tiles), stream, kin, vin, kout, vout, n,
                        a.begin_bit + dbits * p, a.hist + kMaxBins * p,
                        a.status + size_t(p) * kMaxBins * size_t(tiles), a.counters + p, a.error,
                        a.spin_limit, p == 0 ? a.unpublished_tile : -1LL);
-    stage_end(kStSortPass, stream, 1);
+    stage_end(st_pass, stream, 1);
     kin = kout;
     vin = vout;
   }

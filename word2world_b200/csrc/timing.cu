@@ -15,7 +15,8 @@ namespace w2w {
 namespace {
 
 const char* kStageNames[kNumStages] = {"preprocess", "duplicate", "sort_histogram", "sort_onesweep", "blend",
-                                       "backward_render", "backward_gaussians", "scan", "other"};
+                                       "backward_render", "backward_gaussians", "scan", "other", "depth_sort",
+                                       "binning"};
 
 std::atomic<unsigned long long> g_launches{0};
 std::atomic<unsigned> g_mask{0};  // bit s: stage s records events
@@ -68,6 +69,23 @@ std::atomic<long long> g_unpublished[kNumWaitStages] = {{-1}, {-1}, {-1}};
 
 uint32_t spin_limit() { return g_spin_limit.load(std::memory_order_relaxed); }
 
+namespace {
+const char* kTuneNames[kNumTuneKnobs] = {"blend_warps", "backward_split", "backward_ways"};
+std::atomic<int> g_tune[kNumTuneKnobs] = {{4}, {4}, {2}};
+bool tune_valid(int knob, int v) {
+  switch (knob) {
+    case kTuneBlendWarps: return v == 4 || v == 8;
+    case kTuneBwdSplit: return v >= 0 && v <= 16;
+    case kTuneBwdWays: return v == 2 || v == 3;
+    default: return false;
+  }
+}
+}  // namespace
+
+int tune_value(int knob) {
+  return (knob >= 0 && knob < kNumTuneKnobs) ? g_tune[knob].load(std::memory_order_relaxed) : 0;
+}
+
 long long unpublished_tile(int stage) {
   return (stage >= 0 && stage < kNumWaitStages) ? g_unpublished[stage].load(std::memory_order_relaxed) : -1;
 }
@@ -75,6 +93,19 @@ long long unpublished_tile(int stage) {
 }  // namespace w2w
 
 extern "C" {
+
+int w2w_tune_count(void) { return w2w::kNumTuneKnobs; }
+
+const char* w2w_tune_name(int knob) {
+  return (knob >= 0 && knob < w2w::kNumTuneKnobs) ? w2w::kTuneNames[knob] : "";
+}
+
+int w2w_tune_get(int knob) { return w2w::tune_value(knob); }
+
+int w2w_tune_set(int knob, int value) {
+  if (!w2w::tune_valid(knob, value)) return -1;
+  return w2w::g_tune[knob].exchange(value);
+}
 
 unsigned w2w_test_set_spin_limit(unsigned limit) {
   return w2w::g_spin_limit.exchange(limit == 0u ? w2w::kSpinLimit : limit);

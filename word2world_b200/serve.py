@@ -2,14 +2,19 @@
 admitted under an HBM budget and batched as they arrive.
 
 A request is (scene, views, upstream image gradients).  Scenes stay resident
-on the device.  The loop is continuous batching: each time the GPU finishes a
-batch, every request that has arrived and fits the memory budget joins the
-next batch (one BatchRenderer forward + backward over all their views), so
-requests that arrive while others are on the GPU wait at most one batch.
+on the device.  The loop is continuous batching over a few execution slots,
+each with its own CUDA stream and its own grow-only workspace: whenever a slot
+is free, every request that has arrived and fits the memory the in-flight
+batches leave of the budget joins one batch (one BatchRenderer forward +
+backward over all their views), launched on that slot's stream while the
+other slots' batches are still running.  So requests that arrive while others
+are on the GPU start as soon as a slot and memory free up, and their kernels
+overlap on the device with the batches already there; completion is seen by
+polling each batch's end event, never by a device-wide synchronisation.
 Each request's result is what it would get alone: its images are
 bit-identical and its gradients equal up to float atomic order
-(tests/test_serve.py).  Latency is arrival to completion; completion is when
-the batch holding the request has finished on the device.
+(tests/test_serve.py).  Latency is arrival to completion, with start and
+completion taken from the batch's CUDA events on its stream.
 
 The reference has no serving loop; its per-call path is one
 ``Renderer.render`` per view (here: one single-view call at a time, FIFO,
@@ -61,11 +66,25 @@ def request_bytes(req: Request, scenes) -> int:
     return int(total)
 
 
+class _Slot:
+    """One execution slot: a stream, a renderer with its own workspace, and
+    the batch in flight on it (with its start / end events)."""
+
+    def __init__(self, device, grad_mode):
+        self.renderer = BatchRenderer(grad_mode=grad_mode, reuse_buffers=True, device=device)
+        self.stream = torch.cuda.Stream(device=device)
+        self.batch = None
+        self.bytes = 0.0
+        self.ev_start = None
+        self.ev_end = None
+
+
 class Server:
     """Continuous-batching request loop over resident scenes."""
 
     def __init__(self, scenes, hbm_budget_bytes: float = 150e9, max_instances: float = 4e8,
-                 max_batch_work: float = 2e7, grad_mode: str = "reference", keep_results: bool = False):
+                 max_batch_work: float = 2e7, grad_mode: str = "reference", keep_results: bool = False,
+                 slots: int = 2):
         self.scenes = scenes
         self.budget = float(hbm_budget_bytes)
         self.max_instances = float(max_instances)  # keeps a batch's instance count far below the 2^30 limit
@@ -74,23 +93,44 @@ class Server:
         # for 256-1024^2 views), so 2e7 keeps a batch near 50 ms and a request
         # that arrives during one waits at most that long before its own.
         self.max_work = float(max_batch_work)
-        # one grow-only workspace for every batch: no allocator calls once it
-        # has grown to the largest batch (a request's gradients are therefore
-        # valid until the next batch unless keep_results copies them)
-        self.renderer = BatchRenderer(grad_mode=grad_mode, reuse_buffers=True)
+        # every slot keeps one grow-only workspace for its batches: no
+        # allocator calls once it has grown to the largest batch (a request's
+        # gradients are therefore valid until its slot's next batch unless
+        # keep_results copies them)
+        dev = torch.device("cuda", torch.cuda.current_device()) if torch.cuda.is_available() else None
+        self.grad_mode = grad_mode
+        self.slots = [_Slot(dev, grad_mode) for _ in range(max(1, int(slots)))] if dev is not None else []
         self.keep = keep_results
         self.batch_ms = []
+        self.batch_log = []  # (device start s, device end s, request ids) per completed batch
 
-    def _admit(self, queue):
+    @property
+    def renderer(self):
+        return self.slots[0].renderer
+
+    def workspace_bytes(self) -> int:
+        return sum(s.renderer.ws.bytes for s in self.slots)
+
+    def workspace_growths(self) -> int:
+        return sum(s.renderer.ws.grown for s in self.slots)
+
+    def release_workspaces(self):
+        for s in self.slots:
+            s.renderer.ws.bufs.clear()
+
+    def _admit(self, queue, budget=None, at_least_one=True):
         """Requests (in arrival order) that fit the memory budget, the
-        instance bound and the work bound of one batch; at least one."""
+        instance bound and the work bound of one batch; at least one when
+        ``at_least_one`` (nothing else in flight), else possibly none."""
+        budget = self.budget if budget is None else budget
         batch, mem, inst, work = [], 0.0, 0.0, 0.0
         for r in queue:
             b = request_bytes(r, self.scenes)
             P = self.scenes[r.scene].P
             i = sum(12.0 * P * c.width * c.height / (512 * 512) for c in r.cameras)
             w = float(P) * len(r.cameras)
-            if batch and (mem + b > self.budget or inst + i > self.max_instances or work + w > self.max_work):
+            if (batch or not at_least_one) and (mem + b > budget or inst + i > self.max_instances or
+                                                work + w > self.max_work):
                 break
             batch.append(r)
             mem += b
@@ -98,12 +138,13 @@ class Server:
             work += w
         return batch
 
-    def run_batch(self, batch):
+    def run_batch(self, batch, renderer=None):
+        renderer = self.renderer if renderer is None else renderer
         views = [v for r in batch for v in r.views()]
         grads = [g for r in batch for g in r.grads]
         groups = [k for k, r in enumerate(batch) for _ in r.cameras]
-        res = self.renderer.forward(self.scenes, views)
-        out = self.renderer.backward(res, grads, per_element=self.keep, groups=groups)
+        res = renderer.forward(self.scenes, views)
+        out = renderer.backward(res, grads, per_element=self.keep, groups=groups)
         k = 0
         for j, r in enumerate(batch):  # each request: its scene's gradient summed over its views
             r.scene_grads = {name: out[name][j] for name in ("means3D", "opacities", "scales", "rotations", "shs")}
@@ -115,32 +156,60 @@ class Server:
                 k += n
         return res, out
 
+    def _launch(self, slot, batch, origin):
+        slot.stream.wait_stream(torch.cuda.current_stream(slot.stream.device))  # the requests' inputs
+        with torch.cuda.stream(slot.stream):
+            slot.ev_start = torch.cuda.Event(enable_timing=True)
+            slot.ev_start.record(slot.stream)
+            self.run_batch(batch, slot.renderer)
+            slot.ev_end = torch.cuda.Event(enable_timing=True)
+            slot.ev_end.record(slot.stream)
+        slot.batch = batch
+        slot.bytes = float(sum(request_bytes(r, self.scenes) for r in batch))
+
+    def _complete(self, slot, origin):
+        start = origin.elapsed_time(slot.ev_start) / 1e3
+        end = origin.elapsed_time(slot.ev_end) / 1e3
+        for r in slot.batch:
+            r.start, r.done = start, end
+        self.batch_ms.append((end - start) * 1e3)
+        self.batch_log.append((start, end, [r.rid for r in slot.batch]))
+        slot.batch, slot.bytes = None, 0.0
+
     def serve(self, requests, realtime: bool = True):
         """Process requests (sorted by arrival).  With realtime, arrivals are
         honoured against the wall clock (the loop waits for the next arrival
         when idle); otherwise all requests are present at time 0."""
         pending = sorted(requests, key=lambda r: r.arrival)
         queue = []
+        origin = torch.cuda.Event(enable_timing=True)
+        origin.record()
         t0 = time.perf_counter()
         now = lambda: time.perf_counter() - t0
         batches = 0
-        while pending or queue:
+        while pending or queue or any(s.batch is not None for s in self.slots):
             t = now()
             while pending and (not realtime or pending[0].arrival <= t):
                 queue.append(pending.pop(0))
-            if not queue:
-                time.sleep(max(0.0, min(pending[0].arrival - t, 0.001)))
-                continue
-            batch = self._admit(queue)
-            queue = queue[len(batch):]
-            start = now()
-            self.run_batch(batch)
-            torch.cuda.synchronize()
-            end = now()
-            self.batch_ms.append((end - start) * 1e3)
-            for r in batch:
-                r.start, r.done = start, end
-            batches += 1
+            progressed = False
+            for s in self.slots:
+                if s.batch is not None and s.ev_end.query():
+                    self._complete(s, origin)
+                    progressed = True
+            free = [s for s in self.slots if s.batch is None]
+            if queue and free:
+                busy = [s for s in self.slots if s.batch is not None]
+                batch = self._admit(queue, self.budget - sum(s.bytes for s in busy), at_least_one=not busy)
+                if batch:
+                    queue = queue[len(batch):]
+                    self._launch(free[0], batch, origin)
+                    batches += 1
+                    progressed = True
+            if not progressed:
+                if any(s.batch is not None for s in self.slots) or queue:
+                    time.sleep(0.0001)  # a batch is running: poll its end event again shortly
+                elif pending:
+                    time.sleep(max(0.0, min(pending[0].arrival - now(), 0.001)))
         return dict(batches=batches, wall=now())
 
     def serve_plain(self, requests, realtime: bool = True):
@@ -182,6 +251,13 @@ class Server:
             torch.cuda.synchronize()
             r.done = now()
         return dict(wall=now())
+
+
+def overlapping_batches(batch_log) -> int:
+    """Batches that started on the device before the previous one (in start
+    order) had finished there."""
+    log = sorted(batch_log)
+    return sum(1 for a, b in zip(log, log[1:]) if b[0] < a[1])
 
 
 def latency_stats(requests):
