@@ -228,23 +228,26 @@ __device__ __forceinline__ bool ref_eval(float4 q0, float4 q1, float4 q2, float 
 // Walk list positions [lo, top) back to front, kChunk at a time; body(bits,
 // hi) handles one staged chunk whose entry j is list position hi - 1 - j and
 // whose set bits are the entries that may reach this warp's block.
+// wmask / wbit: the warp's block-mask array and bit (the blend's masks), or null.
 template <typename Body>
 __device__ __forceinline__ void walk_back(const float* records, const uint32_t* point_list, uint32_t num_records,
-                                          uint32_t base, int lo, int top, WarpChunk& wc, const TilePixel& tp,
-                                          Body&& body) {
+                                          const uint8_t* wmask, int wbit, uint32_t base, int lo, int top,
+                                          WarpChunk& wc, const TilePixel& tp, Body&& body) {
   const int len = top - lo;
   const int nc = len > 0 ? (len + kChunk - 1) / kChunk : 0;
   ChunkLoad ld;
   uint32_t reach = 0;
   if (nc > 0) {
-    chunk_load(ld, records, point_list, base + top - 1 - tp.lane, tp.lane < len, num_records);
+    chunk_load(ld, records, point_list, base + top - 1 - tp.lane, tp.lane < len, num_records, wmask, wbit);
     reach = chunk_store(wc, ld, tp.bx, tp.by);
   }
   for (int c = 0; c < nc; ++c) {
     const int hi = top - c * kChunk;
     const int hn = hi - kChunk;
     const bool more = c + 1 < nc;
-    if (more) chunk_load(ld, records, point_list, base + hn - 1 - tp.lane, hn - 1 - tp.lane >= lo, num_records);
+    if (more)
+      chunk_load(ld, records, point_list, base + hn - 1 - tp.lane, hn - 1 - tp.lane >= lo, num_records, wmask,
+                 wbit);
     body(reach, hi);
     if (more) {
       __syncwarp();
@@ -294,6 +297,11 @@ __global__ void __launch_bounds__(kBlendThreads, 2) render_ref_kernel(BackwardAr
   const float pxf = float(p.tp.px), pyf = float(p.tp.py);
   const Target tgt = lane_target(a, 0);
   WarpChunk& wc = s_chunk[threadIdx.x >> 5];
+  // the blend's block masks, when this binning state has them: warps 0-3 read
+  // the top array, 4-7 the bottom one, bit = block within that half
+  const bool use_masks = a.masks_valid != nullptr && *a.masks_valid != 0u;
+  const uint8_t* wmask = use_masks ? ((threadIdx.x >> 5) < 4 ? a.mask_top : a.mask_bottom) : nullptr;
+  const int wbit = int(threadIdx.x >> 5) & 3;
   const float4* s = wc.rec;
   auto full = [&](uint32_t bits, int hi) {
     while (bits != 0u) {
@@ -331,13 +339,13 @@ __global__ void __launch_bounds__(kBlendThreads, 2) render_ref_kernel(BackwardAr
     }
   };
   if (role < 0) {
-    walk_back(a.bwd_record, a.point_list, uint32_t(a.P), p.range.x, 0, p.walk, wc, p.tp, full);
+    walk_back(a.bwd_record, a.point_list, uint32_t(a.P), wmask, wbit, p.range.x, 0, p.walk, wc, p.tp, full);
   } else {
     int lo, hi;
     segment_of<kSplitWays>(p.walk, role, lo, hi);
-    walk_back(a.bwd_record, a.point_list, uint32_t(a.P), p.range.x, hi, p.walk, wc, p.tp, state_only);
+    walk_back(a.bwd_record, a.point_list, uint32_t(a.P), wmask, wbit, p.range.x, hi, p.walk, wc, p.tp, state_only);
     __syncwarp();
-    walk_back(a.bwd_record, a.point_list, uint32_t(a.P), p.range.x, lo, hi, wc, p.tp, full);
+    walk_back(a.bwd_record, a.point_list, uint32_t(a.P), wmask, wbit, p.range.x, lo, hi, wc, p.tp, full);
   }
 }
 
@@ -430,6 +438,11 @@ __global__ void __launch_bounds__(kBlendThreads, 2) render_exact_kernel(Backward
   const float pxf = float(p.tp.px), pyf = float(p.tp.py);
   const Target tgt = lane_target(a, 1);
   WarpChunk& wc = s_chunk[threadIdx.x >> 5];
+  // the blend's block masks, when this binning state has them: warps 0-3 read
+  // the top array, 4-7 the bottom one, bit = block within that half
+  const bool use_masks = a.masks_valid != nullptr && *a.masks_valid != 0u;
+  const uint8_t* wmask = use_masks ? ((threadIdx.x >> 5) < 4 ? a.mask_top : a.mask_bottom) : nullptr;
+  const int wbit = int(threadIdx.x >> 5) & 3;
   const float4* s = wc.rec;
   // the forward's Gaussian values of two entries (same division as the blend)
   auto eval2 = [&](int j0, int j1, float& m0, float& m1, float& g0, float& g1) {
@@ -485,13 +498,13 @@ __global__ void __launch_bounds__(kBlendThreads, 2) render_exact_kernel(Backward
     }
   };
   if (role < 0) {
-    walk_back(a.record, a.point_list, uint32_t(a.P), p.range.x, 0, p.walk, wc, p.tp, full);
+    walk_back(a.record, a.point_list, uint32_t(a.P), wmask, wbit, p.range.x, 0, p.walk, wc, p.tp, full);
   } else {
     int lo, hi;
     segment_of<kSplitWays>(p.walk, role, lo, hi);
-    walk_back(a.record, a.point_list, uint32_t(a.P), p.range.x, hi, p.walk, wc, p.tp, state_only);
+    walk_back(a.record, a.point_list, uint32_t(a.P), wmask, wbit, p.range.x, hi, p.walk, wc, p.tp, state_only);
     __syncwarp();
-    walk_back(a.record, a.point_list, uint32_t(a.P), p.range.x, lo, hi, wc, p.tp, full);
+    walk_back(a.record, a.point_list, uint32_t(a.P), wmask, wbit, p.range.x, lo, hi, wc, p.tp, full);
   }
 }
 

@@ -106,14 +106,19 @@ __global__ void __launch_bounds__(32 * kBlendWarps, 16 / kBlendWarps) blend_kern
       stage_load(st[r], a.record, a.point_list, range.x + e, e < n, a.num_records);
     }
   };
-  auto store = [&](int buf) {
+  // block masks for the backward: the upper half's CTA (or the whole tile's)
+  // writes the top array, the lower half's the bottom one
+  uint8_t* lo_dst = a.mask_top == nullptr ? nullptr : (part == 0 ? a.mask_top : a.mask_bottom) + range.x;
+  uint8_t* hi_dst = a.mask_top == nullptr || kBlendParts != 1 ? nullptr : a.mask_bottom + range.x;
+  auto store = [&](int buf, int base) {
 #pragma unroll
     for (int r = 0; r < kStagePer; ++r)
-      stage_store(sm, buf, st[r], r * kBlendCta + int(threadIdx.x), tp.X0, tp.Y0, first_block);
+      stage_store(sm, buf, st[r], r * kBlendCta + int(threadIdx.x), tp.X0, tp.Y0, first_block,
+                  lo_dst ? lo_dst + base : nullptr, hi_dst ? hi_dst + base : nullptr);
   };
   if (nb > 0) {
     load(0);
-    store(0);
+    store(0, 0);
   }
   for (int b = 0; b < nb; ++b) {
     const int cur = b & 1;
@@ -161,7 +166,7 @@ __global__ void __launch_bounds__(32 * kBlendWarps, 16 / kBlendWarps) blend_kern
         if (__all_sync(0xffffffffu, pix.done)) break;
       }
     }
-    if (b + 1 < nb) store(cur ^ 1);
+    if (b + 1 < nb) store(cur ^ 1, next_base);
   }
   if (inside) {
     const size_t q = size_t(tp.py) * W + tp.px;

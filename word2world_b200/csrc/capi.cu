@@ -92,6 +92,7 @@ KeyPlan plan_keys(const w2w_geometry_info& info, int W, int H) {
 __global__ void write_bin_header(BinHeader* h, KeyPlan k, uint32_t R, uint32_t passes, const uint32_t* fold0,
                                  const uint32_t* fold1) {
   h->error = (fold0 != nullptr ? *fold0 : 0u) | (fold1 != nullptr ? *fold1 : 0u);
+  h->masks_valid = 1u;  // the blend that follows writes the block masks
   h->key64 = k.key64;
   h->depth_bits = k.depth_bits;
   h->depth_prefix = k.prefix;
@@ -480,6 +481,11 @@ int w2w_forward_render(const w2w_settings* s, const void* geom_state, const w2w_
   b.point_list = point_list;
   b.record = R > 0 ? at<float>(geom_state, GeomLayout(s->P).record) : nullptr;
   b.num_records = uint32_t(s->P);
+  if (R > 0) {
+    const BinLayout BL(R, T);
+    b.mask_top = at<uint8_t>(binning_state, BL.masks);
+    b.mask_bottom = b.mask_top + R;
+  }
   b.bg = s->background;
   b.out_color = out_color; b.out_depth = out_depth; b.out_alpha = out_alpha;
   b.n_contrib = at<uint32_t>(image_state, IL.n_contrib);
@@ -541,6 +547,12 @@ static int backward_impl(const w2w_settings* s, const float* means3D, const floa
   a.bwd_record = at<float>(geom_state, GL.bwd_record);
   a.ranges = at<uint2>(image_state, IL.ranges);
   a.point_list = R > 0 ? at<uint32_t>(binning_state, BinLayout(R, num_tiles(W, H)).valsA) : nullptr;
+  if (R > 0) {
+    const BinLayout BL(R, num_tiles(W, H));
+    a.mask_top = at<uint8_t>(binning_state, BL.masks);
+    a.mask_bottom = a.mask_top + R;
+    a.masks_valid = &at<BinHeader>(binning_state, BL.header)->masks_valid;
+  }
   a.n_contrib = at<uint32_t>(image_state, IL.n_contrib);
   a.tile_max = at<uint32_t>(image_state, IL.tile_max);
   a.order_bwd = at<uint32_t>(image_state, IL.order_bwd);
@@ -1120,6 +1132,11 @@ int w2w_batch_forward_render(const w2w_batch_item* items, int n, const void* geo
   b.point_list = point_list;
   b.record = R > 0 ? at<float>(geom_state, GeomLayout(E).record) : nullptr;
   b.num_records = uint32_t(E);
+  if (R > 0) {
+    const BinLayout BL(R, T);
+    b.mask_top = at<uint8_t>(binning_state, BL.masks);
+    b.mask_bottom = b.mask_top + R;
+  }
   b.bg = nullptr;
   b.out_color = out_color; b.out_depth = out_depth; b.out_alpha = out_alpha;
   b.n_contrib = at<uint32_t>(image_state, IL.n_contrib);
@@ -1168,6 +1185,12 @@ int w2w_batch_backward(const w2w_batch_item* items, int n, const void* geom_stat
   a.bwd_record = at<float>(geom_state, GL.bwd_record);
   a.ranges = at<uint2>(image_state, IL.ranges);
   a.point_list = R > 0 ? at<uint32_t>(binning_state, BinLayout(R, T).valsA) : nullptr;
+  if (R > 0) {
+    const BinLayout BL(R, T);
+    a.mask_top = at<uint8_t>(binning_state, BL.masks);
+    a.mask_bottom = a.mask_top + R;
+    a.masks_valid = &at<BinHeader>(binning_state, BL.header)->masks_valid;
+  }
   a.n_contrib = at<uint32_t>(image_state, IL.n_contrib);
   a.tile_max = at<uint32_t>(image_state, IL.tile_max);
   a.order_bwd = at<uint32_t>(image_state, IL.order_bwd);

@@ -397,14 +397,15 @@ struct BinHeader {
   uint32_t tile_bits;
   uint32_t passes;         // 8-bit digit passes
   uint32_t num_rendered;
-  uint32_t pad[9];
+  uint32_t masks_valid;    // 1: the blend wrote the block masks (BinLayout::masks) for the backward
+  uint32_t pad[8];
   uint32_t tile_counter[8];  // per-pass tile acquisition counters (onesweep)
 };
 
 constexpr int kSortThreads = 256;
 
 struct BinLayout {
-  size_t header, keysA, keysB, valsA, valsB, hist, status, tile_hist, bin_counts, warp_start, total;
+  size_t header, keysA, keysB, valsA, valsB, hist, status, tile_hist, bin_counts, warp_start, masks, total;
   __host__ __device__ BinLayout(long long R, int num_tiles) {
     size_t o = 0;
     auto take = [&](size_t bytes) { size_t a = align256(o); o = a + bytes; return a; };
@@ -425,6 +426,8 @@ struct BinLayout {
     const size_t chunks = num_tiles > 0 && num_tiles <= kMaxBinTiles ? (r + kBinChunk - 1) / kBinChunk : 0;
     bin_counts = take(chunks * size_t(num_tiles > 0 ? num_tiles : 0) * 4);
     warp_start = take(chunks ? ((r + kBinShare - 1) / kBinShare + 1) * 4 : 0);
+    // the blend's block masks per list position: the tile's upper blocks, then its lower blocks
+    masks = take(2 * r);
     total = align256(o);
   }
 };

@@ -152,6 +152,8 @@ struct BlendArgs {
   const uint32_t* point_list;
   const float* record;
   uint32_t num_records;  // records (Gaussians, or batch elements); larger ids in the list are skipped
+  uint8_t* mask_top;     // block masks for the backward passes (tile_walk.cuh BlockMasks), or null
+  uint8_t* mask_bottom;
   const float* bg;
   float* out_color;
   float* out_depth;
@@ -191,6 +193,9 @@ struct BackwardArgs {
   const uint32_t* n_contrib;
   const uint32_t* tile_max;
   const uint32_t* order_bwd;  // tile order by largest contributor count (written by the blend)
+  const uint8_t* mask_top;    // the blend's block masks (tile_walk.cuh BlockMasks); null: test each entry
+  const uint8_t* mask_bottom;
+  const uint32_t* masks_valid;
   int split;               // heaviest tiles whose walks are split over several CTAs (set at launch)
   const float* T_final;
   const float* out_alpha;

@@ -61,17 +61,34 @@ struct ChunkLoad {
   float4 r0, r1, r2, r3;
   uint32_t id;
   bool has;
+  bool masked;  // `has` already means "may reach the warp's block" (from the blend's block masks)
+};
+
+// Block masks the forward blend leaves for the backward passes: per list
+// position, 4 bits for the tile's upper four 8x4 blocks (array `top`) and 4
+// for its lower four (`bottom`), bit b set when the entry may reach block b
+// (block_mask).  `valid` points at the binning header's flag; a state the
+// blend did not write (a replayed list) has it clear, and the walk tests
+// every entry itself.
+struct BlockMasks {
+  const uint8_t* top;
+  const uint8_t* bottom;
+  const uint32_t* valid;
 };
 
 // Gather entry `pos` of the point list (when `has`).  Records are four float4s;
 // r2.w and r3 hold the culling parameters (hy; beta, gamma, eps, vr).  An id
 // of num_records or more (a list left inconsistent by a sort whose bounded
-// wait ran out, which its error word reports) is skipped, never read.
+// wait ran out, which its error word reports) is skipped, never read.  With
+// `mask` (the warp's mask array, or null) only entries whose bit `bit` is set
+// are gathered.
 __device__ __forceinline__ void chunk_load(ChunkLoad& st, const float* record, const uint32_t* point_list, size_t pos,
-                                           bool has, uint32_t num_records) {
+                                           bool has, uint32_t num_records, const uint8_t* mask = nullptr,
+                                           int bit = 0) {
   st.has = false;
+  st.masked = mask != nullptr;
+  if (has && mask != nullptr) has = (mask[pos] >> bit) & 1u;
   if (has) {
-    const float4* rec = reinterpret_cast<const float4*>(record);
     st.id = point_list[pos];
     st.has = st.id < num_records;
   }
@@ -97,7 +114,7 @@ __device__ __forceinline__ uint32_t chunk_store(WarpChunk& c, const ChunkLoad& s
     s[1] = st.r1;
     s[2] = st.r2;
     c.id[lane] = st.id;
-    reach = block_test(st.r0.x, st.r0.y, st.r2.w, st.r3.x, st.r3.y, st.r3.z, st.r3.w, bx, by);
+    reach = st.masked || block_test(st.r0.x, st.r0.y, st.r2.w, st.r3.x, st.r3.y, st.r3.z, st.r3.w, bx, by);
   }
   __syncwarp();
   return __ballot_sync(0xffffffffu, reach);
@@ -180,9 +197,12 @@ __device__ __forceinline__ void stage_load(Staged& st, const float* record, cons
 // the block masks of the CTA's kW blocks (the tile's blocks first_block ..
 // first_block + kW - 1).  Every thread of a warp must call this for the same
 // chunk (the ballots are full-warp).
+// The masks also go to global memory for the backward passes (BlockMasks):
+// bits 0-3 to lo_dst[j], bits 4-7 (eight-warp CTAs) to hi_dst[j], where the
+// callers offset the arrays to the batch's first list position.
 template <int kW>
 __device__ __forceinline__ void stage_store(TileWalkShared<kW>& sm, int buf, const Staged& st, int j, int X0, int Y0,
-                                            int first_block) {
+                                            int first_block, uint8_t* lo_dst = nullptr, uint8_t* hi_dst = nullptr) {
   const int lane = j & 31, chunk = j >> 5;
   uint32_t mask = 0;
   if (st.has) {
@@ -194,6 +214,8 @@ __device__ __forceinline__ void stage_store(TileWalkShared<kW>& sm, int buf, con
     // the CTA's blocks are kW / 2 rows of two, starting at row group first_block / 2
     mask = block_mask<kW / 2>(st.r0.x, st.r0.y, st.r2.w, st.r3.x, st.r3.y, st.r3.z, st.r3.w, X0,
                               Y0 + kBlockH * (first_block / 2));
+    if (lo_dst != nullptr) lo_dst[j] = uint8_t(mask & 15u);
+    if (hi_dst != nullptr) hi_dst[j] = uint8_t(mask >> 4);
   }
   uint32_t mine = 0;
 #pragma unroll
