@@ -78,5 +78,5 @@ def test_every_knob_setting_gives_the_same_results(restore):
                 for k in ("color", "alpha", "depth_img", "n_contrib"):
                     assert parity.bit_mismatch(f[k], base[0][k]) == 0, (warps, split, ways, k)
                 for k in parity.GRAD_NAMES:
-                    c = parity.grad_check(b[k], base[1][k], row_rtol=1e-3)
+                    c = parity.grad_check(b[k], base[1][k], row_rtol=parity.SAME_IMPL_ROW_RTOL)
                     assert c["norm_rel"] <= 1e-5, (warps, split, ways, k, c)

@@ -74,7 +74,7 @@ def test_batch_matches_single_views(grad_mode, reuse):
             c.tanfovx, c.tanfovy, grads[v], zero, zero, sc.shs, sc.sh_degree, t(c.campos), geom, R, binb, img, alpha,
             False, 0 if grad_mode == "reference" else 1)
         for name, a, b in zip(parity.GRAD_NAMES, g["per_item"][v], gp):
-            chk = parity.grad_check(a.cpu().numpy(), b.cpu().numpy())
+            chk = parity.grad_check(a.cpu().numpy(), b.cpu().numpy(), row_rtol=parity.SAME_IMPL_ROW_RTOL)
             assert chk["norm_rel"] <= 1e-5, (v, name, chk)
             assert chk["n_bad"] == 0, (v, name, chk)
 

@@ -6,7 +6,7 @@ count, the sorted 64-bit keys, the sorted Gaussian ids and the per-tile
 ranges.  Contributor counts: exact except at pixels whose blend decisions
 lie within 1e-5 (relative) of a threshold, where the device and C-library
 exp may round differently.  Images and gradients: |a-b| <= 1e-5 + 1e-4|b|
-(gradients with a per-Gaussian scale term, see parity.grad_check) and
+(gradients with the fp32 accumulation-order term of parity.grad_check) and
 norm-relative error <= 1e-4 per result.
 """
 import numpy as np
