@@ -374,13 +374,18 @@ def run_ours(a):
     hbm, peak_kind = peaks()
     ap = arithmetic_peaks(device)
 
+    # kernels one invocation of a stage launches (a stage runs once per view)
+    kernels_per_call = {"sort_histogram": 2, "binning": 4,
+                        "depth_sort": 3 + max(1, plans[0].get("depth_passes", 2))}
+
     def launch_ms(k):
-        # a stage's launches as timed in the single-stream timed steps when it
-        # was recorded there, else from the untimed stage steps
+        # one invocation of a stage (per view), as timed in the single-stream
+        # timed steps when it was recorded there, else in the untimed stage steps
         src = timed_stages.get(k, (0, 0))
+        per = kernels_per_call.get(k, 1)
         if src[1]:
-            return src[0] / src[1], "single-stream timed steps"
-        return (stage_ms[k] / stage_n[k], "untimed stage steps") if stage_n.get(k) else (None, None)
+            return src[0] / src[1] * per, "single-stream timed steps"
+        return (stage_ms[k] / stage_n[k] * per, "untimed stage steps") if stage_n.get(k) else (None, None)
 
     def fp32_line(k):
         ms, where = launch_ms(k)
@@ -408,8 +413,6 @@ def run_ours(a):
     roofline_hbm = None
     if dom:
         per_launch_ms, where = launch_ms(dom)
-        if dom == "sort_histogram" and where == "untimed stage steps":
-            per_launch_ms *= 2  # the stage brackets the histogram and the offsets kernels
         ach = alg_bytes[dom] / (per_launch_ms / 1e3) / 1e9
         roofline_hbm = {"kernel": dom, "bound": "hbm", "achieved": round(ach, 1), "peak": hbm, "unit": "GB/s",
                         "frac": round(ach / hbm, 4), "peak_source": peak_kind,

@@ -119,10 +119,12 @@ def _scene(P=8192, S=192):
 
 
 def test_render_sort_wait_is_reported_by_the_deferred_check():
+    """The render's sort (the depth sort of its 8192 Gaussians: two onesweep
+    tiles per pass) with its first tile unpublished."""
     arrays, cam = _scene()
     clean = gh.forward(arrays, cam)
-    assert clean["num_rendered"] > 3 * 6144  # several sort tiles
-    with hooked(STAGE_SORT, 1):
+    assert clean["num_rendered"] > 0
+    with hooked(STAGE_SORT, 0):
         gh.forward(arrays, cam)  # returns; its point list is invalid
         with pytest.raises(RuntimeError, match="timed out"):
             _C.check_device_errors()

@@ -180,6 +180,18 @@ class BatchRenderer:
         self.device = torch.device(device) if device is not None else torch.device("cuda", torch.cuda.current_device())
         self.ws = _Workspace(self.device) if reuse_buffers else None
 
+    def _pinned_tables(self, nbytes: int) -> torch.Tensor:
+        """Grow-only pinned host buffer for the group tables; before it is
+        refilled, the previous call's copy out of it has finished."""
+        ev = getattr(self, "_tables_copied", None)
+        if ev is not None:
+            ev.synchronize()
+        buf = getattr(self, "_pinned", None)
+        if buf is None or buf.numel() < nbytes:
+            buf = torch.empty(max(2 * int(nbytes), 4096), dtype=torch.uint8).pin_memory()
+            self._pinned = buf
+        return buf
+
     def _u8(self, role, nbytes):
         if self.ws is not None:
             return self.ws.take(role, nbytes)
@@ -344,7 +356,14 @@ class BatchRenderer:
         tab[G + 1:2 * (G + 1)] = ptr
         tab[2 * (G + 1):] = items
         tables = self._u8("group_tables", tab.nbytes)
-        tables.copy_(torch.from_numpy(tab.view(np.uint8)))
+        # from pinned memory without blocking the host: a copy from pageable
+        # memory would wait for the backward kernels queued before it, so a
+        # serving loop could not launch its next batch meanwhile
+        staged = self._pinned_tables(tab.nbytes)
+        staged[:tab.nbytes].copy_(torch.from_numpy(tab.view(np.uint8)))
+        tables.copy_(staged[:tab.nbytes], non_blocking=True)
+        self._tables_copied = torch.cuda.Event()
+        self._tables_copied.record(torch.cuda.current_stream(dev))
         out = {"groups": order}
         for name, t in (("means3D", g_m3), ("opacities", g_op), ("scales", g_sc), ("rotations", g_rot),
                         ("shs", g_sh)):

@@ -30,6 +30,8 @@
 // Positions are generated, never stored: each warp expands 32 Gaussians at a
 // time (a shuffle binary search finds each lane's owner), so the sequence is
 // read as P-sized data twice instead of R-sized keys once per sort pass.
+#include <type_traits>
+
 #include "common.cuh"
 #include "kernels.h"
 
@@ -94,6 +96,7 @@ __device__ __forceinline__ void walk_positions(const BinArgs& a, uint32_t pa, ui
   while (pos < pb && j < uint32_t(a.P)) {
     const uint32_t jj = j + uint32_t(lane);
     uint32_t cnt = 0, k0 = 0, xy = 0, w = 1, dlow = 0, g = 0;
+    float inv_w = 1.0f;
     if (jj < uint32_t(a.P)) {
       const uint32_t lo = max(a.dprefix[jj], pos), hi = min(a.dprefix[jj + 1], pb);
       if (hi > lo) {
@@ -103,6 +106,7 @@ __device__ __forceinline__ void walk_positions(const BinArgs& a, uint32_t pa, ui
         k0 = o.first_k + (lo - a.dprefix[jj]);
         xy = o.x0 | (o.y0 << 16);
         w = o.w;
+        inv_w = __frcp_rn(float(w));
         const uint32_t db = __float_as_uint(a.depth[g]);
         dlow = a.depth_bits >= 32 ? db : (db & ((1u << a.depth_bits) - 1u));
       }
@@ -128,11 +132,24 @@ __device__ __forceinline__ void walk_positions(const BinArgs& a, uint32_t pa, ui
       const uint32_t ok0 = __shfl_sync(0xffffffffu, k0, o);
       const uint32_t oxy = __shfl_sync(0xffffffffu, xy, o);
       const uint32_t ow = __shfl_sync(0xffffffffu, w, o);
+      const float oinv = __shfl_sync(0xffffffffu, inv_w, o);
       const uint32_t odl = __shfl_sync(0xffffffffu, dlow, o);
       const uint32_t og = __shfl_sync(0xffffffffu, g, o);
       const bool valid = e < total;
       const uint32_t k = ok0 + (e - oex);
-      const uint32_t ty = (oxy >> 16) + k / ow, tx = (oxy & 0xffffu) + k % ow;
+      // k / ow without an integer division: k < 2^24 is exact in float, the
+      // product's rounding moves the quotient by at most one, and the
+      // remainder test corrects it
+      uint32_t q = __float2uint_rz(__uint2float_rn(k) * oinv);
+      int r = int(k) - int(q * ow);
+      if (r < 0) {
+        --q;
+        r += int(ow);
+      } else if (r >= int(ow)) {
+        ++q;
+        r -= int(ow);
+      }
+      const uint32_t ty = (oxy >> 16) + q, tx = (oxy & 0xffffu) + uint32_t(r);
       f(valid, pos + e, og, ty * uint32_t(a.gw) + tx, odl);
     }
     pos += total;
@@ -216,10 +233,40 @@ __global__ void __launch_bounds__(1024) bin_offsets_kernel(BinArgs a, int chunks
   }
 }
 
+// Shared memory of the scatter kernel: per-warp tile counters [kBinWarps][T],
+// the global index of each tile's chunk-local slot 0 [T], then the chunk's
+// keys and ids reordered by tile [kBinChunk].
+template <typename Key>
+struct ScatterSmem {
+  size_t wcnt, gofs, keys, vals, total;
+  __host__ __device__ explicit ScatterSmem(int T) {
+    size_t o = 0;
+    auto take = [&](size_t bytes) { const size_t at = (o + 15) & ~size_t(15); o = at + bytes; return at; };
+    wcnt = take(size_t(kBinWarps) * size_t(T) * 4);
+    gofs = take(size_t(T) * 4);
+    keys = take(size_t(kBinChunk) * sizeof(Key));
+    vals = take(size_t(kBinChunk) * 4);
+    total = (o + 15) & ~size_t(15);
+  }
+};
+
+// The chunk's instances, placed stably by tile: (1) walk counting per warp
+// and tile; (2) each tile's chunk-local slots (tiles in order, warps in order
+// within a tile) and the global index of its slot 0; (3) walk again, ranking
+// equal tiles within 32 positions, and put each instance's key and id in its
+// chunk-local slot; (4) write the chunk out slot by slot, so that each
+// tile's run is stored by consecutive threads.
 template <bool kKey64>
 __global__ void __launch_bounds__(kBinThreads) bin_scatter_kernel(BinArgs a) {
-  extern __shared__ uint32_t s_wcnt[];  // [kBinWarps][T]
+  using Key = typename std::conditional<kKey64, uint64_t, uint32_t>::type;
+  extern __shared__ __align__(16) unsigned char s_raw[];
   const int T = a.T;
+  const ScatterSmem<Key> L(T);
+  uint32_t* s_wcnt = reinterpret_cast<uint32_t*>(s_raw + L.wcnt);
+  uint32_t* s_gofs = reinterpret_cast<uint32_t*>(s_raw + L.gofs);
+  Key* s_key = reinterpret_cast<Key*>(s_raw + L.keys);
+  uint32_t* s_val = reinterpret_cast<uint32_t*>(s_raw + L.vals);
+  __shared__ uint32_t s_part[kBinThreads];
   const int warp = int(threadIdx.x >> 5), lane = int(threadIdx.x & 31);
   for (int i = threadIdx.x; i < kBinWarps * T; i += kBinThreads) s_wcnt[i] = 0u;
   __syncthreads();
@@ -230,18 +277,56 @@ __global__ void __launch_bounds__(kBinThreads) bin_scatter_kernel(BinArgs a) {
     if (valid && tile < uint32_t(T)) atomicAdd(&mine[tile], 1u);
   });
   __syncthreads();
-  // each warp's first slot per tile: the chunk's base plus earlier warps' counts
-  const uint32_t* base = a.counts + size_t(blockIdx.x) * size_t(T);
-  for (int t = threadIdx.x; t < T; t += kBinThreads) {
-    uint32_t run = base[t];
+  // (2) each thread a contiguous run of tiles: per-warp exclusive counts
+  // within each tile, the run's total, then a block scan of the runs
+  const int per = (T + kBinThreads - 1) / kBinThreads;
+  const int t0 = int(threadIdx.x) * per, t1 = min(T, t0 + per);
+  uint32_t run_total = 0;
+  for (int t = t0; t < t1; ++t) {
+    uint32_t r = 0;
 #pragma unroll
     for (int w = 0; w < kBinWarps; ++w) {
       const uint32_t x = s_wcnt[w * T + t];
-      s_wcnt[w * T + t] = run;
-      run += x;
+      s_wcnt[w * T + t] = r;
+      r += x;
+    }
+    s_gofs[t] = r;  // the tile's count in this chunk, for now
+    run_total += r;
+  }
+  s_part[threadIdx.x] = run_total;
+  __syncthreads();
+  if (warp == 0) {  // exclusive scan of the 256 run totals, 8 per lane
+    uint32_t v[kBinThreads / 32], sum = 0;
+#pragma unroll
+    for (int i = 0; i < kBinThreads / 32; ++i) {
+      v[i] = s_part[lane * (kBinThreads / 32) + i];
+      sum += v[i];
+    }
+    uint32_t incl = sum;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+      const uint32_t o = __shfl_up_sync(0xffffffffu, incl, d);
+      if (lane >= d) incl += o;
+    }
+    uint32_t ex = incl - sum;
+#pragma unroll
+    for (int i = 0; i < kBinThreads / 32; ++i) {
+      s_part[lane * (kBinThreads / 32) + i] = ex;
+      ex += v[i];
     }
   }
   __syncthreads();
+  const uint32_t* base = a.counts + size_t(blockIdx.x) * size_t(T);
+  uint32_t local = s_part[threadIdx.x];
+  for (int t = t0; t < t1; ++t) {
+    const uint32_t cnt = s_gofs[t];
+#pragma unroll
+    for (int w = 0; w < kBinWarps; ++w) s_wcnt[w * T + t] += local;
+    s_gofs[t] = base[t] - local;  // global index of chunk-local slot 0 of tile t (mod 2^32)
+    local += cnt;
+  }
+  __syncthreads();
+  // (3) rank and place in shared memory
   const uint32_t lt = (1u << lane) - 1u;
   const uint32_t db = a.depth_bits;
   walk_positions(a, pa, pb, j, [&](bool valid, uint32_t, uint32_t g, uint32_t tile, uint32_t dlow) {
@@ -252,21 +337,31 @@ __global__ void __launch_bounds__(kBinThreads) bin_scatter_kernel(BinArgs a) {
     if (ok) before = mine[tile];
     __syncwarp();
     if (ok) {
-      const uint32_t out = before + __popc(peers & lt);
+      const uint32_t slot = before + __popc(peers & lt);
       if (lane == __ffs(peers) - 1) mine[tile] = before + __popc(peers);
-      if (out < a.R) {
-        if constexpr (kKey64) {
-          reinterpret_cast<uint64_t*>(a.keys)[out] = (uint64_t(tile) << db) | dlow;
-        } else {
-          reinterpret_cast<uint32_t*>(a.keys)[out] = (db >= 32 ? 0u : (tile << db)) | dlow;
-        }
-        a.vals[out] = g;
-      } else {
-        atomicOr(a.error, kErrRange);
+      if (slot < uint32_t(kBinChunk)) {
+        if constexpr (kKey64) s_key[slot] = (uint64_t(tile) << db) | dlow;
+        else s_key[slot] = (db >= 32 ? 0u : (tile << db)) | dlow;
+        s_val[slot] = g;
       }
     }
     __syncwarp();
   });
+  __syncthreads();
+  // (4) chunk-local slot i of tile t goes to s_gofs[t] + i
+  const uint32_t c0 = blockIdx.x * uint32_t(kBinChunk);
+  const int n = int(min(uint32_t(kBinChunk), a.R - c0));
+  for (int i = threadIdx.x; i < n; i += kBinThreads) {
+    const Key key = s_key[i];
+    const uint32_t tile = kKey64 ? uint32_t(uint64_t(key) >> db) : (db >= 32 ? 0u : uint32_t(key) >> db);
+    const uint32_t out = tile < uint32_t(T) ? s_gofs[tile] + uint32_t(i) : 0xffffffffu;
+    if (out < a.R) {
+      reinterpret_cast<Key*>(a.keys)[out] = key;
+      a.vals[out] = s_val[i];
+    } else {
+      atomicOr(a.error, kErrRange);
+    }
+  }
 }
 
 __global__ void iota_kernel(uint32_t* out, int n) {
@@ -276,7 +371,9 @@ __global__ void iota_kernel(uint32_t* out, int n) {
 
 }  // namespace
 
-size_t bin_smem_bytes(int tiles) { return size_t(kBinWarps) * size_t(tiles) * 4; }
+size_t bin_smem_bytes(int tiles, int key64) {
+  return key64 ? ScatterSmem<uint64_t>(tiles).total : ScatterSmem<uint32_t>(tiles).total;
+}
 
 void launch_iota(uint32_t* out, int n, cudaStream_t stream) {
   if (n > 0) iota_kernel<<<(n + 255) / 256, 256, 0, stream>>>(out, n);
@@ -291,13 +388,13 @@ void launch_binning(const BinArgs& a, cudaStream_t stream) {
   if (a.R == 0 || a.P <= 0) return;
   const int chunks = int((a.R + kBinChunk - 1) / kBinChunk);
   const uint32_t shares = (a.R + kWarpShare - 1) / kWarpShare;
-  const size_t scatter_smem = bin_smem_bytes(a.T);
+  const size_t scatter_smem = bin_smem_bytes(a.T, a.key64);
   // the shared-memory opt-in, for the largest tile count, once per device
   static bool opted[64] = {false};
   int dev = 0;
   cudaGetDevice(&dev);
   if (dev < 0 || dev >= 64 || !opted[dev]) {
-    const int most = int(bin_smem_bytes(kMaxBinTiles));
+    const int most = int(bin_smem_bytes(kMaxBinTiles, 1));
     cudaFuncSetAttribute(bin_scatter_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, most);
     cudaFuncSetAttribute(bin_scatter_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, most);
     if (dev >= 0 && dev < 64) opted[dev] = true;

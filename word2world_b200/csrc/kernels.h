@@ -251,7 +251,7 @@ struct BinArgs {
   uint32_t* vals;              // sorted Gaussian ids (the point list)
   uint32_t* error;
 };
-size_t bin_smem_bytes(int tiles);
+size_t bin_smem_bytes(int tiles, int key64);
 void launch_iota(uint32_t* out, int n, cudaStream_t stream);
 void launch_owned_counts(const BinArgs& a, uint32_t* count, cudaStream_t stream);
 void launch_binning(const BinArgs& a, cudaStream_t stream);
