@@ -78,7 +78,7 @@ typedef struct {
     uint32_t depth_min_bits;  /* range of the depth bits of Gaussians that emit keys */
     uint32_t depth_max_bits;
     uint32_t error;           /* device error bits (0 = none) */
-    uint32_t reserved;
+    uint32_t reserved;        /* bit 0: the geometry phase prepared the depth-ordered binning */
 } w2w_geometry_info;
 
 int w2w_version(void);
@@ -117,10 +117,11 @@ size_t w2w_binning_offset(long long num_rendered, int width, int height, const c
  * gaussianForwardPass.cu calcColour and the scan of gaussianRasterizer.cu:233,
  * i.e. gaussianForwardPass, gaussianRasterizer.cu:118-237): one fused kernel.  Writes radii and
  * the geometry state, then reads the instance count and depth-bit range back
- * into *info (synchronising `stream` once).  For images of at most 4096
- * tiles it then enqueues the per-Gaussian half of the binning (the Gaussians
- * sorted stably by depth bits, and the prefix of their owned instance counts
- * in that order) into the geometry state. */
+ * into *info (synchronising `stream` once).  When the "binning" tuning knob
+ * selects the depth-ordered binning and the image has at most 4096 tiles, it
+ * then enqueues the per-Gaussian half of that binning (the Gaussians sorted
+ * stably by depth bits, and the prefix of their owned instance counts in that
+ * order) into the geometry state and sets bit 0 of info->reserved. */
 int w2w_forward_geometry(const w2w_settings* s, const float* means3D, const float* scales,
                          const float* rotations, const float* opacities, const float* shs,
                          int* radii, void* geom_state, w2w_geometry_info* info, w2w_stream_t stream);
@@ -128,11 +129,11 @@ int w2w_forward_geometry(const w2w_settings* s, const float* means3D, const floa
 /* Phase 2 (replaces prepareAndSort, prepareSort.cu:362-435, gaussianTiles,
  * gaussianTiles.cu:6-33, and pixelGaussiansFull, pixelGaussiansFull.cu:99-122):
  * the sorted instance list and tile ranges, then blending.  binning_state
- * must be w2w_binning_state_bytes(info->num_rendered, W, H) long.  Images of
- * at most 4096 tiles: every instance is placed once, by tile, walking the
+ * must be w2w_binning_state_bytes(info->num_rendered, W, H) long.  With bit
+ * 0 of info->reserved set, every instance is placed once, by tile, walking the
  * Gaussians in the depth order phase 1 prepared (a counting sort whose keys
- * are generated, not stored); larger images: key emission and an onesweep
- * radix sort.  Either way the list is the reference's: sorted by tile, then
+ * are generated, not stored); otherwise key emission and an onesweep radix
+ * sort.  Either way the list is the reference's: sorted by tile, then
  * depth bits, ties in slot order.  The sorted keys are kept in the binning
  * state, packed: only the bits in which keys can differ (tile bits and the
  * low depth bits below the depths' common prefix), in 32 bits when they fit;
@@ -371,8 +372,12 @@ int w2w_throughput_probe(int kind, long long iters, int blocks, float* out, long
  * (4: two 4-warp CTAs per tile, 8: one 8-warp CTA; default 4), 1
  * "backward_split" (the per-pixel backward splits its heaviest tiles, up to
  * this many quarters of the SM count, across CTAs; 0..16, default 4), 2
- * "backward_ways" (segments per split tile, 2 or 3; default 2).  Results do
- * not depend on them beyond the order of float atomic additions.
+ * "backward_ways" (segments per split tile, 2 or 3; default 2), 3 "binning"
+ * (how a single-view call of at most 4096 tiles builds its sorted list: 0
+ * key emission and the radix sort, 1 binning from the depth-ordered
+ * Gaussians; default 0; w2w_forward_geometry records the path taken in
+ * w2w_geometry_info.reserved, bit 0, and w2w_forward_render follows it).
+ * Results do not depend on them beyond the order of float atomic additions.
  * w2w_tune_set returns the previous value, or -1 (and changes nothing) for an
  * unknown knob or value. */
 int w2w_tune_count(void);

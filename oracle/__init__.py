@@ -298,11 +298,13 @@ def backward(fwd: dict, dL_dcolor, dL_ddepth=None, dL_dalpha=None, mode: str = "
     if mode == "reference":
         dm2 = np.zeros((P, 3)); dcon = np.zeros((P, 4)); dop = np.zeros(P); dcol = np.zeros((P, 3)); ddep = np.zeros(P)
         abs_sum = np.zeros((P, 10)) if error_bounds else None
+        bmargin = np.zeros(H * W) if error_bounds else None
         getattr(L, "orc_backward_render" + sfx)(
             ctypes.byref(cfg), ctypes.c_int(P), _p(fwd["ranges"]), _p(pl), _p(fwd["means2D"]), _p(fwd["conic_opac"]),
             _p(fwd["rgb"]), _p(fwd["depth"]), _p(np.ascontiguousarray(fwd["alpha"].reshape(-1))),
             _p(np.ascontiguousarray(fwd["n_contrib"].reshape(-1))), _p(dLc), _p(dLd), _p(dLa),
-            _p(dm2), _p(dcon), _p(dop), _p(dcol), _p(ddep), _p(abs_sum) if error_bounds else None)
+            _p(dm2), _p(dcon), _p(dop), _p(dcol), _p(ddep), _p(abs_sum) if error_bounds else None,
+            _p(bmargin) if error_bounds else None)
         tfx = s.tan_fovx if tan_fovx is None else tan_fovx
         tfy = s.tan_fovy if tan_fovy is None else tan_fovy
         h_x = np.float32(W) / (np.float32(2.0) * np.float32(tfx))
@@ -327,6 +329,8 @@ def backward(fwd: dict, dL_dcolor, dL_ddepth=None, dL_dalpha=None, mode: str = "
         g["dL_ddepths"] = ddepR
         if not error_bounds:
             return g
+        # per pixel: how close its backward's skip decisions came to a threshold
+        g["backward_margin"] = bmargin.reshape(H, W)
         # sums of |per-pair contribution|: the scale of fp32 accumulation-order error
         g["abs_dL_dcolors"] = abs_sum[:, 0:3]
         g["abs_dL_dmeans2D"] = np.concatenate([abs_sum[:, 4:6], np.zeros((P, 1))], axis=1)

@@ -618,7 +618,7 @@ typedef struct {
     const REAL* means2D; const REAL* conic_opac; const REAL* rgb; const REAL* depth; const REAL* out_alpha;
     const uint32_t* n_contrib; const float* dL_dpix; const float* dL_ddepth; const float* dL_dalpha;
     double* dmean2D; double* dconic; double* dopac; double* dcolor; double* ddepth; double* abs_sum;
-    double* priv; size_t stride;
+    double* priv; size_t stride; double* margin;
 } SFX(orc_backward_render_ctx);
 
 /* Rows [lo_, hi_) of the per-pixel backward.  With several threads each
@@ -661,6 +661,7 @@ static void SFX(orc_backward_render_part)(void* vc_, long long lo_, long long hi
             REAL bgdot = 0;
             for (int c = 0; c < 3; ++c) bgdot = bgdot + bg[c] * dLp[c];
             REAL qx = (REAL)px, qy = (REAL)py;
+            double mg = 1e30;  /* smallest relative distance of a skip decision from its threshold */
             for (uint32_t jj = e; jj > s; --jj) {
                 uint32_t j = jj - 1;
                 contributor--;
@@ -669,10 +670,15 @@ static void SFX(orc_backward_render_part)(void* vc_, long long lo_, long long hi
                 REAL dx = means2D[2 * id] - qx, dy = means2D[2 * id + 1] - qy;
                 const REAL* co = conic_opac + 4 * id;
                 REAL power = (REAL)-0.5 * (co[0] * dx * dx + co[2] * dy * dy) - co[1] * dx * dy;
+                if (fabs((double)power) < 1e-6 && mg > 0) mg = 0; /* at the power > 0 test */
                 if (power > (REAL)0) continue;
                 REAL G = REXP(power);
                 REAL og = co[3] * G;
                 REAL a = og < (REAL)0.99f ? og : (REAL)0.99f;
+                {
+                    const double ma = fabs((double)a - 1.0 / 255.0) * 255.0;
+                    if (ma < mg) mg = ma;
+                }
                 if (a < (REAL)(1.0f / 255.0f)) continue;
                 T = T / ((REAL)1 - a);
                 REAL dchdc = a * T;
@@ -716,6 +722,7 @@ static void SFX(orc_backward_render_part)(void* vc_, long long lo_, long long hi
                     as[9] += fabs((double)(G * dLdo));
                 }
             }
+            if (c_->margin) c_->margin[pix] = mg;
         }
     }
 }
@@ -725,8 +732,12 @@ void SFX(orc_backward_render)(const orc_cfg* cfg, int P, const uint32_t* ranges,
                               const REAL* depth, const REAL* out_alpha, const uint32_t* n_contrib,
                               const float* dL_dpix, const float* dL_ddepth, const float* dL_dalpha,
                               double* dmean2D, double* dconic, double* dopac, double* dcolor,
-                              double* ddepth, double* abs_sum)
+                              double* ddepth, double* abs_sum, double* margin)
 {
+    /* margin[H*W] (may be NULL): per pixel, the smallest relative distance of
+     * a walked pair's recomputed alpha from the 1/255 skip threshold (0 where
+     * the exponent is within 1e-6 of the power > 0 test): the device's exp
+     * and the C library's may decide such a pair differently */
     /* abs_sum[P*10] (may be NULL): per Gaussian, the sum of |contribution| of
      * each accumulated value (colour r,g,b, depth, mean2D x,y, conic x,y,w,
      * opacity) -- the scale of fp32 accumulation-order error */
@@ -735,7 +746,7 @@ void SFX(orc_backward_render)(const orc_cfg* cfg, int P, const uint32_t* ranges,
     double* priv = nt > 1 ? (double*)calloc((size_t)nt * (size_t)P * stride, sizeof(double)) : NULL;
     SFX(orc_backward_render_ctx) c_ = {cfg, P, ranges, point_list, means2D, conic_opac, rgb, depth, out_alpha,
                                        n_contrib, dL_dpix, dL_ddepth, dL_dalpha, dmean2D, dconic, dopac, dcolor,
-                                       ddepth, abs_sum, priv, stride};
+                                       ddepth, abs_sum, priv, stride, margin};
     if (priv == NULL) {
         SFX(orc_backward_render_part)(&c_, 0, cfg->H, 0);
         return;

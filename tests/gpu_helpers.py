@@ -87,3 +87,19 @@ def backward(fwd, arrays, cam, dL_dcolor, dL_ddepth=None, dL_dalpha=None, degree
     names = ["dL_dmeans2D", "dL_dcolors", "dL_dopacity", "dL_dmeans3D", "dL_dcov3D", "dL_dsh", "dL_dscales",
              "dL_drotations"]
     return {k: v.cpu().numpy() for k, v in zip(names, g)}
+
+
+class tuned:
+    """Tuning knobs set for the duration (word2world_b200.autotune)."""
+
+    def __init__(self, **knobs):
+        self.knobs = knobs
+
+    def __enter__(self):
+        from word2world_b200 import autotune
+        self.prev = autotune.apply(self.knobs)
+        return self
+
+    def __exit__(self, *exc):
+        from word2world_b200 import autotune
+        autotune.apply(self.prev)

@@ -105,10 +105,11 @@ def test_speed_against_reference_kernel():
 
     def best(fn, out):
         ts = []
-        for _ in range(4):
+        for _ in range(10):
             t = time.perf_counter()
             fn(ptr(out), ptr(m), ptr(c), ptr(o), 20000, R, B, relax)
             ts.append(time.perf_counter() - t)
+        print(fn.__name__ if hasattr(fn, "__name__") else fn, [round(x * 1e3, 2) for x in ts])
         return min(ts[1:])
     t_ref = best(ref.compute_voxel_field_cuda, out_r)
     t_w2w = best(lib.w2w_compute_voxel_field, out_w)

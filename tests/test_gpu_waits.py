@@ -118,18 +118,21 @@ def _scene(P=8192, S=192):
     return arrays, camera.orbit_camera(20.0, 10.0, 2.5, S, S)
 
 
-def test_render_sort_wait_is_reported_by_the_deferred_check():
-    """The render's sort (the depth sort of its 8192 Gaussians: two onesweep
-    tiles per pass) with its first tile unpublished."""
+@pytest.mark.parametrize("binning", [0, 1])
+def test_render_sort_wait_is_reported_by_the_deferred_check(binning):
+    """The render's sort with its first tile unpublished: the radix sort of
+    the emitted keys (binning 0), or the depth sort of the 8192 Gaussians
+    (binning 1; two onesweep tiles per pass)."""
     arrays, cam = _scene()
-    clean = gh.forward(arrays, cam)
-    assert clean["num_rendered"] > 0
-    with hooked(STAGE_SORT, 0):
-        gh.forward(arrays, cam)  # returns; its point list is invalid
-        with pytest.raises(RuntimeError, match="timed out"):
-            _C.check_device_errors()
-    again = gh.forward(arrays, cam)
-    _C.check_device_errors()
+    with gh.tuned(binning=binning):
+        clean = gh.forward(arrays, cam)
+        assert clean["num_rendered"] > 2 * 6144
+        with hooked(STAGE_SORT, 0):
+            gh.forward(arrays, cam)  # returns; its point list is invalid
+            with pytest.raises(RuntimeError, match="timed out"):
+                _C.check_device_errors()
+        again = gh.forward(arrays, cam)
+        _C.check_device_errors()
     for key in ("keys", "point_list", "ranges", "n_contrib", "color", "alpha"):
         assert np.array_equal(again[key], clean[key]), key
 

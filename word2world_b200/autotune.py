@@ -31,6 +31,7 @@ CANDIDATES = {
     "blend_warps": [4, 8],
     "backward_split": [0, 2, 4, 8],
     "backward_ways": [2, 3],
+    "binning": [0, 1],
 }
 
 

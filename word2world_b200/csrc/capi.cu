@@ -250,8 +250,13 @@ size_t w2w_binning_offset(long long R, int W, int H, const char* name) {
 }
 
 // Single-view calls with at most kMaxBinTiles tiles bin their instances from
-// the depth-ordered Gaussians (binning.cu); others emit keys and sort them.
-inline bool use_binning(int P, int W, int H) { return P > 0 && num_tiles(W, H) <= kMaxBinTiles; }
+// the depth-ordered Gaussians (binning.cu) when the tuning knob selects it;
+// others emit keys and sort them.  The geometry phase records its choice in
+// the info it returns, so the render follows it whatever the knob says then.
+inline bool use_binning(int P, int W, int H) {
+  return P > 0 && num_tiles(W, H) <= kMaxBinTiles && tune_value(kTuneBinning) == 1;
+}
+constexpr uint32_t kInfoDepthOrder = 1u;  // w2w_geometry_info::reserved: the depth order is prepared
 
 // The binning path's per-Gaussian half, after the projection pass: the
 // Gaussians sorted stably by the depth bits their keys keep, and the prefix of
@@ -356,6 +361,7 @@ static int forward_geometry(const w2w_settings* s, const float* means3D, const f
   if (h.error & kErrCapacity) return W2W_ERR_CAPACITY;
   if (h.num_rendered > 0 && use_binning(s->P, s->width, s->height)) {
     launch_depth_order(s, geom_state, *info, st);
+    info->reserved |= kInfoDepthOrder;  // tells w2w_forward_render which path to take
     return check_launch();
   }
   return W2W_OK;
@@ -396,7 +402,7 @@ int w2w_forward_render(const w2w_settings* s, const void* geom_state, const w2w_
   const void* err_word = nullptr;  // the binning header's error word
   if (R == 0) {
     cudaMemsetAsync(ranges, 0, sizeof(uint2) * size_t(T), st);
-  } else if (use_binning(s->P, W, H)) {
+  } else if ((info->reserved & kInfoDepthOrder) != 0u) {
     const GeomLayout GL(s->P);
     const BinLayout BL(R, T);
     const KeyPlan kp = plan_keys(*info, W, H);

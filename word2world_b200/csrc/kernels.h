@@ -325,7 +325,10 @@ long long unpublished_tile(int stage);
 // per-pixel backward splits (in quarters of the SM count) and into how many
 // segments.  None of them changes a result beyond the order of float atomic
 // additions.
-enum TuneKnob { kTuneBlendWarps = 0, kTuneBwdSplit = 1, kTuneBwdWays = 2, kNumTuneKnobs = 3 };
+// The fourth knob picks how a single-view call builds its sorted list: 0 key
+// emission + radix sort (duplicate.cu, sort.cu), 1 binning from the
+// depth-ordered Gaussians (binning.cu); both give the same list.
+enum TuneKnob { kTuneBlendWarps = 0, kTuneBwdSplit = 1, kTuneBwdWays = 2, kTuneBinning = 3, kNumTuneKnobs = 4 };
 int tune_value(int knob);
 
 size_t scan_scratch_bytes(long long n);
