@@ -87,16 +87,18 @@ def test_batches_overlap_on_the_device():
     import parity
     from word2world_b200 import scenes as S
     from word2world_b200.batch import Scene
+    # batches of several milliseconds of device work (the host issues one in
+    # about a millisecond, so smaller ones would finish before the next starts)
     scs = [Scene.from_arrays(S.make_scene(P, seed=40 + k, layout="ball").activate(), "cuda")
-           for k, P in enumerate((60000, 30000))]
+           for k, P in enumerate((400000, 300000))]
     # at most one request per batch: eight batches through two slots.  A
     # first pass grows both slots' workspaces (a growth returns memory to the
     # driver, which synchronises the device); the second runs as a warmed-up
     # server does.
     srv = sv.Server(scs, keep_results=True, max_batch_work=1.0, slots=2)
-    srv.serve(sv.poisson_requests(8, rate=1000.0, scenes=scs, seed=9, views=(2, 2), res=(256,)), realtime=False)
+    srv.serve(sv.poisson_requests(8, rate=1000.0, scenes=scs, seed=9, views=(4, 4), res=(512,)), realtime=False)
     srv.batch_log = []
-    reqs = sv.poisson_requests(8, rate=1000.0, scenes=scs, seed=9, views=(2, 2), res=(256,))
+    reqs = sv.poisson_requests(8, rate=1000.0, scenes=scs, seed=9, views=(4, 4), res=(512,))
     info = srv.serve(reqs, realtime=False)
     assert info["batches"] == 8 and len(srv.batch_log) == 8
     assert sv.overlapping_batches(srv.batch_log) >= 1, srv.batch_log
