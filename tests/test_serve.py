@@ -91,11 +91,11 @@ def test_batches_overlap_on_the_device():
     # about a millisecond, so smaller ones would finish before the next starts)
     scs = [Scene.from_arrays(S.make_scene(P, seed=40 + k, layout="ball").activate(), "cuda")
            for k, P in enumerate((400000, 300000))]
-    # at most one request per batch: eight batches through two slots.  A
-    # first pass grows both slots' workspaces (a growth returns memory to the
-    # driver, which synchronises the device); the second runs as a warmed-up
-    # server does.
-    srv = sv.Server(scs, keep_results=True, max_batch_work=1.0, slots=2)
+    # at most one request per batch (the work bound holds one request of the
+    # larger scene): eight batches through two slots.  A first pass grows both
+    # slots' workspaces (a growth returns memory to the driver, which
+    # synchronises the device); the second runs as a warmed-up server does.
+    srv = sv.Server(scs, keep_results=True, max_batch_work=1.7e6, slots=2)
     srv.serve(sv.poisson_requests(8, rate=1000.0, scenes=scs, seed=9, views=(4, 4), res=(512,)), realtime=False)
     srv.batch_log = []
     reqs = sv.poisson_requests(8, rate=1000.0, scenes=scs, seed=9, views=(4, 4), res=(512,))

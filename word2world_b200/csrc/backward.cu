@@ -315,18 +315,11 @@ __global__ void __launch_bounds__(kBlendThreads, 2) render_ref_kernel(BackwardAr
       const bool ok0 = ref_eval(a0, a1, a2, pxf, pyf, dx0, dy0, G0, al0) && uint32_t(hi - 1 - j0) < p.last;
       const bool ok1 = ref_eval(b0, b1, b2, pxf, pyf, dx1, dy1, G1, al1) && has1 &&
                        uint32_t(hi - 1 - j1) < p.last;
-      // an entry no lane of the warp takes leaves the state unchanged and adds
-      // nothing: skip its step and reduction (warp-uniform branch)
-      if (__any_sync(0xffffffffu, ok0)) {
-        float c0[kValues];
-        ch.step(ok0, p, a0, a1, a2, dx0, dy0, G0, al0, ddelx_dx, ddely_dy, c0);
-        flush(c0, ok0, wc.id[j0], tgt);
-      }
-      if (__any_sync(0xffffffffu, ok1)) {
-        float c1[kValues];
-        ch.step(ok1, p, b0, b1, b2, dx1, dy1, G1, al1, ddelx_dx, ddely_dy, c1);
-        flush(c1, ok1, wc.id[j1], tgt);
-      }
+      float c0[kValues], c1[kValues];
+      ch.step(ok0, p, a0, a1, a2, dx0, dy0, G0, al0, ddelx_dx, ddely_dy, c0);
+      ch.step(ok1, p, b0, b1, b2, dx1, dy1, G1, al1, ddelx_dx, ddely_dy, c1);
+      flush(c0, ok0, wc.id[j0], tgt);
+      flush(c1, ok1, wc.id[j1], tgt);
     }
   };
   auto state_only = [&](uint32_t bits, int hi) {
@@ -341,8 +334,8 @@ __global__ void __launch_bounds__(kBlendThreads, 2) render_ref_kernel(BackwardAr
       const bool ok0 = ref_eval(a0, a1, a2, pxf, pyf, dx0, dy0, G0, al0) && uint32_t(hi - 1 - j0) < p.last;
       const bool ok1 = ref_eval(b0, b1, b2, pxf, pyf, dx1, dy1, G1, al1) && has1 &&
                        uint32_t(hi - 1 - j1) < p.last;
-      if (__any_sync(0xffffffffu, ok0)) ch.advance(ok0, a1, a2, al0);
-      if (__any_sync(0xffffffffu, ok1)) ch.advance(ok1, b1, b2, al1);
+      ch.advance(ok0, a1, a2, al0);
+      ch.advance(ok1, b1, b2, al1);
     }
   };
   if (role < 0) {
@@ -481,16 +474,11 @@ __global__ void __launch_bounds__(kBlendThreads, 2) render_exact_kernel(Backward
       const float al0 = fminf(0.99f, og0), al1 = fminf(0.99f, og1);
       const bool ok0 = al0 >= 1.0f / 255.0f && uint32_t(hi - 1 - j0) < p.last;
       const bool ok1 = al1 >= 1.0f / 255.0f && has1 && uint32_t(hi - 1 - j1) < p.last;
-      if (__any_sync(0xffffffffu, ok0)) {
-        float c0[kValues];
-        ch.step(ok0, p, a0, a1, s[kRecVec * j0 + 2], pxf, pyf, g0, og0, al0, m0, hW, hH, c0);
-        flush(c0, ok0, wc.id[j0], tgt);
-      }
-      if (__any_sync(0xffffffffu, ok1)) {
-        float c1[kValues];
-        ch.step(ok1, p, b0, b1, s[kRecVec * j1 + 2], pxf, pyf, g1, og1, al1, m1, hW, hH, c1);
-        flush(c1, ok1, wc.id[j1], tgt);
-      }
+      float c0[kValues], c1[kValues];
+      ch.step(ok0, p, a0, a1, s[kRecVec * j0 + 2], pxf, pyf, g0, og0, al0, m0, hW, hH, c0);
+      ch.step(ok1, p, b0, b1, s[kRecVec * j1 + 2], pxf, pyf, g1, og1, al1, m1, hW, hH, c1);
+      flush(c0, ok0, wc.id[j0], tgt);
+      flush(c1, ok1, wc.id[j1], tgt);
     }
   };
   auto state_only = [&](uint32_t bits, int hi) {
@@ -505,8 +493,8 @@ __global__ void __launch_bounds__(kBlendThreads, 2) render_exact_kernel(Backward
       const float al0 = fminf(0.99f, mul(a1.z, g0)), al1 = fminf(0.99f, mul(b1.z, g1));
       const bool ok0 = al0 >= 1.0f / 255.0f && uint32_t(hi - 1 - j0) < p.last;
       const bool ok1 = al1 >= 1.0f / 255.0f && has1 && uint32_t(hi - 1 - j1) < p.last;
-      if (__any_sync(0xffffffffu, ok0)) ch.advance(ok0, a1, s[kRecVec * j0 + 2], al0);
-      if (__any_sync(0xffffffffu, ok1)) ch.advance(ok1, b1, s[kRecVec * j1 + 2], al1);
+      ch.advance(ok0, a1, s[kRecVec * j0 + 2], al0);
+      ch.advance(ok1, b1, s[kRecVec * j1 + 2], al1);
     }
   };
   if (role < 0) {
