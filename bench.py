@@ -491,7 +491,12 @@ def run_e2e(a, sc, cams, device, world):
         cam_rows[v, 32:35] = np.asarray(c.campos, np.float32).ravel()
     host_c = torch.from_numpy(cam_rows).pin_memory()
     h2d = host_g.numel() * 4 + host_c.numel() * 4
-    loss_host = torch.empty(a.views, dtype=torch.float32).pin_memory()
+    # each step's losses come back to pinned host memory; the host reads step
+    # k's once step k + 1 is queued (as a training loop that logs its loss does),
+    # so it never idles the device waiting for the copy
+    loss_host = [torch.empty(a.views, dtype=torch.float32).pin_memory() for _ in range(2)]
+    copied = [None, None]
+    read_back = []
 
     # the step's inputs are copied on a side stream at the step's start: all
     # cameras first (a view's render needs only its camera), then the image
@@ -502,7 +507,7 @@ def run_e2e(a, sc, cams, device, world):
     vstreams = [torch.cuda.Stream(device=device) for _ in cams] if not a.single_stream else None
     quiet_stream_mismatch()
 
-    def step():
+    def step(k):
         for p_ in params.parameters():
             p_.grad = None
         copy_stream.wait_stream(main_stream)  # the previous step is done with the buffers
@@ -539,22 +544,33 @@ def run_e2e(a, sc, cams, device, world):
                 main_stream.wait_stream(vs)
             for x in losses:
                 x.record_stream(main_stream)
-        loss_host.copy_(torch.stack(losses), non_blocking=True)
-        torch.cuda.current_stream().synchronize()
-        return loss_host
+        slot = k % 2
+        loss_host[slot].copy_(torch.stack(losses), non_blocking=True)
+        copied[slot] = torch.cuda.Event()
+        copied[slot].record(main_stream)
+        if k > 0:  # the previous step's losses, on the host
+            read(k - 1)
 
-    for _ in range(max(a.warmup, 1)):
-        step()
+    def read(k):
+        copied[k % 2].synchronize()
+        read_back.append(loss_host[k % 2].tolist())
+
+    for k in range(max(a.warmup, 1)):
+        step(k)
+    read(max(a.warmup, 1) - 1)
     torch.cuda.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record()
-    for _ in range(a.steps):
-        step()
+    for k in range(a.steps):
+        step(k)
+    read(a.steps - 1)  # the last step's losses: every step's result is read inside the timed region
     e1.record()
     torch.cuda.synchronize()
     ms = wd.max_over_ranks(e0.elapsed_time(e1), device=device)
+    assert len(read_back) == max(a.warmup, 1) + a.steps and all(np.isfinite(read_back[-1]))
     return {"value": round(world * a.views * a.steps / (ms / 1e3), 3), "unit": UNIT, "h2d_bytes_per_step": int(h2d),
-            "d2h_bytes_per_step": int(loss_host.numel() * 4), "api": "word2world_b200.renderer.Renderer.render"}
+            "d2h_bytes_per_step": int(loss_host[0].numel() * 4), "api": "word2world_b200.renderer.Renderer.render",
+            "readback": "each step's losses read on the host once the next step is queued"}
 
 
 # ---------------------------------------------------------------------------
@@ -733,6 +749,7 @@ def run_serve(a):
         warm_served()
         reqs = sv.poisson_requests(a.requests, rate, scs, seed=a.seed + 3, device=device)
         srv.batch_ms = []
+        srv.batch_log = []
         grown = srv.workspace_growths()
         info = srv.serve(reqs, realtime=True)
         bm = np.array(srv.batch_ms)
