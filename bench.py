@@ -116,23 +116,35 @@ class ClockSampler:
         self.path = os.path.join("/tmp", f"w2w_clocks_{os.getpid()}.csv")
 
     def __enter__(self):
+        # every 10 ms, so that a timed region of a few tens of ms still gets
+        # several samples; 50 ms if this nvidia-smi refuses the shorter interval
+        for interval in ("10", "50"):
+            if self._start(interval):
+                break
+        return self
+
+    def _start(self, interval):
         try:
             self.f = open(self.path, "w")
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}",
-                                          "--format=csv,noheader,nounits", "-lms", "50"], stdout=self.f,
+                                          "--format=csv,noheader,nounits", "-lms", interval], stdout=self.f,
                                          stderr=subprocess.DEVNULL)
         except Exception:
             self.proc = None
-            return self
+            return True
         # nvidia-smi takes a moment to start: wait (at most 5 s) for its first
         # row so that the samples cover the timed region from its start
         t0 = time.time()
         while time.time() - t0 < 5.0 and self.proc.poll() is None:
             self.f.flush()
             if os.path.getsize(self.path) > 0:
-                break
+                return True
             time.sleep(0.02)
-        return self
+        if self.proc.poll() is not None:  # exited without a row
+            self.f.close()
+            self.proc = None
+            return False
+        return True
 
     def __exit__(self, *exc):
         if self.proc is not None:

@@ -376,7 +376,12 @@ int w2w_throughput_probe(int kind, long long iters, int blocks, float* out, long
  * (how a single-view call of at most 4096 tiles builds its sorted list: 0
  * key emission and the radix sort, 1 binning from the depth-ordered
  * Gaussians; default 0; w2w_forward_geometry records the path taken in
- * w2w_geometry_info.reserved, bit 0, and w2w_forward_render follows it).
+ * w2w_geometry_info.reserved, bit 0, and w2w_forward_render follows it), 4
+ * "blend_queue" (0: one CTA per tile part, launched heaviest first; 1: a
+ * persistent blend, one CTA per resident slot, pulling tile parts from a
+ * device queue in the same order, each CTA a producer warp that gathers the
+ * batches' records with TMA into a three-stage shared-memory ring and
+ * "blend_warps" consumer warps; default 0).
  * Results do not depend on them beyond the order of float atomic additions.
  * w2w_tune_set returns the previous value, or -1 (and changes nothing) for an
  * unknown knob or value. */

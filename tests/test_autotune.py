@@ -36,22 +36,24 @@ def test_knob_setter_validates(restore):
 
 
 def test_descent_finds_the_cheapest_setting_and_caches_it(restore, tmp_path):
-    # a cost model over the knobs: its minimum is blend_warps 8, backward_split 2, backward_ways 3, binning 1
+    # a cost model over the knobs: its minimum is blend_warps 8, backward_split 2, backward_ways 3, binning 1,
+    # blend_queue 1
     def cost():
         k = autotune.current()
         return (1.0 + (0.0 if k["blend_warps"] == 8 else 0.3) + abs(k["backward_split"] - 2) * 0.1 +
-                (0.0 if k["backward_ways"] == 3 else 0.05) + (0.0 if k["binning"] == 1 else 0.02))
+                (0.0 if k["backward_ways"] == 3 else 0.05) + (0.0 if k["binning"] == 1 else 0.02) +
+                (0.0 if k["blend_queue"] == 1 else 0.04))
 
     path = str(tmp_path / "tune.json")
     t = autotune.Autotuner(path=path, timer=lambda step: cost())
-    autotune.apply({"blend_warps": 4, "backward_split": 4, "backward_ways": 2, "binning": 0})
+    autotune.apply({"blend_warps": 4, "backward_split": 4, "backward_ways": 2, "binning": 0, "blend_queue": 0})
     best = t.tune("bucket", step=None)
-    assert best == {"blend_warps": 8, "backward_split": 2, "backward_ways": 3, "binning": 1}
+    assert best == {"blend_warps": 8, "backward_split": 2, "backward_ways": 3, "binning": 1, "blend_queue": 1}
     assert autotune.current() == best
     saved = json.load(open(path))
     assert saved["bucket"]["blend_warps"] == 8
     # a second tuner reads the cache and applies it without timing anything
-    autotune.apply({"blend_warps": 4, "backward_split": 4, "backward_ways": 2, "binning": 0})
+    autotune.apply({"blend_warps": 4, "backward_split": 4, "backward_ways": 2, "binning": 0, "blend_queue": 0})
     t2 = autotune.Autotuner(path=path, timer=lambda step: pytest.fail("timed a cached bucket"))
     assert t2.ensure("bucket", step=None) == best and autotune.current() == best
 
@@ -66,16 +68,17 @@ def test_every_knob_setting_gives_the_same_results(restore):
     cam = camera.orbit_camera(60.0, 15.0, 2.5, 256, 256)
     g = np.random.default_rng(3).normal(size=(3, 256, 256)).astype(np.float32)
     base = None
-    for warps, split, ways, binning in ((4, 4, 2, 0), (8, 4, 2, 0), (4, 0, 2, 1), (4, 8, 3, 1), (8, 8, 2, 1),
-                                        (4, 4, 3, 0)):
-        autotune.apply({"blend_warps": warps, "backward_split": split, "backward_ways": ways, "binning": binning})
+    for warps, split, ways, binning, queue in ((4, 4, 2, 0, 0), (8, 4, 2, 0, 0), (4, 0, 2, 1, 0), (4, 8, 3, 1, 1),
+                                               (8, 8, 2, 1, 1), (4, 4, 3, 0, 1), (8, 4, 2, 0, 1)):
+        autotune.apply({"blend_warps": warps, "backward_split": split, "backward_ways": ways, "binning": binning,
+                        "blend_queue": queue})
         f = gh.forward(arrays, cam)
         b = gh.backward(f, arrays, cam, g, grad_mode=0)
         if base is None:
             base = (f, b)
             continue
         for k in ("color", "alpha", "depth_img", "n_contrib", "keys", "point_list"):
-            assert parity.bit_mismatch(f[k], base[0][k]) == 0, (warps, split, ways, binning, k)
+            assert parity.bit_mismatch(f[k], base[0][k]) == 0, (warps, split, ways, binning, queue, k)
         for k in parity.GRAD_NAMES:
             c = parity.grad_check(b[k], base[1][k], row_rtol=parity.SAME_IMPL_ROW_RTOL)
             assert c["norm_rel"] <= 1e-5, (warps, split, ways, binning, k, c)

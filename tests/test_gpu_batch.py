@@ -38,8 +38,20 @@ def _plain(sc, view):
                                   c.width, bg, True), bg
 
 
-@pytest.mark.parametrize("grad_mode,reuse", [("reference", False), ("exact", False), ("reference", True)])
-def test_batch_matches_single_views(grad_mode, reuse):
+@pytest.mark.parametrize("grad_mode,reuse,queue", [("reference", False, 0), ("exact", False, 0), ("reference", True, 0),
+                                                   ("reference", False, 1)])
+def test_batch_matches_single_views(grad_mode, reuse, queue):
+    """queue = 1: the batched blend is the persistent one, its queue holding
+    every item's tiles."""
+    from word2world_b200 import autotune
+    prev = autotune.apply({"blend_queue": queue})
+    try:
+        _batch_matches_single_views(grad_mode, reuse)
+    finally:
+        autotune.apply(prev)
+
+
+def _batch_matches_single_views(grad_mode, reuse):
     scs, views = _setup()
     br = BatchRenderer(grad_mode=grad_mode, reuse_buffers=reuse)
     rng = np.random.default_rng(11)

@@ -20,7 +20,7 @@ if not torch.cuda.is_available():
 import oracle  # noqa: E402
 import parity  # noqa: E402
 import gpu_helpers as gh  # noqa: E402
-from word2world_b200 import camera, scenes  # noqa: E402
+from word2world_b200 import _C, camera, scenes  # noqa: E402
 
 
 def _setup(P=4096, seed=0, layout="shell", size=128, az=30.0, el=10.0, degree=3, log_scale=(-5.0, -3.0),
@@ -230,3 +230,31 @@ def test_binning_paths_agree(case, compat_spill):
         c = parity.grad_check(b1[k], b0[k], row_rtol=parity.SAME_IMPL_ROW_RTOL)
         assert c["norm_rel"] <= 1e-5 and c["n_bad"] == 0, (k, c)
 
+
+
+QUEUE_CASES = dict(BIN_CASES, heavy_40k_512=dict(P=40000, seed=12, layout="ball", size=512))
+
+
+@pytest.mark.parametrize("warps", [4, 8])
+@pytest.mark.parametrize("case", list(QUEUE_CASES))
+def test_queue_blend_agrees(case, warps):
+    """The persistent blend fed by the device tile queue and TMA row gathers
+    (the "blend_queue" tuning knob) gives bit-identical images, contributor
+    counts and block masks (hence backward gradients) to the per-tile blend."""
+    spec = dict(QUEUE_CASES[case])
+    arrays, cam = _setup(**spec)
+    rng = np.random.default_rng(6)
+    g = rng.normal(size=(3, cam.height, cam.width)).astype(np.float32)
+    out = {}
+    for queue in (0, 1):
+        with gh.tuned(blend_warps=warps, blend_queue=queue):
+            f = gh.forward(arrays, cam)
+            b = gh.backward(f, arrays, cam, g, grad_mode=0)
+            _C.check_device_errors()  # no bounded wait of the queue ran out
+        out[queue] = (f, b)
+    (f0, b0), (f1, b1) = out[0], out[1]
+    for k in ("point_list", "ranges", "n_contrib", "color", "alpha", "depth_img"):
+        assert parity.bit_mismatch(f0[k], f1[k]) == 0, k
+    for k in parity.GRAD_NAMES:
+        c = parity.grad_check(b1[k], b0[k], row_rtol=parity.SAME_IMPL_ROW_RTOL)
+        assert c["norm_rel"] <= 1e-5 and c["n_bad"] == 0, (k, c)

@@ -100,7 +100,9 @@ def test_renderer_render_is_preamble_plus_function(grad_mode, degree):
     for name, a, b in zip(("mean", "sh_dc", "sh_ac", "opacity", "svec", "quaternion"), got, raw):
         a, b = a.cpu().numpy(), b.grad.cpu().numpy()
         if name == "quaternion":  # at the floor torch's clamp has a kink; both sides take g / 1e-12
-            np.testing.assert_allclose(a[:14], b[:14], rtol=1e-5, atol=0)
+            # g is summed by atomics in either order: relative to its row's largest element
+            row = np.abs(b[:14]).max(axis=1, keepdims=True)
+            assert np.all(np.abs(a[:14] - b[:14]) <= 1e-5 * (np.abs(b[:14]) + row)), (a[:14], b[:14])
         chk = parity.grad_check(a, b, row_rtol=parity.SAME_IMPL_ROW_RTOL)
         assert chk["norm_rel"] <= 1e-5 and chk["n_bad"] == 0, (name, chk)
 

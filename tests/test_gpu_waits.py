@@ -118,13 +118,15 @@ def _scene(P=8192, S=192):
     return arrays, camera.orbit_camera(20.0, 10.0, 2.5, S, S)
 
 
-@pytest.mark.parametrize("binning", [0, 1])
-def test_render_sort_wait_is_reported_by_the_deferred_check(binning):
+@pytest.mark.parametrize("binning,queue", [(0, 0), (1, 0), (0, 1)])
+def test_render_sort_wait_is_reported_by_the_deferred_check(binning, queue):
     """The render's sort with its first tile unpublished: the radix sort of
     the emitted keys (binning 0), or the depth sort of the 8192 Gaussians
-    (binning 1; two onesweep tiles per pass)."""
+    (binning 1; two onesweep tiles per pass).  With queue = 1 the persistent
+    blend then walks the inconsistent list (stray ids gather a valid row and
+    are never blended) and the next render is clean."""
     arrays, cam = _scene()
-    with gh.tuned(binning=binning):
+    with gh.tuned(binning=binning, blend_queue=queue):
         clean = gh.forward(arrays, cam)
         assert clean["num_rendered"] > 2 * 6144
         with hooked(STAGE_SORT, 0):

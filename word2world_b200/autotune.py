@@ -1,6 +1,7 @@
 """Launch-shape autotuner: picks the library's tuning knobs (blend CTA shape,
-how many heavy tiles the per-pixel backward splits, and into how many
-segments) for a workload by timing it, and remembers the choice per shape
+per-tile or persistent queue-fed blend, how many heavy tiles the per-pixel
+backward splits and into how many segments, radix or depth-ordered binning)
+for a workload by timing it, and remembers the choice per shape
 bucket.
 
 The reference's launch shapes are constants (pixelGaussiansFull.cu:99-122,
@@ -32,6 +33,7 @@ CANDIDATES = {
     "backward_split": [0, 2, 4, 8],
     "backward_ways": [2, 3],
     "binning": [0, 1],
+    "blend_queue": [0, 1],
 }
 
 

@@ -17,6 +17,10 @@
 #include "common.cuh"
 #include "kernels.h"
 #include "tile_walk.cuh"
+#include "tma.cuh"
+
+#include <algorithm>
+#include <mutex>
 
 namespace w2w {
 namespace {
@@ -194,12 +198,322 @@ __global__ void __launch_bounds__(32 * kBlendWarps, 16 / kBlendWarps) blend_kern
   }
 }
 
+// ---------------------------------------------------------------------------
+// Persistent blend over a device tile queue, staged by TMA row gathers.
+//
+// A CTA runs kW consumer warps (the blocks of one tile half, or of the whole
+// tile for kW = 8) and one producer warp, for as long as the queue (tile
+// halves in the heaviest-first order; every item of a batched call in one
+// queue) has items.  The producer takes the next item with an atomic, reads
+// a batch's Gaussian ids from the list and gathers their 64-byte records
+// into one of kQStages shared-memory stages with TMA (four rows per gather),
+// then computes every staged entry's block bits once (as the cooperative
+// staging does) and publishes the stage.  The consumers walk each stage as
+// the per-tile kernel does and release it; a warp whose pixels have all
+// terminated tells the producer, which skips the rest of a tile once every
+// consumer warp has.  The stages run across tile boundaries, so a CTA never
+// drains its pipeline between tiles, and no warp waits at a CTA barrier for
+// the slowest warp of a batch: warps drift apart by up to kQStages batches.
+// Every wait is bounded (spin_limit polls); one that runs out sets
+// kErrTimeout in `error`, and the CTA stops after its copies in flight land.
+// Results are bit-identical to blend_kernel's (same entries, same order).
+// ---------------------------------------------------------------------------
+constexpr int kQStages = 3;
+constexpr int kQRec = 4;  // float4s per staged record (the whole record)
+
+struct QueueStage {
+  int tile;   // tile id (-1: the queue is empty, stop)
+  int part;   // tile half (kW = 4) or 0
+  int base;   // list position of the batch's first entry, from the tile's start
+  int count;  // entries in the batch
+  int seq;    // the CTA's item number
+  int first;  // 1: the item's first batch
+};
+
+template <int kW>
+struct __align__(128) QueueShared {
+  float4 rec[kQStages][kBatch * kQRec];  // 16 KB per stage; gathers land 256 B at a time
+  uint32_t bal[kQStages][kW][kBatch / 32];
+  QueueStage hdr[kQStages];
+  uint8_t list[kW][kBatch];
+  unsigned long long data_bar[kQStages];   // the stage's gathers landed
+  unsigned long long ready_bar[kQStages];  // the stage's block bits and header are written
+  unsigned long long empty_bar[kQStages];  // every consumer warp is done with the stage
+  uint32_t done[4];                        // per item (seq mod 4): consumer warps whose pixels all terminated
+  uint32_t abort;
+};
+
+template <int kW>
+constexpr size_t queue_smem_bytes() {
+  return sizeof(QueueShared<kW>) + 128;  // + alignment slack of the dynamic shared memory base
+}
+
+// Bounded wait on `bar`'s phase `parity`: at most `limit` polls, spaced by a
+// short sleep after the first few (well under a second at the default
+// limit).  False when it ran out (or another warp's did), after flagging the
+// CTA and the call.
+// Warp-collective: every lane polls (so each acquires the phase itself) and
+// the warp decides together, so its lanes never part ways.
+__device__ __forceinline__ bool queue_wait(unsigned long long* bar, uint32_t parity, volatile uint32_t* abort,
+                                           uint32_t limit, uint32_t* error) {
+  for (uint32_t i = 0; i < limit; ++i) {
+    if (__all_sync(0xffffffffu, tma::bar_test(bar, parity))) return true;
+    if (__any_sync(0xffffffffu, *abort != 0u)) return false;
+    if (i >= 32u) __nanosleep(64);
+  }
+  if ((threadIdx.x & 31u) == 0u) {
+    *abort = 1u;
+    if (error != nullptr) atomicOr(error, kErrTimeout);
+  }
+  return false;
+}
+
+template <int kW>
+__global__ void __launch_bounds__(32 * (kW + 1)) blend_queue_kernel(BlendArgs a, const __grid_constant__ CUtensorMap map) {
+  constexpr int kParts = 8 / kW;
+  extern __shared__ unsigned char q_raw[];
+  QueueShared<kW>& s = *reinterpret_cast<QueueShared<kW>*>((reinterpret_cast<uintptr_t>(q_raw) + 127) & ~uintptr_t(127));
+  const int warp = int(threadIdx.x >> 5), lane = int(threadIdx.x & 31);
+  const uint32_t limit = a.spin_limit;
+  volatile uint32_t* abort = &s.abort;
+  if (threadIdx.x == 0) {
+    for (int i = 0; i < kQStages; ++i) {
+      tma::bar_init(&s.data_bar[i], 1);
+      tma::bar_init(&s.ready_bar[i], 32);
+      tma::bar_init(&s.empty_bar[i], kW);
+    }
+    s.abort = 0u;
+    tma::bar_init_fence();
+  }
+  if (threadIdx.x == 32 * kW) tma::prefetch_map(&map);
+  __syncthreads();
+  const int total_items = a.total_tiles * kParts;  // every tile's parts (all items' tiles in a batched call)
+
+  if (warp == kW) {
+    // ---------------- producer ----------------
+    uint32_t k = 0;       // stages published
+    uint32_t seq = 0;
+    bool in_flight = false;  // gathers issued on stage (k % kQStages) not yet waited for
+    for (;; ++seq) {
+      int item = 0;
+      if (lane == 0) item = int(atomicAdd(a.queue, 1u));
+      item = __shfl_sync(0xffffffffu, item, 0);
+      const bool end = item >= total_items;
+      int tile = -1, part = 0, n = 0, X0 = 0, Y0 = 0;
+      uint2 range = make_uint2(0u, 0u);
+      if (!end) {
+        tile = int(a.order[item / kParts]);
+        part = item % kParts;
+        range = a.ranges[tile];
+        n = int(range.y - range.x);
+        int W = a.W, ltile = tile;
+        if (a.items != nullptr) {
+          const BatchItem& it = a.items[find_item_tile(a.items, a.num_items, uint32_t(tile))];
+          W = it.W;
+          ltile = tile - int(it.tile_base);
+        }
+        const int gw = (W + kTile - 1) / kTile;
+        X0 = (ltile % gw) * kTile;
+        Y0 = (ltile / gw) * kTile + kBlockH * (part * kW / 2);
+      }
+      if (lane == 0) s.done[seq & 3] = 0u;  // published to the consumers by this item's first stage
+      uint8_t* lo_dst = a.mask_top == nullptr ? nullptr : (part == 0 ? a.mask_top : a.mask_bottom) + range.x;
+      uint8_t* hi_dst = a.mask_top == nullptr || kParts != 1 ? nullptr : a.mask_bottom + range.x;
+      const int nb = end ? 1 : max(1, (n + kBatch - 1) / kBatch);
+      for (int b = 0; b < nb; ++b) {
+        // every consumer warp of the item has terminated: skip its other batches
+        uint32_t done = 0;
+        if (lane == 0) done = *reinterpret_cast<volatile uint32_t*>(&s.done[seq & 3]);
+        if (b > 0 && __shfl_sync(0xffffffffu, done, 0) == uint32_t(kW)) break;
+        const int st = int(k % kQStages);
+        const uint32_t ph = (k / kQStages) & 1u;
+        if (!queue_wait(&s.empty_bar[st], ph ^ 1u, abort, limit, a.error)) goto stop;
+        const int base = b * kBatch;
+        const int cnt = end ? 0 : min(kBatch, n - base);
+        const int groups = (cnt + 3) >> 2;
+        // every stage completes one phase of its data barrier (an empty one
+        // with no bytes), so its parity follows the stage count
+        if (lane == 0) tma::bar_arrive_expect(&s.data_bar[st], uint32_t(groups) * 4u * 64u);
+        __syncwarp();
+        in_flight = true;
+        const uint32_t* ids = a.point_list + range.x + base;
+        if (cnt > 0) {
+          for (int g = lane; g < groups; g += 32) {
+            int r[4];
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+              const int e = 4 * g + q;
+              const uint32_t id = e < cnt ? ids[e] : 0u;
+              r[q] = id < a.num_records ? int(id) : 0;  // a stray id gathers row 0; its bits stay clear
+            }
+            tma::gather4(&s.rec[st][kQRec * 4 * g], &map, &s.data_bar[st], r[0], r[1], r[2], r[3]);
+          }
+        }
+        if (!queue_wait(&s.data_bar[st], ph, abort, limit, a.error)) goto stop;
+        in_flight = false;
+        if (cnt > 0) {
+          // every staged entry's block bits, once for the CTA's kW blocks
+#pragma unroll 1
+          for (int c = 0; c < kBatch / 32; ++c) {
+            const int j = 32 * c + lane;
+            uint32_t mask = 0;
+            if (j < cnt && ids[j] < a.num_records) {
+              const float4* r = &s.rec[st][kQRec * j];
+              const float4 r0 = r[0], r2 = r[2], r3 = r[3];
+              mask = block_mask<kW / 2>(r0.x, r0.y, r2.w, r3.x, r3.y, r3.z, r3.w, X0, Y0);
+              if (lo_dst != nullptr) lo_dst[base + j] = uint8_t(mask & 15u);
+              if (hi_dst != nullptr) hi_dst[base + j] = uint8_t(mask >> 4);
+            }
+            uint32_t mine = 0;
+#pragma unroll
+            for (int bb = 0; bb < kW; ++bb) {
+              const uint32_t w = __ballot_sync(0xffffffffu, (mask >> bb) & 1u);
+              if (lane == bb) mine = w;
+            }
+            if (lane < kW) s.bal[st][lane][c] = mine;
+          }
+        } else if (lane < kW) {
+#pragma unroll
+          for (int c = 0; c < kBatch / 32; ++c) s.bal[st][lane][c] = 0u;
+        }
+        if (lane == 0) s.hdr[st] = QueueStage{tile, part, base, cnt, int(seq), b == 0 ? 1 : 0};
+        tma::bar_arrive(&s.ready_bar[st]);  // every lane, after its own writes
+        ++k;
+      }
+      if (end) break;
+    }
+    return;
+  stop:
+    // a wait ran out: let the copies in flight land before the CTA ends
+    if (in_flight) {
+      const int st = int(k % kQStages);
+      for (uint32_t i = 0; i < limit && !tma::bar_test(&s.data_bar[st], (k / kQStages) & 1u); ++i) __nanosleep(64);
+    }
+    return;
+  }
+
+  // ---------------- consumers ----------------
+  BlendPixel pix;
+  pix.done = true;
+  bool have = false, reported = true;
+  int tile = -1, W = 0, H = 0, first_block = 0;
+  size_t pbase = 0;
+  const float* bg = a.bg;
+  TilePixel tp(0, 1, warp);
+  float pxf = 0.f, pyf = 0.f;
+  auto finish = [&]() {
+    if (!have) return;
+    if (tp.px < W && tp.py < H) {
+      const size_t q = size_t(tp.py) * W + tp.px;
+      const size_t p = pbase + q, cp = 3 * pbase + q;
+      const size_t hw = size_t(W) * H;
+      a.n_contrib[p] = pix.last;
+      a.out_alpha[p] = pix.Wt;
+      a.out_depth[p] = pix.D;
+      a.T_final[p] = pix.T;
+      a.out_color[cp] = fma(pix.T, bg[0], pix.C0);
+      a.out_color[hw + cp] = fma(pix.T, bg[1], pix.C1);
+      a.out_color[2 * hw + cp] = fma(pix.T, bg[2], pix.C2);
+    }
+    const uint32_t wm = __reduce_max_sync(0xffffffffu, pix.last);
+    if (lane == 0 && wm != 0u) atomicMax(&a.tile_max[tile], wm);
+  };
+  for (uint32_t k = 0;; ++k) {
+    const int st = int(k % kQStages);
+    const uint32_t ph = (k / kQStages) & 1u;
+    if (!queue_wait(&s.ready_bar[st], ph, abort, limit, a.error)) return;
+    // already complete (the producer waited for it): acquires the gathered
+    // records for this warp directly
+    if (!queue_wait(&s.data_bar[st], ph, abort, limit, a.error)) return;
+    const QueueStage h = s.hdr[st];
+    if (h.first != 0 || h.tile < 0) {
+      finish();
+      if (h.tile < 0) return;
+      tile = h.tile;
+      int ltile = tile;
+      W = a.W;
+      H = a.H;
+      pbase = 0;
+      bg = a.bg;
+      if (a.items != nullptr) {
+        const BatchItem& it = a.items[find_item_tile(a.items, a.num_items, uint32_t(tile))];
+        W = it.W;
+        H = it.H;
+        ltile = tile - int(it.tile_base);
+        pbase = size_t(it.pix_base);
+        bg = it.bg;
+      }
+      first_block = h.part * kW;
+      tp = TilePixel(ltile, (W + kTile - 1) / kTile, first_block + warp);
+      pxf = float(tp.px);
+      pyf = float(tp.py);
+      pix = BlendPixel();
+      pix.done = !(tp.px < W && tp.py < H);
+      have = true;
+      reported = false;
+    }
+    if (!__all_sync(0xffffffffu, pix.done)) {
+      const float4* sr = s.rec[st];
+      // this warp's entries of the stage, in order
+      int cnt = 0;
+      const uint32_t lt = (1u << lane) - 1u;
+#pragma unroll
+      for (int c = 0; c < kBatch / 32; ++c) {
+        const uint32_t bits = s.bal[st][warp][c];
+        if ((bits >> lane) & 1u) s.list[warp][cnt + __popc(bits & lt)] = uint8_t(32 * c + lane);
+        cnt += __popc(bits);
+      }
+      __syncwarp();
+      const uint8_t* lst = s.list[warp];
+      const uint32_t base = uint32_t(h.base) + 1u;
+      for (int k0 = 0; k0 < cnt; k0 += kBlendIlp) {
+        const uint32_t packed = *reinterpret_cast<const uint32_t*>(lst + k0);
+        int j[kBlendIlp];
+#pragma unroll
+        for (int kk = 0; kk < kBlendIlp; ++kk) j[kk] = k0 + kk < cnt ? int((packed >> (8 * kk)) & 255u) : -1;
+        float al[kBlendIlp], num[kBlendIlp], m[kBlendIlp];
+        float4 q1[kBlendIlp], q2[kBlendIlp];
+        bool in_range = true;
+#pragma unroll
+        for (int kk = 0; kk < kBlendIlp; ++kk) {
+          const int jj = j[kk] < 0 ? j[0] : j[kk];
+          const float4 q0 = sr[kQRec * jj];
+          q1[kk] = sr[kQRec * jj + 1];
+          q2[kk] = sr[kQRec * jj + 2];
+          num[kk] = gauss_num(pxf, pyf, q0.x, q0.y, q0.z, q0.w, q1[kk].x);
+          in_range = in_range && div_in_range(num[kk], q1[kk].y);
+        }
+        if (__all_sync(0xffffffffu, in_range)) {
+#pragma unroll
+          for (int kk = 0; kk < kBlendIlp; ++kk) m[kk] = div_markstein(num[kk], q1[kk].y);
+        } else {
+#pragma unroll
+          for (int kk = 0; kk < kBlendIlp; ++kk) m[kk] = div(num[kk], q1[kk].y);
+        }
+#pragma unroll
+        for (int kk = 0; kk < kBlendIlp; ++kk)
+          al[kk] = j[kk] < 0 ? 0.0f : fminf(0.99f, mul(q1[kk].z, gauss_from_m(m[kk])));
+#pragma unroll
+        for (int kk = 0; kk < kBlendIlp; ++kk) pix.step(al[kk], q1[kk], q2[kk], base + uint32_t(j[kk]));
+        if (__all_sync(0xffffffffu, pix.done)) break;
+      }
+    }
+    if (!reported && __all_sync(0xffffffffu, pix.done)) {
+      reported = true;
+      if (lane == 0) atomicAdd(&s.done[h.seq & 3], 1u);
+    }
+    __syncwarp();
+    if (lane == 0) tma::bar_arrive(&s.empty_bar[st]);
+  }
+}
+
 }  // namespace
 
 // Bucket sort of the tiles by decreasing list length (quarter-octave buckets;
 // order within a bucket is arbitrary).  One CTA.
 __global__ void __launch_bounds__(1024) tile_order_kernel(const uint2* ranges, const uint32_t* counts, int num_tiles,
-                                                          uint32_t* order, uint32_t* zero) {
+                                                          uint32_t* order, uint32_t* zero, uint32_t* counter) {
+  if (counter != nullptr && threadIdx.x == 0) *counter = 0u;
   constexpr int kBuckets = 130;
   __shared__ uint32_t s_cnt[kBuckets];
   __shared__ uint32_t s_pos[kBuckets];
@@ -231,21 +545,91 @@ __global__ void __launch_bounds__(1024) tile_order_kernel(const uint2* ranges, c
   for (int t = threadIdx.x; t < num_tiles; t += blockDim.x) order[atomicAdd(&s_pos[bucket(weight(t))], 1u)] = uint32_t(t);
 }
 
+namespace {
+
+// The driver's tensor-map encoder, looked up once through the runtime (the
+// library links only the runtime).
+using EncodeTiled = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                 const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                 CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+EncodeTiled encoder() {
+  static std::once_flag once;
+  static EncodeTiled fn = nullptr;
+  std::call_once(once, [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q{};
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<EncodeTiled>(p);
+  });
+  return fn;
+}
+
+// The records as a 2-D tensor of num_records rows of 16 floats (64 bytes),
+// gathered one row per index (box: one row).  False when the map cannot be
+// made (no encoder, a base not 16-byte aligned, no rows).
+bool record_map(const BlendArgs& a, CUtensorMap* map) {
+  if (a.record == nullptr || a.num_records == 0u || (reinterpret_cast<uintptr_t>(a.record) & 15u) != 0u) return false;
+  const EncodeTiled enc = encoder();
+  if (enc == nullptr) return false;
+  const cuuint64_t dims[2] = {16u, cuuint64_t(a.num_records)};
+  const cuuint64_t strides[1] = {64u};
+  const cuuint32_t box[2] = {16u, 1u};
+  const cuuint32_t elem[2] = {1u, 1u};
+  return enc(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<float*>(a.record), dims, strides, box, elem,
+             CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+// Persistent grid: every CTA the SMs hold at once (at most one per item).
+template <int kW>
+bool launch_queue(const BlendArgs& a, int tiles, cudaStream_t stream) {
+  CUtensorMap map;
+  if (a.queue == nullptr || !record_map(a, &map)) return false;
+  constexpr int threads = 32 * (kW + 1);
+  constexpr size_t smem = queue_smem_bytes<kW>();
+  static std::once_flag once;
+  static int per_sm = 0;
+  std::call_once(once, [] {
+    if (cudaFuncSetAttribute(blend_queue_kernel<kW>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)) ==
+        cudaSuccess)
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, blend_queue_kernel<kW>, threads, smem);
+  });
+  if (per_sm <= 0) return false;
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const int items = tiles * (8 / kW);
+  const int grid = std::min(items, sms * per_sm);
+  BlendArgs b = a;
+  b.total_tiles = tiles;  // the queue's length (a single-view call leaves it unset)
+  blend_queue_kernel<kW><<<grid, threads, smem, stream>>>(b, map);
+  return true;
+}
+
+}  // namespace
+
 void launch_blend(const BlendArgs& a, cudaStream_t stream) {
   const int tiles = a.items ? a.total_tiles : ((a.W + kTile - 1) / kTile) * ((a.H + kTile - 1) / kTile);
   if (tiles <= 0) return;
   const int warps = tune_value(kTuneBlendWarps);
+  const bool queue = tune_value(kTuneBlendQueue) == 1 && a.queue != nullptr;
   stage_begin(kStOther, stream);
-  // with two CTAs per tile they combine their maxima with atomics: clear first
-  tile_order_kernel<<<1, 1024, 0, stream>>>(a.ranges, nullptr, tiles, a.order, warps == 4 ? a.tile_max : nullptr);
+  // with two CTAs per tile (or the queue) the tile's maxima combine with
+  // atomics: clear first; the queue counter starts at zero
+  tile_order_kernel<<<1, 1024, 0, stream>>>(a.ranges, nullptr, tiles, a.order,
+                                            (warps == 4 || queue) ? a.tile_max : nullptr, queue ? a.queue : nullptr);
   stage_end(kStOther, stream, 1);
   stage_begin(kStBlend, stream);
-  if (warps == 4) blend_kernel<4><<<tiles * 2, 128, 0, stream>>>(a);
-  else blend_kernel<8><<<tiles, 256, 0, stream>>>(a);
+  const bool queued = queue && (warps == 4 ? launch_queue<4>(a, tiles, stream) : launch_queue<8>(a, tiles, stream));
+  if (!queued) {
+    if (warps == 4) blend_kernel<4><<<tiles * 2, 128, 0, stream>>>(a);
+    else blend_kernel<8><<<tiles, 256, 0, stream>>>(a);
+  }
   stage_end(kStBlend, stream, 1);
   // the backward's order: by the largest contributor count the blend just found
   stage_begin(kStOther, stream);
-  tile_order_kernel<<<1, 1024, 0, stream>>>(nullptr, a.tile_max, tiles, a.order_bwd, nullptr);
+  tile_order_kernel<<<1, 1024, 0, stream>>>(nullptr, a.tile_max, tiles, a.order_bwd, nullptr, nullptr);
   stage_end(kStOther, stream, 1);
 }
 

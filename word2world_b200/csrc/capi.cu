@@ -499,6 +499,9 @@ int w2w_forward_render(const w2w_settings* s, const void* geom_state, const w2w_
   b.tile_max = at<uint32_t>(image_state, IL.tile_max);
   b.order = at<uint32_t>(image_state, IL.order);
   b.order_bwd = at<uint32_t>(image_state, IL.order_bwd);
+  b.queue = at<uint32_t>(image_state, IL.queue);
+  b.error = const_cast<uint32_t*>(static_cast<const uint32_t*>(err_word));
+  b.spin_limit = spin_limit();
   launch_blend(b, st);
   return finish(err_word, st);
 }
@@ -880,6 +883,8 @@ int w2w_blend(const w2w_settings* s, const void* geom_state, const uint32_t* ran
   b.tile_max = at<uint32_t>(image_state, IL.tile_max);
   b.order = at<uint32_t>(image_state, IL.order);
   b.order_bwd = at<uint32_t>(image_state, IL.order_bwd);
+  b.queue = at<uint32_t>(image_state, IL.queue);
+  b.spin_limit = spin_limit();
   launch_blend(b, S(stream));
   return check_launch();
 }
@@ -1150,6 +1155,9 @@ int w2w_batch_forward_render(const w2w_batch_item* items, int n, const void* geo
   b.tile_max = at<uint32_t>(image_state, IL.tile_max);
   b.order = at<uint32_t>(image_state, IL.order);
   b.order_bwd = at<uint32_t>(image_state, IL.order_bwd);
+  b.queue = at<uint32_t>(image_state, IL.queue);
+  b.error = const_cast<uint32_t*>(static_cast<const uint32_t*>(err_word));
+  b.spin_limit = spin_limit();
   launch_blend(b, st);
   return finish(err_word, st);
 }

@@ -371,7 +371,7 @@ struct GeomLayout {
 };
 
 struct ImageLayout {
-  size_t n_contrib, ranges, T_final, tile_max, order, order_bwd, total;
+  size_t n_contrib, ranges, T_final, tile_max, order, order_bwd, queue, total;
   __host__ __device__ ImageLayout(int W, int H)
       : ImageLayout(size_t(W) * size_t(H), size_t((W + kTile - 1) / kTile) * size_t((H + kTile - 1) / kTile)) {}
   // a batch: all items' pixels and tiles back to back
@@ -384,6 +384,7 @@ struct ImageLayout {
     tile_max = take(tiles * 4);
     order = take(tiles * 4);
     order_bwd = take(tiles * 4);
+    queue = take(4);  // the persistent blend's tile queue counter
     total = align256(o);
   }
 };

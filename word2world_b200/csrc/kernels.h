@@ -163,6 +163,9 @@ struct BlendArgs {
   uint32_t* tile_max;
   uint32_t* order;      // tiles by decreasing list length (the blend's processing order)
   uint32_t* order_bwd;  // tiles by decreasing largest contributor count (the backward's)
+  uint32_t* queue;      // the persistent blend's queue counter (cleared before its launch), or null
+  uint32_t* error;      // error word for the persistent blend's bounded waits, or null
+  uint32_t spin_limit = kSpinLimit;
 };
 void launch_blend(const BlendArgs& a, cudaStream_t stream);
 
@@ -328,7 +331,14 @@ long long unpublished_tile(int stage);
 // The fourth knob picks how a single-view call builds its sorted list: 0 key
 // emission + radix sort (duplicate.cu, sort.cu), 1 binning from the
 // depth-ordered Gaussians (binning.cu); both give the same list.
-enum TuneKnob { kTuneBlendWarps = 0, kTuneBwdSplit = 1, kTuneBwdWays = 2, kTuneBinning = 3, kNumTuneKnobs = 4 };
+enum TuneKnob {
+  kTuneBlendWarps = 0,
+  kTuneBwdSplit = 1,
+  kTuneBwdWays = 2,
+  kTuneBinning = 3,
+  kTuneBlendQueue = 4,
+  kNumTuneKnobs = 5
+};
 int tune_value(int knob);
 
 size_t scan_scratch_bytes(long long n);

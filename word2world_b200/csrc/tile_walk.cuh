@@ -52,9 +52,10 @@ struct TilePixel {
 // from `ranges`, or `counts` when given), so the heaviest start in the first
 // wave instead of wherever the raster order puts them.
 // `zero`, when given, is cleared over num_tiles entries on the way (the
-// blend's per-tile maximum, which its CTAs then combine).
+// blend's per-tile maximum, which its CTAs then combine), and `counter`, when
+// given, set to zero (the persistent blend's queue).
 __global__ void tile_order_kernel(const uint2* ranges, const uint32_t* counts, int num_tiles, uint32_t* order,
-                                  uint32_t* zero);
+                                  uint32_t* zero, uint32_t* counter);
 
 // One entry's record held in registers between its gather and its store.
 struct ChunkLoad {

@@ -70,14 +70,15 @@ std::atomic<long long> g_unpublished[kNumWaitStages] = {{-1}, {-1}, {-1}};
 uint32_t spin_limit() { return g_spin_limit.load(std::memory_order_relaxed); }
 
 namespace {
-const char* kTuneNames[kNumTuneKnobs] = {"blend_warps", "backward_split", "backward_ways", "binning"};
-std::atomic<int> g_tune[kNumTuneKnobs] = {{4}, {4}, {2}, {0}};
+const char* kTuneNames[kNumTuneKnobs] = {"blend_warps", "backward_split", "backward_ways", "binning", "blend_queue"};
+std::atomic<int> g_tune[kNumTuneKnobs] = {{4}, {4}, {2}, {0}, {0}};
 bool tune_valid(int knob, int v) {
   switch (knob) {
     case kTuneBlendWarps: return v == 4 || v == 8;
     case kTuneBwdSplit: return v >= 0 && v <= 16;
     case kTuneBwdWays: return v == 2 || v == 3;
     case kTuneBinning: return v == 0 || v == 1;
+    case kTuneBlendQueue: return v == 0 || v == 1;
     default: return false;
   }
 }
