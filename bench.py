@@ -62,6 +62,8 @@ def parse():
     ap.add_argument("--no-batched", action="store_true", help="skip the batched-call measurement of the workload")
     ap.add_argument("--no-autotune", action="store_true",
                     help="keep the default launch shapes instead of tuning them on the workload first")
+    ap.add_argument("--tune", default="",
+                    help="launch-shape knobs to use instead of tuning, e.g. blend_queue=1,blend_warps=4")
     ap.add_argument("--single-stream", action="store_true",
                     help="run a step's views one after another on one stream (default: one stream per view)")
     ap.add_argument("--config", default="single", choices=["single", "multiscene", "serve", "sortscan"],
@@ -288,7 +290,13 @@ def run_ours(a):
             plans.append(d)
             del out
     tuning = None
-    if not a.no_autotune:
+    if a.tune:
+        # launch shapes given on the command line (no tuning run)
+        from word2world_b200 import autotune
+        knobs = {k: int(v) for k, v in (kv.split("=") for kv in a.tune.split(","))}
+        autotune.apply(knobs)
+        tuning = {"knobs": autotune.current(), "given": True}
+    elif not a.no_autotune:
         # launch shapes tuned on this workload's own step (word2world_b200.autotune)
         from word2world_b200 import autotune
         for _ in range(3):  # settle clocks and caches before the first trial

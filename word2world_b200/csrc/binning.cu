@@ -68,10 +68,14 @@ __device__ __forceinline__ Owned owned_of(const BinArgs& a, uint32_t g) {
 }
 
 // Depth-order owned counts (gathered through the sort's permutation), the
-// input of the prefix scan.
+// input of the prefix scan.  A permutation entry of P or more (left by a depth
+// sort whose bounded wait ran out, which its error word reports) owns nothing
+// and is never used as an index.
 __global__ void owned_count_kernel(BinArgs a, uint32_t* __restrict__ count) {
   const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
-  if (j < uint32_t(a.P)) count[j] = owned_of(a, a.order[j]).count;
+  if (j >= uint32_t(a.P)) return;
+  const uint32_t g = a.order[j];
+  count[j] = g < uint32_t(a.P) ? owned_of(a, g).count : 0u;
 }
 
 // Depth-order index whose position range holds each warp share's first
@@ -99,8 +103,8 @@ __device__ __forceinline__ void walk_positions(const BinArgs& a, uint32_t pa, ui
     float inv_w = 1.0f;
     if (jj < uint32_t(a.P)) {
       const uint32_t lo = max(a.dprefix[jj], pos), hi = min(a.dprefix[jj + 1], pb);
-      if (hi > lo) {
-        g = a.order[jj];
+      g = a.order[jj];
+      if (hi > lo && g < uint32_t(a.P)) {  // (an out-of-range entry: see owned_count_kernel)
         const Owned o = owned_of(a, g);
         cnt = hi - lo;
         k0 = o.first_k + (lo - a.dprefix[jj]);

@@ -205,18 +205,22 @@ __global__ void __launch_bounds__(32 * kBlendWarps, 16 / kBlendWarps) blend_kern
 // tile for kW = 8) and one producer warp, for as long as the queue (tile
 // halves in the heaviest-first order; every item of a batched call in one
 // queue) has items.  The producer takes the next item with an atomic, reads
-// a batch's Gaussian ids from the list and gathers their 64-byte records
-// into one of kQStages shared-memory stages with TMA (four rows per gather),
-// then computes every staged entry's block bits once (as the cooperative
-// staging does) and publishes the stage.  The consumers walk each stage as
-// the per-tile kernel does and release it; a warp whose pixels have all
+// a batch's Gaussian ids from the list, writes the stage's header and the
+// bit mask of its valid entries, and gathers the entries' 64-byte records into
+// one of kQStages shared-memory stages with TMA (four rows per gather),
+// completing on the stage's barrier.  Each consumer warp waits for that
+// barrier, tests the staged entries against its own 8x4 block (block_test,
+// as the backward's warps do), walks the ones that can reach it as the
+// per-tile kernel does, and releases the stage.  A warp whose pixels have all
 // terminated tells the producer, which skips the rest of a tile once every
 // consumer warp has.  The stages run across tile boundaries, so a CTA never
 // drains its pipeline between tiles, and no warp waits at a CTA barrier for
 // the slowest warp of a batch: warps drift apart by up to kQStages batches.
-// Every wait is bounded (spin_limit polls); one that runs out sets
-// kErrTimeout in `error`, and the CTA stops after its copies in flight land.
-// Results are bit-identical to blend_kernel's (same entries, same order).
+// This blend writes no block masks: it clears the binning state's flag, and
+// the backward tests each entry itself.
+// Every wait is bounded; one that runs out sets kErrTimeout in `error`, and
+// the CTA stops after its copies in flight land.  Results are bit-identical
+// to blend_kernel's (same entries, same order).
 // ---------------------------------------------------------------------------
 constexpr int kQStages = 3;
 constexpr int kQRec = 4;  // float4s per staged record (the whole record)
@@ -225,19 +229,18 @@ struct QueueStage {
   int tile;   // tile id (-1: the queue is empty, stop)
   int part;   // tile half (kW = 4) or 0
   int base;   // list position of the batch's first entry, from the tile's start
-  int count;  // entries in the batch
   int seq;    // the CTA's item number
   int first;  // 1: the item's first batch
+  int pad[3];
 };
 
 template <int kW>
 struct __align__(128) QueueShared {
   float4 rec[kQStages][kBatch * kQRec];  // 16 KB per stage; gathers land 256 B at a time
-  uint32_t bal[kQStages][kW][kBatch / 32];
+  uint32_t valid[kQStages][kBatch / 32];  // bit j of word c: entry 32c + j holds a valid id
   QueueStage hdr[kQStages];
   uint8_t list[kW][kBatch];
-  unsigned long long data_bar[kQStages];   // the stage's gathers landed
-  unsigned long long ready_bar[kQStages];  // the stage's block bits and header are written
+  unsigned long long full_bar[kQStages];   // header written and the stage's gathers landed
   unsigned long long empty_bar[kQStages];  // every consumer warp is done with the stage
   uint32_t done[4];                        // per item (seq mod 4): consumer warps whose pixels all terminated
   uint32_t abort;
@@ -248,18 +251,18 @@ constexpr size_t queue_smem_bytes() {
   return sizeof(QueueShared<kW>) + 128;  // + alignment slack of the dynamic shared memory base
 }
 
-// Bounded wait on `bar`'s phase `parity`: at most `limit` polls, spaced by a
-// short sleep after the first few (well under a second at the default
+// Bounded wait on `bar`'s phase `parity`: hardware-suspended waits of at
+// most kQWaitNs each, limit / 256 + 4 of them (about 0.16 s at the default
 // limit).  False when it ran out (or another warp's did), after flagging the
-// CTA and the call.
-// Warp-collective: every lane polls (so each acquires the phase itself) and
-// the warp decides together, so its lanes never part ways.
+// CTA and the call.  Warp-collective: every lane waits (so each acquires the
+// phase itself) and the warp decides together, so its lanes never part ways.
+constexpr uint32_t kQWaitNs = 10000;
 __device__ __forceinline__ bool queue_wait(unsigned long long* bar, uint32_t parity, volatile uint32_t* abort,
                                            uint32_t limit, uint32_t* error) {
-  for (uint32_t i = 0; i < limit; ++i) {
-    if (__all_sync(0xffffffffu, tma::bar_test(bar, parity))) return true;
+  const uint32_t tries = (limit >> 8) + 4u;
+  for (uint32_t i = 0; i < tries; ++i) {
+    if (__all_sync(0xffffffffu, tma::bar_try_wait(bar, parity, kQWaitNs))) return true;
     if (__any_sync(0xffffffffu, *abort != 0u)) return false;
-    if (i >= 32u) __nanosleep(64);
   }
   if ((threadIdx.x & 31u) == 0u) {
     *abort = 1u;
@@ -268,9 +271,54 @@ __device__ __forceinline__ bool queue_wait(unsigned long long* bar, uint32_t par
   return false;
 }
 
+// The producer's position in the queue: its current item (tile part) and
+// the next batch of it to stage.  Warp-uniform.
+struct QueueCursor {
+  int tile = -1, part = 0, n = 0, nb = 1, b = 0;
+  uint32_t rx = 0;
+  bool end = true;
+
+  // Take the next item (lane 0's atomic, broadcast) as item number `seq`;
+  // clears that item's slot of `done` (seen by the consumers through the
+  // item's first stage).
+  template <int kW>
+  __device__ __forceinline__ void fetch(const BlendArgs& a, uint32_t* done, uint32_t seq, int lane) {
+    constexpr int kParts = 8 / kW;
+    int item = 0;
+    if (lane == 0) {
+      item = int(atomicAdd(a.queue, 1u));
+      done[seq & 3u] = 0u;
+    }
+    item = __shfl_sync(0xffffffffu, item, 0);
+    end = item >= a.total_tiles * kParts;
+    b = 0;
+    if (end) {
+      tile = -1;
+      part = 0;
+      n = 0;
+      nb = 1;
+      rx = 0;
+      return;
+    }
+    tile = int(a.order[item / kParts]);
+    part = item % kParts;
+    const uint2 range = a.ranges[tile];
+    rx = range.x;
+    n = int(range.y - range.x);
+    nb = max(1, (n + kBatch - 1) / kBatch);  // an empty list still has its pixels written
+  }
+};
+
+// Every consumer warp of item `seq` has terminated (lane 0 reads, the warp agrees).
+template <int kW>
+__device__ __forceinline__ bool queue_all_done(const uint32_t* done, uint32_t seq, int lane) {
+  uint32_t d = 0;
+  if (lane == 0) d = *reinterpret_cast<const volatile uint32_t*>(&done[seq & 3u]);
+  return __shfl_sync(0xffffffffu, d, 0) == uint32_t(kW);
+}
+
 template <int kW>
 __global__ void __launch_bounds__(32 * (kW + 1)) blend_queue_kernel(BlendArgs a, const __grid_constant__ CUtensorMap map) {
-  constexpr int kParts = 8 / kW;
   extern __shared__ unsigned char q_raw[];
   QueueShared<kW>& s = *reinterpret_cast<QueueShared<kW>*>((reinterpret_cast<uintptr_t>(q_raw) + 127) & ~uintptr_t(127));
   const int warp = int(threadIdx.x >> 5), lane = int(threadIdx.x & 31);
@@ -278,116 +326,74 @@ __global__ void __launch_bounds__(32 * (kW + 1)) blend_queue_kernel(BlendArgs a,
   volatile uint32_t* abort = &s.abort;
   if (threadIdx.x == 0) {
     for (int i = 0; i < kQStages; ++i) {
-      tma::bar_init(&s.data_bar[i], 1);
-      tma::bar_init(&s.ready_bar[i], 32);
+      tma::bar_init(&s.full_bar[i], 1);
       tma::bar_init(&s.empty_bar[i], kW);
     }
     s.abort = 0u;
     tma::bar_init_fence();
+    // this blend leaves no block masks for the backward passes
+    if (blockIdx.x == 0 && a.masks_valid != nullptr) *a.masks_valid = 0u;
   }
   if (threadIdx.x == 32 * kW) tma::prefetch_map(&map);
   __syncthreads();
-  const int total_items = a.total_tiles * kParts;  // every tile's parts (all items' tiles in a batched call)
 
   if (warp == kW) {
     // ---------------- producer ----------------
-    uint32_t k = 0;       // stages published
-    uint32_t seq = 0;
-    bool in_flight = false;  // gathers issued on stage (k % kQStages) not yet waited for
-    for (;; ++seq) {
-      int item = 0;
-      if (lane == 0) item = int(atomicAdd(a.queue, 1u));
-      item = __shfl_sync(0xffffffffu, item, 0);
-      const bool end = item >= total_items;
-      int tile = -1, part = 0, n = 0, X0 = 0, Y0 = 0;
-      uint2 range = make_uint2(0u, 0u);
-      if (!end) {
-        tile = int(a.order[item / kParts]);
-        part = item % kParts;
-        range = a.ranges[tile];
-        n = int(range.y - range.x);
-        int W = a.W, ltile = tile;
-        if (a.items != nullptr) {
-          const BatchItem& it = a.items[find_item_tile(a.items, a.num_items, uint32_t(tile))];
-          W = it.W;
-          ltile = tile - int(it.tile_base);
+    QueueCursor cur;
+    uint32_t seq = 0, k = 0;
+    cur.fetch<kW>(a, s.done, seq, lane);
+    for (;; ++k) {
+      if (cur.b > 0 && (cur.b >= cur.nb || queue_all_done<kW>(s.done, seq, lane))) cur.fetch<kW>(a, s.done, ++seq, lane);
+      const int st = int(k % kQStages);
+      if (!queue_wait(&s.empty_bar[st], ((k / kQStages) & 1u) ^ 1u, abort, limit, a.error)) goto stop;
+      const int base = cur.b * kBatch;
+      const int cnt = cur.end ? 0 : min(kBatch, cur.n - base);
+      const int groups = (cnt + 3) >> 2;
+      // lane l gathers groups l and l + 32 (entries 4g .. 4g + 3)
+      const uint32_t* ids = a.point_list + cur.rx + base;
+      int r[2][4];
+      uint32_t vbits = 0;  // bit 4h + q: entry 4 (l + 32h) + q holds a valid id
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const int g = lane + 32 * h;
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          const int e = 4 * g + q;
+          const uint32_t id = e < cnt ? ids[e] : a.num_records;
+          const bool ok = id < a.num_records;
+          vbits |= ok ? 1u << (4 * h + q) : 0u;
+          r[h][q] = ok ? int(id) : 0;  // a stray id gathers row 0 and stays invalid
         }
-        const int gw = (W + kTile - 1) / kTile;
-        X0 = (ltile % gw) * kTile;
-        Y0 = (ltile / gw) * kTile + kBlockH * (part * kW / 2);
       }
-      if (lane == 0) s.done[seq & 3] = 0u;  // published to the consumers by this item's first stage
-      uint8_t* lo_dst = a.mask_top == nullptr ? nullptr : (part == 0 ? a.mask_top : a.mask_bottom) + range.x;
-      uint8_t* hi_dst = a.mask_top == nullptr || kParts != 1 ? nullptr : a.mask_bottom + range.x;
-      const int nb = end ? 1 : max(1, (n + kBatch - 1) / kBatch);
-      for (int b = 0; b < nb; ++b) {
-        // every consumer warp of the item has terminated: skip its other batches
-        uint32_t done = 0;
-        if (lane == 0) done = *reinterpret_cast<volatile uint32_t*>(&s.done[seq & 3]);
-        if (b > 0 && __shfl_sync(0xffffffffu, done, 0) == uint32_t(kW)) break;
-        const int st = int(k % kQStages);
-        const uint32_t ph = (k / kQStages) & 1u;
-        if (!queue_wait(&s.empty_bar[st], ph ^ 1u, abort, limit, a.error)) goto stop;
-        const int base = b * kBatch;
-        const int cnt = end ? 0 : min(kBatch, n - base);
-        const int groups = (cnt + 3) >> 2;
-        // every stage completes one phase of its data barrier (an empty one
-        // with no bytes), so its parity follows the stage count
-        if (lane == 0) tma::bar_arrive_expect(&s.data_bar[st], uint32_t(groups) * 4u * 64u);
-        __syncwarp();
-        in_flight = true;
-        const uint32_t* ids = a.point_list + range.x + base;
-        if (cnt > 0) {
-          for (int g = lane; g < groups; g += 32) {
-            int r[4];
+      // the stage's valid-entry words and header, by lane 0, before its
+      // arrival (which releases them to the consumers)
 #pragma unroll
-            for (int q = 0; q < 4; ++q) {
-              const int e = 4 * g + q;
-              const uint32_t id = e < cnt ? ids[e] : 0u;
-              r[q] = id < a.num_records ? int(id) : 0;  // a stray id gathers row 0; its bits stay clear
-            }
-            tma::gather4(&s.rec[st][kQRec * 4 * g], &map, &s.data_bar[st], r[0], r[1], r[2], r[3]);
-          }
-        }
-        if (!queue_wait(&s.data_bar[st], ph, abort, limit, a.error)) goto stop;
-        in_flight = false;
-        if (cnt > 0) {
-          // every staged entry's block bits, once for the CTA's kW blocks
-#pragma unroll 1
-          for (int c = 0; c < kBatch / 32; ++c) {
-            const int j = 32 * c + lane;
-            uint32_t mask = 0;
-            if (j < cnt && ids[j] < a.num_records) {
-              const float4* r = &s.rec[st][kQRec * j];
-              const float4 r0 = r[0], r2 = r[2], r3 = r[3];
-              mask = block_mask<kW / 2>(r0.x, r0.y, r2.w, r3.x, r3.y, r3.z, r3.w, X0, Y0);
-              if (lo_dst != nullptr) lo_dst[base + j] = uint8_t(mask & 15u);
-              if (hi_dst != nullptr) hi_dst[base + j] = uint8_t(mask >> 4);
-            }
-            uint32_t mine = 0;
-#pragma unroll
-            for (int bb = 0; bb < kW; ++bb) {
-              const uint32_t w = __ballot_sync(0xffffffffu, (mask >> bb) & 1u);
-              if (lane == bb) mine = w;
-            }
-            if (lane < kW) s.bal[st][lane][c] = mine;
-          }
-        } else if (lane < kW) {
-#pragma unroll
-          for (int c = 0; c < kBatch / 32; ++c) s.bal[st][lane][c] = 0u;
-        }
-        if (lane == 0) s.hdr[st] = QueueStage{tile, part, base, cnt, int(seq), b == 0 ? 1 : 0};
-        tma::bar_arrive(&s.ready_bar[st]);  // every lane, after its own writes
-        ++k;
+      for (int c = 0; c < kBatch / 32; ++c) {
+        const int j = 32 * c + lane, g = j >> 2;
+        const uint32_t w = __ballot_sync(0xffffffffu, (__shfl_sync(0xffffffffu, vbits, g & 31) >> (4 * (g >> 5) + (j & 3))) & 1u);
+        if (lane == 0) s.valid[st][c] = w;
       }
-      if (end) break;
+      if (lane == 0) {
+        s.hdr[st] = QueueStage{cur.tile, cur.part, base, int(seq), cur.b == 0 ? 1 : 0, {0, 0, 0}};
+        tma::bar_arrive_expect(&s.full_bar[st], uint32_t(groups) * 4u * 64u);  // an empty stage completes at once
+      }
+      __syncwarp();
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const int g = lane + 32 * h;
+        if (g < groups) tma::gather4(&s.rec[st][kQRec * 4 * g], &map, &s.full_bar[st], r[h][0], r[h][1], r[h][2], r[h][3]);
+      }
+      ++cur.b;
+      if (cur.end) break;
     }
     return;
   stop:
-    // a wait ran out: let the copies in flight land before the CTA ends
-    if (in_flight) {
-      const int st = int(k % kQStages);
-      for (uint32_t i = 0; i < limit && !tma::bar_test(&s.data_bar[st], (k / kQStages) & 1u); ++i) __nanosleep(64);
+    // a wait ran out: let the copies of the stages issued last land before the CTA ends
+    for (uint32_t kk = k > uint32_t(kQStages) ? k - kQStages : 0u; kk < k; ++kk) {
+      const int st = int(kk % kQStages);
+      for (uint32_t i = 0; i < (limit >> 8) + 4u && !tma::bar_try_wait(&s.full_bar[st], (kk / kQStages) & 1u, kQWaitNs);
+           ++i) {
+      }
     }
     return;
   }
@@ -396,7 +402,7 @@ __global__ void __launch_bounds__(32 * (kW + 1)) blend_queue_kernel(BlendArgs a,
   BlendPixel pix;
   pix.done = true;
   bool have = false, reported = true;
-  int tile = -1, W = 0, H = 0, first_block = 0;
+  int tile = -1, W = 0, H = 0;
   size_t pbase = 0;
   const float* bg = a.bg;
   TilePixel tp(0, 1, warp);
@@ -418,13 +424,10 @@ __global__ void __launch_bounds__(32 * (kW + 1)) blend_queue_kernel(BlendArgs a,
     const uint32_t wm = __reduce_max_sync(0xffffffffu, pix.last);
     if (lane == 0 && wm != 0u) atomicMax(&a.tile_max[tile], wm);
   };
+  const uint32_t lt = (1u << lane) - 1u;
   for (uint32_t k = 0;; ++k) {
     const int st = int(k % kQStages);
-    const uint32_t ph = (k / kQStages) & 1u;
-    if (!queue_wait(&s.ready_bar[st], ph, abort, limit, a.error)) return;
-    // already complete (the producer waited for it): acquires the gathered
-    // records for this warp directly
-    if (!queue_wait(&s.data_bar[st], ph, abort, limit, a.error)) return;
+    if (!queue_wait(&s.full_bar[st], (k / kQStages) & 1u, abort, limit, a.error)) return;
     const QueueStage h = s.hdr[st];
     if (h.first != 0 || h.tile < 0) {
       finish();
@@ -443,8 +446,7 @@ __global__ void __launch_bounds__(32 * (kW + 1)) blend_queue_kernel(BlendArgs a,
         pbase = size_t(it.pix_base);
         bg = it.bg;
       }
-      first_block = h.part * kW;
-      tp = TilePixel(ltile, (W + kTile - 1) / kTile, first_block + warp);
+      tp = TilePixel(ltile, (W + kTile - 1) / kTile, h.part * kW + warp);
       pxf = float(tp.px);
       pyf = float(tp.py);
       pix = BlendPixel();
@@ -454,13 +456,19 @@ __global__ void __launch_bounds__(32 * (kW + 1)) blend_queue_kernel(BlendArgs a,
     }
     if (!__all_sync(0xffffffffu, pix.done)) {
       const float4* sr = s.rec[st];
-      // this warp's entries of the stage, in order
+      // the stage's entries that can reach this warp's block, in order
       int cnt = 0;
-      const uint32_t lt = (1u << lane) - 1u;
-#pragma unroll
+#pragma unroll 2
       for (int c = 0; c < kBatch / 32; ++c) {
-        const uint32_t bits = s.bal[st][warp][c];
-        if ((bits >> lane) & 1u) s.list[warp][cnt + __popc(bits & lt)] = uint8_t(32 * c + lane);
+        const uint32_t vw = s.valid[st][c];
+        bool reach = false;
+        if ((vw >> lane) & 1u) {
+          const int j = 32 * c + lane;
+          const float4 r0 = sr[kQRec * j], r2 = sr[kQRec * j + 2], r3 = sr[kQRec * j + 3];
+          reach = block_test(r0.x, r0.y, r2.w, r3.x, r3.y, r3.z, r3.w, tp.bx, tp.by);
+        }
+        const uint32_t bits = __ballot_sync(0xffffffffu, reach);
+        if (reach) s.list[warp][cnt + __popc(bits & lt)] = uint8_t(32 * c + lane);
         cnt += __popc(bits);
       }
       __syncwarp();

@@ -491,6 +491,7 @@ int w2w_forward_render(const w2w_settings* s, const void* geom_state, const w2w_
     const BinLayout BL(R, T);
     b.mask_top = at<uint8_t>(binning_state, BL.masks);
     b.mask_bottom = b.mask_top + R;
+    b.masks_valid = &at<BinHeader>(binning_state, BL.header)->masks_valid;
   }
   b.bg = s->background;
   b.out_color = out_color; b.out_depth = out_depth; b.out_alpha = out_alpha;
@@ -1147,6 +1148,7 @@ int w2w_batch_forward_render(const w2w_batch_item* items, int n, const void* geo
     const BinLayout BL(R, T);
     b.mask_top = at<uint8_t>(binning_state, BL.masks);
     b.mask_bottom = b.mask_top + R;
+    b.masks_valid = &at<BinHeader>(binning_state, BL.header)->masks_valid;
   }
   b.bg = nullptr;
   b.out_color = out_color; b.out_depth = out_depth; b.out_alpha = out_alpha;

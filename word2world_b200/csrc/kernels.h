@@ -165,6 +165,7 @@ struct BlendArgs {
   uint32_t* order_bwd;  // tiles by decreasing largest contributor count (the backward's)
   uint32_t* queue;      // the persistent blend's queue counter (cleared before its launch), or null
   uint32_t* error;      // error word for the persistent blend's bounded waits, or null
+  uint32_t* masks_valid;  // the binning header's block-mask flag (the persistent blend clears it), or null
   uint32_t spin_limit = kSpinLimit;
 };
 void launch_blend(const BlendArgs& a, cudaStream_t stream);

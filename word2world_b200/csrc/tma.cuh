@@ -55,6 +55,21 @@ __device__ __forceinline__ bool bar_test(unsigned long long* bar, uint32_t parit
   return ok != 0u;
 }
 
+// Waits (suspended in hardware, woken when the phase completes) at most about
+// `hint_ns` nanoseconds for the phase with parity `parity`; true once it has
+// completed (acquire).
+__device__ __forceinline__ bool bar_try_wait(unsigned long long* bar, uint32_t parity, uint32_t hint_ns) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(smem_addr(bar)), "r"(parity), "r"(hint_ns)
+      : "memory");
+  return ok != 0u;
+}
+
 // Four rows (r0..r3) of `map` into dst (4 * row bytes, 128-byte aligned),
 // completing on `bar`.
 __device__ __forceinline__ void gather4(void* dst, const CUtensorMap* map, unsigned long long* bar, int r0, int r1,
