@@ -381,7 +381,9 @@ int w2w_throughput_probe(int kind, long long iters, int blocks, float* out, long
  * persistent blend, one CTA per resident slot, pulling tile parts from a
  * device queue in the same order, each CTA a producer warp that gathers the
  * batches' records with TMA into a three-stage shared-memory ring and
- * "blend_warps" consumer warps; default 0).
+ * "blend_warps" consumer warps; default 0), 5 "preprocess_blocks" (CTAs per
+ * SM the projection pass's register budget is sized for: 4 caps a thread at
+ * 64 registers, 3 at 80, 2 at 128; default 4).
  * Results do not depend on them beyond the order of float atomic additions.
  * w2w_tune_set returns the previous value, or -1 (and changes nothing) for an
  * unknown knob or value. */

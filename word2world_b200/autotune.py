@@ -34,6 +34,7 @@ CANDIDATES = {
     "backward_ways": [2, 3],
     "binning": [0, 1],
     "blend_queue": [0, 1],
+    "preprocess_blocks": [4, 3, 2],
 }
 
 

@@ -26,7 +26,7 @@ BUILD = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libw2w_raster.so")
 CUDA_SOURCES = ["preprocess.cu", "duplicate.cu", "sort.cu", "binning.cu", "blend.cu", "backward.cu", "scan.cu", "activate.cu",
                 "densify.cu", "voxel.cu", "groupsum.cu", "capi.cu", "timing.cu"]
-HEADERS = ["common.cuh", "kernels.h", "pinned_fp.h", "tile_walk.cuh"]
+HEADERS = ["common.cuh", "kernels.h", "pinned_fp.h", "tile_walk.cuh", "tma.cuh"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr"]

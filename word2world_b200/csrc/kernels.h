@@ -338,7 +338,8 @@ enum TuneKnob {
   kTuneBwdWays = 2,
   kTuneBinning = 3,
   kTuneBlendQueue = 4,
-  kNumTuneKnobs = 5
+  kTunePreBlocks = 5,
+  kNumTuneKnobs = 6
 };
 int tune_value(int knob);
 

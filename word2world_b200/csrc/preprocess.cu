@@ -236,8 +236,11 @@ __device__ __forceinline__ void sh_colour(const float* __restrict__ sh, int M, i
 // of each thread gathering its own 192-byte row.
 constexpr int kStageBytes = kPreThreads * kShStride * 4;
 
-template <bool kSh16, bool kRaw, bool kStage>
-__global__ void __launch_bounds__(kPreThreads, 4)
+// kMinBlocks: CTAs per SM the register budget is sized for (the tuning knob
+// "preprocess_blocks"): 4 caps a thread at 64 registers (some spill to local
+// memory), 3 at 80, 2 at 128 (none spill).
+template <bool kSh16, bool kRaw, bool kStage, int kMinBlocks>
+__global__ void __launch_bounds__(kPreThreads, kMinBlocks)
 preprocess_kernel(PreprocessArgs a) {
   __shared__ uint32_t s_tile;
   __shared__ Pair s_warp[kPreThreads / 32];
@@ -553,6 +556,28 @@ preprocess_kernel(PreprocessArgs a) {
 
 }  // namespace
 
+namespace {
+template <int kMinBlocks>
+void launch_preprocess_as(const PreprocessArgs& a, int blocks, bool raw, bool stage, bool sh16, cudaStream_t stream) {
+  // the dynamic shared-memory opt-in of the staging kernels, once per device
+  static bool opted[64] = {false};
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (stage && (dev < 0 || dev >= 64 || !opted[dev])) {
+    cudaFuncSetAttribute(preprocess_kernel<true, false, true, kMinBlocks>,
+                         cudaFuncAttributeMaxDynamicSharedMemorySize, kStageBytes);
+    cudaFuncSetAttribute(preprocess_kernel<false, true, true, kMinBlocks>,
+                         cudaFuncAttributeMaxDynamicSharedMemorySize, kStageBytes);
+    if (dev >= 0 && dev < 64) opted[dev] = true;
+  }
+  if (raw && stage) preprocess_kernel<false, true, true, kMinBlocks><<<blocks, kPreThreads, kStageBytes, stream>>>(a);
+  else if (raw) preprocess_kernel<false, true, false, kMinBlocks><<<blocks, kPreThreads, 0, stream>>>(a);
+  else if (stage) preprocess_kernel<true, false, true, kMinBlocks><<<blocks, kPreThreads, kStageBytes, stream>>>(a);
+  else if (sh16) preprocess_kernel<true, false, false, kMinBlocks><<<blocks, kPreThreads, 0, stream>>>(a);
+  else preprocess_kernel<false, false, false, kMinBlocks><<<blocks, kPreThreads, 0, stream>>>(a);
+}
+}  // namespace
+
 void launch_preprocess(const PreprocessArgs& a, cudaStream_t stream) {
   const int blocks = (a.P + kPreThreads - 1) / kPreThreads;
   if (blocks == 0) return;
@@ -565,23 +590,12 @@ void launch_preprocess(const PreprocessArgs& a, cudaStream_t stream) {
   const bool full_rows = a.M == 16 && (batched ? a.shs != nullptr : a.degree == 3);
   const bool stage = full_rows && (raw ? aligned16(a.sh_dc) && aligned16(a.sh_ac) : aligned16(a.shs));
   const bool sh16 = !raw && full_rows && aligned16(a.shs);
-  // the dynamic shared-memory opt-in of the staging kernels, once per device
-  static bool opted[64] = {false};
-  int dev = 0;
-  cudaGetDevice(&dev);
-  if (stage && (dev < 0 || dev >= 64 || !opted[dev])) {
-    cudaFuncSetAttribute(preprocess_kernel<true, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         kStageBytes);
-    cudaFuncSetAttribute(preprocess_kernel<false, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         kStageBytes);
-    if (dev >= 0 && dev < 64) opted[dev] = true;
-  }
   stage_begin(kStPreprocess, stream);
-  if (raw && stage) preprocess_kernel<false, true, true><<<blocks, kPreThreads, kStageBytes, stream>>>(a);
-  else if (raw) preprocess_kernel<false, true, false><<<blocks, kPreThreads, 0, stream>>>(a);
-  else if (stage) preprocess_kernel<true, false, true><<<blocks, kPreThreads, kStageBytes, stream>>>(a);
-  else if (sh16) preprocess_kernel<true, false, false><<<blocks, kPreThreads, 0, stream>>>(a);
-  else preprocess_kernel<false, false, false><<<blocks, kPreThreads, 0, stream>>>(a);
+  switch (tune_value(kTunePreBlocks)) {
+    case 2: launch_preprocess_as<2>(a, blocks, raw, stage, sh16, stream); break;
+    case 3: launch_preprocess_as<3>(a, blocks, raw, stage, sh16, stream); break;
+    default: launch_preprocess_as<4>(a, blocks, raw, stage, sh16, stream); break;
+  }
   stage_end(kStPreprocess, stream, 1);
 }
 
