@@ -68,16 +68,35 @@ struct Target {
   float* base;
   int mult, off;
   bool active;
+  bool second = false;  // flush_pair: the lane's value belongs to the second entry
 };
 
-__device__ __forceinline__ Target lane_target(const BackwardArgs& a, int mode) {
-  const int lane = threadIdx.x & 31, idx = (lane >> 1) & 15;
-  Target t{nullptr, 0, 0, (lane & 1) == 0 && idx < kValues};
+// The gradient array and component of value idx (0..kValues-1).
+__device__ __forceinline__ Target value_target(const BackwardArgs& a, int mode, int idx, bool active) {
+  Target t{nullptr, 0, 0, active && idx >= 0 && idx < kValues};
+  if (idx < 0) return t;
   if (idx < 3) t = Target{a.dL_dcolors, 3, idx, t.active};
   else if (idx == 3) t = Target{a.acc_depth, 1, 0, t.active};
   else if (idx < 6) t = Target{a.dL_dmean2D, 3, idx - 4, t.active};
   else if (idx < 9) t = Target{a.acc_cov, 4, mode == 0 ? (idx == 8 ? 3 : idx - 6) : idx - 6, t.active};
   else if (idx == 9) t = Target{a.dL_dopacity, 1, 0, t.active};
+  return t;
+}
+
+__device__ __forceinline__ Target lane_target(const BackwardArgs& a, int mode) {
+  const int lane = threadIdx.x & 31, idx = (lane >> 1) & 15;
+  return value_target(a, mode, idx, (lane & 1) == 0);
+}
+
+// flush_pair's lane roles: lane bit 4 picks the entry; within it the 16 lanes
+// of bits 0-3 hold values 5 * b3 + {0, 1, 2, 3, 4} at (b2, b1, b0) = (000,
+// 001, 010, 100, 101), and the other three hold the tree's zero padding.
+__device__ __forceinline__ Target lane_target_pair(const BackwardArgs& a, int mode) {
+  const int lane = threadIdx.x & 31;
+  const int b0 = lane & 1, b1 = (lane >> 1) & 1, b2 = (lane >> 2) & 1, b3 = (lane >> 3) & 1;
+  const int sub = b2 ? (b1 ? -1 : 3 + b0) : (b1 && b0 ? -1 : 2 * b1 + b0);
+  Target t = value_target(a, mode, sub < 0 ? -1 : 5 * b3 + sub, true);
+  t.second = (lane & 16) != 0;
   return t;
 }
 
@@ -105,6 +124,42 @@ __device__ __forceinline__ void flush(const float (&c)[kValues], bool any_contri
   float w1 = (b ? w2[1] : w2[0]) + __shfl_xor_sync(full, b ? w2[0] : w2[1], 2);
   w1 += __shfl_xor_sync(full, w1, 1);
   if (t.active) atomicAdd(t.base + size_t(t.mult) * id + t.off, w1);
+}
+
+// Two entries' sums at once: their 20 values halve over five exchange steps
+// (10, 5, 3, 2 and 1 shuffles, the odd counts padded with a zero) instead of
+// 16 shuffles per entry; 20 lanes then add one total each (lane_target_pair).
+// An entry no lane contributes to is left out: the other goes alone (flush).
+__device__ __forceinline__ void flush_pair(const float (&c0)[kValues], const float (&c1)[kValues], bool any0,
+                                           bool any1, uint32_t id0, uint32_t id1, const Target& t,
+                                           const Target& tp) {
+  const bool has0 = __any_sync(0xffffffffu, any0), has1 = __any_sync(0xffffffffu, any1);
+  if (!has0 || !has1) {
+    if (has0) flush(c0, true, id0, t);
+    if (has1) flush(c1, true, id1, t);
+    return;
+  }
+  static_assert(kValues == 10, "pair tree layout");
+  const unsigned full = 0xffffffffu;
+  const int lane = threadIdx.x & 31;
+  float w10[10], w5[6], w3[4], w2[2];
+  bool b = lane & 16;
+#pragma unroll
+  for (int k = 0; k < 10; ++k) w10[k] = (b ? c1[k] : c0[k]) + __shfl_xor_sync(full, b ? c0[k] : c1[k], 16);
+  b = lane & 8;
+#pragma unroll
+  for (int k = 0; k < 5; ++k) w5[k] = (b ? w10[k + 5] : w10[k]) + __shfl_xor_sync(full, b ? w10[k] : w10[k + 5], 8);
+  w5[5] = 0.0f;
+  b = lane & 4;
+#pragma unroll
+  for (int k = 0; k < 3; ++k) w3[k] = (b ? w5[k + 3] : w5[k]) + __shfl_xor_sync(full, b ? w5[k] : w5[k + 3], 4);
+  w3[3] = 0.0f;
+  b = lane & 2;
+#pragma unroll
+  for (int k = 0; k < 2; ++k) w2[k] = (b ? w3[k + 2] : w3[k]) + __shfl_xor_sync(full, b ? w3[k] : w3[k + 2], 2);
+  b = lane & 1;
+  const float w1 = (b ? w2[1] : w2[0]) + __shfl_xor_sync(full, b ? w2[0] : w2[1], 1);
+  if (tp.active) atomicAdd(tp.base + size_t(tp.mult) * (tp.second ? id1 : id0) + tp.off, w1);
 }
 
 // Pixel-loop prologue shared by both modes: this thread's pixel, its
@@ -185,7 +240,11 @@ struct RefChain {
                                        float G, float alpha, float ddelx_dx, float ddely_dy, float (&c)[kValues]) {
     const Next x = next(alpha);
     const float Tn = x.Tn, n0 = x.n0, n1 = x.n1, n2 = x.n2, nd = x.nd, na = x.na;
-    const float dchdc = alpha * Tn;
+    // a skipped entry's contributions are zeroed through three of their
+    // factors: alpha <= 0.99 and T_final / T finite keep dL_dopa finite, and
+    // the conic (inverse of a covariance with +0.3 on its diagonal) keeps dx,
+    // dy and the products finite, so each contribution is exactly +-0
+    const float dchdc = ok ? alpha * Tn : 0.f;
     float dL_dopa = 0.0f;
     dL_dopa += (q1.w - n0) * p.dLp0;
     dL_dopa += (q2.x - n1) * p.dLp1;
@@ -195,20 +254,21 @@ struct RefChain {
     dL_dopa += (1 - na) * p.dLa;
     dL_dopa *= Tn;
     dL_dopa += div_markstein(-T_final, 1.f - alpha) * bg_dot;
-    const float dL_dG = q1.y * dL_dopa;
-    const float gdx = G * dx, gdy = G * dy;
+    const float Gz = ok ? G : 0.f;  // G itself may be infinite where the entry is skipped
+    const float dL_dG = ok ? q1.y * dL_dopa : 0.f;
+    const float gdx = Gz * dx, gdy = Gz * dy;
     const float dG_ddelx = -gdx * q0.z - gdy * q0.w;
     const float dG_ddely = -gdy * q1.x - gdx * q0.w;
-    c[0] = ok ? dchdc * p.dLp0 : 0.f;
-    c[1] = ok ? dchdc * p.dLp1 : 0.f;
-    c[2] = ok ? dchdc * p.dLp2 : 0.f;
-    c[3] = ok ? dchdc * p.dLd : 0.f;
-    c[4] = ok ? dL_dG * dG_ddelx * ddelx_dx : 0.f;
-    c[5] = ok ? dL_dG * dG_ddely * ddely_dy : 0.f;
-    c[6] = ok ? -0.5f * gdx * dx * dL_dG : 0.f;
-    c[7] = ok ? -0.5f * gdx * dy * dL_dG : 0.f;
-    c[8] = ok ? -0.5f * gdy * dy * dL_dG : 0.f;
-    c[9] = ok ? G * dL_dopa : 0.f;
+    c[0] = dchdc * p.dLp0;
+    c[1] = dchdc * p.dLp1;
+    c[2] = dchdc * p.dLp2;
+    c[3] = dchdc * p.dLd;
+    c[4] = dL_dG * dG_ddelx * ddelx_dx;
+    c[5] = dL_dG * dG_ddely * ddely_dy;
+    c[6] = -0.5f * gdx * dx * dL_dG;
+    c[7] = -0.5f * gdx * dy * dL_dG;
+    c[8] = -0.5f * gdy * dy * dL_dG;
+    c[9] = Gz * dL_dopa;
     commit(ok, x, q1, q2, alpha);
   }
 };
@@ -296,6 +356,7 @@ __global__ void __launch_bounds__(kBlendThreads, 2) render_ref_kernel(BackwardAr
   const float ddelx_dx = 0.5f * float(p.W), ddely_dy = 0.5f * float(p.H);
   const float pxf = float(p.tp.px), pyf = float(p.tp.py);
   const Target tgt = lane_target(a, 0);
+  const Target tgt2 = lane_target_pair(a, 0);
   WarpChunk& wc = s_chunk[threadIdx.x >> 5];
   // the blend's block masks, when this binning state has them: warps 0-3 read
   // the top array, 4-7 the bottom one, bit = block within that half
@@ -318,8 +379,7 @@ __global__ void __launch_bounds__(kBlendThreads, 2) render_ref_kernel(BackwardAr
       float c0[kValues], c1[kValues];
       ch.step(ok0, p, a0, a1, a2, dx0, dy0, G0, al0, ddelx_dx, ddely_dy, c0);
       ch.step(ok1, p, b0, b1, b2, dx1, dy1, G1, al1, ddelx_dx, ddely_dy, c1);
-      flush(c0, ok0, wc.id[j0], tgt);
-      flush(c1, ok1, wc.id[j1], tgt);
+      flush_pair(c0, c1, ok0, ok1, wc.id[j0], wc.id[j1], tgt, tgt2);
     }
   };
   auto state_only = [&](uint32_t bits, int hi) {
@@ -391,10 +451,14 @@ struct ExactChain {
     float dLda = p.dLp0 * (q2.x * Tn - S0 * ia) + p.dLp1 * (q2.y * Tn - S1 * ia) + p.dLp2 * (q2.z * Tn - S2 * ia);
     dLda += p.dLd * (q1.w * Tn - SD * ia);
     dLda += p.dLa * (Tn - SW * ia);
-    c[0] = ok ? aT * p.dLp0 : 0.f;
-    c[1] = ok ? aT * p.dLp1 : 0.f;
-    c[2] = ok ? aT * p.dLp2 : 0.f;
-    c[3] = ok ? aT * p.dLd : 0.f;
+    // skipped entries' contributions are zeroed through one factor each:
+    // 1 - alpha >= 0.01, g <= 1, det >= 0.09 and the mahalanobis distance
+    // (a quotient by det) keep every other factor finite
+    const float aTz = ok ? aT : 0.f;
+    c[0] = aTz * p.dLp0;
+    c[1] = aTz * p.dLp1;
+    c[2] = aTz * p.dLp2;
+    c[3] = aTz * p.dLd;
     if (ok) {
       T = Tn;
       S0 += q2.x * aT;
@@ -404,20 +468,20 @@ struct ExactChain {
       SW += aT;
     }
     const bool unclamped = ok && og < 0.99f;
-    c[9] = unclamped ? dLda * g : 0.f;
+    c[9] = dLda * (unclamped ? g : 0.f);
     const bool inner = unclamped && mahal >= 0.0f;
-    const float dLdm = dLda * q1.z * (-0.5f * g);
+    const float dLdm = inner ? dLda * q1.z * (-0.5f * g) : 0.f;
     const float cxx = q0.z, cxy = q0.w, cyy = q1.x, det = q1.y;
     const float dx = pxf - q0.x, dy = pyf - q0.y;
     // det >= 0.09 (the forward's +0.3 low-pass on a positive semi-definite
     // covariance), where rcp_markstein is the correctly rounded 1/det
     const float idet = rcp_markstein(det);
     const float num = mahal * det;
-    c[4] = inner ? -dLdm * (2.f * cyy * dx - 2.f * cxy * dy) * idet * hW : 0.f;
-    c[5] = inner ? -dLdm * (2.f * cxx * dy - 2.f * cxy * dx) * idet * hH : 0.f;
-    c[6] = inner ? dLdm * (dy * dy * idet - num * cyy * idet * idet) : 0.f;
-    c[7] = inner ? dLdm * (-2.f * dx * dy * idet + 2.f * num * cxy * idet * idet) : 0.f;
-    c[8] = inner ? dLdm * (dx * dx * idet - num * cxx * idet * idet) : 0.f;
+    c[4] = -dLdm * (2.f * cyy * dx - 2.f * cxy * dy) * idet * hW;
+    c[5] = -dLdm * (2.f * cxx * dy - 2.f * cxy * dx) * idet * hH;
+    c[6] = dLdm * (dy * dy * idet - num * cyy * idet * idet);
+    c[7] = dLdm * (-2.f * dx * dy * idet + 2.f * num * cxy * idet * idet);
+    c[8] = dLdm * (dx * dx * idet - num * cxx * idet * idet);
   }
 };
 
@@ -437,6 +501,7 @@ __global__ void __launch_bounds__(kBlendThreads, 2) render_exact_kernel(Backward
   const float hW = 0.5f * float(p.W), hH = 0.5f * float(p.H);
   const float pxf = float(p.tp.px), pyf = float(p.tp.py);
   const Target tgt = lane_target(a, 1);
+  const Target tgt2 = lane_target_pair(a, 1);
   WarpChunk& wc = s_chunk[threadIdx.x >> 5];
   // the blend's block masks, when this binning state has them: warps 0-3 read
   // the top array, 4-7 the bottom one, bit = block within that half
@@ -477,8 +542,7 @@ __global__ void __launch_bounds__(kBlendThreads, 2) render_exact_kernel(Backward
       float c0[kValues], c1[kValues];
       ch.step(ok0, p, a0, a1, s[kRecVec * j0 + 2], pxf, pyf, g0, og0, al0, m0, hW, hH, c0);
       ch.step(ok1, p, b0, b1, s[kRecVec * j1 + 2], pxf, pyf, g1, og1, al1, m1, hW, hH, c1);
-      flush(c0, ok0, wc.id[j0], tgt);
-      flush(c1, ok1, wc.id[j1], tgt);
+      flush_pair(c0, c1, ok0, ok1, wc.id[j0], wc.id[j1], tgt, tgt2);
     }
   };
   auto state_only = [&](uint32_t bits, int hi) {
