@@ -95,6 +95,16 @@ def quiet_stream_mismatch():
         f(False)
 
 
+def accumulators_on_current_stream(leaves):
+    """Create the leaves' autograd gradient accumulators on the current
+    stream (a no-op view of each leaf, kept alive through the backward).
+    Torch runs a leaf's gradient accumulation on the stream that was current
+    when the leaf first entered the step's graph; without this that is the
+    first view's stream, whose own backward then queues behind the other
+    views' accumulations and runs alone at the end of the step."""
+    return [x.view_as(x) for x in leaves]
+
+
 def peaks():
     try:
         with open(PEAKS_FILE) as f:
@@ -262,7 +272,9 @@ def run_ours(a):
                 one_view(v)
             return
         # every view's forward on its stream, then one backward over all views
-        # (each view's backward runs on the stream its forward ran on)
+        # (each view's backward runs on the stream its forward ran on; the
+        # gradient sums over views run on the main stream)
+        anchors = accumulators_on_current_stream(list(L.values()) + [means2D])  # noqa: F841
         colors = []
         for v in range(a.views):
             vstreams[v].wait_stream(main)
@@ -545,6 +557,7 @@ def run_e2e(a, sc, cams, device, world):
             ev_g = torch.cuda.Event()
             ev_g.record(copy_stream)
         losses = []
+        anchors = accumulators_on_current_stream(params.parameters()) if vstreams else None  # noqa: F841
         for v, c in enumerate(cams):
             vs = vstreams[v] if vstreams else main_stream
             if vstreams:

@@ -50,17 +50,20 @@ struct BlendPixel {
 
   // Entry with alpha `al` (record words q1, q2), 1-based list position `pos`.
   // Branch-free: the updates are selected, so a warp's lanes never diverge.
+  // An entry that does not accumulate adds exactly zero: its weight aT is
+  // selected to 0, colours and depth are finite, and C, Wt and D are never
+  // -0 (non-negative colours and weights, positive depths), so x + c * 0 = x.
   __device__ __forceinline__ void step(float al, float4 q1, float4 q2, uint32_t pos) {
     const bool blend = !done && al >= 1.0f / 255.0f;
     const float nT = mul(T, sub(1.0f, al));
     const bool term = blend && nT < 0.0001f;
     const bool acc = blend && !term;
-    const float aT = mul(al, T);
-    C0 = acc ? fma(q2.x, aT, C0) : C0;
-    C1 = acc ? fma(q2.y, aT, C1) : C1;
-    C2 = acc ? fma(q2.z, aT, C2) : C2;
-    Wt = acc ? add(Wt, aT) : Wt;
-    D = acc ? s1<fp::BL_DEPTH>(q1.w, aT, D) : D;
+    const float aT = acc ? mul(al, T) : 0.0f;
+    C0 = fma(q2.x, aT, C0);
+    C1 = fma(q2.y, aT, C1);
+    C2 = fma(q2.z, aT, C2);
+    Wt = add(Wt, aT);
+    D = s1<fp::BL_DEPTH>(q1.w, aT, D);
     T = acc ? nT : T;
     last = acc ? pos : last;
     done = done || term;
