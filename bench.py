@@ -359,6 +359,10 @@ def run_ours(a):
     concurrent_stages = None
     if not a.single_stream:
         concurrent_stages = timed_stages
+        # warm-up of the one-stream pattern: its buffers come from the main
+        # stream's allocator pool, which the per-view-stream steps left empty
+        for _ in range(max(a.warmup, 3)):
+            step(False)
         torch.cuda.synchronize()
         if world > 1:
             dist.barrier()

@@ -331,11 +331,7 @@ __device__ __forceinline__ void onesweep_tile_pass(const K* __restrict__ kin, co
     const uint32_t d = uint32_t(k[i] >> shift) & dmask;
     const bool valid = kFull || wbase + uint32_t(i * 32) < n;
     uint32_t pm = kFull ? 0xffffffffu : __ballot_sync(0xffffffffu, valid);
-#pragma unroll
-    for (int bt = 0; bt < kWidth; ++bt) {
-      const uint32_t bal = __ballot_sync(0xffffffffu, (d >> bt) & 1u);
-      pm &= ((d >> bt) & 1u) ? bal : ~bal;
-    }
+    pm &= __match_any_sync(0xffffffffu, d);
     const uint32_t before = valid ? sm.wcnt[warp][d] : 0u;
     rank[i] = before + __popc(pm & lt);
     __syncwarp();
