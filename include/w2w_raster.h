@@ -338,6 +338,33 @@ int w2w_batch_backward(const w2w_batch_item* items, int n, const void* geom_stat
                        float* dL_dmeans2D, float* dL_dcolors, float* dL_dopacity, float* dL_dmeans3D,
                        float* dL_dcov3D, float* dL_dsh, float* dL_dscales, float* dL_drotations,
                        w2w_stream_t stream);
+/* The same backward with the per-Gaussian pass summing each group's items
+ * (a scene's views, or a serving request's) itself: in place of the five
+ * per-element parameter gradients and a w2w_group_sum per tensor, it writes
+ * the per-group sums g_means3D [rows,3], g_opacity [rows], g_scales [rows,3],
+ * g_rotations [rows,4] and g_sh [rows,M,3] directly, each sum over the
+ * group's items in table order (w2w_group_sum's order; equal to its sums up to
+ * a few ulps of fused multiply-adds).
+ * group_tables is device memory in w2w_group_sum's layout; dL_dmeans2D,
+ * dL_dcolors and dL_dopacity stay per element ([E, ...]).  The reference has
+ * one call per view and sums views in torch's autograd (GaussianTrainer.py:47-88). */
+int w2w_batch_backward_grouped(const w2w_batch_item* items, int n, const void* geom_state,
+                               long long num_rendered, const void* binning_state, const void* image_state,
+                               const int* radii, const float* out_alpha, const float* dL_dcolor,
+                               const float* dL_ddepth, const float* dL_dalpha, int grad_mode, void* scratch,
+                               size_t scratch_bytes, const uint32_t* group_tables, int num_groups,
+                               long long group_rows, float* dL_dmeans2D, float* dL_dcolors, float* dL_dopacity,
+                               float* g_means3D, float* g_opacity, float* g_scales, float* g_rotations,
+                               float* g_sh, w2w_stream_t stream);
+/* The grouped per-Gaussian pass alone, over the per-element accumulators a
+ * previous w2w_batch_backward or w2w_batch_backward_grouped call on the same
+ * state left in `scratch` and in dL_dmeans2D, dL_dcolors and dL_dopacity
+ * (for instance, per-element gradients first, then the group sums). */
+int w2w_batch_gaussians_grouped(const w2w_batch_item* items, int n, const void* geom_state, const int* radii,
+                                int grad_mode, void* scratch, size_t scratch_bytes, const float* dL_dmeans2D,
+                                const float* dL_dcolors, const float* dL_dopacity, const uint32_t* group_tables,
+                                int num_groups, long long group_rows, float* g_means3D, float* g_opacity,
+                                float* g_scales, float* g_rotations, float* g_sh, w2w_stream_t stream);
 
 /* ---- observability ---------------------------------------------------------
  * Number of kernels the library has launched in this process. */

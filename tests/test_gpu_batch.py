@@ -102,3 +102,72 @@ def test_batch_scene_gradient_is_sum_over_its_views():
         want = sum(g["per_item"][v][3] for v in items)
         got = g["means3D"][g["groups"].index(s)]
         assert torch.allclose(got, want, rtol=1e-6, atol=1e-7)
+
+
+def _views_with_straddling_groups():
+    """The _setup views reordered so that the first group (scene 2, 6000
+    Gaussians) ends inside a warp of the grouped pass: rows 5984-6015 mix
+    scene 2 and scene 0."""
+    scs, views = _setup()
+    return scs, [views[3], views[0], views[1], views[2], views[4]]
+
+
+@pytest.mark.parametrize("grad_mode", ["reference", "exact"])
+def test_grouped_pass_equals_group_sum(grad_mode):
+    """The grouped per-Gaussian pass, run over the per-element accumulators a
+    per-element backward left, against w2w_group_sum's sums of that
+    backward's per-element gradients: the same inputs and summation order; the
+    per-view arithmetic, inlined into another kernel, may fuse a multiply-add
+    differently, so values agree to a few ulps (no atomic order is involved)."""
+    import ctypes
+    from word2world_b200.batch import lib
+    scs, views = _views_with_straddling_groups()
+    br = BatchRenderer(grad_mode=grad_mode)
+    res = br.forward(scs, views)
+    rng = np.random.default_rng(5)
+    grads = [torch.from_numpy(rng.normal(size=(3, v.camera.height, v.camera.width)).astype(np.float32)).to(DEV)
+             for v in views]
+    g = br.backward(res, grads, per_element=True)
+    lb, st = br._last_backward, res.state
+    total, M = lb["total"], st["M"]
+    outs = {name: torch.full((total, *shp), float("nan"), device=DEV)
+            for name, shp in (("means3D", (3,)), ("opacities", (1,)), ("scales", (3,)), ("rotations", (4,)),
+                              ("shs", (M, 3)))}
+    p = lambda t: ctypes.c_void_p(t.data_ptr())
+    stream = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    rc = lib().w2w_batch_gaussians_grouped(
+        st["arr"], st["n"], p(st["geom"]), p(st["radii"]), br.grad_mode, p(lb["scratch"]),
+        ctypes.c_size_t(lb["scratch"].numel()), p(lb["g_m2"]), p(lb["g_col"]), p(lb["g_op"]), p(lb["tables"]),
+        lb["G"], ctypes.c_longlong(total), p(outs["means3D"]), p(outs["opacities"]), p(outs["scales"]),
+        p(outs["rotations"]), p(outs["shs"]), stream)
+    assert rc == 0
+    torch.cuda.synchronize()
+    assert g["groups"] == [2, 0, 1]
+    for name in outs:
+        want = torch.cat([x.reshape(x.shape[0], -1) for x in g[name]]).cpu().numpy()
+        got = outs[name].reshape(total, -1).cpu().numpy()
+        chk = parity.grad_check(got, want, row_rtol=parity.SAME_IMPL_ROW_RTOL)
+        assert chk["norm_rel"] <= 1e-6 and chk["n_bad"] == 0, (name, chk)
+
+
+@pytest.mark.parametrize("grad_mode", ["reference", "exact"])
+def test_grouped_backward_sums_the_views(grad_mode):
+    """The default batched backward (grouped pass) against the per-item
+    gradients of a per-element backward summed per scene: equal up to the
+    float atomic order of the per-pixel pass."""
+    scs, views = _views_with_straddling_groups()
+    br = BatchRenderer(grad_mode=grad_mode)
+    res = br.forward(scs, views)
+    rng = np.random.default_rng(6)
+    grads = [torch.from_numpy(rng.normal(size=(3, v.camera.height, v.camera.width)).astype(np.float32)).to(DEV)
+             for v in views]
+    ref = br.backward(res, grads, per_element=True)
+    got = br.backward(res, grads)
+    assert got["groups"] == ref["groups"]
+    for k, s in enumerate(got["groups"]):
+        items = [v for v, view in enumerate(views) if view.scene == s]
+        for name, col in (("means3D", 3), ("scales", 6), ("rotations", 7), ("shs", 5), ("opacities", 2)):
+            want = sum(ref["per_item"][v][col].double() for v in items).float()
+            chk = parity.grad_check(got[name][k].reshape(want.shape).cpu().numpy(), want.cpu().numpy(),
+                                    row_rtol=parity.SAME_IMPL_ROW_RTOL)
+            assert chk["norm_rel"] <= 1e-5, (s, name, chk)

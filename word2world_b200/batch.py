@@ -290,7 +290,7 @@ class BatchRenderer:
 
     # ---- backward -----------------------------------------------------------
     def backward(self, res: BatchResult, dL_dcolor, dL_ddepth=None, dL_dalpha=None, per_element: bool = False,
-                 groups=None):
+                 groups=None, grouped: bool = True):
         """Gradients for upstream image gradients given per item (lists of
         [3,H,W] / [1,H,W] tensors).  Items are summed by group (default: by
         scene; a serving loop groups by request): returns, per group, the sum
@@ -298,7 +298,10 @@ class BatchRenderer:
         order of first appearance (``out["groups"]`` lists the group ids),
         plus the per-item dL/dmeans2D; ``per_element`` also returns the raw
         per-item tensors (the single-view call's eight outputs for every
-        item)."""
+        item).  Without ``per_element`` the per-Gaussian pass sums each
+        group's items itself (w2w_batch_backward_grouped); ``grouped=False``
+        writes per-item gradients and sums them with w2w_group_sum instead
+        (the same sums in the same order, up to a few ulps)."""
         L = lib()
         st = res.state
         arr, n, M, E, R = st["arr"], st["n"], st["M"], st["E"], st["R"]
@@ -316,18 +319,7 @@ class BatchRenderer:
         dld = packed("dld", dL_ddepth) if dL_ddepth is not None else zeros
         dla = packed("dla", dL_dalpha) if dL_dalpha is not None else zeros
         scratch = self._u8("scratch", int(L.w2w_batch_backward_scratch_bytes(arr, n)))
-        Eg = max(E, 1)
-        f = self._f32
-        g_m2, g_col, g_op = f("g_m2", Eg, 3), f("g_col", Eg, 3), f("g_op", Eg, 1)
-        g_m3, g_cov, g_sh = f("g_m3", Eg, 3), f("g_cov", Eg, 6), f("g_sh", Eg, max(M, 1), 3)
-        g_sc, g_rot = f("g_sc", Eg, 3), f("g_rot", Eg, 4)
-        p = lambda t: ctypes.c_void_p(t.data_ptr())
-        _check(L.w2w_batch_backward(arr, n, p(st["geom"]), ctypes.c_longlong(R), p(st["binb"]), p(st["img"]),
-                                    p(st["radii"]), p(st["alpha"]), p(dlc), p(dld), p(dla), self.grad_mode,
-                                    p(scratch), ctypes.c_size_t(scratch.numel()), p(g_m2), p(g_col), p(g_op),
-                                    p(g_m3), p(g_cov), p(g_sh), p(g_sc), p(g_rot), stream), "batch backward")
-        # per-group sums of the items' element ranges: one deterministic
-        # reduction launch per tensor (w2w_group_sum)
+        # the groups' tables (w2w_group_sum's layout): row bases, item pointers, item element bases
         gid = [groups[v] if groups is not None else views[v].scene for v in range(n)]
         order, base, total, members = [], {}, 0, {}
         ebase, e0 = [], 0
@@ -364,14 +356,43 @@ class BatchRenderer:
         tables.copy_(staged[:tab.nbytes], non_blocking=True)
         self._tables_copied = torch.cuda.Event()
         self._tables_copied.record(torch.cuda.current_stream(dev))
+        Eg = max(E, 1)
+        f = self._f32
+        g_m2, g_col, g_op = f("g_m2", Eg, 3), f("g_col", Eg, 3), f("g_op", Eg, 1)
+        p = lambda t: ctypes.c_void_p(t.data_ptr())
+        shapes = (("means3D", (3,)), ("opacities", (1,)), ("scales", (3,)), ("rotations", (4,)),
+                  ("shs", (max(M, 1), 3)))
         out = {"groups": order}
-        for name, t in (("means3D", g_m3), ("opacities", g_op), ("scales", g_sc), ("rotations", g_rot),
-                        ("shs", g_sh)):
-            width = int(np.prod(t.shape[1:]))
-            acc = self._f32("acc_" + name, total, *t.shape[1:])
-            _check(L.w2w_group_sum(p(t), width, G, p(tables), n, p(acc), ctypes.c_longlong(total), stream),
-                   "group sum")
-            out[name] = [acc[base[g]:base[g] + size[g]] for g in order]
+        if grouped and not per_element:
+            acc = {name: f("acc_" + name, max(total, 1), *shp) for name, shp in shapes}
+            _check(L.w2w_batch_backward_grouped(
+                arr, n, p(st["geom"]), ctypes.c_longlong(R), p(st["binb"]), p(st["img"]), p(st["radii"]),
+                p(st["alpha"]), p(dlc), p(dld), p(dla), self.grad_mode, p(scratch), ctypes.c_size_t(scratch.numel()),
+                p(tables), G, ctypes.c_longlong(total), p(g_m2), p(g_col), p(g_op), p(acc["means3D"]),
+                p(acc["opacities"]), p(acc["scales"]), p(acc["rotations"]), p(acc["shs"]), stream),
+                "batch backward (grouped)")
+            for name, _ in shapes:
+                out[name] = [acc[name][base[g]:base[g] + size[g]] for g in order]
+        else:
+            g_m3, g_cov, g_sh = f("g_m3", Eg, 3), f("g_cov", Eg, 6), f("g_sh", Eg, max(M, 1), 3)
+            g_sc, g_rot = f("g_sc", Eg, 3), f("g_rot", Eg, 4)
+            _check(L.w2w_batch_backward(arr, n, p(st["geom"]), ctypes.c_longlong(R), p(st["binb"]), p(st["img"]),
+                                        p(st["radii"]), p(st["alpha"]), p(dlc), p(dld), p(dla), self.grad_mode,
+                                        p(scratch), ctypes.c_size_t(scratch.numel()), p(g_m2), p(g_col), p(g_op),
+                                        p(g_m3), p(g_cov), p(g_sh), p(g_sc), p(g_rot), stream), "batch backward")
+            # per-group sums of the items' element ranges: one deterministic
+            # reduction launch per tensor (w2w_group_sum)
+            for name, t in (("means3D", g_m3), ("opacities", g_op), ("scales", g_sc), ("rotations", g_rot),
+                            ("shs", g_sh)):
+                width = int(np.prod(t.shape[1:]))
+                acc_t = self._f32("acc_" + name, total, *t.shape[1:])
+                _check(L.w2w_group_sum(p(t), width, G, p(tables), n, p(acc_t), ctypes.c_longlong(total), stream),
+                       "group sum")
+                out[name] = [acc_t[base[g]:base[g] + size[g]] for g in order]
+        # the per-element accumulators and tables of this call (a grouped pass
+        # can be re-run over them: w2w_batch_gaussians_grouped)
+        self._last_backward = dict(scratch=scratch, g_m2=g_m2, g_col=g_col, g_op=g_op, tables=tables, G=G,
+                                   total=total)
         e = 0
         out["means2D"] = []
         raw = []

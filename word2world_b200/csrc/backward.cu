@@ -815,6 +815,12 @@ struct GView {
   }
 };
 
+// Element i (global index) of batch item `it`.
+__device__ __forceinline__ GView item_gview(const BatchItem& it, int i) {
+  return GView{it.means3D, it.scales, it.rotations, it.view, i - int(it.elem_base), it.W, it.degree, it.h_x, it.h_y,
+               it.tan_fovx, it.tan_fovy, it.h_x, it.scale_modifier};
+}
+
 __device__ __forceinline__ GView make_gview(const BackwardArgs& a, int i, const float* s_mats) {
   GView g;
   if (a.items == nullptr) {
@@ -823,18 +829,29 @@ __device__ __forceinline__ GView make_gview(const BackwardArgs& a, int i, const 
     g.svec = a.svec;
     g.quat = a.quat;
   } else {
-    const BatchItem& it = a.items[find_item_elem(a.items, a.num_items, uint32_t(i))];
-    g = GView{it.means3D, it.scales, it.rotations, it.view, i - int(it.elem_base), it.W, it.degree, it.h_x, it.h_y,
-              it.tan_fovx, it.tan_fovy, it.h_x, it.scale_modifier};
+    g = item_gview(a.items[find_item_elem(a.items, a.num_items, uint32_t(i))], i);
   }
   return g;
+}
+
+// The per-Gaussian outputs of one element (kept in registers; the kernels
+// store them, or sum them over a group's views).
+struct GOut {
+  float m3[3], cov[6], sc[3], rot[4];
+};
+
+__device__ __forceinline__ void store_gout(const BackwardArgs& a, int i, const GOut& o) {
+  for (int k = 0; k < 3; ++k) a.dL_dmeans3D[3 * i + k] = o.m3[k];
+  for (int k = 0; k < 6; ++k) a.dL_dcov3D[6 * i + k] = o.cov[k];
+  for (int k = 0; k < 3; ++k) a.dL_dscales[3 * i + k] = o.sc[k];
+  for (int k = 0; k < 4; ++k) a.dL_drotations[4 * i + k] = o.rot[k];
 }
 
 // One Gaussian (radius > 0) of the reference-formula pass: every output but
 // dL_dsh, plus the SH basis and masked colour gradient dL_dsh is built from.
 // sh_row: this Gaussian's SH coefficients (staged in shared memory).
 __device__ __forceinline__ void ref_gaussian(const BackwardArgs& a, int i, const GView& gv, const float* sh_row, float (&basis)[16],
-                                             float (&cf)[3]) {
+                                             float (&cf)[3], GOut& o) {
   const int M = a.M;
   const float* mats = gv.mats;
   const float* cam = mats + 32;
@@ -899,7 +916,7 @@ __device__ __forceinline__ void ref_gaussian(const BackwardArgs& a, int i, const
   } else {
     for (int k = 0; k < 6; ++k) dc[k] = 0.f;
   }
-  for (int k = 0; k < 6; ++k) a.dL_dcov3D[6 * i + k] = dc[k];
+  for (int k = 0; k < 6; ++k) o.cov[k] = dc[k];
   const float gT00 = 2.0f * (T[0][0] * Vk[0][0] + T[0][1] * Vk[0][1] + T[0][2] * Vk[0][2]) * ga + (T[1][0] * Vk[0][0] + T[1][1] * Vk[0][1] + T[1][2] * Vk[0][2]) * gb;
   const float gT01 = 2.0f * (T[0][0] * Vk[1][0] + T[0][1] * Vk[1][1] + T[0][2] * Vk[1][2]) * ga + (T[1][0] * Vk[1][0] + T[1][1] * Vk[1][1] + T[1][2] * Vk[1][2]) * gb;
   const float gT02 = 2.0f * (T[0][0] * Vk[2][0] + T[0][1] * Vk[2][1] + T[0][2] * Vk[2][2]) * ga + (T[1][0] * Vk[2][0] + T[1][1] * Vk[2][1] + T[1][2] * Vk[2][2]) * gb;
@@ -989,9 +1006,9 @@ __device__ __forceinline__ void ref_gaussian(const BackwardArgs& a, int i, const
     for (int c = 0; c < 3; ++c) acc += ((c == r ? msq : 0.0f) - rd[c] * rd[r]) * im3 * ag[c];
     sd[r] += acc;
   }
-  a.dL_dmeans3D[3 * i] = sd[0];
-  a.dL_dmeans3D[3 * i + 1] = sd[1];
-  a.dL_dmeans3D[3 * i + 2] = sd[2];
+  o.m3[0] = sd[0];
+  o.m3[1] = sd[1];
+  o.m3[2] = sd[2];
 
   // ---- scale / rotation (backward.cu:446-518) ----
   const float4 qr = gv.rotation();
@@ -1019,9 +1036,9 @@ __device__ __forceinline__ void ref_gaussian(const BackwardArgs& a, int i, const
                  2.f * (qxz - yw) * a31 + 2.f * (qyz + xw) * a32 + (1.f - 2.f * (xx + yy)) * a33};
   if (gv.svec != nullptr)  // raw path: scales = exp(svec)
     for (int k = 0; k < 3; ++k) ds[k] = ds[k] * sc[k];
-  a.dL_dscales[3 * i] = ds[0];
-  a.dL_dscales[3 * i + 1] = ds[1];
-  a.dL_dscales[3 * i + 2] = ds[2];
+  o.sc[0] = ds[0];
+  o.sc[1] = ds[1];
+  o.sc[2] = ds[2];
   float4 dq;
   dq.x = 4.f * (-sz * (a31 * yw - a32 * xw + a33 * qxy) + sy * (a21 * zw - a22 * qxz + a23 * yy) + sx * (a12 * zw - a13 * yw - a11 * qyz));
   dq.y = 4.f * (sz * (a31 * zw + a32 * zz - a33 * qyz) - sy * (a21 * yw + a22 * qxy + a23 * xx) + sx * (a12 * yy + a13 * zw + a11 * qxz));
@@ -1040,10 +1057,10 @@ __device__ __forceinline__ void ref_gaussian(const BackwardArgs& a, int i, const
       dq = make_float4(dq.x * 1e12f, dq.y * 1e12f, dq.z * 1e12f, dq.w * 1e12f);
     }
   }
-  a.dL_drotations[4 * i] = dq.x;
-  a.dL_drotations[4 * i + 1] = dq.y;
-  a.dL_drotations[4 * i + 2] = dq.z;
-  a.dL_drotations[4 * i + 3] = dq.w;
+  o.rot[0] = dq.x;
+  o.rot[1] = dq.y;
+  o.rot[2] = dq.z;
+  o.rot[3] = dq.w;
 }
 
 // 8 CTAs per SM (64 registers, no spills; shared memory allows 9): more
@@ -1077,7 +1094,9 @@ __global__ void __launch_bounds__(kGaussThreads, 8) gaussians_ref_kernel(Backwar
   float basis[16], cf[3] = {0.f, 0.f, 0.f};
   const bool active = lane < n && a.radii[i] > 0;
   if (active) {
-    ref_gaussian(a, i, gv, sw + lane * stride, basis, cf);
+    GOut o;
+    ref_gaussian(a, i, gv, sw + lane * stride, basis, cf, o);
+    store_gout(a, i, o);
   } else if (lane < n) {
     for (int k = 0; k < 3; ++k) a.dL_dmeans3D[3 * i + k] = 0.f;
     for (int k = 0; k < 6; ++k) a.dL_dcov3D[6 * i + k] = 0.f;
@@ -1098,7 +1117,7 @@ __global__ void __launch_bounds__(kGaussThreads, 8) gaussians_ref_kernel(Backwar
 // One Gaussian (radius > 0) of the exact-derivative pass: every output but
 // dL_dsh, plus the outer-product factors of dL_dsh (see ref_gaussian).
 __device__ __forceinline__ void exact_gaussian(const BackwardArgs& a, int i, const GView& gv, const float* sh_row,
-                                               float (&basis)[16], float (&cf)[3]) {
+                                               float (&basis)[16], float (&cf)[3], GOut& o) {
   const int M = a.M;
   const float* mats = gv.mats;
   const float* cam = mats + 32;
@@ -1136,12 +1155,12 @@ __device__ __forceinline__ void exact_gaussian(const BackwardArgs& a, int i, con
   float Gf[3][3];
   for (int p = 0; p < 3; ++p)
     for (int q = 0; q < 3; ++q) Gf[p][q] = gxx * jx[p] * jx[q] + gyy * jy[p] * jy[q] + gxy * jx[p] * jy[q];
-  a.dL_dcov3D[6 * i + 0] = Gf[0][0];
-  a.dL_dcov3D[6 * i + 1] = Gf[0][1] + Gf[1][0];
-  a.dL_dcov3D[6 * i + 2] = Gf[0][2] + Gf[2][0];
-  a.dL_dcov3D[6 * i + 3] = Gf[1][1];
-  a.dL_dcov3D[6 * i + 4] = Gf[1][2] + Gf[2][1];
-  a.dL_dcov3D[6 * i + 5] = Gf[2][2];
+  o.cov[0] = Gf[0][0];
+  o.cov[1] = Gf[0][1] + Gf[1][0];
+  o.cov[2] = Gf[0][2] + Gf[2][0];
+  o.cov[3] = Gf[1][1];
+  o.cov[4] = Gf[1][2] + Gf[2][1];
+  o.cov[5] = Gf[2][2];
   float Sjx[3], Sjy[3];
   for (int p = 0; p < 3; ++p) {
     Sjx[p] = S[p][0] * jx[0] + S[p][1] * jx[1] + S[p][2] * jx[2];
@@ -1186,18 +1205,18 @@ __device__ __forceinline__ void exact_gaussian(const BackwardArgs& a, int i, con
   for (int k = 0; k < 3; ++k) {
     float acc = 0.f;
     for (int p = 0; p < 3; ++p) acc += dM[p][k] * R[p][k];
-    a.dL_dscales[3 * i + k] = acc;
+    o.sc[k] = acc;
   }
   float dR[3][3];
   for (int p = 0; p < 3; ++p)
     for (int k = 0; k < 3; ++k) dR[p][k] = dM[p][k] * s[k];
-  a.dL_drotations[4 * i] = dR[0][1] * (-2.f * z) + dR[0][2] * (2.f * y) + dR[1][0] * (2.f * z) + dR[1][2] * (-2.f * x) +
+  o.rot[0] = dR[0][1] * (-2.f * z) + dR[0][2] * (2.f * y) + dR[1][0] * (2.f * z) + dR[1][2] * (-2.f * x) +
                            dR[2][0] * (-2.f * y) + dR[2][1] * (2.f * x);
-  a.dL_drotations[4 * i + 1] = dR[0][1] * (2.f * y) + dR[0][2] * (2.f * z) + dR[1][0] * (2.f * y) + dR[1][1] * (-4.f * x) +
+  o.rot[1] = dR[0][1] * (2.f * y) + dR[0][2] * (2.f * z) + dR[1][0] * (2.f * y) + dR[1][1] * (-4.f * x) +
                                dR[1][2] * (-2.f * w) + dR[2][0] * (2.f * z) + dR[2][1] * (2.f * w) + dR[2][2] * (-4.f * x);
-  a.dL_drotations[4 * i + 2] = dR[0][0] * (-4.f * y) + dR[0][1] * (2.f * x) + dR[0][2] * (2.f * w) + dR[1][0] * (2.f * x) +
+  o.rot[2] = dR[0][0] * (-4.f * y) + dR[0][1] * (2.f * x) + dR[0][2] * (2.f * w) + dR[1][0] * (2.f * x) +
                                dR[1][2] * (2.f * z) + dR[2][0] * (-2.f * w) + dR[2][1] * (2.f * z) + dR[2][2] * (-4.f * y);
-  a.dL_drotations[4 * i + 3] = dR[0][0] * (-4.f * z) + dR[0][1] * (-2.f * w) + dR[0][2] * (2.f * x) + dR[1][0] * (2.f * w) +
+  o.rot[3] = dR[0][0] * (-4.f * z) + dR[0][1] * (-2.f * w) + dR[0][2] * (2.f * x) + dR[1][0] * (2.f * w) +
                                dR[1][1] * (-4.f * z) + dR[1][2] * (2.f * y) + dR[2][0] * (2.f * x) + dR[2][1] * (2.f * y);
   // colour: rgb = sum_k basis_k(dir) sh_k + 0.5 with the forward's constants
   const float v0 = m0 - cam[0], v1 = m1 - cam[1], v2 = m2 - cam[2];
@@ -1245,9 +1264,9 @@ __device__ __forceinline__ void exact_gaussian(const BackwardArgs& a, int i, con
   const float dd[3] = {X, Y, Z};
   const float dot = dd[0] * gdir[0] + dd[1] * gdir[1] + dd[2] * gdir[2];
   for (int p = 0; p < 3; ++p) gm[p] += (gdir[p] - dd[p] * dot) / vn;
-  a.dL_dmeans3D[3 * i] = gm[0];
-  a.dL_dmeans3D[3 * i + 1] = gm[1];
-  a.dL_dmeans3D[3 * i + 2] = gm[2];
+  o.m3[0] = gm[0];
+  o.m3[1] = gm[1];
+  o.m3[2] = gm[2];
 }
 
 __global__ void __launch_bounds__(kGaussThreads) gaussians_exact_kernel(BackwardArgs a) {
@@ -1277,7 +1296,9 @@ __global__ void __launch_bounds__(kGaussThreads) gaussians_exact_kernel(Backward
   float basis[16], cf[3] = {0.f, 0.f, 0.f};
   const bool active = lane < n && a.radii[i] > 0;
   if (active) {
-    exact_gaussian(a, i, gv, sw + lane * stride, basis, cf);
+    GOut o;
+    exact_gaussian(a, i, gv, sw + lane * stride, basis, cf, o);
+    store_gout(a, i, o);
   } else if (lane < n) {
     for (int k = 0; k < 3; ++k) a.dL_dmeans3D[3 * i + k] = 0.f;
     for (int k = 0; k < 6; ++k) a.dL_dcov3D[6 * i + k] = 0.f;
@@ -1287,7 +1308,116 @@ __global__ void __launch_bounds__(kGaussThreads) gaussians_exact_kernel(Backward
   sh_store_outer(a.dL_dsh, a.M, i0, n, sw, basis, cf, active);
 }
 
+// ---------------------------------------------------------------------------
+// Grouped per-Gaussian pass (batched calls): one thread per output row of a
+// group (a scene, or a serving request), walking the group's items (views) in
+// table order.  Each item's element is the single-view computation above; its
+// outputs are summed in registers in item order, starting from zero, with
+// explicit-rounding adds -- w2w_group_sum's order over the per-element
+// outputs (the per-view arithmetic, inlined here, may fuse a multiply-add
+// differently, so the two agree to a few ulps).  The SH rows are staged once per warp for
+// all views of a scene (a view of another scene reads its own row from
+// memory), and no per-element dL/dSH, dL/dmeans3D, dL/dscales, dL/drotations
+// or dL/dcov3D is written.
+// ---------------------------------------------------------------------------
+template <int kMode>
+__global__ void __launch_bounds__(kGaussThreads) gaussians_group_kernel(BackwardArgs a) {
+  __shared__ float s_sh[kGaussThreads / 32][32 * kShStride];
+  const unsigned full = 0xffffffffu;
+  const int lane = threadIdx.x & 31;
+  float* sw = s_sh[threadIdx.x >> 5];
+  const long long row0 = (long long)blockIdx.x * kGaussThreads + (threadIdx.x & ~31);
+  if (row0 >= a.group_rows) return;  // warp-uniform
+  const int n = int(min(32LL, a.group_rows - row0));
+  const uint32_t row = uint32_t(row0) + uint32_t(lane < n ? lane : 0);
+  const uint32_t* gbase = a.group_tables;
+  const uint32_t* iptr = gbase + (a.num_groups + 1);
+  const uint32_t* ielem = iptr + (a.num_groups + 1);
+  int lo = 0, hi = a.num_groups - 1;  // this row's group: the last g with gbase[g] <= row
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (__ldg(gbase + mid) <= row) lo = mid;
+    else hi = mid - 1;
+  }
+  const int g = lo;
+  const uint32_t r = row - __ldg(gbase + g);
+  const uint32_t k0 = __ldg(iptr + g), k1 = __ldg(iptr + g + 1);
+  const int M = a.M, rg = 3 * M, stride = sh_stride(M);
+  const uint32_t e0 = k0 < k1 ? __ldg(ielem + k0) + r : uint32_t(a.P);
+  const float* shs0 = e0 < uint32_t(a.P) ? a.items[find_item_elem(a.items, a.num_items, e0)].shs : nullptr;
+  // the rows of the warp's first group's scene, contiguous when every lane is in that group
+  if (__all_sync(full, g == __shfl_sync(full, g, 0) && shs0 != nullptr)) {
+    sh_stage_in(shs0, M, int(__shfl_sync(full, r, 0)), n, sw, stride);
+  } else {
+    if (lane < n && shs0 != nullptr)
+      for (int c = 0; c < 3 * (M < 16 ? M : 16); ++c) sw[lane * stride + c] = __ldg(shs0 + size_t(r) * rg + c);
+    __syncwarp();
+  }
+  float am[3] = {0.f, 0.f, 0.f}, asc[3] = {0.f, 0.f, 0.f}, arot[4] = {0.f, 0.f, 0.f, 0.f}, aop = 0.f;
+  float ash[48];
+#pragma unroll
+  for (int c = 0; c < 48; ++c) ash[c] = 0.f;
+  for (uint32_t k = k0; lane < n && k < k1; ++k) {
+    const uint32_t i = __ldg(ielem + k) + r;
+    if (i >= uint32_t(a.P)) continue;  // a table pointing past the elements: nothing is read there
+    const BatchItem& it = a.items[find_item_elem(a.items, a.num_items, i)];
+    const GView gv = item_gview(it, int(i));
+    if (a.radii[i] > 0) {
+      const float* sh_row = it.shs == shs0 ? sw + lane * stride : it.shs + size_t(gv.gi) * rg;
+      float basis[16], cf[3];
+      GOut o;
+      if (kMode == 1) exact_gaussian(a, int(i), gv, sh_row, basis, cf, o);
+      else ref_gaussian(a, int(i), gv, sh_row, basis, cf, o);
+#pragma unroll
+      for (int c = 0; c < 3; ++c) am[c] = add(am[c], o.m3[c]);
+#pragma unroll
+      for (int c = 0; c < 3; ++c) asc[c] = add(asc[c], o.sc[c]);
+#pragma unroll
+      for (int c = 0; c < 4; ++c) arot[c] = add(arot[c], o.rot[c]);
+#pragma unroll
+      for (int b = 0; b < 16; ++b)
+#pragma unroll
+        for (int ch = 0; ch < 3; ++ch) ash[3 * b + ch] = add(ash[3 * b + ch], mul(basis[b], cf[ch]));
+    }
+    aop = add(aop, a.dL_dopacity[i]);
+  }
+  if (lane < n) {
+    for (int c = 0; c < 3; ++c) a.g_means3D[3 * size_t(row) + c] = am[c];
+    for (int c = 0; c < 3; ++c) a.g_scales[3 * size_t(row) + c] = asc[c];
+    for (int c = 0; c < 4; ++c) a.g_rotations[4 * size_t(row) + c] = arot[c];
+    a.g_opacity[row] = aop;
+  }
+  // dL/dSH rows [row0, row0 + n) ([rows, M, 3], contiguous) through shared
+  // memory, so the warp's stores are one contiguous run
+  __syncwarp();  // every lane is done with the staged input rows
+  if (lane < n) {
+#pragma unroll
+    for (int c = 0; c < 48; ++c)
+      if (c < rg) sw[lane * stride + c] = ash[c];
+    for (int c = 48; c < rg; ++c) sw[lane * stride + c] = 0.f;  // bands beyond the 16th (none for M <= 16)
+  }
+  __syncwarp();
+  float* dst = a.g_sh + size_t(row0) * rg;
+  const int total = n * rg;
+  int gr = 0, c = lane;
+  while (c >= rg) { c -= rg; ++gr; }
+  for (int e = lane; e < total; e += 32) {
+    dst[e] = sw[gr * stride + c];
+    c += 32;
+    while (c >= rg) { c -= rg; ++gr; }
+  }
+}
+
 }  // namespace
+
+void launch_backward_groups(const BackwardArgs& a, cudaStream_t stream) {
+  if (a.group_rows <= 0 || a.num_groups <= 0) return;
+  const long long blocks = (a.group_rows + kGaussThreads - 1) / kGaussThreads;
+  stage_begin(kStBwdGaussians, stream);
+  if (a.grad_mode == 1) gaussians_group_kernel<1><<<unsigned(blocks), kGaussThreads, 0, stream>>>(a);
+  else gaussians_group_kernel<0><<<unsigned(blocks), kGaussThreads, 0, stream>>>(a);
+  stage_end(kStBwdGaussians, stream, 1);
+}
 
 void launch_backward_render(const BackwardArgs& a, cudaStream_t stream) {
   const int tiles = a.items ? a.total_tiles : ((a.W + kTile - 1) / kTile) * ((a.H + kTile - 1) / kTile);

@@ -1164,41 +1164,53 @@ int w2w_batch_forward_render(const w2w_batch_item* items, int n, const void* geo
   return finish(err_word, st);
 }
 
-int w2w_batch_backward(const w2w_batch_item* items, int n, const void* geom_state, long long R,
-                       const void* binning_state, const void* image_state, const int* radii, const float* out_alpha,
-                       const float* dL_dcolor, const float* dL_ddepth, const float* dL_dalpha, int grad_mode,
-                       void* scratch, size_t scratch_bytes, float* dL_dmeans2D, float* dL_dcolors, float* dL_dopacity,
-                       float* dL_dmeans3D, float* dL_dcov3D, float* dL_dsh, float* dL_dscales, float* dL_drotations,
-                       w2w_stream_t stream) {
-  const BatchTotals t = batch_totals(items, n);
-  if (!t.ok || (grad_mode != 0 && grad_mode != 1)) return W2W_ERR_INVALID;
-  const long long E = t.elems;
-  if (E == 0) return W2W_OK;
-  if (!geom_state || !image_state || !radii || !out_alpha || !dL_dcolor || !dL_ddepth || !dL_dalpha ||
-      !dL_dmeans2D || !dL_dcolors || !dL_dopacity || !dL_dmeans3D || !dL_dcov3D || !dL_dscales || !dL_drotations ||
-      (t.M > 0 && !dL_dsh) || (R > 0 && !binning_state))
-    return W2W_ERR_INVALID;
-  if (!scratch || scratch_bytes < w2w_batch_backward_scratch_bytes(items, n)) return W2W_ERR_SCRATCH;
-  cudaStream_t st = S(stream);
-  const int T = t.tiles;
+// The per-Gaussian pass's arguments of a batched backward: the item table and
+// geometry state, and the per-element accumulators the per-pixel pass fills
+// (acc_cov and acc_depth in the scratch; dL_dmeans2D, dL_dcolors, dL_dopacity).
+static void batch_gaussian_args(int n, long long E, int M, const void* geom_state, const int* radii, int grad_mode,
+                                void* scratch, float* dL_dmeans2D, float* dL_dcolors, float* dL_dopacity,
+                                BackwardArgs& a) {
   const GeomLayout GL(E);
   const BatchGeomLayout BGL(E, n);
-  const ImageLayout IL(size_t(t.pixels), size_t(T));
-  float* acc_cov = static_cast<float*>(scratch);
-  float* acc_depth = at<float>(scratch, align256(size_t(E) * 16));
-  cudaMemsetAsync(scratch, 0, w2w_batch_backward_scratch_bytes(items, n), st);
-  cudaMemsetAsync(dL_dmeans2D, 0, sizeof(float) * 3 * size_t(E), st);
-  cudaMemsetAsync(dL_dcolors, 0, sizeof(float) * 3 * size_t(E), st);
-  cudaMemsetAsync(dL_dopacity, 0, sizeof(float) * size_t(E), st);
-  BackwardArgs a{};
-  a.P = int(E); a.W = 0; a.H = 0; a.degree = 0; a.M = t.M; a.grad_mode = grad_mode;
-  a.items = at<BatchItem>(geom_state, BGL.items); a.num_items = n; a.total_tiles = T;
+  a = BackwardArgs{};
+  a.P = int(E); a.W = 0; a.H = 0; a.degree = 0; a.M = M; a.grad_mode = grad_mode;
+  a.items = at<BatchItem>(geom_state, BGL.items); a.num_items = n;
   a.shs = nullptr;
   a.radii = radii;
   a.cov3D = at<float>(geom_state, GL.cov3D);
   a.clamped = at<uint8_t>(geom_state, GL.clamped);
   a.record = at<float>(geom_state, GL.record);
   a.bwd_record = at<float>(geom_state, GL.bwd_record);
+  a.dL_dmean2D = dL_dmeans2D; a.dL_dopacity = dL_dopacity; a.dL_dcolors = dL_dcolors;
+  a.acc_cov = static_cast<float*>(scratch);
+  a.acc_depth = at<float>(scratch, align256(size_t(E) * 16));
+}
+
+// The batched backward's common part: argument checks, the per-element
+// accumulators cleared, the per-pixel pass launched; `a` is left ready for a
+// per-Gaussian pass.  Returns W2W_OK, an error, or 1 when there is no element.
+static int batch_backward_begin(const w2w_batch_item* items, int n, const void* geom_state, long long R,
+                                const void* binning_state, const void* image_state, const int* radii,
+                                const float* out_alpha, const float* dL_dcolor, const float* dL_ddepth,
+                                const float* dL_dalpha, int grad_mode, void* scratch, size_t scratch_bytes,
+                                float* dL_dmeans2D, float* dL_dcolors, float* dL_dopacity, cudaStream_t st,
+                                BackwardArgs& a) {
+  const BatchTotals t = batch_totals(items, n);
+  if (!t.ok || (grad_mode != 0 && grad_mode != 1)) return W2W_ERR_INVALID;
+  const long long E = t.elems;
+  if (E == 0) return 1;
+  if (!geom_state || !image_state || !radii || !out_alpha || !dL_dcolor || !dL_ddepth || !dL_dalpha ||
+      !dL_dmeans2D || !dL_dcolors || !dL_dopacity || (R > 0 && !binning_state))
+    return W2W_ERR_INVALID;
+  if (!scratch || scratch_bytes < w2w_batch_backward_scratch_bytes(items, n)) return W2W_ERR_SCRATCH;
+  const int T = t.tiles;
+  const ImageLayout IL(size_t(t.pixels), size_t(T));
+  cudaMemsetAsync(scratch, 0, w2w_batch_backward_scratch_bytes(items, n), st);
+  cudaMemsetAsync(dL_dmeans2D, 0, sizeof(float) * 3 * size_t(E), st);
+  cudaMemsetAsync(dL_dcolors, 0, sizeof(float) * 3 * size_t(E), st);
+  cudaMemsetAsync(dL_dopacity, 0, sizeof(float) * size_t(E), st);
+  batch_gaussian_args(n, E, t.M, geom_state, radii, grad_mode, scratch, dL_dmeans2D, dL_dcolors, dL_dopacity, a);
+  a.total_tiles = T;
   a.ranges = at<uint2>(image_state, IL.ranges);
   a.point_list = R > 0 ? at<uint32_t>(binning_state, BinLayout(R, T).valsA) : nullptr;
   if (R > 0) {
@@ -1213,12 +1225,85 @@ int w2w_batch_backward(const w2w_batch_item* items, int n, const void* geom_stat
   a.T_final = at<float>(image_state, IL.T_final);
   a.out_alpha = out_alpha;
   a.dL_dcolor = dL_dcolor; a.dL_ddepth = dL_ddepth; a.dL_dalpha = dL_dalpha;
-  a.dL_dmean2D = dL_dmeans2D; a.acc_cov = acc_cov; a.dL_dopacity = dL_dopacity; a.dL_dcolors = dL_dcolors;
-  a.acc_depth = acc_depth;
+  if (R > 0) launch_backward_render(a, st);
+  return W2W_OK;
+}
+
+// The grouped outputs' arguments (both grouped entry points).
+static bool group_outputs_ok(const BatchTotals& t, const uint32_t* group_tables, int num_groups, long long group_rows,
+                             const float* g_means3D, const float* g_opacity, const float* g_scales,
+                             const float* g_rotations, const float* g_sh) {
+  return group_tables && num_groups > 0 && group_rows > 0 && group_rows <= t.elems && g_means3D && g_opacity &&
+         g_scales && g_rotations && (t.M == 0 || g_sh);
+}
+
+static void set_group_outputs(BackwardArgs& a, const uint32_t* group_tables, int num_groups, long long group_rows,
+                              float* g_means3D, float* g_opacity, float* g_scales, float* g_rotations, float* g_sh) {
+  a.group_tables = group_tables; a.num_groups = num_groups; a.group_rows = group_rows;
+  a.g_means3D = g_means3D; a.g_opacity = g_opacity; a.g_scales = g_scales; a.g_rotations = g_rotations;
+  a.g_sh = g_sh;
+}
+
+int w2w_batch_backward(const w2w_batch_item* items, int n, const void* geom_state, long long R,
+                       const void* binning_state, const void* image_state, const int* radii, const float* out_alpha,
+                       const float* dL_dcolor, const float* dL_ddepth, const float* dL_dalpha, int grad_mode,
+                       void* scratch, size_t scratch_bytes, float* dL_dmeans2D, float* dL_dcolors, float* dL_dopacity,
+                       float* dL_dmeans3D, float* dL_dcov3D, float* dL_dsh, float* dL_dscales, float* dL_drotations,
+                       w2w_stream_t stream) {
+  const BatchTotals t = batch_totals(items, n);
+  if (t.ok && t.elems > 0 && (!dL_dmeans3D || !dL_dcov3D || !dL_dscales || !dL_drotations || (t.M > 0 && !dL_dsh)))
+    return W2W_ERR_INVALID;
+  BackwardArgs a;
+  const int rc = batch_backward_begin(items, n, geom_state, R, binning_state, image_state, radii, out_alpha,
+                                      dL_dcolor, dL_ddepth, dL_dalpha, grad_mode, scratch, scratch_bytes,
+                                      dL_dmeans2D, dL_dcolors, dL_dopacity, S(stream), a);
+  if (rc != W2W_OK) return rc == 1 ? W2W_OK : rc;
   a.dL_dmeans3D = dL_dmeans3D; a.dL_dcov3D = dL_dcov3D; a.dL_dsh = dL_dsh; a.dL_dscales = dL_dscales;
   a.dL_drotations = dL_drotations;
-  if (R > 0) launch_backward_render(a, st);
-  launch_backward_gaussians(a, st);
+  launch_backward_gaussians(a, S(stream));
+  return check_launch();
+}
+
+int w2w_batch_backward_grouped(const w2w_batch_item* items, int n, const void* geom_state, long long R,
+                               const void* binning_state, const void* image_state, const int* radii,
+                               const float* out_alpha, const float* dL_dcolor, const float* dL_ddepth,
+                               const float* dL_dalpha, int grad_mode, void* scratch, size_t scratch_bytes,
+                               const uint32_t* group_tables, int num_groups, long long group_rows,
+                               float* dL_dmeans2D, float* dL_dcolors, float* dL_dopacity, float* g_means3D,
+                               float* g_opacity, float* g_scales, float* g_rotations, float* g_sh,
+                               w2w_stream_t stream) {
+  const BatchTotals t = batch_totals(items, n);
+  if (t.ok && t.elems > 0 &&
+      !group_outputs_ok(t, group_tables, num_groups, group_rows, g_means3D, g_opacity, g_scales, g_rotations, g_sh))
+    return W2W_ERR_INVALID;
+  BackwardArgs a;
+  const int rc = batch_backward_begin(items, n, geom_state, R, binning_state, image_state, radii, out_alpha,
+                                      dL_dcolor, dL_ddepth, dL_dalpha, grad_mode, scratch, scratch_bytes,
+                                      dL_dmeans2D, dL_dcolors, dL_dopacity, S(stream), a);
+  if (rc != W2W_OK) return rc == 1 ? W2W_OK : rc;
+  set_group_outputs(a, group_tables, num_groups, group_rows, g_means3D, g_opacity, g_scales, g_rotations, g_sh);
+  launch_backward_groups(a, S(stream));
+  return check_launch();
+}
+
+int w2w_batch_gaussians_grouped(const w2w_batch_item* items, int n, const void* geom_state, const int* radii,
+                                int grad_mode, void* scratch, size_t scratch_bytes, const float* dL_dmeans2D,
+                                const float* dL_dcolors, const float* dL_dopacity, const uint32_t* group_tables,
+                                int num_groups, long long group_rows, float* g_means3D, float* g_opacity,
+                                float* g_scales, float* g_rotations, float* g_sh, w2w_stream_t stream) {
+  const BatchTotals t = batch_totals(items, n);
+  if (!t.ok || (grad_mode != 0 && grad_mode != 1)) return W2W_ERR_INVALID;
+  if (t.elems == 0) return W2W_OK;
+  if (!geom_state || !radii || !dL_dmeans2D || !dL_dcolors || !dL_dopacity ||
+      !group_outputs_ok(t, group_tables, num_groups, group_rows, g_means3D, g_opacity, g_scales, g_rotations, g_sh))
+    return W2W_ERR_INVALID;
+  if (!scratch || scratch_bytes < w2w_batch_backward_scratch_bytes(items, n)) return W2W_ERR_SCRATCH;
+  BackwardArgs a;
+  // the pass only reads the per-element accumulators
+  batch_gaussian_args(n, t.elems, t.M, geom_state, radii, grad_mode, scratch, const_cast<float*>(dL_dmeans2D),
+                      const_cast<float*>(dL_dcolors), const_cast<float*>(dL_dopacity), a);
+  set_group_outputs(a, group_tables, num_groups, group_rows, g_means3D, g_opacity, g_scales, g_rotations, g_sh);
+  launch_backward_groups(a, S(stream));
   return check_launch();
 }
 

@@ -225,9 +225,17 @@ struct BackwardArgs {
   // d/dlogit, and dL_dsh_dc / dL_dsh_ac the SH rows split as the inputs)
   const float *svec, *quat, *logit, *sh_dc, *sh_ac;
   float *dL_dsh_dc, *dL_dsh_ac;
+  // grouped per-Gaussian pass (batched calls): per-group sums over the
+  // groups' items, tables laid out as w2w_group_sum's ([G + 1] row bases,
+  // [G + 1] item pointers, item element bases), outputs [group_rows, ...]
+  const uint32_t* group_tables;
+  int num_groups;
+  long long group_rows;
+  float *g_means3D, *g_opacity, *g_scales, *g_rotations, *g_sh;
 };
 void launch_backward_render(const BackwardArgs& a, cudaStream_t stream);
 void launch_backward_gaussians(const BackwardArgs& a, cudaStream_t stream);
+void launch_backward_groups(const BackwardArgs& a, cudaStream_t stream);
 
 // Instance binning from depth-ordered Gaussians (binning.cu): a single-view
 // call's sorted instance list and tile ranges without key emission or an
