@@ -210,11 +210,12 @@ struct RefChain {
   // T < 1e-4) and 1 - alpha in [0.01, 1]: the division is in div_markstein's
   // range, which equals /.
   struct Next {
-    float Tn, n0, n1, n2, nd, na;
+    float Tn, n0, n1, n2, nd, na, y;  // y: RN(1 / (1 - alpha)), shared by the step's two quotients
   };
   __device__ __forceinline__ Next next(float alpha) const {
     Next x;
-    x.Tn = div_markstein(T, 1.f - alpha);
+    x.y = rcp_markstein(1.f - alpha);
+    x.Tn = div_markstein_y(T, 1.f - alpha, x.y);
     x.n0 = last_alpha * lc0 + (1.f - last_alpha) * acc0;
     x.n1 = last_alpha * lc1 + (1.f - last_alpha) * acc1;
     x.n2 = last_alpha * lc2 + (1.f - last_alpha) * acc2;
@@ -253,7 +254,7 @@ struct RefChain {
     dL_dopa += (c_d - nd) * p.dLd;
     dL_dopa += (1 - na) * p.dLa;
     dL_dopa *= Tn;
-    dL_dopa += div_markstein(-T_final, 1.f - alpha) * bg_dot;
+    dL_dopa += div_markstein_y(-T_final, 1.f - alpha, x.y) * bg_dot;
     const float Gz = ok ? G : 0.f;  // G itself may be infinite where the entry is skipped
     const float dL_dG = ok ? q1.y * dL_dopa : 0.f;
     const float gdx = Gz * dx, gdy = Gz * dy;

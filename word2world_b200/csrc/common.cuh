@@ -56,12 +56,13 @@ __device__ __forceinline__ float rcp_markstein(float b) {
   const float y0 = rcp_approx(b);
   return fma(fma(-b, y0, 1.0f), y0, y0);
 }
-__device__ __forceinline__ float div_markstein(float a, float b) {
-  const float y = rcp_markstein(b);
+// div_markstein with y = rcp_markstein(b) given (several quotients by one b)
+__device__ __forceinline__ float div_markstein_y(float a, float b, float y) {
   const float q0 = mul(a, y);
   const float q1 = fma(fma(-b, q0, a), y, q0);
   return fma(fma(-b, q1, a), y, q1);
 }
+__device__ __forceinline__ float div_markstein(float a, float b) { return div_markstein_y(a, b, rcp_markstein(b)); }
 // Operands for which div_markstein equals div: |b| in [2^-20, 2^60] and
 // a = 0 or |a| in [2^-60, 2^100], so the quotient lies in [2^-120, 2^120] and
 // no intermediate (reciprocal, product, remainders) leaves the normal range.
