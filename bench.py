@@ -36,7 +36,7 @@ FALLBACK_HBM_GBS = 6650.0
 # DRAM bytes (read + write) per launch, from one ncu capture of the default
 # workload (500k Gaussians, 512x512; dram__bytes_read.sum + dram__bytes_write.sum)
 NCU_TRAFFIC_500K_512 = {"sort_onesweep": 49.0e6, "preprocess": 181.2e6, "duplicate": 12.2e6,
-                        "sort_histogram": 23.7e6, "backward_gaussians": 232.4e6, "backward_render": 35.2e6,
+                        "sort_histogram": 23.7e6, "backward_gaussians": 232.4e6, "backward_render": 27.2e6,
                         "blend": 17.0e6}
 # Algorithmic work of the per-pixel passes per evaluated Gaussian-pixel pair
 # (the pairs are the reference's: sum over pixels of the contributor count):
