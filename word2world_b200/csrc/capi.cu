@@ -461,6 +461,7 @@ int w2w_forward_render(const w2w_settings* s, const void* geom_state, const w2w_
     SortArgs so{};
     so.n = R; so.key64 = kp.key64; so.begin_bit = 0; so.bits = kp.bits;
     so.keys_in = d.keys; so.vals_in = d.vals;
+    so.match_rank = 1;  // emitted Gaussian by Gaussian: few distinct digits per warp
     so.keys_out = keysA; so.vals_out = valsA;
     so.keys_tmp = keysB; so.vals_tmp = valsB;
     so.hist = at<uint32_t>(binning_state, BL.hist);
@@ -1117,6 +1118,7 @@ int w2w_batch_forward_render(const w2w_batch_item* items, int n, const void* geo
     SortArgs so{};
     so.n = R; so.key64 = kp.key64; so.begin_bit = 0; so.bits = kp.bits;
     so.keys_in = d.keys; so.vals_in = d.vals;
+    so.match_rank = 1;  // emitted Gaussian by Gaussian: few distinct digits per warp
     so.keys_out = keysA; so.vals_out = valsA;
     so.keys_tmp = keysB; so.vals_tmp = valsB;
     so.hist = at<uint32_t>(binning_state, BL.hist);

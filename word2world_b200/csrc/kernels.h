@@ -127,6 +127,7 @@ struct SortArgs {
   uint32_t* error;
   uint32_t spin_limit = kSpinLimit;  // bounded waits (spin_limit())
   long long unpublished_tile = -1;   // first pass: tile that skips publishing (tests; -1 = none)
+  int match_rank = 0;  // 1: rank digits with match.any (keys whose warps hold few distinct digits)
   int stage_hist = -1, stage_pass = -1;  // timing stages (default: the sort's own)
   int tile_shift;
   int num_tiles;

@@ -14,11 +14,17 @@
 //      reference's memset leaves them);
 //   3. one onesweep kernel per digit: each CTA takes the next 4096-key tile
 //      (acquired through an atomic counter, so every earlier tile is already
-//      running), ranks its keys stably with warp match.any, publishes its
+//      running), ranks its keys stably (warp match.any or per-bit ballots), publishes its
 //      per-digit counts and looks back over earlier tiles for their prefix
 //      (decoupled lookback), then scatters through shared memory so the
 //      global stores are coalesced.  Every wait is bounded: a wait that runs
 //      out sets kErrTimeout and the kernel finishes without hanging.
+//
+// Ranking: match.any costs little when a warp's 32 keys hold few distinct
+// digits, as the rasterizer's keys do (emitted Gaussian by Gaussian): 1.5 %
+// faster per pass than ballots there; on random keys (the standalone sort) it
+// measured 12 % slower than one ballot per digit bit, so SortArgs::match_rank
+// chooses.
 //
 // Stability: keys are ranked in input order within a warp, warps in order
 // within a tile, tiles in order globally -- the same order the reference's
@@ -264,7 +270,7 @@ struct OnesweepShared {
 
 // One tile of a pass.  kFull: every key of the tile exists (all tiles but the
 // last), so the per-key bounds checks drop out.  Indices are 32-bit (n < 2^30).
-template <typename K, int kWidth, bool kFull>
+template <typename K, int kWidth, bool kFull, bool kMatch>
 __device__ __forceinline__ void onesweep_tile_pass(const K* __restrict__ kin, const uint32_t* __restrict__ vin,
                                                    K* __restrict__ kout, uint32_t* __restrict__ vout, uint32_t n,
                                                    int shift, const uint32_t* __restrict__ digit_base,
@@ -332,7 +338,15 @@ __device__ __forceinline__ void onesweep_tile_pass(const K* __restrict__ kin, co
     const uint32_t d = uint32_t(k[i] >> shift) & dmask;
     const bool valid = kFull || wbase + uint32_t(i * 32) < n;
     uint32_t pm = kFull ? 0xffffffffu : __ballot_sync(0xffffffffu, valid);
-    pm &= __match_any_sync(0xffffffffu, d);
+    if constexpr (kMatch) {
+      pm &= __match_any_sync(0xffffffffu, d);
+    } else {
+#pragma unroll
+      for (int bt = 0; bt < kWidth; ++bt) {
+        const uint32_t bal = __ballot_sync(0xffffffffu, (d >> bt) & 1u);
+        pm &= ((d >> bt) & 1u) ? bal : ~bal;
+      }
+    }
     const uint32_t before = valid ? sm.wcnt[warp][d] : 0u;
     rank[i] = before + __popc(pm & lt);
     __syncwarp();
@@ -380,8 +394,11 @@ __device__ __forceinline__ void onesweep_tile_pass(const K* __restrict__ kin, co
   }
 }
 
-// kWidth: this pass's digit width (compile-time).
-template <typename K, int kWidth>
+// kWidth: this pass's digit width (compile-time).  kMatch: rank with
+// match.any (keys whose warps hold few distinct digits, such as the
+// rasterizer's, emitted Gaussian by Gaussian) or with one ballot per digit
+// bit (constant cost whatever the keys: random keys).
+template <typename K, int kWidth, bool kMatch>
 __global__ void __launch_bounds__(kSortThreads, OnesweepShape<K>::kMinBlocks)
 onesweep_kernel(const K* __restrict__ kin, const uint32_t* __restrict__ vin, K* __restrict__ kout,
                 uint32_t* __restrict__ vout, long long n, int shift,
@@ -403,14 +420,14 @@ onesweep_kernel(const K* __restrict__ kin, const uint32_t* __restrict__ vin, K* 
   const uint32_t nn = uint32_t(n);  // n < 2^30 (checked by every caller)
   const bool publish = (long long)tile != unpublished_tile;
   if ((unsigned long long)(tile + 1) * kTile <= nn)
-    onesweep_tile_pass<K, kWidth, true>(kin, vin, kout, vout, nn, shift, digit_base, status, err, tile, spin_limit,
+    onesweep_tile_pass<K, kWidth, true, kMatch>(kin, vin, kout, vout, nn, shift, digit_base, status, err, tile, spin_limit,
                                         publish, sm, s_keys, s_vals);
   else
-    onesweep_tile_pass<K, kWidth, false>(kin, vin, kout, vout, nn, shift, digit_base, status, err, tile, spin_limit,
+    onesweep_tile_pass<K, kWidth, false, kMatch>(kin, vin, kout, vout, nn, shift, digit_base, status, err, tile, spin_limit,
                                          publish, sm, s_keys, s_vals);
 }
 
-template <typename K, int kWidth>
+template <typename K, int kWidth, bool kMatch>
 void launch_onesweep_w(int tiles, cudaStream_t stream, const K* kin, const uint32_t* vin, K* kout, uint32_t* vout,
                        long long n, int shift, const uint32_t* digit_base, uint32_t* status, uint32_t* counter,
                        uint32_t* err, uint32_t spin_limit, long long unpublished) {
@@ -421,22 +438,26 @@ void launch_onesweep_w(int tiles, cudaStream_t stream, const K* kin, const uint3
   int dev = 0;
   cudaGetDevice(&dev);
   if (dev < 0 || dev >= 64 || !opted[dev]) {
-    cudaFuncSetAttribute(onesweep_kernel<K, kWidth>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(dyn));
+    cudaFuncSetAttribute(onesweep_kernel<K, kWidth, kMatch>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(dyn));
     if (dev >= 0 && dev < 64) opted[dev] = true;
   }
-  onesweep_kernel<K, kWidth><<<tiles, kSortThreads, dyn, stream>>>(kin, vin, kout, vout, n, shift, digit_base,
+  onesweep_kernel<K, kWidth, kMatch><<<tiles, kSortThreads, dyn, stream>>>(kin, vin, kout, vout, n, shift, digit_base,
                                                                     status, counter, err, spin_limit, unpublished);
 }
 
 template <typename K>
 void launch_onesweep(int width, int tiles, cudaStream_t stream, const K* kin, const uint32_t* vin, K* kout,
                      uint32_t* vout, long long n, int shift, const uint32_t* digit_base, uint32_t* status,
-                     uint32_t* counter, uint32_t* err, uint32_t spin_limit, long long unpublished) {
+                     uint32_t* counter, uint32_t* err, uint32_t spin_limit, long long unpublished, bool match) {
   switch (width) {
 #define W2W_ONESWEEP_CASE(W)                                                                                      \
   case W:                                                                                                         \
-    launch_onesweep_w<K, W>(tiles, stream, kin, vin, kout, vout, n, shift, digit_base, status, counter, err,      \
-                            spin_limit, unpublished);                                                             \
+    if (match)                                                                                                    \
+      launch_onesweep_w<K, W, true>(tiles, stream, kin, vin, kout, vout, n, shift, digit_base, status, counter,   \
+                                    err, spin_limit, unpublished);                                                \
+    else                                                                                                          \
+      launch_onesweep_w<K, W, false>(tiles, stream, kin, vin, kout, vout, n, shift, digit_base, status, counter,  \
+                                     err, spin_limit, unpublished);                                               \
     break;
     W2W_ONESWEEP_CASE(1) W2W_ONESWEEP_CASE(2) W2W_ONESWEEP_CASE(3) W2W_ONESWEEP_CASE(4) W2W_ONESWEEP_CASE(5)
     W2W_ONESWEEP_CASE(6) W2W_ONESWEEP_CASE(7) W2W_ONESWEEP_CASE(8) W2W_ONESWEEP_CASE(9)
@@ -493,7 +514,7 @@ void run_sort(const SortArgs& a, cudaStream_t stream) {
     launch_onesweep<K>(pass_width(p, dbits, a.bits), int(tiles), stream, kin, vin, kout, vout, n,
                        a.begin_bit + dbits * p, a.hist + kMaxBins * p,
                        a.status + size_t(p) * kMaxBins * size_t(tiles), a.counters + p, a.error,
-                       a.spin_limit, p == 0 ? a.unpublished_tile : -1LL);
+                       a.spin_limit, p == 0 ? a.unpublished_tile : -1LL, a.match_rank != 0);
     stage_end(st_pass, stream, 1);
     kin = kout;
     vin = vout;
