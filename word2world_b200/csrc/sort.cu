@@ -12,7 +12,7 @@
 //   2. offsets kernel: exclusive scans of those histograms; the tile scan is
 //      the per-tile [start, end) range table (empty tiles get (0, 0), as the
 //      reference's memset leaves them);
-//   3. one onesweep kernel per digit: each CTA takes the next 4096-key tile
+//   3. one onesweep kernel per digit: each CTA takes the next tile (6144 32-bit or 5120 64-bit keys)
 //      (acquired through an atomic counter, so every earlier tile is already
 //      running), ranks its keys stably (warp match.any or per-bit ballots), publishes its
 //      per-digit counts and looks back over earlier tiles for their prefix
@@ -331,8 +331,7 @@ __device__ __forceinline__ void onesweep_tile_pass(const K* __restrict__ kin, co
 
   // stable rank within the tile's digit: warp base + earlier items of the warp
   // + earlier lanes of this item holding the same digit (the lanes holding
-  // it, from one match.any; measured 1.5 % faster per pass on B200 than one
-  // ballot per digit bit)
+  // it: one match.any, or one ballot per digit bit; see "Ranking" above)
 #pragma unroll
   for (int i = 0; i < kItems; ++i) {
     const uint32_t d = uint32_t(k[i] >> shift) & dmask;
