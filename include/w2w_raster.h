@@ -149,6 +149,53 @@ int w2w_forward_render(const w2w_settings* s, const void* geom_state, const w2w_
                        void* binning_state, void* image_state, float* out_color, float* out_depth,
                        float* out_alpha, w2w_stream_t stream);
 
+/* ---- planned forward (no counterpart in the reference) ----------------------
+ * The reference reads R back before it can size and launch its sort
+ * (prepareSort.cu:382-387), and so does the pair above; a host that renders
+ * many views waits there once per view.  The planned pair launches the whole
+ * forward first and reads R afterwards:
+ *   1. w2w_forward_geometry(_raw)_async: the projection pass, then a copy of
+ *      the geometry header's first 16 bytes into `header_host` (pinned host
+ *      memory the caller owns); nothing is synchronised.
+ *   2. w2w_forward_render_planned with a capacity C and a number of key depth
+ *      bits from earlier views of the same size (w2w_planned_capacity of the
+ *      largest R seen; the most depth bits any of them needed), into a binning
+ *      state of w2w_binning_state_bytes(C, W, H) bytes.  The kernels read R
+ *      from device memory.
+ *   3. Once the header copy has landed (an event recorded after step 1),
+ *      w2w_geometry_info_from_header decodes it.  If R > C or the view needs
+ *      more depth bits than were given (w2w_depth_bits_needed), the planned
+ *      launches processed no instance: render again with w2w_forward_render
+ *      and a binning state sized for R.  Otherwise the result is the exact
+ *      plan's, bit for bit.
+ * A planned binning state is laid out for C: functions that take a binning
+ * state and a count (w2w_backward, w2w_backward_raw, w2w_binning_offset)
+ * take C there, and w2w_binning_layout_count recovers it from R and the
+ * state's size.  Capacities are multiples of W2W_PLAN_QUANTUM. */
+#define W2W_PLAN_QUANTUM 65536LL
+int w2w_forward_geometry_async(const w2w_settings* s, const float* means3D, const float* scales,
+                               const float* rotations, const float* opacities, const float* shs, int* radii,
+                               void* geom_state, void* header_host, w2w_stream_t stream);
+int w2w_forward_geometry_raw_async(const w2w_settings* s, const float* means3D, const float* svec,
+                                   const float* quaternion, const float* opacity_logit, const float* sh_dc,
+                                   const float* sh_ac, int* radii, void* geom_state, void* header_host,
+                                   w2w_stream_t stream);
+/* Decodes a header copied by the async geometry calls; returns its error status. */
+int w2w_geometry_info_from_header(const void* header_host, w2w_geometry_info* info);
+/* Depth bits the view's keys need (the span of its depths' bit patterns). */
+int w2w_depth_bits_needed(const w2w_geometry_info* info);
+/* Capacity for a planned render sized from an instance count: +25 %, rounded up
+ * to a multiple of W2W_PLAN_QUANTUM. */
+long long w2w_planned_capacity(long long num_rendered);
+int w2w_forward_render_planned(const w2w_settings* s, const void* geom_state, long long capacity, int depth_bits,
+                               void* binning_state, void* image_state, float* out_color, float* out_depth,
+                               float* out_alpha, w2w_stream_t stream);
+/* 1 when a planned render did not fit its plan (the header's flag; synchronises `stream`). */
+int w2w_binning_replanned(const void* binning_state, w2w_stream_t stream);
+/* The instance count a binning state of `state_bytes` bytes is laid out for:
+ * num_rendered itself, or a planned render's capacity; -1 if neither. */
+long long w2w_binning_layout_count(long long num_rendered, size_t state_bytes, int width, int height);
+
 /* Device error word of a geometry / binning state (synchronises `stream`). */
 int w2w_state_error(const void* state, int which /* 0 geometry, 1 binning */, w2w_stream_t stream);
 
@@ -292,6 +339,9 @@ int w2w_blend(const w2w_settings* s, const void* geom_state, const uint32_t* ran
  * (tile << 32 | depth bits), out of a binning state. */
 int w2w_binning_keys64(const void* binning_state, long long num_rendered, int width, int height,
                        uint64_t* out, w2w_stream_t stream);
+/* The same for a binning state laid out for layout_count >= num_rendered instances. */
+int w2w_binning_keys64_layout(const void* binning_state, long long num_rendered, long long layout_count, int width,
+                              int height, uint64_t* out, w2w_stream_t stream);
 
 /* ---- batched calls ----------------------------------------------------------
  * Many views of many scenes rendered and back-propagated with one launch per

@@ -63,10 +63,12 @@ def forward(arrays, cam, degree=3, compat_spill=True, bg=(1.0, 1.0, 1.0), focal_
     res.update(unpack_image(img, W, H))
     keys = _C.binning_keys64(binb, R, H, W).cpu().numpy().view(np.uint64) if R > 0 else np.zeros(0, np.uint64)
     b = binb.cpu().numpy()
-    pl = _field(b, _C.binning_offset(R, W, H, "vals_a"), np.uint32, R) if R > 0 else np.zeros(0, np.uint32)
+    # the point list: the state is laid out for R, or for a planned render's capacity
+    LR = _C.binning_layout_count(R, binb, H, W)
+    pl = _field(b, _C.binning_offset(LR, W, H, "vals_a"), np.uint32, R) if R > 0 else np.zeros(0, np.uint32)
     res.update(num_rendered=int(R), color=color.cpu().numpy(), depth_img=depth.cpu().numpy(),
                alpha=alpha.cpu().numpy(), radii=radii.cpu().numpy(), keys=keys, point_list=pl,
-               _tensors=dict(geom=geom, binb=binb, img=img, alpha=alpha, radii=radii))
+               layout_count=int(LR), _tensors=dict(geom=geom, binb=binb, img=img, alpha=alpha, radii=radii))
     return res
 
 

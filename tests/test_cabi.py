@@ -64,3 +64,26 @@ def test_invalid_arguments_rejected_without_gpu(lib):
     assert lib.w2w_sort_pairs_u64(None, None, None, None, ctypes.c_longlong(0), 0, 64, None, ctypes.c_size_t(0),
                                   None) == 0
     assert lib.w2w_scan_u32(None, None, ctypes.c_longlong(-5), 0, None, ctypes.c_size_t(0), None) == 1
+
+
+def test_planned_layout_helpers(lib):
+    """Host-only arithmetic of the planned forward: capacities and the layout
+    count recovered from a binning state's size."""
+    ll, sz = ctypes.c_longlong, ctypes.c_size_t
+    lib.w2w_planned_capacity.restype = ll
+    lib.w2w_planned_capacity.argtypes = [ll]
+    lib.w2w_binning_layout_count.restype = ll
+    lib.w2w_binning_layout_count.argtypes = [ll, sz, ctypes.c_int, ctypes.c_int]
+    lib.w2w_binning_state_bytes.restype = sz
+    lib.w2w_binning_state_bytes.argtypes = [ll, ctypes.c_int, ctypes.c_int]
+    Q = 65536
+    for R in (0, 1, 1000, 65536, 4_000_000, 5_923_615):
+        C = lib.w2w_planned_capacity(R)
+        assert C % Q == 0 and C >= max(Q, R + R // 4)
+        assert C - Q < max(Q, R + R // 4)
+        for W, H in ((256, 256), (512, 512), (800, 800)):
+            exact = lib.w2w_binning_state_bytes(R, W, H)
+            assert lib.w2w_binning_layout_count(R, exact, W, H) == R
+            planned = lib.w2w_binning_state_bytes(C, W, H)
+            assert lib.w2w_binning_layout_count(R, planned, W, H) == C
+            assert lib.w2w_binning_layout_count(R, planned + 256, W, H) == -1

@@ -46,7 +46,9 @@ def bucket_key(width: int, height: int, P: int, grad_mode: str = "reference", de
 
 
 def current() -> dict:
-    return dict(_C.tune_knobs())
+    """The tuned launch-shape knobs (the library's other switches, such as
+    planned_forward, are set with apply but not tuned)."""
+    return {k: v for k, v in _C.tune_knobs().items() if k in CANDIDATES}
 
 
 def apply(knobs: dict) -> dict:

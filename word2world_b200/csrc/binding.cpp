@@ -10,6 +10,7 @@
 
 #include <cuda_runtime.h>
 
+#include <map>
 #include <mutex>
 #include <sstream>
 #include <stdexcept>
@@ -128,6 +129,121 @@ void defer_bin_check(const Tensor& bin, int64_t R, int W, int H, cudaStream_t st
   deferred().add(static_cast<const unsigned char*>(bin.data_ptr()) + off, st, what);
 }
 
+// ---- planned forward --------------------------------------------------------
+// Per image shape (device, P, H, W): the largest instance count and the most
+// key depth bits seen so far.  Once a shape has been rendered, later renders
+// of it launch their whole forward before reading the instance count back
+// (w2w_forward_render_planned); a view that does not fit renders again with
+// the exact plan.  The "planned_forward" tuning knob (default 1) turns this
+// off; the "binning" knob's path always takes the exact plan.
+struct PlanState {
+  long long capacity = 0;
+  int depth_bits = -1;
+};
+std::mutex g_plan_mu;
+std::map<std::tuple<int, int64_t, int, int>, PlanState> g_plans;
+
+int tune_index(const char* name) {
+  for (int k = 0; k < w2w_tune_count(); ++k)
+    if (std::string(w2w_tune_name(k)) == name) return k;
+  return -1;
+}
+
+bool planned_enabled() {
+  static const int planned = tune_index("planned_forward"), binning = tune_index("binning");
+  return planned >= 0 && w2w_tune_get(planned) == 1 && (binning < 0 || w2w_tune_get(binning) == 0);
+}
+
+// This thread's pinned header slot and event on the current device (the slot
+// is read only after the event, within the same call).
+struct HeaderSlot {
+  void* pinned = nullptr;
+  cudaEvent_t ev = nullptr;
+};
+HeaderSlot& header_slot(int dev) {
+  thread_local std::map<int, HeaderSlot> slots;
+  HeaderSlot& h = slots[dev];
+  if (h.pinned == nullptr) {
+    if (cudaHostAlloc(&h.pinned, 64, cudaHostAllocDefault) != cudaSuccess)
+      throw std::runtime_error("could not allocate a pinned header slot");
+    if (cudaEventCreateWithFlags(&h.ev, cudaEventDisableTiming) != cudaSuccess)
+      throw std::runtime_error("could not create the header event");
+  }
+  return h;
+}
+
+// The forward after its geometry arguments are set: `geom_async(header_host)`
+// launches the projection pass and the header copy, `geom_sync(info)` is the
+// synchronous geometry call of the exact plan.  Allocates the binning state
+// into `bin`, renders, returns R.
+template <typename GeomAsync, typename GeomSync>
+int64_t planned_forward(w2w_settings& st, const Tensor& geom, const Tensor& img, const Tensor& color,
+                        const Tensor& depth, const Tensor& alpha, Tensor& bin, const torch::TensorOptions& bopt,
+                        int dev, GeomAsync geom_async, GeomSync geom_sync, w2w_stream_t stream, const char* what) {
+  const int W = st.width, H = st.height;
+  w2w_geometry_info info{};
+  auto render_exact = [&]() {
+    bin = torch::empty({int64_t(w2w_binning_state_bytes(info.num_rendered, W, H))}, bopt);
+    pybind11::gil_scoped_release nogil;
+    check(w2w_forward_render(&st, geom.data_ptr(), &info, bin.data_ptr(), img.data_ptr(), color.data_ptr<float>(),
+                             depth.data_ptr<float>(), alpha.data_ptr<float>(), stream),
+          "w2w_forward_render");
+  };
+  if (st.P == 0 || !planned_enabled()) {
+    {
+      pybind11::gil_scoped_release nogil;
+      check(geom_sync(&info), what);
+    }
+    render_exact();
+    return info.num_rendered;
+  }
+  const auto key = std::make_tuple(dev, int64_t(st.P), H, W);
+  PlanState ps;
+  {
+    std::lock_guard<std::mutex> lk(g_plan_mu);
+    ps = g_plans[key];
+  }
+  HeaderSlot& hs = header_slot(dev);
+  {
+    pybind11::gil_scoped_release nogil;
+    check(geom_async(hs.pinned), what);
+    if (cudaEventRecord(hs.ev, reinterpret_cast<cudaStream_t>(stream)) != cudaSuccess)
+      throw std::runtime_error(std::string(what) + ": could not record the header event");
+  }
+  bool fits = false;
+  if (ps.capacity > 0) {
+    bin = torch::empty({int64_t(w2w_binning_state_bytes(ps.capacity, W, H))}, bopt);
+    pybind11::gil_scoped_release nogil;
+    check(w2w_forward_render_planned(&st, geom.data_ptr(), ps.capacity, ps.depth_bits, bin.data_ptr(),
+                                     img.data_ptr(), color.data_ptr<float>(), depth.data_ptr<float>(),
+                                     alpha.data_ptr<float>(), stream),
+          "w2w_forward_render_planned");
+  }
+  {
+    pybind11::gil_scoped_release nogil;
+    if (cudaEventSynchronize(hs.ev) != cudaSuccess) throw std::runtime_error(std::string(what) + ": CUDA error");
+  }
+  check(w2w_geometry_info_from_header(hs.pinned, &info), what);
+  const int need = w2w_depth_bits_needed(&info);
+  if (ps.capacity > 0) fits = info.num_rendered <= ps.capacity && need <= ps.depth_bits;
+  {
+    std::lock_guard<std::mutex> lk(g_plan_mu);
+    PlanState& p = g_plans[key];
+    if (info.num_rendered > p.capacity) p.capacity = w2w_planned_capacity(info.num_rendered);
+    if (need > p.depth_bits) p.depth_bits = need;
+  }
+  if (!fits) render_exact();  // the planned launches (if any) processed no instance
+  return info.num_rendered;
+}
+
+// The instance count a binning state handed back by the forward is laid out
+// for (R, or a planned render's capacity).
+int64_t layout_count(int64_t R, const Tensor& binningBuffer, int W, int H) {
+  const long long L = w2w_binning_layout_count(R, size_t(binningBuffer.numel()), W, H);
+  TORCH_CHECK(L >= R, "binningBuffer does not match R");
+  return L;
+}
+
 struct Camera {
   Tensor view, proj, campos, bg;
 };
@@ -196,23 +312,21 @@ std::tuple<int64_t, Tensor, Tensor, Tensor, Tensor, Tensor, Tensor, Tensor> rast
   st.projmatrix = cam.proj.data_ptr<float>();
   st.campos = cam.campos.data_ptr<float>();
   st.background = cam.bg.data_ptr<float>();
-  w2w_geometry_info info{};
   const w2w_stream_t stream = cur_stream();
-  {
-    pybind11::gil_scoped_release nogil;
-    check(w2w_forward_geometry(&st, m.data_ptr<float>(), s.data_ptr<float>(), r.data_ptr<float>(),
-                               o.data_ptr<float>(), M > 0 ? shc.data_ptr<float>() : nullptr,
-                               radii.data_ptr<int>(), geom.data_ptr(), &info, stream),
-          "w2w_forward_geometry");
-  }
-  const int64_t R = info.num_rendered;
-  Tensor bin = torch::empty({int64_t(w2w_binning_state_bytes(R, W, H))}, bopt);
-  {
-    pybind11::gil_scoped_release nogil;
-    check(w2w_forward_render(&st, geom.data_ptr(), &info, bin.data_ptr(), img.data_ptr(), color.data_ptr<float>(),
-                             depth.data_ptr<float>(), alpha.data_ptr<float>(), stream),
-          "w2w_forward_render");
-  }
+  const float* shp = M > 0 ? shc.data_ptr<float>() : nullptr;
+  Tensor bin;
+  const int64_t R = planned_forward(
+      st, geom, img, color, depth, alpha, bin, bopt, dev.index(),
+      [&](void* header) {
+        return w2w_forward_geometry_async(&st, m.data_ptr<float>(), s.data_ptr<float>(), r.data_ptr<float>(),
+                                          o.data_ptr<float>(), shp, radii.data_ptr<int>(), geom.data_ptr(), header,
+                                          stream);
+      },
+      [&](w2w_geometry_info* info) {
+        return w2w_forward_geometry(&st, m.data_ptr<float>(), s.data_ptr<float>(), r.data_ptr<float>(),
+                                    o.data_ptr<float>(), shp, radii.data_ptr<int>(), geom.data_ptr(), info, stream);
+      },
+      stream, "w2w_forward_geometry");
   defer_bin_check(bin, R, W, H, reinterpret_cast<cudaStream_t>(stream), "w2w_forward_render");
   return std::make_tuple(R, color, depth, alpha, radii, geom, bin, img);
 }
@@ -257,7 +371,7 @@ std::tuple<Tensor, Tensor, Tensor, Tensor, Tensor, Tensor, Tensor, Tensor> raste
   }
   TORCH_CHECK(geomBuffer.numel() >= int64_t(w2w_geometry_state_bytes(int(P))), "geomBuffer does not match P");
   TORCH_CHECK(imageBuffer.numel() >= int64_t(w2w_image_state_bytes(W, H)), "imageBuffer does not match H, W");
-  TORCH_CHECK(binningBuffer.numel() >= int64_t(w2w_binning_state_bytes(R, W, H)), "binningBuffer does not match R");
+  const int64_t LR = layout_count(R, binningBuffer, W, H);  // R, or a planned render's capacity
   Camera cam = camera(viewmatrix, projmatrix, campos, background, dev);
   const auto fopt = torch::TensorOptions().dtype(torch::kFloat32).device(dev);
   Tensor dmean2D = torch::empty({P, 3}, fopt), dcolors = torch::empty({P, 3}, fopt),
@@ -279,7 +393,7 @@ std::tuple<Tensor, Tensor, Tensor, Tensor, Tensor, Tensor, Tensor, Tensor> raste
   {
     pybind11::gil_scoped_release nogil;
     check(w2w_backward(&st, m.data_ptr<float>(), s.data_ptr<float>(), r.data_ptr<float>(),
-                       M > 0 ? shc.data_ptr<float>() : nullptr, rad.data_ptr<int>(), geomBuffer.data_ptr(), R,
+                       M > 0 ? shc.data_ptr<float>() : nullptr, rad.data_ptr<int>(), geomBuffer.data_ptr(), LR,
                        binningBuffer.data_ptr(), imageBuffer.data_ptr(), al.data_ptr<float>(), g.data_ptr<float>(),
                        gd.numel() ? gd.data_ptr<float>() : nullptr, ga.numel() ? ga.data_ptr<float>() : nullptr,
                        int(grad_mode), scratch.data_ptr(),
@@ -353,23 +467,21 @@ std::tuple<int64_t, Tensor, Tensor, Tensor, Tensor, Tensor, Tensor, Tensor> rast
   st.compat_spill = compat_spill ? 1 : 0;
   st.viewmatrix = cam.view.data_ptr<float>(); st.projmatrix = cam.proj.data_ptr<float>();
   st.campos = cam.campos.data_ptr<float>(); st.background = cam.bg.data_ptr<float>();
-  w2w_geometry_info info{};
   const w2w_stream_t stream = cur_stream();
-  {
-    pybind11::gil_scoped_release nogil;
-    check(w2w_forward_geometry_raw(&st, m.data_ptr<float>(), sv.data_ptr<float>(), q.data_ptr<float>(),
-                                   lo.data_ptr<float>(), dc.data_ptr<float>(), ac.data_ptr<float>(),
-                                   radii.data_ptr<int>(), geom.data_ptr(), &info, stream),
-          "w2w_forward_geometry_raw");
-  }
-  const int64_t R = info.num_rendered;
-  Tensor bin = torch::empty({int64_t(w2w_binning_state_bytes(R, W, H))}, bopt);
-  {
-    pybind11::gil_scoped_release nogil;
-    check(w2w_forward_render(&st, geom.data_ptr(), &info, bin.data_ptr(), img.data_ptr(), color.data_ptr<float>(),
-                             depth.data_ptr<float>(), alpha.data_ptr<float>(), stream),
-          "w2w_forward_render");
-  }
+  Tensor bin;
+  const int64_t R = planned_forward(
+      st, geom, img, color, depth, alpha, bin, bopt, dev.index(),
+      [&](void* header) {
+        return w2w_forward_geometry_raw_async(&st, m.data_ptr<float>(), sv.data_ptr<float>(), q.data_ptr<float>(),
+                                              lo.data_ptr<float>(), dc.data_ptr<float>(), ac.data_ptr<float>(),
+                                              radii.data_ptr<int>(), geom.data_ptr(), header, stream);
+      },
+      [&](w2w_geometry_info* info) {
+        return w2w_forward_geometry_raw(&st, m.data_ptr<float>(), sv.data_ptr<float>(), q.data_ptr<float>(),
+                                        lo.data_ptr<float>(), dc.data_ptr<float>(), ac.data_ptr<float>(),
+                                        radii.data_ptr<int>(), geom.data_ptr(), info, stream);
+      },
+      stream, "w2w_forward_geometry_raw");
   defer_bin_check(bin, R, W, H, reinterpret_cast<cudaStream_t>(stream), "w2w_forward_render");
   return std::make_tuple(R, color, depth, alpha, radii, geom, bin, img);
 }
@@ -401,7 +513,7 @@ std::tuple<Tensor, Tensor, Tensor, Tensor, Tensor, Tensor, Tensor> rasterize_gau
   TORCH_CHECK(radii.is_cuda() && radii.scalar_type() == torch::kInt32 && radii.numel() == P, "radii must be int32 [P]");
   TORCH_CHECK(geomBuffer.numel() >= int64_t(w2w_geometry_state_bytes(int(P))), "geomBuffer does not match P");
   TORCH_CHECK(imageBuffer.numel() >= int64_t(w2w_image_state_bytes(W, H)), "imageBuffer does not match H, W");
-  TORCH_CHECK(binningBuffer.numel() >= int64_t(w2w_binning_state_bytes(R, W, H)), "binningBuffer does not match R");
+  const int64_t LR = layout_count(R, binningBuffer, W, H);  // R, or a planned render's capacity
   Tensor rad = radii.contiguous();
   const int64_t K = ac.size(1);
   Camera cam = camera(viewmatrix, projmatrix, campos, background, dev);
@@ -423,7 +535,7 @@ std::tuple<Tensor, Tensor, Tensor, Tensor, Tensor, Tensor, Tensor> rasterize_gau
   {
     pybind11::gil_scoped_release nogil;
     check(w2w_backward_raw(&st, m.data_ptr<float>(), sv.data_ptr<float>(), q.data_ptr<float>(), lo.data_ptr<float>(),
-                           dc.data_ptr<float>(), ac.data_ptr<float>(), rad.data_ptr<int>(), geomBuffer.data_ptr(), R,
+                           dc.data_ptr<float>(), ac.data_ptr<float>(), rad.data_ptr<int>(), geomBuffer.data_ptr(), LR,
                            binningBuffer.data_ptr(), imageBuffer.data_ptr(), al.data_ptr<float>(), g.data_ptr<float>(),
                            gd.numel() ? gd.data_ptr<float>() : nullptr, ga.numel() ? ga.data_ptr<float>() : nullptr,
                            scratch.data_ptr(), size_t(scratch.numel()),
@@ -578,7 +690,9 @@ std::tuple<Tensor, Tensor, Tensor, Tensor> blend(const Tensor& geomBuffer, int64
 Tensor binning_keys64(const Tensor& binningBuffer, int64_t R, int64_t image_height, int64_t image_width) {
   c10::cuda::CUDAGuard guard(binningBuffer.device());
   Tensor out = torch::empty({R}, binningBuffer.options().dtype(torch::kInt64));
-  check(w2w_binning_keys64(binningBuffer.data_ptr(), R, int(image_width), int(image_height),
+  check(w2w_binning_keys64_layout(binningBuffer.data_ptr(), R,
+                                 layout_count(R, binningBuffer, int(image_width), int(image_height)),
+                                 int(image_width), int(image_height),
                            reinterpret_cast<uint64_t*>(out.data_ptr<int64_t>()), cur_stream()),
         "w2w_binning_keys64");
   return out;
@@ -642,6 +756,10 @@ PYBIND11_MODULE(TORCH_EXTENSION_NAME, m) {
   m.def("blend", &blend, py::arg("geomBuffer"), py::arg("P"), py::arg("ranges"), py::arg("point_list"),
         py::arg("image_height"), py::arg("image_width"), py::arg("background") = py::none());
   m.def("binning_keys64", &binning_keys64);
+  m.def("planned_capacity", [](int64_t R) { return int64_t(w2w_planned_capacity(R)); });
+  m.def("binning_layout_count", [](int64_t R, const Tensor& binningBuffer, int64_t H, int64_t W) {
+    return layout_count(R, binningBuffer, int(W), int(H));
+  });
   m.def("state_error", &state_error);
   m.def("geometry_state_bytes", [](int64_t P) { return int64_t(w2w_geometry_state_bytes(int(P))); });
   m.def("image_state_bytes", [](int64_t W, int64_t H) { return int64_t(w2w_image_state_bytes(int(W), int(H))); });

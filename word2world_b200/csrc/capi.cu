@@ -312,11 +312,10 @@ struct RawParams {
   const float *svec, *quat, *logit, *sh_dc, *sh_ac;
 };
 
-static int forward_geometry(const w2w_settings* s, const float* means3D, const float* scales, const float* rotations,
-                            const float* opacities, const float* shs, const RawParams* raw, int* radii,
-                            void* geom_state, w2w_geometry_info* info, w2w_stream_t stream) {
-  std::memset(info, 0, sizeof(*info));
-  if (s->P == 0) return W2W_OK;
+// The projection pass alone (P > 0): header cleared, preprocess launched.
+static int geometry_launch(const w2w_settings* s, const float* means3D, const float* scales, const float* rotations,
+                           const float* opacities, const float* shs, const RawParams* raw, int* radii,
+                           void* geom_state, w2w_stream_t stream) {
   const GeomLayout L(s->P);
   cudaStream_t st = S(stream);
   cudaMemsetAsync(geom_state, 0, L.depth, st);  // header + scan status
@@ -347,10 +346,20 @@ static int forward_geometry(const w2w_settings* s, const float* means3D, const f
     a.svec = raw->svec; a.quat = raw->quat; a.logit = raw->logit; a.sh_dc = raw->sh_dc; a.sh_ac = raw->sh_ac;
   }
   launch_preprocess(a, st);
-  int rc = check_launch();
+  return check_launch();
+}
+
+static int forward_geometry(const w2w_settings* s, const float* means3D, const float* scales, const float* rotations,
+                            const float* opacities, const float* shs, const RawParams* raw, int* radii,
+                            void* geom_state, w2w_geometry_info* info, w2w_stream_t stream) {
+  std::memset(info, 0, sizeof(*info));
+  if (s->P == 0) return W2W_OK;
+  const int rc = geometry_launch(s, means3D, scales, rotations, opacities, shs, raw, radii, geom_state, stream);
   if (rc) return rc;
+  cudaStream_t st = S(stream);
   GeomHeader h;
-  if (cudaMemcpyAsync(&h, a.header, sizeof(h), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+  if (cudaMemcpyAsync(&h, at<GeomHeader>(geom_state, GeomLayout(s->P).header), sizeof(h), cudaMemcpyDeviceToHost,
+                      st) != cudaSuccess ||
       cudaStreamSynchronize(st) != cudaSuccess)
     return W2W_ERR_CUDA;
   info->num_rendered = h.num_rendered;
@@ -506,6 +515,228 @@ int w2w_forward_render(const w2w_settings* s, const void* geom_state, const w2w_
   b.spin_limit = spin_limit();
   launch_blend(b, st);
   return finish(err_word, st);
+}
+
+// ---- planned forward --------------------------------------------------------
+// A render whose sort and blend are launched before the host knows the view's
+// instance count R: the binning state is laid out for a capacity C and the
+// keys carry a guessed number of depth bits; a one-thread kernel checks both
+// against the projection pass's header on the device and either lets the
+// emission, histogram, sort passes and blend process R instances (read from
+// device memory), or sets `replan` and makes them process none, after which
+// the caller renders again with the exact plan.  A guess with more depth bits
+// than the view needs sorts the same way: the extra bits are the common high
+// bits of every depth (the range of the depths' bit patterns), constant across
+// the keys, so the sorted list, the ranges and everything after them are
+// bit-identical to the exact plan's.
+
+static int geometry_async(const w2w_settings* s, const float* means3D, const float* scales, const float* rotations,
+                          const float* opacities, const float* shs, const RawParams* raw, int* radii,
+                          void* geom_state, void* header_host, w2w_stream_t stream) {
+  if (!header_host) return W2W_ERR_INVALID;
+  if (s->P == 0) {
+    std::memset(header_host, 0, 16);
+    return W2W_OK;
+  }
+  const int rc = geometry_launch(s, means3D, scales, rotations, opacities, shs, raw, radii, geom_state, stream);
+  if (rc) return rc;
+  // the header's first four words: error, depth min (inverted), depth max, R
+  if (cudaMemcpyAsync(header_host, at<GeomHeader>(geom_state, GeomLayout(s->P).header), 16, cudaMemcpyDeviceToHost,
+                      S(stream)) != cudaSuccess)
+    return W2W_ERR_CUDA;
+  return W2W_OK;
+}
+
+int w2w_forward_geometry_async(const w2w_settings* s, const float* means3D, const float* scales,
+                               const float* rotations, const float* opacities, const float* shs, int* radii,
+                               void* geom_state, void* header_host, w2w_stream_t stream) {
+  if (!settings_ok(s) || (s->P > 0 && (!means3D || !scales || !rotations || !opacities || !radii || !geom_state ||
+                                       (s->M > 0 && !shs))))
+    return W2W_ERR_INVALID;
+  return geometry_async(s, means3D, scales, rotations, opacities, shs, nullptr, radii, geom_state, header_host,
+                        stream);
+}
+
+int w2w_forward_geometry_raw_async(const w2w_settings* s, const float* means3D, const float* svec,
+                                   const float* quaternion, const float* opacity_logit, const float* sh_dc,
+                                   const float* sh_ac, int* radii, void* geom_state, void* header_host,
+                                   w2w_stream_t stream) {
+  if (!settings_ok(s) || s->M < 1 || s->M > 16 ||
+      (s->P > 0 && (!means3D || !svec || !quaternion || !opacity_logit || !sh_dc || (s->M > 1 && !sh_ac) ||
+                    !radii || !geom_state)))
+    return W2W_ERR_INVALID;
+  const RawParams raw{svec, quaternion, opacity_logit, sh_dc, sh_ac};
+  return geometry_async(s, means3D, nullptr, nullptr, nullptr, nullptr, &raw, radii, geom_state, header_host, stream);
+}
+
+int w2w_geometry_info_from_header(const void* header_host, w2w_geometry_info* info) {
+  if (!header_host || !info) return W2W_ERR_INVALID;
+  uint32_t w[4];
+  std::memcpy(w, header_host, sizeof(w));
+  std::memset(info, 0, sizeof(*info));
+  info->error = w[0];
+  info->depth_min_bits = ~w[1];
+  info->depth_max_bits = w[2];
+  info->num_rendered = w[3];
+  if (w[0] & kErrTimeout) return W2W_ERR_TIMEOUT;
+  if (w[0] & kErrCapacity) return W2W_ERR_CAPACITY;
+  return W2W_OK;
+}
+
+int w2w_depth_bits_needed(const w2w_geometry_info* info) {
+  if (!info) return -1;
+  const uint32_t x = info->depth_min_bits ^ info->depth_max_bits;
+  int db = 0;
+  while (db < 32 && (x >> db) != 0u) ++db;
+  return db;
+}
+
+long long w2w_planned_capacity(long long num_rendered) {
+  if (num_rendered < 0) return -1;
+  const long long want = num_rendered + num_rendered / 4;  // 25 % headroom over the count it was sized from
+  long long c = (want + W2W_PLAN_QUANTUM - 1) / W2W_PLAN_QUANTUM * W2W_PLAN_QUANTUM;
+  if (c < W2W_PLAN_QUANTUM) c = W2W_PLAN_QUANTUM;
+  return c < (1LL << 30) ? c : -1;
+}
+
+long long w2w_binning_layout_count(long long num_rendered, size_t state_bytes, int W, int H) {
+  if (num_rendered < 0 || W <= 0 || H <= 0) return -1;
+  const int T = num_tiles(W, H);
+  if (BinLayout(num_rendered, T).total == state_bytes) return num_rendered;
+  // a planned render's state: the capacity, a multiple of W2W_PLAN_QUANTUM at
+  // least num_rendered (the layout grows by more than 16 bytes per instance,
+  // so at most state_bytes / 16 of them)
+  long long lo = (num_rendered + W2W_PLAN_QUANTUM - 1) / W2W_PLAN_QUANTUM;
+  long long hi = (long long)(state_bytes / 16) / W2W_PLAN_QUANTUM + 1;
+  if (lo < 1) lo = 1;
+  while (lo < hi) {
+    const long long mid = (lo + hi) / 2;
+    if (BinLayout(mid * W2W_PLAN_QUANTUM, T).total < state_bytes) lo = mid + 1;
+    else hi = mid;
+  }
+  return BinLayout(lo * W2W_PLAN_QUANTUM, T).total == state_bytes ? lo * W2W_PLAN_QUANTUM : -1;
+}
+
+}  // extern "C"
+
+// The planned render's header: the caller's key plan, checked against the
+// view's own count and depth range (the projection pass's header).
+__global__ void plan_bin_header(BinHeader* h, const GeomHeader* g, uint32_t capacity, KeyPlan k, uint32_t passes) {
+  const uint32_t R = g->num_rendered;
+  const uint32_t dmin = ~g->depth_min, dmax = g->depth_max;
+  const uint32_t x = dmin ^ dmax;
+  int need = 0;
+  while (need < 32 && (x >> need) != 0u) ++need;
+  const bool ok = R <= capacity && need <= k.depth_bits && (g->error & (kErrTimeout | kErrCapacity)) == 0u;
+  h->error = 0u;
+  h->masks_valid = 1u;
+  h->key64 = k.key64;
+  h->depth_bits = k.depth_bits;
+  h->depth_prefix = k.depth_bits >= 32 ? 0u : (dmin & ~((1u << k.depth_bits) - 1u));
+  h->tile_bits = k.tile_bits;
+  h->passes = passes;
+  h->num_rendered = R;
+  h->n_sort = ok ? R : 0u;
+  h->replan = ok ? 0u : 1u;
+  for (int i = 0; i < 8; ++i) h->tile_counter[i] = 0;
+}
+
+extern "C" {
+
+int w2w_forward_render_planned(const w2w_settings* s, const void* geom_state, long long capacity, int depth_bits,
+                               void* binning_state, void* image_state, float* out_color, float* out_depth,
+                               float* out_alpha, w2w_stream_t stream) {
+  if (!settings_ok(s) || s->P <= 0 || !geom_state || !binning_state || !image_state || !out_color || !out_depth ||
+      !out_alpha || capacity < 1 || capacity >= (1LL << 30) || depth_bits < 0 || depth_bits > 32)
+    return W2W_ERR_INVALID;
+  cudaStream_t st = S(stream);
+  const int W = s->width, H = s->height, T = num_tiles(W, H);
+  const ImageLayout IL(W, H);
+  const GeomLayout GL(s->P);
+  const BinLayout BL(capacity, T);
+  KeyPlan kp{};
+  kp.depth_bits = depth_bits;
+  kp.tile_bits = ceil_log2(uint32_t(T));
+  kp.bits = kp.tile_bits + kp.depth_bits;
+  kp.key64 = kp.bits > 32 ? 1 : 0;
+  const int passes = sort_passes(kp.bits);
+  BinHeader* bh = at<BinHeader>(binning_state, BL.header);
+  stage_begin(kStOther, st);
+  plan_bin_header<<<1, 1, 0, st>>>(bh, at<GeomHeader>(geom_state, GL.header), uint32_t(capacity), kp,
+                                   uint32_t(passes));
+  stage_end(kStOther, st, 1);
+  // the sort result lands in (keysA, valsA); key emission targets the buffer
+  // that makes the ping-pong end there
+  const bool odd = (passes % 2) == 1;
+  void* keysA = at<void>(binning_state, BL.keysA);
+  void* keysB = at<void>(binning_state, BL.keysB);
+  uint32_t* valsA = at<uint32_t>(binning_state, BL.valsA);
+  uint32_t* valsB = at<uint32_t>(binning_state, BL.valsB);
+  DuplicateArgs d{};
+  d.P = s->P; d.gw = tiles_x(W); d.R = uint32_t(capacity); d.key64 = kp.key64;
+  d.depth_bits = uint32_t(kp.depth_bits);
+  d.tiles = at<uint32_t>(geom_state, GL.tiles);
+  d.offsets = at<uint32_t>(geom_state, GL.offsets);
+  d.rect = at<uint32_t>(geom_state, GL.rect);
+  d.prev_reach = at<uint32_t>(geom_state, GL.prev_reach);
+  d.depth = at<float>(geom_state, GL.depth);
+  d.keys = odd ? keysB : keysA;
+  d.vals = odd ? valsB : valsA;
+  d.n_dev = &bh->n_sort;
+  launch_duplicate(d, st);
+  SortArgs so{};
+  so.n = capacity; so.key64 = kp.key64; so.begin_bit = 0; so.bits = kp.bits;
+  so.keys_in = d.keys; so.vals_in = d.vals;
+  so.match_rank = 1;  // emitted Gaussian by Gaussian: few distinct digits per warp
+  so.n_dev = &bh->n_sort;
+  so.keys_out = keysA; so.vals_out = valsA;
+  so.keys_tmp = keysB; so.vals_tmp = valsB;
+  so.hist = at<uint32_t>(binning_state, BL.hist);
+  so.status = at<uint32_t>(binning_state, BL.status);
+  so.counters = bh->tile_counter;
+  so.error = &bh->error;
+  so.tile_shift = kp.depth_bits;
+  so.num_tiles = T;
+  so.tile_hist = at<uint32_t>(binning_state, BL.tile_hist);
+  so.ranges = at<uint2>(image_state, IL.ranges);
+  so.clear_span = at<void>(binning_state, BL.hist);
+  so.clear_bytes = BL.status - BL.hist + size_t(passes > 0 ? passes : 1) * kMaxBins * 4 *
+                   size_t((capacity + sort_tile_keys(kp.key64) - 1) / sort_tile_keys(kp.key64));
+  so.spin_limit = spin_limit();
+  so.unpublished_tile = unpublished_tile(kWaitSort);
+  launch_sort(so, st);
+  BlendArgs b{};
+  b.W = W; b.H = H;
+  b.ranges = at<uint2>(image_state, IL.ranges);
+  b.point_list = valsA;
+  b.record = at<float>(geom_state, GL.record);
+  b.num_records = uint32_t(s->P);
+  b.mask_top = at<uint8_t>(binning_state, BL.masks);
+  b.mask_bottom = b.mask_top + capacity;
+  b.masks_valid = &bh->masks_valid;
+  b.bg = s->background;
+  b.out_color = out_color; b.out_depth = out_depth; b.out_alpha = out_alpha;
+  b.n_contrib = at<uint32_t>(image_state, IL.n_contrib);
+  b.T_final = at<float>(image_state, IL.T_final);
+  b.tile_max = at<uint32_t>(image_state, IL.tile_max);
+  b.order = at<uint32_t>(image_state, IL.order);
+  b.order_bwd = at<uint32_t>(image_state, IL.order_bwd);
+  b.queue = at<uint32_t>(image_state, IL.queue);
+  b.error = &bh->error;
+  b.spin_limit = spin_limit();
+  launch_blend(b, st);
+  return finish(&bh->error, st);
+}
+
+int w2w_binning_replanned(const void* binning_state, w2w_stream_t stream) {
+  if (!binning_state) return -1;
+  uint32_t v = 0;
+  cudaStream_t st = S(stream);
+  if (cudaMemcpyAsync(&v, &static_cast<const BinHeader*>(binning_state)->replan, 4, cudaMemcpyDeviceToHost, st) !=
+          cudaSuccess ||
+      cudaStreamSynchronize(st) != cudaSuccess)
+    return -1;
+  return int(v);
 }
 
 int w2w_state_error(const void* state, int which, w2w_stream_t stream) {
@@ -891,10 +1122,11 @@ int w2w_blend(const w2w_settings* s, const void* geom_state, const uint32_t* ran
   return check_launch();
 }
 
-int w2w_binning_keys64(const void* binning_state, long long R, int W, int H, uint64_t* out, w2w_stream_t stream) {
-  if (R < 0 || !out || (R > 0 && !binning_state)) return W2W_ERR_INVALID;
+int w2w_binning_keys64_layout(const void* binning_state, long long R, long long layout_count, int W, int H,
+                              uint64_t* out, w2w_stream_t stream) {
+  if (R < 0 || layout_count < R || !out || (R > 0 && !binning_state)) return W2W_ERR_INVALID;
   if (R == 0) return W2W_OK;
-  const BinLayout BL(R, num_tiles(W, H));
+  const BinLayout BL(layout_count, num_tiles(W, H));
   const BinHeader* h = at<BinHeader>(binning_state, BL.header);
   BinHeader hh;
   cudaStream_t st = S(stream);
@@ -907,6 +1139,10 @@ int w2w_binning_keys64(const void* binning_state, long long R, int W, int H, uin
   else expand_keys<uint32_t><<<blocks, 256, 0, st>>>(h, at<uint32_t>(binning_state, BL.keysA), R, out);
   stage_end(kStOther, st, 1);
   return check_launch();
+}
+
+int w2w_binning_keys64(const void* binning_state, long long R, int W, int H, uint64_t* out, w2w_stream_t stream) {
+  return w2w_binning_keys64_layout(binning_state, R, R, W, H, out, stream);
 }
 
 }  // extern "C"

@@ -400,7 +400,9 @@ struct BinHeader {
   uint32_t passes;         // 8-bit digit passes
   uint32_t num_rendered;
   uint32_t masks_valid;    // 1: the blend wrote the block masks (BinLayout::masks) for the backward
-  uint32_t pad[8];
+  uint32_t n_sort;         // planned render: instances the emission and sort process (R, or 0 to replan)
+  uint32_t replan;         // planned render: 1 when R or the depth range did not fit the plan
+  uint32_t pad[6];
   uint32_t tile_counter[8];  // per-pass tile acquisition counters (onesweep)
 };
 

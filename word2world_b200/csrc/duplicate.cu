@@ -30,8 +30,10 @@ __global__ void __launch_bounds__(kDupThreads) duplicate_kernel(DuplicateArgs a)
   const int warp_global = (blockIdx.x * kDupThreads + threadIdx.x) >> 5;
   const int g = warp_global * 32 + lane;
   uint32_t p0 = 0, cnt = 0, start = 0, x0 = 0, y0 = 0, w = 1, dlow = 0, gwv = uint32_t(a.gw), tbase = 0;
+  // a planned render's instance count is read from device memory (a.R is then the capacity)
+  const uint32_t Rlim = a.n_dev != nullptr ? min(*a.n_dev, a.R) : a.R;
   if (g < a.P) {  // Gaussians that emit nothing have an empty rectangle
-    uint32_t end = a.R;
+    uint32_t end = Rlim;
     if (a.items != nullptr) {  // batched: this view's tile grid, first tile id and end slot
       const int item = find_item_elem(a.items, a.num_items, uint32_t(g));
       gwv = uint32_t(a.items[item].gw);
@@ -85,7 +87,7 @@ __global__ void __launch_bounds__(kDupThreads) duplicate_kernel(DuplicateArgs a)
       const uint32_t k = p - ost;
       const uint32_t ty = oy0 + k / ow, tx = ox0 + k % ow;
       const uint32_t tile = otb + ty * ogw + tx;
-      if (p < a.R) {
+      if (p < Rlim) {
         if constexpr (kKey64) {
           reinterpret_cast<uint64_t*>(a.keys)[p] = (uint64_t(tile) << a.depth_bits) | odl;
         } else {

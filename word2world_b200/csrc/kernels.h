@@ -100,6 +100,7 @@ struct DuplicateArgs {
   const float* depth;
   void* keys;
   uint32_t* vals;
+  const uint32_t* n_dev = nullptr;  // planned render: the instance count in device memory (R is then the capacity)
 };
 void launch_duplicate(const DuplicateArgs& a, cudaStream_t stream);
 
@@ -128,6 +129,7 @@ struct SortArgs {
   uint32_t spin_limit = kSpinLimit;  // bounded waits (spin_limit())
   long long unpublished_tile = -1;   // first pass: tile that skips publishing (tests; -1 = none)
   int match_rank = 0;  // 1: rank digits with match.any (keys whose warps hold few distinct digits)
+  const uint32_t* n_dev = nullptr;  // planned render: the key count in device memory (n is then the capacity)
   int stage_hist = -1, stage_pass = -1;  // timing stages (default: the sort's own)
   int tile_shift;
   int num_tiles;
@@ -348,7 +350,8 @@ enum TuneKnob {
   kTuneBinning = 3,
   kTuneBlendQueue = 4,
   kTunePreBlocks = 5,
-  kNumTuneKnobs = 6
+  kTunePlanned = 6,
+  kNumTuneKnobs = 7
 };
 int tune_value(int knob);
 

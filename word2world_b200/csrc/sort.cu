@@ -93,7 +93,8 @@ __device__ __forceinline__ void count_run(const K (&k)[kHistRun], int cnt, int s
 template <typename K>
 __global__ void __launch_bounds__(kHistThreads)
 hist_kernel(const K* __restrict__ keys, long long n, int begin_bit, int passes, int dbits, int bits,
-            uint32_t* __restrict__ hist, int tile_shift, int num_tiles, uint32_t* __restrict__ tile_hist) {
+            uint32_t* __restrict__ hist, int tile_shift, int num_tiles, uint32_t* __restrict__ tile_hist,
+            const uint32_t* __restrict__ n_dev) {
   extern __shared__ uint32_t smem[];
   uint32_t* sh = smem;                      // passes * kMaxBins
   uint32_t* st = smem + passes * kMaxBins;  // num_tiles when they fit
@@ -102,7 +103,8 @@ hist_kernel(const K* __restrict__ keys, long long n, int begin_bit, int passes, 
   if (tiles_in_smem)
     for (int i = threadIdx.x; i < num_tiles; i += blockDim.x) st[i] = 0;
   __syncthreads();
-  const uint32_t nn = uint32_t(n);  // n < 2^30 (checked by every caller)
+  // n < 2^30 (checked by every caller); a planned render's count is in device memory
+  const uint32_t nn = n_dev != nullptr ? min(*n_dev, uint32_t(n)) : uint32_t(n);
   const bool vec = (reinterpret_cast<uintptr_t>(keys) & 15u) == 0u;
   const uint32_t runs = (nn + kHistRun - 1) / kHistRun;
   for (uint32_t c = blockIdx.x * blockDim.x + threadIdx.x; c < runs; c += gridDim.x * blockDim.x) {
@@ -402,7 +404,7 @@ __global__ void __launch_bounds__(kSortThreads, OnesweepShape<K>::kMinBlocks)
 onesweep_kernel(const K* __restrict__ kin, const uint32_t* __restrict__ vin, K* __restrict__ kout,
                 uint32_t* __restrict__ vout, long long n, int shift,
                 const uint32_t* __restrict__ digit_base, uint32_t* status, uint32_t* counter, uint32_t* err,
-                uint32_t spin_limit, long long unpublished_tile) {
+                uint32_t spin_limit, long long unpublished_tile, const uint32_t* __restrict__ n_dev) {
   constexpr int kTile = onesweep_tile<K>();
   static_assert(kSortThreads * 2 >= kMaxBins, "at most two digits per thread");
   __shared__ __align__(16) OnesweepShared<K> sm;
@@ -416,7 +418,11 @@ onesweep_kernel(const K* __restrict__ kin, const uint32_t* __restrict__ vin, K* 
   }
   __syncthreads();
   const uint32_t tile = sm.tile;
-  const uint32_t nn = uint32_t(n);  // n < 2^30 (checked by every caller)
+  // n < 2^30 (checked by every caller).  A planned render launches tiles for
+  // its capacity and reads the count from device memory: a tile past the
+  // count has no keys, and no real tile looks back at it.
+  const uint32_t nn = n_dev != nullptr ? min(*n_dev, uint32_t(n)) : uint32_t(n);
+  if ((unsigned long long)tile * kTile >= nn) return;
   const bool publish = (long long)tile != unpublished_tile;
   if ((unsigned long long)(tile + 1) * kTile <= nn)
     onesweep_tile_pass<K, kWidth, true, kMatch>(kin, vin, kout, vout, nn, shift, digit_base, status, err, tile, spin_limit,
@@ -429,7 +435,7 @@ onesweep_kernel(const K* __restrict__ kin, const uint32_t* __restrict__ vin, K* 
 template <typename K, int kWidth, bool kMatch>
 void launch_onesweep_w(int tiles, cudaStream_t stream, const K* kin, const uint32_t* vin, K* kout, uint32_t* vout,
                        long long n, int shift, const uint32_t* digit_base, uint32_t* status, uint32_t* counter,
-                       uint32_t* err, uint32_t spin_limit, long long unpublished) {
+                       uint32_t* err, uint32_t spin_limit, long long unpublished, const uint32_t* n_dev) {
   const size_t dyn = (sizeof(K) + sizeof(uint32_t)) * size_t(onesweep_tile<K>());
   // the shared-memory opt-in is set once per device (a driver call per launch
   // would widen the gap the device waits between launches)
@@ -441,22 +447,23 @@ void launch_onesweep_w(int tiles, cudaStream_t stream, const K* kin, const uint3
     if (dev >= 0 && dev < 64) opted[dev] = true;
   }
   onesweep_kernel<K, kWidth, kMatch><<<tiles, kSortThreads, dyn, stream>>>(kin, vin, kout, vout, n, shift, digit_base,
-                                                                    status, counter, err, spin_limit, unpublished);
+                                                                    status, counter, err, spin_limit, unpublished, n_dev);
 }
 
 template <typename K>
 void launch_onesweep(int width, int tiles, cudaStream_t stream, const K* kin, const uint32_t* vin, K* kout,
                      uint32_t* vout, long long n, int shift, const uint32_t* digit_base, uint32_t* status,
-                     uint32_t* counter, uint32_t* err, uint32_t spin_limit, long long unpublished, bool match) {
+                     uint32_t* counter, uint32_t* err, uint32_t spin_limit, long long unpublished, bool match,
+                     const uint32_t* n_dev) {
   switch (width) {
 #define W2W_ONESWEEP_CASE(W)                                                                                      \
   case W:                                                                                                         \
     if (match)                                                                                                    \
       launch_onesweep_w<K, W, true>(tiles, stream, kin, vin, kout, vout, n, shift, digit_base, status, counter,   \
-                                    err, spin_limit, unpublished);                                                \
+                                    err, spin_limit, unpublished, n_dev);                                         \
     else                                                                                                          \
       launch_onesweep_w<K, W, false>(tiles, stream, kin, vin, kout, vout, n, shift, digit_base, status, counter,  \
-                                     err, spin_limit, unpublished);                                               \
+                                     err, spin_limit, unpublished, n_dev);                                        \
     break;
     W2W_ONESWEEP_CASE(1) W2W_ONESWEEP_CASE(2) W2W_ONESWEEP_CASE(3) W2W_ONESWEEP_CASE(4) W2W_ONESWEEP_CASE(5)
     W2W_ONESWEEP_CASE(6) W2W_ONESWEEP_CASE(7) W2W_ONESWEEP_CASE(8) W2W_ONESWEEP_CASE(9)
@@ -498,7 +505,7 @@ void run_sort(const SortArgs& a, cudaStream_t stream) {
     stage_begin(st_hist, stream);
     hist_kernel<K><<<grid, kHistThreads, smem, stream>>>(reinterpret_cast<const K*>(a.keys_in), n, a.begin_bit,
                                                          passes, dbits, a.bits, a.hist, a.tile_shift,
-                                                         a.num_tiles, a.tile_hist);
+                                                         a.num_tiles, a.tile_hist, a.n_dev);
     offsets_kernel<<<1, 1024, 0, stream>>>(a.hist, passes, a.tile_hist, a.num_tiles, a.ranges);
     stage_end(st_hist, stream, 2);
   }
@@ -513,7 +520,7 @@ void run_sort(const SortArgs& a, cudaStream_t stream) {
     launch_onesweep<K>(pass_width(p, dbits, a.bits), int(tiles), stream, kin, vin, kout, vout, n,
                        a.begin_bit + dbits * p, a.hist + kMaxBins * p,
                        a.status + size_t(p) * kMaxBins * size_t(tiles), a.counters + p, a.error,
-                       a.spin_limit, p == 0 ? a.unpublished_tile : -1LL, a.match_rank != 0);
+                       a.spin_limit, p == 0 ? a.unpublished_tile : -1LL, a.match_rank != 0, a.n_dev);
     stage_end(st_pass, stream, 1);
     kin = kout;
     vin = vout;

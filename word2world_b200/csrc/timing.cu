@@ -71,8 +71,9 @@ uint32_t spin_limit() { return g_spin_limit.load(std::memory_order_relaxed); }
 
 namespace {
 const char* kTuneNames[kNumTuneKnobs] = {"blend_warps", "backward_split", "backward_ways",
-                                         "binning",     "blend_queue",    "preprocess_blocks"};
-std::atomic<int> g_tune[kNumTuneKnobs] = {{4}, {4}, {2}, {0}, {0}, {4}};
+                                         "binning",     "blend_queue",    "preprocess_blocks",
+                                         "planned_forward"};
+std::atomic<int> g_tune[kNumTuneKnobs] = {{4}, {4}, {2}, {0}, {0}, {4}, {1}};
 bool tune_valid(int knob, int v) {
   switch (knob) {
     case kTuneBlendWarps: return v == 4 || v == 8;
@@ -81,6 +82,7 @@ bool tune_valid(int knob, int v) {
     case kTuneBinning: return v == 0 || v == 1;
     case kTuneBlendQueue: return v == 0 || v == 1;
     case kTunePreBlocks: return v >= 2 && v <= 4;
+    case kTunePlanned: return v == 0 || v == 1;
     default: return false;
   }
 }
