@@ -412,16 +412,21 @@ onesweep_kernel(const K* __restrict__ kin, const uint32_t* __restrict__ vin, K* 
   K* s_keys = reinterpret_cast<K*>(s_dyn);
   uint32_t* s_vals = reinterpret_cast<uint32_t*>(s_dyn + sizeof(K) * kTile);
   if (threadIdx.x == 0) sm.tile = atomicAdd(counter, 1u);
+  // n < 2^30 (checked by every caller).  A planned render launches tiles for
+  // its capacity and reads the count from device memory: a tile past the
+  // count has no keys, and no real tile looks back at it, so it leaves
+  // before any other work.
+  const uint32_t nn = n_dev != nullptr ? min(*n_dev, uint32_t(n)) : uint32_t(n);
+  if (n_dev != nullptr) {  // grid-uniform
+    __syncthreads();
+    if ((unsigned long long)sm.tile * kTile >= nn) return;
+  }
   {
     uint4* z = reinterpret_cast<uint4*>(&sm.wcnt[0][0]);
     for (int i = threadIdx.x; i < int(sizeof(sm.wcnt) / 16); i += kSortThreads) z[i] = make_uint4(0u, 0u, 0u, 0u);
   }
   __syncthreads();
   const uint32_t tile = sm.tile;
-  // n < 2^30 (checked by every caller).  A planned render launches tiles for
-  // its capacity and reads the count from device memory: a tile past the
-  // count has no keys, and no real tile looks back at it.
-  const uint32_t nn = n_dev != nullptr ? min(*n_dev, uint32_t(n)) : uint32_t(n);
   if ((unsigned long long)tile * kTile >= nn) return;
   const bool publish = (long long)tile != unpublished_tile;
   if ((unsigned long long)(tile + 1) * kTile <= nn)

@@ -237,11 +237,20 @@ class Renderer:
         self.grad_mode = grad_mode
         self.compat_spill = compat_spill
         self._bg = None  # the white background (Renderer.py:169), kept across calls
+        self._zeros = None  # the screen-space points' zeros, kept across calls
 
     def render(self, FoVx, FoVy, world_view_transform, full_proj_transform, camera_center, image_width,
                image_height):
         p = self.params
-        accum_grads = torch.zeros_like(p.mean, requires_grad=True)
+        # the screen-space points (Renderer.py:121-126): zeros whose gradient
+        # the backward fills.  Each call gets a fresh leaf (its own .grad) over
+        # one zero buffer kept across calls, which nothing writes (torch
+        # refuses in-place writes to a leaf that requires grad), instead of a
+        # new zero-filled tensor per call
+        z = self._zeros
+        if z is None or z.shape != p.mean.shape or z.device != p.mean.device or z.dtype != p.mean.dtype:
+            z = self._zeros = torch.zeros_like(p.mean)
+        accum_grads = z.detach().requires_grad_(True)
         accum_grads.retain_grad()
         tanfovx = math.tan(float(FoVx) * 0.5)
         tanfovy = math.tan(float(FoVy) * 0.5)
