@@ -498,9 +498,10 @@ void run_sort(const SortArgs& a, cudaStream_t stream) {
     int sms = 148, dev = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    // a few blocks per SM: each block's flush is passes * kMaxBins global atomics
+    // a few blocks per SM: each block's flush is passes * kMaxBins global atomics (4 per SM measured
+    // 0.119 ms of histogram per 4-view step against 0.129 with 2 and 0.135 with 8)
     const long long want = (n + kHistThreads * kHistRun * 4 - 1) / (kHistThreads * kHistRun * 4);
-    const int grid = int(max(1LL, min(want, (long long)sms * 2)));
+    const int grid = int(max(1LL, min(want, (long long)sms * 4)));
     const bool tiles_in_smem = a.tile_hist != nullptr && a.num_tiles <= kSmemTileBins;
     const size_t smem =
         sizeof(uint32_t) * (size_t(passes) * kMaxBins + (tiles_in_smem ? size_t(a.num_tiles) : 0));
