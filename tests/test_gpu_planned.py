@@ -89,3 +89,31 @@ def test_planned_forward_falls_back_when_the_view_does_not_fit():
     f3, g3 = _run(arrays, near, 1, grad)  # the plan has grown to the near view
     assert f3["layout_count"] > f3["num_rendered"]
     _assert_same(f3, fe, g3, ge, "after the plan grew")
+
+
+def test_colour_only_backward_matches_zero_depth_and_alpha_planes():
+    """Absent depth / alpha upstream gradients select the per-pixel backward
+    that leaves their terms out; its gradients equal the general kernel's
+    with zero planes (up to float atomic order)."""
+    arrays = _scene(12003, 24)
+    cam = camera.orbit_camera(45.0, 20.0, 2.5, 256, 256)
+    grad = _grad(256, 256, 4)
+    f = gh.forward(arrays, cam)
+    t = f["_tensors"]
+    means3D, opac, scales, rots, shs = arrays
+    empty = torch.empty(0, device="cuda")
+    zero = torch.zeros(1, 256, 256, device="cuda")
+    bg = gh.dev(np.ones(3, np.float32))
+
+    def bwd(dd, da):
+        g = _C.rasterize_gaussians_backward(
+            bg, gh.dev(means3D), t["radii"], empty, gh.dev(scales), gh.dev(rots), 1.0, empty, gh.dev(cam.viewmatrix),
+            gh.dev(cam.projmatrix), float(cam.tanfovx), float(cam.tanfovy), gh.dev(grad), dd, da, gh.dev(shs), 3,
+            gh.dev(cam.campos), t["geom"], f["num_rendered"], t["binb"], t["img"], t["alpha"], False, 0)
+        return [x.cpu().numpy() for x in g]
+
+    general = bwd(zero, zero)
+    colour_only = bwd(empty, empty)
+    for name, a, b in zip(parity.GRAD_NAMES, colour_only, general):
+        chk = parity.grad_check(a, b, row_rtol=parity.SAME_IMPL_ROW_RTOL)
+        assert chk["norm_rel"] <= 1e-6 and chk["n_bad"] == 0, (name, chk)

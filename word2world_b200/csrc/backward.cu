@@ -200,6 +200,12 @@ struct BwdPixel {
 
 // Reference formulas (backward.cu:552-663), per pixel, for one entry:
 // q0 = (mx, my, conic a, conic b), q1 = (conic c, opacity, depth, r), q2 = (g, b, skip, _).
+// kDA: a loss reaches depth or alpha.  Without one (dL/ddepth and dL/dalpha
+// absent, read as zero) every depth and alpha term adds exactly zero, so
+// RefChain<false> leaves them out (the suffix depth and alpha, their terms of
+// dL/dopacity, the depth contribution): the same results with about 7 % fewer
+// instructions per pair.
+template <bool kDA>
 struct RefChain {
   float T, T_final, bg_dot;
   float acc0 = 0.f, acc1 = 0.f, acc2 = 0.f, acc_d = 0.f, acc_a = 0.f;
@@ -219,15 +225,24 @@ struct RefChain {
     x.n0 = last_alpha * lc0 + (1.f - last_alpha) * acc0;
     x.n1 = last_alpha * lc1 + (1.f - last_alpha) * acc1;
     x.n2 = last_alpha * lc2 + (1.f - last_alpha) * acc2;
-    x.nd = last_alpha * last_depth + (1.f - last_alpha) * acc_d;
-    x.na = last_alpha + (1.f - last_alpha) * acc_a;
+    if constexpr (kDA) {
+      x.nd = last_alpha * last_depth + (1.f - last_alpha) * acc_d;
+      x.na = last_alpha + (1.f - last_alpha) * acc_a;
+    } else {
+      x.nd = 0.f;
+      x.na = 0.f;
+    }
     return x;
   }
   __device__ __forceinline__ void commit(bool ok, const Next& x, float4 q1, float4 q2, float alpha) {
     if (ok) {
       T = x.Tn;
-      acc0 = x.n0; acc1 = x.n1; acc2 = x.n2; acc_d = x.nd; acc_a = x.na;
-      lc0 = q1.w; lc1 = q2.x; lc2 = q2.y; last_depth = q1.z;
+      acc0 = x.n0; acc1 = x.n1; acc2 = x.n2;
+      lc0 = q1.w; lc1 = q2.x; lc2 = q2.y;
+      if constexpr (kDA) {
+        acc_d = x.nd; acc_a = x.na;
+        last_depth = q1.z;
+      }
       last_alpha = alpha;
     }
   }
@@ -250,9 +265,11 @@ struct RefChain {
     dL_dopa += (q1.w - n0) * p.dLp0;
     dL_dopa += (q2.x - n1) * p.dLp1;
     dL_dopa += (q2.y - n2) * p.dLp2;
-    const float c_d = q1.z;
-    dL_dopa += (c_d - nd) * p.dLd;
-    dL_dopa += (1 - na) * p.dLa;
+    if constexpr (kDA) {
+      const float c_d = q1.z;
+      dL_dopa += (c_d - nd) * p.dLd;
+      dL_dopa += (1 - na) * p.dLa;
+    }
     dL_dopa *= Tn;
     dL_dopa += div_markstein_y(-T_final, 1.f - alpha, x.y) * bg_dot;
     const float Gz = ok ? G : 0.f;  // G itself may be infinite where the entry is skipped
@@ -263,7 +280,7 @@ struct RefChain {
     c[0] = dchdc * p.dLp0;
     c[1] = dchdc * p.dLp1;
     c[2] = dchdc * p.dLp2;
-    c[3] = dchdc * p.dLd;
+    c[3] = kDA ? dchdc * p.dLd : 0.f;
     c[4] = dL_dG * dG_ddelx * ddelx_dx;
     c[5] = dL_dG * dG_ddely * ddely_dy;
     c[6] = -0.5f * gdx * dx * dL_dG;
@@ -343,14 +360,14 @@ __device__ __forceinline__ int cta_tile(const BackwardArgs& a, int& seg) {
   return int(a.order_bwd[b - (kSplitWays - 1) * a.split]);
 }
 
-template <int kSplitWays>
+template <int kSplitWays, bool kDA>
 __global__ void __launch_bounds__(kBlendThreads, 2) render_ref_kernel(BackwardArgs a) {
   __shared__ WarpChunk s_chunk[kBlendThreads / 32];
   int role;
   const int gtile = cta_tile<kSplitWays>(a, role);
   const float* bgp;
   const BwdPixel p = make_bwd_pixel(a, gtile, bgp);
-  RefChain ch;
+  RefChain<kDA> ch;
   ch.T_final = p.inside ? 1.0f - a.out_alpha[p.pix] : 0.0f;
   ch.T = ch.T_final;
   ch.bg_dot = bgp[0] * p.dLp0 + bgp[1] * p.dLp1 + bgp[2] * p.dLp2;
@@ -1432,12 +1449,15 @@ void launch_backward_render(const BackwardArgs& a, cudaStream_t stream) {
   const int ways = tune_value(kTuneBwdWays);
   stage_begin(kStBwdRender, stream);
   const int grid = tiles + (ways - 1) * b.split;
+  const bool da = a.dL_ddepth != nullptr || a.dL_dalpha != nullptr;  // a loss reaches depth or alpha
   if (ways == 3) {
     if (a.grad_mode == 1) render_exact_kernel<3><<<grid, kBlendThreads, 0, stream>>>(b);
-    else render_ref_kernel<3><<<grid, kBlendThreads, 0, stream>>>(b);
+    else if (da) render_ref_kernel<3, true><<<grid, kBlendThreads, 0, stream>>>(b);
+    else render_ref_kernel<3, false><<<grid, kBlendThreads, 0, stream>>>(b);
   } else {
     if (a.grad_mode == 1) render_exact_kernel<2><<<grid, kBlendThreads, 0, stream>>>(b);
-    else render_ref_kernel<2><<<grid, kBlendThreads, 0, stream>>>(b);
+    else if (da) render_ref_kernel<2, true><<<grid, kBlendThreads, 0, stream>>>(b);
+    else render_ref_kernel<2, false><<<grid, kBlendThreads, 0, stream>>>(b);
   }
   stage_end(kStBwdRender, stream, 1);
 }
