@@ -73,7 +73,11 @@ namespace {
 const char* kTuneNames[kNumTuneKnobs] = {"blend_warps", "backward_split", "backward_ways",
                                          "binning",     "blend_queue",    "preprocess_blocks",
                                          "planned_forward"};
-std::atomic<int> g_tune[kNumTuneKnobs] = {{4}, {4}, {2}, {0}, {0}, {4}, {1}};
+// defaults: 4-warp blend CTAs, the heaviest half-SM-count tiles' backward
+// walks split in two (backward_split 2 measured 3.09 against 3.21 ms per 4-view
+// step for 4, same B200), radix sort, per-tile blend, 4 projection CTAs per SM,
+// planned forward on
+std::atomic<int> g_tune[kNumTuneKnobs] = {{4}, {2}, {2}, {0}, {0}, {4}, {1}};
 bool tune_valid(int knob, int v) {
   switch (knob) {
     case kTuneBlendWarps: return v == 4 || v == 8;
