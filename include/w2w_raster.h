@@ -380,7 +380,8 @@ int w2w_batch_forward_render(const w2w_batch_item* items, int n, const void* geo
                              const w2w_geometry_info* info, void* binning_state, void* image_state,
                              float* out_color, float* out_depth, float* out_alpha, w2w_stream_t stream);
 /* Per-element gradients ([E, ...]; a scene's gradient is the sum over its
- * items' element ranges). */
+ * items' element ranges).  dL_ddepth and dL_dalpha may be NULL, as in
+ * w2w_backward (no loss on depth / alpha). */
 int w2w_batch_backward(const w2w_batch_item* items, int n, const void* geom_state, long long num_rendered,
                        const void* binning_state, const void* image_state, const int* radii,
                        const float* out_alpha, const float* dL_dcolor, const float* dL_ddepth,

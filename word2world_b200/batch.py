@@ -313,11 +313,10 @@ class BatchRenderer:
             torch.cat([g.reshape(-1) for g in gs], out=out)
             return out
         dlc = packed("dlc", dL_dcolor)
-        if dL_ddepth is None or dL_dalpha is None:
-            zeros = self._f32("zeros", st["npix"])
-            zeros.zero_()
-        dld = packed("dld", dL_ddepth) if dL_ddepth is not None else zeros
-        dla = packed("dla", dL_dalpha) if dL_dalpha is not None else zeros
+        # absent depth / alpha gradients go to the library as null (read as
+        # zero; without both, the per-pixel backward leaves their terms out)
+        dld = packed("dld", dL_ddepth) if dL_ddepth is not None else None
+        dla = packed("dla", dL_dalpha) if dL_dalpha is not None else None
         scratch = self._u8("scratch", int(L.w2w_batch_backward_scratch_bytes(arr, n)))
         # the groups' tables (w2w_group_sum's layout): row bases, item pointers, item element bases
         gid = [groups[v] if groups is not None else views[v].scene for v in range(n)]
@@ -359,7 +358,7 @@ class BatchRenderer:
         Eg = max(E, 1)
         f = self._f32
         g_m2, g_col, g_op = f("g_m2", Eg, 3), f("g_col", Eg, 3), f("g_op", Eg, 1)
-        p = lambda t: ctypes.c_void_p(t.data_ptr())
+        p = lambda t: ctypes.c_void_p(t.data_ptr() if t is not None else None)
         shapes = (("means3D", (3,)), ("opacities", (1,)), ("scales", (3,)), ("rotations", (4,)),
                   ("shs", (max(M, 1), 3)))
         out = {"groups": order}

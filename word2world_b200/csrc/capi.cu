@@ -1437,8 +1437,9 @@ static int batch_backward_begin(const w2w_batch_item* items, int n, const void* 
   if (!t.ok || (grad_mode != 0 && grad_mode != 1)) return W2W_ERR_INVALID;
   const long long E = t.elems;
   if (E == 0) return 1;
-  if (!geom_state || !image_state || !radii || !out_alpha || !dL_dcolor || !dL_ddepth || !dL_dalpha ||
-      !dL_dmeans2D || !dL_dcolors || !dL_dopacity || (R > 0 && !binning_state))
+  // dL_ddepth / dL_dalpha may be null: no loss reaches depth / alpha (read as zero)
+  if (!geom_state || !image_state || !radii || !out_alpha || !dL_dcolor || !dL_dmeans2D || !dL_dcolors ||
+      !dL_dopacity || (R > 0 && !binning_state))
     return W2W_ERR_INVALID;
   if (!scratch || scratch_bytes < w2w_batch_backward_scratch_bytes(items, n)) return W2W_ERR_SCRATCH;
   const int T = t.tiles;
