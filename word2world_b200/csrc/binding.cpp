@@ -229,7 +229,11 @@ int64_t planned_forward(w2w_settings& st, const Tensor& geom, const Tensor& img,
   {
     std::lock_guard<std::mutex> lk(g_plan_mu);
     PlanState& p = g_plans[key];
-    if (info.num_rendered > p.capacity) p.capacity = w2w_planned_capacity(info.num_rendered);
+    // the capacity follows the counts: it grows to a larger view, and shrinks
+    // back when a view uses less than a quarter of it (a plan sized for one
+    // outsized view would make every later view clear and launch for it)
+    if (info.num_rendered > p.capacity || info.num_rendered < p.capacity / 4)
+      p.capacity = w2w_planned_capacity(info.num_rendered);
     if (need > p.depth_bits) p.depth_bits = need;
   }
   if (!fits) render_exact();  // the planned launches (if any) processed no instance
