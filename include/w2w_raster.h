@@ -276,6 +276,21 @@ int w2w_backward_raw(const w2w_settings* s, const float* means3D, const float* s
                      float* dL_dcolors, float* dL_dopacity_logit, float* dL_dmeans3D, float* dL_dcov3D,
                      float* dL_dsh_dc, float* dL_dsh_ac, float* dL_dsvec, float* dL_dquaternion,
                      w2w_stream_t stream);
+/* w2w_backward_raw that also accumulates the training loop's densification
+ * statistics (gaussians_handler.py:116-118, which the reference computes
+ * after the backward with boolean-mask indexing) in its per-Gaussian pass:
+ * for every Gaussian with radius > 0, dens_counter[i] += 1 and dens_accum[i]
+ * += |dL/dmean2D[i, 0:2]| (both [P], updated in place with atomics, so views
+ * back-propagated on concurrent streams may share them; both null: none). */
+int w2w_backward_raw_densify(const w2w_settings* s, const float* means3D, const float* svec,
+                             const float* quaternion, const float* opacity_logit, const float* sh_dc,
+                             const float* sh_ac, const int* radii, const void* geom_state, long long num_rendered,
+                             const void* binning_state, const void* image_state, const float* out_alpha,
+                             const float* dL_dcolor, const float* dL_ddepth, const float* dL_dalpha, void* scratch,
+                             size_t scratch_bytes, float* dL_dmeans2D, float* dL_dcolors, float* dL_dopacity_logit,
+                             float* dL_dmeans3D, float* dL_dcov3D, float* dL_dsh_dc, float* dL_dsh_ac,
+                             float* dL_dsvec, float* dL_dquaternion, float* dens_accum, float* dens_counter,
+                             w2w_stream_t stream);
 
 /* The activation preamble of Renderer.render (Renderer.py:164-167) in one
  * pass: opacity = sigmoid(logit) [P], scales = exp(svec) [P,3], rotations =

@@ -237,3 +237,30 @@ def test_views_on_separate_streams_match_one_stream():
     for name, a_, b_ in zip(("means3D", "shs", "opacity", "scales", "rotations", "means2D"), g1, g2):
         chk = parity.grad_check(a_, b_, row_rtol=parity.SAME_IMPL_ROW_RTOL)
         assert chk["norm_rel"] <= 1e-5 and chk["n_bad"] == 0, (name, chk)
+
+
+def test_densification_fused_into_the_backward_matches_collect():
+    """Renderer(densification=stats): each render's backward accumulates the
+    statistics in its per-Gaussian pass; over three views they equal collect
+    calls on the same renders' gradients after each backward, exactly (the
+    same arithmetic on the same values, in the same order on one stream)."""
+    from word2world_b200 import camera
+    from word2world_b200.renderer import DensificationStats
+    sc, cam0, t = _setup(P=20000, S=256, seed=9)
+    cams = camera.orbit_views(3, 2.5, 256, 256)
+    gen = torch.Generator(device=DEV).manual_seed(8)
+    gs = [torch.randn(3, 256, 256, device=DEV, generator=gen) for _ in cams]
+    params = GaussianParams.from_scene(sc, device=DEV)
+    fused = DensificationStats(params.mean.shape[0])
+    collected = DensificationStats(params.mean.shape[0])
+    r = Renderer(params, sh_degree=3, densification=fused)
+    for c, g in zip(cams, gs):
+        out = r.render(c.fovx, c.fovy, t(c.viewmatrix), t(c.projmatrix), t(c.campos), 256, 256)
+        (out["image"] * g).sum().backward()
+        collected.collect(out["accum_grads"], out["available_pts"].to(torch.int32))
+    torch.cuda.synchronize()
+    assert torch.count_nonzero(collected.counter) > 0
+    assert torch.equal(fused.counter, collected.counter)
+    assert torch.equal(fused.mean_gradient_accum, collected.mean_gradient_accum)
+    with pytest.raises(ValueError):
+        Renderer(GaussianParams.from_scene(sc, device=DEV), grad_mode="exact", densification=fused)

@@ -1126,6 +1126,13 @@ __global__ void __launch_bounds__(kGaussThreads, 8) gaussians_ref_kernel(Backwar
     const float y = __frcp_rn(1.f + expf(-__ldg(&a.logit[i])));  // sigmoid, within an ulp of the forward's
     a.dL_dopacity[i] = a.dL_dopacity[i] * (1.f - y) * y;
   }
+  // densification statistics (gaussians_handler.py:116-118) in this pass, not
+  // one of their own; atomic, because views on other streams may add too
+  if (a.dens_accum != nullptr && lane < n && a.radii[i] > 0) {
+    const float gx = a.dL_dmean2D[3 * i], gy = a.dL_dmean2D[3 * i + 1];
+    atomicAdd(&a.dens_accum[i], __fsqrt_rn(__fadd_rn(__fmul_rn(gx, gx), __fmul_rn(gy, gy))));
+    atomicAdd(&a.dens_counter[i], 1.0f);
+  }
   // dL_dsh[k][ch] = basis[k] * cf[ch] for the first min(M, 16) bands, 0 beyond
   if (a.dL_dsh_dc != nullptr) sh_store_outer_raw(a.dL_dsh_dc, a.dL_dsh_ac, a.M, i0, n, sw, basis, cf, active);
   else sh_store_outer(a.dL_dsh, a.M, i0, n, sw, basis, cf, active);

@@ -498,9 +498,24 @@ std::tuple<Tensor, Tensor, Tensor, Tensor, Tensor, Tensor, Tensor> rasterize_gau
     const Tensor& opacity_logit, const Tensor& svec, const Tensor& quaternion, const Tensor& radii,
     const Tensor& viewmatrix, const Tensor& projmatrix, const Tensor& campos, double tan_fovx, double tan_fovy,
     int64_t degree, const Tensor& dL_dout_color, const Tensor& dL_dout_depth, const Tensor& dL_dout_alpha,
-    const Tensor& geomBuffer, int64_t R, const Tensor& binningBuffer, const Tensor& imageBuffer, const Tensor& alpha) {
+    const Tensor& geomBuffer, int64_t R, const Tensor& binningBuffer, const Tensor& imageBuffer, const Tensor& alpha,
+    const c10::optional<Tensor>& dens_accum, const c10::optional<Tensor>& dens_counter) {
   deferred().poll(false);
   const auto dev = means3D.device();
+  // densification statistics accumulated in the pass (renderer.DensificationStats' [P, 1] tensors)
+  float* dacc = nullptr;
+  float* dcnt = nullptr;
+  if (dens_accum.has_value() && dens_counter.has_value()) {
+    const Tensor& A = *dens_accum;
+    const Tensor& Cn = *dens_counter;
+    TORCH_CHECK(A.is_cuda() && Cn.is_cuda() && A.device() == dev && Cn.device() == dev &&
+                    A.scalar_type() == torch::kFloat32 && Cn.scalar_type() == torch::kFloat32 &&
+                    A.is_contiguous() && Cn.is_contiguous() && A.numel() == means3D.size(0) &&
+                    Cn.numel() == means3D.size(0),
+                "densification accumulators must be contiguous float32 [P] tensors on the means' device");
+    dacc = A.data_ptr<float>();
+    dcnt = Cn.data_ptr<float>();
+  }
   c10::cuda::CUDAGuard guard(dev);
   const int64_t P = means3D.size(0);
   Tensor m = f32(means3D, "means3D", dev), dc = f32(sh_dc, "sh_dc", dev), ac = f32(sh_ac, "sh_ac", dev);
@@ -538,14 +553,15 @@ std::tuple<Tensor, Tensor, Tensor, Tensor, Tensor, Tensor, Tensor> rasterize_gau
   const w2w_stream_t stream = cur_stream();
   {
     pybind11::gil_scoped_release nogil;
-    check(w2w_backward_raw(&st, m.data_ptr<float>(), sv.data_ptr<float>(), q.data_ptr<float>(), lo.data_ptr<float>(),
+    check(w2w_backward_raw_densify(&st, m.data_ptr<float>(), sv.data_ptr<float>(), q.data_ptr<float>(), lo.data_ptr<float>(),
                            dc.data_ptr<float>(), ac.data_ptr<float>(), rad.data_ptr<int>(), geomBuffer.data_ptr(), LR,
                            binningBuffer.data_ptr(), imageBuffer.data_ptr(), al.data_ptr<float>(), g.data_ptr<float>(),
                            gd.numel() ? gd.data_ptr<float>() : nullptr, ga.numel() ? ga.data_ptr<float>() : nullptr,
                            scratch.data_ptr(), size_t(scratch.numel()),
                            dmean2D.data_ptr<float>(), dcolors.data_ptr<float>(), dlogit.data_ptr<float>(),
                            dmean3D.data_ptr<float>(), dcov3D.data_ptr<float>(), ddc.data_ptr<float>(),
-                           dac.data_ptr<float>(), dsvec.data_ptr<float>(), dquat.data_ptr<float>(), stream),
+                           dac.data_ptr<float>(), dsvec.data_ptr<float>(), dquat.data_ptr<float>(), dacc, dcnt,
+                           stream),
           "w2w_backward_raw");
   }
   return std::make_tuple(dmean2D, dmean3D, ddc, dac, dlogit, dsvec, dquat);
@@ -752,7 +768,13 @@ PYBIND11_MODULE(TORCH_EXTENSION_NAME, m) {
   });
   m.def("activate", &activate);
   m.def("rasterize_gaussians_raw", &rasterize_gaussians_raw);
-  m.def("rasterize_gaussians_backward_raw", &rasterize_gaussians_backward_raw);
+  m.def("rasterize_gaussians_backward_raw", &rasterize_gaussians_backward_raw, py::arg("background"),
+        py::arg("means3D"), py::arg("sh_dc"), py::arg("sh_ac"), py::arg("opacity_logit"), py::arg("svec"),
+        py::arg("quaternion"), py::arg("radii"), py::arg("viewmatrix"), py::arg("projmatrix"), py::arg("campos"),
+        py::arg("tan_fovx"), py::arg("tan_fovy"), py::arg("degree"), py::arg("dL_dout_color"),
+        py::arg("dL_dout_depth"), py::arg("dL_dout_alpha"), py::arg("geomBuffer"), py::arg("R"),
+        py::arg("binningBuffer"), py::arg("imageBuffer"), py::arg("alpha"), py::arg("dens_accum") = py::none(),
+        py::arg("dens_counter") = py::none());
   m.def("densification_stats", &densification_stats);
   m.def("voxel_field", &voxel_field);
   m.def("activate_backward", &activate_backward);

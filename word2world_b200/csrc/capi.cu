@@ -752,6 +752,7 @@ int w2w_state_error(const void* state, int which, w2w_stream_t stream) {
 struct RawGrads {
   const float *svec, *quat, *logit, *sh_dc, *sh_ac;
   float *d_sh_dc, *d_sh_ac;
+  float *dens_accum, *dens_counter;  // densification statistics, or null
 };
 
 static int backward_impl(const w2w_settings* s, const float* means3D, const float* scales, const float* rotations,
@@ -808,6 +809,7 @@ static int backward_impl(const w2w_settings* s, const float* means3D, const floa
   if (raw != nullptr) {
     a.svec = raw->svec; a.quat = raw->quat; a.logit = raw->logit; a.sh_dc = raw->sh_dc; a.sh_ac = raw->sh_ac;
     a.dL_dsh_dc = raw->d_sh_dc; a.dL_dsh_ac = raw->d_sh_ac;
+    a.dens_accum = raw->dens_accum; a.dens_counter = raw->dens_counter;
   }
   if (R > 0) launch_backward_render(a, st);
   launch_backward_gaussians(a, st);
@@ -834,13 +836,14 @@ int w2w_backward(const w2w_settings* s, const float* means3D, const float* scale
                        dL_drotations, stream);
 }
 
-int w2w_backward_raw(const w2w_settings* s, const float* means3D, const float* svec, const float* quaternion,
+int w2w_backward_raw_densify(const w2w_settings* s, const float* means3D, const float* svec, const float* quaternion,
                      const float* opacity_logit, const float* sh_dc, const float* sh_ac, const int* radii,
                      const void* geom_state, long long R, const void* binning_state, const void* image_state,
                      const float* out_alpha, const float* dL_dcolor, const float* dL_ddepth, const float* dL_dalpha,
                      void* scratch, size_t scratch_bytes, float* dL_dmeans2D, float* dL_dcolors,
                      float* dL_dopacity_logit, float* dL_dmeans3D, float* dL_dcov3D, float* dL_dsh_dc,
-                     float* dL_dsh_ac, float* dL_dsvec, float* dL_dquaternion, w2w_stream_t stream) {
+                     float* dL_dsh_ac, float* dL_dsvec, float* dL_dquaternion, float* dens_accum,
+                             float* dens_counter, w2w_stream_t stream) {
   if (!settings_ok(s) || s->M < 1 || s->M > 16) return W2W_ERR_INVALID;
   const int P = s->P;
   if (P == 0) return W2W_OK;
@@ -849,11 +852,25 @@ int w2w_backward_raw(const w2w_settings* s, const float* means3D, const float* s
       !dL_dmeans2D || !dL_dcolors || !dL_dopacity_logit || !dL_dmeans3D || !dL_dcov3D || !dL_dsh_dc || !dL_dsvec ||
       !dL_dquaternion || (R > 0 && !binning_state))
     return W2W_ERR_INVALID;
-  const RawGrads raw{svec, quaternion, opacity_logit, sh_dc, sh_ac, dL_dsh_dc, dL_dsh_ac};
+  if ((dens_accum == nullptr) != (dens_counter == nullptr)) return W2W_ERR_INVALID;
+  const RawGrads raw{svec, quaternion, opacity_logit, sh_dc, sh_ac, dL_dsh_dc, dL_dsh_ac, dens_accum, dens_counter};
   return backward_impl(s, means3D, nullptr, nullptr, nullptr, &raw, radii, geom_state, R, binning_state, image_state,
                        out_alpha, dL_dcolor, dL_ddepth, dL_dalpha, 0, scratch, scratch_bytes, dL_dmeans2D,
                        dL_dcolors, dL_dopacity_logit, dL_dmeans3D, dL_dcov3D, nullptr, dL_dsvec, dL_dquaternion,
                        stream);
+}
+
+int w2w_backward_raw(const w2w_settings* s, const float* means3D, const float* svec, const float* quaternion,
+                     const float* opacity_logit, const float* sh_dc, const float* sh_ac, const int* radii,
+                     const void* geom_state, long long R, const void* binning_state, const void* image_state,
+                     const float* out_alpha, const float* dL_dcolor, const float* dL_ddepth, const float* dL_dalpha,
+                     void* scratch, size_t scratch_bytes, float* dL_dmeans2D, float* dL_dcolors,
+                     float* dL_dopacity_logit, float* dL_dmeans3D, float* dL_dcov3D, float* dL_dsh_dc,
+                     float* dL_dsh_ac, float* dL_dsvec, float* dL_dquaternion, w2w_stream_t stream) {
+  return w2w_backward_raw_densify(s, means3D, svec, quaternion, opacity_logit, sh_dc, sh_ac, radii, geom_state, R,
+                                  binning_state, image_state, out_alpha, dL_dcolor, dL_ddepth, dL_dalpha, scratch,
+                                  scratch_bytes, dL_dmeans2D, dL_dcolors, dL_dopacity_logit, dL_dmeans3D, dL_dcov3D,
+                                  dL_dsh_dc, dL_dsh_ac, dL_dsvec, dL_dquaternion, nullptr, nullptr, stream);
 }
 
 size_t w2w_sort_scratch_bytes(long long n) {

@@ -228,6 +228,9 @@ struct BackwardArgs {
   // d/dlogit, and dL_dsh_dc / dL_dsh_ac the SH rows split as the inputs)
   const float *svec, *quat, *logit, *sh_dc, *sh_ac;
   float *dL_dsh_dc, *dL_dsh_ac;
+  // densification statistics accumulated by the per-Gaussian pass (or null):
+  // for radius > 0, dens_counter += 1 and dens_accum += |dL/dmean2D[:2]|
+  float *dens_accum, *dens_counter;
   // grouped per-Gaussian pass (batched calls): per-group sums over the
   // groups' items, tables laid out as w2w_group_sum's ([G + 1] row bases,
   // [G + 1] item pointers, item element bases), outputs [group_rows, ...]

@@ -143,7 +143,7 @@ class _RasterizeRaw(torch.autograd.Function):
 
     @staticmethod
     def forward(ctx, means3D, means2D, sh_dc, sh_ac, opacity_logit, svec, quaternion, bg, viewmatrix, projmatrix,
-                tanfovx, tanfovy, sh_degree, campos, image_height, image_width, compat_spill):
+                tanfovx, tanfovy, sh_degree, campos, image_height, image_width, compat_spill, densification=None):
         focal_x = image_width / (2.0 * tanfovx)
         num_rend, color, depth, alpha, radii, geom, binb, img = _C.rasterize_gaussians_raw(
             means3D, sh_dc, sh_ac, opacity_logit, svec, quaternion, viewmatrix, projmatrix, campos, focal_x,
@@ -151,6 +151,7 @@ class _RasterizeRaw(torch.autograd.Function):
         ctx.num_rend = num_rend
         ctx.bg, ctx.vmat, ctx.pmat, ctx.campos = bg, viewmatrix, projmatrix, campos
         ctx.fx, ctx.fy, ctx.sh_deg = tanfovx, tanfovy, sh_degree
+        ctx.dens = densification  # a DensificationStats the backward updates, or None
         ctx.save_for_backward(means3D, sh_dc, sh_ac, opacity_logit, svec, quaternion, radii, geom, binb, img, alpha)
         ctx.mark_non_differentiable(radii)
         ctx.set_materialize_grads(False)
@@ -163,9 +164,11 @@ class _RasterizeRaw(torch.autograd.Function):
         g_means2D, g_means3D, g_dc, g_ac, g_logit, g_svec, g_quat = _C.rasterize_gaussians_backward_raw(
             ctx.bg, means3D, sh_dc, sh_ac, opacity_logit, svec, quaternion, radii, ctx.vmat, ctx.pmat, ctx.campos,
             ctx.fx, ctx.fy, ctx.sh_deg, g_color, g_depth, g_alpha, geom,
-            ctx.num_rend, binb, img, alpha)
+            ctx.num_rend, binb, img, alpha,
+            dens_accum=ctx.dens.mean_gradient_accum if ctx.dens is not None else None,
+            dens_counter=ctx.dens.counter if ctx.dens is not None else None)
         return (g_means3D, g_means2D, g_dc, g_ac, g_logit, g_svec, g_quat,
-                None, None, None, None, None, None, None, None, None, None)
+                None, None, None, None, None, None, None, None, None, None, None)
 
 
 @dataclass
@@ -231,8 +234,16 @@ class Renderer:
     """
 
     def __init__(self, params: GaussianParams, sh_degree: int = 0, grad_mode: str = "reference",
-                 compat_spill: bool = True):
+                 compat_spill: bool = True, densification: "DensificationStats | None" = None):
+        """``densification``: statistics every render's backward accumulates
+        (reference-formula gradients), in the per-Gaussian pass itself,
+        instead of a ``collect`` call after each backward (the reference's
+        trainer collects after the backward, ``GaussianTrainer.py:119``)."""
+        if densification is not None and grad_mode != "reference":
+            raise ValueError("fused densification statistics come with reference-formula gradients; with "
+                             "grad_mode='exact' call DensificationStats.collect after the backward")
         self.params = params
+        self.densification = densification
         self.sh_degree = sh_degree
         self.grad_mode = grad_mode
         self.compat_spill = compat_spill
@@ -263,7 +274,7 @@ class Renderer:
             image, radii, _, _ = _RasterizeRaw.apply(
                 p.mean, accum_grads, p.sh_dc, p.sh_ac, p.opacity, p.svec, p.quaternion, bg, world_view_transform,
                 full_proj_transform, tanfovx, tanfovy, self.sh_degree, camera_center, int(image_height),
-                int(image_width), bool(self.compat_spill))
+                int(image_width), bool(self.compat_spill), self.densification)
             available = radii > 0
             return {"image": image, "accum_grads": accum_grads, "avaialble_pts": available,
                     "available_pts": available}
