@@ -464,7 +464,7 @@ int w2w_throughput_probe(int kind, long long iters, int blocks, float* out, long
  * (pixelGaussiansFull.cu:99-122).  Knobs (w2w_tune_name): 0 "blend_warps"
  * (4: two 4-warp CTAs per tile, 8: one 8-warp CTA; default 4), 1
  * "backward_split" (the per-pixel backward splits its heaviest tiles, up to
- * this many quarters of the SM count, across CTAs; 0..16, default 4), 2
+ * this many quarters of the SM count, across CTAs; 0..16, default 2), 2
  * "backward_ways" (segments per split tile, 2 or 3; default 2), 3 "binning"
  * (how a single-view call of at most 4096 tiles builds its sorted list: 0
  * key emission and the radix sort, 1 binning from the depth-ordered
@@ -476,7 +476,12 @@ int w2w_throughput_probe(int kind, long long iters, int blocks, float* out, long
  * batches' records with TMA into a three-stage shared-memory ring and
  * "blend_warps" consumer warps; default 0), 5 "preprocess_blocks" (CTAs per
  * SM the projection pass's register budget is sized for: 4 caps a thread at
- * 64 registers, 3 at 80, 2 at 128; default 4).
+ * 64 registers, 3 at 80, 2 at 128; default 4), 6 "planned_forward" (the torch
+ * binding's planned forward for repeated image sizes, 1 on, 0 off; default 1;
+ * not tuned, the C ABI's entry points take the plan explicitly), 7
+ * "blend_stage" (how the per-tile blend gathers a batch's records while it
+ * walks the previous one: 0 into registers, 1 into shared memory with
+ * cp.async, which fits five 4-warp CTAs per SM instead of four; default 1).
  * Results do not depend on them beyond the order of float atomic additions.
  * w2w_tune_set returns the previous value, or -1 (and changes nothing) for an
  * unknown knob or value. */

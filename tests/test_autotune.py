@@ -47,17 +47,17 @@ def test_descent_finds_the_cheapest_setting_and_caches_it(restore, tmp_path):
     path = str(tmp_path / "tune.json")
     t = autotune.Autotuner(path=path, timer=lambda step: cost())
     autotune.apply({"blend_warps": 4, "backward_split": 4, "backward_ways": 2, "binning": 0, "blend_queue": 0,
-                    "preprocess_blocks": 4})
+                    "preprocess_blocks": 4, "blend_stage": 1})
     best = t.tune("bucket", step=None)
-    # preprocess_blocks does not enter the cost: it keeps its starting value
+    # preprocess_blocks and blend_stage do not enter the cost: they keep their starting values
     assert best == {"blend_warps": 8, "backward_split": 2, "backward_ways": 3, "binning": 1, "blend_queue": 1,
-                    "preprocess_blocks": 4}
+                    "preprocess_blocks": 4, "blend_stage": 1}
     assert autotune.current() == best
     saved = json.load(open(path))
     assert saved["bucket"]["blend_warps"] == 8
     # a second tuner reads the cache and applies it without timing anything
     autotune.apply({"blend_warps": 4, "backward_split": 4, "backward_ways": 2, "binning": 0, "blend_queue": 0,
-                    "preprocess_blocks": 4})
+                    "preprocess_blocks": 4, "blend_stage": 1})
     t2 = autotune.Autotuner(path=path, timer=lambda step: pytest.fail("timed a cached bucket"))
     assert t2.ensure("bucket", step=None) == best and autotune.current() == best
 
@@ -72,11 +72,13 @@ def test_every_knob_setting_gives_the_same_results(restore):
     cam = camera.orbit_camera(60.0, 15.0, 2.5, 256, 256)
     g = np.random.default_rng(3).normal(size=(3, 256, 256)).astype(np.float32)
     base = None
-    for warps, split, ways, binning, queue, pre in ((4, 4, 2, 0, 0, 4), (8, 4, 2, 0, 0, 3), (4, 0, 2, 1, 0, 2),
-                                                    (4, 8, 3, 1, 1, 4), (8, 8, 2, 1, 1, 2), (4, 4, 3, 0, 1, 3),
-                                                    (8, 4, 2, 0, 1, 4)):
+    for warps, split, ways, binning, queue, pre, stage in ((4, 4, 2, 0, 0, 4, 1), (8, 4, 2, 0, 0, 3, 1),
+                                                           (4, 0, 2, 1, 0, 2, 0), (4, 8, 3, 1, 1, 4, 1),
+                                                           (8, 8, 2, 1, 1, 2, 0), (4, 4, 3, 0, 1, 3, 0),
+                                                           (8, 4, 2, 0, 1, 4, 1), (4, 2, 2, 0, 0, 4, 0),
+                                                           (8, 2, 2, 0, 0, 4, 0)):
         autotune.apply({"blend_warps": warps, "backward_split": split, "backward_ways": ways, "binning": binning,
-                        "blend_queue": queue, "preprocess_blocks": pre})
+                        "blend_queue": queue, "preprocess_blocks": pre, "blend_stage": stage})
         f = gh.forward(arrays, cam)
         b = gh.backward(f, arrays, cam, g, grad_mode=0)
         if base is None:

@@ -1,7 +1,8 @@
 """Launch-shape autotuner: picks the library's tuning knobs (blend CTA shape,
-per-tile or persistent queue-fed blend, how many heavy tiles the per-pixel
-backward splits and into how many segments, radix or depth-ordered binning)
-for a workload by timing it, and remembers the choice per shape
+per-tile or persistent queue-fed blend, the blend's batch staging (registers
+or cp.async), how many heavy tiles the per-pixel backward splits and into how
+many segments, radix or depth-ordered binning, the projection pass's register
+budget) for a workload by timing it, and remembers the choice per shape
 bucket.
 
 The reference's launch shapes are constants (pixelGaussiansFull.cu:99-122,
@@ -35,6 +36,7 @@ CANDIDATES = {
     "binning": [0, 1],
     "blend_queue": [0, 1],
     "preprocess_blocks": [4, 3, 2],
+    "blend_stage": [1, 0],
 }
 
 

@@ -72,14 +72,24 @@ struct BlendPixel {
 
 // Warps per CTA, kBlendWarps: 8 (one CTA per tile) or 4 (two CTAs per tile,
 // upper and lower eight rows; see tile_walk.cuh), chosen at run time (the
-// tuning knob W2W_TUNE_BLEND_WARPS).  Results are identical either way.
-template <int kBlendWarps>
-__global__ void __launch_bounds__(32 * kBlendWarps, 16 / kBlendWarps) blend_kernel(BlendArgs a) {
+// tuning knob "blend_warps"); kAsync: the next batch is copied into shared
+// memory with cp.async instead of gathered into registers (the knob
+// "blend_stage"), which leaves the 4-warp CTA few enough registers for five
+// CTAs per SM instead of four.  Results are identical in every combination.
+template <int kBlendWarps, bool kAsync>
+constexpr int blend_min_blocks() {
+  return kAsync && kBlendWarps == 4 ? 5 : 16 / kBlendWarps;
+}
+
+template <int kBlendWarps, bool kAsync>
+__global__ void __launch_bounds__(32 * kBlendWarps, (blend_min_blocks<kBlendWarps, kAsync>()))
+    blend_kernel(BlendArgs a) {
   constexpr int kBlendParts = 8 / kBlendWarps;  // CTAs per tile
   constexpr int kBlendCta = 32 * kBlendWarps;
   constexpr int kStagePer = kBatch / kBlendCta;  // entries each thread stages per batch
+  constexpr int kVec = kAsync ? kStageVec : kRecVec;  // float4s per staged record
   static_assert(kBatch % kBlendCta == 0, "whole entries per thread");
-  __shared__ TileWalkShared<kBlendWarps> sm;
+  __shared__ TileWalkShared<kBlendWarps, kVec> sm;
   const int part = int(blockIdx.x) % kBlendParts;
   const int tile = int(a.order[blockIdx.x / kBlendParts]);
   // this tile's image: the call's, or its batch item's
@@ -105,26 +115,36 @@ __global__ void __launch_bounds__(32 * kBlendWarps, 16 / kBlendWarps) blend_kern
   BlendPixel pix;
   pix.done = !inside;
   const int nb = (n + kBatch - 1) / kBatch;
-  Staged st[kStagePer];
-  auto load = [&](int base) {
+  Staged st[kAsync ? 1 : kStagePer];    // register staging: the batch in flight
+  bool staged[kAsync ? kStagePer : 1];  // cp.async staging: slot r * kBlendCta + threadIdx.x holds a record
+  auto load = [&](int buf, int base) {
 #pragma unroll
     for (int r = 0; r < kStagePer; ++r) {
-      const int e = base + r * kBlendCta + int(threadIdx.x);
-      stage_load(st[r], a.record, a.point_list, range.x + e, e < n, a.num_records);
+      const int j = r * kBlendCta + int(threadIdx.x), e = base + j;
+      if constexpr (kAsync)
+        staged[r] = stage_copy(&sm.rec[buf][kVec * j], a.record, a.point_list, range.x + e, e < n, a.num_records);
+      else
+        stage_load(st[r], a.record, a.point_list, range.x + e, e < n, a.num_records);
     }
+    if constexpr (kAsync) cp_async_commit();
   };
   // block masks for the backward: the upper half's CTA (or the whole tile's)
   // writes the top array, the lower half's the bottom one
   uint8_t* lo_dst = a.mask_top == nullptr ? nullptr : (part == 0 ? a.mask_top : a.mask_bottom) + range.x;
   uint8_t* hi_dst = a.mask_top == nullptr || kBlendParts != 1 ? nullptr : a.mask_bottom + range.x;
   auto store = [&](int buf, int base) {
+    if constexpr (kAsync) cp_async_wait_all();
 #pragma unroll
-    for (int r = 0; r < kStagePer; ++r)
-      stage_store(sm, buf, st[r], r * kBlendCta + int(threadIdx.x), tp.X0, tp.Y0, first_block,
-                  lo_dst ? lo_dst + base : nullptr, hi_dst ? hi_dst + base : nullptr);
+    for (int r = 0; r < kStagePer; ++r) {
+      const int j = r * kBlendCta + int(threadIdx.x);
+      uint8_t* lo = lo_dst ? lo_dst + base : nullptr;
+      uint8_t* hi = hi_dst ? hi_dst + base : nullptr;
+      if constexpr (kAsync) stage_mask(sm, buf, staged[r], j, tp.X0, tp.Y0, first_block, lo, hi);
+      else stage_store(sm, buf, st[r], j, tp.X0, tp.Y0, first_block, lo, hi);
+    }
   };
   if (nb > 0) {
-    load(0);
+    load(0, 0);
     store(0, 0);
   }
   for (int b = 0; b < nb; ++b) {
@@ -132,7 +152,7 @@ __global__ void __launch_bounds__(32 * kBlendWarps, 16 / kBlendWarps) blend_kern
     // barrier: batch b is staged; every warp has finished batch b-1
     if (__syncthreads_count(pix.done ? 1 : 0) == kBlendCta) break;
     const int next_base = (b + 1) * kBatch;
-    if (b + 1 < nb) load(next_base);
+    if (b + 1 < nb) load(cur ^ 1, next_base);  // in flight while batch b is walked
     if (!__all_sync(0xffffffffu, pix.done)) {
       const float4* s = sm.rec[cur];
       const int cnt = build_list(sm, cur, warp, tp.lane);
@@ -151,9 +171,9 @@ __global__ void __launch_bounds__(32 * kBlendWarps, 16 / kBlendWarps) blend_kern
 #pragma unroll
         for (int k = 0; k < kBlendIlp; ++k) {
           const int jj = j[k] < 0 ? j[0] : j[k];
-          const float4 q0 = s[kRecVec * jj];
-          q1[k] = s[kRecVec * jj + 1];
-          q2[k] = s[kRecVec * jj + 2];
+          const float4 q0 = s[kVec * jj];
+          q1[k] = s[kVec * jj + 1];
+          q2[k] = s[kVec * jj + 2];
           num[k] = gauss_num(pxf, pyf, q0.x, q0.y, q0.z, q0.w, q1[k].x);
           in_range = in_range && div_in_range(num[k], q1[k].y);
         }
@@ -624,6 +644,7 @@ void launch_blend(const BlendArgs& a, cudaStream_t stream) {
   const int tiles = a.items ? a.total_tiles : ((a.W + kTile - 1) / kTile) * ((a.H + kTile - 1) / kTile);
   if (tiles <= 0) return;
   const int warps = tune_value(kTuneBlendWarps);
+  const bool async = tune_value(kTuneBlendStage) == 1;
   const bool queue = tune_value(kTuneBlendQueue) == 1 && a.queue != nullptr;
   stage_begin(kStOther, stream);
   // with two CTAs per tile (or the queue) the tile's maxima combine with
@@ -634,8 +655,10 @@ void launch_blend(const BlendArgs& a, cudaStream_t stream) {
   stage_begin(kStBlend, stream);
   const bool queued = queue && (warps == 4 ? launch_queue<4>(a, tiles, stream) : launch_queue<8>(a, tiles, stream));
   if (!queued) {
-    if (warps == 4) blend_kernel<4><<<tiles * 2, 128, 0, stream>>>(a);
-    else blend_kernel<8><<<tiles, 256, 0, stream>>>(a);
+    if (warps == 4 && async) blend_kernel<4, true><<<tiles * 2, 128, 0, stream>>>(a);
+    else if (warps == 4) blend_kernel<4, false><<<tiles * 2, 128, 0, stream>>>(a);
+    else if (async) blend_kernel<8, true><<<tiles, 256, 0, stream>>>(a);
+    else blend_kernel<8, false><<<tiles, 256, 0, stream>>>(a);
   }
   stage_end(kStBlend, stream, 1);
   // the backward's order: by the largest contributor count the blend just found

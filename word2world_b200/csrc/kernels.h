@@ -354,7 +354,8 @@ enum TuneKnob {
   kTuneBlendQueue = 4,
   kTunePreBlocks = 5,
   kTunePlanned = 6,
-  kNumTuneKnobs = 7
+  kTuneBlendStage = 7,
+  kNumTuneKnobs = 8
 };
 int tune_value(int knob);
 

@@ -139,19 +139,25 @@ __device__ __forceinline__ int pop_entry(uint32_t& bits) {
 // kW = 8: one CTA per tile; kW = 4: two CTAs per tile (its upper and lower
 // eight rows), each staging the whole list, so that fewer warps wait at each
 // batch's barrier for the slowest of them.
+// The next batch is gathered while the current one is walked, in one of two
+// ways (the blend's "blend_stage" tuning knob): into registers, stored to
+// shared memory after the walk (stage_load / stage_store; kVec = kRecVec), or
+// copied straight into shared memory with cp.async (stage_copy / stage_mask;
+// kVec = kStageVec), which holds no registers through the walk.
 // ---------------------------------------------------------------------------
-template <int kW>
+constexpr int kStageVec = 4;  // float4s per record copied by cp.async (the whole record: the test reads r2.w, r3)
+
+template <int kW, int kVec>
 struct TileWalkShared {
-  float4 rec[2][kBatch * kRecVec];
-  uint32_t id[2][kBatch];
+  float4 rec[2][kBatch * kVec];
   uint32_t bal[2][kW][kBatch / 32];  // [buffer][warp's block][32-entry chunk]
   uint8_t list[kW][kBatch];          // per warp: its entries of the current batch, in order
 };
 
 // Expand this warp's flag words into its entry list (in order); returns the
 // count.  Warp-collective.
-template <int kW>
-__device__ __forceinline__ int build_list(TileWalkShared<kW>& sm, int buf, int warp, int lane, int start = 0) {
+template <int kW, int kVec>
+__device__ __forceinline__ int build_list(TileWalkShared<kW, kVec>& sm, int buf, int warp, int lane, int start = 0) {
   __syncwarp();  // the previous walk's reads of the list are done
   int count = 0;
   const uint32_t lt = (1u << lane) - 1u;
@@ -167,54 +173,22 @@ __device__ __forceinline__ int build_list(TileWalkShared<kW>& sm, int buf, int w
   return count;
 }
 
-// One entry's record held in registers between its gather and its store.
-struct Staged {
-  float4 r0, r1, r2, r3;
-  uint32_t id;
-  bool has;
-};
-
-// Gather entry `pos` of the point list (when `has`).  Records are four float4s;
-// r2.w and r3 hold the culling parameters (hy; beta, gamma, eps, vr).  Ids of
-// num_records or more are skipped (see chunk_load).
-__device__ __forceinline__ void stage_load(Staged& st, const float* record, const uint32_t* point_list, size_t pos,
-                                           bool has, uint32_t num_records) {
-  st.has = false;
-  if (has) {
-    st.id = point_list[pos];
-    st.has = st.id < num_records;
-  }
-  if (st.has) {
-    const float4* rec = reinterpret_cast<const float4*>(record);
-    const float4* r = rec + 4 * size_t(st.id);
-    st.r0 = __ldg(r);
-    st.r1 = __ldg(r + 1);
-    st.r2 = __ldg(r + 2);
-    st.r3 = __ldg(r + 3);
-  }
-}
-
-// Store the staged entry j (slot j of the batch) into buffer `buf` and publish
-// the block masks of the CTA's kW blocks (the tile's blocks first_block ..
-// first_block + kW - 1).  Every thread of a warp must call this for the same
-// chunk (the ballots are full-warp).
-// The masks also go to global memory for the backward passes (BlockMasks):
-// bits 0-3 to lo_dst[j], bits 4-7 (eight-warp CTAs) to hi_dst[j], where the
-// callers offset the arrays to the batch's first list position.
-template <int kW>
-__device__ __forceinline__ void stage_store(TileWalkShared<kW>& sm, int buf, const Staged& st, int j, int X0, int Y0,
-                                            int first_block, uint8_t* lo_dst = nullptr, uint8_t* hi_dst = nullptr) {
+// Block bits of one entry for the CTA's kW blocks (the tile's blocks
+// first_block .. first_block + kW - 1), published as the CTA's ballot words of
+// slot j; the masks also go to global memory for the backward passes
+// (BlockMasks): bits 0-3 to lo_dst[j], bits 4-7 (eight-warp CTAs) to
+// hi_dst[j], where the callers offset the arrays to the batch's first list
+// position.  Every thread of a warp must call this for the same chunk (the
+// ballots are full-warp).
+template <int kW, int kVec>
+__device__ __forceinline__ void publish_mask(TileWalkShared<kW, kVec>& sm, int buf, bool has, float mx, float my,
+                                             float hy, float4 c, int j, int X0, int Y0, int first_block,
+                                             uint8_t* lo_dst, uint8_t* hi_dst) {
   const int lane = j & 31, chunk = j >> 5;
   uint32_t mask = 0;
-  if (st.has) {
-    float4* s = &sm.rec[buf][kRecVec * j];
-    s[0] = st.r0;
-    s[1] = st.r1;
-    s[2] = st.r2;
-    sm.id[buf][j] = st.id;
+  if (has) {
     // the CTA's blocks are kW / 2 rows of two, starting at row group first_block / 2
-    mask = block_mask<kW / 2>(st.r0.x, st.r0.y, st.r2.w, st.r3.x, st.r3.y, st.r3.z, st.r3.w, X0,
-                              Y0 + kBlockH * (first_block / 2));
+    mask = block_mask<kW / 2>(mx, my, hy, c.x, c.y, c.z, c.w, X0, Y0 + kBlockH * (first_block / 2));
     if (lo_dst != nullptr) lo_dst[j] = uint8_t(mask & 15u);
     if (hi_dst != nullptr) hi_dst[j] = uint8_t(mask >> 4);
   }
@@ -225,6 +199,85 @@ __device__ __forceinline__ void stage_store(TileWalkShared<kW>& sm, int buf, con
     if (lane == b) mine = w;
   }
   if (lane < kW) sm.bal[buf][lane][chunk] = mine;
+}
+
+// One entry's record held in registers between its gather and its store.
+struct Staged {
+  float4 r0, r1, r2, r3;
+  bool has;
+};
+
+// Gather entry `pos` of the point list (when `has`) into registers.  Records
+// are four float4s; r2.w and r3 hold the culling parameters (hy; beta, gamma,
+// eps, vr).  Ids of num_records or more are skipped (see chunk_load).
+__device__ __forceinline__ void stage_load(Staged& st, const float* record, const uint32_t* point_list, size_t pos,
+                                           bool has, uint32_t num_records) {
+  st.has = false;
+  uint32_t id = 0;
+  if (has) {
+    id = point_list[pos];
+    st.has = id < num_records;
+  }
+  if (st.has) {
+    const float4* r = reinterpret_cast<const float4*>(record) + 4 * size_t(id);
+    st.r0 = __ldg(r);
+    st.r1 = __ldg(r + 1);
+    st.r2 = __ldg(r + 2);
+    st.r3 = __ldg(r + 3);
+  }
+}
+
+// Store the gathered entry j (slot j of the batch) into buffer `buf` and
+// publish its block masks (publish_mask).
+template <int kW>
+__device__ __forceinline__ void stage_store(TileWalkShared<kW, kRecVec>& sm, int buf, const Staged& st, int j, int X0,
+                                            int Y0, int first_block, uint8_t* lo_dst, uint8_t* hi_dst) {
+  if (st.has) {
+    float4* s = &sm.rec[buf][kRecVec * j];
+    s[0] = st.r0;
+    s[1] = st.r1;
+    s[2] = st.r2;
+  }
+  publish_mask(sm, buf, st.has, st.r0.x, st.r0.y, st.r2.w, st.r3, j, X0, Y0, first_block, lo_dst, hi_dst);
+}
+
+__device__ __forceinline__ void cp_async16(void* smem_dst, const void* gmem_src) {
+  const uint32_t d = static_cast<uint32_t>(__cvta_generic_to_shared(smem_dst));
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(gmem_src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+// This thread's copies have landed (and are visible to it).
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
+
+// Start the copy of entry `pos` of the point list (when `has`) into slot
+// `dst` (kStageVec float4s); returns whether the slot will hold a record.
+// Ids of num_records or more are skipped.  The caller commits the group.
+__device__ __forceinline__ bool stage_copy(float4* dst, const float* record, const uint32_t* point_list, size_t pos,
+                                           bool has, uint32_t num_records) {
+  if (!has) return false;
+  const uint32_t id = point_list[pos];
+  if (id >= num_records) return false;
+  const float4* r = reinterpret_cast<const float4*>(record) + 4 * size_t(id);
+#pragma unroll
+  for (int u = 0; u < kStageVec; ++u) cp_async16(dst + u, r + u);
+  return true;
+}
+
+// Publish the block masks of copied entry j (slot j of buffer `buf`, copied
+// by this thread, whose copies have landed).
+template <int kW>
+__device__ __forceinline__ void stage_mask(TileWalkShared<kW, kStageVec>& sm, int buf, bool has, int j, int X0,
+                                           int Y0, int first_block, uint8_t* lo_dst, uint8_t* hi_dst) {
+  float2 m = make_float2(0.f, 0.f);
+  float hy = 0.f;
+  float4 c = make_float4(0.f, 0.f, 0.f, 0.f);
+  if (has) {
+    const float4* s = &sm.rec[buf][kStageVec * j];
+    m = *reinterpret_cast<const float2*>(s);
+    hy = s[2].w;
+    c = s[3];
+  }
+  publish_mask(sm, buf, has, m.x, m.y, hy, c, j, X0, Y0, first_block, lo_dst, hi_dst);
 }
 
 }  // namespace w2w

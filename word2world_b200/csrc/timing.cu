@@ -72,12 +72,15 @@ uint32_t spin_limit() { return g_spin_limit.load(std::memory_order_relaxed); }
 namespace {
 const char* kTuneNames[kNumTuneKnobs] = {"blend_warps", "backward_split", "backward_ways",
                                          "binning",     "blend_queue",    "preprocess_blocks",
-                                         "planned_forward"};
+                                         "planned_forward", "blend_stage"};
 // defaults: 4-warp blend CTAs, the heaviest half-SM-count tiles' backward
 // walks split in two (backward_split 2 measured 3.09 against 3.21 ms per 4-view
 // step for 4, same B200), radix sort, per-tile blend, 4 projection CTAs per SM,
-// planned forward on
-std::atomic<int> g_tune[kNumTuneKnobs] = {{4}, {2}, {2}, {0}, {0}, {4}, {1}};
+// planned forward on, blend batches copied with cp.async (five 4-warp CTAs per
+// SM: 1416-1423 against 1388-1396 views/s for the 4-view step with the views
+// on their own streams; alone the kernel takes 0.218 against 0.199 ms, so a
+// single-stream caller's autotuning may pick 0)
+std::atomic<int> g_tune[kNumTuneKnobs] = {{4}, {2}, {2}, {0}, {0}, {4}, {1}, {1}};
 bool tune_valid(int knob, int v) {
   switch (knob) {
     case kTuneBlendWarps: return v == 4 || v == 8;
@@ -87,6 +90,7 @@ bool tune_valid(int knob, int v) {
     case kTuneBlendQueue: return v == 0 || v == 1;
     case kTunePreBlocks: return v >= 2 && v <= 4;
     case kTunePlanned: return v == 0 || v == 1;
+    case kTuneBlendStage: return v == 0 || v == 1;
     default: return false;
   }
 }
