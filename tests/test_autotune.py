@@ -30,6 +30,8 @@ def test_knob_setter_validates(restore):
         _C.tune_set("blend_warps", 5)
     with pytest.raises(ValueError):
         _C.tune_set("no_such_knob", 1)
+    with pytest.raises(ValueError):
+        _C.tune_set("blend_stage", 2)  # 0: records gathered into registers, 1: copied by cp.async
     assert autotune.current() == knobs
     prev = autotune.apply({"backward_ways": 3})
     assert prev == {"backward_ways": knobs["backward_ways"]} and autotune.current()["backward_ways"] == 3

@@ -87,3 +87,27 @@ def test_planned_layout_helpers(lib):
             planned = lib.w2w_binning_state_bytes(C, W, H)
             assert lib.w2w_binning_layout_count(R, planned, W, H) == C
             assert lib.w2w_binning_layout_count(R, planned + 256, W, H) == -1
+
+
+def test_tuning_knobs_through_the_c_abi(lib):
+    """Every knob the header documents is named by the library, the autotuner
+    tunes all but planned_forward, and an invalid value changes nothing."""
+    lib.w2w_tune_name.restype = ctypes.c_char_p
+    names = [lib.w2w_tune_name(k).decode() for k in range(lib.w2w_tune_count())]
+    assert names == ["blend_warps", "backward_split", "backward_ways", "binning", "blend_queue",
+                     "preprocess_blocks", "planned_forward", "blend_stage"]
+    text = " ".join(re.sub(r"\n\s*\*(?!/)", " ", open(HEADER).read()).split())  # comment text, one line
+    for k, n in enumerate(names):
+        assert f'{k} "{n}"' in text, n  # documented with its number
+    assert lib.w2w_tune_name(len(names)) == b""
+    stage = names.index("blend_stage")
+    before = lib.w2w_tune_get(stage)
+    assert before in (0, 1)
+    assert lib.w2w_tune_set(stage, 2) == -1 and lib.w2w_tune_get(stage) == before
+    assert lib.w2w_tune_set(stage, 1 - before) == before and lib.w2w_tune_get(stage) == 1 - before
+    assert lib.w2w_tune_set(stage, before) == 1 - before
+    try:
+        from word2world_b200 import autotune
+    except ImportError:  # the torch extension is not built: the library part above still ran
+        return
+    assert set(autotune.CANDIDATES) == set(names) - {"planned_forward"}
