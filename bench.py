@@ -987,12 +987,13 @@ def run_reference(a):
     path is the oracle (a restatement of the reference's arithmetic) run on
     every host core (one process per view, the cores split among them as
     threads).  Each step renders and back-propagates all views of the
-    workload.  The timed steps stop early, with the count reported, once
-    150 s have passed, so the run ends within a few minutes."""
+    workload.  The requested warm-up steps run first (at least one, at most
+    ten); the timed steps stop early, with the count reported, once 150 s
+    have passed, so the run ends within a few minutes."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    warm = max(1, min(a.warmup, 1))
+    warm = max(1, min(a.warmup, 10))
     steps, dt, procs, threads = _cpu_steps(a, 150.0, a.steps, warm=warm)
     value = a.views * steps / dt
     note = "" if steps == a.steps else f" (stopped after {steps} of {a.steps} steps at the 150 s bound)"
