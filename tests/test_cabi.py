@@ -111,3 +111,27 @@ def test_tuning_knobs_through_the_c_abi(lib):
     except ImportError:  # the torch extension is not built: the library part above still ran
         return
     assert set(autotune.CANDIDATES) == set(names) - {"planned_forward"}
+
+
+class _GeomInfo(ctypes.Structure):
+    _fields_ = [("num_rendered", ctypes.c_longlong), ("depth_min_bits", ctypes.c_uint32),
+                ("depth_max_bits", ctypes.c_uint32), ("error", ctypes.c_uint32), ("reserved", ctypes.c_uint32)]
+
+
+def test_planned_header_decoding(lib):
+    """The host half of the planned forward: decoding the 16 header bytes the
+    projection pass copies out (error word, complemented minimum and maximum
+    of the depth bit patterns, instance count) and the key depth bits a view
+    needs (the span of its depth patterns: the bits below their common
+    prefix)."""
+    import struct
+    decode = lib.w2w_geometry_info_from_header
+    need = lib.w2w_depth_bits_needed
+    info = _GeomInfo()
+    for err, lo, hi, R, status in ((0, 0x3F000000, 0x3F01FFFF, 5923615, 0), (1, 7, 7, 3, 3), (2, 1, 2, 9, 4),
+                                   (3, 0, 0, 0, 4), (4, 0, 0xFFFFFFFF, 1 << 29, 0)):
+        hdr = ctypes.create_string_buffer(struct.pack("<4I", err, (~lo) & 0xFFFFFFFF, hi, R), 16)
+        assert decode(hdr, ctypes.byref(info)) == status, (err, status)  # timeout wins over capacity
+        assert (info.error, info.depth_min_bits, info.depth_max_bits, info.num_rendered) == (err, lo, hi, R)
+        assert need(ctypes.byref(info)) == (lo ^ hi).bit_length()
+    assert decode(None, ctypes.byref(info)) == 1 and need(None) == -1
