@@ -120,3 +120,36 @@ def test_finite_differences_exact_mode():
             assert abs(fd - an) <= 1e-3 * max(1.0, abs(fd)), (name, idx, fd, an)
             checked += 1
     assert checked >= 15
+
+
+@pytest.mark.parametrize("case", ["empty", "culled", "one"])
+def test_empty_culled_and_single_inputs(case):
+    """The oracle on the edge inputs the GPU tests hand it: no Gaussians, every
+    Gaussian at the camera centre (culled by the near test), one Gaussian.
+    Nothing rendered leaves the background, zero contributor counts,
+    transmittance one and zero gradients; one Gaussian gives a sorted list of
+    its own tiles."""
+    P = {"empty": 0, "culled": 500, "one": 1}[case]
+    sc = scenes.make_scene(P, seed=9)
+    m, o, s, q, sh = sc.activate()
+    cam = camera.orbit_camera(30.0, 10.0, 2.5, 64, 48)
+    if case == "culled":
+        m = np.repeat(-np.asarray(cam.campos, np.float32)[None], P, axis=0)
+    st = oracle.RasterSettings.from_camera(cam, bg=(0.25, 0.5, 1.0))
+    f = oracle.forward(st, m, s, q, o, sh)
+    g = np.random.default_rng(4).normal(size=(3, 48, 64)).astype(np.float32)
+    b = oracle.backward(f, g)
+    if case != "one":
+        assert f["num_rendered"] == 0 and np.all(np.asarray(f["radii"]) == 0)
+        assert np.array_equal(np.asarray(f["color"]), np.broadcast_to(np.float32([0.25, 0.5, 1.0])[:, None, None],
+                                                                        (3, 48, 64)))
+        assert np.all(np.asarray(f["n_contrib"]) == 0) and np.all(np.asarray(f["alpha"]) == 0)
+        for k, v in b.items():
+            if k.startswith(("dL_", "abs_")):  # every gradient and its sum of |terms|
+                assert not np.any(np.asarray(v)), k
+        return
+    R = f["num_rendered"]
+    assert R == int(np.asarray(f["tiles"])[0]) > 0
+    keys = np.asarray(f["keys"])[:R]
+    assert np.all(np.diff(keys.astype(np.int64)) > 0)  # one Gaussian: distinct tiles, ascending
+    assert np.all(np.asarray(f["point_list"])[:R] == 0)
