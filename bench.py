@@ -397,7 +397,8 @@ def run_ours(a):
     pairs = statistics.mean(p["pairs"] for p in plans)
     kb = 8 if any(p["key64"] for p in plans) else 4
     alg_bytes = {
-        # projection + SH read, geometry state written (the survey's 323 B per Gaussian per view)
+        # projection + SH read, geometry state written: the 323 B per Gaussian per view the
+        # reference's preprocess must move (parameters and SH in, its geometry buffers out)
         "preprocess": P * 323,
         # the depth order: one 4-byte key and id read and written per digit pass, a histogram read,
         # the owned-count gather (id, offset, count, rectangle, reach read; count written)
