@@ -135,3 +135,21 @@ def test_planned_header_decoding(lib):
         assert (info.error, info.depth_min_bits, info.depth_max_bits, info.num_rendered) == (err, lo, hi, R)
         assert need(ctypes.byref(info)) == (lo ^ hi).bit_length()
     assert decode(None, ctypes.byref(info)) == 1 and need(None) == -1
+
+
+def test_knob_defaults_match_the_header(lib):  # the fixture builds the library when absent
+    """A freshly loaded library's knob values are the defaults the header
+    documents (read in a child process, so no earlier test's setting leaks)."""
+    import subprocess
+    import sys
+    text = " ".join(re.sub(r"\n\s*\*(?!/)", " ", open(HEADER).read()).split())
+    doc = text[text.index("---- launch-shape tuning"):]
+    code = ("import ctypes,sys; L=ctypes.CDLL(sys.argv[1]); L.w2w_tune_name.restype=ctypes.c_char_p; "
+            "print(';'.join(f'{L.w2w_tune_name(k).decode()}={L.w2w_tune_get(k)}' for k in range(L.w2w_tune_count())))")
+    out = subprocess.run([sys.executable, "-c", code, LIB], capture_output=True, text=True, timeout=120)
+    assert out.returncode == 0, out.stderr
+    values = dict(kv.split("=") for kv in out.stdout.strip().split(";"))
+    for k, (name, v) in enumerate(values.items()):
+        start = doc.index(f'{k} "{name}"')
+        m = re.compile(r"default (\d+)").search(doc, start)
+        assert m is not None and int(m.group(1)) == int(v), (name, v, m and m.group(0))
