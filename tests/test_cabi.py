@@ -153,3 +153,43 @@ def test_knob_defaults_match_the_header(lib):  # the fixture builds the library 
         start = doc.index(f'{k} "{name}"')
         m = re.compile(r"default (\d+)").search(doc, start)
         assert m is not None and int(m.group(1)) == int(v), (name, v, m and m.group(0))
+
+
+C_HOST = r"""
+#include "w2w_raster.h"
+#include <stdio.h>
+int main(void) {
+  w2w_geometry_info info = {0};
+  const unsigned char hdr[16] = {0};
+  if (w2w_geometry_info_from_header(hdr, &info) != W2W_OK || info.num_rendered != 0) return 2;
+  printf("%d %zu %lld %d", w2w_version(), w2w_geometry_state_bytes(1000), w2w_planned_capacity(100000),
+         w2w_tune_count());
+  for (int k = 0; k < w2w_tune_count(); ++k) printf(" %s", w2w_tune_name(k));
+  printf("\n");
+  return 0;
+}
+"""
+
+
+def test_plain_c_host_compiles_links_and_runs(lib, tmp_path):
+    """The header is C99 (no C++), and a C host links the library and calls its
+    host-only entry points: what a cgo / JNI / N-API shim builds on."""
+    import shutil
+    import subprocess
+    gcc = shutil.which("gcc")
+    if gcc is None:
+        pytest.skip("no C compiler")
+    src = tmp_path / "host.c"
+    src.write_text(C_HOST)
+    exe = tmp_path / "host"
+    libdir = os.path.dirname(LIB)
+    r = subprocess.run([gcc, "-std=c99", "-Wall", "-Wextra", "-pedantic", "-Werror", "-I", os.path.dirname(HEADER),
+                        str(src), "-L", libdir, "-lw2w_raster", f"-Wl,-rpath,{libdir}", "-o", str(exe)],
+                       capture_output=True, text=True, timeout=120)
+    assert r.returncode == 0, r.stderr
+    r = subprocess.run([str(exe)], capture_output=True, text=True, timeout=60)
+    assert r.returncode == 0, (r.returncode, r.stderr)
+    out = r.stdout.split()
+    lib.w2w_tune_name.restype = ctypes.c_char_p
+    assert int(out[0]) == lib.w2w_version() and int(out[3]) == lib.w2w_tune_count()
+    assert out[4:] == [lib.w2w_tune_name(k).decode() for k in range(lib.w2w_tune_count())]
