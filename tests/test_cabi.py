@@ -113,6 +113,14 @@ def test_tuning_knobs_through_the_c_abi(lib):
     assert set(autotune.CANDIDATES) == set(names) - {"planned_forward"}
 
 
+class _Settings(ctypes.Structure):  # w2w_settings, field for field
+    _fields_ = [("P", ctypes.c_int), ("degree", ctypes.c_int), ("M", ctypes.c_int), ("width", ctypes.c_int),
+                ("height", ctypes.c_int), ("focal_x", ctypes.c_float), ("tan_fovx", ctypes.c_float),
+                ("tan_fovy", ctypes.c_float), ("scale_modifier", ctypes.c_float), ("compat_spill", ctypes.c_int),
+                ("viewmatrix", ctypes.c_void_p), ("projmatrix", ctypes.c_void_p), ("campos", ctypes.c_void_p),
+                ("background", ctypes.c_void_p)]
+
+
 class _GeomInfo(ctypes.Structure):
     _fields_ = [("num_rendered", ctypes.c_longlong), ("depth_min_bits", ctypes.c_uint32),
                 ("depth_max_bits", ctypes.c_uint32), ("error", ctypes.c_uint32), ("reserved", ctypes.c_uint32)]
@@ -157,8 +165,13 @@ def test_knob_defaults_match_the_header(lib):  # the fixture builds the library 
 
 C_HOST = r"""
 #include "w2w_raster.h"
+#include <stddef.h>
 #include <stdio.h>
 int main(void) {
+  /* the structs' layout, as an FFI binding declares it */
+  fprintf(stderr, "%zu %zu %zu %zu %zu %zu\n", sizeof(w2w_settings), offsetof(w2w_settings, compat_spill),
+          offsetof(w2w_settings, viewmatrix), offsetof(w2w_settings, background), sizeof(w2w_geometry_info),
+          offsetof(w2w_geometry_info, reserved));
   w2w_geometry_info info = {0};
   const unsigned char hdr[16] = {0};
   if (w2w_geometry_info_from_header(hdr, &info) != W2W_OK || info.num_rendered != 0) return 2;
@@ -190,6 +203,10 @@ def test_plain_c_host_compiles_links_and_runs(lib, tmp_path):
     r = subprocess.run([str(exe)], capture_output=True, text=True, timeout=60)
     assert r.returncode == 0, (r.returncode, r.stderr)
     out = r.stdout.split()
+    layout = [int(x) for x in r.stderr.split()]
+    S = _Settings
+    assert layout == [ctypes.sizeof(S), S.compat_spill.offset, S.viewmatrix.offset, S.background.offset,
+                      ctypes.sizeof(_GeomInfo), _GeomInfo.reserved.offset]
     lib.w2w_tune_name.restype = ctypes.c_char_p
     assert int(out[0]) == lib.w2w_version() and int(out[3]) == lib.w2w_tune_count()
     assert out[4:] == [lib.w2w_tune_name(k).decode() for k in range(lib.w2w_tune_count())]
